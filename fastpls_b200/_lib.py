@@ -1,0 +1,360 @@
+"""ctypes binding of libfastpls_b200.so (C ABI in include/fastpls_b200.h).
+
+Each wrapper mirrors one `.Call` routine of the R package fastPLS used with
+backend = "cuda" and returns the same fields as the reference's R list.  There
+is no fallback: if the library or a B200 device is missing, calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfastpls_b200.so")
+
+_c_double_p = ctypes.POINTER(ctypes.c_double)
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_lib = None
+
+FPLS_ERRORS = {1: "argument", 2: "cuda", 3: "numerical", 4: "no_device", 5: "internal"}
+
+
+class FastPLSError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"fastpls_b200 [{FPLS_ERRORS.get(code, code)}]: {msg}")
+        self.code = code
+
+
+# name -> argtypes (restype int unless noted)
+_D, _I, _DP, _IP, _S, _C = (ctypes.c_double, ctypes.c_int, _c_double_p, _c_int_p,
+                            ctypes.c_size_t, ctypes.c_char_p)
+SIGNATURES = {
+    "fpls_has_cuda": ([], ctypes.c_int),
+    "fpls_version": ([], ctypes.c_char_p),
+    "fpls_reset_workspace": ([_C, _S], ctypes.c_int),
+    "fpls_matrix_multiply": ([_DP, _I, _I, _DP, _I, _DP, _C, _S], ctypes.c_int),
+    "fpls_truncated_svd": ([_DP, _I, _I, _I, _I, _I, _I, _D, _I, _I, _DP, _DP, _DP, _IP, _C, _S],
+                           ctypes.c_int),
+    "fpls_pls_model1": ([_DP, _I, _I, _DP, _I, _IP, _I, _I, _I, _I, _I, _I, _D, _I, _IP, _DP,
+                         _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S],
+                        ctypes.c_int),
+    "fpls_pls_model2_fast": ([_DP, _I, _I, _DP, _I, _IP, _I, _I, _I, _I, _DP, _DP, _DP, _DP, _DP,
+                              _DP, _DP, _DP, _IP, _C, _S], ctypes.c_int),
+    "fpls_pls_model2": ([_DP, _I, _I, _DP, _I, _IP, _I, _I, _I, _I, _I, _I, _D, _I, _DP, _DP,
+                         _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S], ctypes.c_int),
+    "fpls_predict_lowrank": ([_DP, _I, _I, _DP, _DP, _DP, _I, _DP, _I, _DP, _IP, _I, _DP, _DP,
+                              _C, _S], ctypes.c_int),
+    "fpls_predict_classes": ([_DP, _I, _I, _DP, _DP, _DP, _I, _DP, _I, _DP, _IP, _I, _DP, _I,
+                              _IP, _DP, _C, _S], ctypes.c_int),
+    "fpls_lda_train_prefix": ([_DP, _I, _I, _IP, _I, _IP, _I, _D, _DP, _DP, _DP, _DP, _DP, _C,
+                               _S], ctypes.c_int),
+    "fpls_lda_project_train_prefix": ([_DP, _I, _I, _DP, _I, _DP, _IP, _I, _IP, _I, _D, _DP, _DP,
+                                       _DP, _DP, _DP, _C, _S], ctypes.c_int),
+    "fpls_lda_predict": ([_DP, _I, _I, _DP, _DP, _I, _IP, _DP, _C, _S], ctypes.c_int),
+    "fpls_lda_project_predict": ([_DP, _I, _I, _DP, _I, _DP, _DP, _DP, _I, _IP, _DP, _C, _S],
+                                 ctypes.c_int),
+}
+
+
+def load():
+    """Loads the library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m fastpls_b200.build` "
+                "(there is no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (argtypes, restype) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = argtypes
+            fn.restype = restype
+        _lib = lib
+    return _lib
+
+
+def exported_symbols():
+    return sorted(SIGNATURES)
+
+
+def has_cuda():
+    return bool(load().fpls_has_cuda())
+
+
+def version():
+    return load().fpls_version().decode()
+
+
+# ---------------------------------------------------------------- helpers ---
+def _f64(a, shape=None):
+    a = np.asarray(a, dtype=np.float64)
+    if shape is not None:
+        a = a.reshape(shape)
+    return np.asfortranarray(a)
+
+
+def _i32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32).ravel())
+
+
+def _p(a):
+    if a is None:
+        return None
+    if a.dtype == np.int32:
+        return a.ctypes.data_as(_c_int_p)
+    return a.ctypes.data_as(_c_double_p)
+
+
+def _out(*shape):
+    return np.zeros(shape, dtype=np.float64, order="F")
+
+
+def _call(name, *args):
+    err = ctypes.create_string_buffer(1024)
+    rc = getattr(load(), name)(*args, err, ctypes.sizeof(err))
+    if rc != 0:
+        raise FastPLSError(rc, err.value.decode(errors="replace"))
+
+
+def reset_workspace():
+    _call("fpls_reset_workspace")
+
+
+# -------------------------------------------------------------- wrappers ---
+def matrix_multiply(A, B):
+    A = _f64(A)
+    B = _f64(B)
+    C = _out(A.shape[0], B.shape[1])
+    _call("fpls_matrix_multiply", _p(A), A.shape[0], A.shape[1], _p(B), B.shape[1], _p(C))
+    return C
+
+
+def truncated_svd(A, k, svd_method=4, oversample=10, power_iters=1, svds_tol=0.0, seed=1,
+                  left_only=False):
+    A = _f64(A)
+    rows, cols = A.shape
+    kcap = min(rows, cols, max(int(k), 1))
+    U = _out(rows, kcap)
+    s = np.zeros(kcap)
+    Vt = None if left_only else _out(kcap, cols)
+    rank = ctypes.c_int(0)
+    _call("fpls_truncated_svd", _p(A), rows, cols, int(k), int(svd_method), int(oversample),
+          int(power_iters), float(svds_tol), int(seed), int(bool(left_only)), _p(U), _p(s),
+          _p(Vt), ctypes.byref(rank))
+    r = rank.value
+    return dict(u=U[:, :r], d=s[:r], vt=None if Vt is None else Vt[:r, :])
+
+
+def pls_model1(X, Y, ncomp, scaling=1, fit=False, svd_method=4, oversample=10, power_iters=1,
+               svds_tol=0.0, seed=1, store_B=True):
+    X = _f64(X)
+    Y = _f64(Y)
+    n, p = X.shape
+    m = Y.shape[1]
+    nc = _i32(np.atleast_1d(ncomp))
+    L = nc.size
+    max_rank = min(n, p, m)
+    K0 = min(int(np.clip(nc, 1, max_rank).max()), max_rank)
+    out = dict(C_latent=_out(K0, K0, L), W_latent=_out(K0, m, L), Q=_out(m, K0), Ttrain=_out(n, K0),
+               R=_out(p, K0), mX=_out(1, p), vX=_out(1, p), mY=_out(1, m),
+               B=_out(p, m, L) if store_B else None, Yfit=_out(n, m, L) if fit else None,
+               R2Y=np.zeros(L), singular_values=np.zeros(K0))
+    nco = np.zeros(L, dtype=np.int32)
+    keff = ctypes.c_int(0)
+    _call("fpls_pls_model1", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
+          int(svd_method), int(oversample), int(power_iters), float(svds_tol), int(seed), _p(nco),
+          _p(out["C_latent"]), _p(out["W_latent"]), _p(out["Q"]), _p(out["Ttrain"]), _p(out["R"]),
+          _p(out["mX"]), _p(out["vX"]), _p(out["mY"]), _p(out["B"]), _p(out["Yfit"]),
+          _p(out["R2Y"]), _p(out["singular_values"]), ctypes.byref(keff))
+    k = keff.value
+    out["R"] = out["R"][:, :k]
+    out["Q"] = out["Q"][:, :k]
+    out["Ttrain"] = out["Ttrain"][:, :k]
+    out["singular_values"] = out["singular_values"][:k]
+    out.update(ncomp=nco, p=p, m=m, pls_method="plssvd", B_stored=bool(store_B),
+               compact_prediction=not store_B)
+    if not store_B:
+        out.pop("B")
+    return out
+
+
+def pls_model2_fast(X, Y, ncomp, scaling=1, fit=False, seed=1, store_B=True):
+    X = _f64(X)
+    Y = _f64(Y)
+    n, p = X.shape
+    m = Y.shape[1]
+    nc = _i32(np.maximum(np.atleast_1d(ncomp), 1))
+    L = nc.size
+    K = int(nc.max())
+    out = dict(R=_out(p, K), Q=_out(m, K), mX=_out(1, p), vX=_out(1, p), mY=_out(1, m),
+               B=_out(p, m, L) if store_B else None, Yfit=_out(n, m, L) if fit else None,
+               R2Y=np.zeros(L))
+    ncmp = ctypes.c_int(0)
+    _call("fpls_pls_model2_fast", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
+          int(seed), _p(out["R"]), _p(out["Q"]), _p(out["mX"]), _p(out["vX"]), _p(out["mY"]),
+          _p(out["B"]), _p(out["Yfit"]), _p(out["R2Y"]), ctypes.byref(ncmp))
+    out.update(ncomp=nc, p=p, m=m, pls_method="simpls", n_components=ncmp.value,
+               B_stored=bool(store_B), compact_prediction=not store_B)
+    if not store_B:
+        out.pop("B")
+    return out
+
+
+def pls_model2(X, Y, ncomp, scaling=1, fit=False, svd_method=3, oversample=10, power_iters=1,
+               svds_tol=0.0, seed=1, store_B=True):
+    X = _f64(X)
+    Y = _f64(Y)
+    n, p = X.shape
+    m = Y.shape[1]
+    nc = _i32(np.atleast_1d(ncomp))
+    L = nc.size
+    K = int(nc.max())
+    out = dict(R=_out(p, K), Q=_out(m, K), P=_out(p, K), Ttrain=_out(n, K), mX=_out(1, p),
+               vX=_out(1, p), mY=_out(1, m), B=_out(p, m, L) if store_B else None,
+               Yfit=_out(n, m, L) if fit else None, R2Y=np.zeros(L))
+    ncmp = ctypes.c_int(0)
+    _call("fpls_pls_model2", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
+          int(svd_method), int(oversample), int(power_iters), float(svds_tol), int(seed),
+          _p(out["R"]), _p(out["Q"]), _p(out["P"]), _p(out["Ttrain"]), _p(out["mX"]),
+          _p(out["vX"]), _p(out["mY"]), _p(out["B"]), _p(out["Yfit"]), _p(out["R2Y"]),
+          ctypes.byref(ncmp))
+    out.update(ncomp=nc, p=p, m=m, pls_method="simpls", n_components=ncmp.value,
+               B_stored=bool(store_B), compact_prediction=not store_B)
+    if not store_B:
+        out.pop("B")
+    return out
+
+
+def compact_weights(model):
+    """Per-slice latent weights (kmax x m x L) as compact_prediction_weights
+    (src/fastPLS.cpp:3737-3836)."""
+    R = model["R"]
+    kmax = R.shape[1]
+    m = int(model["m"])
+    nc = np.atleast_1d(model["ncomp"])
+    L = nc.size
+    W = np.zeros((kmax, m, L), order="F")
+    if model["pls_method"] in ("simpls", "simpls_fast"):
+        Q = model["Q"]
+        for a in range(L):
+            mc = int(nc[a])
+            W[:mc, :, a] = Q[:, :mc].T
+    elif "W_latent" in model:
+        Wl = model["W_latent"]
+        W[:, :, :] = Wl[:kmax, :, :L]
+    else:
+        C = model["C_latent"]
+        Q = model["Q"]
+        for a in range(L):
+            mc = int(nc[a])
+            W[:mc, :, a] = C[:mc, :mc, a] @ Q[:, :mc].T
+    return W
+
+
+def predict_lowrank(model, Xtest, proj=False):
+    Xt = _f64(Xtest)
+    w, p = Xt.shape
+    R = _f64(model["R"])
+    kmax = R.shape[1]
+    W = _f64(compact_weights(model))
+    m = int(model["m"])
+    nc = _i32(np.minimum(np.atleast_1d(model["ncomp"]), kmax))
+    L = nc.size
+    Yp = _out(w, m, L)
+    T = _out(w, kmax) if proj else None
+    _call("fpls_predict_lowrank", _p(Xt), w, p, _p(_f64(model["mX"]).ravel()),
+          _p(_f64(model["vX"]).ravel()), _p(_f64(model["mY"]).ravel()), m, _p(R), kmax, _p(W),
+          _p(nc), L, _p(Yp), _p(T))
+    out = dict(Ypred=Yp)
+    if proj:
+        out["Ttest"] = T
+    return out
+
+
+def predict_classes(model, Xtest, class_bias=None, top_k=1, return_scores=False):
+    Xt = _f64(Xtest)
+    w, p = Xt.shape
+    R = _f64(model["R"])
+    kmax = R.shape[1]
+    W = _f64(compact_weights(model))
+    m = int(model["m"])
+    nc = _i32(np.minimum(np.atleast_1d(model["ncomp"]), kmax))
+    L = nc.size
+    idx = np.zeros((w, top_k, L), dtype=np.int32, order="F")
+    sc = _out(w, top_k, L) if return_scores else None
+    bias = None if class_bias is None else np.ascontiguousarray(class_bias, dtype=np.float64)
+    _call("fpls_predict_classes", _p(Xt), w, p, _p(_f64(model["mX"]).ravel()),
+          _p(_f64(model["vX"]).ravel()), _p(_f64(model["mY"]).ravel()), m, _p(R), kmax, _p(W),
+          _p(nc), L, _p(bias), int(top_k), idx.ctypes.data_as(_c_int_p), _p(sc))
+    return dict(top_index=idx, top_score=sc)
+
+
+def _lda_unpack(means, linear, constants, priors, lam, ncomp):
+    models = {}
+    for a, kk in enumerate(ncomp):
+        kk = int(kk)
+        models[str(kk)] = dict(means=means[:, :kk, a].copy(), linear=linear[:, :kk, a].copy(),
+                               constants=constants[:, a].copy(), priors=priors.copy(),
+                               ridge=float(lam[a]))
+    return models
+
+
+def lda_train_prefix(T, y, n_classes, ncomp, ridge=1e-8):
+    T = _f64(T)
+    n, kmax = T.shape
+    yy = _i32(y)
+    nc = _i32(np.atleast_1d(ncomp))
+    L = nc.size
+    km = int(nc.max())
+    C = int(n_classes)
+    means, linear = _out(C, km, L), _out(C, km, L)
+    constants, priors, lam = _out(C, L), np.zeros(C), np.zeros(L)
+    _call("fpls_lda_train_prefix", _p(T), n, kmax, _p(yy), C, _p(nc), L, float(ridge), _p(means),
+          _p(linear), _p(constants), _p(priors), _p(lam))
+    return _lda_unpack(means, linear, constants, priors, lam, nc)
+
+
+def lda_project_train_prefix(X, R, offset, y, n_classes, ncomp, ridge=1e-8):
+    X = _f64(X)
+    R = _f64(R)
+    n, p = X.shape
+    k = R.shape[1]
+    off = None if offset is None else np.ascontiguousarray(offset, dtype=np.float64).ravel()
+    yy = _i32(y)
+    nc = _i32(np.atleast_1d(ncomp))
+    L = nc.size
+    km = int(nc.max())
+    C = int(n_classes)
+    means, linear = _out(C, km, L), _out(C, km, L)
+    constants, priors, lam = _out(C, L), np.zeros(C), np.zeros(L)
+    _call("fpls_lda_project_train_prefix", _p(X), n, p, _p(R), k, _p(off), _p(yy), C, _p(nc), L,
+          float(ridge), _p(means), _p(linear), _p(constants), _p(priors), _p(lam))
+    return _lda_unpack(means, linear, constants, priors, lam, nc)
+
+
+def lda_predict(T, lda, return_scores=False):
+    T = _f64(T)
+    w, k = T.shape
+    lin = _f64(lda["linear"])
+    C = lin.shape[0]
+    const = np.ascontiguousarray(lda["constants"], dtype=np.float64).ravel()
+    lab = np.zeros(w, dtype=np.int32)
+    sc = _out(w, C) if return_scores else None
+    _call("fpls_lda_predict", _p(T), w, k, _p(lin), _p(const), C, _p(lab), _p(sc))
+    return dict(pred=lab, scores=sc) if return_scores else dict(pred=lab)
+
+
+def lda_project_predict(X, R, offset, lda, return_scores=False):
+    X = _f64(X)
+    R = _f64(R)
+    w, p = X.shape
+    k = R.shape[1]
+    lin = _f64(lda["linear"])
+    C = lin.shape[0]
+    const = np.ascontiguousarray(lda["constants"], dtype=np.float64).ravel()
+    off = None if offset is None else np.ascontiguousarray(offset, dtype=np.float64).ravel()
+    lab = np.zeros(w, dtype=np.int32)
+    sc = _out(w, C) if return_scores else None
+    _call("fpls_lda_project_predict", _p(X), w, p, _p(R), k, _p(off), _p(lin), _p(const), C,
+          _p(lab), _p(sc))
+    return dict(pred=lab, scores=sc) if return_scores else dict(pred=lab)

@@ -1,0 +1,434 @@
+#include "blas_f64.cuh"
+#include "context.cuh"
+
+namespace fpls {
+namespace {
+
+constexpr int BM = 64;
+constexpr int BN = 64;
+constexpr int BK = 16;
+constexpr int PAD = 4;  // row stride of 68 doubles keeps the DMMA fragment loads conflict-free
+constexpr int GEMM_THREADS = 128;
+
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// Tile loader: fetches the BK x BM slice of op(A) (or BK x BN of op(B)) for the
+// k-block starting at k0 into registers; out-of-range elements read as zero.
+template <bool KContig>
+__device__ __forceinline__ void load_tile(double (&r)[8], const double* __restrict__ P, int ld,
+                                          int mn0, int k0, int MN, int K, int kend) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int mn, k;
+    if (KContig) {  // element (mn, k) at P[k + mn*ld]
+      k = t & 15;
+      mn = (t >> 4) + 8 * i;
+    } else {        // element (mn, k) at P[mn + k*ld]
+      mn = t & 63;
+      k = (t >> 6) + 2 * i;
+    }
+    const int gm = mn0 + mn;
+    const int gk = k0 + k;
+    double v = 0.0;
+    if (gm < MN && gk < kend && gk < K) {
+      v = KContig ? __ldg(P + (size_t)gm * ld + gk) : __ldg(P + gm + (size_t)gk * ld);
+    }
+    r[i] = v;
+  }
+}
+
+template <bool KContig>
+__device__ __forceinline__ void store_tile(double (*S)[BM + PAD], const double (&r)[8]) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int mn, k;
+    if (KContig) {
+      k = t & 15;
+      mn = (t >> 4) + 8 * i;
+    } else {
+      mn = t & 63;
+      k = (t >> 6) + 2 * i;
+    }
+    S[k][mn] = r[i];
+  }
+}
+
+// op(A) (m,k): transA ? A[k + m*lda] : A[m + k*lda]   -> K-contiguous when transA
+// op(B) (k,n): transB ? B[n + k*ldb] : B[k + n*ldb]   -> K-contiguous when !transB
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(GEMM_THREADS)
+gemm_f64_dmma(int M, int N, int K, double alpha, const double* __restrict__ A, int lda,
+              const double* __restrict__ B, int ldb, double beta, double* __restrict__ C, int ldc,
+              int k_per_split, int use_atomic) {
+  __shared__ double As[2][BK][BM + PAD];
+  __shared__ double Bs[2][BK][BN + PAD];
+  const int bm = blockIdx.x * BM;
+  const int bn = blockIdx.y * BN;
+  const int kbeg = blockIdx.z * k_per_split;
+  const int kend = min(K, kbeg + k_per_split);
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int gid = lane >> 2;
+  const int tig = lane & 3;
+  const int wm = (warp & 1) * 32;
+  const int wn = (warp >> 1) * 32;
+
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  double ra[8], rb[8];
+  if (kbeg < kend) {
+    load_tile<TA>(ra, A, lda, bm, kbeg, M, K, kend);
+    load_tile<!TB>(rb, B, ldb, bn, kbeg, N, K, kend);
+    store_tile<TA>(As[0], ra);
+    store_tile<!TB>(Bs[0], rb);
+  }
+  __syncthreads();
+  int buf = 0;
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    const bool has_next = (k0 + BK) < kend;
+    if (has_next) {
+      load_tile<TA>(ra, A, lda, bm, k0 + BK, M, K, kend);
+      load_tile<!TB>(rb, B, ldb, bn, k0 + BK, N, K, kend);
+    }
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[buf][kk + tig][wm + i * 8 + gid];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk + tig][wn + j * 8 + gid];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+    if (has_next) {
+      store_tile<TA>(As[buf ^ 1], ra);
+      store_tile<!TB>(Bs[buf ^ 1], rb);
+    }
+    __syncthreads();
+    buf ^= 1;
+  }
+
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int m = bm + wm + i * 8 + gid;
+    if (m >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int n = bn + wn + j * 8 + tig * 2 + e;
+        if (n >= N) continue;
+        double* cp = C + m + (size_t)n * ldc;
+        const double v = alpha * acc[i][j][e];
+        if (use_atomic) {
+          atomicAdd(cp, v);
+        } else {
+          *cp = (beta == 0.0) ? v : (v + beta * *cp);
+        }
+      }
+    }
+  }
+}
+
+__global__ void scale_matrix_kernel(double* C, int M, int N, int ldc, double beta) {
+  const size_t total = (size_t)M * N;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int m = static_cast<int>(idx % M);
+    const int n = static_cast<int>(idx / M);
+    double* cp = C + m + (size_t)n * ldc;
+    *cp = (beta == 0.0) ? 0.0 : beta * *cp;
+  }
+}
+
+// y[m] = alpha * sum_k A[m + k*lda] x[k] (+ beta y) ; grid.y splits K, atomics combine.
+__global__ void gemv_n_kernel(int M, int K, double alpha, const double* __restrict__ A, int lda,
+                              const double* __restrict__ x, double* __restrict__ y,
+                              int k_per_split, int use_atomic, double beta) {
+  __shared__ double xs[256];
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int kbeg = blockIdx.y * k_per_split;
+  const int kend = min(K, kbeg + k_per_split);
+  double acc = 0.0;
+  for (int kc = kbeg; kc < kend; kc += 256) {
+    const int kn = min(256, kend - kc);
+    __syncthreads();
+    if (threadIdx.x < kn) xs[threadIdx.x] = x[kc + threadIdx.x];
+    __syncthreads();
+    if (m < M) {
+      const double* ap = A + m + (size_t)kc * lda;
+      int k = 0;
+      for (; k + 4 <= kn; k += 4) {
+        acc = fma(__ldg(ap + (size_t)k * lda), xs[k], acc);
+        acc = fma(__ldg(ap + (size_t)(k + 1) * lda), xs[k + 1], acc);
+        acc = fma(__ldg(ap + (size_t)(k + 2) * lda), xs[k + 2], acc);
+        acc = fma(__ldg(ap + (size_t)(k + 3) * lda), xs[k + 3], acc);
+      }
+      for (; k < kn; ++k) acc = fma(__ldg(ap + (size_t)k * lda), xs[k], acc);
+    }
+  }
+  if (m < M) {
+    if (use_atomic) atomicAdd(y + m, alpha * acc);
+    else y[m] = (beta == 0.0) ? alpha * acc : alpha * acc + beta * y[m];
+  }
+}
+
+// y[n] = alpha * sum_k A[k + n*lda] x[k] + beta y[n] ; one warp per column.
+__global__ void gemv_t_kernel(int K, int N, double alpha, const double* __restrict__ A, int lda,
+                              const double* __restrict__ x, double beta, double* __restrict__ y) {
+  const int warps_per_block = blockDim.x >> 5;
+  const int n = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (n >= N) return;
+  const double* ap = A + (size_t)n * lda;
+  double acc = 0.0;
+  for (int k = lane; k < K; k += 32) acc = fma(__ldg(ap + k), __ldg(x + k), acc);
+  acc = warp_sum(acc);
+  if (lane == 0) y[n] = (beta == 0.0) ? alpha * acc : alpha * acc + beta * y[n];
+}
+
+__global__ void col_mean_kernel(const double* __restrict__ X, int n, int p, int ldx,
+                                double* __restrict__ out) {
+  const int warps_per_block = blockDim.x >> 5;
+  const int j = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= p) return;
+  const double* xp = X + (size_t)j * ldx;
+  double s = 0.0;
+  for (int i = lane; i < n; i += 32) s += xp[i];
+  s = warp_sum(s);
+  if (lane == 0) out[j] = s / static_cast<double>(n);
+}
+
+__global__ void col_sd_kernel(const double* __restrict__ X, int n, int p, int ldx,
+                              double* __restrict__ out) {
+  const int warps_per_block = blockDim.x >> 5;
+  const int j = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= p) return;
+  const double* xp = X + (size_t)j * ldx;
+  // Two-pass (mean of the centred column, then squares) matches Welford to rounding.
+  double s = 0.0;
+  for (int i = lane; i < n; i += 32) s += xp[i];
+  s = warp_sum(s);
+  const double mu = s / static_cast<double>(n);
+  double q = 0.0;
+  for (int i = lane; i < n; i += 32) {
+    const double d = xp[i] - mu;
+    q += d * d;
+  }
+  q = warp_sum(q);
+  if (lane == 0) out[j] = sqrt(q / static_cast<double>(n - 1));
+}
+
+__global__ void center_scale_kernel(double* X, int n, int p, int ldx, const double* mean,
+                                    const double* scale) {
+  const size_t total = (size_t)n * p;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = static_cast<int>(idx % n);
+    const int j = static_cast<int>(idx / n);
+    double* xp = X + i + (size_t)j * ldx;
+    double v = *xp;
+    if (mean) v -= mean[j];
+    if (scale) v /= scale[j];
+    *xp = v;
+  }
+}
+
+__global__ void copy_matrix_kernel(double* dst, int ldd, const double* src, int lds, int n, int p) {
+  const size_t total = (size_t)n * p;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = static_cast<int>(idx % n);
+    const int j = static_cast<int>(idx / n);
+    dst[i + (size_t)j * ldd] = src[i + (size_t)j * lds];
+  }
+}
+
+__global__ void add_row_vector_kernel(double* X, int n, int p, int ldx, const double* v) {
+  const size_t total = (size_t)n * p;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = static_cast<int>(idx % n);
+    const int j = static_cast<int>(idx / n);
+    X[i + (size_t)j * ldx] += v[j];
+  }
+}
+
+__global__ void rq_sums_kernel(const double* __restrict__ Y, const double* __restrict__ Yp,
+                               int n, int m, double* out2) {
+  __shared__ double scratch[32];
+  double press = 0.0, tss = 0.0;
+  for (int j = 0; j < m; ++j) {
+    const double* yc = Y + (size_t)j * n;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += yc[i];
+    s = block_sum(s, scratch);
+    const double mu = s / static_cast<double>(n);
+    const double* pc = Yp + (size_t)j * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const double d = yc[i] - pc[i];
+      const double e = yc[i] - mu;
+      press += d * d;
+      tss += e * e;
+    }
+  }
+  press = block_sum(press, scratch);
+  tss = block_sum(tss, scratch);
+  if (threadIdx.x == 0) {
+    out2[0] = press;
+    out2[1] = tss;
+  }
+}
+
+__global__ void fill_kernel(double* x, size_t n, double v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+__global__ void scale_vec_kernel(double* x, size_t n, double a) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] *= a;
+}
+
+int grid_for(size_t total, int threads) {
+  size_t g = (total + threads - 1) / threads;
+  const size_t cap = (size_t)kSMCount * 16;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return static_cast<int>(g);
+}
+
+}  // namespace
+
+void gemm(bool transA, bool transB, int M, int N, int K, double alpha, const double* A, int lda,
+          const double* B, int ldb, double beta, double* C, int ldc) {
+  if (M <= 0 || N <= 0) return;
+  cudaStream_t st = Context::get().stream;
+  if (K <= 0) {
+    scale_matrix_kernel<<<grid_for((size_t)M * N, 256), 256, 0, st>>>(C, M, N, ldc, beta);
+    FPLS_CHECK_LAUNCH();
+    return;
+  }
+  const int gm = ceil_div(M, BM);
+  const int gn = ceil_div(N, BN);
+  // Split K so that the grid covers the SMs at least twice for skinny outputs.
+  int splits = 1;
+  const int tiles = gm * gn;
+  const int target = 2 * Context::get().sm_count;
+  if (tiles < target && K >= 4 * BK) {
+    splits = std::min(ceil_div(target, tiles), ceil_div(K, 8 * BK));
+    if (splits < 1) splits = 1;
+  }
+  int kps = ceil_div(K, splits);
+  kps = ceil_div(kps, BK) * BK;
+  splits = ceil_div(K, kps);
+  const int use_atomic = splits > 1 ? 1 : 0;
+  if (use_atomic) {
+    scale_matrix_kernel<<<grid_for((size_t)M * N, 256), 256, 0, st>>>(C, M, N, ldc, beta);
+    FPLS_CHECK_LAUNCH();
+  }
+  dim3 grid(gm, gn, splits);
+  if (!transA && !transB)
+    gemm_f64_dmma<false, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic);
+  else if (transA && !transB)
+    gemm_f64_dmma<true, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic);
+  else if (!transA && transB)
+    gemm_f64_dmma<false, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic);
+  else
+    gemm_f64_dmma<true, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic);
+  FPLS_CHECK_LAUNCH();
+}
+
+void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda, const double* x,
+          double beta, double* y) {
+  cudaStream_t st = Context::get().stream;
+  if (!trans) {
+    if (rows <= 0) return;
+    if (cols <= 0) {
+      scale_matrix_kernel<<<grid_for(rows, 256), 256, 0, st>>>(y, rows, 1, rows, beta);
+      FPLS_CHECK_LAUNCH();
+      return;
+    }
+    const int gx = ceil_div(rows, 256);
+    int splits = 1;
+    const int target = 4 * Context::get().sm_count;
+    if (gx < target) splits = std::max(1, std::min(ceil_div(target, gx), ceil_div(cols, 256)));
+    int kps = ceil_div(cols, splits);
+    splits = ceil_div(cols, kps);
+    const int use_atomic = splits > 1 ? 1 : 0;
+    if (use_atomic) {
+      scale_matrix_kernel<<<grid_for(rows, 256), 256, 0, st>>>(y, rows, 1, rows, beta);
+      FPLS_CHECK_LAUNCH();
+    }
+    gemv_n_kernel<<<dim3(gx, splits), 256, 0, st>>>(rows, cols, alpha, A, lda, x, y, kps, use_atomic, beta);
+  } else {
+    if (cols <= 0) return;
+    gemv_t_kernel<<<ceil_div(cols, 8), 256, 0, st>>>(rows, cols, alpha, A, lda, x, beta, y);
+  }
+  FPLS_CHECK_LAUNCH();
+}
+
+void col_mean(const double* X, int n, int p, int ldx, double* out) {
+  if (p <= 0) return;
+  col_mean_kernel<<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, out);
+  FPLS_CHECK_LAUNCH();
+}
+
+void col_sd_centered(const double* X, int n, int p, int ldx, double* out) {
+  if (p <= 0) return;
+  col_sd_kernel<<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, out);
+  FPLS_CHECK_LAUNCH();
+}
+
+void center_scale(double* X, int n, int p, int ldx, const double* mean, const double* scale) {
+  if ((size_t)n * p == 0) return;
+  center_scale_kernel<<<grid_for((size_t)n * p, 256), 256, 0, Context::get().stream>>>(X, n, p, ldx, mean, scale);
+  FPLS_CHECK_LAUNCH();
+}
+
+void copy_matrix(double* dst, int ldd, const double* src, int lds, int n, int p) {
+  if ((size_t)n * p == 0) return;
+  copy_matrix_kernel<<<grid_for((size_t)n * p, 256), 256, 0, Context::get().stream>>>(dst, ldd, src, lds, n, p);
+  FPLS_CHECK_LAUNCH();
+}
+
+void add_row_vector(double* X, int n, int p, int ldx, const double* v) {
+  if ((size_t)n * p == 0) return;
+  add_row_vector_kernel<<<grid_for((size_t)n * p, 256), 256, 0, Context::get().stream>>>(X, n, p, ldx, v);
+  FPLS_CHECK_LAUNCH();
+}
+
+void rq_sums(const double* Y, const double* Yp, int n, int m, double* out2) {
+  rq_sums_kernel<<<1, 512, 0, Context::get().stream>>>(Y, Yp, n, m, out2);
+  FPLS_CHECK_LAUNCH();
+}
+
+void fill(double* x, size_t n, double v) {
+  if (n == 0) return;
+  fill_kernel<<<grid_for(n, 256), 256, 0, Context::get().stream>>>(x, n, v);
+  FPLS_CHECK_LAUNCH();
+}
+
+void scale_vec(double* x, size_t n, double a) {
+  if (n == 0) return;
+  scale_vec_kernel<<<grid_for(n, 256), 256, 0, Context::get().stream>>>(x, n, a);
+  FPLS_CHECK_LAUNCH();
+}
+
+}  // namespace fpls

@@ -1,0 +1,578 @@
+// extern "C" entry points of libfastpls_b200.so (declared in include/fastpls_b200.h).
+#include "../../include/fastpls_b200.h"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "blas_f64.cuh"
+#include "context.cuh"
+#include "fits.cuh"
+#include "heads.cuh"
+#include "simpls_engine.cuh"
+#include "svd.cuh"
+
+using namespace fpls;
+
+namespace {
+
+void set_err(char* err, size_t errlen, const char* msg) {
+  if (!err || errlen == 0) return;
+  std::strncpy(err, msg, errlen - 1);
+  err[errlen - 1] = '\0';
+}
+
+template <typename Fn>
+int guarded(char* err, size_t errlen, Fn&& fn) {
+  if (err && errlen) err[0] = '\0';
+  try {
+    fn();
+    return FPLS_OK;
+  } catch (const Error& e) {
+    set_err(err, errlen, e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    set_err(err, errlen, e.what());
+    return FPLS_ERR_INTERNAL;
+  } catch (...) {
+    set_err(err, errlen, "fastpls_b200: unknown internal error");
+    return FPLS_ERR_INTERNAL;
+  }
+}
+
+template <typename T>
+T* upload(const T* host, size_t n) {
+  T* d = Context::get().arena.alloc_n<T>(n ? n : 1);
+  if (n) h2d(d, host, n * sizeof(T));
+  return d;
+}
+
+template <typename T>
+void download(T* host, const T* dev, size_t n) {
+  if (host && n) d2h(host, dev, n * sizeof(T));
+}
+
+int max_of(const int* v, int L) {
+  int m = 0;
+  for (int i = 0; i < L; ++i) m = std::max(m, v[i]);
+  return m;
+}
+
+__global__ void transpose_small(const double* A, int rows, int cols, double* B) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= rows * cols) return;
+  const int i = t % rows, j = t / rows;
+  B[j + (size_t)i * cols] = A[t];
+}
+
+__global__ void scale_column_kernel(const double* src, int n, double inv, double* dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[i] * inv;
+}
+
+__global__ void center_copy_kernel(const double* X, int w, int p, const double* mX,
+                                   const double* vX, double* out) {
+  const size_t total = (size_t)w * p;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int j = static_cast<int>(t / w);
+    out[t] = (X[t] - mX[j]) / vX[j];
+  }
+}
+
+double* centered_test_copy(const double* Xh, int w, int p, const double* mX_d, const double* vX_d) {
+  Context& ctx = Context::get();
+  double* X = upload(Xh, (size_t)w * p);
+  center_copy_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(X, w, p, mX_d, vX_d, X);
+  FPLS_CHECK_LAUNCH();
+  return X;
+}
+
+void lda_outputs_to_host(const LdaModelsDev& d, int C, int kmax, int L, double* means,
+                         double* linear, double* constants, double* priors) {
+  download(means, d.means, (size_t)C * kmax * L);
+  download(linear, d.linear, (size_t)C * kmax * L);
+  download(constants, d.constants, (size_t)C * L);
+  download(priors, d.priors, (size_t)C);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fpls_version(void) { return "fastpls_b200 0.1 (sm_100a)"; }
+
+int fpls_has_cuda(void) {
+  try {
+    Context::get();
+    return 1;
+  } catch (...) {
+    return 0;
+  }
+}
+
+int fpls_reset_workspace(char* err, size_t errlen) {
+  return guarded(err, errlen, [&] { Context::get().release(); });
+}
+
+int fpls_matrix_multiply(const double* A, int a_rows, int a_cols, const double* B, int b_cols,
+                         double* C, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(a_rows >= 0 && a_cols >= 0 && b_cols >= 0, "matrix dimensions must be >= 0");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* dA = upload(A, (size_t)a_rows * a_cols);
+    const double* dB = upload(B, (size_t)a_cols * b_cols);
+    double* dC = ctx.arena.alloc_n<double>((size_t)a_rows * b_cols + 1);
+    gemm(false, false, a_rows, b_cols, a_cols, 1.0, dA, a_rows, dB, a_cols, 0.0, dC, a_rows);
+    download(C, dC, (size_t)a_rows * b_cols);
+    ctx.sync();
+  });
+}
+
+int fpls_truncated_svd(const double* A, int rows, int cols, int k, int svd_method, int oversample,
+                       int power_iters, double svds_tol, int seed, int left_only, double* U,
+                       double* s, double* Vt, int* rank_out, char* err, size_t errlen) {
+  (void)svds_tol;
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(rows > 0 && cols > 0, "truncated_svd requires a non-empty matrix");
+    FPLS_REQUIRE(k >= 1, "truncated_svd: k must be >= 1");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const int kcap = std::min(std::min(rows, cols), std::max(k, 1));
+    const double* dA = upload(A, (size_t)rows * cols);
+    double* dU = ctx.arena.alloc_n<double>((size_t)rows * kcap);
+    double* ds = ctx.arena.alloc_n<double>(kcap);
+    double* dV = ctx.arena.alloc_n<double>((size_t)cols * kcap);
+    dzero(dU, (size_t)rows * kcap * sizeof(double));
+    dzero(ds, kcap * sizeof(double));
+    dzero(dV, (size_t)cols * kcap * sizeof(double));
+    SvdResult r = truncated_svd_device(dA, rows, cols, rows, k, svd_method, oversample,
+                                       power_iters, static_cast<unsigned int>(seed), left_only != 0,
+                                       false, dU, rows, ds, left_only ? nullptr : dV, cols);
+    download(U, dU, (size_t)rows * kcap);
+    download(s, ds, kcap);
+    if (!left_only && Vt) {
+      double* dVt = ctx.arena.alloc_n<double>((size_t)cols * kcap);
+      transpose_small<<<ceil_div((long long)cols * kcap, 256), 256, 0, ctx.stream>>>(dV, cols, kcap, dVt);
+      FPLS_CHECK_LAUNCH();
+      download(Vt, dVt, (size_t)cols * kcap);
+    }
+    ctx.sync();
+    if (rank_out) *rank_out = r.rank;
+  });
+}
+
+int fpls_pls_model1(const double* X, int n, int p, const double* Y, int m, const int* ncomp, int L,
+                    int scaling, int fit, int svd_method, int oversample, int power_iters,
+                    double svds_tol, int seed, int* ncomp_out, double* C_latent, double* W_latent,
+                    double* Q, double* Ttrain, double* R, double* mX, double* vX, double* mY,
+                    double* B, double* Yfit, double* R2Y, double* s, int* k_eff, char* err,
+                    size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && m > 0, "pls_model1 requires non-empty X and Y");
+    FPLS_REQUIRE(L >= 1 && ncomp, "ncomp must contain at least one value");
+    FPLS_REQUIRE(!(fit && !Yfit), "fit = 1 requires a Yfit buffer");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const int max_rank = std::min(n, std::min(p, m));
+    std::vector<int> nc(ncomp, ncomp + L);
+    for (int& c : nc) c = std::max(1, std::min(c, max_rank));
+    const int K0 = std::min(max_of(nc.data(), L), max_rank);
+    double* dX = upload(X, (size_t)n * p);
+    double* dY = upload(Y, (size_t)n * m);
+    double* dmX = ctx.arena.alloc_n<double>(p);
+    double* dvX = ctx.arena.alloc_n<double>(p);
+    double* dmY = ctx.arena.alloc_n<double>(m);
+    center_scale_xy(dX, n, p, dY, m, scaling, dmX, dvX, dmY);
+    FitOptions opt;
+    opt.scaling = scaling;
+    opt.fit = fit != 0;
+    opt.svd_method = svd_method;
+    opt.oversample = oversample;
+    opt.power_iters = power_iters;
+    opt.svds_tol = svds_tol;
+    opt.seed = static_cast<unsigned int>(seed);
+    PlssvdOut o;
+    o.C_latent = ctx.arena.alloc_n<double>((size_t)K0 * K0 * L);
+    o.W_latent = ctx.arena.alloc_n<double>((size_t)K0 * m * L);
+    o.R = ctx.arena.alloc_n<double>((size_t)p * K0);
+    o.Q = ctx.arena.alloc_n<double>((size_t)m * K0);
+    o.T = ctx.arena.alloc_n<double>((size_t)n * K0);
+    o.s = ctx.arena.alloc_n<double>(K0);
+    o.B = B ? ctx.arena.alloc_n<double>((size_t)p * m * L) : nullptr;
+    o.Yfit = fit ? ctx.arena.alloc_n<double>((size_t)n * m * L) : nullptr;
+    std::vector<double> r2(L, 0.0);
+    o.R2Y = r2.data();
+    const int keff = plssvd_fit_centered(dX, n, p, dY, m, nc.data(), L, K0, opt, dmY, o);
+    download(C_latent, o.C_latent, (size_t)K0 * K0 * L);
+    download(W_latent, o.W_latent, (size_t)K0 * m * L);
+    download(Q, o.Q, (size_t)m * K0);
+    download(Ttrain, o.T, (size_t)n * K0);
+    download(R, o.R, (size_t)p * K0);
+    download(mX, dmX, p);
+    download(vX, dvX, p);
+    download(mY, dmY, m);
+    if (B) download(B, o.B, (size_t)p * m * L);
+    if (fit) download(Yfit, o.Yfit, (size_t)n * m * L);
+    download(s, o.s, K0);
+    ctx.sync();
+    if (R2Y) std::copy(r2.begin(), r2.end(), R2Y);
+    if (ncomp_out) std::copy(nc.begin(), nc.end(), ncomp_out);
+    if (k_eff) *k_eff = keff;
+  });
+}
+
+int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
+                         int L, int scaling, int fit, int seed, double* R, double* Q, double* mX,
+                         double* vX, double* mY, double* B, double* Yfit, double* R2Y,
+                         int* n_components, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && m > 0, "pls_model2_fast requires non-empty X and Y");
+    FPLS_REQUIRE(L >= 1 && ncomp, "ncomp must contain at least one value");
+    FPLS_REQUIRE(!(fit && !Yfit), "fit = 1 requires a Yfit buffer");
+    FPLS_REQUIRE(p > 5 || m == 1,
+                 "pls_model2_fast with <= 5 predictors and several responses is not supported on "
+                 "the GPU path");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    std::vector<int> nc(ncomp, ncomp + L);
+    for (int& c : nc) c = std::max(1, c);
+    const int K = max_of(nc.data(), L);
+    double* dX = upload(X, (size_t)n * p);
+    double* dYc = upload(Y, (size_t)n * m);
+    double* dmX = ctx.arena.alloc_n<double>(p);
+    double* dvX = ctx.arena.alloc_n<double>(p);
+    double* dmY = ctx.arena.alloc_n<double>(m);
+    center_scale_xy(dX, n, p, dYc, m, scaling, dmX, dvX, dmY);
+    // Single fit on all rows: S = Xc^T Yc as the reference (fastPLS.cpp:2499).
+    XOperatorF64 xop(dX, n, p);
+    SimplsBatch b;
+    b.n = n; b.p = p; b.m = m; b.F = 1; b.K = K;
+    int iters = 2;
+    if (const char* e = std::getenv("FASTPLS_FAST_INC_ITERS")) {
+      char* endp = nullptr;
+      long v = std::strtol(e, &endp, 10);
+      if (endp != e) iters = static_cast<int>(std::min(6L, std::max(1L, v)));
+    }
+    b.power_iters = iters;
+    b.X = &xop;
+    b.Yg = dYc;
+    b.S = ctx.arena.alloc_n<double>((size_t)p * m);
+    gemm(true, false, p, m, n, 1.0, dX, n, dYc, n, 0.0, b.S, p);
+    std::vector<double> om(p);
+    host_gaussian(om.data(), p, static_cast<unsigned int>(seed));
+    b.omega = upload(om.data(), p);
+    b.m1_mode = (m == 1);
+    b.R = ctx.arena.alloc_n<double>((size_t)p * K);
+    b.Q = ctx.arena.alloc_n<double>((size_t)m * K);
+    b.V = ctx.arena.alloc_n<double>((size_t)p * K);
+    b.tnorm = ctx.arena.alloc_n<double>(K);
+    b.Tkeep = fit ? ctx.arena.alloc_n<double>((size_t)n * K) : nullptr;
+    b.ncomp_done = ctx.arena.alloc_n<int>(1);
+    b.status = ctx.arena.alloc_n<int>(1);
+    simpls_batch_run(b);
+    int done = 0;
+    d2h(&done, b.ncomp_done, sizeof(int));
+    std::vector<double> tn(K);
+    d2h(tn.data(), b.tnorm, K * sizeof(double));
+    ctx.sync();
+    // Slices exactly as the reference's while loop assigns them (fastPLS.cpp:2648-2661).
+    double* dB = B ? ctx.arena.alloc_n<double>((size_t)p * m * L) : nullptr;
+    if (dB) dzero(dB, (size_t)p * m * L * sizeof(double));
+    double* dYf = fit ? ctx.arena.alloc_n<double>((size_t)n * m * L) : nullptr;
+    double* cur = fit ? ctx.arena.alloc_n<double>((size_t)n * m) : nullptr;
+    double* tcol = fit ? ctx.arena.alloc_n<double>(n) : nullptr;
+    double* rq = fit ? ctx.arena.alloc_n<double>(2 * L) : nullptr;
+    if (fit) {
+      dzero(dYf, (size_t)n * m * L * sizeof(double));
+      dzero(cur, (size_t)n * m * sizeof(double));
+    }
+    std::vector<int> filled(L, 0);
+    int i_out = 0;
+    for (int a = 0; a < done; ++a) {
+      while (i_out < L && a == nc[i_out] - 1) {
+        if (dB) gemm(false, true, p, m, a + 1, 1.0, b.R, p, b.Q, m, 0.0, dB + (size_t)i_out * p * m, p);
+        if (fit) {
+          scale_column_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(b.Tkeep + (size_t)a * n, n, 1.0 / tn[a], tcol);
+          FPLS_CHECK_LAUNCH();
+          gemm(false, true, n, m, 1, 1.0, tcol, n, b.Q + (size_t)a * m, m, 1.0, cur, n);
+          rq_sums(dYc, cur, n, m, rq + 2 * i_out);
+          double* sl = dYf + (size_t)i_out * n * m;
+          d2d(sl, cur, (size_t)n * m * sizeof(double));
+          add_row_vector(sl, n, m, n, dmY);
+        }
+        filled[i_out] = 1;
+        ++i_out;
+      }
+    }
+    download(R, b.R, (size_t)p * K);
+    download(Q, b.Q, (size_t)m * K);
+    download(mX, dmX, p);
+    download(vX, dvX, p);
+    download(mY, dmY, m);
+    if (B) download(B, dB, (size_t)p * m * L);
+    std::vector<double> hrq(2 * L, 0.0);
+    if (fit) {
+      download(Yfit, dYf, (size_t)n * m * L);
+      download(hrq.data(), rq, 2 * (size_t)L);
+    }
+    ctx.sync();
+    if (R2Y) {
+      for (int i = 0; i < L; ++i)
+        R2Y[i] = (fit && filled[i]) ? 1.0 - hrq[2 * i] / hrq[2 * i + 1] : 0.0;
+    }
+    if (n_components) *n_components = done;
+  });
+}
+
+int fpls_pls_model2(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
+                    int L, int scaling, int fit, int svd_method, int oversample, int power_iters,
+                    double svds_tol, int seed, double* R, double* Q, double* P, double* Ttrain,
+                    double* mX, double* vX, double* mY, double* B, double* Yfit, double* R2Y,
+                    int* n_components, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && m > 0, "pls_model2 requires non-empty X and Y");
+    FPLS_REQUIRE(L >= 1 && ncomp, "ncomp must contain at least one value");
+    FPLS_REQUIRE(!(fit && !Yfit), "fit = 1 requires a Yfit buffer");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const int K = max_of(ncomp, L);
+    FPLS_REQUIRE(K >= 1, "ncomp must be >= 1");
+    double* dX = upload(X, (size_t)n * p);
+    double* dYraw = upload(Y, (size_t)n * m);
+    double* dY = ctx.arena.alloc_n<double>((size_t)n * m);
+    d2d(dY, dYraw, (size_t)n * m * sizeof(double));
+    double* dmX = ctx.arena.alloc_n<double>(p);
+    double* dvX = ctx.arena.alloc_n<double>(p);
+    double* dmY = ctx.arena.alloc_n<double>(m);
+    center_scale_xy(dX, n, p, dY, m, scaling, dmX, dvX, dmY);
+    FitOptions opt;
+    opt.scaling = scaling;
+    opt.fit = fit != 0;
+    opt.svd_method = svd_method;
+    opt.oversample = oversample;
+    opt.power_iters = power_iters;
+    opt.svds_tol = svds_tol;
+    opt.seed = static_cast<unsigned int>(seed);
+    SimplsOut o;
+    o.R = ctx.arena.alloc_n<double>((size_t)p * K);
+    o.Q = ctx.arena.alloc_n<double>((size_t)m * K);
+    o.P = ctx.arena.alloc_n<double>((size_t)p * K);
+    o.T = ctx.arena.alloc_n<double>((size_t)n * K);
+    o.B = B ? ctx.arena.alloc_n<double>((size_t)p * m * L) : nullptr;
+    if (o.B) dzero(o.B, (size_t)p * m * L * sizeof(double));
+    o.Yfit = fit ? ctx.arena.alloc_n<double>((size_t)n * m * L) : nullptr;
+    if (o.Yfit) dzero(o.Yfit, (size_t)n * m * L * sizeof(double));
+    std::vector<double> r2(L, 0.0);
+    o.R2Y = r2.data();
+    const int done = simpls_classic_fit(dX, n, p, dY, m, dYraw, ncomp, L, opt, dmY, o);
+    download(R, o.R, (size_t)p * K);
+    download(Q, o.Q, (size_t)m * K);
+    download(P, o.P, (size_t)p * K);
+    download(Ttrain, o.T, (size_t)n * K);
+    download(mX, dmX, p);
+    download(vX, dvX, p);
+    download(mY, dmY, m);
+    if (B) download(B, o.B, (size_t)p * m * L);
+    if (fit) download(Yfit, o.Yfit, (size_t)n * m * L);
+    ctx.sync();
+    if (R2Y) std::copy(r2.begin(), r2.end(), R2Y);
+    if (n_components) *n_components = done;
+  });
+}
+
+int fpls_predict_lowrank(const double* Xtest, int w, int p, const double* mX, const double* vX,
+                         const double* mY, int m, const double* R, int kmax, const double* W,
+                         const int* ncomp, int L, double* Ypred, double* Ttest, char* err,
+                         size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(w > 0 && p > 0 && m > 0 && kmax > 0 && L > 0, "predict: empty input");
+    for (int a = 0; a < L; ++a)
+      FPLS_REQUIRE(ncomp[a] >= 1 && ncomp[a] <= kmax, "ncomp exceeds latent rank for prediction");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* dmX = upload(mX, p);
+    const double* dvX = upload(vX, p);
+    const double* dmY = upload(mY, m);
+    const double* dR = upload(R, (size_t)p * kmax);
+    const double* dW = upload(W, (size_t)kmax * m * L);
+    double* dX = centered_test_copy(Xtest, w, p, dmX, dvX);
+    double* dT = ctx.arena.alloc_n<double>((size_t)w * kmax);
+    double* dYp = ctx.arena.alloc_n<double>((size_t)w * m * L);
+    lowrank_predict(dX, w, p, dR, kmax, dW, m, ncomp, L, dmY, dT, dYp);
+    download(Ypred, dYp, (size_t)w * m * L);
+    if (Ttest) download(Ttest, dT, (size_t)w * kmax);
+    ctx.sync();
+  });
+}
+
+int fpls_predict_classes(const double* Xtest, int w, int p, const double* mX, const double* vX,
+                         const double* mY, int m, const double* R, int kmax, const double* W,
+                         const int* ncomp, int L, const double* class_bias, int top_k,
+                         int* top_index, double* top_score, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(w > 0 && p > 0 && m > 0 && kmax > 0 && L > 0, "predict: empty input");
+    FPLS_REQUIRE(top_k >= 1 && top_k <= std::min(m, 32), "top_k must be in 1..min(m, 32)");
+    for (int a = 0; a < L; ++a)
+      FPLS_REQUIRE(ncomp[a] >= 1 && ncomp[a] <= kmax, "ncomp exceeds latent rank for prediction");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* dmX = upload(mX, p);
+    const double* dvX = upload(vX, p);
+    const double* dmY = upload(mY, m);
+    const double* dR = upload(R, (size_t)p * kmax);
+    const double* dW = upload(W, (size_t)kmax * m * L);
+    const double* dbias = class_bias ? upload(class_bias, m) : nullptr;
+    double* dX = centered_test_copy(Xtest, w, p, dmX, dvX);
+    double* dT = ctx.arena.alloc_n<double>((size_t)w * kmax);
+    double* dYp = ctx.arena.alloc_n<double>((size_t)w * m * L);
+    lowrank_predict(dX, w, p, dR, kmax, dW, m, ncomp, L, dmY, dT, dYp);
+    int* didx = ctx.arena.alloc_n<int>((size_t)w * top_k * L);
+    double* dsc = ctx.arena.alloc_n<double>((size_t)w * top_k * L);
+    for (int a = 0; a < L; ++a) {
+      const double* Ya = dYp + (size_t)a * w * m;
+      if (top_k == 1 && !top_score) {
+        row_argmax(Ya, w, m, dbias, didx + (size_t)a * w);
+      } else {
+        row_topk(Ya, w, m, dbias, top_k, didx + (size_t)a * w * top_k, dsc + (size_t)a * w * top_k);
+      }
+    }
+    download(top_index, didx, (size_t)w * top_k * L);
+    if (top_score) download(top_score, dsc, (size_t)w * top_k * L);
+    ctx.sync();
+  });
+}
+
+int fpls_lda_train_prefix(const double* T, int n, int kmax, const int* y, int n_classes,
+                          const int* ncomp, int L, double ridge, double* means, double* linear,
+                          double* constants, double* priors, double* lambda, char* err,
+                          size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && kmax > 0, "lda_train_prefix requires a non-empty score matrix");
+    FPLS_REQUIRE(L >= 1, "lda_train_prefix requires at least one component count");
+    const int km = max_of(ncomp, L);
+    for (int a = 0; a < L; ++a)
+      FPLS_REQUIRE(ncomp[a] >= 1 && ncomp[a] <= kmax,
+                   "lda_train_prefix component counts must be in 1..ncol(Ttrain)");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* dT = upload(T, (size_t)n * kmax);
+    const int* dy = upload(y, n);
+    LdaModelsDev d;
+    d.means = ctx.arena.alloc_n<double>((size_t)n_classes * km * L);
+    d.linear = ctx.arena.alloc_n<double>((size_t)n_classes * km * L);
+    d.constants = ctx.arena.alloc_n<double>((size_t)n_classes * L);
+    d.priors = ctx.arena.alloc_n<double>(n_classes);
+    std::vector<double> lam(L);
+    d.lambda = lam.data();
+    lda_train_prefix(dT, n, km, dy, n_classes, ncomp, L, ridge, d);
+    lda_outputs_to_host(d, n_classes, km, L, means, linear, constants, priors);
+    ctx.sync();
+    if (lambda) std::copy(lam.begin(), lam.end(), lambda);
+  });
+}
+
+int fpls_lda_project_train_prefix(const double* X, int n, int p, const double* R, int k,
+                                  const double* offset, const int* y, int n_classes,
+                                  const int* ncomp, int L, double ridge, double* means,
+                                  double* linear, double* constants, double* priors,
+                                  double* lambda, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0, "lda_project_train_prefix requires a non-empty predictor matrix");
+    FPLS_REQUIRE(k > 0, "lda_project_train_prefix projection matrix has incompatible dimensions");
+    const int km = max_of(ncomp, L);
+    for (int a = 0; a < L; ++a)
+      FPLS_REQUIRE(ncomp[a] >= 1 && ncomp[a] <= k, "component counts must be in 1..ncol(R)");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* dX = upload(X, (size_t)n * p);
+    const double* dR = upload(R, (size_t)p * k);
+    double* dT = ctx.arena.alloc_n<double>((size_t)n * k);
+    gemm(false, false, n, k, p, 1.0, dX, n, dR, p, 0.0, dT, n);
+    if (offset) {
+      double* doff = upload(offset, k);
+      scale_vec(doff, k, -1.0);
+      add_row_vector(dT, n, k, n, doff);
+    }
+    const int* dy = upload(y, n);
+    LdaModelsDev d;
+    d.means = ctx.arena.alloc_n<double>((size_t)n_classes * km * L);
+    d.linear = ctx.arena.alloc_n<double>((size_t)n_classes * km * L);
+    d.constants = ctx.arena.alloc_n<double>((size_t)n_classes * L);
+    d.priors = ctx.arena.alloc_n<double>(n_classes);
+    std::vector<double> lam(L);
+    d.lambda = lam.data();
+    lda_train_prefix(dT, n, km, dy, n_classes, ncomp, L, ridge, d);
+    lda_outputs_to_host(d, n_classes, km, L, means, linear, constants, priors);
+    ctx.sync();
+    if (lambda) std::copy(lam.begin(), lam.end(), lambda);
+  });
+}
+
+int fpls_lda_predict(const double* T, int w, int k, const double* linear,
+                     const double* constants, int n_classes, int* labels, double* scores,
+                     char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(w > 0 && k > 0 && n_classes > 0, "lda_predict requires a non-empty score matrix");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* dT = upload(T, (size_t)w * k);
+    const double* dL = upload(linear, (size_t)n_classes * k);
+    const double* dc = upload(constants, n_classes);
+    double* dS = ctx.arena.alloc_n<double>((size_t)w * n_classes);
+    gemm(false, true, w, n_classes, k, 1.0, dT, w, dL, n_classes, 0.0, dS, w);
+    int* dlab = ctx.arena.alloc_n<int>(w);
+    row_argmax(dS, w, n_classes, dc, dlab);
+    download(labels, dlab, w);
+    if (scores) {
+      add_row_vector(dS, w, n_classes, w, dc);
+      download(scores, dS, (size_t)w * n_classes);
+    }
+    ctx.sync();
+  });
+}
+
+int fpls_lda_project_predict(const double* X, int w, int p, const double* R, int k,
+                             const double* offset, const double* linear,
+                             const double* constants, int n_classes, int* labels,
+                             double* scores, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(w > 0 && p > 0 && k > 0 && n_classes > 0,
+                 "lda_project_predict requires non-empty X and projection matrices");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* dX = upload(X, (size_t)w * p);
+    const double* dR = upload(R, (size_t)p * k);
+    const double* dL = upload(linear, (size_t)n_classes * k);
+    double* dc = upload(constants, n_classes);
+    double* dS = ctx.arena.alloc_n<double>((size_t)w * n_classes);
+    // constants_adj = constants - offset linear^T
+    if (offset) {
+      const double* doff = upload(offset, k);
+      gemv(false, n_classes, k, -1.0, dL, n_classes, doff, 1.0, dc);
+    }
+    const double nn = w, pp = p, kk = k, cc = n_classes;
+    const double latent_ops = nn * kk * (pp + cc);
+    const double direct_ops = nn * pp * cc;
+    if (direct_ops < 0.5 * latent_ops) {
+      double* dW = ctx.arena.alloc_n<double>((size_t)p * n_classes);
+      gemm(false, true, p, n_classes, k, 1.0, dR, p, dL, n_classes, 0.0, dW, p);
+      gemm(false, false, w, n_classes, p, 1.0, dX, w, dW, p, 0.0, dS, w);
+    } else {
+      double* dT = ctx.arena.alloc_n<double>((size_t)w * k);
+      gemm(false, false, w, k, p, 1.0, dX, w, dR, p, 0.0, dT, w);
+      gemm(false, true, w, n_classes, k, 1.0, dT, w, dL, n_classes, 0.0, dS, w);
+    }
+    int* dlab = ctx.arena.alloc_n<int>(w);
+    row_argmax(dS, w, n_classes, dc, dlab);
+    download(labels, dlab, w);
+    if (scores) {
+      add_row_vector(dS, w, n_classes, w, dc);
+      download(scores, dS, (size_t)w * n_classes);
+    }
+    ctx.sync();
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,115 @@
+#include "context.cuh"
+
+#include <algorithm>
+
+namespace fpls {
+
+Arena::~Arena() {}
+
+void* Arena::alloc(size_t bytes) {
+  bytes = (bytes + 255) & ~size_t(255);
+  if (bytes == 0) bytes = 256;
+  for (auto& b : blocks_) {
+    if (b.size - b.used >= bytes) {
+      void* p = b.base + b.used;
+      b.used += bytes;
+      return p;
+    }
+  }
+  size_t want = std::max<size_t>(bytes, size_t(64) << 20);
+  char* base = nullptr;
+  FPLS_CUDA(cudaMalloc(&base, want));
+  blocks_.push_back({base, want, bytes});
+  return base;
+}
+
+size_t Arena::capacity() const {
+  size_t c = 0;
+  for (auto& b : blocks_) c += b.size;
+  return c;
+}
+
+void Arena::reset() {
+  size_t used = 0;
+  for (auto& b : blocks_) used += b.used;
+  high_water_ = std::max(high_water_, used);
+  if (blocks_.size() > 1) {
+    size_t total = capacity();
+    for (auto& b : blocks_) cudaFree(b.base);
+    blocks_.clear();
+    char* base = nullptr;
+    FPLS_CUDA(cudaMalloc(&base, total));
+    blocks_.push_back({base, total, 0});
+  } else {
+    for (auto& b : blocks_) b.used = 0;
+  }
+}
+
+void Arena::release() {
+  for (auto& b : blocks_) cudaFree(b.base);
+  blocks_.clear();
+}
+
+Context& Context::get() {
+  static Context ctx;
+  if (ctx.device < 0) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n < 1) {
+      throw Error(kErrNoDevice, "fastpls_b200: no CUDA device is available");
+    }
+    int dev = 0;
+    FPLS_CUDA(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    FPLS_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10) {
+      throw Error(kErrNoDevice, std::string("fastpls_b200 is built for sm_100a (B200); device is ") +
+                                    prop.name);
+    }
+    ctx.sm_count = prop.multiProcessorCount;
+    FPLS_CUDA(cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking));
+    FPLS_CUDA(cudaMalloc(&ctx.d_status, 64 * sizeof(int)));
+    FPLS_CUDA(cudaMemset(ctx.d_status, 0, 64 * sizeof(int)));
+    ctx.device = dev;
+  }
+  return ctx;
+}
+
+void Context::begin_call() {
+  arena.reset();
+  FPLS_CUDA(cudaMemsetAsync(d_status, 0, 64 * sizeof(int), stream));
+}
+
+int Context::read_status() {
+  int s = 0;
+  FPLS_CUDA(cudaMemcpyAsync(&s, d_status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  FPLS_CUDA(cudaStreamSynchronize(stream));
+  return s;
+}
+
+void Context::sync() { FPLS_CUDA(cudaStreamSynchronize(stream)); }
+
+void Context::release() {
+  if (device < 0) return;
+  cudaStreamSynchronize(stream);
+  arena.release();
+}
+
+void h2d(void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return;
+  FPLS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, Context::get().stream));
+}
+void d2h(void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return;
+  FPLS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, Context::get().stream));
+}
+void d2d(void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return;
+  FPLS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, Context::get().stream));
+}
+void dzero(void* dst, size_t bytes) {
+  if (bytes == 0) return;
+  FPLS_CUDA(cudaMemsetAsync(dst, 0, bytes, Context::get().stream));
+}
+
+}  // namespace fpls

@@ -1,0 +1,480 @@
+#include "blas_f64.cuh"
+#include "context.cuh"
+#include "simpls_engine.cuh"
+
+#include <algorithm>
+
+namespace fpls {
+namespace {
+
+constexpr int kThreads = 256;
+
+struct Eng {
+  int n, p, m, F, K, cp, cn, szp, szn;
+  const double* Yg;
+  const int* labels;
+  const double* mY_all;
+  const uint8_t* mask;
+  const double* delta;
+  const double* colscale;
+  const double* dY;
+  double* S;
+  const double* omega;
+  int m1_mode;
+  double* R;
+  double* Q;
+  double* V;
+  double* tnorm;
+  double* Tkeep;
+  int* ncomp_done;
+  int* status;
+  // workspace
+  double* y;       // F x p
+  double* zA;      // F x cp x m
+  double* zB;      // F x cp x m
+  double* npart;   // F x cp
+  double* r;       // F x p (unit r before the t normalisation)
+  double* Rhat;    // p x F
+  double* cpart;   // F x cp
+  double* U;       // n x F
+  double* T;       // n x F
+  double* tpart;   // F x cn x 2
+  double* qpart;   // F x cn x m
+  double* P;       // p x F
+  double* pv;      // F x p
+  double* wpart;   // F x cp x K
+  double* v;       // F x p
+  double* vpart;   // F x cp
+  double* vSpart;  // F x cp x m
+};
+
+__device__ __forceinline__ void chunk_range(int chunk, int sz, int total, int& b, int& e) {
+  b = chunk * sz;
+  e = min(total, b + sz);
+}
+
+__device__ __forceinline__ double sum_parts(const double* parts, int count, int stride) {
+  double s = 0.0;
+  for (int c = 0; c < count; ++c) s += parts[(size_t)c * stride];
+  return s;
+}
+
+// zout[f][chunk][j] = sum_{i in chunk} S_f[i,j] y[i]  (block reductions per column)
+__device__ void partial_StY(const Eng& e, int f, int chunk, int b, int en, const double* yv,
+                            double* zout, double* scratch) {
+  const double* Sf = e.S + (size_t)f * e.p * e.m;
+  for (int j = 0; j < e.m; ++j) {
+    double a = 0.0;
+    for (int i = b + threadIdx.x; i < en; i += blockDim.x) a += Sf[i + (size_t)j * e.p] * yv[i];
+    a = block_sum(a, scratch);
+    if (threadIdx.x == 0) zout[((size_t)f * e.cp + chunk) * e.m + j] = a;
+  }
+}
+
+__global__ void k_refresh_start(Eng e, int a, int iters) {
+  __shared__ double scratch[32];
+  const int f = blockIdx.y, chunk = blockIdx.x;
+  if (e.status[f]) return;
+  int b, en;
+  chunk_range(chunk, e.szp, e.p, b, en);
+  const double* Sf = e.S + (size_t)f * e.p * e.m;
+  const double* y0;
+  if (e.m1_mode) y0 = Sf;                                   // exact left vector of p x 1
+  else if (a == 0) y0 = e.omega + (size_t)f * e.p;          // Gaussian sketch, seed
+  else y0 = e.R + ((size_t)f * e.K + (a - 1)) * e.p;        // warm start r_{a-1}
+  double* yf = e.y + (size_t)f * e.p;
+  double ss = 0.0;
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+    const double v = y0[i];
+    yf[i] = v;
+    ss += v * v;
+  }
+  if (iters > 0) {
+    __syncthreads();
+    partial_StY(e, f, chunk, b, en, yf, e.zA, scratch);
+  } else {
+    ss = block_sum(ss, scratch);
+    if (threadIdx.x == 0) e.npart[(size_t)f * e.cp + chunk] = ss;
+  }
+}
+
+__global__ void k_refresh_apply(Eng e, const double* zin, double* zout, int last) {
+  extern __shared__ double zs[];
+  __shared__ double scratch[32];
+  const int f = blockIdx.y, chunk = blockIdx.x;
+  if (e.status[f]) return;
+  int b, en;
+  chunk_range(chunk, e.szp, e.p, b, en);
+  for (int j = threadIdx.x; j < e.m; j += blockDim.x)
+    zs[j] = sum_parts(zin + (size_t)f * e.cp * e.m + j, e.cp, e.m);
+  __syncthreads();
+  const double* Sf = e.S + (size_t)f * e.p * e.m;
+  double* yf = e.y + (size_t)f * e.p;
+  double ss = 0.0;
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+    double acc = 0.0;
+    for (int j = 0; j < e.m; ++j) acc += Sf[i + (size_t)j * e.p] * zs[j];
+    yf[i] = acc;
+    ss += acc * acc;
+  }
+  if (!last) {
+    __syncthreads();
+    partial_StY(e, f, chunk, b, en, yf, zout, scratch);
+  } else {
+    ss = block_sum(ss, scratch);
+    if (threadIdx.x == 0) e.npart[(size_t)f * e.cp + chunk] = ss;
+  }
+}
+
+// r = -sign(y0) y / ||y|| (Householder QR of a single column; the 1 x m core
+// SVD from gesvd keeps U = 1).  Rhat = colscale * r; cpart = delta . Rhat.
+__global__ void k_refresh_finish(Eng e) {
+  __shared__ double scratch[32];
+  const int f = blockIdx.y, chunk = blockIdx.x;
+  if (e.status[f]) return;
+  int b, en;
+  chunk_range(chunk, e.szp, e.p, b, en);
+  const double nrm = sqrt(sum_parts(e.npart + (size_t)f * e.cp, e.cp, 1));
+  if (!(nrm > 0.0) || !isfinite(nrm)) {
+    // Degenerate refresh: the reference's refresh returns false and the loop stops.
+    if (chunk == 0 && threadIdx.x == 0) e.status[f] = 1;
+    return;
+  }
+  const double* yf = e.y + (size_t)f * e.p;
+  const double sgn = (yf[0] >= 0.0) ? -1.0 : 1.0;
+  const double* sc = e.colscale ? e.colscale + (size_t)f * e.p : nullptr;
+  const double* dl = e.delta ? e.delta + (size_t)f * e.p : nullptr;
+  double c = 0.0;
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+    const double ri = sgn * yf[i] / nrm;
+    e.r[(size_t)f * e.p + i] = ri;
+    const double rh = sc ? ri * sc[i] : ri;
+    e.Rhat[(size_t)f * e.p + i] = rh;
+    if (dl) c += dl[i] * rh;
+  }
+  if (dl) {
+    c = block_sum(c, scratch);
+    if (threadIdx.x == 0) e.cpart[(size_t)f * e.cp + chunk] = c;
+  }
+}
+
+// t = mask * (U - delta.rhat); partial sums of t^2 and t; q partials.
+__global__ void k_scores(Eng e, int a) {
+  extern __shared__ double qs[];
+  __shared__ double scratch[32];
+  const int f = blockIdx.y, chunk = blockIdx.x;
+  if (e.status[f]) {
+    return;
+  }
+  int b, en;
+  chunk_range(chunk, e.szn, e.n, b, en);
+  const double c = e.delta ? sum_parts(e.cpart + (size_t)f * e.cp, e.cp, 1) : 0.0;
+  const uint8_t* mk = e.mask ? e.mask + (size_t)f * e.n : nullptr;
+  const double* Uf = e.U + (size_t)f * e.n;
+  double* Tf = e.T + (size_t)f * e.n;
+  double* keep = e.Tkeep ? e.Tkeep + ((size_t)f * e.K + a) * e.n : nullptr;
+  if (e.labels) {
+    for (int j = threadIdx.x; j < e.m; j += blockDim.x) qs[j] = 0.0;
+    __syncthreads();
+  }
+  double s2 = 0.0, s1 = 0.0;
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+    const double u = Uf[i] - c;
+    const double t = (mk && !mk[i]) ? 0.0 : u;
+    Tf[i] = t;
+    if (keep) keep[i] = u;
+    s2 += t * t;
+    s1 += t;
+    if (e.labels && t != 0.0) atomicAdd(&qs[e.labels[i]], t);
+  }
+  s2 = block_sum(s2, scratch);
+  s1 = block_sum(s1, scratch);
+  if (threadIdx.x == 0) {
+    e.tpart[((size_t)f * e.cn + chunk) * 2 + 0] = s2;
+    e.tpart[((size_t)f * e.cn + chunk) * 2 + 1] = s1;
+  }
+  double* qp = e.qpart + ((size_t)f * e.cn + chunk) * e.m;
+  if (e.labels) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < e.m; j += blockDim.x) qp[j] = qs[j];
+  } else {
+    __syncthreads();
+    for (int j = 0; j < e.m; ++j) {
+      double acc = 0.0;
+      const double* yc = e.Yg + (size_t)j * e.n;
+      for (int i = b + threadIdx.x; i < en; i += blockDim.x) acc += Tf[i] * yc[i];
+      acc = block_sum(acc, scratch);
+      if (threadIdx.x == 0) qp[j] = acc;
+    }
+  }
+}
+
+__device__ __forceinline__ void t_stats(const Eng& e, int f, double& tn, double& st) {
+  double s2 = 0.0, s1 = 0.0;
+  const double* tp = e.tpart + (size_t)f * e.cn * 2;
+  for (int c = 0; c < e.cn; ++c) {
+    s2 += tp[2 * c];
+    s1 += tp[2 * c + 1];
+  }
+  tn = sqrt(s2);
+  st = s1;
+}
+
+// p = colscale * (P - delta * sum(t)) / ||t||; partial V^T p.
+__global__ void k_loading(Eng e, int a) {
+  __shared__ double scratch[32];
+  const int f = blockIdx.y, chunk = blockIdx.x;
+  if (e.status[f]) return;
+  double tn, st;
+  t_stats(e, f, tn, st);
+  if (!(tn > 0.0) || !isfinite(tn)) {
+    if (chunk == 0 && threadIdx.x == 0) e.status[f] = 1;
+    return;
+  }
+  int b, en;
+  chunk_range(chunk, e.szp, e.p, b, en);
+  const double* sc = e.colscale ? e.colscale + (size_t)f * e.p : nullptr;
+  const double* dl = e.delta ? e.delta + (size_t)f * e.p : nullptr;
+  const double* Pf = e.P + (size_t)f * e.p;
+  double* pf = e.pv + (size_t)f * e.p;
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+    double v = Pf[i];
+    if (dl) v -= dl[i] * st;
+    if (sc) v *= sc[i];
+    pf[i] = v / tn;
+  }
+  __syncthreads();
+  const double* Vf = e.V + (size_t)f * e.p * e.K;
+  for (int l = 0; l < a; ++l) {
+    double acc = 0.0;
+    for (int i = b + threadIdx.x; i < en; i += blockDim.x) acc += Vf[i + (size_t)l * e.p] * pf[i];
+    acc = block_sum(acc, scratch);
+    if (threadIdx.x == 0) e.wpart[((size_t)f * e.cp + chunk) * e.K + l] = acc;
+  }
+}
+
+// v = p - V (V^T p); partial ||v||^2.
+__global__ void k_orth(Eng e, int a) {
+  extern __shared__ double ws[];
+  __shared__ double scratch[32];
+  const int f = blockIdx.y, chunk = blockIdx.x;
+  if (e.status[f]) return;
+  int b, en;
+  chunk_range(chunk, e.szp, e.p, b, en);
+  for (int l = threadIdx.x; l < a; l += blockDim.x)
+    ws[l] = sum_parts(e.wpart + (size_t)f * e.cp * e.K + l, e.cp, e.K);
+  __syncthreads();
+  const double* Vf = e.V + (size_t)f * e.p * e.K;
+  const double* pf = e.pv + (size_t)f * e.p;
+  double* vf = e.v + (size_t)f * e.p;
+  double ss = 0.0;
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+    double acc = pf[i];
+    for (int l = 0; l < a; ++l) acc -= Vf[i + (size_t)l * e.p] * ws[l];
+    vf[i] = acc;
+    ss += acc * acc;
+  }
+  ss = block_sum(ss, scratch);
+  if (threadIdx.x == 0) e.vpart[(size_t)f * e.cp + chunk] = ss;
+}
+
+// v /= ||v||; V[:, a] = v; partial v^T S.
+__global__ void k_vnorm(Eng e, int a) {
+  __shared__ double scratch[32];
+  const int f = blockIdx.y, chunk = blockIdx.x;
+  if (e.status[f]) return;
+  const double vn = sqrt(sum_parts(e.vpart + (size_t)f * e.cp, e.cp, 1));
+  if (!(vn > 0.0) || !isfinite(vn)) {
+    if (chunk == 0 && threadIdx.x == 0) e.status[f] = 1;
+    return;
+  }
+  int b, en;
+  chunk_range(chunk, e.szp, e.p, b, en);
+  double* vf = e.v + (size_t)f * e.p;
+  double* Vcol = e.V + ((size_t)f * e.K + a) * e.p;
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+    const double x = vf[i] / vn;
+    vf[i] = x;
+    Vcol[i] = x;
+  }
+  __syncthreads();
+  const double* Sf = e.S + (size_t)f * e.p * e.m;
+  for (int j = 0; j < e.m; ++j) {
+    double acc = 0.0;
+    for (int i = b + threadIdx.x; i < en; i += blockDim.x) acc += vf[i] * Sf[i + (size_t)j * e.p];
+    acc = block_sum(acc, scratch);
+    if (threadIdx.x == 0) e.vSpart[((size_t)f * e.cp + chunk) * e.m + j] = acc;
+  }
+}
+
+// S -= v (v^T S); R[:, a] = r / ||t||; Q[:, a] = q / ||t||.
+__global__ void k_deflate(Eng e, int a) {
+  extern __shared__ double vs[];
+  const int f = blockIdx.y, chunk = blockIdx.x;
+  if (e.status[f]) return;
+  int b, en;
+  chunk_range(chunk, e.szp, e.p, b, en);
+  for (int j = threadIdx.x; j < e.m; j += blockDim.x)
+    vs[j] = sum_parts(e.vSpart + (size_t)f * e.cp * e.m + j, e.cp, e.m);
+  __syncthreads();
+  double tn, st;
+  t_stats(e, f, tn, st);
+  double* Sf = e.S + (size_t)f * e.p * e.m;
+  const double* vf = e.v + (size_t)f * e.p;
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+    const double vi = vf[i];
+    for (int j = 0; j < e.m; ++j) Sf[i + (size_t)j * e.p] -= vi * vs[j];
+  }
+  double* Rcol = e.R + ((size_t)f * e.K + a) * e.p;
+  const double* rf = e.r + (size_t)f * e.p;
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) Rcol[i] = rf[i] / tn;
+  if (chunk == 0) {
+    double* Qcol = e.Q + ((size_t)f * e.K + a) * e.m;
+    for (int j = threadIdx.x; j < e.m; j += blockDim.x) {
+      double q = sum_parts(e.qpart + (size_t)f * e.cn * e.m + j, e.cn, e.m);
+      double off = 0.0;
+      if (e.labels) off += e.mY_all[j];
+      if (e.dY) off += e.dY[(size_t)f * e.m + j];
+      q -= off * st;
+      Qcol[j] = q / tn;
+    }
+    if (threadIdx.x == 0) {
+      e.tnorm[(size_t)f * e.K + a] = tn;
+      e.ncomp_done[f] = a + 1;
+    }
+  }
+}
+
+// Masked response block M[:, f*m + j] = mask_f * Y'[:, j] (Y' = one-hot or Yg).
+__global__ void k_masked_response(Eng e, double* M) {
+  const size_t total = (size_t)e.n * e.F * e.m;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int i = static_cast<int>(t % e.n);
+    const size_t col = t / e.n;
+    const int f = static_cast<int>(col / e.m), j = static_cast<int>(col % e.m);
+    const bool in = !e.mask || e.mask[(size_t)f * e.n + i];
+    double v = 0.0;
+    if (in) v = e.labels ? (e.labels[i] == j ? 1.0 : 0.0) : e.Yg[i + (size_t)j * e.n];
+    M[t] = v;
+  }
+}
+
+__global__ void k_crosscov_finish(Eng e, const double* P, const int* n_train) {
+  const size_t total = (size_t)e.F * e.p * e.m;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int i = static_cast<int>(t % e.p);
+    const size_t col = t / e.p;
+    const int f = static_cast<int>(col / e.m), j = static_cast<int>(col % e.m);
+    double v = P[i + col * e.p];
+    if (e.delta) {
+      double off = 0.0;
+      if (e.labels) off += e.mY_all[j];
+      if (e.dY) off += e.dY[(size_t)f * e.m + j];
+      v -= static_cast<double>(n_train[f]) * e.delta[(size_t)f * e.p + i] * off;
+    }
+    if (e.colscale) v *= e.colscale[(size_t)f * e.p + i];
+    e.S[(size_t)f * e.p * e.m + i + (size_t)j * e.p] = v;
+  }
+}
+
+Eng make_eng(const SimplsBatch& b) {
+  Eng e{};
+  e.n = b.n; e.p = b.p; e.m = b.m; e.F = b.F; e.K = b.K;
+  const int target = 2 * Context::get().sm_count;
+  e.cp = std::max(1, std::min(ceil_div(target, b.F), ceil_div(b.p, 128)));
+  e.szp = ceil_div(b.p, e.cp);
+  e.cp = ceil_div(b.p, e.szp);
+  e.cn = std::max(1, std::min(ceil_div(target, b.F), ceil_div(b.n, 128)));
+  e.szn = ceil_div(b.n, e.cn);
+  e.cn = ceil_div(b.n, e.szn);
+  e.Yg = b.Yg; e.labels = b.labels; e.mY_all = b.mY_all; e.mask = b.mask; e.delta = b.delta;
+  e.colscale = b.colscale; e.dY = b.dY; e.S = b.S; e.omega = b.omega; e.m1_mode = b.m1_mode;
+  e.R = b.R; e.Q = b.Q; e.V = b.V; e.tnorm = b.tnorm; e.Tkeep = b.Tkeep;
+  e.ncomp_done = b.ncomp_done; e.status = b.status;
+  return e;
+}
+
+}  // namespace
+
+void XOperatorF64::times(const double* Rhat, int F, double* U) {
+  if (F == 1) gemv(false, n, p, 1.0, Xc, n, Rhat, 0.0, U);
+  else gemm(false, false, n, F, p, 1.0, Xc, n, Rhat, p, 0.0, U, n);
+}
+
+void XOperatorF64::t_times(const double* T, int F, double* P) {
+  if (F == 1) gemv(true, n, p, 1.0, Xc, n, T, 0.0, P);
+  else gemm(true, false, p, F, n, 1.0, Xc, n, T, n, 0.0, P, p);
+}
+
+void simpls_batch_crosscov(const SimplsBatch& b, const double* /*Xc*/, const int* n_train) {
+  Context& ctx = Context::get();
+  Eng e = make_eng(b);
+  double* M = ctx.arena.alloc_n<double>((size_t)b.n * b.F * b.m);
+  double* P = ctx.arena.alloc_n<double>((size_t)b.p * b.F * b.m);
+  k_masked_response<<<2 * ctx.sm_count, kThreads, 0, ctx.stream>>>(e, M);
+  FPLS_CHECK_LAUNCH();
+  b.X->t_times(M, b.F * b.m, P);
+  k_crosscov_finish<<<2 * ctx.sm_count, kThreads, 0, ctx.stream>>>(e, P, n_train);
+  FPLS_CHECK_LAUNCH();
+}
+
+void simpls_batch_run(const SimplsBatch& b) {
+  Context& ctx = Context::get();
+  Eng e = make_eng(b);
+  Arena& ar = ctx.arena;
+  const size_t F = b.F;
+  e.y = ar.alloc_n<double>(F * b.p);
+  e.zA = ar.alloc_n<double>(F * e.cp * b.m);
+  e.zB = ar.alloc_n<double>(F * e.cp * b.m);
+  e.npart = ar.alloc_n<double>(F * e.cp);
+  e.r = ar.alloc_n<double>(F * b.p);
+  e.Rhat = ar.alloc_n<double>(F * b.p);
+  e.cpart = ar.alloc_n<double>(F * e.cp);
+  e.U = ar.alloc_n<double>(F * b.n);
+  e.T = ar.alloc_n<double>(F * b.n);
+  e.tpart = ar.alloc_n<double>(F * e.cn * 2);
+  e.qpart = ar.alloc_n<double>(F * e.cn * b.m);
+  e.P = ar.alloc_n<double>(F * b.p);
+  e.pv = ar.alloc_n<double>(F * b.p);
+  e.wpart = ar.alloc_n<double>(F * e.cp * std::max(b.K, 1));
+  e.v = ar.alloc_n<double>(F * b.p);
+  e.vpart = ar.alloc_n<double>(F * e.cp);
+  e.vSpart = ar.alloc_n<double>(F * e.cp * b.m);
+  dzero(b.status, F * sizeof(int));
+  dzero(b.ncomp_done, F * sizeof(int));
+  dzero(b.R, F * b.p * b.K * sizeof(double));
+  dzero(b.Q, F * b.m * b.K * sizeof(double));
+  dzero(b.V, F * b.p * b.K * sizeof(double));
+  dzero(b.tnorm, F * b.K * sizeof(double));
+  const dim3 gp(e.cp, b.F), gn(e.cn, b.F);
+  const size_t sm_m = std::max<size_t>(b.m, 1) * sizeof(double);
+  const size_t sm_k = std::max<size_t>(b.K, 1) * sizeof(double);
+  const int iters = b.m1_mode ? 0 : std::max(b.power_iters, 0);
+  cudaStream_t st = ctx.stream;
+  for (int a = 0; a < b.K; ++a) {
+    // Refresh: y <- S (S^T y) `iters` times from the warm start, then normalise.
+    k_refresh_start<<<gp, kThreads, 0, st>>>(e, a, iters);
+    double* zin = e.zA;
+    double* zout = e.zB;
+    for (int it = 0; it < iters; ++it) {
+      const int last = (it == iters - 1) ? 1 : 0;
+      k_refresh_apply<<<gp, kThreads, sm_m, st>>>(e, zin, zout, last);
+      std::swap(zin, zout);
+    }
+    k_refresh_finish<<<gp, kThreads, 0, st>>>(e);
+    FPLS_CHECK_LAUNCH();
+    b.X->times(e.Rhat, b.F, e.U);
+    k_scores<<<gn, kThreads, b.labels ? sm_m : 0, st>>>(e, a);
+    FPLS_CHECK_LAUNCH();
+    b.X->t_times(e.T, b.F, e.P);
+    k_loading<<<gp, kThreads, 0, st>>>(e, a);
+    k_orth<<<gp, kThreads, sm_k, st>>>(e, a);
+    k_vnorm<<<gp, kThreads, 0, st>>>(e, a);
+    k_deflate<<<gp, kThreads, sm_m, st>>>(e, a);
+    FPLS_CHECK_LAUNCH();
+  }
+}
+
+}  // namespace fpls

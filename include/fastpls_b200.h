@@ -1,0 +1,164 @@
+/*
+ * fastpls_b200 — C ABI of the B200 (sm_100a) fit/predict library for fastPLS.
+ *
+ * Every entry point replaces one `.Call` routine of the R package fastPLS
+ * (tkcaccia/fastPLS) for backend = "cuda"; the citation names the routine's
+ * registration in src/RcppExports.cpp and the engine function it runs.
+ *
+ * Conventions
+ *  - Matrices are column-major double (R / Armadillo layout); "cubes" are
+ *    rows x cols x slices, slice-major, as R arrays.
+ *  - Class labels are int32, 1-based.  ncomp vectors are int32.
+ *  - All pointers are HOST pointers owned by the caller; outputs are written
+ *    into caller-allocated buffers of the documented sizes.  Optional outputs
+ *    may be NULL.
+ *  - Every function returns 0 on success or a non-zero fpls_status; on failure a
+ *    NUL-terminated message is written to err[0..errlen-1] (err may be NULL).
+ *    No exception crosses this boundary and there is no CPU fallback: without
+ *    a B200 the calls return FPLS_ERR_NO_DEVICE.
+ *  - The library keeps one device context per process (stream, scratch arena),
+ *    used from one host thread at a time, like the reference's thread_local
+ *    CUDA workspace (src/svd_cuda_rsvd.cpp:2092).
+ */
+#ifndef FASTPLS_B200_H
+#define FASTPLS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum fpls_status {
+  FPLS_OK = 0,
+  FPLS_ERR_ARGUMENT = 1,
+  FPLS_ERR_CUDA = 2,
+  FPLS_ERR_NUMERICAL = 3,
+  FPLS_ERR_NO_DEVICE = 4,
+  FPLS_ERR_INTERNAL = 5
+};
+
+/* Precision of the predictor passes in the batched CV grid. */
+enum fpls_precision { FPLS_PREC_FP64 = 0, FPLS_PREC_BF16X3 = 1 };
+
+/* 1 when a B200 (sm_100a) device is usable.
+ * Replaces _fastPLS_has_cuda (RcppExports.cpp:87; fastPLS.cpp:1607-1609). */
+int fpls_has_cuda(void);
+
+/* Library version string. */
+const char* fpls_version(void);
+
+/* Releases the scratch arena and cached device state.
+ * Replaces _fastPLS_cuda_reset_workspace (RcppExports.cpp:107; fastPLS.cpp:1617-1620). */
+int fpls_reset_workspace(char* err, size_t errlen);
+
+/* C (a_rows x b_cols) = A (a_rows x a_cols) * B (a_cols x b_cols), FP64.
+ * Replaces _fastPLS_cuda_matrix_multiply (RcppExports.cpp:116; svd_cuda_rsvd.cpp:2106-2180). */
+int fpls_matrix_multiply(const double* A, int a_rows, int a_cols, const double* B, int b_cols,
+                         double* C, char* err, size_t errlen);
+
+/* Truncated SVD of A (rows x cols) with the CPU recipe of the reference
+ * (svd_method 3 exact, 4/5 randomized).  kcap = min(rows, cols, max(k,1));
+ * U: rows x kcap, s: kcap, Vt: kcap x cols (NULL when left_only).  *rank_out is
+ * the number of columns written (the rSVD may return fewer usable ones).
+ * Replaces _fastPLS_truncated_svd_debug (RcppExports.cpp:334; fastPLS.cpp:2229-2257). */
+int fpls_truncated_svd(const double* A, int rows, int cols, int k, int svd_method, int oversample,
+                       int power_iters, double svds_tol, int seed, int left_only, double* U,
+                       double* s, double* Vt, int* rank_out, char* err, size_t errlen);
+
+/* PLSSVD fit.  ncomp values are capped to [1, min(n,p,m)] and written to
+ * ncomp_out (L).  K0 = min(max(ncomp_out), min(n,p,m)).  Outputs:
+ * C_latent K0 x K0 x L, W_latent K0 x m x L, Q m x K0, Ttrain n x K0, R p x K0,
+ * mX p, vX p, mY m, B p x m x L (optional), Yfit n x m x L (optional, fit=1),
+ * R2Y L, s K0; *k_eff = effective rank (columns of R/Q/Ttrain written).
+ * Replaces _fastPLS_pls_model1_gpu (RcppExports.cpp:668; fastPLS.cpp:5989-6082);
+ * numerics follow pls_model1 (fastPLS.cpp:4780-4986). */
+int fpls_pls_model1(const double* X, int n, int p, const double* Y, int m, const int* ncomp, int L,
+                    int scaling, int fit, int svd_method, int oversample, int power_iters,
+                    double svds_tol, int seed, int* ncomp_out, double* C_latent, double* W_latent,
+                    double* Q, double* Ttrain, double* R, double* mX, double* vX, double* mY,
+                    double* B, double* Yfit, double* R2Y, double* s, int* k_eff, char* err,
+                    size_t errlen);
+
+/* Fast SIMPLS fit (warm-started 1-column refresh, 2 power iterations).
+ * K = max(ncomp).  Outputs: R p x K, Q m x K, mX p, vX p, mY m,
+ * B p x m x L (optional), Yfit n x m x L (optional), R2Y L; *n_components =
+ * components computed (the loop stops early on a degenerate component).
+ * Replaces _fastPLS_pls_model2_fast_gpu (RcppExports.cpp:392; fastPLS.cpp:2781-3207);
+ * numerics follow pls_model2_fast (fastPLS.cpp:2454-2778). */
+int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
+                         int L, int scaling, int fit, int seed, double* R, double* Q, double* mX,
+                         double* vX, double* mY, double* B, double* Yfit, double* R2Y,
+                         int* n_components, char* err, size_t errlen);
+
+/* Classic SIMPLS with a fresh leading left singular vector per component
+ * ("exact" mode when svd_method = 3).  K = max(ncomp).  Outputs: R p x K,
+ * Q m x K, P p x K (optional), Ttrain n x K (optional; required when fit=1),
+ * mX, vX, mY, B (optional), Yfit (optional), R2Y.
+ * Replaces _fastPLS_pls_model2 (RcppExports.cpp:352; fastPLS.cpp:2260-2451). */
+int fpls_pls_model2(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
+                    int L, int scaling, int fit, int svd_method, int oversample, int power_iters,
+                    double svds_tol, int seed, double* R, double* Q, double* P, double* Ttrain,
+                    double* mX, double* vX, double* mY, double* B, double* Yfit, double* R2Y,
+                    int* n_components, char* err, size_t errlen);
+
+/* Low-rank prediction Ypred[:,:,a] = ((Xtest - mX)/vX) R[:, :mc] W[:mc, :, a] + mY,
+ * mc = ncomp[a].  W is kmax x m x L (SIMPLS: Q^T prefixes; PLSSVD: W_latent).
+ * Ypred w x m x L; Ttest w x kmax (optional).
+ * Replaces _fastPLS_pls_predict_flash_cuda (RcppExports.cpp:425; fastPLS.cpp:3448-3585). */
+int fpls_predict_lowrank(const double* Xtest, int w, int p, const double* mX, const double* vX,
+                         const double* mY, int m, const double* R, int kmax, const double* W,
+                         const int* ncomp, int L, double* Ypred, double* Ttest, char* err,
+                         size_t errlen);
+
+/* Class prediction from the same low-rank model: per slice, the top_k classes
+ * of Ypred + class_bias (first maximum wins ties).  class_bias: m or NULL.
+ * top_index w x top_k x L (1-based), top_score w x top_k x L (optional).
+ * Replaces _fastPLS_pls_class_predict_topk_cuda (RcppExports.cpp:468;
+ * fastPLS.cpp:3863-4113) and pls_predict_classes_compact_cuda (fastPLS.cpp:4156-4201). */
+int fpls_predict_classes(const double* Xtest, int w, int p, const double* mX, const double* vX,
+                         const double* mY, int m, const double* R, int kmax, const double* W,
+                         const int* ncomp, int L, const double* class_bias, int top_k,
+                         int* top_index, double* top_score, char* err, size_t errlen);
+
+/* Prefix LDA models on latent scores T (n x kmax), labels y (n, 1-based).
+ * For slice a (kk = ncomp[a]): means[:, :kk, a] (C x kmax x L, ld C),
+ * linear[:, :kk, a] (C x kmax x L), constants[:, a] (C x L), priors C,
+ * lambda L.  Replaces _fastPLS_lda_train_prefix_cuda (RcppExports.cpp:225);
+ * numerics follow lda_train_prefix_cpp (fastPLS.cpp:1817-1927). */
+int fpls_lda_train_prefix(const double* T, int n, int kmax, const int* y, int n_classes,
+                          const int* ncomp, int L, double ridge, double* means, double* linear,
+                          double* constants, double* priors, double* lambda, char* err,
+                          size_t errlen);
+
+/* Same on projected scores T = X R - offset (X n x p, R p x k, offset k).
+ * Replaces _fastPLS_lda_project_train_prefix_cuda (RcppExports.cpp:240;
+ * fastPLS.cpp:1930-1957). */
+int fpls_lda_project_train_prefix(const double* X, int n, int p, const double* R, int k,
+                                  const double* offset, const int* y, int n_classes,
+                                  const int* ncomp, int L, double ridge, double* means,
+                                  double* linear, double* constants, double* priors,
+                                  double* lambda, char* err, size_t errlen);
+
+/* LDA labels for scores T (w x k): argmax_c T linear^T + constants.
+ * linear: C x k, constants: C.  labels w; scores w x C (optional, includes constants).
+ * Replaces _fastPLS_lda_predict_cuda / _lda_predict_labels_cuda (RcppExports.cpp:295, 307). */
+int fpls_lda_predict(const double* T, int w, int k, const double* linear,
+                     const double* constants, int n_classes, int* labels, double* scores,
+                     char* err, size_t errlen);
+
+/* LDA labels for predictors X (w x p) with projection R (p x k) and offset (k):
+ * the direct route X (R linear^T) when cheaper, else (X R - offset) linear^T.
+ * scores (optional) w x C = (X R) linear^T + constants - offset linear^T.
+ * Replaces _fastPLS_lda_project_predict_cuda (RcppExports.cpp:319;
+ * fastPLS.cpp:2100-2147 for the route rule). */
+int fpls_lda_project_predict(const double* X, int w, int p, const double* R, int k,
+                             const double* offset, const double* linear,
+                             const double* constants, int n_classes, int* labels,
+                             double* scores, char* err, size_t errlen);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTPLS_B200_H */

@@ -53,6 +53,11 @@ SIGNATURES = {
     "fpls_lda_predict": ([_DP, _I, _I, _DP, _DP, _I, _IP, _DP, _C, _S], ctypes.c_int),
     "fpls_lda_project_predict": ([_DP, _I, _I, _DP, _I, _DP, _DP, _DP, _I, _IP, _DP, _C, _S],
                                  ctypes.c_int),
+    "fpls_bf16x3_gemm": ([_DP, _I, _I, _DP, _I, _DP, _C, _S], ctypes.c_int),
+    "fpls_cv_predict": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I, _I, _I,
+                         _I, _IP, _IP, _C, _S], ctypes.c_int),
+    "fpls_double_cv": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I,
+                        _I, _I, _I, _IP, _DP, _IP, _IP, _IP, _C, _S], ctypes.c_int),
 }
 
 
@@ -358,3 +363,68 @@ def lda_project_predict(X, R, offset, lda, return_scores=False):
     _call("fpls_lda_project_predict", _p(X), w, p, _p(R), k, _p(off), _p(lin), _p(const), C,
           _p(lab), _p(sc))
     return dict(pred=lab, scores=sc) if return_scores else dict(pred=lab)
+
+
+PREC = {"fp64": 0, "bf16x3": 1}
+
+
+def bf16x3_gemm(A, B):
+    """C = A B through the BF16 split-precision tensor-core kernel (diagnostic)."""
+    A = _f64(A)
+    B = _f64(B)
+    C = _out(A.shape[0], B.shape[1])
+    _call("fpls_bf16x3_gemm", _p(A), A.shape[0], A.shape[1], _p(B), B.shape[1], _p(C))
+    return C
+
+
+def _x_arg(X):
+    if np.asarray(X).dtype == np.float32:
+        Xa = np.asfortranarray(X, dtype=np.float32)
+        return Xa, 1
+    return _f64(X), 0
+
+
+def cv_predict(X, y, fold, ncomp, n_classes, method=3, scaling=1, seed=1, precision="fp64",
+               batched=True):
+    """Cross-validated class predictions (argmax classifier), folds 0-based."""
+    Xa, is32 = _x_arg(X)
+    n, p = Xa.shape
+    yy = _i32(y)
+    fd = _i32(fold)
+    nc = _i32(np.atleast_1d(ncomp))
+    L = nc.size
+    kfold = int(fd.max()) + 1
+    cp = np.zeros((n, L), dtype=np.int32, order="F")
+    st = np.zeros(kfold, dtype=np.int32)
+    _call("fpls_cv_predict", Xa.ctypes.data, is32, n, p, _p(yy), int(n_classes), _p(fd), kfold,
+          _p(nc), L, int(method), int(scaling), int(seed), PREC[precision], int(bool(batched)),
+          cp.ctypes.data_as(_c_int_p), _p(st))
+    return dict(class_pred=cp, status=st)
+
+
+def double_cv(X, y, outer_fold, inner_fold, ncomp, n_classes, scaling=1, seed=1, run=1,
+              precision="fp64", batched=True, return_inner=False):
+    """Double CV of SIMPLS PLS-DA over the supplied outer/inner folds (0-based)."""
+    Xa, is32 = _x_arg(X)
+    n, p = Xa.shape
+    yy = _i32(y)
+    of = _i32(outer_fold)
+    inf_ = np.asfortranarray(np.asarray(inner_fold, dtype=np.int32))
+    Ko = int(of.max()) + 1
+    Ki = int(inf_.max()) + 1
+    nc = _i32(np.atleast_1d(ncomp))
+    L = nc.size
+    best = np.zeros(Ko, dtype=np.int32)
+    acc = _out(Ko, L)
+    pred = np.zeros(n, dtype=np.int32)
+    inner = np.zeros((n, L, Ko), dtype=np.int32, order="F") if return_inner else None
+    fst = np.zeros(Ko * Ki + Ko, dtype=np.int32)
+    _call("fpls_double_cv", Xa.ctypes.data, is32, n, p, _p(yy), int(n_classes), _p(of), Ko,
+          inf_.ctypes.data_as(_c_int_p), Ki, _p(nc), L, int(scaling), int(seed), int(run),
+          PREC[precision], int(bool(batched)), _p(best), _p(acc), _p(pred),
+          None if inner is None else inner.ctypes.data_as(_c_int_p), _p(fst))
+    out = dict(best_comp=best, inner_accuracy=acc, pred=pred, fit_status=fst,
+               accuracy=float(np.mean(pred == yy)))
+    if return_inner:
+        out["inner_pred"] = inner
+    return out

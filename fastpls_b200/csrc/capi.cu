@@ -2,15 +2,18 @@
 #include "../../include/fastpls_b200.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "blas_f64.cuh"
 #include "context.cuh"
+#include "cv_driver.cuh"
 #include "fits.cuh"
 #include "heads.cuh"
 #include "simpls_engine.cuh"
 #include "svd.cuh"
+#include "xop_split.cuh"
 
 using namespace fpls;
 
@@ -572,6 +575,170 @@ int fpls_lda_project_predict(const double* X, int w, int p, const double* R, int
       download(scores, dS, (size_t)w * n_classes);
     }
     ctx.sync();
+  });
+}
+
+int fpls_bf16x3_gemm(const double* A, int M, int K, const double* B, int N, double* C, char* err,
+                     size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(M > 0 && N > 0 && K > 0, "bf16x3_gemm: dimensions must be positive");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* dA = upload(A, (size_t)M * K);
+    const double* dB = upload(B, (size_t)K * N);
+    double* dC = ctx.arena.alloc_n<double>((size_t)M * N);
+    dzero(ctx.d_status + 16, sizeof(int));
+    split_gemm_test(dA, dB, M, N, K, dC);
+    download(C, dC, (size_t)M * N);
+    int e = 0;
+    d2h(&e, ctx.d_status + 16, sizeof(int));
+    ctx.sync();
+    if (e) throw Error(FPLS_ERR_CUDA, "tensor-core pipeline wait timed out");
+  });
+}
+
+static void run_cv_grid(const CvFitSet& fs, const void* X, int x_is_float32, const int* y,
+                        const int* ncomp, int L, int scaling, int precision, int batched,
+                        CvGridResult& res) {
+  Context& ctx = Context::get();
+  FPLS_REQUIRE(precision == FPLS_PREC_FP64 || precision == FPLS_PREC_BF16X3, "unknown precision");
+  CvGridOptions opt;
+  opt.scaling = scaling;
+  opt.precision = precision;
+  opt.batched = batched != 0;
+  if (const char* e = std::getenv("FASTPLS_FAST_INC_ITERS")) {
+    char* endp = nullptr;
+    long v = std::strtol(e, &endp, 10);
+    if (endp != e) opt.power_iters = static_cast<int>(std::min(6L, std::max(1L, v)));
+  }
+  const size_t np = (size_t)fs.n * fs.p;
+  dzero(ctx.d_status + 16, sizeof(int));
+  if (x_is_float32) {
+    const float* d = upload(static_cast<const float*>(X), np);
+    cv_grid_classify(fs, nullptr, d, y, ncomp, L, opt, res);
+  } else {
+    const double* d = upload(static_cast<const double*>(X), np);
+    cv_grid_classify(fs, d, nullptr, y, ncomp, L, opt, res);
+  }
+  int e = 0;
+  d2h(&e, ctx.d_status + 16, sizeof(int));
+  ctx.sync();
+  if (e) throw Error(FPLS_ERR_CUDA, "tensor-core pipeline wait timed out");
+}
+
+int fpls_cv_predict(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                    const int* fold, int kfold, const int* ncomp, int L, int method, int scaling,
+                    int seed, int precision, int batched, int* class_pred, int* status,
+                    char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n >= 2 && p > 0, "Xdata must contain at least two samples");
+    FPLS_REQUIRE(n_classes >= 1, "n_classes must be >= 1");
+    FPLS_REQUIRE(method == 3 || method == 2, "the GPU CV grid runs method 3 (simpls_fast)");
+    FPLS_REQUIRE(kfold >= 1 && L >= 1, "kfold and ncomp must be >= 1");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    CvFitSet fs;
+    fs.n = n; fs.p = p; fs.m = n_classes; fs.F = kfold; fs.G = 1;
+    fs.train.assign((size_t)kfold * n, 0);
+    fs.test.assign((size_t)kfold * n, 0);
+    fs.group.assign(kfold, 0);
+    fs.seeds.resize(kfold);
+    for (int f = 0; f < kfold; ++f) {
+      fs.seeds[f] = static_cast<unsigned>(seed + f);
+      for (int i = 0; i < n; ++i) {
+        FPLS_REQUIRE(fold[i] >= 0 && fold[i] < kfold, "fold ids must be in 0..kfold-1");
+        (fold[i] == f ? fs.test : fs.train)[(size_t)f * n + i] = 1;
+      }
+    }
+    std::vector<int> nc(ncomp, ncomp + L);
+    for (int& c : nc) c = std::max(1, c);
+    CvGridResult res;
+    run_cv_grid(fs, X, x_is_float32, y, nc.data(), L, scaling, precision, batched, res);
+    std::copy(res.pred.begin(), res.pred.end(), class_pred);
+    if (status) std::copy(res.status.begin(), res.status.end(), status);
+  });
+}
+
+int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                   const int* outer_fold, int kfold_outer, const int* inner_fold, int kfold_inner,
+                   const int* ncomp, int L, int scaling, int seed, int run, int precision,
+                   int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
+                   int* inner_pred, int* fit_status, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n >= 2 && p > 0, "Xdata must contain at least two samples");
+    FPLS_REQUIRE(kfold_outer >= 1 && kfold_inner >= 1 && L >= 1, "fold counts and ncomp must be >= 1");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const int Ko = kfold_outer, Ki = kfold_inner;
+    std::vector<int> nc(ncomp, ncomp + L);
+    for (int& c : nc) c = std::max(1, c);
+    CvFitSet fs;
+    fs.n = n; fs.p = p; fs.m = n_classes; fs.F = Ko * Ki + Ko; fs.G = Ko + 1;
+    fs.train.assign((size_t)fs.F * n, 0);
+    fs.test.assign((size_t)fs.F * n, 0);
+    fs.group.assign(fs.F, 0);
+    fs.seeds.resize(fs.F);
+    std::vector<int> outer_classes(Ko, 0), fallback(Ko, 1);
+    for (int o = 0; o < Ko; ++o) {
+      std::vector<int> cnt(n_classes, 0);
+      for (int i = 0; i < n; ++i)
+        if (outer_fold[i] != o) cnt[y[i] - 1]++;
+      int best = 0;
+      for (int c = 0; c < n_classes; ++c) {
+        if (cnt[c] > 0) outer_classes[o]++;
+        if (cnt[c] > cnt[best]) best = c;
+      }
+      fallback[o] = best + 1;
+    }
+    for (int o = 0; o < Ko; ++o) {
+      const bool skip = outer_classes[o] < 2;  // pls.double.cv's single-class fallback
+      for (int i0 = 0; i0 < Ki; ++i0) {
+        const int f = o * Ki + i0;
+        fs.group[f] = o;
+        fs.seeds[f] = static_cast<unsigned>(seed + 1000 * run + (o + 1) + i0);
+        if (skip) continue;
+        for (int i = 0; i < n; ++i) {
+          if (outer_fold[i] == o) continue;
+          const int fi = inner_fold[i + (size_t)o * n];
+          if (fi == i0) fs.test[(size_t)f * n + i] = 1;
+          else fs.train[(size_t)f * n + i] = 1;
+        }
+      }
+      const int f = Ko * Ki + o;
+      fs.group[f] = Ko;
+      fs.seeds[f] = static_cast<unsigned>(seed + 2000 * run + (o + 1));
+      if (skip) continue;
+      for (int i = 0; i < n; ++i) (outer_fold[i] == o ? fs.test : fs.train)[(size_t)f * n + i] = 1;
+    }
+    CvGridResult res;
+    run_cv_grid(fs, X, x_is_float32, y, nc.data(), L, scaling, precision, batched, res);
+    // Inner accuracy per (outer fold, ncomp) and the chosen ncomp (first maximum).
+    for (int o = 0; o < Ko; ++o) {
+      int bi = 0;
+      double bv = -1.0;
+      bool any = false;
+      for (int s = 0; s < L; ++s) {
+        long long ok = 0, tot = 0;
+        const int* pr = res.pred.data() + ((size_t)o * L + s) * n;
+        for (int i = 0; i < n; ++i) {
+          if (outer_fold[i] == o || pr[i] < 1) continue;
+          ++tot;
+          ok += (pr[i] == y[i]);
+        }
+        const double acc = tot ? static_cast<double>(ok) / tot : std::nan("");
+        if (inner_accuracy) inner_accuracy[o + (size_t)s * Ko] = acc;
+        if (std::isfinite(acc) && (!any || acc > bv)) { bv = acc; bi = s; any = true; }
+      }
+      const bool skip = outer_classes[o] < 2;
+      int bc = skip ? *std::min_element(nc.begin(), nc.end()) : nc[bi];
+      if (best_comp) best_comp[o] = bc;
+      for (int i = 0; i < n; ++i) {
+        if (outer_fold[i] != o) continue;
+        outer_pred[i] = skip ? fallback[o] : res.pred[((size_t)Ko * L + bi) * n + i];
+      }
+    }
+    if (inner_pred) std::copy(res.pred.begin(), res.pred.begin() + (size_t)Ko * L * n, inner_pred);
+    if (fit_status) std::copy(res.status.begin(), res.status.end(), fit_status);
   });
 }
 

@@ -1,0 +1,367 @@
+#include "blas_f64.cuh"
+#include "context.cuh"
+#include "cv_driver.cuh"
+#include "fits.cuh"
+#include "heads.cuh"
+#include "simpls_engine.cuh"
+#include "svd.cuh"
+#include "xop_split.cuh"
+
+#include <algorithm>
+#include <memory>
+#include <numeric>
+
+namespace fpls {
+namespace {
+
+constexpr int kMaxClassesCv = 128;
+
+__global__ void widen_f32_kernel(const float* __restrict__ src, double* __restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = static_cast<double>(src[i]);
+}
+
+__global__ void mask_to_double_kernel(const uint8_t* __restrict__ mask, size_t total,
+                                      double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = mask[i] ? 1.0 : 0.0;
+}
+
+__global__ void scale_cols_kernel(double* P, int p, int F, const double* inv_nf) {
+  const size_t total = (size_t)p * F;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x)
+    P[t] *= inv_nf[t / p];
+}
+
+// Gathers rows `idx` (device, cnt) of X (n x p) into out (cnt x p).
+__global__ void gather_rows_kernel(const double* __restrict__ X, int n, int p,
+                                   const int* __restrict__ idx, int cnt, double* __restrict__ out) {
+  const size_t total = (size_t)cnt * p;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int r = static_cast<int>(t % cnt);
+    const int j = static_cast<int>(t / cnt);
+    out[t] = X[idx[r] + (size_t)j * n];
+  }
+}
+
+__global__ void onehot_kernel(const int* __restrict__ lab0, int cnt, int m, double* Y) {
+  const size_t total = (size_t)cnt * m;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int r = static_cast<int>(t % cnt);
+    const int j = static_cast<int>(t / cnt);
+    Y[t] = (lab0[r] == j) ? 1.0 : 0.0;
+  }
+}
+
+// Class predictions of the test rows of every fit for every ncomp slice from the
+// kept scores: y_a = sum_{b<=a} (t_b[i] / ||t_b||) q_b + mY_f, label = first argmax.
+__global__ void cv_predict_kernel(int F, int n, int m, int K, int L, const int* __restrict__ ncomp,
+                                  const uint8_t* __restrict__ test, const int* __restrict__ group,
+                                  const double* __restrict__ Tkeep, const double* __restrict__ tnorm,
+                                  const double* __restrict__ Q, const int* __restrict__ ncomp_done,
+                                  const double* __restrict__ mYf, int* __restrict__ pred) {
+  const int f = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !test[(size_t)f * n + i]) return;
+  const int done = ncomp_done[f];
+  const int g = group[f];
+  double y[kMaxClassesCv];
+  for (int j = 0; j < m; ++j) y[j] = 0.0;
+  const double* Qf = Q + (size_t)f * m * K;
+  for (int a = 0; a < K; ++a) {
+    if (a < done) {
+      const double c = Tkeep[((size_t)f * K + a) * n + i] / tnorm[(size_t)f * K + a];
+      for (int j = 0; j < m; ++j) y[j] += c * Qf[j + (size_t)a * m];
+    }
+    for (int s = 0; s < L; ++s) {
+      if (ncomp[s] != a + 1) continue;
+      int best = 0;
+      double bv = y[0] + mYf[(size_t)f * m];
+      for (int j = 1; j < m; ++j) {
+        const double v = y[j] + mYf[(size_t)f * m + j];
+        if (v > bv) { bv = v; best = j; }
+      }
+      pred[((size_t)g * L + s) * n + i] = best + 1;
+    }
+  }
+}
+
+// Fold status and class counts of each fit (host): the reference's rules
+// (fastPLS.cpp:6805-6870): 2 empty test fold, 3 no training rows, 4 at most
+// one class present in the training rows (constant prediction).
+void classify_fits(const CvFitSet& fs, const int* y, std::vector<int>& status,
+                   std::vector<int>& fallback, std::vector<double>& counts) {
+  status.assign(fs.F, 1);
+  fallback.assign(fs.F, 1);
+  counts.assign((size_t)fs.F * fs.m, 0.0);
+  for (int f = 0; f < fs.F; ++f) {
+    int ntest = 0, ntrain = 0;
+    for (int i = 0; i < fs.n; ++i) {
+      if (fs.test[(size_t)f * fs.n + i]) ++ntest;
+      if (fs.train[(size_t)f * fs.n + i]) {
+        ++ntrain;
+        counts[(size_t)f * fs.m + (y[i] - 1)] += 1.0;
+      }
+    }
+    if (ntest == 0) { status[f] = 2; continue; }
+    if (ntrain == 0) { status[f] = 3; continue; }
+    int active = 0, last = -1;
+    for (int c = 0; c < fs.m; ++c)
+      if (counts[(size_t)f * fs.m + c] > 0.5) { ++active; last = c; }
+    if (active <= 1) {
+      status[f] = 4;
+      fallback[f] = active == 1 ? last + 1 : 1;
+    }
+  }
+}
+
+void fill_special_predictions(const CvFitSet& fs, const int* y, const std::vector<int>& status,
+                              const std::vector<int>& fallback, int L, std::vector<int>& pred) {
+  for (int f = 0; f < fs.F; ++f) {
+    if (status[f] == 1 || status[f] == 2) continue;
+    const int g = fs.group[f];
+    for (int i = 0; i < fs.n; ++i) {
+      if (!fs.test[(size_t)f * fs.n + i]) continue;
+      const int v = status[f] == 3 ? y[i] : fallback[f];
+      for (int s = 0; s < L; ++s) pred[((size_t)g * L + s) * fs.n + i] = v;
+    }
+  }
+}
+
+void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, int L,
+                 const CvGridOptions& opt, const std::vector<int>& status,
+                 const std::vector<double>& counts, CvGridResult& res) {
+  Context& ctx = Context::get();
+  Arena& ar = ctx.arena;
+  const int n = fs.n, p = fs.p, m = fs.m;
+  const int K = *std::max_element(ncomp, ncomp + L);
+  FPLS_REQUIRE(m <= kMaxClassesCv, "batched CV supports at most 128 classes");
+  // Active fits only (status 1) go to the engine.
+  std::vector<int> act;
+  for (int f = 0; f < fs.F; ++f)
+    if (status[f] == 1) act.push_back(f);
+  const int Fa = static_cast<int>(act.size());
+  res.ncomp_done.assign(fs.F, 0);
+  if (Fa == 0) return;
+  // Global centring (scaling < 3): Xc = X - mean(X); folds shift by delta_f.
+  const bool center = opt.scaling < 3;
+  if (center) {
+    double* mall = ar.alloc_n<double>(p);
+    col_mean(X, n, p, n, mall);
+    center_scale(X, n, p, n, mall, nullptr);
+  }
+  std::unique_ptr<XOperator> xop;
+  if (opt.precision == 1) xop = make_split_operator(X, n, p);
+  else xop.reset(new XOperatorF64(X, n, p));
+  std::vector<uint8_t> tr((size_t)Fa * n), te((size_t)Fa * n);
+  std::vector<int> grp(Fa), ntrain(Fa);
+  std::vector<double> inv_nf(Fa), mYf((size_t)Fa * m), mYall(m, 0.0), dY((size_t)Fa * m);
+  for (int i = 0; i < n; ++i) mYall[y[i] - 1] += 1.0 / n;
+  std::vector<double> om((size_t)Fa * p);
+  for (int a = 0; a < Fa; ++a) {
+    const int f = act[a];
+    std::copy(fs.train.begin() + (size_t)f * n, fs.train.begin() + (size_t)(f + 1) * n, tr.begin() + (size_t)a * n);
+    std::copy(fs.test.begin() + (size_t)f * n, fs.test.begin() + (size_t)(f + 1) * n, te.begin() + (size_t)a * n);
+    grp[a] = fs.group[f];
+    int nt = 0;
+    for (int i = 0; i < n; ++i) nt += fs.train[(size_t)f * n + i];
+    ntrain[a] = nt;
+    inv_nf[a] = 1.0 / nt;
+    for (int c = 0; c < m; ++c) {
+      mYf[(size_t)a * m + c] = counts[(size_t)f * m + c] / nt;
+      dY[(size_t)a * m + c] = mYf[(size_t)a * m + c] - mYall[c];
+    }
+    host_gaussian(om.data() + (size_t)a * p, p, fs.seeds[f]);
+  }
+  uint8_t* d_tr = ar.alloc_n<uint8_t>(tr.size());
+  uint8_t* d_te = ar.alloc_n<uint8_t>(te.size());
+  int* d_grp = ar.alloc_n<int>(Fa);
+  int* d_nt = ar.alloc_n<int>(Fa);
+  double* d_inv = ar.alloc_n<double>(Fa);
+  double* d_mYf = ar.alloc_n<double>(mYf.size());
+  double* d_mYall = ar.alloc_n<double>(m);
+  double* d_dY = ar.alloc_n<double>(dY.size());
+  double* d_om = ar.alloc_n<double>(om.size());
+  int* d_lab = ar.alloc_n<int>(n);
+  int* d_nc = ar.alloc_n<int>(L);
+  std::vector<int> lab0(n);
+  for (int i = 0; i < n; ++i) lab0[i] = y[i] - 1;
+  h2d(d_tr, tr.data(), tr.size());
+  h2d(d_te, te.data(), te.size());
+  h2d(d_grp, grp.data(), Fa * sizeof(int));
+  h2d(d_nt, ntrain.data(), Fa * sizeof(int));
+  h2d(d_inv, inv_nf.data(), Fa * sizeof(double));
+  h2d(d_mYf, mYf.data(), mYf.size() * sizeof(double));
+  h2d(d_mYall, mYall.data(), m * sizeof(double));
+  h2d(d_dY, dY.data(), dY.size() * sizeof(double));
+  h2d(d_om, om.data(), om.size() * sizeof(double));
+  h2d(d_lab, lab0.data(), n * sizeof(int));
+  h2d(d_nc, ncomp, L * sizeof(int));
+  SimplsBatch b;
+  b.n = n; b.p = p; b.m = m; b.F = Fa; b.K = K;
+  b.power_iters = opt.power_iters;
+  b.X = xop.get();
+  b.labels = d_lab;
+  b.mY_all = d_mYall;
+  b.mask = d_tr;
+  b.dY = d_dY;
+  b.omega = d_om;
+  b.m1_mode = (m == 1);
+  double* delta = nullptr;
+  if (center) {
+    double* Mtr = ar.alloc_n<double>((size_t)Fa * n);
+    delta = ar.alloc_n<double>((size_t)Fa * p);
+    mask_to_double_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(d_tr, (size_t)Fa * n, Mtr);
+    FPLS_CHECK_LAUNCH();
+    xop->t_times(Mtr, Fa, delta);
+    scale_cols_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(delta, p, Fa, d_inv);
+    FPLS_CHECK_LAUNCH();
+  }
+  b.delta = delta;
+  b.S = ar.alloc_n<double>((size_t)Fa * p * m);
+  simpls_batch_crosscov(b, X, d_nt);
+  b.R = ar.alloc_n<double>((size_t)Fa * p * K);
+  b.Q = ar.alloc_n<double>((size_t)Fa * m * K);
+  b.V = ar.alloc_n<double>((size_t)Fa * p * K);
+  b.tnorm = ar.alloc_n<double>((size_t)Fa * K);
+  b.Tkeep = ar.alloc_n<double>((size_t)Fa * n * K);
+  b.ncomp_done = ar.alloc_n<int>(Fa);
+  b.status = ar.alloc_n<int>(Fa);
+  simpls_batch_run(b);
+  int* d_pred = ar.alloc_n<int>((size_t)fs.G * L * n);
+  dzero(d_pred, (size_t)fs.G * L * n * sizeof(int));
+  cv_predict_kernel<<<dim3(ceil_div(n, 128), Fa), 128, 0, ctx.stream>>>(
+      Fa, n, m, K, L, d_nc, d_te, d_grp, b.Tkeep, b.tnorm, b.Q, b.ncomp_done, d_mYf, d_pred);
+  FPLS_CHECK_LAUNCH();
+  std::vector<int> pred((size_t)fs.G * L * n);
+  std::vector<int> done(Fa);
+  d2h(pred.data(), d_pred, pred.size() * sizeof(int));
+  d2h(done.data(), b.ncomp_done, Fa * sizeof(int));
+  ctx.sync();
+  for (size_t t = 0; t < pred.size(); ++t)
+    if (pred[t] != 0) res.pred[t] = pred[t];
+  for (int a = 0; a < Fa; ++a) res.ncomp_done[act[a]] = done[a];
+}
+
+void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int* ncomp, int L,
+                    const CvGridOptions& opt, const std::vector<int>& status, CvGridResult& res) {
+  Context& ctx = Context::get();
+  Arena& ar = ctx.arena;
+  const int n = fs.n, p = fs.p, m = fs.m;
+  const int K = *std::max_element(ncomp, ncomp + L);
+  res.ncomp_done.assign(fs.F, 0);
+  // Per-fit buffers sized for the largest fold, reused fit after fit.
+  double* Xf = ar.alloc_n<double>((size_t)n * p);
+  double* Xt = ar.alloc_n<double>((size_t)n * p);
+  double* Yf = ar.alloc_n<double>((size_t)n * m);
+  int* d_idx = ar.alloc_n<int>(n);
+  int* d_lab = ar.alloc_n<int>(n);
+  double* mX = ar.alloc_n<double>(p);
+  double* vX = ar.alloc_n<double>(p);
+  double* mY = ar.alloc_n<double>(m);
+  double* om = ar.alloc_n<double>(p);
+  double* S = ar.alloc_n<double>((size_t)p * m);
+  double* R = ar.alloc_n<double>((size_t)p * K);
+  double* Q = ar.alloc_n<double>((size_t)m * K);
+  double* V = ar.alloc_n<double>((size_t)p * K);
+  double* tn = ar.alloc_n<double>(K);
+  int* ncd = ar.alloc_n<int>(1);
+  int* st = ar.alloc_n<int>(1);
+  double* W = ar.alloc_n<double>((size_t)K * m * L);
+  double* T = ar.alloc_n<double>((size_t)n * K);
+  double* Yp = ar.alloc_n<double>((size_t)n * m * L);
+  int* lab = ar.alloc_n<int>((size_t)n * L);
+  std::vector<double> omh(p), Wh((size_t)K * m * L), Qh((size_t)m * K);
+  std::vector<int> rows, trows, labs, labh((size_t)n * L);
+  for (int f = 0; f < fs.F; ++f) {
+    if (status[f] != 1) continue;
+    rows.clear();
+    trows.clear();
+    labs.clear();
+    for (int i = 0; i < n; ++i) {
+      if (fs.train[(size_t)f * n + i]) { rows.push_back(i); labs.push_back(y[i] - 1); }
+      if (fs.test[(size_t)f * n + i]) trows.push_back(i);
+    }
+    const int nf = static_cast<int>(rows.size());
+    const int nt = static_cast<int>(trows.size());
+    h2d(d_idx, rows.data(), nf * sizeof(int));
+    h2d(d_lab, labs.data(), nf * sizeof(int));
+    gather_rows_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(X, n, p, d_idx, nf, Xf);
+    onehot_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(d_lab, nf, m, Yf);
+    FPLS_CHECK_LAUNCH();
+    center_scale_xy(Xf, nf, p, Yf, m, opt.scaling, mX, vX, mY);
+    gemm(true, false, p, m, nf, 1.0, Xf, nf, Yf, nf, 0.0, S, p);
+    host_gaussian(omh.data(), p, fs.seeds[f]);
+    h2d(om, omh.data(), p * sizeof(double));
+    XOperatorF64 xop(Xf, nf, p);
+    SimplsBatch b;
+    b.n = nf; b.p = p; b.m = m; b.F = 1; b.K = K;
+    b.power_iters = opt.power_iters;
+    b.X = &xop;
+    b.Yg = Yf;
+    b.S = S;
+    b.omega = om;
+    b.m1_mode = (m == 1);
+    b.R = R; b.Q = Q; b.V = V; b.tnorm = tn; b.ncomp_done = ncd; b.status = st;
+    simpls_batch_run(b);
+    // Compact class prediction of the test rows (pls_predict_classes_compact_cuda).
+    d2h(Qh.data(), Q, (size_t)m * K * sizeof(double));
+    int done = 0;
+    d2h(&done, ncd, sizeof(int));
+    ctx.sync();
+    res.ncomp_done[f] = done;
+    std::fill(Wh.begin(), Wh.end(), 0.0);
+    for (int s = 0; s < L; ++s)
+      for (int a = 0; a < ncomp[s]; ++a)
+        for (int j = 0; j < m; ++j) Wh[a + (size_t)j * K + (size_t)s * K * m] = Qh[j + (size_t)a * m];
+    h2d(W, Wh.data(), Wh.size() * sizeof(double));
+    h2d(d_idx, trows.data(), nt * sizeof(int));
+    gather_rows_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(X, n, p, d_idx, nt, Xt);
+    FPLS_CHECK_LAUNCH();
+    center_scale(Xt, nt, p, nt, mX, opt.scaling == 2 ? vX : nullptr);
+    lowrank_predict(Xt, nt, p, R, K, W, m, ncomp, L, mY, T, Yp);
+    for (int s = 0; s < L; ++s) row_argmax(Yp + (size_t)s * nt * m, nt, m, nullptr, lab + (size_t)s * nt);
+    d2h(labh.data(), lab, (size_t)nt * L * sizeof(int));
+    ctx.sync();
+    const int g = fs.group[f];
+    for (int s = 0; s < L; ++s)
+      for (int r = 0; r < nt; ++r) res.pred[((size_t)g * L + s) * n + trows[r]] = labh[(size_t)s * nt + r];
+  }
+}
+
+}  // namespace
+
+void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
+                      const int* labels_host, const int* ncomp, int L,
+                      const CvGridOptions& opt, CvGridResult& res) {
+  Context& ctx = Context::get();
+  FPLS_REQUIRE(L >= 1, "ncomp must contain at least one value");
+  for (int s = 0; s < L; ++s) FPLS_REQUIRE(ncomp[s] >= 1, "ncomp values must be >= 1");
+  for (int i = 0; i < fs.n; ++i)
+    FPLS_REQUIRE(labels_host[i] >= 1 && labels_host[i] <= fs.m, "labels must be in 1..n_classes");
+  FPLS_REQUIRE(fs.p > 5 || fs.m == 1, "CV with <= 5 predictors is not supported on the GPU path");
+  std::vector<int> status, fallback;
+  std::vector<double> counts;
+  classify_fits(fs, labels_host, status, fallback, counts);
+  res.status = status;
+  res.pred.assign((size_t)fs.G * L * fs.n, 0);
+  fill_special_predictions(fs, labels_host, status, fallback, L, res.pred);
+  // Working FP64 copy of X (the batched path centres it in place).
+  double* X = ctx.arena.alloc_n<double>((size_t)fs.n * fs.p);
+  if (x64) {
+    d2d(X, x64, (size_t)fs.n * fs.p * sizeof(double));
+  } else {
+    widen_f32_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(x32, X, (size_t)fs.n * fs.p);
+    FPLS_CHECK_LAUNCH();
+  }
+  const bool batched = opt.batched && opt.scaling != 2;
+  if (batched) run_batched(fs, X, labels_host, ncomp, L, opt, status, counts, res);
+  else run_sequential(fs, X, labels_host, ncomp, L, opt, status, res);
+}
+
+}  // namespace fpls

@@ -1,0 +1,43 @@
+// Cross-validation grids on the device: every fold fit of a CV (or double CV)
+// runs in one batched SIMPLS engine pass over one resident predictor matrix,
+// and the test rows' class predictions for every ncomp come from the scores
+// of the same passes (no extra pass over X).
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace fpls {
+
+// A set of classification fits over the rows of a resident matrix.
+struct CvFitSet {
+  int n = 0, p = 0, m = 0;          // rows, predictors, classes
+  int F = 0;                        // fits
+  int G = 0;                        // prediction groups
+  std::vector<uint8_t> train;       // F x n
+  std::vector<uint8_t> test;        // F x n
+  std::vector<int> group;           // F: prediction group of each fit
+  std::vector<unsigned> seeds;      // F
+};
+
+struct CvGridOptions {
+  int scaling = 1;                  // 1 centre, 2 autoscale, 3 none
+  int precision = 0;                // 0 FP64, 1 BF16x3 split
+  bool batched = true;              // false: one fit after another (plain drop-in path)
+  int power_iters = 2;              // FASTPLS_FAST_INC_ITERS
+};
+
+struct CvGridResult {
+  std::vector<int> pred;            // G x L x n (0 where the row is not predicted)
+  std::vector<int> ncomp_done;      // F
+  std::vector<int> status;          // F: 1 ok, 2 empty test, 3 no train, 4 degenerate
+};
+
+// X: device predictor matrix n x p, FP64 (x64) or FP32 (x32, exactly widened).
+// labels_host: 1-based class labels.  ncomp: L values (host).
+void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
+                      const int* labels_host, const int* ncomp, int L,
+                      const CvGridOptions& opt, CvGridResult& res);
+
+}  // namespace fpls

@@ -1,0 +1,484 @@
+// BF16 split-precision GEMM on the sm_100a tensor cores (tcgen05 + TMA + TMEM).
+//
+//   C (M x N, FP64) = A (M x K) * B (N x K)^T
+//
+// where A and B are each held as a pair of BF16 matrices (hi = bf16(x),
+// lo = bf16(x - hi)), K-contiguous.  Every 16-wide K step issues three UMMAs
+// into the same FP32 TMEM accumulator: hi*hi + hi*lo + lo*hi.
+//
+// Kernel structure (persistent, one CTA per SM, 6 warps):
+//   warp 0 lane 0  TMA producer: A_hi, A_lo (128 x 64) and B_hi, B_lo (64 x 64)
+//                  tiles per 64-wide K block into a 4-stage SWIZZLE_128B ring;
+//   warp 1 lane 0  MMA issuer: 12 tcgen05.mma (M128 N64 K16) per K block,
+//                  tcgen05.commit frees the stage; accumulators double-buffered
+//                  in TMEM (2 x 64 columns) so the epilogue overlaps the next tile;
+//   warps 2..5     epilogue: tcgen05.ld of the 128 x 64 FP32 accumulator, one
+//                  TMEM lane quarter per warp, stored as a stream-K partial.
+// Work is split stream-K: the (tile, K block) iteration space is cut into
+// equal contiguous ranges per CTA; a second kernel sums each tile's partials in
+// FP64.  All mbarrier waits are bounded by a clock budget and raise an error
+// flag instead of spinning forever.  No cluster multicast is used.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <memory>
+#include <vector>
+
+#include "blas_f64.cuh"
+#include "context.cuh"
+#include "xop_split.cuh"
+
+namespace fpls {
+namespace {
+
+constexpr int BM = 128;
+constexpr int BN = 64;
+constexpr int BK = 64;
+constexpr int STAGES = 4;
+constexpr int A_TILE = BM * BK * 2;                 // 16 KB
+constexpr int B_TILE = BN * BK * 2;                 // 8 KB
+constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;  // 48 KB
+constexpr int BAR_BYTES = 256;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
+constexpr int NUM_THREADS = 192;
+constexpr int TMEM_COLS = 2 * BN;
+constexpr long long kWaitBudget = 1ll << 33;        // ~4 s at 2 GHz
+
+// Instruction descriptor: D F32, A/B BF16, both K-major, N = 64, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                            (uint32_t(BN >> 3) << 17) | (uint32_t(BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
+// Bounded parity wait: returns false (and raises *err) when the budget runs out
+// or an error was already raised by another thread.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err,
+                                          bool stop_on_error = true) {
+  const long long t0 = clock64();
+  for (uint32_t spin = 0;; ++spin) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (stop_on_error && (spin & 63) == 63 && *(volatile int*)err) return false;
+    if (clock64() - t0 > kWaitBudget) {
+      atomicExch(err, 1);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint32_t dst, uint32_t bar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, SWIZZLE_128B, 8-row core groups 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>(1) << 16;              // leading byte offset (unused for SW128 K-major)
+  d |= static_cast<uint64_t>(1024 >> 4) << 32;      // stride byte offset
+  d |= static_cast<uint64_t>(1) << 46;              // descriptor version for sm_100
+  d |= static_cast<uint64_t>(2) << 61;              // SWIZZLE_128B
+  return d;
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+split_gemm_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
+                  const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo,
+                  const int4* __restrict__ segs, const int* __restrict__ cta_seg_begin,
+                  int n_tiles_n, float* __restrict__ part, int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~static_cast<uintptr_t>(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + STAGES;
+  uint64_t* tfull = bars + 2 * STAGES;
+  uint64_t* tempty = bars + 2 * STAGES + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 4);
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int sbeg = cta_seg_begin[blockIdx.x];
+  const int send = cta_seg_begin[blockIdx.x + 1];
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&tfull[b]), 1);
+      mbar_init(smem_u32(&tempty[b]), 128);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------------------------------------------------- producer
+    int it = 0;
+    bool ok = true;
+    for (int sg = sbeg; sg < send && ok; ++sg) {
+      const int4 seg = segs[sg];
+      const int mt = seg.x / n_tiles_n, nt = seg.x % n_tiles_n;
+      for (int kb = seg.y; kb < seg.z; ++kb, ++it) {
+        const int s = it % STAGES;
+        const uint32_t ph = (it / STAGES) & 1;
+        if (!mbar_wait(smem_u32(&empty[s]), ph ^ 1, err)) {
+          ok = false;
+          // Error path: let the copies already issued into the ring land before
+          // the CTA exits (bounded waits that ignore the error flag).
+          for (int d = 1; d <= STAGES && it - d >= 0; ++d) {
+            const int ps = (it - d) % STAGES;
+            mbar_wait(smem_u32(&full[ps]), ((it - d) / STAGES) & 1, err, false);
+          }
+          break;
+        }
+        const uint32_t fb = smem_u32(&full[s]);
+        mbar_expect_tx(fb, STAGE_BYTES);
+        uint8_t* st = smem + s * STAGE_BYTES;
+        tma_load_2d(&mAhi, smem_u32(st), fb, kb * BK, mt * BM);
+        tma_load_2d(&mAlo, smem_u32(st + A_TILE), fb, kb * BK, mt * BM);
+        tma_load_2d(&mBhi, smem_u32(st + 2 * A_TILE), fb, kb * BK, nt * BN);
+        tma_load_2d(&mBlo, smem_u32(st + 2 * A_TILE + B_TILE), fb, kb * BK, nt * BN);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------------------------------------------------- MMA issuer
+    int it = 0, j = 0;
+    bool ok = true;
+    for (int sg = sbeg; sg < send && ok; ++sg, ++j) {
+      const int4 seg = segs[sg];
+      const int b = j & 1;
+      const uint32_t jph = (j >> 1) & 1;
+      if (!mbar_wait(smem_u32(&tempty[b]), jph ^ 1, err)) { ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t acc = tmem + static_cast<uint32_t>(b * BN);
+      for (int kb = seg.y; kb < seg.z; ++kb, ++it) {
+        const int s = it % STAGES;
+        const uint32_t ph = (it / STAGES) & 1;
+        if (!mbar_wait(smem_u32(&full[s]), ph, err)) { ok = false; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a_hi = smem_u32(smem + s * STAGE_BYTES);
+        const uint32_t a_lo = a_hi + A_TILE;
+        const uint32_t b_hi = a_hi + 2 * A_TILE;
+        const uint32_t b_lo = b_hi + B_TILE;
+#pragma unroll
+        for (int k = 0; k < BK / 16; ++k) {
+          const uint32_t off = k * 32;  // 16 BF16 = 32 bytes along K inside the swizzle atom
+          const uint64_t dah = sw128_desc(a_hi + off), dal = sw128_desc(a_lo + off);
+          const uint64_t dbh = sw128_desc(b_hi + off), dbl = sw128_desc(b_lo + off);
+          umma_bf16(acc, dah, dbh, (kb > seg.y || k > 0) ? 1u : 0u);
+          umma_bf16(acc, dah, dbl, 1u);
+          umma_bf16(acc, dal, dbh, 1u);
+        }
+        umma_commit(smem_u32(&empty[s]));
+      }
+      umma_commit(smem_u32(&tfull[b]));
+    }
+  } else if (warp >= 2) {
+    // ---------------------------------------------------------- epilogue
+    const int q = warp & 3;  // TMEM lane quarter accessible to this warp
+    int j = 0;
+    for (int sg = sbeg; sg < send; ++sg, ++j) {
+      const int b = j & 1;
+      const uint32_t jph = (j >> 1) & 1;
+      const bool ok = mbar_wait(smem_u32(&tfull[b]), jph, err);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      float v[BN];
+      const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(b * BN);
+#pragma unroll
+      for (int c = 0; c < BN / 16; ++c) tmem_ld16(base + c * 16, v + c * 16);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(smem_u32(&tempty[b]));
+      if (!ok) break;
+      float* dst = part + static_cast<size_t>(sg) * BN * BM + q * 32 + lane;
+#pragma unroll
+      for (int c = 0; c < BN; ++c) dst[static_cast<size_t>(c) * BM] = v[c];
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
+                 : "memory");
+  }
+}
+
+// C[m + n*ldc] = alpha * sum_{segments of the tile} part + beta * C   (FP64)
+__global__ void split_reduce_kernel(const float* __restrict__ part, const int* __restrict__ tile_seg,
+                                    int n_tiles_n, int M, int N, double alpha, double beta,
+                                    double* __restrict__ C, int ldc) {
+  const int tile = blockIdx.x;
+  const int mt = tile / n_tiles_n, nt = tile % n_tiles_n;
+  const int s0 = tile_seg[tile], s1 = tile_seg[tile + 1];
+  for (int e = threadIdx.x; e < BM * BN; e += blockDim.x) {
+    const int mm = e % BM, nn = e / BM;
+    const int m = mt * BM + mm, n = nt * BN + nn;
+    if (m >= M || n >= N) continue;
+    double acc = 0.0;
+    for (int s = s0; s < s1; ++s) acc += static_cast<double>(part[(static_cast<size_t>(s) * BN + nn) * BM + mm]);
+    double* cp = C + m + static_cast<size_t>(n) * ldc;
+    *cp = (beta == 0.0) ? alpha * acc : alpha * acc + beta * *cp;
+  }
+}
+
+// hi/lo split of a column-major FP64 matrix (rows x cols, ld) written as
+// cols x ldo row-major BF16 pairs (row j = column j), zero padded to ldo.
+__global__ void split_cols_kernel(const double* __restrict__ X, int rows, int cols, int ld,
+                                  __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
+                                  int ldo) {
+  const size_t total = static_cast<size_t>(cols) * ldo;
+  for (size_t t = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(t % ldo);
+    const int j = static_cast<int>(t / ldo);
+    double x = (i < rows) ? X[i + static_cast<size_t>(j) * ld] : 0.0;
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    hi[t] = h;
+    lo[t] = __double2bfloat16(x - static_cast<double>(__bfloat162float(h)));
+  }
+}
+
+// hi/lo split with transpose: X (rows x cols col-major, ld) -> rows x ldo
+// row-major pairs (row i holds X[i, :]), zero padded.  32 x 32 tiles via smem.
+__global__ void split_rows_kernel(const double* __restrict__ X, int rows, int cols, int ld,
+                                  __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
+                                  int ldo) {
+  __shared__ double tile[32][33];
+  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    const int i = i0 + tx, j = j0 + r;
+    tile[r][tx] = (i < rows && j < cols) ? X[i + static_cast<size_t>(j) * ld] : 0.0;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int i = i0 + r, j = j0 + tx;
+    if (i < rows && j < ldo) {
+      const double x = tile[tx][r];
+      const __nv_bfloat16 h = __double2bfloat16(x);
+      hi[static_cast<size_t>(i) * ldo + j] = h;
+      lo[static_cast<size_t>(i) * ldo + j] = __double2bfloat16(x - static_cast<double>(__bfloat162float(h)));
+    }
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    FPLS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (!p || q != cudaDriverEntryPointSuccess)
+      throw Error(kErrCuda, "cuTensorMapEncodeTiled is unavailable");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 2-D BF16 tensor map: `rows` rows of `k` elements, row pitch ld elements.
+CUtensorMap make_map(const __nv_bfloat16* base, int rows, int k, int ld, int box_rows) {
+  CUtensorMap m;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(k), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 2};
+  cuuint32_t box[2] = {static_cast<cuuint32_t>(BK), static_cast<cuuint32_t>(box_rows)};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(base), dims,
+                           strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(kErrCuda, "cuTensorMapEncodeTiled failed");
+  return m;
+}
+
+int round_up(int x, int a) { return (x + a - 1) / a * a; }
+
+struct SplitPair {
+  __nv_bfloat16* hi = nullptr;
+  __nv_bfloat16* lo = nullptr;
+  int rows = 0, k = 0, ld = 0;
+};
+
+SplitPair alloc_pair(int rows, int k) {
+  SplitPair s;
+  s.rows = rows;
+  s.k = k;
+  s.ld = round_up(std::max(k, 1), BK);
+  Arena& ar = Context::get().arena;
+  s.hi = ar.alloc_n<__nv_bfloat16>(static_cast<size_t>(rows) * s.ld);
+  s.lo = ar.alloc_n<__nv_bfloat16>(static_cast<size_t>(rows) * s.ld);
+  return s;
+}
+
+// C (M x N) = alpha * A B^T + beta C, A: M x K pair, B: N x K pair.
+void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,
+                double beta, double* C, int ldc) {
+  Context& ctx = Context::get();
+  static bool attr = false;
+  if (!attr) {
+    FPLS_CUDA(cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    attr = true;
+  }
+  const int mt = (M + BM - 1) / BM, ntn = (N + BN - 1) / BN;
+  const int tiles = mt * ntn;
+  const int kbt = (K + BK - 1) / BK;
+  const long long total = static_cast<long long>(tiles) * kbt;
+  const int ctas = static_cast<int>(std::min<long long>(ctx.sm_count, total));
+  std::vector<int4> segs;
+  std::vector<int> cta_begin(ctas + 1, 0), tile_begin(tiles + 1, 0);
+  // Stream-K: CTA c covers iterations [c*total/ctas, (c+1)*total/ctas) in (tile, kb) order.
+  for (int c = 0; c < ctas; ++c) {
+    cta_begin[c] = static_cast<int>(segs.size());
+    long long a = total * c / ctas, e = total * (c + 1) / ctas;
+    while (a < e) {
+      const int t = static_cast<int>(a / kbt);
+      const int kb0 = static_cast<int>(a % kbt);
+      const int kb1 = static_cast<int>(std::min<long long>(kbt, kb0 + (e - a)));
+      segs.push_back(make_int4(t, kb0, kb1, 0));
+      a += kb1 - kb0;
+    }
+  }
+  cta_begin[ctas] = static_cast<int>(segs.size());
+  // Segments of a tile are contiguous (tile-major order).
+  {
+    int s = 0;
+    for (int t = 0; t < tiles; ++t) {
+      tile_begin[t] = s;
+      while (s < static_cast<int>(segs.size()) && segs[s].x == t) ++s;
+    }
+    tile_begin[tiles] = s;
+  }
+  Arena& ar = ctx.arena;
+  int4* d_segs = ar.alloc_n<int4>(segs.size());
+  int* d_cb = ar.alloc_n<int>(cta_begin.size());
+  int* d_tb = ar.alloc_n<int>(tile_begin.size());
+  float* part = ar.alloc_n<float>(segs.size() * static_cast<size_t>(BM) * BN);
+  h2d(d_segs, segs.data(), segs.size() * sizeof(int4));
+  h2d(d_cb, cta_begin.data(), cta_begin.size() * sizeof(int));
+  h2d(d_tb, tile_begin.data(), tile_begin.size() * sizeof(int));
+  const CUtensorMap mAhi = make_map(A.hi, M, K, A.ld, BM);
+  const CUtensorMap mAlo = make_map(A.lo, M, K, A.ld, BM);
+  const CUtensorMap mBhi = make_map(B.hi, N, K, B.ld, BN);
+  const CUtensorMap mBlo = make_map(B.lo, N, K, B.ld, BN);
+  int* err = ctx.d_status + 16;
+  split_gemm_kernel<<<ctas, NUM_THREADS, SMEM_BYTES, ctx.stream>>>(mAhi, mAlo, mBhi, mBlo, d_segs, d_cb,
+                                                                   ntn, part, err);
+  FPLS_CHECK_LAUNCH();
+  split_reduce_kernel<<<tiles, 256, 0, ctx.stream>>>(part, d_tb, ntn, M, N, alpha, beta, C, ldc);
+  FPLS_CHECK_LAUNCH();
+}
+
+void split_cols(const double* X, int rows, int cols, int ld, const SplitPair& out) {
+  Context& ctx = Context::get();
+  split_cols_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(X, rows, cols, ld, out.hi, out.lo, out.ld);
+  FPLS_CHECK_LAUNCH();
+}
+
+void split_rows(const double* X, int rows, int cols, int ld, const SplitPair& out) {
+  Context& ctx = Context::get();
+  dim3 grid((out.ld + 31) / 32, (rows + 31) / 32);
+  split_rows_kernel<<<grid, dim3(32, 8), 0, ctx.stream>>>(X, rows, cols, ld, out.hi, out.lo, out.ld);
+  FPLS_CHECK_LAUNCH();
+}
+
+struct XOperatorSplit : public XOperator {
+  SplitPair xr;   // n x p  (A of X * R)
+  SplitPair xc;   // p x n  (A of X^T * T)
+  XOperatorSplit(const double* X, int n_, int p_) {
+    n = n_;
+    p = p_;
+    xr = alloc_pair(n, p);
+    xc = alloc_pair(p, n);
+    split_rows(X, n, p, n, xr);
+    split_cols(X, n, p, n, xc);
+  }
+  void times(const double* Rhat, int F, double* U) override {
+    SplitPair b = alloc_pair(F, p);
+    split_cols(Rhat, p, F, p, b);
+    split_gemm(xr, b, n, F, p, 1.0, 0.0, U, n);
+  }
+  void t_times(const double* T, int F, double* P) override {
+    SplitPair b = alloc_pair(F, n);
+    split_cols(T, n, F, n, b);
+    split_gemm(xc, b, p, F, n, 1.0, 0.0, P, p);
+  }
+};
+
+}  // namespace
+
+std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p) {
+  return std::unique_ptr<XOperator>(new XOperatorSplit(X, n, p));
+}
+
+void split_gemm_test(const double* A, const double* B, int M, int N, int K, double* C) {
+  // A: M x K col-major, B: K x N col-major; C = A B.
+  SplitPair a = alloc_pair(M, K);
+  SplitPair b = alloc_pair(N, K);
+  split_rows(A, M, K, M, a);
+  split_cols(B, K, N, K, b);
+  split_gemm(a, b, M, N, K, 1.0, 0.0, C, M);
+}
+
+}  // namespace fpls

@@ -1,0 +1,20 @@
+// Mixed-precision predictor operator: X held once as BF16 hi/lo pairs (in both
+// row- and column-major order), both passes run as three-product BF16 GEMMs
+// (hi*hi + hi*lo + lo*hi) on the tcgen05 tensor cores with FP32 accumulation in
+// TMEM and FP64 reduction of the K-split partials.
+#pragma once
+
+#include <memory>
+
+#include "simpls_engine.cuh"
+
+namespace fpls {
+
+// Builds the split operator from an FP64 device matrix (n x p, ld n).
+std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p);
+
+// Plain C = A (M x K) * B^T (N x K) with A, B given as FP64 and split on the fly
+// into BF16 hi/lo; used by tests of the tensor-core kernel.  C is M x N (ld M).
+void split_gemm_test(const double* A, const double* B, int M, int N, int K, double* C);
+
+}  // namespace fpls

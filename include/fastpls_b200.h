@@ -157,6 +157,47 @@ int fpls_lda_project_predict(const double* X, int w, int p, const double* R, int
                              const double* constants, int n_classes, int* labels,
                              double* scores, char* err, size_t errlen);
 
+/* C (M x N) = A (M x K) * B (K x N) through the BF16 split-precision tensor-core
+ * path (hi/lo three-product tcgen05 GEMM, FP32 accumulation, FP64 reduction of
+ * the K-split partials).  A diagnostic of the mixed-precision kernel; it has no
+ * counterpart in the reference. */
+int fpls_bf16x3_gemm(const double* A, int M, int K, const double* B, int N, double* C,
+                     char* err, size_t errlen);
+
+/* Cross-validated class predictions with the argmax classifier for method 3
+ * (simpls_fast).  X is n x p, FP64 (x_is_float32 = 0) or FP32 (= 1); y are
+ * 1-based labels; fold holds 0-based fold ids (drawn by the caller, as the R
+ * shim draws them with R's RNG); fit f uses seed + f.  All fold fits run in one
+ * batched engine pass when batched = 1 (precision FPLS_PREC_FP64 or
+ * FPLS_PREC_BF16X3), else one after another in FP64 (the plain drop-in path).
+ * class_pred n x L (1-based; 0 where not predicted), status kfold (1 ok,
+ * 2 empty fold, 3 no training rows, 4 single-class training fold).
+ * Replaces _fastPLS_pls_cv_predict_compiled (RcppExports.cpp:731;
+ * fastPLS.cpp:6615-7151) with backend = 1 and classifier = 0. */
+int fpls_cv_predict(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                    const int* fold, int kfold, const int* ncomp, int L, int method, int scaling,
+                    int seed, int precision, int batched, int* class_pred, int* status,
+                    char* err, size_t errlen);
+
+/* Double cross-validation of SIMPLS PLS-DA (argmax classifier): for every outer
+ * fold o, an inner CV over its training rows picks ncomp (first maximum of the
+ * inner accuracy), then a refit on the outer training rows predicts fold o.
+ * outer_fold: n 0-based ids; inner_fold: n x kfold_outer, inner fold id of row i
+ * within outer fold o (ignored for the rows of fold o).  Seeds follow
+ * pls.double.cv: inner fits seed + 1000 run + (o+1) + inner fold, refits
+ * seed + 2000 run + (o+1).  All kfold_outer x (kfold_inner + 1) fits run in one
+ * batched engine pass (batched = 1) or one after another (batched = 0).
+ * Outputs: best_comp kfold_outer, inner_accuracy kfold_outer x L, outer_pred n,
+ * inner_pred kfold_outer x L x n (optional), fit_status (optional).
+ * Replaces the loop of pls.double.cv (R/main.R:6586-6760) over
+ * _fastPLS_pls_cv_predict_compiled (RcppExports.cpp:731) and pls() refits; no
+ * single reference routine covers the whole grid. */
+int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                   const int* outer_fold, int kfold_outer, const int* inner_fold, int kfold_inner,
+                   const int* ncomp, int L, int scaling, int seed, int run, int precision,
+                   int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
+                   int* inner_pred, int* fit_status, char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,322 @@
+#!/usr/bin/env python
+"""Benchmark: CV-grid fits/s of the batched mixed-precision double CV on B200.
+
+Workload (C4): synthetic omics PLS-DA, X 3000 x 20000 FP32 (log1p of
+log-normal, column-centred, 50 informative features), 4 classes 40/30/20/10 %,
+groups of 1..5 samples, 10 outer x 5 inner stratified folds, SIMPLS ncomp
+1..30.  One step = one complete double CV: 50 inner SIMPLS paths of 30
+components (= 1500 (fold, ncomp) fits, the count the reference reports) plus
+the 10 outer refits, test-row predictions, inner accuracies and ncomp choice.
+
+  value     batched + BF16x3 split, X already resident in HBM (FP32)
+  e2e       the same through the public host-buffer call (H2D of X, D2H of
+            predictions inside the timed region)
+  plain     FP64, one fit after another (the drop-in path), X resident
+
+Device time comes from CUDA events on the library's stream around each call;
+multi-GPU runs (torchrun) are weak-scaled replicas and report the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FITS_PER_RUN = 10 * 5 * 30
+CONFIG = dict(workload="C4 double CV SIMPLS PLS-DA 3000x20000 fp32, 10x5 folds, ncomp 1..30",
+              n=3000, p=20000, n_classes=4, kfold_outer=10, kfold_inner=5, ncomp_max=30,
+              l2="inputs larger than L2 (X fp32 240 MB, split copies 480 MB)")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="reduced shapes (profiling captures)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+def workload(small=False, seed=1):
+    from fastpls_b200 import synthetic
+    from fastpls_b200.folds import double_cv_folds
+    if small:
+        d = synthetic.c4_omics(seed=seed, n=1500, p=8000)
+    else:
+        d = synthetic.c4_omics(seed=seed)
+    outer, inner = double_cv_folds(d["y"], d["groups"], 10, 5, seed=seed)
+    d["outer"], d["inner"] = outer, inner
+    d["ncomp"] = np.arange(1, 31, dtype=np.int32)
+    return d
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons during a timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
+                                 f".clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            self.proc.wait()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        return dict(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=smax,
+                    reasons=sorted(reasons), samples=len(sm))
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def profile_traffic():
+    """Per-launch DRAM traffic of the split GEMM from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "split_gemm_c4_traffic.json")
+    if os.path.exists(path):
+        try:
+            return json.load(open(path)).get("traffic_bytes_per_launch_full_size")
+        except (OSError, ValueError):
+            return None
+    return None
+
+
+def cpu_baseline(d, max_seconds=30.0):
+    """The oracle (numpy/scipy, all host threads) on a bounded sample: inner
+    fold paths of the first outer fold (30 fits each) with their predictions."""
+    from oracle import pls as opls
+    from oracle import cv as ocv
+    X = d["X"].astype(np.float64)
+    y = d["y"]
+    o = 0
+    tr = np.where(d["outer"] != o)[0]
+    Xo, yo, fo = X[tr], y[tr], d["inner"][tr, o]
+    fits = 0
+    t0 = time.perf_counter()
+    for i in range(int(fo.max()) + 1):
+        train = np.where(fo != i)[0]
+        test = np.where(fo == i)[0]
+        model = opls.pls_model2_fast(Xo[train], ocv.response_rows(yo, train, d["n_classes"]),
+                                     d["ncomp"], seed=1 + 1000 + o + 1 + i)
+        opls.pls_predict_classes_compact(model, Xo[test])
+        fits += len(d["ncomp"])
+        if time.perf_counter() - t0 > max_seconds:
+            break
+    dt = time.perf_counter() - t0
+    return dict(value=fits / dt, unit="fits/s", cores=os.cpu_count(), kind="port",
+                sample=f"{fits // 30} inner-fold SIMPLS paths (30 ncomp fits each) + predictions of "
+                       f"the full C4 shape, numpy/OpenBLAS restatement", seconds=dt)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    d = workload(args.small)
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(d, max_seconds=1.0)
+    for _ in range(args.steps):
+        r = cpu_baseline(d, max_seconds=5.0)
+        vals.append(r["value"])
+    v = float(np.median(vals))
+    cb = cpu_baseline(d, max_seconds=5.0)
+    cb["value"] = v
+    print(json.dumps(dict(
+        impl="reference", metric="CV-grid fits/s", value=v, unit="fits/s", n_gpus=args.gpus,
+        steps=args.steps, warmup=args.warmup, ms_per_step=1000.0 * 30 / v, higher_is_better=True,
+        scaling="weak", vs_baseline=None, dtype="f64", data="synthetic", config=CONFIG,
+        cpu_baseline=cb, e2e=dict(value=v, unit="fits/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+        note="reference arm = CPU restatement of the reference algorithm (R/Armadillo build is not "
+             "available); each step is a bounded sample (inner-fold paths) of the C4 workload")))
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    os.environ["FASTPLS_DEVICE"] = str(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def run_ours(args):
+    world, rank, local, pg = dist_init(args)
+    from fastpls_b200 import _lib as lib
+    lib.load()
+    if not lib.has_cuda():
+        raise SystemExit("no B200 device")
+    d = workload(args.small, seed=1 + rank)
+    n, p = d["X"].shape
+    kw = dict(ncomp=d["ncomp"], n_classes=d["n_classes"], seed=1)
+    h = lib.x_upload(d["X"])
+
+    def step_value(prec="bf16x3", batched=True):
+        r = lib.double_cv_resident(h, n, d["y"], d["outer"], d["inner"], precision=prec,
+                                   batched=batched, **kw)
+        return r, lib.last_call_ms()
+
+    # warm-up
+    for _ in range(max(args.warmup, 3)):
+        step_value()
+    barrier(pg)
+    launches0 = lib.launch_count()
+    lib.profile_begin()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            r_mixed, ms = step_value()
+            times.append(ms)
+    prof = lib.profile_end()
+    launches = lib.launch_count() - launches0
+    clocks = clk.summary()
+    barrier(pg)
+    total_ms = reduce_max(pg, float(np.sum(times)))
+    value = world * FITS_PER_RUN * args.steps / (total_ms / 1e3)
+
+    # e2e through the host-buffer call
+    for _ in range(2):
+        lib.double_cv(d["X"], d["y"], d["outer"], d["inner"], precision="bf16x3", **kw)
+    barrier(pg)
+    e2e_times = []
+    for _ in range(args.steps):
+        lib.double_cv(d["X"], d["y"], d["outer"], d["inner"], precision="bf16x3", **kw)
+        e2e_times.append(lib.last_call_ms())
+    barrier(pg)
+    e2e_ms = reduce_max(pg, float(np.sum(e2e_times)))
+    e2e_value = world * FITS_PER_RUN * args.steps / (e2e_ms / 1e3)
+    h2d = d["X"].nbytes + d["y"].nbytes + d["outer"].nbytes + d["inner"].nbytes + 4 * 30
+    d2h = 4 * (10 + 10 * 30 * 2 + n + 60)  # best comps, accuracies, predictions, statuses
+
+    # FP64 arms (same work, both batched and one fit after another)
+    _, fp64_batched_ms = step_value("fp64", True)
+    r64 = lib.double_cv_resident(h, n, d["y"], d["outer"], d["inner"], precision="fp64",
+                                 batched=True, **kw)
+    plain_ms = None
+    if not args.no_plain:
+        r_plain, plain_ms = step_value("fp64", False)
+    barrier(pg)
+
+    peak, peak_src = measured_peaks()
+    per_launch_bytes = prof["bytes"] / max(prof["launches"], 1)
+    per_launch_ms = prof["ms"] / max(prof["launches"], 1)
+    achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else None
+    agree = float(np.mean(r_mixed["pred"] == r64["pred"]))
+    rows_per_fit = np.mean([np.sum((d["outer"] != o) & (d["inner"][:, o] != i))
+                            for o in range(10) for i in range(5)])
+    ms_per_step = total_ms / args.steps
+    out = dict(
+        metric="CV-grid fits/s", value=value, unit="fits/s", n_gpus=world, steps=args.steps,
+        warmup=args.warmup, ms_per_step=ms_per_step, higher_is_better=True, scaling="weak",
+        vs_baseline=None, dtype="bf16x3 split (fp32 accumulate) + fp64", data="synthetic",
+        config=dict(CONFIG, parallelism=f"{world} independent replicas" if world > 1 else "1 GPU",
+                    precision="bf16x3", batched=True),
+        x_rows_per_s=world * rows_per_fit * 50 * args.steps / (total_ms / 1e3),
+        e2e=dict(value=e2e_value, unit="fits/s", h2d_bytes_per_step=int(h2d),
+                 d2h_bytes_per_step=int(d2h), ms_per_step=e2e_ms / args.steps),
+        roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s",
+                      frac=(achieved / peak) if achieved else None, traffic=profile_traffic(),
+                      kernel="split_gemm_kernel (tcgen05 BF16x3 skinny GEMM)",
+                      launches=prof["launches"], avg_launch_ms=per_launch_ms,
+                      algorithmic_bytes_per_launch=per_launch_bytes, peak_source=peak_src),
+        clocks=clocks, gpu_launches=int(launches),
+        fp64_batched=dict(ms_per_step=fp64_batched_ms, fits_per_s=FITS_PER_RUN / (fp64_batched_ms / 1e3)),
+        parity=dict(outer_pred_agreement_bf16x3_vs_fp64=agree,
+                    best_comp_equal=bool(np.array_equal(r_mixed["best_comp"], r64["best_comp"])),
+                    inner_accuracy_max_abs_diff=float(np.nanmax(np.abs(r_mixed["inner_accuracy"] - r64["inner_accuracy"]))),
+                    accuracy_bf16x3=r_mixed["accuracy"], accuracy_fp64=r64["accuracy"]),
+    )
+    if plain_ms is not None:
+        out["plain_fp64"] = dict(ms_per_step=plain_ms, fits_per_s=FITS_PER_RUN / (plain_ms / 1e3),
+                                 best_comp_equal=bool(np.array_equal(r_plain["best_comp"], r64["best_comp"])))
+        out["speedup_vs_plain_fp64"] = (plain_ms / ms_per_step)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(d)
+    lib.x_free(h)
+    if rank == 0:
+        print(json.dumps(out))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -58,6 +58,13 @@ SIGNATURES = {
                          _I, _IP, _IP, _C, _S], ctypes.c_int),
     "fpls_double_cv": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I,
                         _I, _I, _I, _IP, _DP, _IP, _IP, _IP, _C, _S], ctypes.c_int),
+    "fpls_x_upload": ([ctypes.c_void_p, _I, _I, _I, _IP, _C, _S], ctypes.c_int),
+    "fpls_x_free": ([_I, _C, _S], ctypes.c_int),
+    "fpls_double_cv_resident": ([_I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I, _I, _I, _I,
+                                 _IP, _DP, _IP, _IP, _IP, _C, _S], ctypes.c_int),
+    "fpls_launch_count": ([], ctypes.c_longlong),
+    "fpls_last_call_ms": ([], ctypes.c_double),
+    "fpls_profile": ([_I, _DP, ctypes.POINTER(ctypes.c_longlong), _DP, _C, _S], ctypes.c_int),
 }
 
 
@@ -428,3 +435,60 @@ def double_cv(X, y, outer_fold, inner_fold, ncomp, n_classes, scaling=1, seed=1,
     if return_inner:
         out["inner_pred"] = inner
     return out
+
+
+def x_upload(X):
+    """Registers X in device memory; returns a handle for double_cv_resident."""
+    Xa, is32 = _x_arg(X)
+    h = ctypes.c_int(-1)
+    _call("fpls_x_upload", Xa.ctypes.data, is32, Xa.shape[0], Xa.shape[1], ctypes.byref(h))
+    return h.value
+
+
+def x_free(handle):
+    _call("fpls_x_free", int(handle))
+
+
+def double_cv_resident(handle, n, y, outer_fold, inner_fold, ncomp, n_classes, scaling=1, seed=1,
+                       run=1, precision="fp64", batched=True, return_inner=False):
+    yy = _i32(y)
+    of = _i32(outer_fold)
+    inf_ = np.asfortranarray(np.asarray(inner_fold, dtype=np.int32))
+    Ko = int(of.max()) + 1
+    Ki = int(inf_.max()) + 1
+    nc = _i32(np.atleast_1d(ncomp))
+    L = nc.size
+    best = np.zeros(Ko, dtype=np.int32)
+    acc = _out(Ko, L)
+    pred = np.zeros(n, dtype=np.int32)
+    inner = np.zeros((n, L, Ko), dtype=np.int32, order="F") if return_inner else None
+    fst = np.zeros(Ko * Ki + Ko, dtype=np.int32)
+    _call("fpls_double_cv_resident", int(handle), _p(yy), int(n_classes), _p(of), Ko,
+          inf_.ctypes.data_as(_c_int_p), Ki, _p(nc), L, int(scaling), int(seed), int(run),
+          PREC[precision], int(bool(batched)), _p(best), _p(acc), _p(pred),
+          None if inner is None else inner.ctypes.data_as(_c_int_p), _p(fst))
+    out = dict(best_comp=best, inner_accuracy=acc, pred=pred, fit_status=fst,
+               accuracy=float(np.mean(pred == yy)))
+    if return_inner:
+        out["inner_pred"] = inner
+    return out
+
+
+def launch_count():
+    return int(load().fpls_launch_count())
+
+
+def last_call_ms():
+    return float(load().fpls_last_call_ms())
+
+
+def profile_begin():
+    _call("fpls_profile", 1, None, None, None)
+
+
+def profile_end():
+    ms = ctypes.c_double(0.0)
+    cnt = ctypes.c_longlong(0)
+    by = ctypes.c_double(0.0)
+    _call("fpls_profile", 0, ctypes.byref(ms), ctypes.byref(cnt), ctypes.byref(by))
+    return dict(ms=ms.value, launches=cnt.value, bytes=by.value)

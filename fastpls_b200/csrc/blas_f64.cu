@@ -321,7 +321,7 @@ void gemm(bool transA, bool transB, int M, int N, int K, double alpha, const dou
   if (M <= 0 || N <= 0) return;
   cudaStream_t st = Context::get().stream;
   if (K <= 0) {
-    scale_matrix_kernel<<<grid_for((size_t)M * N, 256), 256, 0, st>>>(C, M, N, ldc, beta);
+    scale_matrix_kernel<<<grid_for((size_t)M * N, 256), 256, 0, st>>>(C, M, N, ldc, beta); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     return;
   }
@@ -340,7 +340,7 @@ void gemm(bool transA, bool transB, int M, int N, int K, double alpha, const dou
   splits = ceil_div(K, kps);
   const int use_atomic = splits > 1 ? 1 : 0;
   if (use_atomic) {
-    scale_matrix_kernel<<<grid_for((size_t)M * N, 256), 256, 0, st>>>(C, M, N, ldc, beta);
+    scale_matrix_kernel<<<grid_for((size_t)M * N, 256), 256, 0, st>>>(C, M, N, ldc, beta); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
   dim3 grid(gm, gn, splits);
@@ -352,6 +352,7 @@ void gemm(bool transA, bool transB, int M, int N, int K, double alpha, const dou
     gemm_f64_dmma<false, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic);
   else
     gemm_f64_dmma<true, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic);
+  ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -361,7 +362,7 @@ void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda
   if (!trans) {
     if (rows <= 0) return;
     if (cols <= 0) {
-      scale_matrix_kernel<<<grid_for(rows, 256), 256, 0, st>>>(y, rows, 1, rows, beta);
+      scale_matrix_kernel<<<grid_for(rows, 256), 256, 0, st>>>(y, rows, 1, rows, beta); ::fpls::note_launch();
       FPLS_CHECK_LAUNCH();
       return;
     }
@@ -373,61 +374,61 @@ void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda
     splits = ceil_div(cols, kps);
     const int use_atomic = splits > 1 ? 1 : 0;
     if (use_atomic) {
-      scale_matrix_kernel<<<grid_for(rows, 256), 256, 0, st>>>(y, rows, 1, rows, beta);
+      scale_matrix_kernel<<<grid_for(rows, 256), 256, 0, st>>>(y, rows, 1, rows, beta); ::fpls::note_launch();
       FPLS_CHECK_LAUNCH();
     }
-    gemv_n_kernel<<<dim3(gx, splits), 256, 0, st>>>(rows, cols, alpha, A, lda, x, y, kps, use_atomic, beta);
+    gemv_n_kernel<<<dim3(gx, splits), 256, 0, st>>>(rows, cols, alpha, A, lda, x, y, kps, use_atomic, beta); ::fpls::note_launch();
   } else {
     if (cols <= 0) return;
-    gemv_t_kernel<<<ceil_div(cols, 8), 256, 0, st>>>(rows, cols, alpha, A, lda, x, beta, y);
+    gemv_t_kernel<<<ceil_div(cols, 8), 256, 0, st>>>(rows, cols, alpha, A, lda, x, beta, y); ::fpls::note_launch();
   }
   FPLS_CHECK_LAUNCH();
 }
 
 void col_mean(const double* X, int n, int p, int ldx, double* out) {
   if (p <= 0) return;
-  col_mean_kernel<<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, out);
+  col_mean_kernel<<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, out); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void col_sd_centered(const double* X, int n, int p, int ldx, double* out) {
   if (p <= 0) return;
-  col_sd_kernel<<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, out);
+  col_sd_kernel<<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, out); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void center_scale(double* X, int n, int p, int ldx, const double* mean, const double* scale) {
   if ((size_t)n * p == 0) return;
-  center_scale_kernel<<<grid_for((size_t)n * p, 256), 256, 0, Context::get().stream>>>(X, n, p, ldx, mean, scale);
+  center_scale_kernel<<<grid_for((size_t)n * p, 256), 256, 0, Context::get().stream>>>(X, n, p, ldx, mean, scale); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void copy_matrix(double* dst, int ldd, const double* src, int lds, int n, int p) {
   if ((size_t)n * p == 0) return;
-  copy_matrix_kernel<<<grid_for((size_t)n * p, 256), 256, 0, Context::get().stream>>>(dst, ldd, src, lds, n, p);
+  copy_matrix_kernel<<<grid_for((size_t)n * p, 256), 256, 0, Context::get().stream>>>(dst, ldd, src, lds, n, p); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void add_row_vector(double* X, int n, int p, int ldx, const double* v) {
   if ((size_t)n * p == 0) return;
-  add_row_vector_kernel<<<grid_for((size_t)n * p, 256), 256, 0, Context::get().stream>>>(X, n, p, ldx, v);
+  add_row_vector_kernel<<<grid_for((size_t)n * p, 256), 256, 0, Context::get().stream>>>(X, n, p, ldx, v); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void rq_sums(const double* Y, const double* Yp, int n, int m, double* out2) {
-  rq_sums_kernel<<<1, 512, 0, Context::get().stream>>>(Y, Yp, n, m, out2);
+  rq_sums_kernel<<<1, 512, 0, Context::get().stream>>>(Y, Yp, n, m, out2); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void fill(double* x, size_t n, double v) {
   if (n == 0) return;
-  fill_kernel<<<grid_for(n, 256), 256, 0, Context::get().stream>>>(x, n, v);
+  fill_kernel<<<grid_for(n, 256), 256, 0, Context::get().stream>>>(x, n, v); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void scale_vec(double* x, size_t n, double a) {
   if (n == 0) return;
-  scale_vec_kernel<<<grid_for(n, 256), 256, 0, Context::get().stream>>>(x, n, a);
+  scale_vec_kernel<<<grid_for(n, 256), 256, 0, Context::get().stream>>>(x, n, a); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 

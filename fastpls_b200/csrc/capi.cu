@@ -30,6 +30,7 @@ int guarded(char* err, size_t errlen, Fn&& fn) {
   if (err && errlen) err[0] = '\0';
   try {
     fn();
+    Context::get().end_call();
     return FPLS_OK;
   } catch (const Error& e) {
     set_err(err, errlen, e.what());
@@ -86,7 +87,7 @@ __global__ void center_copy_kernel(const double* X, int w, int p, const double* 
 double* centered_test_copy(const double* Xh, int w, int p, const double* mX_d, const double* vX_d) {
   Context& ctx = Context::get();
   double* X = upload(Xh, (size_t)w * p);
-  center_copy_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(X, w, p, mX_d, vX_d, X);
+  center_copy_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(X, w, p, mX_d, vX_d, X); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   return X;
 }
@@ -157,7 +158,7 @@ int fpls_truncated_svd(const double* A, int rows, int cols, int k, int svd_metho
     download(s, ds, kcap);
     if (!left_only && Vt) {
       double* dVt = ctx.arena.alloc_n<double>((size_t)cols * kcap);
-      transpose_small<<<ceil_div((long long)cols * kcap, 256), 256, 0, ctx.stream>>>(dV, cols, kcap, dVt);
+      transpose_small<<<ceil_div((long long)cols * kcap, 256), 256, 0, ctx.stream>>>(dV, cols, kcap, dVt); ::fpls::note_launch();
       FPLS_CHECK_LAUNCH();
       download(Vt, dVt, (size_t)cols * kcap);
     }
@@ -297,7 +298,7 @@ int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, 
       while (i_out < L && a == nc[i_out] - 1) {
         if (dB) gemm(false, true, p, m, a + 1, 1.0, b.R, p, b.Q, m, 0.0, dB + (size_t)i_out * p * m, p);
         if (fit) {
-          scale_column_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(b.Tkeep + (size_t)a * n, n, 1.0 / tn[a], tcol);
+          scale_column_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(b.Tkeep + (size_t)a * n, n, 1.0 / tn[a], tcol); ::fpls::note_launch();
           FPLS_CHECK_LAUNCH();
           gemm(false, true, n, m, 1, 1.0, tcol, n, b.Q + (size_t)a * m, m, 1.0, cur, n);
           rq_sums(dYc, cur, n, m, rq + 2 * i_out);
@@ -597,9 +598,9 @@ int fpls_bf16x3_gemm(const double* A, int M, int K, const double* B, int N, doub
   });
 }
 
-static void run_cv_grid(const CvFitSet& fs, const void* X, int x_is_float32, const int* y,
-                        const int* ncomp, int L, int scaling, int precision, int batched,
-                        CvGridResult& res) {
+static void run_cv_grid(const CvFitSet& fs, const void* X, int x_is_float32, bool x_on_device,
+                        const int* y, const int* ncomp, int L, int scaling, int precision,
+                        int batched, CvGridResult& res) {
   Context& ctx = Context::get();
   FPLS_REQUIRE(precision == FPLS_PREC_FP64 || precision == FPLS_PREC_BF16X3, "unknown precision");
   CvGridOptions opt;
@@ -614,10 +615,10 @@ static void run_cv_grid(const CvFitSet& fs, const void* X, int x_is_float32, con
   const size_t np = (size_t)fs.n * fs.p;
   dzero(ctx.d_status + 16, sizeof(int));
   if (x_is_float32) {
-    const float* d = upload(static_cast<const float*>(X), np);
+    const float* d = x_on_device ? static_cast<const float*>(X) : upload(static_cast<const float*>(X), np);
     cv_grid_classify(fs, nullptr, d, y, ncomp, L, opt, res);
   } else {
-    const double* d = upload(static_cast<const double*>(X), np);
+    const double* d = x_on_device ? static_cast<const double*>(X) : upload(static_cast<const double*>(X), np);
     cv_grid_classify(fs, d, nullptr, y, ncomp, L, opt, res);
   }
   int e = 0;
@@ -653,18 +654,19 @@ int fpls_cv_predict(const void* X, int x_is_float32, int n, int p, const int* y,
     std::vector<int> nc(ncomp, ncomp + L);
     for (int& c : nc) c = std::max(1, c);
     CvGridResult res;
-    run_cv_grid(fs, X, x_is_float32, y, nc.data(), L, scaling, precision, batched, res);
+    run_cv_grid(fs, X, x_is_float32, false, y, nc.data(), L, scaling, precision, batched, res);
     std::copy(res.pred.begin(), res.pred.end(), class_pred);
     if (status) std::copy(res.status.begin(), res.status.end(), status);
   });
 }
 
-int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
-                   const int* outer_fold, int kfold_outer, const int* inner_fold, int kfold_inner,
-                   const int* ncomp, int L, int scaling, int seed, int run, int precision,
-                   int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
-                   int* inner_pred, int* fit_status, char* err, size_t errlen) {
-  return guarded(err, errlen, [&] {
+static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, int n, int p,
+                           const int* y, int n_classes, const int* outer_fold, int kfold_outer,
+                           const int* inner_fold, int kfold_inner, const int* ncomp, int L,
+                           int scaling, int seed, int run, int precision, int batched,
+                           int* best_comp, double* inner_accuracy, int* outer_pred,
+                           int* inner_pred, int* fit_status) {
+  {
     FPLS_REQUIRE(n >= 2 && p > 0, "Xdata must contain at least two samples");
     FPLS_REQUIRE(kfold_outer >= 1 && kfold_inner >= 1 && L >= 1, "fold counts and ncomp must be >= 1");
     Context& ctx = Context::get();
@@ -711,7 +713,7 @@ int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, 
       for (int i = 0; i < n; ++i) (outer_fold[i] == o ? fs.test : fs.train)[(size_t)f * n + i] = 1;
     }
     CvGridResult res;
-    run_cv_grid(fs, X, x_is_float32, y, nc.data(), L, scaling, precision, batched, res);
+    run_cv_grid(fs, X, x_is_float32, x_on_device, y, nc.data(), L, scaling, precision, batched, res);
     // Inner accuracy per (outer fold, ncomp) and the chosen ncomp (first maximum).
     for (int o = 0; o < Ko; ++o) {
       int bi = 0;
@@ -739,6 +741,104 @@ int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, 
     }
     if (inner_pred) std::copy(res.pred.begin(), res.pred.begin() + (size_t)Ko * L * n, inner_pred);
     if (fit_status) std::copy(res.status.begin(), res.status.end(), fit_status);
+    }
+}
+
+int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                   const int* outer_fold, int kfold_outer, const int* inner_fold, int kfold_inner,
+                   const int* ncomp, int L, int scaling, int seed, int run, int precision,
+                   int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
+                   int* inner_pred, int* fit_status, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    double_cv_impl(X, x_is_float32, false, n, p, y, n_classes, outer_fold, kfold_outer, inner_fold,
+                   kfold_inner, ncomp, L, scaling, seed, run, precision, batched, best_comp,
+                   inner_accuracy, outer_pred, inner_pred, fit_status);
+  });
+}
+
+int fpls_x_upload(const void* X, int x_is_float32, int n, int p, int* handle, char* err,
+                  size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && X && handle, "x_upload: empty matrix");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    ResidentX r;
+    r.n = n;
+    r.p = p;
+    r.f32 = x_is_float32 != 0;
+    const size_t bytes = (size_t)n * p * (r.f32 ? sizeof(float) : sizeof(double));
+    FPLS_CUDA(cudaMalloc(&r.ptr, bytes));
+    FPLS_CUDA(cudaMemcpyAsync(r.ptr, X, bytes, cudaMemcpyHostToDevice, ctx.stream));
+    ctx.sync();
+    int h = -1;
+    for (size_t i = 0; i < ctx.resident.size(); ++i)
+      if (!ctx.resident[i].ptr) { h = static_cast<int>(i); break; }
+    if (h < 0) { h = static_cast<int>(ctx.resident.size()); ctx.resident.push_back(r); }
+    else ctx.resident[h] = r;
+    *handle = h;
+  });
+}
+
+int fpls_x_free(int handle, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    Context& ctx = Context::get();
+    FPLS_REQUIRE(handle >= 0 && handle < static_cast<int>(ctx.resident.size()) &&
+                     ctx.resident[handle].ptr, "x_free: unknown handle");
+    FPLS_CUDA(cudaFree(ctx.resident[handle].ptr));
+    ctx.resident[handle] = ResidentX();
+  });
+}
+
+int fpls_double_cv_resident(int handle, const int* y, int n_classes, const int* outer_fold,
+                            int kfold_outer, const int* inner_fold, int kfold_inner,
+                            const int* ncomp, int L, int scaling, int seed, int run, int precision,
+                            int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
+                            int* inner_pred, int* fit_status, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    Context& ctx = Context::get();
+    FPLS_REQUIRE(handle >= 0 && handle < static_cast<int>(ctx.resident.size()) &&
+                     ctx.resident[handle].ptr, "double_cv_resident: unknown handle");
+    const ResidentX r = ctx.resident[handle];
+    double_cv_impl(r.ptr, r.f32 ? 1 : 0, true, r.n, r.p, y, n_classes, outer_fold, kfold_outer,
+                   inner_fold, kfold_inner, ncomp, L, scaling, seed, run, precision, batched,
+                   best_comp, inner_accuracy, outer_pred, inner_pred, fit_status);
+  });
+}
+
+long long fpls_launch_count(void) { return launch_count(); }
+
+double fpls_last_call_ms(void) {
+  try {
+    return Context::get().last_call_ms;
+  } catch (...) {
+    return 0.0;
+  }
+}
+
+int fpls_profile(int enable, double* gemm_ms, long long* gemm_launches, double* gemm_bytes,
+                 char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    Context& ctx = Context::get();
+    if (enable) {
+      for (cudaEvent_t e : ctx.prof_events) cudaEventDestroy(e);
+      ctx.prof_events.clear();
+      ctx.prof_bytes = 0.0;
+      ctx.profile = true;
+      return;
+    }
+    ctx.profile = false;
+    ctx.sync();
+    double total = 0.0;
+    for (size_t i = 0; i + 1 < ctx.prof_events.size(); i += 2) {
+      float ms = 0.f;
+      FPLS_CUDA(cudaEventElapsedTime(&ms, ctx.prof_events[i], ctx.prof_events[i + 1]));
+      total += ms;
+    }
+    if (gemm_ms) *gemm_ms = total;
+    if (gemm_launches) *gemm_launches = static_cast<long long>(ctx.prof_events.size() / 2);
+    if (gemm_bytes) *gemm_bytes = ctx.prof_bytes;
+    for (cudaEvent_t e : ctx.prof_events) cudaEventDestroy(e);
+    ctx.prof_events.clear();
   });
 }
 

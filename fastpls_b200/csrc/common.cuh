@@ -44,6 +44,11 @@ enum Status : int {
 
 constexpr int kSMCount = 148;  // B200: 2 dies x 74 SMs
 
+// Host-side count of kernel launches issued by this library (every launch
+// site calls note_launch() right after its <<<...>>>).
+void note_launch();
+long long launch_count();
+
 inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -1,6 +1,7 @@
 #include "context.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace fpls {
 
@@ -59,6 +60,12 @@ Context& Context::get() {
       throw Error(kErrNoDevice, "fastpls_b200: no CUDA device is available");
     }
     int dev = 0;
+    // One process per GPU: FASTPLS_DEVICE selects the ordinal (default: current device).
+    if (const char* e = std::getenv("FASTPLS_DEVICE")) {
+      char* endp = nullptr;
+      const long v = std::strtol(e, &endp, 10);
+      if (endp != e && v >= 0 && v < n) FPLS_CUDA(cudaSetDevice(static_cast<int>(v)));
+    }
     FPLS_CUDA(cudaGetDevice(&dev));
     cudaDeviceProp prop;
     FPLS_CUDA(cudaGetDeviceProperties(&prop, dev));
@@ -75,9 +82,32 @@ Context& Context::get() {
   return ctx;
 }
 
+namespace {
+long long g_launches = 0;
+}
+
+void note_launch() { ++g_launches; }
+long long launch_count() { return g_launches; }
+
 void Context::begin_call() {
   arena.reset();
+  if (!call_start) {
+    FPLS_CUDA(cudaEventCreate(&call_start));
+    FPLS_CUDA(cudaEventCreate(&call_stop));
+  }
+  FPLS_CUDA(cudaEventRecord(call_start, stream));
+  call_started = true;
   FPLS_CUDA(cudaMemsetAsync(d_status, 0, 64 * sizeof(int), stream));
+}
+
+void Context::end_call() {
+  if (!call_started) return;
+  call_started = false;
+  FPLS_CUDA(cudaEventRecord(call_stop, stream));
+  FPLS_CUDA(cudaEventSynchronize(call_stop));
+  float ms = 0.f;
+  FPLS_CUDA(cudaEventElapsedTime(&ms, call_start, call_stop));
+  last_call_ms = ms;
 }
 
 int Context::read_status() {

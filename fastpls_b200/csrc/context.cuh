@@ -28,15 +28,32 @@ class Arena {
   size_t high_water_ = 0;
 };
 
+// Device-resident predictor matrices registered by the caller (kept across calls).
+struct ResidentX {
+  void* ptr = nullptr;
+  int n = 0, p = 0;
+  bool f32 = false;
+};
+
 struct Context {
   int device = -1;
   cudaStream_t stream = nullptr;
   Arena arena;
   int* d_status = nullptr;     // device-side failure flag (0 = ok)
   int sm_count = kSMCount;
+  // Timing of the last ABI call (events on `stream`, bracketing the whole call).
+  cudaEvent_t call_start = nullptr, call_stop = nullptr;
+  bool call_started = false;
+  double last_call_ms = 0.0;
+  // Optional profiling window of the tensor-core GEMM (events around each launch).
+  bool profile = false;
+  std::vector<cudaEvent_t> prof_events;   // start/stop pairs
+  double prof_bytes = 0.0;                // algorithmic bytes of the profiled launches
+  std::vector<ResidentX> resident;
 
   static Context& get();       // initialises the device on first use
-  void begin_call();           // resets the arena and the status flag
+  void begin_call();           // resets the arena and the status flag, starts the call timer
+  void end_call();             // stops the call timer (after the final synchronisation)
   int read_status();           // synchronises the stream and reads the flag
   void sync();
   void release();

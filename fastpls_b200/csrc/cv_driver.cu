@@ -216,10 +216,10 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   if (center) {
     double* Mtr = ar.alloc_n<double>((size_t)Fa * n);
     delta = ar.alloc_n<double>((size_t)Fa * p);
-    mask_to_double_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(d_tr, (size_t)Fa * n, Mtr);
+    mask_to_double_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(d_tr, (size_t)Fa * n, Mtr); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     xop->t_times(Mtr, Fa, delta);
-    scale_cols_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(delta, p, Fa, d_inv);
+    scale_cols_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(delta, p, Fa, d_inv); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
   b.delta = delta;
@@ -236,7 +236,7 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   int* d_pred = ar.alloc_n<int>((size_t)fs.G * L * n);
   dzero(d_pred, (size_t)fs.G * L * n * sizeof(int));
   cv_predict_kernel<<<dim3(ceil_div(n, 128), Fa), 128, 0, ctx.stream>>>(
-      Fa, n, m, K, L, d_nc, d_te, d_grp, b.Tkeep, b.tnorm, b.Q, b.ncomp_done, d_mYf, d_pred);
+      Fa, n, m, K, L, d_nc, d_te, d_grp, b.Tkeep, b.tnorm, b.Q, b.ncomp_done, d_mYf, d_pred); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   std::vector<int> pred((size_t)fs.G * L * n);
   std::vector<int> done(Fa);
@@ -291,8 +291,8 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
     const int nt = static_cast<int>(trows.size());
     h2d(d_idx, rows.data(), nf * sizeof(int));
     h2d(d_lab, labs.data(), nf * sizeof(int));
-    gather_rows_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(X, n, p, d_idx, nf, Xf);
-    onehot_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(d_lab, nf, m, Yf);
+    gather_rows_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(X, n, p, d_idx, nf, Xf); ::fpls::note_launch();
+    onehot_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(d_lab, nf, m, Yf); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     center_scale_xy(Xf, nf, p, Yf, m, opt.scaling, mX, vX, mY);
     gemm(true, false, p, m, nf, 1.0, Xf, nf, Yf, nf, 0.0, S, p);
@@ -321,7 +321,7 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
         for (int j = 0; j < m; ++j) Wh[a + (size_t)j * K + (size_t)s * K * m] = Qh[j + (size_t)a * m];
     h2d(W, Wh.data(), Wh.size() * sizeof(double));
     h2d(d_idx, trows.data(), nt * sizeof(int));
-    gather_rows_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(X, n, p, d_idx, nt, Xt);
+    gather_rows_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(X, n, p, d_idx, nt, Xt); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     center_scale(Xt, nt, p, nt, mX, opt.scaling == 2 ? vX : nullptr);
     lowrank_predict(Xt, nt, p, R, K, W, m, ncomp, L, mY, T, Yp);
@@ -356,7 +356,7 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
   if (x64) {
     d2d(X, x64, (size_t)fs.n * fs.p * sizeof(double));
   } else {
-    widen_f32_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(x32, X, (size_t)fs.n * fs.p);
+    widen_f32_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(x32, X, (size_t)fs.n * fs.p); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
   const bool batched = opt.batched && opt.scaling != 2;

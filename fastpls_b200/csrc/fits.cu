@@ -179,7 +179,7 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
   double* rq = ctx.arena.alloc_n<double>(2 * L);
   for (int a = 0; a < L; ++a) {
     const int mc = std::min(ncomp[a], keff);
-    diag_kernel<<<1, 256, 0, ctx.stream>>>(D, mc, out.s);
+    diag_kernel<<<1, 256, 0, ctx.stream>>>(D, mc, out.s); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     // G_a is the leading mc x mc block of G (leading dimension keff).
     spd_solve(mc, G, keff, mc, D, mc, Cw, mc, ctx.d_status + 2);
@@ -256,7 +256,7 @@ int simpls_classic_fit(const double* X, int n, int p, const double* Y, int m, co
       dzero(ctx.d_status + 3, sizeof(int));
       leading_left_power_kernel<<<1, 1024, 0, ctx.stream>>>(S, p, m, omega, max_iters,
                                                             std::max(opt.svds_tol, 1e-8), u, vtmp,
-                                                            u2, ctx.d_status + 3);
+                                                            u2, ctx.d_status + 3); ::fpls::note_launch();
       FPLS_CHECK_LAUNCH();
       int bad = 0;
       d2h(&bad, ctx.d_status + 3, sizeof(int));
@@ -274,12 +274,12 @@ int simpls_classic_fit(const double* X, int n, int p, const double* Y, int m, co
     d2d(rr, rr_src, p * sizeof(double));
     // tt = X rr, centred, normalised
     gemv(false, n, p, 1.0, X, n, rr, 0.0, t);
-    sum_kernel<<<1, 512, 0, ctx.stream>>>(t, n, sc);
+    sum_kernel<<<1, 512, 0, ctx.stream>>>(t, n, sc); ::fpls::note_launch();
     const double mt = read_scalar(sc) / static_cast<double>(n);
-    affine_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(t, n, 1.0, mt);
-    dot_kernel<<<1, 512, 0, ctx.stream>>>(t, t, n, sc);
+    affine_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(t, n, 1.0, mt); ::fpls::note_launch();
+    dot_kernel<<<1, 512, 0, ctx.stream>>>(t, t, n, sc); ::fpls::note_launch();
     const double tnorm = std::sqrt(read_scalar(sc));
-    affine_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(t, n, 1.0 / tnorm, 0.0);
+    affine_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(t, n, 1.0 / tnorm, 0.0); ::fpls::note_launch();
     scale_vec(rr, p, 1.0 / tnorm);
     FPLS_CHECK_LAUNCH();
     gemv(true, n, p, 1.0, X, n, t, 0.0, pp);
@@ -289,11 +289,11 @@ int simpls_classic_fit(const double* X, int n, int p, const double* Y, int m, co
       gemv(true, p, a, 1.0, V, p, pp, 0.0, w);
       gemv(false, p, a, -1.0, V, p, w, 1.0, vv);
     }
-    dot_kernel<<<1, 512, 0, ctx.stream>>>(vv, vv, p, sc);
+    dot_kernel<<<1, 512, 0, ctx.stream>>>(vv, vv, p, sc); ::fpls::note_launch();
     const double vn = std::sqrt(read_scalar(sc));
     scale_vec(vv, p, 1.0 / vn);
     gemv(true, p, m, 1.0, S, p, vv, 0.0, vS);
-    rank1_left_kernel<<<256, 256, 0, ctx.stream>>>(S, p, m, vv, vS);
+    rank1_left_kernel<<<256, 256, 0, ctx.stream>>>(S, p, m, vv, vS); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     d2d(V + (size_t)a * p, vv, p * sizeof(double));
     if (out.T) d2d(out.T + (size_t)a * n, t, n * sizeof(double));

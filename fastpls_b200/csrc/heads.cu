@@ -161,7 +161,7 @@ void lowrank_predict(const double* Xs, int w, int p, const double* R, int kmax, 
 
 void row_argmax(const double* S, int w, int C, const double* bias, int* labels) {
   if (w <= 0) return;
-  argmax_kernel<<<ceil_div(w, 256), 256, 0, Context::get().stream>>>(S, w, C, bias, labels);
+  argmax_kernel<<<ceil_div(w, 256), 256, 0, Context::get().stream>>>(S, w, C, bias, labels); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -169,7 +169,7 @@ void row_topk(const double* S, int w, int C, const double* bias, int top_k, int*
               double* score) {
   FPLS_REQUIRE(top_k >= 1 && top_k <= 32, "top-k supports 1..32 classes per row");
   if (w <= 0) return;
-  topk_kernel<<<ceil_div(w, 128), 128, 0, Context::get().stream>>>(S, w, C, bias, top_k, idx, score);
+  topk_kernel<<<ceil_div(w, 128), 128, 0, Context::get().stream>>>(S, w, C, bias, top_k, idx, score); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -183,7 +183,7 @@ void lda_train_prefix(const double* T, int n, int kmax, const int* y, int C,
   double* counts = ctx.arena.alloc_n<double>(C);
   int* bad = ctx.d_status + 4;
   dzero(bad, sizeof(int));
-  class_sums_kernel<<<kmax, 256, C * sizeof(double), ctx.stream>>>(T, n, kmax, y, C, M, counts, bad);
+  class_sums_kernel<<<kmax, 256, C * sizeof(double), ctx.stream>>>(T, n, kmax, y, C, M, counts, bad); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   std::vector<double> hc(C);
   int hbad = 0;
@@ -193,13 +193,13 @@ void lda_train_prefix(const double* T, int n, int kmax, const int* y, int C,
   if (hbad) throw Error(kErrArgument, "lda_train_prefix labels must be encoded as 1..n_classes");
   for (int c = 0; c < C; ++c)
     if (hc[c] <= 0.0) throw Error(kErrArgument, "lda_train_prefix received an empty class");
-  means_from_sums_kernel<<<ceil_div(C * kmax, 256), 256, 0, ctx.stream>>>(M, C, kmax, counts, Mw);
+  means_from_sums_kernel<<<ceil_div(C * kmax, 256), 256, 0, ctx.stream>>>(M, C, kmax, counts, Mw); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   double* P = ctx.arena.alloc_n<double>((size_t)kmax * kmax);
   gemm(true, false, kmax, kmax, n, 1.0, T, n, T, n, 0.0, P, kmax);
   gemm(true, false, kmax, kmax, C, -1.0, M, C, Mw, C, 1.0, P, kmax);
   const double df = std::max(1.0, static_cast<double>(n) - static_cast<double>(C));
-  symm_upper_scale_kernel<<<ceil_div(kmax * kmax, 256), 256, 0, ctx.stream>>>(P, kmax, 1.0 / df);
+  symm_upper_scale_kernel<<<ceil_div(kmax * kmax, 256), 256, 0, ctx.stream>>>(P, kmax, 1.0 / df); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   double* Pk = ctx.arena.alloc_n<double>((size_t)kmax * kmax);
   double* Mt = ctx.arena.alloc_n<double>((size_t)kmax * C);
@@ -207,8 +207,8 @@ void lda_train_prefix(const double* T, int n, int kmax, const int* y, int C,
   double* lam = ctx.arena.alloc_n<double>(L);
   for (int a = 0; a < L; ++a) {
     const int kk = ncomp_host[a];
-    ridge_block_kernel<<<1, 256, 0, ctx.stream>>>(P, kmax, kk, ridge, Pk, lam + a);
-    transpose_block_kernel<<<ceil_div(C * kk, 256), 256, 0, ctx.stream>>>(M, C, kk, C, Mt, kk);
+    ridge_block_kernel<<<1, 256, 0, ctx.stream>>>(P, kmax, kk, ridge, Pk, lam + a); ::fpls::note_launch();
+    transpose_block_kernel<<<ceil_div(C * kk, 256), 256, 0, ctx.stream>>>(M, C, kk, C, Mt, kk); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     spd_solve(kk, Pk, kk, C, Mt, kk, Xs, kk, ctx.d_status + 5);
     double* Ma = out.means + (size_t)a * C * kmax;
@@ -216,9 +216,9 @@ void lda_train_prefix(const double* T, int n, int kmax, const int* y, int C,
     dzero(Ma, (size_t)C * kmax * sizeof(double));
     dzero(La, (size_t)C * kmax * sizeof(double));
     copy_matrix(Ma, C, M, C, C, kk);
-    transpose_block_kernel<<<ceil_div(C * kk, 256), 256, 0, ctx.stream>>>(Xs, kk, C, kk, La, C);
+    transpose_block_kernel<<<ceil_div(C * kk, 256), 256, 0, ctx.stream>>>(Xs, kk, C, kk, La, C); ::fpls::note_launch();
     lda_constants_kernel<<<ceil_div(C, 128), 128, 0, ctx.stream>>>(
-        Ma, La, C, kk, C, counts, n, out.constants + (size_t)a * C, a == 0 ? out.priors : nullptr);
+        Ma, La, C, kk, C, counts, n, out.constants + (size_t)a * C, a == 0 ? out.priors : nullptr); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
   std::vector<double> hl(L);

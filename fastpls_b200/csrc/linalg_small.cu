@@ -418,7 +418,7 @@ void spd_solve(int k, const double* G, int ldg, int nrhs, const double* B, int l
   Context& ctx = Context::get();
   double* W = ctx.arena.alloc_n<double>((size_t)k * (k + nrhs));
   spd_solve_kernel<<<1, 512, 0, ctx.stream>>>(k, G, ldg, nrhs, B, ldb, X, ldx, W,
-                                              d_flag ? d_flag : ctx.d_status + 1, ridge_rel);
+                                              d_flag ? d_flag : ctx.d_status + 1, ridge_rel); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -433,8 +433,8 @@ static void cgs2_orthonormalize(int rows, int cols, const double* Y, int ldy, do
       gemv(true, rows, j, 1.0, Q, ldq, q, 0.0, w);
       gemv(false, rows, j, -1.0, Q, ldq, w, 1.0, q);
     }
-    dot_self_kernel<<<1, 512, 0, ctx.stream>>>(q, rows, nrm);
-    normalize_col_kernel<<<ceil_div(rows, 256), 256, 0, ctx.stream>>>(q, rows, nrm);
+    dot_self_kernel<<<1, 512, 0, ctx.stream>>>(q, rows, nrm); ::fpls::note_launch();
+    normalize_col_kernel<<<ceil_div(rows, 256), 256, 0, ctx.stream>>>(q, rows, nrm); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
 }
@@ -457,8 +457,8 @@ void qr_orthonormalize(int rows, int cols, const double* Y, int ldy, double* Q, 
     }
     for (int pass = 0; pass < 2; ++pass) {
       gemm(true, false, cols, cols, rows, 1.0, src, lds, src, lds, 0.0, G, cols);
-      chol_upper_kernel<<<1, 512, 0, ctx.stream>>>(G, cols, flag);
-      trsm_rows_kernel<<<ceil_div(rows, 128), 128, smem, ctx.stream>>>(rows, cols, src, lds, G, Q, ldq);
+      chol_upper_kernel<<<1, 512, 0, ctx.stream>>>(G, cols, flag); ::fpls::note_launch();
+      trsm_rows_kernel<<<ceil_div(rows, 128), 128, smem, ctx.stream>>>(rows, cols, src, lds, G, Q, ldq); ::fpls::note_launch();
       FPLS_CHECK_LAUNCH();
       src = Q;
       lds = ldq;
@@ -479,7 +479,7 @@ void eig_sym_desc(int l, const double* G, int ldg, double* evals, double* V, int
   copy_matrix(W, l, G, ldg, l, l);
   const int npair = (l + 1) / 2;
   const size_t smem = (size_t)npair * 2 * sizeof(double) + (size_t)(2 * npair + 2 * npair) * sizeof(int) + 64;
-  jacobi_eig_kernel<<<1, 1024, smem, ctx.stream>>>(l, W, Vw, evals, V, ldv, 60);
+  jacobi_eig_kernel<<<1, 1024, smem, ctx.stream>>>(l, W, Vw, evals, V, ldv, 60); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -495,14 +495,14 @@ void svd_thin(int rows, int cols, const double* A, int lda, double* U, int ldu, 
   if (tall) {
     copy_matrix(W, r, A, lda, rows, cols);
   } else {
-    transpose_kernel<<<256, 256, 0, ctx.stream>>>(A, rows, cols, lda, W);
+    transpose_kernel<<<256, 256, 0, ctx.stream>>>(A, rows, cols, lda, W); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
   const int ce = c + (c & 1);
   const size_t smem = (size_t)(2 * ce + 2) * sizeof(int) + (size_t)(c + 2) * sizeof(double) + 64;
   // tall: U (rows x c) <- normalised W, V (cols x c) <- rotations.
   // wide: A^T = U' S V'^T, so U (rows x c) <- V', V (cols x c) <- U'.
-  jacobi_svd_kernel<<<1, 1024, smem, ctx.stream>>>(r, c, W, Vw, 60, U, ldu, s, V, ldv, tall ? 0 : 1);
+  jacobi_svd_kernel<<<1, 1024, smem, ctx.stream>>>(r, c, W, Vw, 60, U, ldu, s, V, ldv, tall ? 0 : 1); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 

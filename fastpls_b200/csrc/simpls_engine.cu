@@ -413,10 +413,10 @@ void simpls_batch_crosscov(const SimplsBatch& b, const double* /*Xc*/, const int
   Eng e = make_eng(b);
   double* M = ctx.arena.alloc_n<double>((size_t)b.n * b.F * b.m);
   double* P = ctx.arena.alloc_n<double>((size_t)b.p * b.F * b.m);
-  k_masked_response<<<2 * ctx.sm_count, kThreads, 0, ctx.stream>>>(e, M);
+  k_masked_response<<<2 * ctx.sm_count, kThreads, 0, ctx.stream>>>(e, M); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   b.X->t_times(M, b.F * b.m, P);
-  k_crosscov_finish<<<2 * ctx.sm_count, kThreads, 0, ctx.stream>>>(e, P, n_train);
+  k_crosscov_finish<<<2 * ctx.sm_count, kThreads, 0, ctx.stream>>>(e, P, n_train); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -455,24 +455,24 @@ void simpls_batch_run(const SimplsBatch& b) {
   cudaStream_t st = ctx.stream;
   for (int a = 0; a < b.K; ++a) {
     // Refresh: y <- S (S^T y) `iters` times from the warm start, then normalise.
-    k_refresh_start<<<gp, kThreads, 0, st>>>(e, a, iters);
+    k_refresh_start<<<gp, kThreads, 0, st>>>(e, a, iters); ::fpls::note_launch();
     double* zin = e.zA;
     double* zout = e.zB;
     for (int it = 0; it < iters; ++it) {
       const int last = (it == iters - 1) ? 1 : 0;
-      k_refresh_apply<<<gp, kThreads, sm_m, st>>>(e, zin, zout, last);
+      k_refresh_apply<<<gp, kThreads, sm_m, st>>>(e, zin, zout, last); ::fpls::note_launch();
       std::swap(zin, zout);
     }
-    k_refresh_finish<<<gp, kThreads, 0, st>>>(e);
+    k_refresh_finish<<<gp, kThreads, 0, st>>>(e); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     b.X->times(e.Rhat, b.F, e.U);
-    k_scores<<<gn, kThreads, b.labels ? sm_m : 0, st>>>(e, a);
+    k_scores<<<gn, kThreads, b.labels ? sm_m : 0, st>>>(e, a); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     b.X->t_times(e.T, b.F, e.P);
-    k_loading<<<gp, kThreads, 0, st>>>(e, a);
-    k_orth<<<gp, kThreads, sm_k, st>>>(e, a);
-    k_vnorm<<<gp, kThreads, 0, st>>>(e, a);
-    k_deflate<<<gp, kThreads, sm_m, st>>>(e, a);
+    k_loading<<<gp, kThreads, 0, st>>>(e, a); ::fpls::note_launch();
+    k_orth<<<gp, kThreads, sm_k, st>>>(e, a); ::fpls::note_launch();
+    k_vnorm<<<gp, kThreads, 0, st>>>(e, a); ::fpls::note_launch();
+    k_deflate<<<gp, kThreads, sm_m, st>>>(e, a); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
 }

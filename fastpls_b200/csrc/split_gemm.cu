@@ -423,23 +423,37 @@ void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, dou
   const CUtensorMap mBhi = make_map(B.hi, N, K, B.ld, BN);
   const CUtensorMap mBlo = make_map(B.lo, N, K, B.ld, BN);
   int* err = ctx.d_status + 16;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (ctx.profile) {
+    FPLS_CUDA(cudaEventCreate(&ev0));
+    FPLS_CUDA(cudaEventCreate(&ev1));
+    FPLS_CUDA(cudaEventRecord(ev0, ctx.stream));
+  }
   split_gemm_kernel<<<ctas, NUM_THREADS, SMEM_BYTES, ctx.stream>>>(mAhi, mAlo, mBhi, mBlo, d_segs, d_cb,
-                                                                   ntn, part, err);
+                                                                   ntn, part, err); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
-  split_reduce_kernel<<<tiles, 256, 0, ctx.stream>>>(part, d_tb, ntn, M, N, alpha, beta, C, ldc);
+  if (ctx.profile) {
+    FPLS_CUDA(cudaEventRecord(ev1, ctx.stream));
+    ctx.prof_events.push_back(ev0);
+    ctx.prof_events.push_back(ev1);
+    // Algorithmic bytes: both BF16 halves of A and B once, the FP64 result once.
+    ctx.prof_bytes += 4.0 * (static_cast<double>(M) * K + static_cast<double>(N) * K) +
+                      8.0 * static_cast<double>(M) * N;
+  }
+  split_reduce_kernel<<<tiles, 256, 0, ctx.stream>>>(part, d_tb, ntn, M, N, alpha, beta, C, ldc); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void split_cols(const double* X, int rows, int cols, int ld, const SplitPair& out) {
   Context& ctx = Context::get();
-  split_cols_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(X, rows, cols, ld, out.hi, out.lo, out.ld);
+  split_cols_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(X, rows, cols, ld, out.hi, out.lo, out.ld); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void split_rows(const double* X, int rows, int cols, int ld, const SplitPair& out) {
   Context& ctx = Context::get();
   dim3 grid((out.ld + 31) / 32, (rows + 31) / 32);
-  split_rows_kernel<<<grid, dim3(32, 8), 0, ctx.stream>>>(X, rows, cols, ld, out.hi, out.lo, out.ld);
+  split_rows_kernel<<<grid, dim3(32, 8), 0, ctx.stream>>>(X, rows, cols, ld, out.hi, out.lo, out.ld); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 

@@ -110,12 +110,12 @@ SvdResult truncated_svd_device(const double* A, int rows, int cols, int lda, int
     while (usable < l && evh[usable] > tol) ++usable;
     usable = std::min(usable, rank);
     if (usable > 0) {
-      sqrt_clamp_kernel<<<1, 256, 0, ctx.stream>>>(ev, s, usable);
+      sqrt_clamp_kernel<<<1, 256, 0, ctx.stream>>>(ev, s, usable); ::fpls::note_launch();
       FPLS_CHECK_LAUNCH();
       gemm(false, false, rows, usable, l, 1.0, Q, rows, Uh, l, 0.0, U, ldu);
       if (!left_only && V) {
         gemm(true, false, cols, usable, l, 1.0, B, l, Uh, l, 0.0, V, ldv);
-        scale_cols_inv_kernel<<<64, 256, 0, ctx.stream>>>(V, cols, usable, ldv, s);
+        scale_cols_inv_kernel<<<64, 256, 0, ctx.stream>>>(V, cols, usable, ldv, s); ::fpls::note_launch();
         FPLS_CHECK_LAUNCH();
       }
       res.rank = usable;

@@ -198,6 +198,33 @@ int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, 
                    int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
                    int* inner_pred, int* fit_status, char* err, size_t errlen);
 
+/* Registers a predictor matrix (n x p, FP64 or FP32) in device memory for
+ * repeated calls; *handle identifies it until fpls_x_free.  Lets a caller keep
+ * X resident across CV runs instead of re-sending it (the reference re-uploads
+ * X for every fold, fastPLS.cpp:6834-6836); no counterpart in the reference. */
+int fpls_x_upload(const void* X, int x_is_float32, int n, int p, int* handle, char* err,
+                  size_t errlen);
+int fpls_x_free(int handle, char* err, size_t errlen);
+
+/* fpls_double_cv on a registered (device-resident) predictor matrix. */
+int fpls_double_cv_resident(int handle, const int* y, int n_classes, const int* outer_fold,
+                            int kfold_outer, const int* inner_fold, int kfold_inner,
+                            const int* ncomp, int L, int scaling, int seed, int run, int precision,
+                            int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
+                            int* inner_pred, int* fit_status, char* err, size_t errlen);
+
+/* Instrumentation: number of kernels this library has launched since load, and
+ * the device time (CUDA events on the library stream) of the last call,
+ * host <-> device copies included. */
+long long fpls_launch_count(void);
+double fpls_last_call_ms(void);
+
+/* Profiling window of the tensor-core GEMM: enable = 1 opens it, enable = 0
+ * closes it and returns the summed device time of its launches (CUDA events on
+ * the launching stream), the launch count and their algorithmic bytes. */
+int fpls_profile(int enable, double* gemm_ms, long long* gemm_launches, double* gemm_bytes,
+                 char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,8 @@ SIGNATURES = {
                          _I, _IP, _IP, _C, _S], ctypes.c_int),
     "fpls_double_cv": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I,
                         _I, _I, _I, _IP, _DP, _IP, _IP, _IP, _C, _S], ctypes.c_int),
+    "fpls_bf16x3_gemm_noalloc": ([ctypes.c_void_p, _I, _I, ctypes.c_void_p, _I, ctypes.c_void_p,
+                                  _C, _S], ctypes.c_int),
     "fpls_x_upload": ([ctypes.c_void_p, _I, _I, _I, _IP, _C, _S], ctypes.c_int),
     "fpls_x_free": ([_I, _C, _S], ctypes.c_int),
     "fpls_double_cv_resident": ([_I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I, _I, _I, _I,

@@ -361,100 +361,157 @@ struct SplitPair {
   int rows = 0, k = 0, ld = 0;
 };
 
-SplitPair alloc_pair(int rows, int k) {
+SplitPair pair_at(__nv_bfloat16* base, int rows, int k) {
   SplitPair s;
   s.rows = rows;
   s.k = k;
   s.ld = round_up(std::max(k, 1), BK);
-  Arena& ar = Context::get().arena;
-  s.hi = ar.alloc_n<__nv_bfloat16>(static_cast<size_t>(rows) * s.ld);
-  s.lo = ar.alloc_n<__nv_bfloat16>(static_cast<size_t>(rows) * s.ld);
+  s.hi = base;
+  s.lo = base + static_cast<size_t>(rows) * s.ld;
   return s;
 }
 
-// C (M x N) = alpha * A B^T + beta C, A: M x K pair, B: N x K pair.
-void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,
-                double beta, double* C, int ldc) {
-  Context& ctx = Context::get();
+size_t pair_elems(int rows, int k) { return 2 * static_cast<size_t>(rows) * round_up(std::max(k, 1), BK); }
+
+SplitPair alloc_pair(int rows, int k) {
+  return pair_at(Context::get().arena.alloc_n<__nv_bfloat16>(pair_elems(rows, k)), rows, k);
+}
+
+// Stream-K work plan: CTA c covers iterations [c*total/ctas, (c+1)*total/ctas)
+// of the (tile, K block) space, cut into per-tile segments.
+struct GemmPlan {
+  int tiles = 0, ntn = 0, ctas = 0;
+  std::vector<int4> segs;
+  std::vector<int> cta_begin, tile_begin;
+};
+
+GemmPlan plan_gemm(int M, int N, int K, int sm_count) {
+  GemmPlan g;
+  const int mt = (M + BM - 1) / BM;
+  g.ntn = (N + BN - 1) / BN;
+  g.tiles = mt * g.ntn;
+  const int kbt = (K + BK - 1) / BK;
+  const long long total = static_cast<long long>(g.tiles) * kbt;
+  g.ctas = static_cast<int>(std::min<long long>(sm_count, total));
+  g.cta_begin.assign(g.ctas + 1, 0);
+  g.tile_begin.assign(g.tiles + 1, 0);
+  for (int c = 0; c < g.ctas; ++c) {
+    g.cta_begin[c] = static_cast<int>(g.segs.size());
+    long long a = total * c / g.ctas, e = total * (c + 1) / g.ctas;
+    while (a < e) {
+      const int t = static_cast<int>(a / kbt);
+      const int kb0 = static_cast<int>(a % kbt);
+      const int kb1 = static_cast<int>(std::min<long long>(kbt, kb0 + (e - a)));
+      g.segs.push_back(make_int4(t, kb0, kb1, 0));
+      a += kb1 - kb0;
+    }
+  }
+  g.cta_begin[g.ctas] = static_cast<int>(g.segs.size());
+  int s = 0;
+  for (int t = 0; t < g.tiles; ++t) {
+    g.tile_begin[t] = s;
+    while (s < static_cast<int>(g.segs.size()) && g.segs[s].x == t) ++s;
+  }
+  g.tile_begin[g.tiles] = s;
+  return g;
+}
+
+// Device scratch of one GEMM: segment tables and the FP32 stream-K partials.
+struct GemmScratch {
+  int4* segs = nullptr;
+  int* cta_begin = nullptr;
+  int* tile_begin = nullptr;
+  float* part = nullptr;
+};
+
+size_t gemm_scratch_bytes(const GemmPlan& g) {
+  auto up = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  return up(g.segs.size() * sizeof(int4)) + up(g.cta_begin.size() * sizeof(int)) +
+         up(g.tile_begin.size() * sizeof(int)) + up(g.segs.size() * static_cast<size_t>(BM) * BN * sizeof(float));
+}
+
+GemmScratch carve_gemm_scratch(const GemmPlan& g, char* base) {
+  auto up = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  GemmScratch s;
+  s.segs = reinterpret_cast<int4*>(base);
+  base += up(g.segs.size() * sizeof(int4));
+  s.cta_begin = reinterpret_cast<int*>(base);
+  base += up(g.cta_begin.size() * sizeof(int));
+  s.tile_begin = reinterpret_cast<int*>(base);
+  base += up(g.tile_begin.size() * sizeof(int));
+  s.part = reinterpret_cast<float*>(base);
+  return s;
+}
+
+void ensure_smem_attr() {
   static bool attr = false;
   if (!attr) {
     FPLS_CUDA(cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     attr = true;
   }
-  const int mt = (M + BM - 1) / BM, ntn = (N + BN - 1) / BN;
-  const int tiles = mt * ntn;
-  const int kbt = (K + BK - 1) / BK;
-  const long long total = static_cast<long long>(tiles) * kbt;
-  const int ctas = static_cast<int>(std::min<long long>(ctx.sm_count, total));
-  std::vector<int4> segs;
-  std::vector<int> cta_begin(ctas + 1, 0), tile_begin(tiles + 1, 0);
-  // Stream-K: CTA c covers iterations [c*total/ctas, (c+1)*total/ctas) in (tile, kb) order.
-  for (int c = 0; c < ctas; ++c) {
-    cta_begin[c] = static_cast<int>(segs.size());
-    long long a = total * c / ctas, e = total * (c + 1) / ctas;
-    while (a < e) {
-      const int t = static_cast<int>(a / kbt);
-      const int kb0 = static_cast<int>(a % kbt);
-      const int kb1 = static_cast<int>(std::min<long long>(kbt, kb0 + (e - a)));
-      segs.push_back(make_int4(t, kb0, kb1, 0));
-      a += kb1 - kb0;
-    }
-  }
-  cta_begin[ctas] = static_cast<int>(segs.size());
-  // Segments of a tile are contiguous (tile-major order).
-  {
-    int s = 0;
-    for (int t = 0; t < tiles; ++t) {
-      tile_begin[t] = s;
-      while (s < static_cast<int>(segs.size()) && segs[s].x == t) ++s;
-    }
-    tile_begin[tiles] = s;
-  }
-  Arena& ar = ctx.arena;
-  int4* d_segs = ar.alloc_n<int4>(segs.size());
-  int* d_cb = ar.alloc_n<int>(cta_begin.size());
-  int* d_tb = ar.alloc_n<int>(tile_begin.size());
-  float* part = ar.alloc_n<float>(segs.size() * static_cast<size_t>(BM) * BN);
-  h2d(d_segs, segs.data(), segs.size() * sizeof(int4));
-  h2d(d_cb, cta_begin.data(), cta_begin.size() * sizeof(int));
-  h2d(d_tb, tile_begin.data(), tile_begin.size() * sizeof(int));
+}
+
+// C (M x N) = alpha * A B^T + beta C on stream `st` with the given scratch; no allocation.
+void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,
+                    double beta, double* C, int ldc, const GemmPlan& g, const GemmScratch& s,
+                    int* err, cudaStream_t st, Context* prof) {
+  ensure_smem_attr();
+  FPLS_CUDA(cudaMemcpyAsync(s.segs, g.segs.data(), g.segs.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+  FPLS_CUDA(cudaMemcpyAsync(s.cta_begin, g.cta_begin.data(), g.cta_begin.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  FPLS_CUDA(cudaMemcpyAsync(s.tile_begin, g.tile_begin.data(), g.tile_begin.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   const CUtensorMap mAhi = make_map(A.hi, M, K, A.ld, BM);
   const CUtensorMap mAlo = make_map(A.lo, M, K, A.ld, BM);
   const CUtensorMap mBhi = make_map(B.hi, N, K, B.ld, BN);
   const CUtensorMap mBlo = make_map(B.lo, N, K, B.ld, BN);
-  int* err = ctx.d_status + 16;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  if (ctx.profile) {
+  if (prof) {
     FPLS_CUDA(cudaEventCreate(&ev0));
     FPLS_CUDA(cudaEventCreate(&ev1));
-    FPLS_CUDA(cudaEventRecord(ev0, ctx.stream));
+    FPLS_CUDA(cudaEventRecord(ev0, st));
   }
-  split_gemm_kernel<<<ctas, NUM_THREADS, SMEM_BYTES, ctx.stream>>>(mAhi, mAlo, mBhi, mBlo, d_segs, d_cb,
-                                                                   ntn, part, err); ::fpls::note_launch();
+  split_gemm_kernel<<<g.ctas, NUM_THREADS, SMEM_BYTES, st>>>(mAhi, mAlo, mBhi, mBlo, s.segs, s.cta_begin,
+                                                             g.ntn, s.part, err); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
-  if (ctx.profile) {
-    FPLS_CUDA(cudaEventRecord(ev1, ctx.stream));
-    ctx.prof_events.push_back(ev0);
-    ctx.prof_events.push_back(ev1);
+  if (prof) {
+    FPLS_CUDA(cudaEventRecord(ev1, st));
+    prof->prof_events.push_back(ev0);
+    prof->prof_events.push_back(ev1);
     // Algorithmic bytes: both BF16 halves of A and B once, the FP64 result once.
-    ctx.prof_bytes += 4.0 * (static_cast<double>(M) * K + static_cast<double>(N) * K) +
-                      8.0 * static_cast<double>(M) * N;
+    prof->prof_bytes += 4.0 * (static_cast<double>(M) * K + static_cast<double>(N) * K) +
+                        8.0 * static_cast<double>(M) * N;
   }
-  split_reduce_kernel<<<tiles, 256, 0, ctx.stream>>>(part, d_tb, ntn, M, N, alpha, beta, C, ldc); ::fpls::note_launch();
+  split_reduce_kernel<<<g.tiles, 256, 0, st>>>(s.part, s.tile_begin, g.ntn, M, N, alpha, beta, C, ldc); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,
+                double beta, double* C, int ldc) {
+  Context& ctx = Context::get();
+  const GemmPlan g = plan_gemm(M, N, K, ctx.sm_count);
+  char* base = ctx.arena.alloc_n<char>(gemm_scratch_bytes(g));
+  split_gemm_run(A, B, M, N, K, alpha, beta, C, ldc, g, carve_gemm_scratch(g, base),
+                 ctx.d_status + 16, ctx.stream, ctx.profile ? &ctx : nullptr);
+}
+
+void split_cols_on(const double* X, int rows, int cols, int ld, const SplitPair& out, cudaStream_t st,
+                   int sm_count) {
+  split_cols_kernel<<<4 * sm_count, 256, 0, st>>>(X, rows, cols, ld, out.hi, out.lo, out.ld); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+void split_rows_on(const double* X, int rows, int cols, int ld, const SplitPair& out, cudaStream_t st) {
+  dim3 grid((out.ld + 31) / 32, (rows + 31) / 32);
+  split_rows_kernel<<<grid, dim3(32, 8), 0, st>>>(X, rows, cols, ld, out.hi, out.lo, out.ld); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void split_cols(const double* X, int rows, int cols, int ld, const SplitPair& out) {
   Context& ctx = Context::get();
-  split_cols_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(X, rows, cols, ld, out.hi, out.lo, out.ld); ::fpls::note_launch();
-  FPLS_CHECK_LAUNCH();
+  split_cols_on(X, rows, cols, ld, out, ctx.stream, ctx.sm_count);
 }
 
 void split_rows(const double* X, int rows, int cols, int ld, const SplitPair& out) {
-  Context& ctx = Context::get();
-  dim3 grid((out.ld + 31) / 32, (rows + 31) / 32);
-  split_rows_kernel<<<grid, dim3(32, 8), 0, ctx.stream>>>(X, rows, cols, ld, out.hi, out.lo, out.ld); ::fpls::note_launch();
-  FPLS_CHECK_LAUNCH();
+  split_rows_on(X, rows, cols, ld, out, Context::get().stream);
 }
 
 struct XOperatorSplit : public XOperator {
@@ -493,6 +550,28 @@ void split_gemm_test(const double* A, const double* B, int M, int N, int K, doub
   split_rows(A, M, K, M, a);
   split_cols(B, K, N, K, b);
   split_gemm(a, b, M, N, K, 1.0, 0.0, C, M);
+}
+
+size_t split_gemm_scratch_need(int M, int N, int K, int sm_count) {
+  const GemmPlan g = plan_gemm(M, N, K, sm_count);
+  return 2 * (pair_elems(M, K) + pair_elems(N, K)) + gemm_scratch_bytes(g) + 256;
+}
+
+void split_gemm_in_scratch(const double* A, const double* B, int M, int N, int K, double* C,
+                           void* scratch, size_t scratch_bytes, int* err, cudaStream_t st,
+                           int sm_count) {
+  const GemmPlan g = plan_gemm(M, N, K, sm_count);
+  const size_t need = 2 * (pair_elems(M, K) + pair_elems(N, K)) + gemm_scratch_bytes(g) + 256;
+  if (need > scratch_bytes) throw Error(kErrArgument, "split GEMM shape exceeds the fixed scratch size");
+  char* base = static_cast<char*>(scratch);
+  SplitPair a = pair_at(reinterpret_cast<__nv_bfloat16*>(base), M, K);
+  base += 2 * pair_elems(M, K);
+  SplitPair b = pair_at(reinterpret_cast<__nv_bfloat16*>(base), N, K);
+  base += 2 * pair_elems(N, K);
+  base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(base) + 255) & ~static_cast<uintptr_t>(255));
+  split_rows_on(A, M, K, M, a, st);
+  split_cols_on(B, K, N, K, b, st, sm_count);
+  split_gemm_run(a, b, M, N, K, 1.0, 0.0, C, M, g, carve_gemm_scratch(g, base), err, st, nullptr);
 }
 
 }  // namespace fpls

@@ -17,4 +17,13 @@ std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p);
 // into BF16 hi/lo; used by tests of the tensor-core kernel.  C is M x N (ld M).
 void split_gemm_test(const double* A, const double* B, int M, int N, int K, double* C);
 
+// Same product with every temporary (split operands, stream-K tables and
+// partials) placed in a caller-provided device buffer, on stream `st`, with no
+// allocation.  Throws when the shape needs more than scratch_bytes (see
+// split_gemm_scratch_need).  A, B, C: device, column-major (M x K, K x N, M x N).
+size_t split_gemm_scratch_need(int M, int N, int K, int sm_count);
+void split_gemm_in_scratch(const double* A, const double* B, int M, int N, int K, double* C,
+                           void* scratch, size_t scratch_bytes, int* err, cudaStream_t st,
+                           int sm_count);
+
 }  // namespace fpls

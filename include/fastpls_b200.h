@@ -198,6 +198,23 @@ int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, 
                    int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
                    int* inner_pred, int* fit_status, char* err, size_t errlen);
 
+/* C (M x N) = A (M x K) * B (K x N) through the BF16 split tensor-core kernel,
+ * for callers that cannot allocate device memory (a host that runs inside
+ * another runtime's fixed memory pool, a stream callback, an allocation-free
+ * loop).  No counterpart in the reference.  A, B and C are DEVICE pointers
+ * (column-major, FP64) owned by the caller on the library's current device
+ * (device 0, or FASTPLS_DEVICE).  The call allocates nothing: every temporary
+ * lives in one fixed 16 MiB device array that each GPU loading the library
+ * holds until exit; shapes needing more (about (M + N) x K above 2.5 million
+ * elements at N <= 64) are rejected with FPLS_ERR_ARGUMENT.  The first call on
+ * a device resolves that array's address (cudaGetSymbolAddress), so make it
+ * before any stream capture.  Work runs on the legacy default stream and the
+ * call returns after it finishes.  All calls share the one array, which keeps
+ * the last call's contents: calls that overlap on the GPU (other threads,
+ * other streams) race. */
+int fpls_bf16x3_gemm_noalloc(const double* A, int M, int K, const double* B, int N, double* C,
+                             char* err, size_t errlen);
+
 /* Registers a predictor matrix (n x p, FP64 or FP32) in device memory for
  * repeated calls; *handle identifies it until fpls_x_free.  Lets a caller keep
  * X resident across CV runs instead of re-sending it (the reference re-uploads

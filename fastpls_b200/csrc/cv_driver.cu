@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <memory>
 #include <numeric>
+#include <thread>
 
 namespace fpls {
 namespace {
@@ -162,7 +163,24 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   std::vector<int> grp(Fa), ntrain(Fa);
   std::vector<double> inv_nf(Fa), mYf((size_t)Fa * m), mYall(m, 0.0), dY((size_t)Fa * m);
   for (int i = 0; i < n; ++i) mYall[y[i] - 1] += 1.0 / n;
+  // The per-fit Gaussian sketches (libstdc++ mt19937 streams, one per seed) are
+  // drawn on host threads while the device runs the set-up below.
   std::vector<double> om((size_t)Fa * p);
+  std::vector<std::thread> pool;
+  struct Joiner {
+    std::vector<std::thread>& v;
+    ~Joiner() {
+      for (auto& t : v)
+        if (t.joinable()) t.join();
+    }
+  } joiner{pool};
+  {
+    const int nt = std::max(1, std::min<int>(Fa, static_cast<int>(std::thread::hardware_concurrency())));
+    for (int t = 0; t < nt; ++t)
+      pool.emplace_back([&om, &fs, &act, p, Fa, nt, t] {
+        for (int a = t; a < Fa; a += nt) host_gaussian(om.data() + (size_t)a * p, p, fs.seeds[act[a]]);
+      });
+  }
   for (int a = 0; a < Fa; ++a) {
     const int f = act[a];
     std::copy(fs.train.begin() + (size_t)f * n, fs.train.begin() + (size_t)(f + 1) * n, tr.begin() + (size_t)a * n);
@@ -176,7 +194,6 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
       mYf[(size_t)a * m + c] = counts[(size_t)f * m + c] / nt;
       dY[(size_t)a * m + c] = mYf[(size_t)a * m + c] - mYall[c];
     }
-    host_gaussian(om.data() + (size_t)a * p, p, fs.seeds[f]);
   }
   uint8_t* d_tr = ar.alloc_n<uint8_t>(tr.size());
   uint8_t* d_te = ar.alloc_n<uint8_t>(te.size());
@@ -199,7 +216,6 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   h2d(d_mYf, mYf.data(), mYf.size() * sizeof(double));
   h2d(d_mYall, mYall.data(), m * sizeof(double));
   h2d(d_dY, dY.data(), dY.size() * sizeof(double));
-  h2d(d_om, om.data(), om.size() * sizeof(double));
   h2d(d_lab, lab0.data(), n * sizeof(int));
   h2d(d_nc, ncomp, L * sizeof(int));
   SimplsBatch b;
@@ -225,6 +241,9 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   b.delta = delta;
   b.S = ar.alloc_n<double>((size_t)Fa * p * m);
   simpls_batch_crosscov(b, X, d_nt);
+  for (auto& th : pool)
+    if (th.joinable()) th.join();
+  h2d(d_om, om.data(), om.size() * sizeof(double));
   b.R = ar.alloc_n<double>((size_t)Fa * p * K);
   b.Q = ar.alloc_n<double>((size_t)Fa * m * K);
   b.V = ar.alloc_n<double>((size_t)Fa * p * K);

@@ -8,6 +8,7 @@ namespace fpls {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
 
 struct Eng {
   int n, p, m, F, K, cp, cn, szp, szn;
@@ -21,6 +22,7 @@ struct Eng {
   double* S;
   const double* omega;
   int m1_mode;
+  int iters;
   double* R;
   double* Q;
   double* V;
@@ -59,48 +61,74 @@ __device__ __forceinline__ double sum_parts(const double* parts, int count, int 
   return s;
 }
 
-// zout[f][chunk][j] = sum_{i in chunk} S_f[i,j] y[i]  (block reductions per column)
-__device__ void partial_StY(const Eng& e, int f, int chunk, int b, int en, const double* yv,
-                            double* zout, double* scratch) {
-  const double* Sf = e.S + (size_t)f * e.p * e.m;
-  for (int j = 0; j < e.m; ++j) {
-    double a = 0.0;
-    for (int i = b + threadIdx.x; i < en; i += blockDim.x) a += Sf[i + (size_t)j * e.p] * yv[i];
-    a = block_sum(a, scratch);
-    if (threadIdx.x == 0) zout[((size_t)f * e.cp + chunk) * e.m + j] = a;
+// Block-wide sums of the first `count` entries of a per-thread vector; the
+// result is written to out[0..count) by threads 0..count-1.  One pass of warp
+// shuffles per entry and a single shared-memory exchange for all entries.
+template <int NV>
+__device__ __forceinline__ void block_sum_vec(double (&v)[NV], int count, double* out, int out_stride) {
+  __shared__ double sm[kWarps][NV];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    if (j < count) {
+      const double w = warp_sum(v[j]);
+      if (lane == 0) sm[warp][j] = w;
+    }
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < count; j += blockDim.x) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) s += sm[w][j];
+    out[(size_t)j * out_stride] = s;
+  }
+  __syncthreads();
+}
+
+constexpr int NV = 16;   // register block of per-thread partial sums
+
+// zout[f][chunk][j] = sum_{i in chunk} S_f[i,j] y[i] for every column j (blocks of
+// NV columns), or the chunk's ||y||^2 when `norm_only`.
+__device__ __forceinline__ void chunk_StY(const Eng& e, int f, int chunk, const double* Sf,
+                                          const double* yf, int b, int en, double* zout,
+                                          bool norm_only) {
+  double acc[NV];
+  if (norm_only) {
+    acc[0] = 0.0;
+    for (int i = b + threadIdx.x; i < en; i += blockDim.x) acc[0] += yf[i] * yf[i];
+    block_sum_vec<NV>(acc, 1, e.npart + (size_t)f * e.cp + chunk, 1);
+    return;
+  }
+  for (int j0 = 0; j0 < e.m; j0 += NV) {
+    const int cnt = min(NV, e.m - j0);
+#pragma unroll
+    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+    for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+      const double yi = yf[i];
+#pragma unroll
+      for (int j = 0; j < NV; ++j)
+        if (j < cnt) acc[j] += Sf[i + (size_t)(j0 + j) * e.p] * yi;
+    }
+    block_sum_vec<NV>(acc, cnt, zout + ((size_t)f * e.cp + chunk) * e.m + j0, 1);
   }
 }
 
-__global__ void k_refresh_start(Eng e, int a, int iters) {
-  __shared__ double scratch[32];
+// First component's refresh start: y = Omega (or the single column of S).
+__global__ void k_refresh_start(Eng e) {
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   int b, en;
   chunk_range(chunk, e.szp, e.p, b, en);
   const double* Sf = e.S + (size_t)f * e.p * e.m;
-  const double* y0;
-  if (e.m1_mode) y0 = Sf;                                   // exact left vector of p x 1
-  else if (a == 0) y0 = e.omega + (size_t)f * e.p;          // Gaussian sketch, seed
-  else y0 = e.R + ((size_t)f * e.K + (a - 1)) * e.p;        // warm start r_{a-1}
+  const double* y0 = e.m1_mode ? Sf : e.omega + (size_t)f * e.p;
   double* yf = e.y + (size_t)f * e.p;
-  double ss = 0.0;
-  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
-    const double v = y0[i];
-    yf[i] = v;
-    ss += v * v;
-  }
-  if (iters > 0) {
-    __syncthreads();
-    partial_StY(e, f, chunk, b, en, yf, e.zA, scratch);
-  } else {
-    ss = block_sum(ss, scratch);
-    if (threadIdx.x == 0) e.npart[(size_t)f * e.cp + chunk] = ss;
-  }
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) yf[i] = y0[i];
+  chunk_StY(e, f, chunk, Sf, yf, b, en, e.zA, e.iters == 0);
 }
 
+// y <- S z with z = sum of the partials of S^T y; then the next partials (or ||y||^2).
 __global__ void k_refresh_apply(Eng e, const double* zin, double* zout, int last) {
   extern __shared__ double zs[];
-  __shared__ double scratch[32];
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   int b, en;
@@ -110,20 +138,12 @@ __global__ void k_refresh_apply(Eng e, const double* zin, double* zout, int last
   __syncthreads();
   const double* Sf = e.S + (size_t)f * e.p * e.m;
   double* yf = e.y + (size_t)f * e.p;
-  double ss = 0.0;
   for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
     double acc = 0.0;
     for (int j = 0; j < e.m; ++j) acc += Sf[i + (size_t)j * e.p] * zs[j];
     yf[i] = acc;
-    ss += acc * acc;
   }
-  if (!last) {
-    __syncthreads();
-    partial_StY(e, f, chunk, b, en, yf, zout, scratch);
-  } else {
-    ss = block_sum(ss, scratch);
-    if (threadIdx.x == 0) e.npart[(size_t)f * e.cp + chunk] = ss;
-  }
+  chunk_StY(e, f, chunk, Sf, yf, b, en, zout, last != 0);
 }
 
 // r = -sign(y0) y / ||y|| (Householder QR of a single column; the 1 x m core
@@ -158,14 +178,11 @@ __global__ void k_refresh_finish(Eng e) {
   }
 }
 
-// t = mask * (U - delta.rhat); partial sums of t^2 and t; q partials.
+// t = mask * (U - delta.rhat); partial sums of t^2, t and q = Y^T t.
 __global__ void k_scores(Eng e, int a) {
   extern __shared__ double qs[];
-  __shared__ double scratch[32];
   const int f = blockIdx.y, chunk = blockIdx.x;
-  if (e.status[f]) {
-    return;
-  }
+  if (e.status[f]) return;
   int b, en;
   chunk_range(chunk, e.szn, e.n, b, en);
   const double c = e.delta ? sum_parts(e.cpart + (size_t)f * e.cp, e.cp, 1) : 0.0;
@@ -177,35 +194,34 @@ __global__ void k_scores(Eng e, int a) {
     for (int j = threadIdx.x; j < e.m; j += blockDim.x) qs[j] = 0.0;
     __syncthreads();
   }
-  double s2 = 0.0, s1 = 0.0;
+  double acc[NV];
+  acc[0] = acc[1] = 0.0;
   for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
     const double u = Uf[i] - c;
     const double t = (mk && !mk[i]) ? 0.0 : u;
     Tf[i] = t;
     if (keep) keep[i] = u;
-    s2 += t * t;
-    s1 += t;
+    acc[0] += t * t;
+    acc[1] += t;
     if (e.labels && t != 0.0) atomicAdd(&qs[e.labels[i]], t);
   }
-  s2 = block_sum(s2, scratch);
-  s1 = block_sum(s1, scratch);
-  if (threadIdx.x == 0) {
-    e.tpart[((size_t)f * e.cn + chunk) * 2 + 0] = s2;
-    e.tpart[((size_t)f * e.cn + chunk) * 2 + 1] = s1;
-  }
+  block_sum_vec<NV>(acc, 2, e.tpart + ((size_t)f * e.cn + chunk) * 2, 1);
   double* qp = e.qpart + ((size_t)f * e.cn + chunk) * e.m;
   if (e.labels) {
-    __syncthreads();
     for (int j = threadIdx.x; j < e.m; j += blockDim.x) qp[j] = qs[j];
-  } else {
-    __syncthreads();
-    for (int j = 0; j < e.m; ++j) {
-      double acc = 0.0;
-      const double* yc = e.Yg + (size_t)j * e.n;
-      for (int i = b + threadIdx.x; i < en; i += blockDim.x) acc += Tf[i] * yc[i];
-      acc = block_sum(acc, scratch);
-      if (threadIdx.x == 0) qp[j] = acc;
+    return;
+  }
+  for (int j0 = 0; j0 < e.m; j0 += NV) {
+    const int cnt = min(NV, e.m - j0);
+#pragma unroll
+    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+    for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+      const double t = Tf[i];
+#pragma unroll
+      for (int j = 0; j < NV; ++j)
+        if (j < cnt) acc[j] += t * e.Yg[i + (size_t)(j0 + j) * e.n];
     }
+    block_sum_vec<NV>(acc, cnt, qp + j0, 1);
   }
 }
 
@@ -220,9 +236,10 @@ __device__ __forceinline__ void t_stats(const Eng& e, int f, double& tn, double&
   st = s1;
 }
 
-// p = colscale * (P - delta * sum(t)) / ||t||; partial V^T p.
+constexpr int KV = 32;   // register block of Gram-Schmidt dot products
+
+// p = colscale * (P - delta * sum(t)) / ||t||; partial w = V^T p (blocks of KV loadings).
 __global__ void k_loading(Eng e, int a) {
-  __shared__ double scratch[32];
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   double tn, st;
@@ -237,26 +254,31 @@ __global__ void k_loading(Eng e, int a) {
   const double* dl = e.delta ? e.delta + (size_t)f * e.p : nullptr;
   const double* Pf = e.P + (size_t)f * e.p;
   double* pf = e.pv + (size_t)f * e.p;
+  const double* Vf = e.V + (size_t)f * e.p * e.K;
   for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
     double v = Pf[i];
     if (dl) v -= dl[i] * st;
     if (sc) v *= sc[i];
     pf[i] = v / tn;
   }
-  __syncthreads();
-  const double* Vf = e.V + (size_t)f * e.p * e.K;
-  for (int l = 0; l < a; ++l) {
-    double acc = 0.0;
-    for (int i = b + threadIdx.x; i < en; i += blockDim.x) acc += Vf[i + (size_t)l * e.p] * pf[i];
-    acc = block_sum(acc, scratch);
-    if (threadIdx.x == 0) e.wpart[((size_t)f * e.cp + chunk) * e.K + l] = acc;
+  double acc[KV];
+  for (int l0 = 0; l0 < a; l0 += KV) {
+    const int cnt = min(KV, a - l0);
+#pragma unroll
+    for (int l = 0; l < KV; ++l) acc[l] = 0.0;
+    for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+      const double v = pf[i];
+#pragma unroll
+      for (int l = 0; l < KV; ++l)
+        if (l < cnt) acc[l] += Vf[i + (size_t)(l0 + l) * e.p] * v;
+    }
+    block_sum_vec<KV>(acc, cnt, e.wpart + ((size_t)f * e.cp + chunk) * e.K + l0, 1);
   }
 }
 
-// v = p - V (V^T p); partial ||v||^2.
+// v = p - V (V^T p); partials of ||v||^2 and of S^T v.
 __global__ void k_orth(Eng e, int a) {
   extern __shared__ double ws[];
-  __shared__ double scratch[32];
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   int b, en;
@@ -266,21 +288,43 @@ __global__ void k_orth(Eng e, int a) {
   __syncthreads();
   const double* Vf = e.V + (size_t)f * e.p * e.K;
   const double* pf = e.pv + (size_t)f * e.p;
+  const double* Sf = e.S + (size_t)f * e.p * e.m;
   double* vf = e.v + (size_t)f * e.p;
-  double ss = 0.0;
+  double acc[NV];
+  acc[0] = 0.0;
   for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
-    double acc = pf[i];
-    for (int l = 0; l < a; ++l) acc -= Vf[i + (size_t)l * e.p] * ws[l];
-    vf[i] = acc;
-    ss += acc * acc;
+    double x = pf[i];
+    int l = 0;
+    for (; l + 4 <= a; l += 4) {
+      const double v0 = Vf[i + (size_t)l * e.p], v1 = Vf[i + (size_t)(l + 1) * e.p];
+      const double v2 = Vf[i + (size_t)(l + 2) * e.p], v3 = Vf[i + (size_t)(l + 3) * e.p];
+      x -= v0 * ws[l] + v1 * ws[l + 1] + v2 * ws[l + 2] + v3 * ws[l + 3];
+    }
+    for (; l < a; ++l) x -= Vf[i + (size_t)l * e.p] * ws[l];
+    vf[i] = x;
+    acc[0] += x * x;
   }
-  ss = block_sum(ss, scratch);
-  if (threadIdx.x == 0) e.vpart[(size_t)f * e.cp + chunk] = ss;
+  block_sum_vec<NV>(acc, 1, e.vpart + (size_t)f * e.cp + chunk, 1);
+  // S^T v (unnormalised) for the deflation, blocks of NV columns.
+  for (int j0 = 0; j0 < e.m; j0 += NV) {
+    const int cnt = min(NV, e.m - j0);
+#pragma unroll
+    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+    for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+      const double x = vf[i];
+#pragma unroll
+      for (int j = 0; j < NV; ++j)
+        if (j < cnt) acc[j] += x * Sf[i + (size_t)(j0 + j) * e.p];
+    }
+    block_sum_vec<NV>(acc, cnt, e.vSpart + ((size_t)f * e.cp + chunk) * e.m + j0, 1);
+  }
 }
 
-// v /= ||v||; V[:, a] = v; partial v^T S.
-__global__ void k_vnorm(Eng e, int a) {
-  __shared__ double scratch[32];
+// v /= ||v||; V[:, a] = v; S -= v (v^T S); R[:, a] = r / ||t||; Q[:, a] = q / ||t||;
+// then the next component's refresh start (partials of S^T r_a over the
+// deflated S, or ||S[:,0]||^2 when m == 1).
+__global__ void k_deflate(Eng e, int a, int next) {
+  extern __shared__ double vs[];
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   const double vn = sqrt(sum_parts(e.vpart + (size_t)f * e.cp, e.cp, 1));
@@ -290,44 +334,26 @@ __global__ void k_vnorm(Eng e, int a) {
   }
   int b, en;
   chunk_range(chunk, e.szp, e.p, b, en);
-  double* vf = e.v + (size_t)f * e.p;
-  double* Vcol = e.V + ((size_t)f * e.K + a) * e.p;
-  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
-    const double x = vf[i] / vn;
-    vf[i] = x;
-    Vcol[i] = x;
-  }
-  __syncthreads();
-  const double* Sf = e.S + (size_t)f * e.p * e.m;
-  for (int j = 0; j < e.m; ++j) {
-    double acc = 0.0;
-    for (int i = b + threadIdx.x; i < en; i += blockDim.x) acc += vf[i] * Sf[i + (size_t)j * e.p];
-    acc = block_sum(acc, scratch);
-    if (threadIdx.x == 0) e.vSpart[((size_t)f * e.cp + chunk) * e.m + j] = acc;
-  }
-}
-
-// S -= v (v^T S); R[:, a] = r / ||t||; Q[:, a] = q / ||t||.
-__global__ void k_deflate(Eng e, int a) {
-  extern __shared__ double vs[];
-  const int f = blockIdx.y, chunk = blockIdx.x;
-  if (e.status[f]) return;
-  int b, en;
-  chunk_range(chunk, e.szp, e.p, b, en);
   for (int j = threadIdx.x; j < e.m; j += blockDim.x)
-    vs[j] = sum_parts(e.vSpart + (size_t)f * e.cp * e.m + j, e.cp, e.m);
+    vs[j] = sum_parts(e.vSpart + (size_t)f * e.cp * e.m + j, e.cp, e.m) / vn;
   __syncthreads();
   double tn, st;
   t_stats(e, f, tn, st);
   double* Sf = e.S + (size_t)f * e.p * e.m;
-  const double* vf = e.v + (size_t)f * e.p;
-  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
-    const double vi = vf[i];
-    for (int j = 0; j < e.m; ++j) Sf[i + (size_t)j * e.p] -= vi * vs[j];
-  }
+  double* vf = e.v + (size_t)f * e.p;
+  double* Vcol = e.V + ((size_t)f * e.K + a) * e.p;
   double* Rcol = e.R + ((size_t)f * e.K + a) * e.p;
   const double* rf = e.r + (size_t)f * e.p;
-  for (int i = b + threadIdx.x; i < en; i += blockDim.x) Rcol[i] = rf[i] / tn;
+  double* yf = e.y + (size_t)f * e.p;
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+    const double vi = vf[i] / vn;
+    vf[i] = vi;
+    Vcol[i] = vi;
+    for (int j = 0; j < e.m; ++j) Sf[i + (size_t)j * e.p] -= vi * vs[j];
+    const double ri = rf[i] / tn;
+    Rcol[i] = ri;
+    if (next) yf[i] = e.m1_mode ? Sf[i] : ri;
+  }
   if (chunk == 0) {
     double* Qcol = e.Q + ((size_t)f * e.K + a) * e.m;
     for (int j = threadIdx.x; j < e.m; j += blockDim.x) {
@@ -343,9 +369,9 @@ __global__ void k_deflate(Eng e, int a) {
       e.ncomp_done[f] = a + 1;
     }
   }
+  if (next) chunk_StY(e, f, chunk, Sf, yf, b, en, e.zA, e.iters == 0);
 }
 
-// Masked response block M[:, f*m + j] = mask_f * Y'[:, j] (Y' = one-hot or Yg).
 __global__ void k_masked_response(Eng e, double* M) {
   const size_t total = (size_t)e.n * e.F * e.m;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
@@ -382,15 +408,16 @@ __global__ void k_crosscov_finish(Eng e, const double* P, const int* n_train) {
 Eng make_eng(const SimplsBatch& b) {
   Eng e{};
   e.n = b.n; e.p = b.p; e.m = b.m; e.F = b.F; e.K = b.K;
-  const int target = 2 * Context::get().sm_count;
-  e.cp = std::max(1, std::min(ceil_div(target, b.F), ceil_div(b.p, 128)));
+  const int target = 4 * Context::get().sm_count;
+  e.cp = std::max(1, std::min(ceil_div(target, b.F), ceil_div(b.p, 256)));
   e.szp = ceil_div(b.p, e.cp);
   e.cp = ceil_div(b.p, e.szp);
-  e.cn = std::max(1, std::min(ceil_div(target, b.F), ceil_div(b.n, 128)));
+  e.cn = std::max(1, std::min(ceil_div(target, b.F), ceil_div(b.n, 256)));
   e.szn = ceil_div(b.n, e.cn);
   e.cn = ceil_div(b.n, e.szn);
   e.Yg = b.Yg; e.labels = b.labels; e.mY_all = b.mY_all; e.mask = b.mask; e.delta = b.delta;
   e.colscale = b.colscale; e.dY = b.dY; e.S = b.S; e.omega = b.omega; e.m1_mode = b.m1_mode;
+  e.iters = b.m1_mode ? 0 : std::max(b.power_iters, 0);
   e.R = b.R; e.Q = b.Q; e.V = b.V; e.tnorm = b.tnorm; e.Tkeep = b.Tkeep;
   e.ncomp_done = b.ncomp_done; e.status = b.status;
   return e;
@@ -451,16 +478,17 @@ void simpls_batch_run(const SimplsBatch& b) {
   const dim3 gp(e.cp, b.F), gn(e.cn, b.F);
   const size_t sm_m = std::max<size_t>(b.m, 1) * sizeof(double);
   const size_t sm_k = std::max<size_t>(b.K, 1) * sizeof(double);
-  const int iters = b.m1_mode ? 0 : std::max(b.power_iters, 0);
   cudaStream_t st = ctx.stream;
+  k_refresh_start<<<gp, kThreads, 0, st>>>(e); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
   for (int a = 0; a < b.K; ++a) {
     // Refresh: y <- S (S^T y) `iters` times from the warm start, then normalise.
-    k_refresh_start<<<gp, kThreads, 0, st>>>(e, a, iters); ::fpls::note_launch();
     double* zin = e.zA;
     double* zout = e.zB;
-    for (int it = 0; it < iters; ++it) {
-      const int last = (it == iters - 1) ? 1 : 0;
+    for (int it = 0; it < e.iters; ++it) {
+      const int last = (it == e.iters - 1) ? 1 : 0;
       k_refresh_apply<<<gp, kThreads, sm_m, st>>>(e, zin, zout, last); ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
       std::swap(zin, zout);
     }
     k_refresh_finish<<<gp, kThreads, 0, st>>>(e); ::fpls::note_launch();
@@ -470,9 +498,10 @@ void simpls_batch_run(const SimplsBatch& b) {
     FPLS_CHECK_LAUNCH();
     b.X->t_times(e.T, b.F, e.P);
     k_loading<<<gp, kThreads, 0, st>>>(e, a); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
     k_orth<<<gp, kThreads, sm_k, st>>>(e, a); ::fpls::note_launch();
-    k_vnorm<<<gp, kThreads, 0, st>>>(e, a); ::fpls::note_launch();
-    k_deflate<<<gp, kThreads, sm_m, st>>>(e, a); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    k_deflate<<<gp, kThreads, sm_m, st>>>(e, a, a + 1 < b.K ? 1 : 0); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
 }

@@ -268,13 +268,18 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constan
 }
 
 // C[m + n*ldc] = alpha * sum_{segments of the tile} part + beta * C   (FP64)
+constexpr int kReduceSplit = 8;
+
 __global__ void split_reduce_kernel(const float* __restrict__ part, const int* __restrict__ tile_seg,
                                     int n_tiles_n, int M, int N, double alpha, double beta,
                                     double* __restrict__ C, int ldc) {
-  const int tile = blockIdx.x;
+  // kReduceSplit blocks per tile, each covering BN / kReduceSplit columns.
+  const int tile = blockIdx.x / kReduceSplit;
+  const int part_idx = blockIdx.x % kReduceSplit;
   const int mt = tile / n_tiles_n, nt = tile % n_tiles_n;
   const int s0 = tile_seg[tile], s1 = tile_seg[tile + 1];
-  for (int e = threadIdx.x; e < BM * BN; e += blockDim.x) {
+  const int e0 = part_idx * (BM * BN / kReduceSplit), e1 = e0 + BM * BN / kReduceSplit;
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
     const int mm = e % BM, nn = e / BM;
     const int m = mt * BM + mm, n = nt * BN + nn;
     if (m >= M || n >= N) continue;
@@ -480,7 +485,7 @@ void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K,
     prof->prof_bytes += 4.0 * (static_cast<double>(M) * K + static_cast<double>(N) * K) +
                         8.0 * static_cast<double>(M) * N;
   }
-  split_reduce_kernel<<<g.tiles, 256, 0, st>>>(s.part, s.tile_begin, g.ntn, M, N, alpha, beta, C, ldc); ::fpls::note_launch();
+  split_reduce_kernel<<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, g.ntn, M, N, alpha, beta, C, ldc); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 

@@ -116,7 +116,11 @@ int fpls_has_cuda(void) {
 }
 
 int fpls_reset_workspace(char* err, size_t errlen) {
-  return guarded(err, errlen, [&] { Context::get().release(); });
+  return guarded(err, errlen, [&] {
+    Context::get().sync();
+    split_gemm_release_cache();
+    Context::get().release();
+  });
 }
 
 int fpls_matrix_multiply(const double* A, int a_rows, int a_cols, const double* B, int b_cols,

@@ -23,6 +23,8 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -457,13 +459,17 @@ void ensure_smem_attr() {
 }
 
 // C (M x N) = alpha * A B^T + beta C on stream `st` with the given scratch; no allocation.
+void upload_plan_tables(const GemmPlan& g, const GemmScratch& s, cudaStream_t st) {
+  FPLS_CUDA(cudaMemcpyAsync(s.segs, g.segs.data(), g.segs.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+  FPLS_CUDA(cudaMemcpyAsync(s.cta_begin, g.cta_begin.data(), g.cta_begin.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  FPLS_CUDA(cudaMemcpyAsync(s.tile_begin, g.tile_begin.data(), g.tile_begin.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+}
+
+// Launches the GEMM and its reduction; the plan tables must already be in `s`.
 void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,
                     double beta, double* C, int ldc, const GemmPlan& g, const GemmScratch& s,
                     int* err, cudaStream_t st, Context* prof) {
   ensure_smem_attr();
-  FPLS_CUDA(cudaMemcpyAsync(s.segs, g.segs.data(), g.segs.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
-  FPLS_CUDA(cudaMemcpyAsync(s.cta_begin, g.cta_begin.data(), g.cta_begin.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-  FPLS_CUDA(cudaMemcpyAsync(s.tile_begin, g.tile_begin.data(), g.tile_begin.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   const CUtensorMap mAhi = make_map(A.hi, M, K, A.ld, BM);
   const CUtensorMap mAlo = make_map(A.lo, M, K, A.ld, BM);
   const CUtensorMap mBhi = make_map(B.hi, N, K, B.ld, BN);
@@ -489,13 +495,38 @@ void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K,
   FPLS_CHECK_LAUNCH();
 }
 
+// Plans (with their device tables and partial buffers) are kept per GEMM shape
+// so that the repeated products of the SIMPLS loop issue no host-to-device copy
+// (a pageable copy would synchronise the stream on every call).
+struct CachedPlan {
+  GemmPlan g;
+  char* dev = nullptr;
+  GemmScratch s;
+};
+std::map<std::array<int, 4>, CachedPlan>& plan_cache() {
+  static std::map<std::array<int, 4>, CachedPlan> cache;
+  return cache;
+}
+
+const CachedPlan& cached_plan(int M, int N, int K, int sm_count, cudaStream_t st) {
+  auto& cache = plan_cache();
+  const std::array<int, 4> key{M, N, K, sm_count};
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  CachedPlan c;
+  c.g = plan_gemm(M, N, K, sm_count);
+  FPLS_CUDA(cudaMalloc(&c.dev, gemm_scratch_bytes(c.g)));
+  c.s = carve_gemm_scratch(c.g, c.dev);
+  upload_plan_tables(c.g, c.s, st);
+  return cache.emplace(key, std::move(c)).first->second;
+}
+
 void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,
                 double beta, double* C, int ldc) {
   Context& ctx = Context::get();
-  const GemmPlan g = plan_gemm(M, N, K, ctx.sm_count);
-  char* base = ctx.arena.alloc_n<char>(gemm_scratch_bytes(g));
-  split_gemm_run(A, B, M, N, K, alpha, beta, C, ldc, g, carve_gemm_scratch(g, base),
-                 ctx.d_status + 16, ctx.stream, ctx.profile ? &ctx : nullptr);
+  const CachedPlan& c = cached_plan(M, N, K, ctx.sm_count, ctx.stream);
+  split_gemm_run(A, B, M, N, K, alpha, beta, C, ldc, c.g, c.s, ctx.d_status + 16, ctx.stream,
+                 ctx.profile ? &ctx : nullptr);
 }
 
 void split_cols_on(const double* X, int rows, int cols, int ld, const SplitPair& out, cudaStream_t st,
@@ -544,6 +575,11 @@ struct XOperatorSplit : public XOperator {
 
 }  // namespace
 
+void split_gemm_release_cache() {
+  for (auto& kv : plan_cache()) cudaFree(kv.second.dev);
+  plan_cache().clear();
+}
+
 std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p) {
   return std::unique_ptr<XOperator>(new XOperatorSplit(X, n, p));
 }
@@ -576,7 +612,9 @@ void split_gemm_in_scratch(const double* A, const double* B, int M, int N, int K
   base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(base) + 255) & ~static_cast<uintptr_t>(255));
   split_rows_on(A, M, K, M, a, st);
   split_cols_on(B, K, N, K, b, st, sm_count);
-  split_gemm_run(a, b, M, N, K, 1.0, 0.0, C, M, g, carve_gemm_scratch(g, base), err, st, nullptr);
+  const GemmScratch gs = carve_gemm_scratch(g, base);
+  upload_plan_tables(g, gs, st);
+  split_gemm_run(a, b, M, N, K, 1.0, 0.0, C, M, g, gs, err, st, nullptr);
 }
 
 }  // namespace fpls

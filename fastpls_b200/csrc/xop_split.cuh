@@ -10,6 +10,9 @@
 
 namespace fpls {
 
+// Frees the per-shape GEMM plans kept on the device (fpls_reset_workspace).
+void split_gemm_release_cache();
+
 // Builds the split operator from an FP64 device matrix (n x p, ld n).
 std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p);
 

@@ -1,7 +1,9 @@
 #include "context.cuh"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
+#include <string>
 
 namespace fpls {
 
@@ -140,6 +142,53 @@ void d2d(void* dst, const void* src, size_t bytes) {
 void dzero(void* dst, size_t bytes) {
   if (bytes == 0) return;
   FPLS_CUDA(cudaMemsetAsync(dst, 0, bytes, Context::get().stream));
+}
+
+}  // namespace fpls
+
+namespace fpls {
+
+PhaseTimer::PhaseTimer(const char* title) : title_(title) {
+  const char* e = std::getenv("FASTPLS_TRACE");
+  on_ = e && e[0] == '1';
+  mark("start");
+}
+
+PhaseTimer::~PhaseTimer() {
+  if (on_ && !reported_) {
+    try {
+      report();
+    } catch (...) {
+    }
+  }
+  for (auto& m : marks_) cudaEventDestroy(m.second);
+}
+
+void PhaseTimer::mark(const char* name) {
+  if (!on_) return;
+  cudaEvent_t ev;
+  FPLS_CUDA(cudaEventCreate(&ev));
+  FPLS_CUDA(cudaEventRecord(ev, Context::get().stream));
+  marks_.emplace_back(name, ev);
+}
+
+void PhaseTimer::report() {
+  if (!on_ || reported_) return;
+  reported_ = true;
+  FPLS_CUDA(cudaStreamSynchronize(Context::get().stream));
+  std::vector<std::pair<std::string, double>> acc;
+  double total = 0.0;
+  for (size_t k = 1; k < marks_.size(); ++k) {
+    float ms = 0.f;
+    FPLS_CUDA(cudaEventElapsedTime(&ms, marks_[k - 1].second, marks_[k].second));
+    total += ms;
+    bool found = false;
+    for (auto& a : acc)
+      if (a.first == marks_[k].first) { a.second += ms; found = true; }
+    if (!found) acc.emplace_back(marks_[k].first, ms);
+  }
+  std::fprintf(stderr, "[fastpls trace] %s: %.3f ms\n", title_, total);
+  for (auto& a : acc) std::fprintf(stderr, "  %-14s %8.3f ms\n", a.first.c_str(), a.second);
 }
 
 }  // namespace fpls

@@ -59,6 +59,23 @@ struct Context {
   void release();
 };
 
+// Opt-in phase timer (FASTPLS_TRACE=1): CUDA events on the context stream
+// between named marks; the sums per name are printed to stderr by report().
+class PhaseTimer {
+ public:
+  explicit PhaseTimer(const char* title);
+  ~PhaseTimer();
+  void mark(const char* name);
+  void report();
+  bool enabled() const { return on_; }
+
+ private:
+  const char* title_;
+  bool on_ = false;
+  bool reported_ = false;
+  std::vector<std::pair<const char*, cudaEvent_t>> marks_;
+};
+
 // Host <-> device copies on the context stream (synchronous w.r.t. the caller
 // once sync() is called).
 void h2d(void* dst, const void* src, size_t bytes);

@@ -149,6 +149,7 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   const int Fa = static_cast<int>(act.size());
   res.ncomp_done.assign(fs.F, 0);
   if (Fa == 0) return;
+  PhaseTimer pt("CV grid (batched)");
   // Global centring (scaling < 3): Xc = X - mean(X); folds shift by delta_f.
   const bool center = opt.scaling < 3;
   if (center) {
@@ -156,9 +157,11 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
     col_mean(X, n, p, n, mall);
     center_scale(X, n, p, n, mall, nullptr);
   }
+  pt.mark("centre");
   std::unique_ptr<XOperator> xop;
   if (opt.precision == 1) xop = make_split_operator(X, n, p);
   else xop.reset(new XOperatorF64(X, n, p));
+  pt.mark("operator");
   std::vector<uint8_t> tr((size_t)Fa * n), te((size_t)Fa * n);
   std::vector<int> grp(Fa), ntrain(Fa);
   std::vector<double> inv_nf(Fa), mYf((size_t)Fa * m), mYall(m, 0.0), dY((size_t)Fa * m);
@@ -239,11 +242,14 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
     FPLS_CHECK_LAUNCH();
   }
   b.delta = delta;
+  pt.mark("fold means");
   b.S = ar.alloc_n<double>((size_t)Fa * p * m);
   simpls_batch_crosscov(b, X, d_nt);
+  pt.mark("crosscov");
   for (auto& th : pool)
     if (th.joinable()) th.join();
   h2d(d_om, om.data(), om.size() * sizeof(double));
+  pt.mark("sketch");
   b.R = ar.alloc_n<double>((size_t)Fa * p * K);
   b.Q = ar.alloc_n<double>((size_t)Fa * m * K);
   b.V = ar.alloc_n<double>((size_t)Fa * p * K);
@@ -252,11 +258,13 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   b.ncomp_done = ar.alloc_n<int>(Fa);
   b.status = ar.alloc_n<int>(Fa);
   simpls_batch_run(b);
+  pt.mark("simpls");
   int* d_pred = ar.alloc_n<int>((size_t)fs.G * L * n);
   dzero(d_pred, (size_t)fs.G * L * n * sizeof(int));
   cv_predict_kernel<<<dim3(ceil_div(n, 128), Fa), 128, 0, ctx.stream>>>(
       Fa, n, m, K, L, d_nc, d_te, d_grp, b.Tkeep, b.tnorm, b.Q, b.ncomp_done, d_mYf, d_pred); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+  pt.mark("predict");
   std::vector<int> pred((size_t)fs.G * L * n);
   std::vector<int> done(Fa);
   d2h(pred.data(), d_pred, pred.size() * sizeof(int));
@@ -265,6 +273,8 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   for (size_t t = 0; t < pred.size(); ++t)
     if (pred[t] != 0) res.pred[t] = pred[t];
   for (int a = 0; a < Fa; ++a) res.ncomp_done[act[a]] = done[a];
+  pt.mark("d2h");
+  pt.report();
 }
 
 void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int* ncomp, int L,

@@ -3,6 +3,11 @@
 #include "simpls_engine.cuh"
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <string>
+#include <vector>
 
 namespace fpls {
 namespace {
@@ -85,36 +90,68 @@ __device__ __forceinline__ void block_sum_vec(double (&v)[NV], int count, double
   __syncthreads();
 }
 
-constexpr int NV = 16;   // register block of per-thread partial sums
+constexpr int NV = 16;      // register block of per-thread partial sums
+constexpr int kMaxChunk = 4096;  // rows of a chunk staged in shared memory
 
-// zout[f][chunk][j] = sum_{i in chunk} S_f[i,j] y[i] for every column j (blocks of
-// NV columns), or the chunk's ||y||^2 when `norm_only`.
-__device__ __forceinline__ void chunk_StY(const Eng& e, int f, int chunk, const double* Sf,
-                                          const double* yf, int b, int en, double* zout,
-                                          bool norm_only) {
-  double acc[NV];
-  if (norm_only) {
-    acc[0] = 0.0;
-    for (int i = b + threadIdx.x; i < en; i += blockDim.x) acc[0] += yf[i] * yf[i];
-    block_sum_vec<NV>(acc, 1, e.npart + (size_t)f * e.cp + chunk, 1);
+// out[j * out_stride] = sum_{r < rows} M[r + j*ld] * xs[r] for j < ncols, with xs
+// (the chunk's vector) in shared memory.  Warps take columns; when there are
+// fewer columns than warps, several warps split the rows of one column.  Each
+// lane streams consecutive rows, so every column read is coalesced.
+__device__ void chunk_dots(const double* __restrict__ M, size_t ld, int ncols,
+                           const double* xs, int rows, double* out, int out_stride) {
+  __shared__ double red[kWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (ncols >= kWarps) {
+    for (int j = warp; j < ncols; j += kWarps) {
+      const double* col = M + (size_t)j * ld;
+      double a0 = 0.0, a1 = 0.0;
+      int r = lane;
+      for (; r + 32 < rows; r += 64) {
+        a0 += col[r] * xs[r];
+        a1 += col[r + 32] * xs[r + 32];
+      }
+      if (r < rows) a0 += col[r] * xs[r];
+      const double acc = warp_sum(a0 + a1);
+      if (lane == 0) out[(size_t)j * out_stride] = acc;
+    }
     return;
   }
-  for (int j0 = 0; j0 < e.m; j0 += NV) {
-    const int cnt = min(NV, e.m - j0);
-#pragma unroll
-    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
-    for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
-      const double yi = yf[i];
-#pragma unroll
-      for (int j = 0; j < NV; ++j)
-        if (j < cnt) acc[j] += Sf[i + (size_t)(j0 + j) * e.p] * yi;
-    }
-    block_sum_vec<NV>(acc, cnt, zout + ((size_t)f * e.cp + chunk) * e.m + j0, 1);
+  const int g = kWarps / max(ncols, 1);   // warps per column
+  const int j = warp / g, sub = warp % g;
+  double acc = 0.0;
+  if (j < ncols) {
+    const double* col = M + (size_t)j * ld;
+    for (int r = sub * 32 + lane; r < rows; r += 32 * g) acc += col[r] * xs[r];
   }
+  acc = warp_sum(acc);
+  if (lane == 0) red[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x < ncols) {
+    double t = 0.0;
+    for (int u = 0; u < g; ++u) t += red[threadIdx.x * g + u];
+    out[(size_t)threadIdx.x * out_stride] = t;
+  }
+  __syncthreads();
+}
+
+// Partials of S_f^T y over the chunk (y staged in ys), or the chunk's ||y||^2.
+__device__ __forceinline__ void chunk_StY(const Eng& e, int f, int chunk, const double* Sf,
+                                          const double* ys, int b, int en, double* zout,
+                                          bool norm_only) {
+  if (norm_only) {
+    __shared__ double scratch[32];
+    double s2 = 0.0;
+    for (int r = threadIdx.x; r < en - b; r += blockDim.x) s2 += ys[r] * ys[r];
+    s2 = block_sum(s2, scratch);
+    if (threadIdx.x == 0) e.npart[(size_t)f * e.cp + chunk] = s2;
+    return;
+  }
+  chunk_dots(Sf + b, e.p, e.m, ys, en - b, zout + ((size_t)f * e.cp + chunk) * e.m, 1);
 }
 
 // First component's refresh start: y = Omega (or the single column of S).
 __global__ void k_refresh_start(Eng e) {
+  __shared__ double ys[kMaxChunk];
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   int b, en;
@@ -122,13 +159,18 @@ __global__ void k_refresh_start(Eng e) {
   const double* Sf = e.S + (size_t)f * e.p * e.m;
   const double* y0 = e.m1_mode ? Sf : e.omega + (size_t)f * e.p;
   double* yf = e.y + (size_t)f * e.p;
-  for (int i = b + threadIdx.x; i < en; i += blockDim.x) yf[i] = y0[i];
-  chunk_StY(e, f, chunk, Sf, yf, b, en, e.zA, e.iters == 0);
+  for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
+    yf[i] = y0[i];
+    ys[i - b] = y0[i];
+  }
+  __syncthreads();
+  chunk_StY(e, f, chunk, Sf, ys, b, en, e.zA, e.iters == 0);
 }
 
 // y <- S z with z = sum of the partials of S^T y; then the next partials (or ||y||^2).
 __global__ void k_refresh_apply(Eng e, const double* zin, double* zout, int last) {
   extern __shared__ double zs[];
+  __shared__ double ys[kMaxChunk];
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   int b, en;
@@ -142,8 +184,10 @@ __global__ void k_refresh_apply(Eng e, const double* zin, double* zout, int last
     double acc = 0.0;
     for (int j = 0; j < e.m; ++j) acc += Sf[i + (size_t)j * e.p] * zs[j];
     yf[i] = acc;
+    ys[i - b] = acc;
   }
-  chunk_StY(e, f, chunk, Sf, yf, b, en, zout, last != 0);
+  __syncthreads();
+  chunk_StY(e, f, chunk, Sf, ys, b, en, zout, last != 0);
 }
 
 // r = -sign(y0) y / ||y|| (Householder QR of a single column; the 1 x m core
@@ -181,6 +225,8 @@ __global__ void k_refresh_finish(Eng e) {
 // t = mask * (U - delta.rhat); partial sums of t^2, t and q = Y^T t.
 __global__ void k_scores(Eng e, int a) {
   extern __shared__ double qs[];
+  __shared__ double ts[kMaxChunk];
+  __shared__ double scratch[32];
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   int b, en;
@@ -194,35 +240,29 @@ __global__ void k_scores(Eng e, int a) {
     for (int j = threadIdx.x; j < e.m; j += blockDim.x) qs[j] = 0.0;
     __syncthreads();
   }
-  double acc[NV];
-  acc[0] = acc[1] = 0.0;
+  double s2 = 0.0, s1 = 0.0;
   for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
     const double u = Uf[i] - c;
     const double t = (mk && !mk[i]) ? 0.0 : u;
     Tf[i] = t;
+    ts[i - b] = t;
     if (keep) keep[i] = u;
-    acc[0] += t * t;
-    acc[1] += t;
+    s2 += t * t;
+    s1 += t;
     if (e.labels && t != 0.0) atomicAdd(&qs[e.labels[i]], t);
   }
-  block_sum_vec<NV>(acc, 2, e.tpart + ((size_t)f * e.cn + chunk) * 2, 1);
+  s2 = block_sum(s2, scratch);
+  s1 = block_sum(s1, scratch);
+  if (threadIdx.x == 0) {
+    e.tpart[((size_t)f * e.cn + chunk) * 2 + 0] = s2;
+    e.tpart[((size_t)f * e.cn + chunk) * 2 + 1] = s1;
+  }
   double* qp = e.qpart + ((size_t)f * e.cn + chunk) * e.m;
   if (e.labels) {
     for (int j = threadIdx.x; j < e.m; j += blockDim.x) qp[j] = qs[j];
     return;
   }
-  for (int j0 = 0; j0 < e.m; j0 += NV) {
-    const int cnt = min(NV, e.m - j0);
-#pragma unroll
-    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
-    for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
-      const double t = Tf[i];
-#pragma unroll
-      for (int j = 0; j < NV; ++j)
-        if (j < cnt) acc[j] += t * e.Yg[i + (size_t)(j0 + j) * e.n];
-    }
-    block_sum_vec<NV>(acc, cnt, qp + j0, 1);
-  }
+  chunk_dots(e.Yg + b, e.n, e.m, ts, en - b, qp, 1);
 }
 
 __device__ __forceinline__ void t_stats(const Eng& e, int f, double& tn, double& st) {
@@ -236,10 +276,9 @@ __device__ __forceinline__ void t_stats(const Eng& e, int f, double& tn, double&
   st = s1;
 }
 
-constexpr int KV = 32;   // register block of Gram-Schmidt dot products
-
-// p = colscale * (P - delta * sum(t)) / ||t||; partial w = V^T p (blocks of KV loadings).
+// p = colscale * (P - delta * sum(t)) / ||t||; partial w = V^T p.
 __global__ void k_loading(Eng e, int a) {
+  __shared__ double ps[kMaxChunk];
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   double tn, st;
@@ -254,31 +293,25 @@ __global__ void k_loading(Eng e, int a) {
   const double* dl = e.delta ? e.delta + (size_t)f * e.p : nullptr;
   const double* Pf = e.P + (size_t)f * e.p;
   double* pf = e.pv + (size_t)f * e.p;
-  const double* Vf = e.V + (size_t)f * e.p * e.K;
   for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
     double v = Pf[i];
     if (dl) v -= dl[i] * st;
     if (sc) v *= sc[i];
-    pf[i] = v / tn;
+    v /= tn;
+    pf[i] = v;
+    ps[i - b] = v;
   }
-  double acc[KV];
-  for (int l0 = 0; l0 < a; l0 += KV) {
-    const int cnt = min(KV, a - l0);
-#pragma unroll
-    for (int l = 0; l < KV; ++l) acc[l] = 0.0;
-    for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
-      const double v = pf[i];
-#pragma unroll
-      for (int l = 0; l < KV; ++l)
-        if (l < cnt) acc[l] += Vf[i + (size_t)(l0 + l) * e.p] * v;
-    }
-    block_sum_vec<KV>(acc, cnt, e.wpart + ((size_t)f * e.cp + chunk) * e.K + l0, 1);
-  }
+  __syncthreads();
+  if (a > 0)
+    chunk_dots(e.V + (size_t)f * e.p * e.K + b, e.p, a, ps, en - b,
+               e.wpart + ((size_t)f * e.cp + chunk) * e.K, 1);
 }
 
 // v = p - V (V^T p); partials of ||v||^2 and of S^T v.
 __global__ void k_orth(Eng e, int a) {
   extern __shared__ double ws[];
+  __shared__ double vsh[kMaxChunk];
+  __shared__ double scratch[32];
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   int b, en;
@@ -288,10 +321,8 @@ __global__ void k_orth(Eng e, int a) {
   __syncthreads();
   const double* Vf = e.V + (size_t)f * e.p * e.K;
   const double* pf = e.pv + (size_t)f * e.p;
-  const double* Sf = e.S + (size_t)f * e.p * e.m;
   double* vf = e.v + (size_t)f * e.p;
-  double acc[NV];
-  acc[0] = 0.0;
+  double s2 = 0.0;
   for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
     double x = pf[i];
     int l = 0;
@@ -302,22 +333,14 @@ __global__ void k_orth(Eng e, int a) {
     }
     for (; l < a; ++l) x -= Vf[i + (size_t)l * e.p] * ws[l];
     vf[i] = x;
-    acc[0] += x * x;
+    vsh[i - b] = x;
+    s2 += x * x;
   }
-  block_sum_vec<NV>(acc, 1, e.vpart + (size_t)f * e.cp + chunk, 1);
-  // S^T v (unnormalised) for the deflation, blocks of NV columns.
-  for (int j0 = 0; j0 < e.m; j0 += NV) {
-    const int cnt = min(NV, e.m - j0);
-#pragma unroll
-    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
-    for (int i = b + threadIdx.x; i < en; i += blockDim.x) {
-      const double x = vf[i];
-#pragma unroll
-      for (int j = 0; j < NV; ++j)
-        if (j < cnt) acc[j] += x * Sf[i + (size_t)(j0 + j) * e.p];
-    }
-    block_sum_vec<NV>(acc, cnt, e.vSpart + ((size_t)f * e.cp + chunk) * e.m + j0, 1);
-  }
+  s2 = block_sum(s2, scratch);
+  if (threadIdx.x == 0) e.vpart[(size_t)f * e.cp + chunk] = s2;
+  // S^T v (unnormalised) for the deflation.
+  chunk_dots(e.S + (size_t)f * e.p * e.m + b, e.p, e.m, vsh, en - b,
+             e.vSpart + ((size_t)f * e.cp + chunk) * e.m, 1);
 }
 
 // v /= ||v||; V[:, a] = v; S -= v (v^T S); R[:, a] = r / ||t||; Q[:, a] = q / ||t||;
@@ -325,6 +348,7 @@ __global__ void k_orth(Eng e, int a) {
 // deflated S, or ||S[:,0]||^2 when m == 1).
 __global__ void k_deflate(Eng e, int a, int next) {
   extern __shared__ double vs[];
+  __shared__ double ysh[kMaxChunk];
   const int f = blockIdx.y, chunk = blockIdx.x;
   if (e.status[f]) return;
   const double vn = sqrt(sum_parts(e.vpart + (size_t)f * e.cp, e.cp, 1));
@@ -352,7 +376,11 @@ __global__ void k_deflate(Eng e, int a, int next) {
     for (int j = 0; j < e.m; ++j) Sf[i + (size_t)j * e.p] -= vi * vs[j];
     const double ri = rf[i] / tn;
     Rcol[i] = ri;
-    if (next) yf[i] = e.m1_mode ? Sf[i] : ri;
+    if (next) {
+      const double y0 = e.m1_mode ? Sf[i] : ri;
+      yf[i] = y0;
+      ysh[i - b] = y0;
+    }
   }
   if (chunk == 0) {
     double* Qcol = e.Q + ((size_t)f * e.K + a) * e.m;
@@ -369,7 +397,10 @@ __global__ void k_deflate(Eng e, int a, int next) {
       e.ncomp_done[f] = a + 1;
     }
   }
-  if (next) chunk_StY(e, f, chunk, Sf, yf, b, en, e.zA, e.iters == 0);
+  if (next) {
+    __syncthreads();
+    chunk_StY(e, f, chunk, Sf, ysh, b, en, e.zA, e.iters == 0);
+  }
 }
 
 __global__ void k_masked_response(Eng e, double* M) {
@@ -410,9 +441,11 @@ Eng make_eng(const SimplsBatch& b) {
   e.n = b.n; e.p = b.p; e.m = b.m; e.F = b.F; e.K = b.K;
   const int target = 4 * Context::get().sm_count;
   e.cp = std::max(1, std::min(ceil_div(target, b.F), ceil_div(b.p, 256)));
+  e.cp = std::max(e.cp, ceil_div(b.p, kMaxChunk));
   e.szp = ceil_div(b.p, e.cp);
   e.cp = ceil_div(b.p, e.szp);
   e.cn = std::max(1, std::min(ceil_div(target, b.F), ceil_div(b.n, 256)));
+  e.cn = std::max(e.cn, ceil_div(b.n, kMaxChunk));
   e.szn = ceil_div(b.n, e.cn);
   e.cn = ceil_div(b.n, e.szn);
   e.Yg = b.Yg; e.labels = b.labels; e.mY_all = b.mY_all; e.mask = b.mask; e.delta = b.delta;
@@ -479,6 +512,18 @@ void simpls_batch_run(const SimplsBatch& b) {
   const size_t sm_m = std::max<size_t>(b.m, 1) * sizeof(double);
   const size_t sm_k = std::max<size_t>(b.K, 1) * sizeof(double);
   cudaStream_t st = ctx.stream;
+  // Optional per-phase device timing (FASTPLS_TRACE=1), printed to stderr.
+  const char* trace_env = std::getenv("FASTPLS_TRACE");
+  const bool trace = trace_env && trace_env[0] == '1';
+  std::vector<std::pair<const char*, cudaEvent_t>> marks;
+  auto mark = [&](const char* name) {
+    if (!trace) return;
+    cudaEvent_t ev;
+    FPLS_CUDA(cudaEventCreate(&ev));
+    FPLS_CUDA(cudaEventRecord(ev, st));
+    marks.emplace_back(name, ev);
+  };
+  mark("start");
   k_refresh_start<<<gp, kThreads, 0, st>>>(e); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   for (int a = 0; a < b.K; ++a) {
@@ -493,16 +538,38 @@ void simpls_batch_run(const SimplsBatch& b) {
     }
     k_refresh_finish<<<gp, kThreads, 0, st>>>(e); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    mark("refresh");
     b.X->times(e.Rhat, b.F, e.U);
+    mark("X*R");
     k_scores<<<gn, kThreads, b.labels ? sm_m : 0, st>>>(e, a); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    mark("scores");
     b.X->t_times(e.T, b.F, e.P);
+    mark("X^T*T");
     k_loading<<<gp, kThreads, 0, st>>>(e, a); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    mark("loading");
     k_orth<<<gp, kThreads, sm_k, st>>>(e, a); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    mark("orth");
     k_deflate<<<gp, kThreads, sm_m, st>>>(e, a, a + 1 < b.K ? 1 : 0); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    mark("deflate");
+  }
+  if (trace) {
+    FPLS_CUDA(cudaStreamSynchronize(st));
+    std::map<std::string, double> acc;
+    for (size_t k = 1; k < marks.size(); ++k) {
+      float ms = 0.f;
+      FPLS_CUDA(cudaEventElapsedTime(&ms, marks[k - 1].second, marks[k].second));
+      acc[marks[k].first] += ms;
+    }
+    double total = 0.0;
+    for (auto& kv : acc) total += kv.second;
+    std::fprintf(stderr, "[fastpls trace] SIMPLS engine F=%d n=%d p=%d m=%d K=%d: %.3f ms\n", b.F, b.n,
+                 b.p, b.m, b.K, total);
+    for (auto& kv : acc) std::fprintf(stderr, "  %-10s %8.3f ms\n", kv.first.c_str(), kv.second);
+    for (auto& mk : marks) cudaEventDestroy(mk.second);
   }
 }
 

@@ -92,6 +92,18 @@ double* centered_test_copy(const double* Xh, int w, int p, const double* mX_d, c
   return X;
 }
 
+// outer_pred[i] = prediction of the refit of i's outer fold at the chosen slice
+// (or the single-class fallback).
+__global__ void gather_outer_pred_kernel(const int* __restrict__ pred, const int* __restrict__ outer,
+                                         const int* __restrict__ best_slice, const int* __restrict__ fb,
+                                         int Ko, int L, int n, int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int o = outer[i];
+  if (o < 0 || o >= Ko) { out[i] = 0; return; }
+  out[i] = fb[o] ? fb[o] : pred[((size_t)Ko * L + best_slice[o]) * n + i];
+}
+
 void lda_outputs_to_host(const LdaModelsDev& d, int C, int kmax, int L, double* means,
                          double* linear, double* constants, double* priors) {
   download(means, d.means, (size_t)C * kmax * L);
@@ -659,7 +671,8 @@ int fpls_cv_predict(const void* X, int x_is_float32, int n, int p, const int* y,
     for (int& c : nc) c = std::max(1, c);
     CvGridResult res;
     run_cv_grid(fs, X, x_is_float32, false, y, nc.data(), L, scaling, precision, batched, res);
-    std::copy(res.pred.begin(), res.pred.end(), class_pred);
+    download(class_pred, res.d_pred, (size_t)n * L);
+    ctx.sync();
     if (status) std::copy(res.status.begin(), res.status.end(), status);
   });
 }
@@ -718,32 +731,36 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     }
     CvGridResult res;
     run_cv_grid(fs, X, x_is_float32, x_on_device, y, nc.data(), L, scaling, precision, batched, res);
-    // Inner accuracy per (outer fold, ncomp) and the chosen ncomp (first maximum).
+    // Inner accuracy per (outer fold, ncomp) on the device; the chosen ncomp is the
+    // first maximum (.cv_best_index); only counts and the outer predictions return.
+    const int* d_y = upload(y, n);
+    const int* d_outer = upload(outer_fold, n);
+    std::vector<long long> cnts;
+    cv_prediction_counts(res.d_pred, Ko, L, n, d_y, d_outer, cnts);
+    std::vector<int> best_slice(Ko, 0), fb(Ko, 0);
     for (int o = 0; o < Ko; ++o) {
       int bi = 0;
       double bv = -1.0;
       bool any = false;
       for (int s = 0; s < L; ++s) {
-        long long ok = 0, tot = 0;
-        const int* pr = res.pred.data() + ((size_t)o * L + s) * n;
-        for (int i = 0; i < n; ++i) {
-          if (outer_fold[i] == o || pr[i] < 1) continue;
-          ++tot;
-          ok += (pr[i] == y[i]);
-        }
+        const long long ok = cnts[2 * ((size_t)o * L + s)], tot = cnts[2 * ((size_t)o * L + s) + 1];
         const double acc = tot ? static_cast<double>(ok) / tot : std::nan("");
         if (inner_accuracy) inner_accuracy[o + (size_t)s * Ko] = acc;
         if (std::isfinite(acc) && (!any || acc > bv)) { bv = acc; bi = s; any = true; }
       }
       const bool skip = outer_classes[o] < 2;
-      int bc = skip ? *std::min_element(nc.begin(), nc.end()) : nc[bi];
-      if (best_comp) best_comp[o] = bc;
-      for (int i = 0; i < n; ++i) {
-        if (outer_fold[i] != o) continue;
-        outer_pred[i] = skip ? fallback[o] : res.pred[((size_t)Ko * L + bi) * n + i];
-      }
+      best_slice[o] = bi;
+      fb[o] = skip ? fallback[o] : 0;
+      if (best_comp) best_comp[o] = skip ? *std::min_element(nc.begin(), nc.end()) : nc[bi];
     }
-    if (inner_pred) std::copy(res.pred.begin(), res.pred.begin() + (size_t)Ko * L * n, inner_pred);
+    int* d_best = upload(best_slice.data(), Ko);
+    int* d_fb = upload(fb.data(), Ko);
+    int* d_out = ctx.arena.alloc_n<int>(n);
+    gather_outer_pred_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(res.d_pred, d_outer, d_best, d_fb, Ko, L, n, d_out); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    download(outer_pred, d_out, n);
+    if (inner_pred) download(inner_pred, res.d_pred, (size_t)Ko * L * n);
+    ctx.sync();
     if (fit_status) std::copy(res.status.begin(), res.status.end(), fit_status);
     }
 }

@@ -59,6 +59,70 @@ __global__ void onehot_kernel(const int* __restrict__ lab0, int cnt, int m, doub
   }
 }
 
+// Scatters the class labels of one fit's test rows into the prediction grid.
+__global__ void scatter_pred_kernel(const int* __restrict__ lab, int nt, int L, const int* __restrict__ rows,
+                                    int n, int g, int* __restrict__ pred) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt * L) return;
+  const int r = t % nt, s = t / nt;
+  pred[((size_t)g * L + s) * n + rows[r]] = lab[t];
+}
+
+__global__ void pred_counts_kernel(const int* __restrict__ pred, int L, int n, const int* __restrict__ y,
+                                   const int* __restrict__ exclude, long long* __restrict__ counts) {
+  __shared__ double scratch[32];
+  const int gs = blockIdx.x;          // g * L + s
+  const int g = gs / L;
+  const int* pr = pred + (size_t)gs * n;
+  double ok = 0.0, tot = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (exclude && exclude[i] == g) continue;
+    const int v = pr[i];
+    if (v < 1) continue;
+    tot += 1.0;
+    ok += (v == y[i]) ? 1.0 : 0.0;
+  }
+  ok = block_sum(ok, scratch);
+  tot = block_sum(tot, scratch);
+  if (threadIdx.x == 0) {
+    counts[2 * (size_t)gs] = static_cast<long long>(ok);
+    counts[2 * (size_t)gs + 1] = static_cast<long long>(tot);
+  }
+}
+
+// Draws the per-fit Gaussian sketches (libstdc++ mt19937 streams, one per
+// seed) on host threads while the device runs the grid's set-up.
+class SketchPool {
+ public:
+  ~SketchPool() { join(); }
+  void start(const std::vector<unsigned>& seeds, int p) {
+    om_.assign(seeds.size() * (size_t)p, 0.0);
+    const int F = static_cast<int>(seeds.size());
+    const int nt = std::max(1, std::min<int>(F, static_cast<int>(std::thread::hardware_concurrency())));
+    double* out = om_.data();
+    const std::vector<unsigned>* sd = &seeds_;
+    seeds_ = seeds;
+    for (int t = 0; t < nt; ++t)
+      th_.emplace_back([out, sd, p, F, nt, t] {
+        for (int a = t; a < F; a += nt) host_gaussian(out + (size_t)a * p, p, (*sd)[a]);
+      });
+  }
+  const std::vector<double>& wait() {
+    join();
+    return om_;
+  }
+
+ private:
+  void join() {
+    for (auto& t : th_)
+      if (t.joinable()) t.join();
+    th_.clear();
+  }
+  std::vector<double> om_;
+  std::vector<unsigned> seeds_;
+  std::vector<std::thread> th_;
+};
+
 // Class predictions of the test rows of every fit for every ncomp slice from the
 // kept scores: y_a = sum_{b<=a} (t_b[i] / ||t_b||) q_b + mY_f, label = first argmax.
 __global__ void cv_predict_kernel(int F, int n, int m, int K, int L, const int* __restrict__ ncomp,
@@ -136,7 +200,7 @@ void fill_special_predictions(const CvFitSet& fs, const int* y, const std::vecto
 
 void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, int L,
                  const CvGridOptions& opt, const std::vector<int>& status,
-                 const std::vector<double>& counts, CvGridResult& res) {
+                 const std::vector<double>& counts, SketchPool& sketches, CvGridResult& res) {
   Context& ctx = Context::get();
   Arena& ar = ctx.arena;
   const int n = fs.n, p = fs.p, m = fs.m;
@@ -166,24 +230,7 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   std::vector<int> grp(Fa), ntrain(Fa);
   std::vector<double> inv_nf(Fa), mYf((size_t)Fa * m), mYall(m, 0.0), dY((size_t)Fa * m);
   for (int i = 0; i < n; ++i) mYall[y[i] - 1] += 1.0 / n;
-  // The per-fit Gaussian sketches (libstdc++ mt19937 streams, one per seed) are
-  // drawn on host threads while the device runs the set-up below.
-  std::vector<double> om((size_t)Fa * p);
-  std::vector<std::thread> pool;
-  struct Joiner {
-    std::vector<std::thread>& v;
-    ~Joiner() {
-      for (auto& t : v)
-        if (t.joinable()) t.join();
-    }
-  } joiner{pool};
-  {
-    const int nt = std::max(1, std::min<int>(Fa, static_cast<int>(std::thread::hardware_concurrency())));
-    for (int t = 0; t < nt; ++t)
-      pool.emplace_back([&om, &fs, &act, p, Fa, nt, t] {
-        for (int a = t; a < Fa; a += nt) host_gaussian(om.data() + (size_t)a * p, p, fs.seeds[act[a]]);
-      });
-  }
+  const size_t om_size = (size_t)Fa * p;
   for (int a = 0; a < Fa; ++a) {
     const int f = act[a];
     std::copy(fs.train.begin() + (size_t)f * n, fs.train.begin() + (size_t)(f + 1) * n, tr.begin() + (size_t)a * n);
@@ -206,7 +253,7 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   double* d_mYf = ar.alloc_n<double>(mYf.size());
   double* d_mYall = ar.alloc_n<double>(m);
   double* d_dY = ar.alloc_n<double>(dY.size());
-  double* d_om = ar.alloc_n<double>(om.size());
+  double* d_om = ar.alloc_n<double>(om_size);
   int* d_lab = ar.alloc_n<int>(n);
   int* d_nc = ar.alloc_n<int>(L);
   std::vector<int> lab0(n);
@@ -246,9 +293,8 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   b.S = ar.alloc_n<double>((size_t)Fa * p * m);
   simpls_batch_crosscov(b, X, d_nt);
   pt.mark("crosscov");
-  for (auto& th : pool)
-    if (th.joinable()) th.join();
-  h2d(d_om, om.data(), om.size() * sizeof(double));
+  const std::vector<double>& om = sketches.wait();
+  h2d(d_om, om.data(), om_size * sizeof(double));
   pt.mark("sketch");
   b.R = ar.alloc_n<double>((size_t)Fa * p * K);
   b.Q = ar.alloc_n<double>((size_t)Fa * m * K);
@@ -259,19 +305,14 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   b.status = ar.alloc_n<int>(Fa);
   simpls_batch_run(b);
   pt.mark("simpls");
-  int* d_pred = ar.alloc_n<int>((size_t)fs.G * L * n);
-  dzero(d_pred, (size_t)fs.G * L * n * sizeof(int));
+  int* d_pred = res.d_pred;
   cv_predict_kernel<<<dim3(ceil_div(n, 128), Fa), 128, 0, ctx.stream>>>(
       Fa, n, m, K, L, d_nc, d_te, d_grp, b.Tkeep, b.tnorm, b.Q, b.ncomp_done, d_mYf, d_pred); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   pt.mark("predict");
-  std::vector<int> pred((size_t)fs.G * L * n);
   std::vector<int> done(Fa);
-  d2h(pred.data(), d_pred, pred.size() * sizeof(int));
   d2h(done.data(), b.ncomp_done, Fa * sizeof(int));
   ctx.sync();
-  for (size_t t = 0; t < pred.size(); ++t)
-    if (pred[t] != 0) res.pred[t] = pred[t];
   for (int a = 0; a < Fa; ++a) res.ncomp_done[act[a]] = done[a];
   pt.mark("d2h");
   pt.report();
@@ -306,7 +347,7 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
   double* Yp = ar.alloc_n<double>((size_t)n * m * L);
   int* lab = ar.alloc_n<int>((size_t)n * L);
   std::vector<double> omh(p), Wh((size_t)K * m * L), Qh((size_t)m * K);
-  std::vector<int> rows, trows, labs, labh((size_t)n * L);
+  std::vector<int> rows, trows, labs;
   for (int f = 0; f < fs.F; ++f) {
     if (status[f] != 1) continue;
     rows.clear();
@@ -355,11 +396,8 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
     center_scale(Xt, nt, p, nt, mX, opt.scaling == 2 ? vX : nullptr);
     lowrank_predict(Xt, nt, p, R, K, W, m, ncomp, L, mY, T, Yp);
     for (int s = 0; s < L; ++s) row_argmax(Yp + (size_t)s * nt * m, nt, m, nullptr, lab + (size_t)s * nt);
-    d2h(labh.data(), lab, (size_t)nt * L * sizeof(int));
-    ctx.sync();
-    const int g = fs.group[f];
-    for (int s = 0; s < L; ++s)
-      for (int r = 0; r < nt; ++r) res.pred[((size_t)g * L + s) * n + trows[r]] = labh[(size_t)s * nt + r];
+    scatter_pred_kernel<<<ceil_div((long long)nt * L, 256), 256, 0, ctx.stream>>>(lab, nt, L, d_idx, n, fs.group[f], res.d_pred); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
   }
 }
 
@@ -378,8 +416,27 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
   std::vector<double> counts;
   classify_fits(fs, labels_host, status, fallback, counts);
   res.status = status;
-  res.pred.assign((size_t)fs.G * L * fs.n, 0);
-  fill_special_predictions(fs, labels_host, status, fallback, L, res.pred);
+  const bool batched = opt.batched && opt.scaling != 2;
+  // Start the host-side sketches first so they overlap every device step below.
+  SketchPool sketches;
+  if (batched) {
+    std::vector<unsigned> seeds;
+    for (int f = 0; f < fs.F; ++f)
+      if (status[f] == 1) seeds.push_back(fs.seeds[f]);
+    sketches.start(seeds, fs.p);
+  }
+  const size_t npred = (size_t)fs.G * L * fs.n;
+  res.d_pred = ctx.arena.alloc_n<int>(npred);
+  bool special = false;
+  for (int f = 0; f < fs.F; ++f) special |= (status[f] == 3 || status[f] == 4);
+  if (special) {
+    std::vector<int> pred(npred, 0);
+    fill_special_predictions(fs, labels_host, status, fallback, L, pred);
+    h2d(res.d_pred, pred.data(), npred * sizeof(int));
+    ctx.sync();
+  } else {
+    dzero(res.d_pred, npred * sizeof(int));
+  }
   // Working FP64 copy of X (the batched path centres it in place).
   double* X = ctx.arena.alloc_n<double>((size_t)fs.n * fs.p);
   if (x64) {
@@ -388,9 +445,19 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
     widen_f32_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(x32, X, (size_t)fs.n * fs.p); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
-  const bool batched = opt.batched && opt.scaling != 2;
-  if (batched) run_batched(fs, X, labels_host, ncomp, L, opt, status, counts, res);
+  if (batched) run_batched(fs, X, labels_host, ncomp, L, opt, status, counts, sketches, res);
   else run_sequential(fs, X, labels_host, ncomp, L, opt, status, res);
+}
+
+void cv_prediction_counts(const int* d_pred, int G, int L, int n, const int* d_labels,
+                          const int* d_exclude, std::vector<long long>& counts) {
+  Context& ctx = Context::get();
+  long long* d_counts = ctx.arena.alloc_n<long long>(2 * (size_t)G * L);
+  pred_counts_kernel<<<G * L, 256, 0, ctx.stream>>>(d_pred, L, n, d_labels, d_exclude, d_counts); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  counts.assign(2 * (size_t)G * L, 0);
+  d2h(counts.data(), d_counts, counts.size() * sizeof(long long));
+  ctx.sync();
 }
 
 }  // namespace fpls

@@ -60,6 +60,12 @@ SIGNATURES = {
                         _I, _I, _I, _IP, _DP, _IP, _IP, _IP, _C, _S], ctypes.c_int),
     "fpls_bf16x3_gemm_noalloc": ([ctypes.c_void_p, _I, _I, ctypes.c_void_p, _I, ctypes.c_void_p,
                                   _C, _S], ctypes.c_int),
+    "fpls_gaussian_y_encode": ([_DP, _I, _I, _DP, _I, _DP, _DP, _DP, _C, _S], ctypes.c_int),
+    "fpls_gaussian_y_decode": ([_DP, _I, _I, _DP, _DP, _I, _DP, _C, _S], ctypes.c_int),
+    "fpls_nearest_code_classes": ([_DP, _I, _I, _DP, _I, _IP, _C, _S], ctypes.c_int),
+    "fpls_opls_filter": ([_DP, _I, _I, _DP, _I, _I, _I, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S],
+                         ctypes.c_int),
+    "fpls_opls_apply_filter": ([_DP, _I, _I, _DP, _DP, _DP, _DP, _I, _DP, _C, _S], ctypes.c_int),
     "fpls_x_upload": ([ctypes.c_void_p, _I, _I, _I, _IP, _C, _S], ctypes.c_int),
     "fpls_x_free": ([_I, _C, _S], ctypes.c_int),
     "fpls_double_cv_resident": ([_I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I, _I, _I, _I,
@@ -494,3 +500,58 @@ def profile_end():
     by = ctypes.c_double(0.0)
     _call("fpls_profile", 0, ctypes.byref(ms), ctypes.byref(cnt), ctypes.byref(by))
     return dict(ms=ms.value, launches=cnt.value, bytes=by.value)
+
+
+def gaussian_y_encode(Y, projection):
+    """Regression response compression (R/main.R:2000-2064); projection q x d."""
+    Y = _f64(Y)
+    G = _f64(projection)
+    n, q = Y.shape
+    d = G.shape[1]
+    Z, mu, dec = _out(n, d), np.zeros(q), _out(d, q)
+    _call("fpls_gaussian_y_encode", _p(Y), n, q, _p(G), d, _p(Z), _p(mu), _p(dec))
+    return dict(Z=Z, y_center=mu, decoder=dec)
+
+
+def gaussian_y_decode(Z, decoder, y_center):
+    Z = _f64(Z)
+    D = _f64(decoder)
+    mu = np.ascontiguousarray(y_center, dtype=np.float64).ravel()
+    w, d = Z.shape
+    q = D.shape[1]
+    Y = _out(w, q)
+    _call("fpls_gaussian_y_decode", _p(Z), w, d, _p(D), _p(mu), q, _p(Y))
+    return Y
+
+
+def nearest_code_classes(Z, codes):
+    Z = _f64(Z)
+    C = _f64(codes)
+    lab = np.zeros(Z.shape[0], dtype=np.int32)
+    _call("fpls_nearest_code_classes", _p(Z), Z.shape[0], Z.shape[1], _p(C), C.shape[0], _p(lab))
+    return lab
+
+
+def opls_filter(X, Y, north, scaling=1):
+    X = _f64(X)
+    Y = _f64(Y)
+    n, p = X.shape
+    q = Y.shape[1]
+    Xf, mX, vX = _out(n, p), np.zeros(p), np.zeros(p)
+    W, P = _out(p, max(north, 1)), _out(p, max(north, 1))
+    used = ctypes.c_int(0)
+    _call("fpls_opls_filter", _p(X), n, p, _p(Y), q, int(north), int(scaling), _p(Xf), _p(mX),
+          _p(vX), _p(W), _p(P), ctypes.byref(used))
+    k = used.value
+    return dict(X=Xf, mX=mX, vX=vX, W_orth=W[:, :k], P_orth=P[:, :k], north=k)
+
+
+def opls_apply_filter(X, mX, vX, W_orth, P_orth):
+    X = _f64(X)
+    w, p = X.shape
+    W = _f64(W_orth)
+    P = _f64(P_orth)
+    out = _out(w, p)
+    _call("fpls_opls_apply_filter", _p(X), w, p, _p(np.ascontiguousarray(mX, dtype=np.float64).ravel()),
+          _p(np.ascontiguousarray(vX, dtype=np.float64).ravel()), _p(W), _p(P), W.shape[1], _p(out))
+    return out

@@ -198,6 +198,40 @@ int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, 
                    int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
                    int* inner_pred, int* fit_status, char* err, size_t errlen);
 
+/* Gaussian response compression, regression branch: Yc = Y - colMeans(Y),
+ * Z = Yc * projection (projection q x d is drawn by the caller, as R draws it
+ * with rnorm), decoder = (ZᵀZ + 1e-8·mean(diag(ZᵀZ)) I)⁻¹ ZᵀYc.
+ * Outputs Z n x d, y_center q, decoder d x q.  Replaces the cuda_matrix_multiply
+ * calls of .prepare_gaussian_y / .gaussian_y_ridge_decoder (R/main.R:1968-2064;
+ * _fastPLS_cuda_matrix_multiply, RcppExports.cpp:116). */
+int fpls_gaussian_y_encode(const double* Y, int n, int q, const double* projection, int d, double* Z,
+                           double* y_center, double* decoder, char* err, size_t errlen);
+
+/* Y (w x q) = Z (w x d) * decoder + y_center: .decode_gaussian_y_matrix
+ * (R/main.R:2085-2104). */
+int fpls_gaussian_y_decode(const double* Z, int w, int d, const double* decoder,
+                           const double* y_center, int q, double* Y, char* err, size_t errlen);
+
+/* labels[i] = 1 + argmax_c (2 z_i·code_c − ‖code_c‖²) for class codes
+ * (n_classes x d): nearest_code_classes (fastPLS.cpp:4203-4215). */
+int fpls_nearest_code_classes(const double* Z, int w, int d, const double* codes, int n_classes,
+                              int* labels, char* err, size_t errlen);
+
+/* OPLS orthogonal filter: centre (scale), then per orthogonal component
+ * w = u1(XᵀY), t = Xw, p = Xᵀt/tᵀt, w_o = p − w(wᵀp)/(wᵀw) normalised,
+ * t_o = Xw_o, p_o = Xᵀt_o/t_oᵀt_o, X −= t_o p_oᵀ.  Outputs the filtered X
+ * (n x p), mX, vX, W_orth and P_orth (p x north, first *used columns).
+ * Replaces _fastPLS_opls_filter_cpp (RcppExports.cpp:523; fastPLS.cpp:4377-4460). */
+int fpls_opls_filter(const double* X, int n, int p, const double* Y, int q, int north, int scaling,
+                     double* Xf, double* mX, double* vX, double* W_orth, double* P_orth, int* used,
+                     char* err, size_t errlen);
+
+/* Applies a fitted OPLS filter to new rows (w x p).  Replaces
+ * _fastPLS_opls_apply_filter_cpp (RcppExports.cpp:537; fastPLS.cpp:4463-4483). */
+int fpls_opls_apply_filter(const double* X, int w, int p, const double* mX, const double* vX,
+                           const double* W_orth, const double* P_orth, int north, double* Xf,
+                           char* err, size_t errlen);
+
 /* C (M x N) = A (M x K) * B (K x N) through the BF16 split tensor-core kernel,
  * for callers that cannot allocate device memory (a host that runs inside
  * another runtime's fixed memory pool, a stream callback, an allocation-free

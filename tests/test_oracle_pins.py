@@ -146,3 +146,42 @@ def test_oracle_golden_fixtures():
             if k.startswith("in_"):
                 continue
             assert np.allclose(got[k], v, rtol=1e-10, atol=1e-12), (name, k)
+
+
+def test_gaussian_y_identities():
+    # tests/testthat/test-gaussian-y.R: decoded predictions keep Y's shape and are
+    # finite; the decoder solves the ridge normal equations of R/main.R:1968-1981.
+    from oracle import gaussian_y as og
+    rng = np.random.default_rng(120)
+    Y = rng.standard_normal((70, 24))
+    G = rng.standard_normal((24, 7)) / np.sqrt(7)
+    enc = og.prepare_regression(Y, G)
+    Z, D = enc["Z"], enc["decoder"]
+    assert Z.shape == (70, 7) and D.shape == (7, 24)
+    ztz = Z.T @ Z
+    lhs = (ztz + 1e-8 * np.mean(np.diag(ztz)) * np.eye(7)) @ D
+    assert np.allclose(lhs, Z.T @ (Y - Y.mean(axis=0)), rtol=1e-10, atol=1e-10)
+    out = og.decode_regression(Z[:9], D, enc["y_center"])
+    assert out.shape == (9, 24) and np.all(np.isfinite(out))
+    # class codes: centred columns, unit rows; a code decodes to its own class
+    codes = og.class_codes(rng.standard_normal((6, 5)) / np.sqrt(5))
+    assert np.allclose(np.linalg.norm(codes, axis=1), 1.0)
+    assert np.array_equal(og.nearest_code_classes(codes, codes), np.arange(1, 7))
+
+
+def test_opls_filter_identities():
+    # Each removed orthogonal score is orthogonal to the filtered X, weights are
+    # unit vectors, and applying the stored filter to the training rows
+    # reproduces the filtered training matrix (src/fastPLS.cpp:4377-4483).
+    from oracle import opls as oo
+    rng = np.random.default_rng(7)
+    X = rng.standard_normal((60, 20)) + rng.standard_normal((60, 1)) * rng.standard_normal(20)
+    Y = X[:, :3] @ rng.standard_normal((3, 2)) + 0.1 * rng.standard_normal((60, 2))
+    for scaling in (1, 2, 3):
+        f = oo.opls_filter(X, Y, 3, scaling=scaling)
+        assert f["north"] == 3
+        assert np.allclose(np.linalg.norm(f["W_orth"], axis=0), 1.0)
+        again = oo.opls_apply_filter(X, f["mX"], f["vX"], f["W_orth"], f["P_orth"])
+        assert np.allclose(again, f["X"], atol=1e-10)
+    f0 = oo.opls_filter(X, Y, 0)
+    assert f0["north"] == 0 and f0["W_orth"].shape == (20, 0)

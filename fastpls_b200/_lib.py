@@ -65,6 +65,10 @@ SIGNATURES = {
     "fpls_nearest_code_classes": ([_DP, _I, _I, _DP, _I, _IP, _C, _S], ctypes.c_int),
     "fpls_opls_filter": ([_DP, _I, _I, _DP, _I, _I, _I, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S],
                          ctypes.c_int),
+    "fpls_candidate_scores": ([_DP, _I, _I, _DP, _DP, _C, _S], ctypes.c_int),
+    "fpls_candidate_centroids": ([_DP, _I, _I, _IP, _I, _DP, _C, _S], ctypes.c_int),
+    "fpls_candidate_knn_predict": ([_DP, _I, _DP, _I, _I, _IP, _DP, _I, _DP, _I, _I, _I, _D, _D,
+                                    _IP, _DP, _C, _S], ctypes.c_int),
     "fpls_opls_apply_filter": ([_DP, _I, _I, _DP, _DP, _DP, _DP, _I, _DP, _C, _S], ctypes.c_int),
     "fpls_x_upload": ([ctypes.c_void_p, _I, _I, _I, _IP, _C, _S], ctypes.c_int),
     "fpls_x_free": ([_I, _C, _S], ctypes.c_int),
@@ -555,3 +559,39 @@ def opls_apply_filter(X, mX, vX, W_orth, P_orth):
     _call("fpls_opls_apply_filter", _p(X), w, p, _p(np.ascontiguousarray(mX, dtype=np.float64).ravel()),
           _p(np.ascontiguousarray(vX, dtype=np.float64).ravel()), _p(W), _p(P), W.shape[1], _p(out))
     return out
+
+
+def candidate_scores(T, Ck=None):
+    """row_l2(T Ck) (R/main.R:657-662, 700-730)."""
+    T = _f64(T)
+    n, k = T.shape
+    out = _out(n, k)
+    _call("fpls_candidate_scores", _p(T), n, k, _p(_f64(Ck)) if Ck is not None else None, _p(out))
+    return out
+
+
+def candidate_centroids(Tn, y_codes, n_classes):
+    Tn = _f64(Tn)
+    n, k = Tn.shape
+    y = np.ascontiguousarray(y_codes, dtype=np.int32)
+    out = _out(n_classes, k)
+    _call("fpls_candidate_centroids", _p(Tn), n, k, _p(y), int(n_classes), _p(out))
+    return out
+
+
+def candidate_knn_predict(Ttest_norm, Ttrain_norm, y_codes, centroids, bias=None, top_k=1,
+                          top_m=20, knn_k=3, tau=0.2, alpha=0.5):
+    Tt = _f64(Ttest_norm)
+    Tr = _f64(Ttrain_norm)
+    C = _f64(centroids)
+    y = np.ascontiguousarray(y_codes, dtype=np.int32)
+    ntest, k = Tt.shape
+    nc = C.shape[0]
+    tk = max(1, min(int(top_k), nc))
+    ti = np.zeros((ntest, tk), dtype=np.int32, order="F")
+    ts = _out(ntest, tk)
+    b = None if bias is None else np.ascontiguousarray(bias, dtype=np.float64)
+    _call("fpls_candidate_knn_predict", _p(Tt), ntest, _p(Tr), Tr.shape[0], k, _p(y), _p(C), nc,
+          _p(b) if b is not None else None, int(top_k), int(top_m), int(knn_k), float(tau),
+          float(alpha), _p(ti), _p(ts))
+    return dict(top_index=ti, top_score=ts)

@@ -1,0 +1,591 @@
+// Candidate-kNN classifier on the device: latent score space, class centroids,
+// candidate classes by centroid similarity, and the smoothed class-kNN rerank.
+//
+// Reference behaviour (R package fastPLS):
+//   score space / row L2 / centroids   R/main.R:657-730
+//   candidate_knn_predict_cuda         src/fastPLS.cpp:1653-1711 -> 1322-1467
+//   per-(row, candidate) class kNN     src/lda_cuda_kernels.cu:180-243 (at most
+//                                      32 neighbour similarities are kept)
+//
+// The reference scores every (test row, candidate class) pair with one thread
+// that walks the whole class serially.  Here the pairs are grouped by class:
+// for each class the test rows that list it as a candidate form 64-row tiles,
+// the class's training rows (gathered class-contiguous, row-major) are cut into
+// chunks, and one CTA computes the 64 x 64 similarity tiles of a (class, tile,
+// chunk) item with FP64 tensor-core MMA, folding each tile into per-row top-k
+// lists held in shared memory.  A merge pass combines the chunk lists of a pair
+// and applies the smoothed score; a rerank pass keeps the top classes.
+#include "../../include/fastpls_b200.h"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <vector>
+
+#include "blas_f64.cuh"
+#include "capi_util.cuh"
+#include "context.cuh"
+
+namespace fpls {
+namespace {
+
+constexpr int kKnnMax = 32;      // neighbour list cap of the replaced CUDA scorer
+constexpr int kTileM = 64;       // test rows per tile
+constexpr int kTileN = 64;       // training rows per similarity tile
+constexpr int kBK = 16;
+constexpr int kPad = 4;
+constexpr int kTileThreads = 128;
+constexpr int kMaxChunks = 64;   // chunk lists merged per pair
+constexpr int kMinChunkRows = 2048;
+
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// Strict '>' insertion into a descending list of length k (earlier entries win
+// ties), list entries strided by `stride` (src/fastPLS.cpp:1249-1267).
+template <typename V, typename I>
+__device__ __forceinline__ void insert_desc(V* vals, I* idx, int k, size_t stride, V v, I id) {
+  if (!(v > vals[(size_t)(k - 1) * stride])) return;
+  int j = 0;
+  while (!(v > vals[(size_t)j * stride])) ++j;
+  for (int h = k - 1; h > j; --h) {
+    vals[(size_t)h * stride] = vals[(size_t)(h - 1) * stride];
+    if (idx) idx[(size_t)h * stride] = idx[(size_t)(h - 1) * stride];
+  }
+  vals[(size_t)j * stride] = v;
+  if (idx) idx[(size_t)j * stride] = id;
+}
+
+// ---------------------------------------------------------------- fit side
+
+// Tn = row_l2(T Ck) or row_l2(T); zero / non-finite row norms become 1
+// (R/main.R:657-662).  One thread per row, sums in column order.
+__global__ void row_l2_kernel(const double* __restrict__ A, int n, int k, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int j = 0; j < k; ++j) {
+    const double v = A[i + (size_t)j * n];
+    s += v * v;
+  }
+  double nr = sqrt(s);
+  if (!isfinite(nr) || nr == 0.0) nr = 1.0;
+  for (int j = 0; j < k; ++j) out[i + (size_t)j * n] = A[i + (size_t)j * n] / nr;
+}
+
+__global__ void class_hist_kernel(const int* __restrict__ codes, int n, int C, int* counts) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = codes[i];
+    if (c >= 1 && c <= C) atomicAdd(counts + (c - 1), 1);
+  }
+}
+
+// dest[i] = slot of row i in class-contiguous order (-1 for codes outside 1..C).
+__global__ void class_slot_kernel(const int* __restrict__ codes, int n, int C,
+                                  const int* __restrict__ offs, int* cursor, int* dest) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = codes[i];
+    dest[i] = (c >= 1 && c <= C) ? offs[c - 1] + atomicAdd(cursor + (c - 1), 1) : -1;
+  }
+}
+
+// Column-major A (n x k) -> row-major rows out[dest[i] * k + j] (rows with
+// dest < 0 dropped); dest == null keeps the order.  32 x 32 tiles through
+// shared memory so both sides are coalesced.
+__global__ void transpose_scatter_kernel(const double* __restrict__ A, int n, int k,
+                                         const int* __restrict__ dest, double* __restrict__ out) {
+  __shared__ double tile[32][33];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = j0 + r, i = i0 + threadIdx.x;
+    if (i < n && j < k) tile[r][threadIdx.x] = A[i + (size_t)j * n];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, j = j0 + threadIdx.x;
+    if (i < n && j < k) {
+      const int d = dest ? dest[i] : i;
+      if (d >= 0) out[(size_t)d * k + j] = tile[threadIdx.x][r];
+    }
+  }
+}
+
+// Class sums over class-contiguous row-major rows, then / max(count, 1), then
+// row L2 of the centroid (R/main.R:686-698).  One CTA per class, 32 columns x 8
+// row groups; the 8 partial sums are added in a fixed order.
+__global__ void centroid_kernel(const double* __restrict__ Ts, int k, const int* __restrict__ offs,
+                                int C, double* __restrict__ cent) {
+  __shared__ double part[8][33];
+  __shared__ double red[32];
+  const int c = blockIdx.x;
+  const int r0 = offs[c], r1 = offs[c + 1];
+  const int col = threadIdx.x & 31, grp = threadIdx.x >> 5;
+  const double cnt = (r1 > r0) ? (double)(r1 - r0) : 1.0;
+  double sq = 0.0;  // only meaningful in group 0
+  for (int j0 = 0; j0 < k; j0 += 32) {
+    const int j = j0 + col;
+    double s = 0.0;
+    if (j < k)
+      for (int r = r0 + grp; r < r1; r += 8) s += Ts[(size_t)r * k + j];
+    part[grp][col] = s;
+    __syncthreads();
+    if (grp == 0 && j < k) {
+      double t = 0.0;
+      for (int g = 0; g < 8; ++g) t += part[g][col];
+      t /= cnt;
+      cent[c + (size_t)j * C] = t;
+      sq += t * t;
+    }
+    __syncthreads();
+  }
+  if (grp == 0) red[col] = sq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int t = 0; t < 32; ++t) s += red[t];
+    double nr = sqrt(s);
+    if (!isfinite(nr) || nr == 0.0) nr = 1.0;
+    red[0] = nr;
+  }
+  __syncthreads();
+  const double nr = red[0];
+  for (int j = threadIdx.x; j < k; j += blockDim.x) cent[c + (size_t)j * C] /= nr;
+}
+
+// ---------------------------------------------------------------- predict side
+
+// Top-m classes of each test row by centroid similarity (insertion order of
+// src/fastPLS.cpp:1401-1415): cand = class code (1-based) or -1.
+__global__ void select_candidates_kernel(const double* __restrict__ base, int ntest, int C, int top_m,
+                                         int* __restrict__ cand, double* __restrict__ cbase) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ntest) return;
+  double* vals = cbase + i;
+  int* idx = cand + i;
+  for (int j = 0; j < top_m; ++j) {
+    vals[(size_t)j * ntest] = -INFINITY;
+    idx[(size_t)j * ntest] = -1;
+  }
+  for (int c = 0; c < C; ++c)
+    insert_desc(vals, idx, top_m, (size_t)ntest, base[i + (size_t)c * ntest], c + 1);
+}
+
+__global__ void pair_hist_kernel(const int* __restrict__ cand, long long npairs, int C, int* counts) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npairs;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int c = cand[p];
+    if (c >= 1 && c <= C) atomicAdd(counts + (c - 1), 1);
+  }
+}
+
+// pairs[slot] = flat (row + slot_j * ntest) index into the candidate matrix.
+__global__ void pair_scatter_kernel(const int* __restrict__ cand, long long npairs, int C,
+                                    const int* __restrict__ offs, int* cursor, int* pairs) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npairs;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int c = cand[p];
+    if (c >= 1 && c <= C) pairs[offs[c - 1] + atomicAdd(cursor + (c - 1), 1)] = (int)p;
+  }
+}
+
+struct KnnItem {
+  int cls;    // 0-based class
+  int tile;   // 64-pair tile within the class's pair list
+  int chunk;  // training-row chunk within the class
+  int pad;
+};
+
+struct KnnClassInfo {
+  const int* row_offs;         // C + 1 class-contiguous training row offsets
+  const int* pair_offs;        // C + 1 class-sorted pair offsets
+  const int* chunk_rows;       // C rows per chunk
+  const int* nchunks;          // C
+  const long long* part_base;  // C partial-list base offsets (in doubles)
+};
+
+// One (class, 64-pair tile, training chunk) item: 64 x 64 FP64 MMA similarity
+// tiles over the chunk, folded into per-row top-k lists (two half-row lists
+// per test row, merged at the end) and written as one sorted list per pair.
+__global__ void __launch_bounds__(kTileThreads)
+knn_tile_kernel(const KnnItem* __restrict__ items, KnnClassInfo ci, const int* __restrict__ pairs,
+                int ntest, const double* __restrict__ Tq, const double* __restrict__ Ts, int K,
+                int use_k, double* __restrict__ part) {
+  extern __shared__ double smem[];
+  double (*As)[kBK][kTileM + kPad] = reinterpret_cast<double (*)[kBK][kTileM + kPad]>(smem);
+  double (*Bs)[kBK][kTileN + kPad] =
+      reinterpret_cast<double (*)[kBK][kTileN + kPad]>(smem + 2 * kBK * (kTileM + kPad));
+  double (*sim)[kTileN + 1] =
+      reinterpret_cast<double (*)[kTileN + 1]>(smem + 2 * kBK * (kTileM + kPad) + 2 * kBK * (kTileN + kPad));
+  double* lv = smem + 2 * kBK * (kTileM + kPad) + 2 * kBK * (kTileN + kPad) + kTileM * (kTileN + 1);
+  __shared__ int prow[kTileM];
+
+  const KnnItem it = items[blockIdx.x];
+  const int c = it.cls;
+  const int p0 = ci.pair_offs[c] + it.tile * kTileM;
+  const int np = min(kTileM, ci.pair_offs[c + 1] - p0);
+  const int cr = ci.chunk_rows[c];
+  const int r0 = ci.row_offs[c] + it.chunk * cr;
+  const int r1 = min(ci.row_offs[c + 1], r0 + cr);
+  const int tid = threadIdx.x;
+  if (tid < kTileM) prow[tid] = (tid < np) ? (int)(pairs[p0 + tid] % ntest) : -1;
+  for (int e = 0; e < use_k; ++e) lv[e * kTileThreads + tid] = -INFINITY;
+  double tail = -INFINITY;
+
+  const int warp = tid >> 5, lane = tid & 31, gid = lane >> 2, tig = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  __syncthreads();
+
+  for (int n0 = r0; n0 < r1; n0 += kTileN) {
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    double ra[8], rb[8];
+    auto load = [&](int k0) {
+      const int kk = tid & 15;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int mn = (tid >> 4) + 8 * i;
+        const int gk = k0 + kk;
+        const int tr = prow[mn];
+        ra[i] = (tr >= 0 && gk < K) ? __ldg(Tq + (size_t)tr * K + gk) : 0.0;
+        rb[i] = (n0 + mn < r1 && gk < K) ? __ldg(Ts + (size_t)(n0 + mn) * K + gk) : 0.0;
+      }
+    };
+    auto store = [&](int b) {
+      const int kk = tid & 15;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int mn = (tid >> 4) + 8 * i;
+        As[b][kk][mn] = ra[i];
+        Bs[b][kk][mn] = rb[i];
+      }
+    };
+    load(0);
+    store(0);
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = 0; k0 < K; k0 += kBK) {
+      const bool has_next = k0 + kBK < K;
+      if (has_next) load(k0 + kBK);
+#pragma unroll
+      for (int kk = 0; kk < kBK; kk += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[buf][kk + tig][wm + i * 8 + gid];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk + tig][wn + j * 8 + gid];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+      }
+      if (has_next) store(buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) sim[wm + i * 8 + gid][wn + j * 8 + tig * 2 + e] = acc[i][j][e];
+    __syncthreads();
+    {
+      const int m = tid & (kTileM - 1), h = tid >> 6;
+      const int ncol = min(32, r1 - n0 - h * 32);
+      for (int cidx = 0; cidx < ncol; ++cidx) {
+        const double v = sim[m][h * 32 + cidx];
+        if (v > tail) {
+          insert_desc<double, int>(lv + tid, nullptr, use_k, kTileThreads, v, 0);
+          tail = lv[(use_k - 1) * kTileThreads + tid];
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // Merge the two half-row lists of each test row; write the pair's list.
+  if (tid < kTileM && tid < np) {
+    const int q = p0 + tid - ci.pair_offs[c];
+    double* out = part + ci.part_base[c] + ((long long)q * ci.nchunks[c] + it.chunk) * use_k;
+    const double* la = lv + tid;
+    const double* lb = lv + tid + kTileM;
+    int ia = 0, ib = 0;
+    for (int e = 0; e < use_k; ++e) {
+      const double va = la[ia * kTileThreads], vb = lb[ib * kTileThreads];
+      if (!(vb > va)) { out[e] = va; ++ia; } else { out[e] = vb; ++ib; }
+    }
+  }
+}
+
+// Per pair: merge its chunk lists, smoothed class score (src/fastPLS.cpp:1287-1320,
+// src/lda_cuda_kernels.cu:225-242), add alpha * base + bias.
+__global__ void knn_merge_kernel(const int* __restrict__ pairs, long long total_pairs,
+                                 const int* __restrict__ cand, const double* __restrict__ cbase,
+                                 KnnClassInfo ci, const double* __restrict__ part, int use_k,
+                                 double tau, double alpha, const double* __restrict__ bias,
+                                 double* __restrict__ cscore) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= total_pairs) return;
+  const int flat = pairs[q];
+  const int c = cand[flat] - 1;
+  const int found = ci.row_offs[c + 1] - ci.row_offs[c];
+  double top[kKnnMax];
+  for (int e = 0; e < use_k; ++e) top[e] = -INFINITY;
+  const int S = ci.nchunks[c];
+  const double* src = part + ci.part_base[c] + (q - ci.pair_offs[c]) * (long long)S * use_k;
+  for (int s = 0; s < S; ++s)
+    for (int e = 0; e < use_k; ++e) {
+      const double v = src[(size_t)s * use_k + e];
+      if (!(v > top[use_k - 1])) break;  // lists are sorted: the rest is smaller
+      insert_desc<double, int>(top, nullptr, use_k, 1, v, 0);
+    }
+  double local;
+  if (found < 1 || !isfinite(top[0])) {
+    local = -INFINITY;
+  } else {
+    const int denom = max(1, min(use_k, found));
+    const double mx = top[0];
+    double acc = 0.0;
+    for (int j = 0; j < denom; ++j) acc += exp((top[j] - mx) / tau);
+    local = mx + tau * log(acc / (double)denom);
+  }
+  cscore[flat] = __dadd_rn(__dadd_rn(local, __dmul_rn(alpha, cbase[flat])), bias[c]);
+}
+
+// Rerank the candidates of each row by score (src/fastPLS.cpp:1447-1466).
+__global__ void knn_rerank_kernel(const int* __restrict__ cand, const double* __restrict__ cscore,
+                                  int ntest, int C, int top_m, int top_k, int* __restrict__ top_index,
+                                  double* __restrict__ top_score) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ntest) return;
+  for (int j = 0; j < top_k; ++j) {
+    top_score[i + (size_t)j * ntest] = -INFINITY;
+    top_index[i + (size_t)j * ntest] = -1;
+  }
+  for (int j = 0; j < top_m; ++j) {
+    const int cls = cand[i + (size_t)j * ntest];
+    if (cls < 1 || cls > C) continue;
+    insert_desc(top_score + i, top_index + i, top_k, (size_t)ntest, cscore[i + (size_t)j * ntest], cls);
+  }
+}
+
+__global__ void fill_int_kernel(int* x, size_t n, int v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+// Class-contiguous, row-major copy of the rows of T (n x k, column-major) by
+// class code; returns the C + 1 row offsets on the host and device.
+struct ClassRows {
+  double* Ts = nullptr;       // rows in class order, row-major (nvalid x k)
+  int* d_offs = nullptr;      // C + 1
+  std::vector<int> offs;      // C + 1 (host)
+};
+
+ClassRows group_rows_by_class(const double* dT, int n, int k, const int* dcodes, int C) {
+  Context& ctx = Context::get();
+  ClassRows cr;
+  int* counts = ctx.arena.alloc_n<int>(C);
+  int* cursor = ctx.arena.alloc_n<int>(C);
+  int* dest = ctx.arena.alloc_n<int>(std::max(n, 1));
+  fill_int_kernel<<<ceil_div(C, 256), 256, 0, ctx.stream>>>(counts, C, 0); ::fpls::note_launch();
+  fill_int_kernel<<<ceil_div(C, 256), 256, 0, ctx.stream>>>(cursor, C, 0); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  const int g = std::max(1, std::min(ceil_div(n, 256), 8 * ctx.sm_count));
+  class_hist_kernel<<<g, 256, 0, ctx.stream>>>(dcodes, n, C, counts); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  std::vector<int> h(C);
+  d2h(h.data(), counts, C * sizeof(int));
+  ctx.sync();
+  cr.offs.assign(C + 1, 0);
+  for (int c = 0; c < C; ++c) cr.offs[c + 1] = cr.offs[c] + h[c];
+  cr.d_offs = ctx.arena.alloc_n<int>(C + 1);
+  h2d(cr.d_offs, cr.offs.data(), (C + 1) * sizeof(int));
+  class_slot_kernel<<<g, 256, 0, ctx.stream>>>(dcodes, n, C, cr.d_offs, cursor, dest); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  const int nvalid = cr.offs[C];
+  cr.Ts = ctx.arena.alloc_n<double>((size_t)std::max(nvalid, 1) * k);
+  dim3 grid(ceil_div(n, 32), ceil_div(k, 32));
+  transpose_scatter_kernel<<<grid, dim3(32, 8), 0, ctx.stream>>>(dT, n, k, dest, cr.Ts); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  return cr;
+}
+
+}  // namespace
+}  // namespace fpls
+
+using namespace fpls;
+using capi::upload;
+
+extern "C" {
+
+int fpls_candidate_scores(const double* T, int n, int k, const double* Ck, double* Tn, char* err,
+                          size_t errlen) {
+  return capi::guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && k > 0, "candidate-kNN requires at least one latent component");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* dT = upload(T, (size_t)n * k);
+    const double* src = dT;
+    if (Ck) {
+      const double* dC = upload(Ck, (size_t)k * k);
+      double* prod = ctx.arena.alloc_n<double>((size_t)n * k);
+      gemm(false, false, n, k, k, 1.0, dT, n, dC, k, 0.0, prod, n);
+      src = prod;
+    }
+    double* out = ctx.arena.alloc_n<double>((size_t)n * k);
+    row_l2_kernel<<<ceil_div(n, 128), 128, 0, ctx.stream>>>(src, n, k, out); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    d2h(Tn, out, (size_t)n * k * sizeof(double));
+    ctx.sync();
+  });
+}
+
+int fpls_candidate_centroids(const double* Tn, int n, int k, const int* y_codes, int n_classes,
+                             double* centroids, char* err, size_t errlen) {
+  return capi::guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && k > 0, "candidate centroids: empty score matrix");
+    FPLS_REQUIRE(n_classes >= 1, "candidate-kNN requires at least one class");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* dT = upload(Tn, (size_t)n * k);
+    const int* dy = upload(y_codes, n);
+    ClassRows cr = group_rows_by_class(dT, n, k, dy, n_classes);
+    double* dC = ctx.arena.alloc_n<double>((size_t)n_classes * k);
+    centroid_kernel<<<n_classes, 256, 0, ctx.stream>>>(cr.Ts, k, cr.d_offs, n_classes, dC); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    d2h(centroids, dC, (size_t)n_classes * k * sizeof(double));
+    ctx.sync();
+  });
+}
+
+int fpls_candidate_knn_predict(const double* Ttest_norm, int ntest, const double* Ttrain_norm,
+                               int ntrain, int kdim, const int* y_codes, const double* centroids,
+                               int n_classes, const double* candidate_bias, int top_k, int top_m,
+                               int knn_k, double tau, double alpha, int* top_index,
+                               double* top_score, char* err, size_t errlen) {
+  return capi::guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n_classes >= 1, "candidate-kNN requires at least one class");
+    FPLS_REQUIRE(ntest > 0 && ntrain > 0 && kdim > 0, "candidate-kNN: empty score matrices");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const int C = n_classes;
+    const int tk = std::max(1, std::min(top_k, C));
+    const int tm = std::max(tk, std::min(std::max(1, top_m), C));
+    const int use_k = std::max(1, std::min(std::max(1, knn_k), kKnnMax));
+    const double tau_e = (std::isfinite(tau) && tau > 0.0) ? tau : 0.2;
+    const double alpha_e = std::isfinite(alpha) ? alpha : 0.5;
+    const long long npairs = (long long)ntest * tm;
+    FPLS_REQUIRE(npairs < (1ll << 31), "candidate-kNN: ntest * top_m must stay below 2^31");
+
+    const double* dTt = upload(Ttest_norm, (size_t)ntest * kdim);
+    const double* dTr = upload(Ttrain_norm, (size_t)ntrain * kdim);
+    const int* dy = upload(y_codes, ntrain);
+    const double* dC = upload(centroids, (size_t)C * kdim);
+    double* dbias = ctx.arena.alloc_n<double>(C);
+    if (candidate_bias) h2d(dbias, candidate_bias, C * sizeof(double));
+    else fill(dbias, C, 0.0);
+
+    // base scores and candidate classes
+    double* base = ctx.arena.alloc_n<double>((size_t)ntest * C);
+    gemm(false, true, ntest, C, kdim, 1.0, dTt, ntest, dC, C, 0.0, base, ntest);
+    int* cand = ctx.arena.alloc_n<int>((size_t)npairs);
+    double* cbase = ctx.arena.alloc_n<double>((size_t)npairs);
+    select_candidates_kernel<<<ceil_div(ntest, 128), 128, 0, ctx.stream>>>(base, ntest, C, tm, cand, cbase); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+
+    // training rows grouped by class (row-major), test rows row-major
+    ClassRows cr = group_rows_by_class(dTr, ntrain, kdim, dy, C);
+    double* Tq = ctx.arena.alloc_n<double>((size_t)ntest * kdim);
+    {
+      dim3 grid(ceil_div(ntest, 32), ceil_div(kdim, 32));
+      transpose_scatter_kernel<<<grid, dim3(32, 8), 0, ctx.stream>>>(dTt, ntest, kdim, nullptr, Tq); ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+    }
+
+    // (row, candidate) pairs grouped by class
+    int* pcount = ctx.arena.alloc_n<int>(C);
+    int* pcursor = ctx.arena.alloc_n<int>(C);
+    fill_int_kernel<<<ceil_div(C, 256), 256, 0, ctx.stream>>>(pcount, C, 0); ::fpls::note_launch();
+    fill_int_kernel<<<ceil_div(C, 256), 256, 0, ctx.stream>>>(pcursor, C, 0); ::fpls::note_launch();
+    const int g = std::max(1, std::min(ceil_div(npairs, 256), 8 * ctx.sm_count));
+    pair_hist_kernel<<<g, 256, 0, ctx.stream>>>(cand, npairs, C, pcount); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    std::vector<int> hp(C);
+    d2h(hp.data(), pcount, C * sizeof(int));
+    ctx.sync();
+    std::vector<int> poffs(C + 1, 0), chunk_rows(C, 0), nchunks(C, 0);
+    std::vector<long long> part_base(C, 0);
+    std::vector<KnnItem> items;
+    long long part_total = 0;
+    for (int c = 0; c < C; ++c) {
+      poffs[c + 1] = poffs[c] + hp[c];
+      const int rows = cr.offs[c + 1] - cr.offs[c];
+      int S = 0, cr_rows = 0;
+      if (rows > 0) {
+        S = std::min(kMaxChunks, std::max(1, ceil_div(rows, kMinChunkRows)));
+        cr_rows = ceil_div(ceil_div(rows, S), kTileN) * kTileN;
+        S = ceil_div(rows, cr_rows);
+      }
+      chunk_rows[c] = cr_rows;
+      nchunks[c] = S;
+      part_base[c] = part_total;
+      part_total += (long long)hp[c] * S * use_k;
+      if (rows > 0 && hp[c] > 0) {
+        const int tiles = ceil_div(hp[c], kTileM);
+        for (int t = 0; t < tiles; ++t)
+          for (int s = 0; s < S; ++s) items.push_back(KnnItem{c, t, s, 0});
+      }
+    }
+    const long long total_pairs = poffs[C];
+    int* pairs = ctx.arena.alloc_n<int>((size_t)std::max<long long>(total_pairs, 1));
+    int* d_poffs = ctx.arena.alloc_n<int>(C + 1);
+    h2d(d_poffs, poffs.data(), (C + 1) * sizeof(int));
+    pair_scatter_kernel<<<g, 256, 0, ctx.stream>>>(cand, npairs, C, d_poffs, pcursor, pairs); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+
+    KnnClassInfo ci;
+    ci.row_offs = cr.d_offs;
+    ci.pair_offs = d_poffs;
+    ci.chunk_rows = upload(chunk_rows.data(), C);
+    ci.nchunks = upload(nchunks.data(), C);
+    ci.part_base = upload(part_base.data(), C);
+    double* part = ctx.arena.alloc_n<double>((size_t)std::max<long long>(part_total, 1));
+    double* cscore = ctx.arena.alloc_n<double>((size_t)npairs);
+    if (!items.empty()) {
+      const KnnItem* ditems = upload(items.data(), items.size());
+      const size_t smem = sizeof(double) * (2 * kBK * (kTileM + kPad) + 2 * kBK * (kTileN + kPad) +
+                                            kTileM * (kTileN + 1) + (size_t)kKnnMax * kTileThreads);
+      static bool attr_set = false;
+      if (!attr_set) {
+        FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+      }
+      FPLS_REQUIRE(items.size() < (1u << 31), "candidate-kNN: too many work items");
+      knn_tile_kernel<<<(unsigned)items.size(), kTileThreads, smem, ctx.stream>>>(
+          ditems, ci, pairs, ntest, Tq, cr.Ts, kdim, use_k, part); ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+    }
+    fill(cscore, (size_t)npairs, -INFINITY);
+    if (total_pairs > 0) {
+      knn_merge_kernel<<<ceil_div(total_pairs, 128), 128, 0, ctx.stream>>>(
+          pairs, total_pairs, cand, cbase, ci, part, use_k, tau_e, alpha_e, dbias, cscore); ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+    }
+    int* d_ti = ctx.arena.alloc_n<int>((size_t)ntest * tk);
+    double* d_ts = ctx.arena.alloc_n<double>((size_t)ntest * tk);
+    knn_rerank_kernel<<<ceil_div(ntest, 128), 128, 0, ctx.stream>>>(cand, cscore, ntest, C, tm, tk, d_ti, d_ts); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    d2h(top_index, d_ti, (size_t)ntest * tk * sizeof(int));
+    d2h(top_score, d_ts, (size_t)ntest * tk * sizeof(double));
+    ctx.sync();
+  });
+}
+
+}  // extern "C"

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "blas_f64.cuh"
+#include "capi_util.cuh"
 #include "context.cuh"
 #include "fits.cuh"
 #include "linalg_small.cuh"
@@ -153,49 +154,18 @@ void leading_left_vector(const double* S, int p, int q, double* u, unsigned int 
 
 using namespace fpls;
 
-namespace {
-
-void put_err(char* err, size_t errlen, const char* msg) {
-  if (!err || errlen == 0) return;
-  std::strncpy(err, msg, errlen - 1);
-  err[errlen - 1] = '\0';
-}
-
-template <typename Fn>
-int guard(char* err, size_t errlen, Fn&& fn) {
-  if (err && errlen) err[0] = '\0';
-  try {
-    fn();
-    Context::get().end_call();
-    return FPLS_OK;
-  } catch (const Error& e) {
-    put_err(err, errlen, e.what());
-    return e.code;
-  } catch (const std::exception& e) {
-    put_err(err, errlen, e.what());
-    return FPLS_ERR_INTERNAL;
-  }
-}
-
-template <typename T>
-T* up(const T* h, size_t n) {
-  T* d = Context::get().arena.alloc_n<T>(n ? n : 1);
-  if (n) h2d(d, h, n * sizeof(T));
-  return d;
-}
-
-}  // namespace
+using capi::upload;
 
 extern "C" {
 
 int fpls_gaussian_y_encode(const double* Y, int n, int q, const double* projection, int d, double* Z,
                            double* y_center, double* decoder, char* err, size_t errlen) {
-  return guard(err, errlen, [&] {
+  return capi::guarded(err, errlen, [&] {
     FPLS_REQUIRE(n > 0 && q > 0 && d > 0, "gaussian_y_encode: empty input");
     Context& ctx = Context::get();
     ctx.begin_call();
-    double* dY = up(Y, (size_t)n * q);
-    const double* dG = up(projection, (size_t)q * d);
+    double* dY = upload(Y, (size_t)n * q);
+    const double* dG = upload(projection, (size_t)q * d);
     double* dmu = ctx.arena.alloc_n<double>(q);
     col_mean(dY, n, q, n, dmu);
     center_scale(dY, n, q, n, dmu, nullptr);
@@ -220,13 +190,13 @@ int fpls_gaussian_y_encode(const double* Y, int n, int q, const double* projecti
 
 int fpls_gaussian_y_decode(const double* Z, int w, int d, const double* decoder,
                            const double* y_center, int q, double* Y, char* err, size_t errlen) {
-  return guard(err, errlen, [&] {
+  return capi::guarded(err, errlen, [&] {
     FPLS_REQUIRE(w > 0 && d > 0 && q > 0, "gaussian_y_decode: empty input");
     Context& ctx = Context::get();
     ctx.begin_call();
-    const double* dZ = up(Z, (size_t)w * d);
-    const double* dD = up(decoder, (size_t)d * q);
-    const double* dmu = up(y_center, q);
+    const double* dZ = upload(Z, (size_t)w * d);
+    const double* dD = upload(decoder, (size_t)d * q);
+    const double* dmu = upload(y_center, q);
     double* dY = ctx.arena.alloc_n<double>((size_t)w * q);
     gemm(false, false, w, q, d, 1.0, dZ, w, dD, d, 0.0, dY, w);
     add_row_vector(dY, w, q, w, dmu);
@@ -237,12 +207,12 @@ int fpls_gaussian_y_decode(const double* Z, int w, int d, const double* decoder,
 
 int fpls_nearest_code_classes(const double* Z, int w, int d, const double* codes, int n_classes,
                               int* labels, char* err, size_t errlen) {
-  return guard(err, errlen, [&] {
+  return capi::guarded(err, errlen, [&] {
     FPLS_REQUIRE(w > 0 && d > 0 && n_classes > 0, "nearest_code_classes: empty input");
     Context& ctx = Context::get();
     ctx.begin_call();
-    const double* dZ = up(Z, (size_t)w * d);
-    const double* dC = up(codes, (size_t)n_classes * d);
+    const double* dZ = upload(Z, (size_t)w * d);
+    const double* dC = upload(codes, (size_t)n_classes * d);
     double* dS = ctx.arena.alloc_n<double>((size_t)w * n_classes);
     double* cn = ctx.arena.alloc_n<double>(n_classes);
     int* dl = ctx.arena.alloc_n<int>(w);
@@ -259,13 +229,13 @@ int fpls_nearest_code_classes(const double* Z, int w, int d, const double* codes
 int fpls_opls_filter(const double* X, int n, int p, const double* Y, int q, int north, int scaling,
                      double* Xf, double* mX, double* vX, double* W_orth, double* P_orth, int* used,
                      char* err, size_t errlen) {
-  return guard(err, errlen, [&] {
+  return capi::guarded(err, errlen, [&] {
     FPLS_REQUIRE(n > 0 && p > 0 && q > 0, "opls_filter: X and Y must be non-empty");
     FPLS_REQUIRE(north >= 0, "north must be >= 0");
     Context& ctx = Context::get();
     ctx.begin_call();
-    double* dX = up(X, (size_t)n * p);
-    double* dY = up(Y, (size_t)n * q);
+    double* dX = upload(X, (size_t)n * p);
+    double* dY = upload(Y, (size_t)n * q);
     double* dmX = ctx.arena.alloc_n<double>(p);
     double* dvX = ctx.arena.alloc_n<double>(p);
     double* dmY = ctx.arena.alloc_n<double>(q);
@@ -346,17 +316,17 @@ int fpls_opls_filter(const double* X, int n, int p, const double* Y, int q, int 
 int fpls_opls_apply_filter(const double* X, int w, int p, const double* mX, const double* vX,
                            const double* W_orth, const double* P_orth, int north, double* Xf,
                            char* err, size_t errlen) {
-  return guard(err, errlen, [&] {
+  return capi::guarded(err, errlen, [&] {
     FPLS_REQUIRE(w > 0 && p > 0 && north >= 0, "opls_apply_filter: empty input");
     Context& ctx = Context::get();
     ctx.begin_call();
-    double* dX = up(X, (size_t)w * p);
-    const double* dm = up(mX, p);
-    const double* dv = up(vX, p);
+    double* dX = upload(X, (size_t)w * p);
+    const double* dm = upload(mX, p);
+    const double* dv = upload(vX, p);
     center_scale(dX, w, p, w, dm, dv);
     if (north > 0) {
-      const double* dW = up(W_orth, (size_t)p * north);
-      const double* dP = up(P_orth, (size_t)p * north);
+      const double* dW = upload(W_orth, (size_t)p * north);
+      const double* dP = upload(P_orth, (size_t)p * north);
       double* t = ctx.arena.alloc_n<double>(w);
       for (int a = 0; a < north; ++a) {
         gemv(false, w, p, 1.0, dX, w, dW + (size_t)a * p, 0.0, t);

@@ -232,6 +232,38 @@ int fpls_opls_apply_filter(const double* X, int w, int p, const double* mX, cons
                            const double* W_orth, const double* P_orth, int north, double* Xf,
                            char* err, size_t errlen);
 
+/* Candidate-kNN score space: Tn = row_l2(T Ck) (Ck k x k, or null for T
+ * itself), T n x k column-major; zero row norms are replaced by 1.  Replaces
+ * the R-side .candidate_score_space + .candidate_row_l2 arithmetic
+ * (R/main.R:657-662, 700-730); no .Call counterpart. */
+int fpls_candidate_scores(const double* T, int n, int k, const double* Ck, double* Tn, char* err,
+                          size_t errlen);
+
+/* Class centroids of row-normalised scores: per class mean of Tn rows with
+ * code c (1-based; empty classes give a zero row), then row L2.  centroids is
+ * n_classes x k column-major.  Replaces .candidate_centroids
+ * (R/main.R:686-698); no .Call counterpart. */
+int fpls_candidate_centroids(const double* Tn, int n, int k, const int* y_codes, int n_classes,
+                             double* centroids, char* err, size_t errlen);
+
+/* Candidate-kNN prediction.  base = Ttest_norm centroidsᵀ; the top_m classes
+ * by base score (ties: lower class first) are candidates; each candidate c is
+ * scored local + alpha*base + bias[c], local = mx + tau*log(mean_j
+ * exp((s_j - mx)/tau)) over the k' = min(knn_k, 32, |c|) largest cosine
+ * similarities s_j of the test row to the training rows of class c; the
+ * candidates are reranked and the best top_k kept.  Effective parameters as
+ * the reference: top_k in [1, n_classes], top_m in [top_k, n_classes],
+ * tau <= 0 or non-finite -> 0.2, alpha non-finite -> 0.5, candidate_bias null
+ * -> zeros.  top_index (int, 1-based class codes, -1 when absent) and
+ * top_score are ntest x max(1, min(top_k, n_classes)) column-major.
+ * Replaces _fastPLS_candidate_knn_predict_cuda (RcppExports.cpp:148;
+ * fastPLS.cpp:1653-1711, 1322-1467; lda_cuda_kernels.cu:180-243). */
+int fpls_candidate_knn_predict(const double* Ttest_norm, int ntest, const double* Ttrain_norm,
+                               int ntrain, int kdim, const int* y_codes, const double* centroids,
+                               int n_classes, const double* candidate_bias, int top_k, int top_m,
+                               int knn_k, double tau, double alpha, int* top_index,
+                               double* top_score, char* err, size_t errlen);
+
 /* C (M x N) = A (M x K) * B (K x N) through the BF16 split tensor-core kernel,
  * for callers that cannot allocate device memory (a host that runs inside
  * another runtime's fixed memory pool, a stream callback, an allocation-free

@@ -185,3 +185,33 @@ def test_opls_filter_identities():
         assert np.allclose(again, f["X"], atol=1e-10)
     f0 = oo.opls_filter(X, Y, 0)
     assert f0["north"] == 0 and f0["W_orth"].shape == (20, 0)
+
+
+def test_cknn_known_answer():
+    # Two classes in 2-D, worked by hand from src/fastPLS.cpp:1287-1467.
+    import math
+    from oracle import cknn
+    Tr = np.array([[1.0, 0.0], [0.8, 0.6], [0.0, 1.0]])
+    y = np.array([1, 1, 2], dtype=np.int32)
+    cents = cknn.centroids(Tr, y, 2)
+    assert np.allclose(cents[0], np.array([0.9, 0.3]) / math.hypot(0.9, 0.3))
+    Tt = np.array([[1.0, 0.0]])
+    out = cknn.candidate_knn_predict(Tt, Tr, y, cents, top_k=2, top_m=2, knn_k=2, tau=0.2,
+                                     alpha=0.75)
+    base1 = cents[0] @ Tt[0]
+    local1 = 1.0 + 0.2 * math.log((1.0 + math.exp((0.8 - 1.0) / 0.2)) / 2.0)
+    assert out["top_index"].tolist() == [[1, 2]]
+    assert np.allclose(out["top_score"], [[local1 + 0.75 * base1, 0.0]], atol=1e-15)
+    # tau <= 0 falls back to 0.2; top is clamped to the class count (test-class-bias-top5.R:70-72)
+    again = cknn.candidate_knn_predict(Tt, Tr, y, cents, top_k=5, top_m=9, knn_k=2, tau=-1.0,
+                                       alpha=0.75)
+    assert again["top_index"].shape == (1, 2)
+    assert np.array_equal(again["top_score"], out["top_score"])
+
+
+def test_cknn_insertion_ties_keep_first():
+    from oracle import cknn
+    s, ix = [-np.inf] * 3, [-1] * 3
+    for c, v in enumerate([0.5, 0.7, 0.5, 0.7]):
+        cknn.insert_top(s, ix, v, c + 1)
+    assert ix == [2, 4, 1] and s == [0.7, 0.7, 0.5]

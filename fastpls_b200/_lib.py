@@ -65,6 +65,9 @@ SIGNATURES = {
     "fpls_nearest_code_classes": ([_DP, _I, _I, _DP, _I, _IP, _C, _S], ctypes.c_int),
     "fpls_opls_filter": ([_DP, _I, _I, _DP, _I, _I, _I, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S],
                          ctypes.c_int),
+    "fpls_plssvd_label_aware": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _I, _I, _I, _I, _I,
+                                 _IP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S],
+                                ctypes.c_int),
     "fpls_candidate_scores": ([_DP, _I, _I, _DP, _DP, _C, _S], ctypes.c_int),
     "fpls_candidate_centroids": ([_DP, _I, _I, _IP, _I, _DP, _C, _S], ctypes.c_int),
     "fpls_candidate_knn_predict": ([_DP, _I, _DP, _I, _I, _IP, _DP, _I, _DP, _I, _I, _I, _D, _D,
@@ -595,3 +598,32 @@ def candidate_knn_predict(Ttest_norm, Ttrain_norm, y_codes, centroids, bias=None
           _p(b) if b is not None else None, int(top_k), int(top_m), int(knn_k), float(tau),
           float(alpha), _p(ti), _p(ts))
     return dict(top_index=ti, top_score=ts)
+
+
+def plssvd_label_aware(X, y_codes, m, ncomp, scaling=1, svd_method=3, oversample=10,
+                       power_iters=1, seed=1, keep_scores=False):
+    """Label-aware PLSSVD (R/main.R:513-655); X float32 or float64, y_codes 1..m."""
+    X = np.asfortranarray(X)
+    f32 = X.dtype == np.float32
+    if not f32:
+        X = _f64(X)
+    n, p = X.shape
+    y = np.ascontiguousarray(y_codes, dtype=np.int32)
+    nc = np.ascontiguousarray(ncomp, dtype=np.int32)
+    L = len(nc)
+    K = int(min(max(int(nc.max()), 1), n, p, m))
+    out = dict(C_latent=np.zeros((K, K, L), order="F"), W_latent=np.zeros((K, m, L), order="F"),
+               Q=_out(m, K), R=_out(p, K), mX=np.zeros(p), vX=np.zeros(p), mY=np.zeros(m),
+               s=np.zeros(K))
+    T = _out(n, K) if keep_scores else None
+    nco = np.zeros(L, dtype=np.int32)
+    kr = ctypes.c_int(0)
+    _call("fpls_plssvd_label_aware", X.ctypes.data_as(ctypes.c_void_p), int(f32), n, p, _p(y), int(m),
+          _p(nc), L, int(scaling), int(svd_method), int(oversample), int(power_iters), int(seed),
+          _p(nco), _p(out["C_latent"]), _p(out["W_latent"]), _p(out["Q"]), _p(out["R"]),
+          _p(out["mX"]), _p(out["vX"]), _p(out["mY"]), _p(out["s"]), _p(T), ctypes.byref(kr))
+    out["ncomp"] = nco
+    out["max_rank"] = kr.value
+    if keep_scores:
+        out["Ttrain"] = T
+    return out

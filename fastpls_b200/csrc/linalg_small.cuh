@@ -31,4 +31,10 @@ void eig_sym_desc(int l, const double* G, int ldg, double* evals, double* V, int
 void svd_thin(int rows, int cols, const double* A, int lda, double* U, int ldu, double* s,
               double* V, int ldv);
 
+// Same contract as svd_thin, computed by a cooperative one-sided Jacobi over
+// the whole GPU (one warp per column pair, grid barrier per round); for
+// min(rows, cols) in the hundreds and above.
+void svd_jacobi_coop(int rows, int cols, const double* A, int lda, double* U, int ldu, double* s,
+                     double* V, int ldv);
+
 }  // namespace fpls

@@ -26,6 +26,9 @@ __global__ void scale_cols_inv_kernel(double* V, int rows, int cols, int ldv, co
   }
 }
 
+// Above this many singular values the exact SVD runs across the whole GPU.
+constexpr int kCoopSvdMin = 96;
+
 SvdResult exact_svd(const double* A, int rows, int cols, int lda, int k, bool left_only,
                     double* U, int ldu, double* s, double* V, int ldv) {
   Context& ctx = Context::get();
@@ -36,7 +39,8 @@ SvdResult exact_svd(const double* A, int rows, int cols, int lda, int k, bool le
   double* Uw = ctx.arena.alloc_n<double>((size_t)rows * max_rank);
   double* sw = ctx.arena.alloc_n<double>(max_rank);
   double* Vw = ctx.arena.alloc_n<double>((size_t)cols * max_rank);
-  svd_thin(rows, cols, A, lda, Uw, rows, sw, Vw, cols);
+  if (max_rank > kCoopSvdMin) svd_jacobi_coop(rows, cols, A, lda, Uw, rows, sw, Vw, cols);
+  else svd_thin(rows, cols, A, lda, Uw, rows, sw, Vw, cols);
   copy_matrix(U, ldu, Uw, rows, rows, rank);
   d2d(s, sw, rank * sizeof(double));
   if (!left_only && V) copy_matrix(V, ldv, Vw, cols, cols, rank);

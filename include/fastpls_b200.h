@@ -232,6 +232,25 @@ int fpls_opls_apply_filter(const double* X, int w, int p, const double* mX, cons
                            const double* W_orth, const double* P_orth, int north, double* Xf,
                            char* err, size_t errlen);
 
+/* Label-aware PLSSVD for a factor response, with no dense one-hot Y: column
+ * statistics (mX; vX from sums of squares for scaling 2), class sums of the
+ * centred rows, S = class_sums - total mYᵀ (mY = class counts / n), the SVD of
+ * S (svd_method 3 = exact, as R's svd(); 4 / 5 = the seeded rSVD recipe with
+ * oversample / power_iters), T = X̃R, G = TᵀT and per requested ncomp k
+ * C_k = (G_k + 1e-10·mean(diag G_k) I)⁻¹ diag(d_k), W_k = C_k Q_kᵀ.  ncomp is
+ * capped to [1, min(n, p, m)] (ncomp_out); K = max(ncomp_out) is written to
+ * *max_rank and sizes the outputs: C_latent K x K x L, W_latent K x m x L,
+ * Q m x K, R p x K, mX / vX p, mY m, s K (nullable), Ttrain n x K (nullable).
+ * X is n x p column-major FP64 (x_is_float32 = 0) or FP32; y_codes in 1..m.
+ * Replaces .plssvd_label_aware_stream_model (R/main.R:513-655), which runs in
+ * R for both backends; no .Call counterpart. */
+int fpls_plssvd_label_aware(const void* X, int x_is_float32, int n, int p, const int* y_codes, int m,
+                            const int* ncomp, int L, int scaling, int svd_method, int oversample,
+                            int power_iters, int seed, int* ncomp_out, double* C_latent,
+                            double* W_latent, double* Q, double* R, double* mX, double* vX,
+                            double* mY, double* s, double* Ttrain, int* max_rank, char* err,
+                            size_t errlen);
+
 /* Candidate-kNN score space: Tn = row_l2(T Ck) (Ck k x k, or null for T
  * itself), T n x k column-major; zero row norms are replaced by 1.  Replaces
  * the R-side .candidate_score_space + .candidate_row_l2 arithmetic

@@ -24,8 +24,6 @@
 namespace fpls {
 namespace {
 
-constexpr int kRowsPerCta = 2048;
-
 // Column sums (and sums of squares) of the raw predictors, one CTA per column
 // (R/main.R:542-551).
 template <typename T>
@@ -88,11 +86,6 @@ __global__ void transpose_center_kernel(const T* __restrict__ X, int n, int p, c
   }
 }
 
-__global__ void la_hist_kernel(const int* __restrict__ y, int n, int* counts) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    atomicAdd(counts + (y[i] - 1), 1);
-}
-
 __global__ void la_sort_kernel(const int* __restrict__ y, int n, const int* __restrict__ offs, int* cursor,
                                int* __restrict__ perm, int* __restrict__ ysorted) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -103,17 +96,26 @@ __global__ void la_sort_kernel(const int* __restrict__ y, int n, const int* __re
   }
 }
 
-// Class sums over class-sorted rows: each CTA walks kRowsPerCta sorted rows,
-// each thread owns up to kColsPerThread columns and keeps running sums in
-// registers, flushing them (atomicAdd into cs, p x m column-major) when the
-// class changes and at the end of its range.
+// Class sums over class-sorted rows: each CTA walks `rows` sorted rows (their
+// row indices and classes staged in shared memory), each thread owns up to
+// kColsPerThread columns and keeps running sums in registers, flushing them
+// (atomicAdd into cs, p x m column-major) when the class changes and at the
+// end of its range.  Loads of kRowBatch rows are issued before they are
+// accumulated, so each thread keeps 32 loads in flight.
 constexpr int kColsPerThread = 4;
+constexpr int kRowBatch = 8;
 __global__ void __launch_bounds__(256) class_sum_kernel(const double* __restrict__ Xt, int p, int n,
                                                         const int* __restrict__ perm,
                                                         const int* __restrict__ ysorted, int col0,
-                                                        double* __restrict__ cs) {
-  const int s0 = blockIdx.x * kRowsPerCta;
-  const int s1 = min(n, s0 + kRowsPerCta);
+                                                        int rows, double* __restrict__ cs) {
+  extern __shared__ int sidx[];  // [rows] row index, [rows] class
+  const int s0 = blockIdx.x * rows;
+  const int nr = min(n, s0 + rows) - s0;
+  for (int t = threadIdx.x; t < nr; t += blockDim.x) {
+    sidx[t] = perm[s0 + t];
+    sidx[rows + t] = ysorted[s0 + t];
+  }
+  __syncthreads();
   int jcol[kColsPerThread];
   double acc[kColsPerThread];
 #pragma unroll
@@ -121,21 +123,33 @@ __global__ void __launch_bounds__(256) class_sum_kernel(const double* __restrict
     jcol[u] = col0 + threadIdx.x + u * blockDim.x;
     acc[u] = 0.0;
   }
-  int cur = ysorted[s0];
-  for (int s = s0; s < s1; ++s) {
-    const int c = ysorted[s];
-    if (c != cur) {
+  int cur = sidx[rows];
+  for (int base = 0; base < nr; base += kRowBatch) {
+    double v[kRowBatch][kColsPerThread];
 #pragma unroll
-      for (int u = 0; u < kColsPerThread; ++u) {
-        if (jcol[u] < p) atomicAdd(cs + jcol[u] + (size_t)cur * p, acc[u]);
-        acc[u] = 0.0;
-      }
-      cur = c;
+    for (int g = 0; g < kRowBatch; ++g) {
+      const int r = base + g;
+      const double* row = Xt + (size_t)(r < nr ? sidx[r] : 0) * p;
+#pragma unroll
+      for (int u = 0; u < kColsPerThread; ++u)
+        v[g][u] = (r < nr && jcol[u] < p) ? __ldg(row + jcol[u]) : 0.0;
     }
-    const double* row = Xt + (size_t)perm[s] * p;
 #pragma unroll
-    for (int u = 0; u < kColsPerThread; ++u)
-      if (jcol[u] < p) acc[u] += __ldg(row + jcol[u]);
+    for (int g = 0; g < kRowBatch; ++g) {
+      const int r = base + g;
+      if (r >= nr) break;
+      const int c = sidx[rows + r];
+      if (c != cur) {
+#pragma unroll
+        for (int u = 0; u < kColsPerThread; ++u) {
+          if (jcol[u] < p) atomicAdd(cs + jcol[u] + (size_t)cur * p, acc[u]);
+          acc[u] = 0.0;
+        }
+        cur = c;
+      }
+#pragma unroll
+      for (int u = 0; u < kColsPerThread; ++u) acc[u] += v[g][u];
+    }
   }
 #pragma unroll
   for (int u = 0; u < kColsPerThread; ++u)
@@ -176,6 +190,7 @@ LabelAwareFit label_aware_fit(const void* dX, bool f32, int n, int p, const int*
   Context& ctx = Context::get();
   FPLS_REQUIRE(n >= 1 && p >= 1 && m >= 2,
                "label-aware PLSSVD requires non-empty X and at least two classes");
+  PhaseTimer pt("label-aware PLSSVD");
   LabelAwareFit f;
   f.n = n;
   f.p = p;
@@ -207,6 +222,7 @@ LabelAwareFit label_aware_fit(const void* dX, bool f32, int n, int p, const int*
     ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
+  pt.mark("stats + centred copy");
 
   // class-sorted row order (counting sort of the labels)
   std::vector<int> counts_h(m, 0);
@@ -224,17 +240,21 @@ LabelAwareFit label_aware_fit(const void* dX, bool f32, int n, int p, const int*
   const int g = std::max(1, std::min(ceil_div(n, 256), 8 * ctx.sm_count));
   la_sort_kernel<<<g, 256, 0, ctx.stream>>>(dy, n, d_offs, cursor, perm, ysorted); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+  pt.mark("class sort");
 
   // class sums -> S (p x m)
   f.S = ctx.arena.alloc_n<double>((size_t)p * m);
   fill(f.S, (size_t)p * m, 0.0);
+  const int rows = std::min(4096, std::max(256, ceil_div(ceil_div(n, 4 * ctx.sm_count), 8) * 8));
   for (int col0 = 0; col0 < p; col0 += 256 * kColsPerThread) {
-    class_sum_kernel<<<ceil_div(n, kRowsPerCta), 256, 0, ctx.stream>>>(f.Xt, p, n, perm, ysorted, col0, f.S); ::fpls::note_launch();
+    class_sum_kernel<<<ceil_div(n, rows), 256, 2 * rows * sizeof(int), ctx.stream>>>(f.Xt, p, n, perm, ysorted,
+                                                                                    col0, rows, f.S); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
   f.mY = ctx.arena.alloc_n<double>(m);
   la_crosscov_kernel<<<ceil_div(p, 128), 128, 0, ctx.stream>>>(f.S, p, m, counts, n, f.mY); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+  pt.mark("class sums");
 
   // SVD of S: R = U[:, :K], Q = V[:, :K], d
   f.R = ctx.arena.alloc_n<double>((size_t)p * K);
@@ -247,12 +267,14 @@ LabelAwareFit label_aware_fit(const void* dX, bool f32, int n, int p, const int*
   SvdResult sr = truncated_svd_device(f.S, p, m, p, K, exact ? kSvdExact : svd_method, oversample,
                                       power_iters, seed, false, exact, f.R, p, f.d, f.Q, m);
   f.rank = sr.rank;
+  pt.mark("svd");
 
   // T = X~ R (n x K), G = T^T T
   f.T = ctx.arena.alloc_n<double>((size_t)n * K);
   gemm(true, false, n, K, p, 1.0, f.Xt, p, f.R, p, 0.0, f.T, n);
   f.G = ctx.arena.alloc_n<double>((size_t)K * K);
   gemm(true, false, K, K, n, 1.0, f.T, n, f.T, n, 0.0, f.G, K);
+  pt.mark("scores + gram");
 
   // per-ncomp coefficients
   f.C = ctx.arena.alloc_n<double>((size_t)K * K * L);
@@ -273,6 +295,8 @@ LabelAwareFit label_aware_fit(const void* dX, bool f32, int n, int p, const int*
   int bad = 0;
   d2h(&bad, flag, sizeof(int));
   ctx.sync();
+  pt.mark("coefficients");
+  pt.report();
   if (bad) throw Error(kErrNumerical, "label-aware PLSSVD: latent Gram system is singular");
   return f;
 }

@@ -25,6 +25,11 @@ void qr_orthonormalize(int rows, int cols, const double* Y, int ldy, double* Q, 
 // order.  G (l x l) is read only; evals[l], V (l x l).
 void eig_sym_desc(int l, const double* G, int ldg, double* evals, double* V, int ldv);
 
+// Eigen-decomposition of a symmetric positive semi-definite G (l x l),
+// eigenvalues descending: the single-CTA Jacobi for small l, else the
+// whole-GPU one-sided Jacobi SVD of G (singular values = eigenvalues).
+void eig_psd_desc(int l, const double* G, int ldg, double* evals, double* V, int ldv);
+
 // Thin SVD A = U diag(s) V^T of a rows x cols matrix by one-sided Jacobi,
 // singular values descending, U rows x r, V cols x r with r = min(rows, cols).
 // Null directions are completed to an orthonormal set.
@@ -32,7 +37,7 @@ void svd_thin(int rows, int cols, const double* A, int lda, double* U, int ldu, 
               double* V, int ldv);
 
 // Same contract as svd_thin, computed by a cooperative one-sided Jacobi over
-// the whole GPU (one warp per column pair, grid barrier per round); for
+// the whole GPU (one CTA per column pair, grid barrier per round); for
 // min(rows, cols) in the hundreds and above.
 void svd_jacobi_coop(int rows, int cols, const double* A, int lda, double* U, int ldu, double* s,
                      double* V, int ldv);

@@ -124,7 +124,7 @@ void leading_left_vector(const double* S, int p, int q, double* u, unsigned int 
     if (it % kCheck) continue;
     gemm(false, false, m, l, m, 1.0, G, m, Q, m, 0.0, GQ, m);
     gemm(true, false, l, l, m, 1.0, Q, m, GQ, m, 0.0, H, l);
-    eig_sym_desc(l, H, l, ev, Uh, l);
+    eig_psd_desc(l, H, l, ev, Uh, l);
     gemv(false, m, l, 1.0, Q, m, Uh, 0.0, v);
     dot2_kernel<<<1, 512, 0, ctx.stream>>>(v, vprev, m, dots); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();

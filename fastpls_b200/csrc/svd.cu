@@ -104,7 +104,7 @@ SvdResult truncated_svd_device(const double* A, int rows, int cols, int lda, int
     double* ev = ctx.arena.alloc_n<double>(l);
     double* Uh = ctx.arena.alloc_n<double>((size_t)l * l);
     gemm(false, true, l, l, cols, 1.0, B, l, B, l, 0.0, G, l);
-    eig_sym_desc(l, G, l, ev, Uh, l);
+    eig_psd_desc(l, G, l, ev, Uh, l);
     std::vector<double> evh(l);
     d2h(evh.data(), ev, l * sizeof(double));
     ctx.sync();

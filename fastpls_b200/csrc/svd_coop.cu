@@ -1,5 +1,5 @@
 // Thin SVD by one-sided (Hestenes) Jacobi spread over the whole GPU: one
-// cooperative launch, one warp per column pair of a round-robin round, a
+// cooperative launch, one CTA per column pair of a round-robin round, a
 // grid-wide barrier between rounds.  Used for the exact SVD of matrices too
 // large for the single-CTA Jacobi (e.g. the 768 x 1000 class-sum
 // cross-covariance of label-aware PLSSVD, which the reference hands to
@@ -75,30 +75,49 @@ __device__ __forceinline__ void circle_pair(int ne, int rd, int k, int& i, int& 
   }
 }
 
+__device__ __forceinline__ double block_sum3(double& a, double& b, double& c, double (*red)[3]) {
+  a = warp_sum(a);
+  b = warp_sum(b);
+  c = warp_sum(c);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[w][0] = a;
+    red[w][1] = b;
+    red[w][2] = c;
+  }
+  __syncthreads();
+  a = b = c = 0.0;
+  for (int u = 0; u < kCoopThreads / 32; ++u) {
+    a += red[u][0];
+    b += red[u][1];
+    c += red[u][2];
+  }
+  __syncthreads();
+  return a;
+}
+
+// One CTA per column pair of the round (the CTA loops when there are more
+// pairs than CTAs); all threads of the CTA share the pair's dots and update.
 __global__ void __launch_bounds__(kCoopThreads) jacobi_coop_kernel(CoopJacobi J) {
-  const int lane = threadIdx.x & 31;
-  const int gwarp = blockIdx.x * (kCoopThreads / 32) + (threadIdx.x >> 5);
-  const int nwarps = gridDim.x * (kCoopThreads / 32);
+  __shared__ double red[kCoopThreads / 32][3];
   const int npairs = J.ne / 2;
   for (int sweep = 0; sweep < J.max_sweeps; ++sweep) {
     if (blockIdx.x == 0 && threadIdx.x == 0) J.rot[(sweep + 1) % 3] = 0u;
     for (int rd = 0; rd < J.ne - 1; ++rd) {
-      for (int k = gwarp; k < npairs; k += nwarps) {
+      for (int k = blockIdx.x; k < npairs; k += gridDim.x) {
         int i, j;
         circle_pair(J.ne, rd, k, i, j);
         if (i >= J.r || j >= J.r) continue;
         double* a = J.M + (size_t)i * J.L;
         double* b = J.M + (size_t)j * J.L;
         double al = 0.0, be = 0.0, ga = 0.0;
-        for (int t = lane; t < J.L; t += 32) {
+        for (int t = threadIdx.x; t < J.L; t += kCoopThreads) {
           const double x = __ldcg(a + t), y = __ldcg(b + t);
           al += x * x;
           be += y * y;
           ga += x * y;
         }
-        al = warp_sum(al);
-        be = warp_sum(be);
-        ga = warp_sum(ga);
+        block_sum3(al, be, ga, red);
         if (!(ga != 0.0) || !(fabs(ga) > J.tol * sqrt(al) * sqrt(be))) continue;
         const double zeta = (be - al) / (2.0 * ga);
         double t;
@@ -109,19 +128,19 @@ __global__ void __launch_bounds__(kCoopThreads) jacobi_coop_kernel(CoopJacobi J)
         }
         const double c = 1.0 / sqrt(1.0 + t * t);
         const double s = c * t;
-        for (int u = lane; u < J.L; u += 32) {
+        for (int u = threadIdx.x; u < J.L; u += kCoopThreads) {
           const double x = __ldcg(a + u), y = __ldcg(b + u);
           __stcg(a + u, c * x - s * y);
           __stcg(b + u, s * x + c * y);
         }
         double* wa = J.W + (size_t)i * J.r;
         double* wb = J.W + (size_t)j * J.r;
-        for (int u = lane; u < J.r; u += 32) {
+        for (int u = threadIdx.x; u < J.r; u += kCoopThreads) {
           const double x = __ldcg(wa + u), y = __ldcg(wb + u);
           __stcg(wa + u, c * x - s * y);
           __stcg(wb + u, s * x + c * y);
         }
-        if (lane == 0) atomicAdd(J.rot + (sweep % 3), 1u);
+        if (threadIdx.x == 0) atomicAdd(J.rot + (sweep % 3), 1u);
       }
       if (!coop_barrier(J)) return;
     }
@@ -271,8 +290,7 @@ void svd_jacobi_coop(int rows, int cols, const double* A, int lda, double* U, in
   }
   FPLS_REQUIRE(max_blocks_per_sm > 0, "svd_jacobi_coop: kernel cannot be resident");
   const int ne = r + (r & 1);
-  const int warps_needed = ne / 2;
-  const int blocks_needed = ceil_div(warps_needed, kCoopThreads / 32);
+  const int blocks_needed = ne / 2;
   const int grid = std::max(1, std::min(blocks_needed, max_blocks_per_sm * ctx.sm_count));
 
   CoopJacobi J;
@@ -305,6 +323,15 @@ void svd_jacobi_coop(int rows, int cols, const double* A, int lda, double* U, in
       M, W, L, r, nrm, order, tall, U, ldu, s, V, ldv); ::fpls::note_launch();
   complete_null_kernel<<<1, 512, 0, ctx.stream>>>(L, r, s, tall, U, ldu, V, ldv); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+}
+
+void eig_psd_desc(int l, const double* G, int ldg, double* evals, double* V, int ldv) {
+  if (l <= 64) {
+    eig_sym_desc(l, G, ldg, evals, V, ldv);
+    return;
+  }
+  double* U = Context::get().arena.alloc_n<double>((size_t)l * l);
+  svd_jacobi_coop(l, l, G, ldg, U, l, evals, V, ldv);
 }
 
 }  // namespace fpls

@@ -68,6 +68,10 @@ SIGNATURES = {
     "fpls_plssvd_label_aware": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _I, _I, _I, _I, _I,
                                  _IP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S],
                                 ctypes.c_int),
+    "fpls_label_aware_cknn": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, ctypes.c_void_p, _I, _I, _I, _I,
+                               _I, _I, _I, _I, _D, _D, _I, _I, _IP, _DP, _C, _S], ctypes.c_int),
+    "fpls_label_aware_cknn_resident": ([_I, _IP, _I, _I, _I, _I, _I, _I, _I, _I, _I, _D, _D, _I, _I,
+                                        _IP, _DP, _C, _S], ctypes.c_int),
     "fpls_candidate_scores": ([_DP, _I, _I, _DP, _DP, _C, _S], ctypes.c_int),
     "fpls_candidate_centroids": ([_DP, _I, _I, _IP, _I, _DP, _C, _S], ctypes.c_int),
     "fpls_candidate_knn_predict": ([_DP, _I, _DP, _I, _I, _IP, _DP, _I, _DP, _I, _I, _I, _D, _D,
@@ -627,3 +631,35 @@ def plssvd_label_aware(X, y_codes, m, ncomp, scaling=1, svd_method=3, oversample
     if keep_scores:
         out["Ttrain"] = T
     return out
+
+
+def _knn_out(ntest, m, top_k):
+    tk = max(1, min(int(top_k), int(m)))
+    return np.zeros((ntest, tk), dtype=np.int32, order="F"), _out(ntest, tk)
+
+
+def label_aware_cknn(Xtrain, y_codes, m, Xtest, ncomp, scaling=1, svd_method=4, oversample=10,
+                     power_iters=1, seed=1, knn_k=10, tau=0.2, alpha=0.75, top_m=20, top_k=5):
+    """Label-aware PLSSVD + candidate-kNN on host buffers (FP32 or FP64, same type)."""
+    f32 = np.asarray(Xtrain).dtype == np.float32
+    dt = np.float32 if f32 else np.float64
+    Xtr = np.asfortranarray(Xtrain, dtype=dt)
+    Xte = np.asfortranarray(Xtest, dtype=dt)
+    y = np.ascontiguousarray(y_codes, dtype=np.int32)
+    ti, ts = _knn_out(Xte.shape[0], m, top_k)
+    _call("fpls_label_aware_cknn", Xtr.ctypes.data_as(ctypes.c_void_p), int(f32), Xtr.shape[0],
+          Xtr.shape[1], _p(y), int(m), Xte.ctypes.data_as(ctypes.c_void_p), Xte.shape[0], int(ncomp),
+          int(scaling), int(svd_method), int(oversample), int(power_iters), int(seed), int(knn_k),
+          float(tau), float(alpha), int(top_m), int(top_k), _p(ti), _p(ts))
+    return dict(top_index=ti, top_score=ts)
+
+
+def label_aware_cknn_resident(xtrain_handle, y_codes, m, xtest_handle, ntest, ncomp, scaling=1,
+                              svd_method=4, oversample=10, power_iters=1, seed=1, knn_k=10, tau=0.2,
+                              alpha=0.75, top_m=20, top_k=5):
+    y = np.ascontiguousarray(y_codes, dtype=np.int32)
+    ti, ts = _knn_out(ntest, m, top_k)
+    _call("fpls_label_aware_cknn_resident", int(xtrain_handle), _p(y), int(m), int(xtest_handle),
+          int(ncomp), int(scaling), int(svd_method), int(oversample), int(power_iters), int(seed),
+          int(knn_k), float(tau), float(alpha), int(top_m), int(top_k), _p(ti), _p(ts))
+    return dict(top_index=ti, top_score=ts)

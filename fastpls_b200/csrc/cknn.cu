@@ -24,6 +24,7 @@
 
 #include "blas_f64.cuh"
 #include "capi_util.cuh"
+#include "cknn.cuh"
 #include "context.cuh"
 
 namespace fpls {
@@ -418,10 +419,138 @@ ClassRows group_rows_by_class(const double* dT, int n, int k, const int* dcodes,
 }
 
 }  // namespace
+
+using capi::upload;
+
+void candidate_scores_device(const double* dT, int n, int k, const double* dCk, double* dTn) {
+  Context& ctx = Context::get();
+  const double* src = dT;
+  if (dCk) {
+    double* prod = ctx.arena.alloc_n<double>((size_t)n * k);
+    gemm(false, false, n, k, k, 1.0, dT, n, dCk, k, 0.0, prod, n);
+    src = prod;
+  }
+  row_l2_kernel<<<ceil_div(n, 128), 128, 0, ctx.stream>>>(src, n, k, dTn); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+void candidate_centroids_device(const double* dTn, int n, int k, const int* dy, int C, double* dCent) {
+  Context& ctx = Context::get();
+  ClassRows cr = group_rows_by_class(dTn, n, k, dy, C);
+  centroid_kernel<<<C, 256, 0, ctx.stream>>>(cr.Ts, k, cr.d_offs, C, dCent); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+void candidate_knn_predict_device(const double* dTt, int ntest, const double* dTr, int ntrain, int kdim,
+                                  const int* dy, const double* dC, int C, const double* dbias, int top_k,
+                                  int top_m, int knn_k, double tau, double alpha, int* d_ti, double* d_ts) {
+  Context& ctx = Context::get();
+  const int tk = std::max(1, std::min(top_k, C));
+  const int tm = std::max(tk, std::min(std::max(1, top_m), C));
+  const int use_k = std::max(1, std::min(std::max(1, knn_k), kKnnMax));
+  const double tau_e = (std::isfinite(tau) && tau > 0.0) ? tau : 0.2;
+  const double alpha_e = std::isfinite(alpha) ? alpha : 0.5;
+  const long long npairs = (long long)ntest * tm;
+  FPLS_REQUIRE(npairs < (1ll << 31), "candidate-kNN: ntest * top_m must stay below 2^31");
+  double* bias0 = nullptr;
+  if (!dbias) {
+    bias0 = ctx.arena.alloc_n<double>(C);
+    fill(bias0, C, 0.0);
+    dbias = bias0;
+  }
+  // base scores and candidate classes
+  double* base = ctx.arena.alloc_n<double>((size_t)ntest * C);
+  gemm(false, true, ntest, C, kdim, 1.0, dTt, ntest, dC, C, 0.0, base, ntest);
+  int* cand = ctx.arena.alloc_n<int>((size_t)npairs);
+  double* cbase = ctx.arena.alloc_n<double>((size_t)npairs);
+  select_candidates_kernel<<<ceil_div(ntest, 128), 128, 0, ctx.stream>>>(base, ntest, C, tm, cand, cbase); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+
+  // training rows grouped by class (row-major), test rows row-major
+  ClassRows cr = group_rows_by_class(dTr, ntrain, kdim, dy, C);
+  double* Tq = ctx.arena.alloc_n<double>((size_t)ntest * kdim);
+  {
+    dim3 grid(ceil_div(ntest, 32), ceil_div(kdim, 32));
+    transpose_scatter_kernel<<<grid, dim3(32, 8), 0, ctx.stream>>>(dTt, ntest, kdim, nullptr, Tq); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+  }
+
+  // (row, candidate) pairs grouped by class
+  int* pcount = ctx.arena.alloc_n<int>(C);
+  int* pcursor = ctx.arena.alloc_n<int>(C);
+  fill_int_kernel<<<ceil_div(C, 256), 256, 0, ctx.stream>>>(pcount, C, 0); ::fpls::note_launch();
+  fill_int_kernel<<<ceil_div(C, 256), 256, 0, ctx.stream>>>(pcursor, C, 0); ::fpls::note_launch();
+  const int g = std::max(1, std::min(ceil_div(npairs, 256), 8 * ctx.sm_count));
+  pair_hist_kernel<<<g, 256, 0, ctx.stream>>>(cand, npairs, C, pcount); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  std::vector<int> hp(C);
+  d2h(hp.data(), pcount, C * sizeof(int));
+  ctx.sync();
+  std::vector<int> poffs(C + 1, 0), chunk_rows(C, 0), nchunks(C, 0);
+  std::vector<long long> part_base(C, 0);
+  std::vector<KnnItem> items;
+  long long part_total = 0;
+  for (int c = 0; c < C; ++c) {
+    poffs[c + 1] = poffs[c] + hp[c];
+    const int rows = cr.offs[c + 1] - cr.offs[c];
+    int S = 0, cr_rows = 0;
+    if (rows > 0) {
+      S = std::min(kMaxChunks, std::max(1, ceil_div(rows, kMinChunkRows)));
+      cr_rows = ceil_div(ceil_div(rows, S), kTileN) * kTileN;
+      S = ceil_div(rows, cr_rows);
+    }
+    chunk_rows[c] = cr_rows;
+    nchunks[c] = S;
+    part_base[c] = part_total;
+    part_total += (long long)hp[c] * S * use_k;
+    if (rows > 0 && hp[c] > 0) {
+      const int tiles = ceil_div(hp[c], kTileM);
+      for (int t = 0; t < tiles; ++t)
+        for (int s = 0; s < S; ++s) items.push_back(KnnItem{c, t, s, 0});
+    }
+  }
+  const long long total_pairs = poffs[C];
+  int* pairs = ctx.arena.alloc_n<int>((size_t)std::max<long long>(total_pairs, 1));
+  int* d_poffs = ctx.arena.alloc_n<int>(C + 1);
+  h2d(d_poffs, poffs.data(), (C + 1) * sizeof(int));
+  pair_scatter_kernel<<<g, 256, 0, ctx.stream>>>(cand, npairs, C, d_poffs, pcursor, pairs); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+
+  KnnClassInfo ci;
+  ci.row_offs = cr.d_offs;
+  ci.pair_offs = d_poffs;
+  ci.chunk_rows = upload(chunk_rows.data(), C);
+  ci.nchunks = upload(nchunks.data(), C);
+  ci.part_base = upload(part_base.data(), C);
+  double* part = ctx.arena.alloc_n<double>((size_t)std::max<long long>(part_total, 1));
+  double* cscore = ctx.arena.alloc_n<double>((size_t)npairs);
+  if (!items.empty()) {
+    const KnnItem* ditems = upload(items.data(), items.size());
+    const size_t smem = sizeof(double) * (2 * kBK * (kTileM + kPad) + 2 * kBK * (kTileN + kPad) +
+                                          kTileM * (kTileN + 1) + (size_t)kKnnMax * kTileThreads);
+    static bool attr_set = false;
+    if (!attr_set) {
+      FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr_set = true;
+    }
+    FPLS_REQUIRE(items.size() < (1u << 31), "candidate-kNN: too many work items");
+    knn_tile_kernel<<<(unsigned)items.size(), kTileThreads, smem, ctx.stream>>>(
+        ditems, ci, pairs, ntest, Tq, cr.Ts, kdim, use_k, part); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+  }
+  fill(cscore, (size_t)npairs, -INFINITY);
+  if (total_pairs > 0) {
+    knn_merge_kernel<<<ceil_div(total_pairs, 128), 128, 0, ctx.stream>>>(
+        pairs, total_pairs, cand, cbase, ci, part, use_k, tau_e, alpha_e, dbias, cscore); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+  }
+  knn_rerank_kernel<<<ceil_div(ntest, 128), 128, 0, ctx.stream>>>(cand, cscore, ntest, C, tm, tk, d_ti, d_ts); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
 }  // namespace fpls
 
 using namespace fpls;
-using capi::upload;
 
 extern "C" {
 
@@ -432,16 +561,9 @@ int fpls_candidate_scores(const double* T, int n, int k, const double* Ck, doubl
     Context& ctx = Context::get();
     ctx.begin_call();
     const double* dT = upload(T, (size_t)n * k);
-    const double* src = dT;
-    if (Ck) {
-      const double* dC = upload(Ck, (size_t)k * k);
-      double* prod = ctx.arena.alloc_n<double>((size_t)n * k);
-      gemm(false, false, n, k, k, 1.0, dT, n, dC, k, 0.0, prod, n);
-      src = prod;
-    }
+    const double* dC = Ck ? upload(Ck, (size_t)k * k) : nullptr;
     double* out = ctx.arena.alloc_n<double>((size_t)n * k);
-    row_l2_kernel<<<ceil_div(n, 128), 128, 0, ctx.stream>>>(src, n, k, out); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
+    candidate_scores_device(dT, n, k, dC, out);
     d2h(Tn, out, (size_t)n * k * sizeof(double));
     ctx.sync();
   });
@@ -456,10 +578,8 @@ int fpls_candidate_centroids(const double* Tn, int n, int k, const int* y_codes,
     ctx.begin_call();
     const double* dT = upload(Tn, (size_t)n * k);
     const int* dy = upload(y_codes, n);
-    ClassRows cr = group_rows_by_class(dT, n, k, dy, n_classes);
     double* dC = ctx.arena.alloc_n<double>((size_t)n_classes * k);
-    centroid_kernel<<<n_classes, 256, 0, ctx.stream>>>(cr.Ts, k, cr.d_offs, n_classes, dC); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
+    candidate_centroids_device(dT, n, k, dy, n_classes, dC);
     d2h(centroids, dC, (size_t)n_classes * k * sizeof(double));
     ctx.sync();
   });
@@ -477,111 +597,15 @@ int fpls_candidate_knn_predict(const double* Ttest_norm, int ntest, const double
     ctx.begin_call();
     const int C = n_classes;
     const int tk = std::max(1, std::min(top_k, C));
-    const int tm = std::max(tk, std::min(std::max(1, top_m), C));
-    const int use_k = std::max(1, std::min(std::max(1, knn_k), kKnnMax));
-    const double tau_e = (std::isfinite(tau) && tau > 0.0) ? tau : 0.2;
-    const double alpha_e = std::isfinite(alpha) ? alpha : 0.5;
-    const long long npairs = (long long)ntest * tm;
-    FPLS_REQUIRE(npairs < (1ll << 31), "candidate-kNN: ntest * top_m must stay below 2^31");
-
     const double* dTt = upload(Ttest_norm, (size_t)ntest * kdim);
     const double* dTr = upload(Ttrain_norm, (size_t)ntrain * kdim);
     const int* dy = upload(y_codes, ntrain);
     const double* dC = upload(centroids, (size_t)C * kdim);
-    double* dbias = ctx.arena.alloc_n<double>(C);
-    if (candidate_bias) h2d(dbias, candidate_bias, C * sizeof(double));
-    else fill(dbias, C, 0.0);
-
-    // base scores and candidate classes
-    double* base = ctx.arena.alloc_n<double>((size_t)ntest * C);
-    gemm(false, true, ntest, C, kdim, 1.0, dTt, ntest, dC, C, 0.0, base, ntest);
-    int* cand = ctx.arena.alloc_n<int>((size_t)npairs);
-    double* cbase = ctx.arena.alloc_n<double>((size_t)npairs);
-    select_candidates_kernel<<<ceil_div(ntest, 128), 128, 0, ctx.stream>>>(base, ntest, C, tm, cand, cbase); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
-
-    // training rows grouped by class (row-major), test rows row-major
-    ClassRows cr = group_rows_by_class(dTr, ntrain, kdim, dy, C);
-    double* Tq = ctx.arena.alloc_n<double>((size_t)ntest * kdim);
-    {
-      dim3 grid(ceil_div(ntest, 32), ceil_div(kdim, 32));
-      transpose_scatter_kernel<<<grid, dim3(32, 8), 0, ctx.stream>>>(dTt, ntest, kdim, nullptr, Tq); ::fpls::note_launch();
-      FPLS_CHECK_LAUNCH();
-    }
-
-    // (row, candidate) pairs grouped by class
-    int* pcount = ctx.arena.alloc_n<int>(C);
-    int* pcursor = ctx.arena.alloc_n<int>(C);
-    fill_int_kernel<<<ceil_div(C, 256), 256, 0, ctx.stream>>>(pcount, C, 0); ::fpls::note_launch();
-    fill_int_kernel<<<ceil_div(C, 256), 256, 0, ctx.stream>>>(pcursor, C, 0); ::fpls::note_launch();
-    const int g = std::max(1, std::min(ceil_div(npairs, 256), 8 * ctx.sm_count));
-    pair_hist_kernel<<<g, 256, 0, ctx.stream>>>(cand, npairs, C, pcount); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
-    std::vector<int> hp(C);
-    d2h(hp.data(), pcount, C * sizeof(int));
-    ctx.sync();
-    std::vector<int> poffs(C + 1, 0), chunk_rows(C, 0), nchunks(C, 0);
-    std::vector<long long> part_base(C, 0);
-    std::vector<KnnItem> items;
-    long long part_total = 0;
-    for (int c = 0; c < C; ++c) {
-      poffs[c + 1] = poffs[c] + hp[c];
-      const int rows = cr.offs[c + 1] - cr.offs[c];
-      int S = 0, cr_rows = 0;
-      if (rows > 0) {
-        S = std::min(kMaxChunks, std::max(1, ceil_div(rows, kMinChunkRows)));
-        cr_rows = ceil_div(ceil_div(rows, S), kTileN) * kTileN;
-        S = ceil_div(rows, cr_rows);
-      }
-      chunk_rows[c] = cr_rows;
-      nchunks[c] = S;
-      part_base[c] = part_total;
-      part_total += (long long)hp[c] * S * use_k;
-      if (rows > 0 && hp[c] > 0) {
-        const int tiles = ceil_div(hp[c], kTileM);
-        for (int t = 0; t < tiles; ++t)
-          for (int s = 0; s < S; ++s) items.push_back(KnnItem{c, t, s, 0});
-      }
-    }
-    const long long total_pairs = poffs[C];
-    int* pairs = ctx.arena.alloc_n<int>((size_t)std::max<long long>(total_pairs, 1));
-    int* d_poffs = ctx.arena.alloc_n<int>(C + 1);
-    h2d(d_poffs, poffs.data(), (C + 1) * sizeof(int));
-    pair_scatter_kernel<<<g, 256, 0, ctx.stream>>>(cand, npairs, C, d_poffs, pcursor, pairs); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
-
-    KnnClassInfo ci;
-    ci.row_offs = cr.d_offs;
-    ci.pair_offs = d_poffs;
-    ci.chunk_rows = upload(chunk_rows.data(), C);
-    ci.nchunks = upload(nchunks.data(), C);
-    ci.part_base = upload(part_base.data(), C);
-    double* part = ctx.arena.alloc_n<double>((size_t)std::max<long long>(part_total, 1));
-    double* cscore = ctx.arena.alloc_n<double>((size_t)npairs);
-    if (!items.empty()) {
-      const KnnItem* ditems = upload(items.data(), items.size());
-      const size_t smem = sizeof(double) * (2 * kBK * (kTileM + kPad) + 2 * kBK * (kTileN + kPad) +
-                                            kTileM * (kTileN + 1) + (size_t)kKnnMax * kTileThreads);
-      static bool attr_set = false;
-      if (!attr_set) {
-        FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-      }
-      FPLS_REQUIRE(items.size() < (1u << 31), "candidate-kNN: too many work items");
-      knn_tile_kernel<<<(unsigned)items.size(), kTileThreads, smem, ctx.stream>>>(
-          ditems, ci, pairs, ntest, Tq, cr.Ts, kdim, use_k, part); ::fpls::note_launch();
-      FPLS_CHECK_LAUNCH();
-    }
-    fill(cscore, (size_t)npairs, -INFINITY);
-    if (total_pairs > 0) {
-      knn_merge_kernel<<<ceil_div(total_pairs, 128), 128, 0, ctx.stream>>>(
-          pairs, total_pairs, cand, cbase, ci, part, use_k, tau_e, alpha_e, dbias, cscore); ::fpls::note_launch();
-      FPLS_CHECK_LAUNCH();
-    }
+    const double* dbias = candidate_bias ? upload(candidate_bias, C) : nullptr;
     int* d_ti = ctx.arena.alloc_n<int>((size_t)ntest * tk);
     double* d_ts = ctx.arena.alloc_n<double>((size_t)ntest * tk);
-    knn_rerank_kernel<<<ceil_div(ntest, 128), 128, 0, ctx.stream>>>(cand, cscore, ntest, C, tm, tk, d_ti, d_ts); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
+    candidate_knn_predict_device(dTt, ntest, dTr, ntrain, kdim, dy, dC, C, dbias, top_k, top_m, knn_k,
+                                 tau, alpha, d_ti, d_ts);
     d2h(top_index, d_ti, (size_t)ntest * tk * sizeof(int));
     d2h(top_score, d_ts, (size_t)ntest * tk * sizeof(double));
     ctx.sync();

@@ -16,6 +16,7 @@
 
 #include "blas_f64.cuh"
 #include "capi_util.cuh"
+#include "cknn.cuh"
 #include "context.cuh"
 #include "label_aware.cuh"
 #include "linalg_small.cuh"
@@ -168,6 +169,20 @@ __global__ void la_crosscov_kernel(double* cs, int p, int m, const int* counts, 
     for (int c = threadIdx.x; c < m; c += blockDim.x) mY[c] = (double)counts[c] / n;
 }
 
+// out (n x p, column-major FP64) = (X - mX) / vX as the model's scaling.
+template <typename T>
+__global__ void center_to_f64_kernel(const T* __restrict__ X, int n, int p, const double* __restrict__ mX,
+                                     const double* __restrict__ vX, int scaling, double* __restrict__ out) {
+  const size_t total = (size_t)n * p;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int j = static_cast<int>(t / n);
+    double v = static_cast<double>(X[t]);
+    if (scaling < 3) v -= mX[j];
+    if (scaling == 2) v /= vX[j];
+    out[t] = v;
+  }
+}
+
 __global__ void diag_rhs_kernel(const double* d, int k, double* D) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < k * k; t += gridDim.x * blockDim.x)
     D[t] = (t % k == t / k) ? d[t % k] : 0.0;
@@ -301,6 +316,47 @@ LabelAwareFit label_aware_fit(const void* dX, bool f32, int n, int p, const int*
   return f;
 }
 
+
+// Label-aware PLSSVD fit, candidate-kNN fit in the PLSSVD prediction-latent
+// score space (T C_k, row-normalised; R/main.R:700-730, 795-873) and
+// candidate-kNN prediction of the test rows (R/main.R:875-950), all on
+// device buffers.  d_ti / d_ts: ntest x max(1, min(top_k, m)).
+void label_aware_cknn_device(const void* dX, const void* dXtest, bool f32, int n, int ntest, int p,
+                             const int* dy, const int* y_host, int m, int ncomp, int scaling, int svd_method,
+                             int oversample, int power_iters, unsigned int seed, int knn_k, double tau,
+                             double alpha, int top_m, int top_k, int* d_ti, double* d_ts) {
+  Context& ctx = Context::get();
+  const std::vector<int> nc = cap_plssvd_ncomp(&ncomp, 1, n, p, m, nullptr);
+  LabelAwareFit f = label_aware_fit(dX, f32, n, p, dy, y_host, m, nc, scaling, svd_method, oversample,
+                                    power_iters, seed);
+  PhaseTimer pt("candidate-kNN on label-aware scores");
+  const int K = f.K;
+  double* Tn = ctx.arena.alloc_n<double>((size_t)n * K);
+  candidate_scores_device(f.T, n, K, f.C, Tn);
+  double* cent = ctx.arena.alloc_n<double>((size_t)m * K);
+  candidate_centroids_device(Tn, n, K, dy, m, cent);
+  pt.mark("train scores + centroids");
+  double* Xc = ctx.arena.alloc_n<double>((size_t)ntest * p);
+  const int g = std::max(1, std::min(ceil_div((long long)ntest * p, 256), 8 * ctx.sm_count));
+  if (f32)
+    center_to_f64_kernel<float><<<g, 256, 0, ctx.stream>>>(static_cast<const float*>(dXtest), ntest, p, f.mX,
+                                                          f.vX, scaling, Xc);
+  else
+    center_to_f64_kernel<double><<<g, 256, 0, ctx.stream>>>(static_cast<const double*>(dXtest), ntest, p, f.mX,
+                                                           f.vX, scaling, Xc);
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  double* Tt = ctx.arena.alloc_n<double>((size_t)ntest * K);
+  gemm(false, false, ntest, K, p, 1.0, Xc, ntest, f.R, p, 0.0, Tt, ntest);
+  double* Ttn = ctx.arena.alloc_n<double>((size_t)ntest * K);
+  candidate_scores_device(Tt, ntest, K, f.C, Ttn);
+  pt.mark("test scores");
+  candidate_knn_predict_device(Ttn, ntest, Tn, n, K, dy, cent, m, nullptr, top_k, top_m, knn_k, tau, alpha,
+                               d_ti, d_ts);
+  pt.mark("candidate-kNN predict");
+  pt.report();
+}
+
 }  // namespace fpls
 
 using namespace fpls;
@@ -345,6 +401,79 @@ int fpls_plssvd_label_aware(const void* X, int x_is_float32, int n, int p, const
     d2h(mY, f.mY, m * sizeof(double));
     if (s) d2h(s, f.d, K * sizeof(double));
     if (Ttrain) d2h(Ttrain, f.T, (size_t)n * K * sizeof(double));
+    ctx.sync();
+  });
+}
+
+int fpls_label_aware_cknn(const void* Xtrain, int x_is_float32, int n, int p, const int* y_codes, int m,
+                          const void* Xtest, int ntest, int ncomp, int scaling, int svd_method,
+                          int oversample, int power_iters, int seed, int knn_k, double tau,
+                          double alpha, int top_m, int top_k, int* top_index, double* top_score,
+                          char* err, size_t errlen) {
+  return capi::guarded(err, errlen, [&] {
+    FPLS_REQUIRE(Xtrain && Xtest && y_codes && top_index && top_score, "label-aware cKNN: missing inputs");
+    FPLS_REQUIRE(n >= 1 && p >= 1 && m >= 2 && ntest >= 1,
+                 "label-aware PLSSVD requires non-empty X and at least two classes");
+    FPLS_REQUIRE(scaling >= 1 && scaling <= 3, "scaling must be 1, 2 or 3");
+    FPLS_REQUIRE(svd_method == kSvdExact || svd_method == kSvdCpuRsvd || svd_method == kSvdCudaRsvd,
+                 "label-aware PLSSVD: svd_method must be exact (3) or rsvd (4 / 5)");
+    FPLS_REQUIRE(std::isfinite(tau) && tau > 0.0, "candidate_tau must be positive");
+    FPLS_REQUIRE(std::isfinite(alpha), "candidate_alpha must be finite");
+    for (int i = 0; i < n; ++i)
+      FPLS_REQUIRE(y_codes[i] >= 1 && y_codes[i] <= m, "label-aware PLSSVD: class code outside 1..m");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const size_t es = x_is_float32 ? sizeof(float) : sizeof(double);
+    void* dX = ctx.arena.alloc_n<char>((size_t)n * p * es);
+    void* dXt = ctx.arena.alloc_n<char>((size_t)ntest * p * es);
+    h2d(dX, Xtrain, (size_t)n * p * es);
+    h2d(dXt, Xtest, (size_t)ntest * p * es);
+    const int* dy = upload(y_codes, n);
+    const int tk = std::max(1, std::min(top_k, m));
+    int* d_ti = ctx.arena.alloc_n<int>((size_t)ntest * tk);
+    double* d_ts = ctx.arena.alloc_n<double>((size_t)ntest * tk);
+    label_aware_cknn_device(dX, dXt, x_is_float32 != 0, n, ntest, p, dy, y_codes, m, ncomp, scaling,
+                            svd_method, oversample, power_iters, static_cast<unsigned int>(seed), knn_k,
+                            tau, alpha, top_m, top_k, d_ti, d_ts);
+    d2h(top_index, d_ti, (size_t)ntest * tk * sizeof(int));
+    d2h(top_score, d_ts, (size_t)ntest * tk * sizeof(double));
+    ctx.sync();
+  });
+}
+
+int fpls_label_aware_cknn_resident(int xtrain_handle, const int* y_codes, int m, int xtest_handle,
+                                   int ncomp, int scaling, int svd_method, int oversample,
+                                   int power_iters, int seed, int knn_k, double tau, double alpha,
+                                   int top_m, int top_k, int* top_index, double* top_score, char* err,
+                                   size_t errlen) {
+  return capi::guarded(err, errlen, [&] {
+    Context& ctx = Context::get();
+    const int nres = static_cast<int>(ctx.resident.size());
+    FPLS_REQUIRE(xtrain_handle >= 0 && xtrain_handle < nres && ctx.resident[xtrain_handle].ptr,
+                 "label-aware cKNN: unknown training handle");
+    FPLS_REQUIRE(xtest_handle >= 0 && xtest_handle < nres && ctx.resident[xtest_handle].ptr,
+                 "label-aware cKNN: unknown test handle");
+    const ResidentX tr = ctx.resident[xtrain_handle];
+    const ResidentX te = ctx.resident[xtest_handle];
+    FPLS_REQUIRE(tr.p == te.p && tr.f32 == te.f32, "label-aware cKNN: train / test matrices differ in p or type");
+    FPLS_REQUIRE(m >= 2, "label-aware PLSSVD requires non-empty X and at least two classes");
+    FPLS_REQUIRE(scaling >= 1 && scaling <= 3, "scaling must be 1, 2 or 3");
+    FPLS_REQUIRE(svd_method == kSvdExact || svd_method == kSvdCpuRsvd || svd_method == kSvdCudaRsvd,
+                 "label-aware PLSSVD: svd_method must be exact (3) or rsvd (4 / 5)");
+    FPLS_REQUIRE(std::isfinite(tau) && tau > 0.0, "candidate_tau must be positive");
+    FPLS_REQUIRE(std::isfinite(alpha), "candidate_alpha must be finite");
+    for (int i = 0; i < tr.n; ++i)
+      FPLS_REQUIRE(y_codes[i] >= 1 && y_codes[i] <= m, "label-aware PLSSVD: class code outside 1..m");
+    ctx.begin_call();
+    const int* dy = upload(y_codes, tr.n);
+    const int tk = std::max(1, std::min(top_k, m));
+    int* d_ti = ctx.arena.alloc_n<int>((size_t)te.n * tk);
+    double* d_ts = ctx.arena.alloc_n<double>((size_t)te.n * tk);
+    label_aware_cknn_device(tr.ptr, te.ptr, tr.f32, tr.n, te.n, tr.p, dy, y_codes, m, ncomp, scaling,
+                            svd_method, oversample, power_iters, static_cast<unsigned int>(seed), knn_k,
+                            tau, alpha, top_m, top_k, d_ti, d_ts);
+    d2h(top_index, d_ti, (size_t)te.n * tk * sizeof(int));
+    d2h(top_score, d_ts, (size_t)te.n * tk * sizeof(double));
     ctx.sync();
   });
 }

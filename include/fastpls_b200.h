@@ -251,6 +251,27 @@ int fpls_plssvd_label_aware(const void* X, int x_is_float32, int n, int p, const
                             double* mY, double* s, double* Ttrain, int* max_rank, char* err,
                             size_t errlen);
 
+/* Label-aware PLSSVD + candidate-kNN, end to end on the device: the
+ * fpls_plssvd_label_aware fit at one ncomp, training scores T C_k row-
+ * normalised, class centroids, test scores ((Xtest - mX)/vX) R C_k
+ * row-normalised, then fpls_candidate_knn_predict.  Xtest has the same type
+ * and p as Xtrain; top_index / top_score are ntest x max(1, min(top_k, m)).
+ * Composes pls(method = "simpls") on the label-aware route (R/main.R:3281-3302),
+ * .fit_candidate_knn (R/main.R:795-873) and .candidate_knn_predictions
+ * (R/main.R:875-950); no .Call counterpart. */
+int fpls_label_aware_cknn(const void* Xtrain, int x_is_float32, int n, int p, const int* y_codes, int m,
+                          const void* Xtest, int ntest, int ncomp, int scaling, int svd_method,
+                          int oversample, int power_iters, int seed, int knn_k, double tau,
+                          double alpha, int top_m, int top_k, int* top_index, double* top_score,
+                          char* err, size_t errlen);
+
+/* The same on matrices registered with fpls_x_upload (training rows, test rows). */
+int fpls_label_aware_cknn_resident(int xtrain_handle, const int* y_codes, int m, int xtest_handle,
+                                   int ncomp, int scaling, int svd_method, int oversample,
+                                   int power_iters, int seed, int knn_k, double tau, double alpha,
+                                   int top_m, int top_k, int* top_index, double* top_score, char* err,
+                                   size_t errlen);
+
 /* Candidate-kNN score space: Tn = row_l2(T Ck) (Ck k x k, or null for T
  * itself), T n x k column-major; zero row norms are replaced by 1.  Replaces
  * the R-side .candidate_score_space + .candidate_row_l2 arithmetic

@@ -111,3 +111,43 @@ def test_label_aware_scores_and_errors(lib):
     bad[0] = 6
     with pytest.raises(lib.FastPLSError):
         lib.plssvd_label_aware(X, bad, 5, [2])
+
+
+def _oracle_pipeline(X, y, m, Xtest, ncomp, svd_method, knn_k, tau, alpha, top_m, top_k, **kw):
+    from oracle import cknn as ok
+    fit = ola.label_aware_plssvd(X, y, m, [ncomp], svd_method=svd_method, **kw)
+    C = fit["C_latent"][:, :, 0]
+    T = ((X - fit["mX"]) / fit["vX"]) @ fit["R"]
+    Tn = ok.row_l2(T @ C)
+    cents = ok.centroids(Tn, y, m)
+    Tt = ok.row_l2((((Xtest - fit["mX"]) / fit["vX"]) @ fit["R"]) @ C)
+    return ok.candidate_knn_predict(Tt, Tn, y, cents, top_k=top_k, top_m=top_m, knn_k=knn_k,
+                                    tau=tau, alpha=alpha)
+
+
+@pytest.mark.parametrize("svd_method", [3, 4])
+def test_label_aware_cknn_pipeline(lib, svd_method):
+    X, y = _zipf_data(9, 7000, 48, 40)
+    Xte, _ = _zipf_data(10, 150, 48, 40)
+    kw = dict(knn_k=10, tau=0.2, alpha=0.75, top_m=20, top_k=5)
+    got = lib.label_aware_cknn(X, y, 40, Xte, 24, svd_method=svd_method, oversample=10,
+                               power_iters=1, seed=3, **kw)
+    extra = {} if svd_method == 3 else dict(oversample=10, power_iters=1, seed=3)
+    ref = _oracle_pipeline(X, y, 40, Xte, 24, svd_method, **kw, **extra)
+    assert np.array_equal(got["top_index"], ref["top_index"])
+    assert np.max(np.abs(got["top_score"] - ref["top_score"])) < 1e-9
+
+
+def test_label_aware_cknn_resident_matches_host(lib):
+    X, y = _zipf_data(11, 5000, 64, 30)
+    Xte, _ = _zipf_data(12, 100, 64, 30)
+    X32, Xte32 = X.astype(np.float32), Xte.astype(np.float32)
+    host = lib.label_aware_cknn(X32, y, 30, Xte32, 16, svd_method=4, seed=2)
+    htr, hte = lib.x_upload(X32), lib.x_upload(Xte32)
+    try:
+        res = lib.label_aware_cknn_resident(htr, y, 30, hte, Xte32.shape[0], 16, svd_method=4, seed=2)
+    finally:
+        lib.x_free(htr)
+        lib.x_free(hte)
+    assert np.array_equal(host["top_index"], res["top_index"])
+    assert np.max(np.abs(host["top_score"] - res["top_score"])) < 1e-12

@@ -18,6 +18,7 @@
 #include "../../include/fastpls_b200.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <limits>
 #include <vector>
@@ -114,46 +115,66 @@ __global__ void transpose_scatter_kernel(const double* __restrict__ A, int n, in
   }
 }
 
-// Class sums over class-contiguous row-major rows, then / max(count, 1), then
-// row L2 of the centroid (R/main.R:686-698).  One CTA per class, 32 columns x 8
-// row groups; the 8 partial sums are added in a fixed order.
-__global__ void centroid_kernel(const double* __restrict__ Ts, int k, const int* __restrict__ offs,
-                                int C, double* __restrict__ cent) {
-  __shared__ double part[8][33];
-  __shared__ double red[32];
-  const int c = blockIdx.x;
-  const int r0 = offs[c], r1 = offs[c + 1];
-  const int col = threadIdx.x & 31, grp = threadIdx.x >> 5;
-  const double cnt = (r1 > r0) ? (double)(r1 - r0) : 1.0;
-  double sq = 0.0;  // only meaningful in group 0
-  for (int j0 = 0; j0 < k; j0 += 32) {
-    const int j = j0 + col;
-    double s = 0.0;
-    if (j < k)
-      for (int r = r0 + grp; r < r1; r += 8) s += Ts[(size_t)r * k + j];
-    part[grp][col] = s;
-    __syncthreads();
-    if (grp == 0 && j < k) {
-      double t = 0.0;
-      for (int g = 0; g < 8; ++g) t += part[g][col];
-      t /= cnt;
-      cent[c + (size_t)j * C] = t;
-      sq += t * t;
+// Class sums of class-contiguous row-major rows (R/main.R:686-698): each CTA
+// walks a fixed range of rows, locating its first class by binary search in
+// the class offsets; each thread keeps up to 4 column sums in registers and
+// flushes them (atomicAdd into sums, C x k column-major) at class boundaries,
+// so a very large class is spread over many CTAs.
+constexpr int kCentCols = 4;
+__global__ void __launch_bounds__(128) class_rowsum_kernel(const double* __restrict__ Ts, int k, int nrows,
+                                                           const int* __restrict__ offs, int C, int rows,
+                                                           int col0, double* __restrict__ sums) {
+  const int s0 = blockIdx.x * rows;
+  const int s1 = min(nrows, s0 + rows);
+  int lo = 0, hi = C - 1;  // last class with offs[c] <= s0
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (offs[mid] <= s0) lo = mid; else hi = mid - 1;
+  }
+  int c = lo;
+  int cend = offs[c + 1];
+  int jc[kCentCols];
+  double acc[kCentCols];
+#pragma unroll
+  for (int u = 0; u < kCentCols; ++u) {
+    jc[u] = col0 + threadIdx.x + u * blockDim.x;
+    acc[u] = 0.0;
+  }
+  for (int r = s0; r < s1; ++r) {
+    if (r >= cend) {
+#pragma unroll
+      for (int u = 0; u < kCentCols; ++u) {
+        if (jc[u] < k) atomicAdd(sums + c + (size_t)jc[u] * C, acc[u]);
+        acc[u] = 0.0;
+      }
+      while (r >= offs[c + 1]) ++c;
+      cend = offs[c + 1];
     }
-    __syncthreads();
+    const double* row = Ts + (size_t)r * k;
+#pragma unroll
+    for (int u = 0; u < kCentCols; ++u)
+      if (jc[u] < k) acc[u] += __ldg(row + jc[u]);
   }
-  if (grp == 0) red[col] = sq;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int t = 0; t < 32; ++t) s += red[t];
-    double nr = sqrt(s);
-    if (!isfinite(nr) || nr == 0.0) nr = 1.0;
-    red[0] = nr;
+#pragma unroll
+  for (int u = 0; u < kCentCols; ++u)
+    if (jc[u] < k) atomicAdd(sums + c + (size_t)jc[u] * C, acc[u]);
+}
+
+// centroid = row_l2(sums / max(count, 1)); one thread per class.
+__global__ void centroid_finish_kernel(const double* __restrict__ sums, int k, const int* __restrict__ offs,
+                                       int C, double* __restrict__ cent) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  const int cnt = offs[c + 1] - offs[c];
+  const double den = cnt > 0 ? (double)cnt : 1.0;
+  double sq = 0.0;
+  for (int j = 0; j < k; ++j) {
+    const double t = sums[c + (size_t)j * C] / den;
+    sq += t * t;
   }
-  __syncthreads();
-  const double nr = red[0];
-  for (int j = threadIdx.x; j < k; j += blockDim.x) cent[c + (size_t)j * C] /= nr;
+  double nr = sqrt(sq);
+  if (!isfinite(nr) || nr == 0.0) nr = 1.0;
+  for (int j = 0; j < k; ++j) cent[c + (size_t)j * C] = (sums[c + (size_t)j * C] / den) / nr;
 }
 
 // ---------------------------------------------------------------- predict side
@@ -437,7 +458,18 @@ void candidate_scores_device(const double* dT, int n, int k, const double* dCk, 
 void candidate_centroids_device(const double* dTn, int n, int k, const int* dy, int C, double* dCent) {
   Context& ctx = Context::get();
   ClassRows cr = group_rows_by_class(dTn, n, k, dy, C);
-  centroid_kernel<<<C, 256, 0, ctx.stream>>>(cr.Ts, k, cr.d_offs, C, dCent); ::fpls::note_launch();
+  const int nvalid = cr.offs[C];
+  double* sums = ctx.arena.alloc_n<double>((size_t)C * k);
+  fill(sums, (size_t)C * k, 0.0);
+  if (nvalid > 0) {
+    const int rows = std::min(2048, std::max(64, ceil_div(nvalid, 4 * ctx.sm_count)));
+    for (int col0 = 0; col0 < k; col0 += 128 * kCentCols) {
+      class_rowsum_kernel<<<ceil_div(nvalid, rows), 128, 0, ctx.stream>>>(cr.Ts, k, nvalid, cr.d_offs, C, rows,
+                                                                         col0, sums); ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+    }
+  }
+  centroid_finish_kernel<<<ceil_div(C, 128), 128, 0, ctx.stream>>>(sums, k, cr.d_offs, C, dCent); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -458,6 +490,7 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
     fill(bias0, C, 0.0);
     dbias = bias0;
   }
+  PhaseTimer pt("candidate-kNN predict");
   // base scores and candidate classes
   double* base = ctx.arena.alloc_n<double>((size_t)ntest * C);
   gemm(false, true, ntest, C, kdim, 1.0, dTt, ntest, dC, C, 0.0, base, ntest);
@@ -467,6 +500,7 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
   FPLS_CHECK_LAUNCH();
 
   // training rows grouped by class (row-major), test rows row-major
+  pt.mark("base scores + candidates");
   ClassRows cr = group_rows_by_class(dTr, ntrain, kdim, dy, C);
   double* Tq = ctx.arena.alloc_n<double>((size_t)ntest * kdim);
   {
@@ -510,6 +544,12 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
     }
   }
   const long long total_pairs = poffs[C];
+  if (pt.enabled()) {
+    double work = 0.0;
+    for (int c = 0; c < C; ++c) work += (double)hp[c] * (cr.offs[c + 1] - cr.offs[c]);
+    std::fprintf(stderr, "[fastpls trace] candidate-kNN: %lld pairs, %.3e pair-rows (%.3e flop), %zu items\n",
+                 total_pairs, work, 2.0 * work * kdim, items.size());
+  }
   int* pairs = ctx.arena.alloc_n<int>((size_t)std::max<long long>(total_pairs, 1));
   int* d_poffs = ctx.arena.alloc_n<int>(C + 1);
   h2d(d_poffs, poffs.data(), (C + 1) * sizeof(int));
@@ -524,6 +564,7 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
   ci.part_base = upload(part_base.data(), C);
   double* part = ctx.arena.alloc_n<double>((size_t)std::max<long long>(part_total, 1));
   double* cscore = ctx.arena.alloc_n<double>((size_t)npairs);
+  pt.mark("class rows + pair lists");
   if (!items.empty()) {
     const KnnItem* ditems = upload(items.data(), items.size());
     const size_t smem = sizeof(double) * (2 * kBK * (kTileM + kPad) + 2 * kBK * (kTileN + kPad) +
@@ -538,6 +579,7 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
         ditems, ci, pairs, ntest, Tq, cr.Ts, kdim, use_k, part); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
+  pt.mark("similarity tiles");
   fill(cscore, (size_t)npairs, -INFINITY);
   if (total_pairs > 0) {
     knn_merge_kernel<<<ceil_div(total_pairs, 128), 128, 0, ctx.stream>>>(
@@ -546,6 +588,8 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
   }
   knn_rerank_kernel<<<ceil_div(ntest, 128), 128, 0, ctx.stream>>>(cand, cscore, ntest, C, tm, tk, d_ti, d_ts); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+  pt.mark("merge + rerank");
+  pt.report();
 }
 
 }  // namespace fpls

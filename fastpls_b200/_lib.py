@@ -40,6 +40,11 @@ SIGNATURES = {
                         ctypes.c_int),
     "fpls_pls_model2_fast": ([_DP, _I, _I, _DP, _I, _IP, _I, _I, _I, _I, _DP, _DP, _DP, _DP, _DP,
                               _DP, _DP, _DP, _IP, _C, _S], ctypes.c_int),
+    "fpls_pls_model1_xprod": ([_DP, _I, _I, _DP, _I, _IP, _I, _I, _I, _I, _I, _D, _I, _I, _IP, _DP,
+                               _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S],
+                              ctypes.c_int),
+    "fpls_pls_model2_fast_xprod": ([_DP, _I, _I, _DP, _I, _IP, _I, _I, _I, _I, _I, _DP, _DP, _DP,
+                                    _DP, _DP, _DP, _DP, _DP, _IP, _C, _S], ctypes.c_int),
     "fpls_pls_model2": ([_DP, _I, _I, _DP, _I, _IP, _I, _I, _I, _I, _I, _I, _D, _I, _DP, _DP,
                          _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S], ctypes.c_int),
     "fpls_predict_lowrank": ([_DP, _I, _I, _DP, _DP, _DP, _I, _DP, _I, _DP, _IP, _I, _DP, _DP,
@@ -177,7 +182,8 @@ def truncated_svd(A, k, svd_method=4, oversample=10, power_iters=1, svds_tol=0.0
 
 
 def pls_model1(X, Y, ncomp, scaling=1, fit=False, svd_method=4, oversample=10, power_iters=1,
-               svds_tol=0.0, seed=1, store_B=True):
+               svds_tol=0.0, seed=1, store_B=True, xprod=False):
+    """PLSSVD (fpls_pls_model1), or its matrix-free form with xprod=True."""
     X = _f64(X)
     Y = _f64(Y)
     n, p = X.shape
@@ -192,8 +198,13 @@ def pls_model1(X, Y, ncomp, scaling=1, fit=False, svd_method=4, oversample=10, p
                R2Y=np.zeros(L), singular_values=np.zeros(K0))
     nco = np.zeros(L, dtype=np.int32)
     keff = ctypes.c_int(0)
-    _call("fpls_pls_model1", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
-          int(svd_method), int(oversample), int(power_iters), float(svds_tol), int(seed), _p(nco),
+    if xprod:
+        head = ("fpls_pls_model1_xprod", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling),
+                int(bool(fit)), int(oversample), int(power_iters), float(svds_tol), int(seed), 3)
+    else:
+        head = ("fpls_pls_model1", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
+                int(svd_method), int(oversample), int(power_iters), float(svds_tol), int(seed))
+    _call(*head, _p(nco),
           _p(out["C_latent"]), _p(out["W_latent"]), _p(out["Q"]), _p(out["Ttrain"]), _p(out["R"]),
           _p(out["mX"]), _p(out["vX"]), _p(out["mY"]), _p(out["B"]), _p(out["Yfit"]),
           _p(out["R2Y"]), _p(out["singular_values"]), ctypes.byref(keff))
@@ -209,7 +220,8 @@ def pls_model1(X, Y, ncomp, scaling=1, fit=False, svd_method=4, oversample=10, p
     return out
 
 
-def pls_model2_fast(X, Y, ncomp, scaling=1, fit=False, seed=1, store_B=True):
+def pls_model2_fast(X, Y, ncomp, scaling=1, fit=False, seed=1, store_B=True, xprod=False):
+    """Fast SIMPLS (fpls_pls_model2_fast), or its matrix-free form with xprod=True."""
     X = _f64(X)
     Y = _f64(Y)
     n, p = X.shape
@@ -221,8 +233,11 @@ def pls_model2_fast(X, Y, ncomp, scaling=1, fit=False, seed=1, store_B=True):
                B=_out(p, m, L) if store_B else None, Yfit=_out(n, m, L) if fit else None,
                R2Y=np.zeros(L))
     ncmp = ctypes.c_int(0)
-    _call("fpls_pls_model2_fast", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
-          int(seed), _p(out["R"]), _p(out["Q"]), _p(out["mX"]), _p(out["vX"]), _p(out["mY"]),
+    head = (("fpls_pls_model2_fast_xprod", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling),
+             int(bool(fit)), int(seed), 3) if xprod else
+            ("fpls_pls_model2_fast", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
+             int(seed)))
+    _call(*head, _p(out["R"]), _p(out["Q"]), _p(out["mX"]), _p(out["vX"]), _p(out["mY"]),
           _p(out["B"]), _p(out["Yfit"]), _p(out["R2Y"]), ctypes.byref(ncmp))
     out.update(ncomp=nc, p=p, m=m, pls_method="simpls", n_components=ncmp.value,
                B_stored=bool(store_B), compact_prediction=not store_B)

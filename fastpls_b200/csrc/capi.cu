@@ -15,6 +15,7 @@
 #include "simpls_engine.cuh"
 #include "svd.cuh"
 #include "xop_split.cuh"
+#include "xprod.cuh"
 
 using namespace fpls;
 
@@ -151,11 +152,15 @@ int fpls_truncated_svd(const double* A, int rows, int cols, int k, int svd_metho
   });
 }
 
-int fpls_pls_model1(const double* X, int n, int p, const double* Y, int m, const int* ncomp, int L,
+}  // extern "C"
+
+namespace {
+
+int pls_model1_impl(const double* X, int n, int p, const double* Y, int m, const int* ncomp, int L,
                     int scaling, int fit, int svd_method, int oversample, int power_iters,
-                    double svds_tol, int seed, int* ncomp_out, double* C_latent, double* W_latent,
-                    double* Q, double* Ttrain, double* R, double* mX, double* vX, double* mY,
-                    double* B, double* Yfit, double* R2Y, double* s, int* k_eff, char* err,
+                    double svds_tol, int seed, bool xprod, int* ncomp_out, double* C_latent,
+                    double* W_latent, double* Q, double* Ttrain, double* R, double* mX, double* vX,
+                    double* mY, double* B, double* Yfit, double* R2Y, double* s, int* k_eff, char* err,
                     size_t errlen) {
   return guarded(err, errlen, [&] {
     FPLS_REQUIRE(n > 0 && p > 0 && m > 0, "pls_model1 requires non-empty X and Y");
@@ -181,6 +186,7 @@ int fpls_pls_model1(const double* X, int n, int p, const double* Y, int m, const
     opt.power_iters = power_iters;
     opt.svds_tol = svds_tol;
     opt.seed = static_cast<unsigned int>(seed);
+    opt.xprod = xprod;
     PlssvdOut o;
     o.C_latent = ctx.arena.alloc_n<double>((size_t)K0 * K0 * L);
     o.W_latent = ctx.arena.alloc_n<double>((size_t)K0 * m * L);
@@ -208,6 +214,84 @@ int fpls_pls_model1(const double* X, int n, int p, const double* Y, int m, const
     if (R2Y) std::copy(r2.begin(), r2.end(), R2Y);
     if (ncomp_out) std::copy(nc.begin(), nc.end(), ncomp_out);
     if (k_eff) *k_eff = keff;
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+int fpls_pls_model1(const double* X, int n, int p, const double* Y, int m, const int* ncomp, int L,
+                    int scaling, int fit, int svd_method, int oversample, int power_iters,
+                    double svds_tol, int seed, int* ncomp_out, double* C_latent, double* W_latent,
+                    double* Q, double* Ttrain, double* R, double* mX, double* vX, double* mY,
+                    double* B, double* Yfit, double* R2Y, double* s, int* k_eff, char* err,
+                    size_t errlen) {
+  return pls_model1_impl(X, n, p, Y, m, ncomp, L, scaling, fit, svd_method, oversample, power_iters,
+                         svds_tol, seed, false, ncomp_out, C_latent, W_latent, Q, Ttrain, R, mX, vX,
+                         mY, B, Yfit, R2Y, s, k_eff, err, errlen);
+}
+
+int fpls_pls_model1_xprod(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
+                          int L, int scaling, int fit, int oversample, int power_iters,
+                          double svds_tol, int seed, int xprod_precision, int* ncomp_out,
+                          double* C_latent, double* W_latent, double* Q, double* Ttrain, double* R,
+                          double* mX, double* vX, double* mY, double* B, double* Yfit, double* R2Y,
+                          double* s, int* k_eff, char* err, size_t errlen) {
+  if (xprod_precision != 3) {
+    capi::set_err(err, errlen, xprod_precision == 5
+                                   ? "xprod_precision 5 (IRLBA operator) is a CPU-only path in fastPLS"
+                                   : "xprod_precision values 1, 2, and 4 have been removed from fastPLS.");
+    return FPLS_ERR_ARGUMENT;
+  }
+  return pls_model1_impl(X, n, p, Y, m, ncomp, L, scaling, fit, kSvdCpuRsvd, oversample, power_iters,
+                         svds_tol, seed, true, ncomp_out, C_latent, W_latent, Q, Ttrain, R, mX, vX, mY,
+                         B, Yfit, R2Y, s, k_eff, err, errlen);
+}
+
+int fpls_pls_model2_fast_xprod(const double* X, int n, int p, const double* Y, int m,
+                               const int* ncomp, int L, int scaling, int fit, int seed,
+                               int xprod_precision, double* R, double* Q, double* mX, double* vX,
+                               double* mY, double* B, double* Yfit, double* R2Y, int* n_components,
+                               char* err, size_t errlen) {
+  if (xprod_precision != 3) {
+    capi::set_err(err, errlen, xprod_precision == 5
+                                   ? "xprod_precision 5 (IRLBA operator) is a CPU-only path in fastPLS"
+                                   : "xprod_precision values 1, 2, and 4 have been removed from fastPLS.");
+    return FPLS_ERR_ARGUMENT;
+  }
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && m > 0, "pls_model2_fast requires non-empty X and Y");
+    FPLS_REQUIRE(L >= 1 && ncomp, "ncomp must contain at least one value");
+    FPLS_REQUIRE(!(fit && !Yfit), "fit = 1 requires a Yfit buffer");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    std::vector<int> nc(ncomp, ncomp + L);
+    for (int& c : nc) c = std::max(1, c);
+    const int K = max_of(nc.data(), L);
+    double* dX = upload(X, (size_t)n * p);
+    double* dY = upload(Y, (size_t)n * m);
+    double* dmX = ctx.arena.alloc_n<double>(p);
+    double* dvX = ctx.arena.alloc_n<double>(p);
+    double* dmY = ctx.arena.alloc_n<double>(m);
+    center_scale_xy(dX, n, p, dY, m, scaling, dmX, dvX, dmY);
+    double* dR = ctx.arena.alloc_n<double>((size_t)p * K);
+    double* dQ = ctx.arena.alloc_n<double>((size_t)m * K);
+    double* dB = B ? ctx.arena.alloc_n<double>((size_t)p * m * L) : nullptr;
+    double* dYf = fit ? ctx.arena.alloc_n<double>((size_t)n * m * L) : nullptr;
+    std::vector<double> r2(L, 0.0);
+    const int done = simpls_xprod_fit(dX, n, p, dY, m, nc.data(), L, fit != 0,
+                                      static_cast<unsigned int>(seed), dmY, dR, dQ, dB, dYf, r2.data());
+    download(R, dR, (size_t)p * K);
+    download(Q, dQ, (size_t)m * K);
+    download(mX, dmX, p);
+    download(vX, dvX, p);
+    download(mY, dmY, m);
+    if (B) download(B, dB, (size_t)p * m * L);
+    if (fit) download(Yfit, dYf, (size_t)n * m * L);
+    ctx.sync();
+    if (R2Y) std::copy(r2.begin(), r2.end(), R2Y);
+    if (n_components) *n_components = done;
   });
 }
 

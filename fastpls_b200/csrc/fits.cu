@@ -3,6 +3,7 @@
 #include "fits.cuh"
 #include "linalg_small.cuh"
 #include "svd.cuh"
+#include "xprod.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -149,8 +150,11 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
                         int L, int K0, const FitOptions& opt, const double* mY, PlssvdOut out) {
   Context& ctx = Context::get();
   const int max_rank = std::min(n, std::min(p, m));
-  double* S = ctx.arena.alloc_n<double>((size_t)p * m);
-  gemm(true, false, p, m, n, 1.0, X, n, Y, n, 0.0, S, p);
+  double* S = nullptr;
+  if (!opt.xprod) {
+    S = ctx.arena.alloc_n<double>((size_t)p * m);
+    gemm(true, false, p, m, n, 1.0, X, n, Y, n, 0.0, S, p);
+  }
   int thr = 32;
   if (const char* e = std::getenv("FASTPLS_PLSSVD_SMALL_EXACT_MAX_RANK")) {
     char* endp = nullptr;
@@ -161,9 +165,12 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
   dzero(out.R, (size_t)p * K0 * sizeof(double));
   dzero(out.Q, (size_t)m * K0 * sizeof(double));
   dzero(out.s, (size_t)K0 * sizeof(double));
-  SvdResult sr = truncated_svd_device(S, p, m, p, K0, opt.svd_method, opt.oversample,
-                                      opt.power_iters, opt.seed, false, small_exact, out.R, p,
-                                      out.s, out.Q, m);
+  SvdResult sr = opt.xprod
+                     ? truncated_rsvd_crossprod_device(X, n, p, Y, m, K0, opt.oversample, opt.power_iters,
+                                                       opt.seed, small_exact, out.R, p, out.s, out.Q, m)
+                     : truncated_svd_device(S, p, m, p, K0, opt.svd_method, opt.oversample,
+                                            opt.power_iters, opt.seed, false, small_exact, out.R, p,
+                                            out.s, out.Q, m);
   int keff = std::min(K0, sr.rank);
   FPLS_REQUIRE(keff >= 1, "plssvd effective rank is < 1 after SVD");
   dzero(out.T, (size_t)n * K0 * sizeof(double));

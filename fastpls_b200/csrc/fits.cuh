@@ -15,6 +15,7 @@ struct FitOptions {
   double svds_tol = 0.0;
   unsigned int seed = 1;
   bool store_B = true;    // should_store_coefficients() decided by the caller
+  bool xprod = false;     // PLSSVD: matrix-free X^T Y (src/fastPLS.cpp:5518-5690)
 };
 
 // Centres / scales X (n x p) and Y (n x m) in place, writing mX, vX (p) and mY (m).

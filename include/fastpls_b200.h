@@ -80,6 +80,31 @@ int fpls_pls_model1(const double* X, int n, int p, const double* Y, int m, const
                     double* B, double* Yfit, double* R2Y, double* s, int* k_eff, char* err,
                     size_t errlen);
 
+/* Matrix-free PLSSVD: as fpls_pls_model1 with the rank-K SVD of XᵀY taken
+ * by the operator rSVD (sketch Ω m x l, A M = Xᵀ(Y M), Aᵀ M = Yᵀ(X M), QR,
+ * B = (XQ)ᵀY, svd_econ(B)); XᵀY is formed only for the exact fallback
+ * (min(n,p,m) <= 32, or l >= min(p, m)).  xprod_precision must be 3 (5 is
+ * the CPU-only IRLBA operator; 1, 2, 4 were removed).  Outputs as
+ * fpls_pls_model1.  Replaces _fastPLS_pls_model1_rsvd_xprod_precision
+ * (RcppExports.cpp:628; fastPLS.cpp:5518-5690, 550-622). */
+int fpls_pls_model1_xprod(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
+                          int L, int scaling, int fit, int oversample, int power_iters,
+                          double svds_tol, int seed, int xprod_precision, int* ncomp_out,
+                          double* C_latent, double* W_latent, double* Q, double* Ttrain, double* R,
+                          double* mX, double* vX, double* mY, double* B, double* Yfit, double* R2Y,
+                          double* s, int* k_eff, char* err, size_t errlen);
+
+/* Matrix-free fast SIMPLS: the refresh applies P_V XᵀY implicitly
+ * (P_V = I − V Vᵀ over the loadings so far) instead of deflating a stored
+ * p x m matrix.  xprod_precision must be 3.  Outputs as fpls_pls_model2_fast.
+ * Replaces _fastPLS_pls_model2_fast_rsvd_xprod_precision (RcppExports.cpp:648;
+ * fastPLS.cpp:5695-5986, 936-1000). */
+int fpls_pls_model2_fast_xprod(const double* X, int n, int p, const double* Y, int m,
+                               const int* ncomp, int L, int scaling, int fit, int seed,
+                               int xprod_precision, double* R, double* Q, double* mX, double* vX,
+                               double* mY, double* B, double* Yfit, double* R2Y, int* n_components,
+                               char* err, size_t errlen);
+
 /* Fast SIMPLS fit (warm-started 1-column refresh, 2 power iterations).
  * K = max(ncomp).  Outputs: R p x K, Q m x K, mX p, vX p, mY m,
  * B p x m x L (optional), Yfit n x m x L (optional), R2Y L; *n_components =

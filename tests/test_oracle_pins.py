@@ -215,3 +215,17 @@ def test_cknn_insertion_ties_keep_first():
     for c, v in enumerate([0.5, 0.7, 0.5, 0.7]):
         cknn.insert_top(s, ix, v, c + 1)
     assert ix == [2, 4, 1] and s == [0.7, 0.7, 0.5]
+
+
+def test_xprod_oracle_equals_materialized():
+    # The implicit operator applies the same A = XᵀY (and P_V A after deflation) as the
+    # materialized paths, so the models agree to rounding (fastPLS.cpp:550-622, 936-1000).
+    from oracle import xprod as ox
+    d = synthetic.c1_simpls_regression(seed=3, n=300, p=120, m=60, rank=8)
+    X, Y = d["Xtrain"], d["Ytrain"]
+    a = ox.pls_model1_xprod(X, Y, [3, 6], rsvd_oversample=5, rsvd_power=2, seed=4)
+    b = opls.pls_model1(X, Y, [3, 6], svd_method=4, rsvd_oversample=5, rsvd_power=2, seed=4)
+    assert np.allclose(a["B"], b["B"], rtol=1e-10, atol=1e-12)
+    c = ox.pls_model2_fast_xprod(X, Y, [2, 5, 9], seed=3)
+    e = opls.pls_model2_fast(X, Y, [2, 5, 9], seed=3)
+    assert np.linalg.norm(c["B"] - e["B"]) < 1e-10 * np.linalg.norm(e["B"])

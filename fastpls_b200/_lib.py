@@ -77,6 +77,7 @@ SIGNATURES = {
                                _I, _I, _I, _I, _D, _D, _I, _I, _IP, _DP, _C, _S], ctypes.c_int),
     "fpls_label_aware_cknn_resident": ([_I, _IP, _I, _I, _I, _I, _I, _I, _I, _I, _I, _D, _D, _I, _I,
                                         _IP, _DP, _C, _S], ctypes.c_int),
+    "fpls_gaussian_sketch": ([_I, _I, ctypes.c_uint, _DP, _C, _S], ctypes.c_int),
     "fpls_candidate_scores": ([_DP, _I, _I, _DP, _DP, _C, _S], ctypes.c_int),
     "fpls_candidate_centroids": ([_DP, _I, _I, _IP, _I, _DP, _C, _S], ctypes.c_int),
     "fpls_candidate_knn_predict": ([_DP, _I, _DP, _I, _I, _IP, _DP, _I, _DP, _I, _I, _I, _D, _D,
@@ -678,3 +679,10 @@ def label_aware_cknn_resident(xtrain_handle, y_codes, m, xtest_handle, ntest, nc
           int(ncomp), int(scaling), int(svd_method), int(oversample), int(power_iters), int(seed),
           int(knn_k), float(tau), float(alpha), int(top_m), int(top_k), _p(ti), _p(ts))
     return dict(top_index=ti, top_score=ts)
+
+
+def gaussian_sketch(rows, cols, seed):
+    """The device-drawn Gaussian sketch (mt19937 + normal_distribution stream)."""
+    out = _out(rows, cols)
+    _call("fpls_gaussian_sketch", int(rows), int(cols), int(seed) & 0xFFFFFFFF, _p(out))
+    return out

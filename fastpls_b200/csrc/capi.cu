@@ -6,6 +6,7 @@
 #include <cstring>
 #include <vector>
 
+#include "gaussian.cuh"
 #include "blas_f64.cuh"
 #include "capi_util.cuh"
 #include "context.cuh"
@@ -332,9 +333,9 @@ int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, 
     b.Yg = dYc;
     b.S = ctx.arena.alloc_n<double>((size_t)p * m);
     gemm(true, false, p, m, n, 1.0, dX, n, dYc, n, 0.0, b.S, p);
-    std::vector<double> om(p);
-    host_gaussian(om.data(), p, static_cast<unsigned int>(seed));
-    b.omega = upload(om.data(), p);
+    double* om = ctx.arena.alloc_n<double>(p);
+    device_gaussian(om, p, static_cast<unsigned int>(seed));
+    b.omega = om;
     b.m1_mode = (m == 1);
     b.R = ctx.arena.alloc_n<double>((size_t)p * K);
     b.Q = ctx.arena.alloc_n<double>((size_t)m * K);

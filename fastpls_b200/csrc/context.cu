@@ -77,6 +77,8 @@ Context& Context::get() {
     }
     ctx.sm_count = prop.multiProcessorCount;
     FPLS_CUDA(cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking));
+    FPLS_CUDA(cudaStreamCreateWithFlags(&ctx.side, cudaStreamNonBlocking));
+    FPLS_CUDA(cudaEventCreateWithFlags(&ctx.side_done, cudaEventDisableTiming));
     FPLS_CUDA(cudaMalloc(&ctx.d_status, 64 * sizeof(int)));
     FPLS_CUDA(cudaMemset(ctx.d_status, 0, 64 * sizeof(int)));
     ctx.device = dev;
@@ -123,6 +125,7 @@ void Context::sync() { FPLS_CUDA(cudaStreamSynchronize(stream)); }
 
 void Context::release() {
   if (device < 0) return;
+  cudaStreamSynchronize(side);
   cudaStreamSynchronize(stream);
   arena.release();
 }

@@ -38,6 +38,8 @@ struct ResidentX {
 struct Context {
   int device = -1;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;   // second stream for work that overlaps `stream` (joined by events)
+  cudaEvent_t side_done = nullptr;
   Arena arena;
   int* d_status = nullptr;     // device-side failure flag (0 = ok)
   int sm_count = kSMCount;

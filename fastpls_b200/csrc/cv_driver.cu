@@ -1,6 +1,7 @@
 #include "blas_f64.cuh"
 #include "context.cuh"
 #include "cv_driver.cuh"
+#include "gaussian.cuh"
 #include "fits.cuh"
 #include "heads.cuh"
 #include "simpls_engine.cuh"
@@ -90,39 +91,6 @@ __global__ void pred_counts_kernel(const int* __restrict__ pred, int L, int n, c
   }
 }
 
-// Draws the per-fit Gaussian sketches (libstdc++ mt19937 streams, one per
-// seed) on host threads while the device runs the grid's set-up.
-class SketchPool {
- public:
-  ~SketchPool() { join(); }
-  void start(const std::vector<unsigned>& seeds, int p) {
-    om_.assign(seeds.size() * (size_t)p, 0.0);
-    const int F = static_cast<int>(seeds.size());
-    const int nt = std::max(1, std::min<int>(F, static_cast<int>(std::thread::hardware_concurrency())));
-    double* out = om_.data();
-    const std::vector<unsigned>* sd = &seeds_;
-    seeds_ = seeds;
-    for (int t = 0; t < nt; ++t)
-      th_.emplace_back([out, sd, p, F, nt, t] {
-        for (int a = t; a < F; a += nt) host_gaussian(out + (size_t)a * p, p, (*sd)[a]);
-      });
-  }
-  const std::vector<double>& wait() {
-    join();
-    return om_;
-  }
-
- private:
-  void join() {
-    for (auto& t : th_)
-      if (t.joinable()) t.join();
-    th_.clear();
-  }
-  std::vector<double> om_;
-  std::vector<unsigned> seeds_;
-  std::vector<std::thread> th_;
-};
-
 // Class predictions of the test rows of every fit for every ncomp slice from the
 // kept scores: y_a = sum_{b<=a} (t_b[i] / ||t_b||) q_b + mY_f, label = first argmax.
 __global__ void cv_predict_kernel(int F, int n, int m, int K, int L, const int* __restrict__ ncomp,
@@ -200,7 +168,7 @@ void fill_special_predictions(const CvFitSet& fs, const int* y, const std::vecto
 
 void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, int L,
                  const CvGridOptions& opt, const std::vector<int>& status,
-                 const std::vector<double>& counts, SketchPool& sketches, CvGridResult& res) {
+                 const std::vector<double>& counts, double* d_om, CvGridResult& res) {
   Context& ctx = Context::get();
   Arena& ar = ctx.arena;
   const int n = fs.n, p = fs.p, m = fs.m;
@@ -230,7 +198,6 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   std::vector<int> grp(Fa), ntrain(Fa);
   std::vector<double> inv_nf(Fa), mYf((size_t)Fa * m), mYall(m, 0.0), dY((size_t)Fa * m);
   for (int i = 0; i < n; ++i) mYall[y[i] - 1] += 1.0 / n;
-  const size_t om_size = (size_t)Fa * p;
   for (int a = 0; a < Fa; ++a) {
     const int f = act[a];
     std::copy(fs.train.begin() + (size_t)f * n, fs.train.begin() + (size_t)(f + 1) * n, tr.begin() + (size_t)a * n);
@@ -253,7 +220,6 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   double* d_mYf = ar.alloc_n<double>(mYf.size());
   double* d_mYall = ar.alloc_n<double>(m);
   double* d_dY = ar.alloc_n<double>(dY.size());
-  double* d_om = ar.alloc_n<double>(om_size);
   int* d_lab = ar.alloc_n<int>(n);
   int* d_nc = ar.alloc_n<int>(L);
   std::vector<int> lab0(n);
@@ -293,8 +259,7 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   b.S = ar.alloc_n<double>((size_t)Fa * p * m);
   simpls_batch_crosscov(b, X, d_nt);
   pt.mark("crosscov");
-  const std::vector<double>& om = sketches.wait();
-  h2d(d_om, om.data(), om_size * sizeof(double));
+  FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0));
   pt.mark("sketch");
   b.R = ar.alloc_n<double>((size_t)Fa * p * K);
   b.Q = ar.alloc_n<double>((size_t)Fa * m * K);
@@ -346,7 +311,7 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
   double* T = ar.alloc_n<double>((size_t)n * K);
   double* Yp = ar.alloc_n<double>((size_t)n * m * L);
   int* lab = ar.alloc_n<int>((size_t)n * L);
-  std::vector<double> omh(p), Wh((size_t)K * m * L), Qh((size_t)m * K);
+  std::vector<double> Wh((size_t)K * m * L), Qh((size_t)m * K);
   std::vector<int> rows, trows, labs;
   for (int f = 0; f < fs.F; ++f) {
     if (status[f] != 1) continue;
@@ -366,8 +331,7 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
     FPLS_CHECK_LAUNCH();
     center_scale_xy(Xf, nf, p, Yf, m, opt.scaling, mX, vX, mY);
     gemm(true, false, p, m, nf, 1.0, Xf, nf, Yf, nf, 0.0, S, p);
-    host_gaussian(omh.data(), p, fs.seeds[f]);
-    h2d(om, omh.data(), p * sizeof(double));
+    device_gaussian(om, p, fs.seeds[f]);
     XOperatorF64 xop(Xf, nf, p);
     SimplsBatch b;
     b.n = nf; b.p = p; b.m = m; b.F = 1; b.K = K;
@@ -417,13 +381,23 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
   classify_fits(fs, labels_host, status, fallback, counts);
   res.status = status;
   const bool batched = opt.batched && opt.scaling != 2;
-  // Start the host-side sketches first so they overlap every device step below.
-  SketchPool sketches;
+  // The per-fit sketches are drawn on the side stream, overlapping every
+  // device step below until the SIMPLS loop needs them.
+  double* d_om = nullptr;
   if (batched) {
     std::vector<unsigned> seeds;
     for (int f = 0; f < fs.F; ++f)
       if (status[f] == 1) seeds.push_back(fs.seeds[f]);
-    sketches.start(seeds, fs.p);
+    if (!seeds.empty()) {
+      unsigned int* d_seeds = ctx.arena.alloc_n<unsigned int>(seeds.size());
+      d_om = ctx.arena.alloc_n<double>(seeds.size() * (size_t)fs.p);
+      FPLS_CUDA(cudaEventRecord(ctx.side_done, ctx.stream));  // arena reuse: after earlier work
+      FPLS_CUDA(cudaStreamWaitEvent(ctx.side, ctx.side_done, 0));
+      FPLS_CUDA(cudaMemcpyAsync(d_seeds, seeds.data(), seeds.size() * sizeof(unsigned), cudaMemcpyHostToDevice,
+                                ctx.side));
+      device_gaussian_streams(d_om, fs.p, fs.p, d_seeds, static_cast<int>(seeds.size()), ctx.side);
+      FPLS_CUDA(cudaEventRecord(ctx.side_done, ctx.side));
+    }
   }
   const size_t npred = (size_t)fs.G * L * fs.n;
   res.d_pred = ctx.arena.alloc_n<int>(npred);
@@ -445,7 +419,7 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
     widen_f32_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(x32, X, (size_t)fs.n * fs.p); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
-  if (batched) run_batched(fs, X, labels_host, ncomp, L, opt, status, counts, sketches, res);
+  if (batched) run_batched(fs, X, labels_host, ncomp, L, opt, status, counts, d_om, res);
   else run_sequential(fs, X, labels_host, ncomp, L, opt, status, res);
 }
 

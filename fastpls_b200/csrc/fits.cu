@@ -1,3 +1,4 @@
+#include "gaussian.cuh"
 #include "blas_f64.cuh"
 #include "context.cuh"
 #include "fits.cuh"
@@ -254,12 +255,10 @@ int simpls_classic_fit(const double* X, int n, int p, const double* Y, int m, co
   }
   int i_out = 0;
   int done = 0;
-  std::vector<double> omh(m);
   for (int a = 0; a < max_ncomp; ++a) {
     const double* rr_src = nullptr;
     if (rsvd) {
-      host_gaussian(omh.data(), m, opt.seed + a + std::max(opt.oversample, 0));
-      h2d(omega, omh.data(), m * sizeof(double));
+      device_gaussian(omega, m, opt.seed + a + std::max(opt.oversample, 0));
       dzero(ctx.d_status + 3, sizeof(int));
       leading_left_power_kernel<<<1, 1024, 0, ctx.stream>>>(S, p, m, omega, max_iters,
                                                             std::max(opt.svds_tol, 1e-8), u, vtmp,

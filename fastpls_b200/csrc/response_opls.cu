@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 
+#include "gaussian.cuh"
 #include "blas_f64.cuh"
 #include "capi_util.cuh"
 #include "context.cuh"
@@ -102,8 +103,6 @@ void leading_left_vector(const double* S, int p, int q, double* u, unsigned int 
   if (right) gemm(true, false, q, q, p, 1.0, S, p, S, p, 0.0, G, q);
   else gemm(false, true, p, p, q, 1.0, S, p, S, p, 0.0, G, p);
   const int l = std::min(m, 8);
-  std::vector<double> om((size_t)m * l);
-  host_gaussian(om.data(), om.size(), seed);
   double* Y = ctx.arena.alloc_n<double>((size_t)m * l);
   double* Q = ctx.arena.alloc_n<double>((size_t)m * l);
   double* GQ = ctx.arena.alloc_n<double>((size_t)m * l);
@@ -113,7 +112,7 @@ void leading_left_vector(const double* S, int p, int q, double* u, unsigned int 
   double* v = ctx.arena.alloc_n<double>(m);
   double* vprev = ctx.arena.alloc_n<double>(m);
   double* dots = ctx.arena.alloc_n<double>(2);
-  h2d(Y, om.data(), om.size() * sizeof(double));
+  device_gaussian(Y, (long long)m * l, seed);
   qr_orthonormalize(m, l, Y, m, Q, m);
   fill(vprev, m, 0.0);
   double lam1 = 0.0;

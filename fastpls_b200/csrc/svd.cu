@@ -1,3 +1,4 @@
+#include "gaussian.cuh"
 #include "blas_f64.cuh"
 #include "context.cuh"
 #include "linalg_small.cuh"
@@ -50,11 +51,6 @@ SvdResult exact_svd(const double* A, int rows, int cols, int lda, int k, bool le
 
 }  // namespace
 
-void host_gaussian(double* out, size_t n_elem, unsigned int seed) {
-  std::mt19937 rng(seed);
-  std::normal_distribution<double> norm(0.0, 1.0);
-  for (size_t i = 0; i < n_elem; ++i) out[i] = norm(rng);
-}
 
 SvdResult truncated_svd_device(const double* A, int rows, int cols, int lda, int k, int method,
                                int oversample, int power_iters, unsigned int seed, bool left_only,
@@ -73,10 +69,8 @@ SvdResult truncated_svd_device(const double* A, int rows, int cols, int lda, int
   if (l >= max_rank) return exact_svd(A, rows, cols, lda, target, left_only, U, ldu, s, V, ldv);
 
   Context& ctx = Context::get();
-  std::vector<double> omega_h((size_t)cols * l);
-  host_gaussian(omega_h.data(), omega_h.size(), seed);
   double* Omega = ctx.arena.alloc_n<double>((size_t)cols * l);
-  h2d(Omega, omega_h.data(), omega_h.size() * sizeof(double));
+  device_gaussian(Omega, (long long)cols * l, seed);
   double* Y = ctx.arena.alloc_n<double>((size_t)rows * l);
   double* Z = ctx.arena.alloc_n<double>((size_t)cols * l);
   double* Qz = ctx.arena.alloc_n<double>((size_t)cols * l);

@@ -12,9 +12,6 @@ enum SvdMethod : int {
   kSvdCudaRsvd = 5,   // follows the CPU rSVD recipe (parity target)
 };
 
-// Host-side Gaussian sketch: std::mt19937(seed) + std::normal_distribution<double>
-// filling a column-major rows x cols matrix (reference src/svd_cpu_rsvd.cpp:10-22).
-void host_gaussian(double* out, size_t n_elem, unsigned int seed);
 
 struct SvdResult {
   int rank = 0;   // columns written to U / s / V

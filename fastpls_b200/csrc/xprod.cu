@@ -6,6 +6,7 @@
 //                                     refresh of :936-1000 (k_block = 1)
 //
 // X (n x p) and Y (n x m) are the centred (scaled) device matrices.
+#include "gaussian.cuh"
 #include "xprod.cuh"
 
 #include <algorithm>
@@ -109,12 +110,7 @@ SvdResult truncated_rsvd_crossprod_device(const double* X, int n, int p, const d
     gemm(false, false, n, l, p, 1.0, X, n, M, p, 0.0, T, n);
     gemm(true, false, m, l, n, 1.0, Y, n, T, n, 0.0, out, m);
   };
-  {
-    std::vector<double> om((size_t)m * l);
-    host_gaussian(om.data(), om.size(), seed);
-    h2d(Zm, om.data(), om.size() * sizeof(double));
-    ctx.sync();
-  }
+  device_gaussian(Zm, (long long)m * l, seed);
   a_times(Zm, Ys);
   power_iters = std::max(power_iters, 0);
   if (power_iters == 1) {
@@ -187,9 +183,7 @@ int simpls_xprod_fit(const double* X, int n, int p, const double* Y, int m, cons
   for (; a < K; ++a) {
     // refresh: start vector, projections, two power iterations of A A^T
     if (a == 0) {
-      std::vector<double> om(p);
-      host_gaussian(om.data(), om.size(), seed + a);
-      h2d(y, om.data(), p * sizeof(double));
+      device_gaussian(y, p, seed + a);
     } else {
       d2d(y, rr, p * sizeof(double));
     }

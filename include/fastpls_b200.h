@@ -297,6 +297,13 @@ int fpls_label_aware_cknn_resident(int xtrain_handle, const int* y_codes, int m,
                                    int top_m, int top_k, int* top_index, double* top_score, char* err,
                                    size_t errlen);
 
+/* The Gaussian sketch every randomized path draws (rSVD Ω, the SIMPLS start
+ * vector, the OPLS and matrix-free subspace starts), generated on the device:
+ * std::mt19937(seed) + std::normal_distribution<double>(0, 1) as libstdc++
+ * implements them, filling a rows x cols column-major matrix (the reference's
+ * gaussian_matrix, src/svd_cpu_rsvd.cpp:10-22).  No .Call counterpart. */
+int fpls_gaussian_sketch(int rows, int cols, unsigned int seed, double* out, char* err, size_t errlen);
+
 /* Candidate-kNN score space: Tn = row_l2(T Ck) (Ck k x k, or null for T
  * itself), T n x k column-major; zero row norms are replaced by 1.  Replaces
  * the R-side .candidate_score_space + .candidate_row_l2 arithmetic

@@ -77,6 +77,8 @@ SIGNATURES = {
                                _I, _I, _I, _I, _D, _D, _I, _I, _IP, _DP, _C, _S], ctypes.c_int),
     "fpls_label_aware_cknn_resident": ([_I, _IP, _I, _I, _I, _I, _I, _I, _I, _I, _I, _D, _D, _I, _I,
                                         _IP, _DP, _C, _S], ctypes.c_int),
+    "fpls_host_register": ([ctypes.c_void_p, _S, _C, _S], ctypes.c_int),
+    "fpls_host_unregister": ([ctypes.c_void_p, _C, _S], ctypes.c_int),
     "fpls_gaussian_sketch": ([_I, _I, ctypes.c_uint, _DP, _C, _S], ctypes.c_int),
     "fpls_candidate_scores": ([_DP, _I, _I, _DP, _DP, _C, _S], ctypes.c_int),
     "fpls_candidate_centroids": ([_DP, _I, _I, _IP, _I, _DP, _C, _S], ctypes.c_int),
@@ -686,3 +688,12 @@ def gaussian_sketch(rows, cols, seed):
     out = _out(rows, cols)
     _call("fpls_gaussian_sketch", int(rows), int(cols), int(seed) & 0xFFFFFFFF, _p(out))
     return out
+
+
+def host_register(a):
+    """Pins the memory of numpy array `a` (page-locked) until host_unregister."""
+    _call("fpls_host_register", ctypes.c_void_p(a.ctypes.data), ctypes.c_size_t(a.nbytes))
+
+
+def host_unregister(a):
+    _call("fpls_host_unregister", ctypes.c_void_p(a.ctypes.data))

@@ -863,6 +863,22 @@ int fpls_x_free(int handle, char* err, size_t errlen) {
   });
 }
 
+int fpls_host_register(void* ptr, size_t bytes, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(ptr && bytes > 0, "host_register: empty buffer");
+    Context::get();
+    FPLS_CUDA(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+  });
+}
+
+int fpls_host_unregister(void* ptr, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(ptr, "host_unregister: null buffer");
+    Context::get();
+    FPLS_CUDA(cudaHostUnregister(ptr));
+  });
+}
+
 int fpls_double_cv_resident(int handle, const int* y, int n_classes, const int* outer_fold,
                             int kfold_outer, const int* inner_fold, int kfold_inner,
                             const int* ncomp, int L, int scaling, int seed, int run, int precision,

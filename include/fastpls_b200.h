@@ -361,6 +361,12 @@ int fpls_x_upload(const void* X, int x_is_float32, int n, int p, int* handle, ch
                   size_t errlen);
 int fpls_x_free(int handle, char* err, size_t errlen);
 
+/* Page-locks (pins) an existing host buffer so that the host-buffer entry
+ * points copy it to and from the device at full link speed, e.g. an R matrix
+ * reused across calls; undo with fpls_host_unregister before freeing it. */
+int fpls_host_register(void* ptr, size_t bytes, char* err, size_t errlen);
+int fpls_host_unregister(void* ptr, char* err, size_t errlen);
+
 /* fpls_double_cv on a registered (device-resident) predictor matrix. */
 int fpls_double_cv_resident(int handle, const int* y, int n_classes, const int* outer_fold,
                             int kfold_outer, const int* inner_fold, int kfold_inner,

@@ -1,6 +1,7 @@
 #include "blas_f64.cuh"
 #include "context.cuh"
 #include "cv_driver.cuh"
+#include "dual_engine.cuh"
 #include "gaussian.cuh"
 #include "fits.cuh"
 #include "heads.cuh"
@@ -190,8 +191,11 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
     center_scale(X, n, p, n, mall, nullptr);
   }
   pt.mark("centre");
+  // Short, wide predictor blocks run the loop in the row space of X (the
+  // row Gram K = Xc Xc^T); otherwise in the predictor space.
+  const bool dual = dual_engine_applies(n, p, m, K);
   std::unique_ptr<XOperator> xop;
-  if (opt.precision == 1) xop = make_split_operator(X, n, p);
+  if (opt.precision == 1) xop = make_split_operator(X, n, p, !dual);
   else xop.reset(new XOperatorF64(X, n, p));
   pt.mark("operator");
   std::vector<uint8_t> tr((size_t)Fa * n), te((size_t)Fa * n);
@@ -234,49 +238,84 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   h2d(d_dY, dY.data(), dY.size() * sizeof(double));
   h2d(d_lab, lab0.data(), n * sizeof(int));
   h2d(d_nc, ncomp, L * sizeof(int));
-  SimplsBatch b;
-  b.n = n; b.p = p; b.m = m; b.F = Fa; b.K = K;
-  b.power_iters = opt.power_iters;
-  b.X = xop.get();
-  b.labels = d_lab;
-  b.mY_all = d_mYall;
-  b.mask = d_tr;
-  b.dY = d_dY;
-  b.omega = d_om;
-  b.m1_mode = (m == 1);
-  double* delta = nullptr;
-  if (center) {
-    double* Mtr = ar.alloc_n<double>((size_t)Fa * n);
-    delta = ar.alloc_n<double>((size_t)Fa * p);
-    mask_to_double_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(d_tr, (size_t)Fa * n, Mtr); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
-    xop->t_times(Mtr, Fa, delta);
-    scale_cols_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(delta, p, Fa, d_inv); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
+  double* Qo = ar.alloc_n<double>((size_t)Fa * m * K);
+  double* tno = ar.alloc_n<double>((size_t)Fa * K);
+  double* Tko = ar.alloc_n<double>((size_t)Fa * n * K);
+  int* ncd = ar.alloc_n<int>(Fa);
+  int* sto = ar.alloc_n<int>(Fa);
+  if (dual) {
+    double* Kg = ar.alloc_n<double>((size_t)n * n);
+    xop->gram(Kg);
+    symmetrize(Kg, n);
+    std::unique_ptr<XOperator> kop;
+    if (opt.precision == 1) kop = make_split_operator(Kg, n, n, false);
+    else kop.reset(new XOperatorF64(Kg, n, n));
+    pt.mark("row gram");
+    FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0));
+    double* XOm = ar.alloc_n<double>((size_t)n * Fa);
+    xop->times(d_om, Fa, XOm);
+    pt.mark("sketch");
+    DualBatch db;
+    db.n = n; db.m = m; db.F = Fa; db.K = K;
+    db.power_iters = opt.power_iters;
+    db.m1_mode = (m == 1);
+    db.center = center;
+    db.Kop = kop.get();
+    db.x0 = X;
+    db.XOmega = XOm;
+    db.mask = d_tr;
+    db.labels = d_lab;
+    db.mY_all = d_mYall;
+    db.dY = d_dY;
+    db.ntrain = d_nt;
+    db.Q = Qo; db.tnorm = tno; db.Tkeep = Tko; db.ncomp_done = ncd; db.status = sto;
+    dual_simpls_run(db);
+    pt.mark("simpls");
+  } else {
+    SimplsBatch b;
+    b.n = n; b.p = p; b.m = m; b.F = Fa; b.K = K;
+    b.power_iters = opt.power_iters;
+    b.X = xop.get();
+    b.labels = d_lab;
+    b.mY_all = d_mYall;
+    b.mask = d_tr;
+    b.dY = d_dY;
+    b.omega = d_om;
+    b.m1_mode = (m == 1);
+    double* delta = nullptr;
+    if (center) {
+      double* Mtr = ar.alloc_n<double>((size_t)Fa * n);
+      delta = ar.alloc_n<double>((size_t)Fa * p);
+      mask_to_double_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(d_tr, (size_t)Fa * n, Mtr); ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+      xop->t_times(Mtr, Fa, delta);
+      scale_cols_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(delta, p, Fa, d_inv); ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+    }
+    b.delta = delta;
+    pt.mark("fold means");
+    b.S = ar.alloc_n<double>((size_t)Fa * p * m);
+    simpls_batch_crosscov(b, X, d_nt);
+    pt.mark("crosscov");
+    FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0));
+    pt.mark("sketch");
+    b.R = ar.alloc_n<double>((size_t)Fa * p * K);
+    b.Q = Qo;
+    b.V = ar.alloc_n<double>((size_t)Fa * p * K);
+    b.tnorm = tno;
+    b.Tkeep = Tko;
+    b.ncomp_done = ncd;
+    b.status = sto;
+    simpls_batch_run(b);
+    pt.mark("simpls");
   }
-  b.delta = delta;
-  pt.mark("fold means");
-  b.S = ar.alloc_n<double>((size_t)Fa * p * m);
-  simpls_batch_crosscov(b, X, d_nt);
-  pt.mark("crosscov");
-  FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0));
-  pt.mark("sketch");
-  b.R = ar.alloc_n<double>((size_t)Fa * p * K);
-  b.Q = ar.alloc_n<double>((size_t)Fa * m * K);
-  b.V = ar.alloc_n<double>((size_t)Fa * p * K);
-  b.tnorm = ar.alloc_n<double>((size_t)Fa * K);
-  b.Tkeep = ar.alloc_n<double>((size_t)Fa * n * K);
-  b.ncomp_done = ar.alloc_n<int>(Fa);
-  b.status = ar.alloc_n<int>(Fa);
-  simpls_batch_run(b);
-  pt.mark("simpls");
   int* d_pred = res.d_pred;
   cv_predict_kernel<<<dim3(ceil_div(n, 128), Fa), 128, 0, ctx.stream>>>(
-      Fa, n, m, K, L, d_nc, d_te, d_grp, b.Tkeep, b.tnorm, b.Q, b.ncomp_done, d_mYf, d_pred); ::fpls::note_launch();
+      Fa, n, m, K, L, d_nc, d_te, d_grp, Tko, tno, Qo, ncd, d_mYf, d_pred); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   pt.mark("predict");
   std::vector<int> done(Fa);
-  d2h(done.data(), b.ncomp_done, Fa * sizeof(int));
+  d2h(done.data(), ncd, Fa * sizeof(int));
   ctx.sync();
   for (int a = 0; a < Fa; ++a) res.ncomp_done[act[a]] = done[a];
   pt.mark("d2h");

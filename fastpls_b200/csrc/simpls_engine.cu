@@ -468,6 +468,8 @@ void XOperatorF64::t_times(const double* T, int F, double* P) {
   else gemm(true, false, p, F, n, 1.0, Xc, n, T, n, 0.0, P, p);
 }
 
+void XOperatorF64::gram(double* K) { gemm(false, true, n, n, p, 1.0, Xc, n, Xc, n, 0.0, K, n); }
+
 void simpls_batch_crosscov(const SimplsBatch& b, const double* /*Xc*/, const int* n_train) {
   Context& ctx = Context::get();
   Eng e = make_eng(b);

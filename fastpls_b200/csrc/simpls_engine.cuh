@@ -27,6 +27,8 @@ struct XOperator {
   virtual ~XOperator() {}
   virtual void times(const double* Rhat, int F, double* U) = 0;
   virtual void t_times(const double* T, int F, double* P) = 0;
+  // K (n x n) = Xc Xc^T, the row Gram of the predictors.
+  virtual void gram(double* K) = 0;
   int n = 0, p = 0;
 };
 
@@ -36,6 +38,7 @@ struct XOperatorF64 : public XOperator {
   XOperatorF64(const double* X, int n_, int p_) : Xc(X) { n = n_; p = p_; }
   void times(const double* Rhat, int F, double* U) override;
   void t_times(const double* T, int F, double* P) override;
+  void gram(double* K) override;
 };
 
 struct SimplsBatch {

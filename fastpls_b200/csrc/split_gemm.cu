@@ -553,20 +553,25 @@ void split_rows(const double* X, int rows, int cols, int ld, const SplitPair& ou
 struct XOperatorSplit : public XOperator {
   SplitPair xr;   // n x p  (A of X * R)
   SplitPair xc;   // p x n  (A of X^T * T)
-  XOperatorSplit(const double* X, int n_, int p_) {
+  bool has_t = true;
+  XOperatorSplit(const double* X, int n_, int p_, bool need_t) : has_t(need_t) {
     n = n_;
     p = p_;
     xr = alloc_pair(n, p);
-    xc = alloc_pair(p, n);
     split_rows(X, n, p, n, xr);
-    split_cols(X, n, p, n, xc);
+    if (has_t) {
+      xc = alloc_pair(p, n);
+      split_cols(X, n, p, n, xc);
+    }
   }
   void times(const double* Rhat, int F, double* U) override {
     SplitPair b = alloc_pair(F, p);
     split_cols(Rhat, p, F, p, b);
     split_gemm(xr, b, n, F, p, 1.0, 0.0, U, n);
   }
+  void gram(double* K) override { split_gemm(xr, xr, n, n, p, 1.0, 0.0, K, n); }
   void t_times(const double* T, int F, double* P) override {
+    FPLS_REQUIRE(has_t, "split operator built without its transposed copy");
     SplitPair b = alloc_pair(F, n);
     split_cols(T, n, F, n, b);
     split_gemm(xc, b, p, F, n, 1.0, 0.0, P, p);
@@ -580,8 +585,8 @@ void split_gemm_release_cache() {
   plan_cache().clear();
 }
 
-std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p) {
-  return std::unique_ptr<XOperator>(new XOperatorSplit(X, n, p));
+std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p, bool need_t) {
+  return std::unique_ptr<XOperator>(new XOperatorSplit(X, n, p, need_t));
 }
 
 void split_gemm_test(const double* A, const double* B, int M, int N, int K, double* C) {

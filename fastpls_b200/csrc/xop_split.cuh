@@ -13,8 +13,9 @@ namespace fpls {
 // Frees the per-shape GEMM plans kept on the device (fpls_reset_workspace).
 void split_gemm_release_cache();
 
-// Builds the split operator from an FP64 device matrix (n x p, ld n).
-std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p);
+// Builds the split operator from an FP64 device matrix (n x p, ld n); without
+// need_t only the row-major copy (for times() and gram()) is kept.
+std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p, bool need_t = true);
 
 // Plain C = A (M x K) * B^T (N x K) with A, B given as FP64 and split on the fly
 // into BF16 hi/lo; used by tests of the tensor-core kernel.  C is M x N (ld M).

@@ -1,0 +1,66 @@
+"""The row-space (dual) batched SIMPLS engine against the predictor-space engine
+and the oracle on a short, wide predictor block (n <= p / 2)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import cv as ocv
+from fastpls_b200 import synthetic
+from fastpls_b200.folds import double_cv_folds, stratified_group_folds
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def wide():
+    return synthetic.c4_omics(seed=3, n=300, p=1500, n_informative=25)
+
+
+def _with_env(value, fn):
+    old = os.environ.get("FASTPLS_DUAL")
+    os.environ["FASTPLS_DUAL"] = value
+    try:
+        return fn()
+    finally:
+        if old is None:
+            os.environ.pop("FASTPLS_DUAL")
+        else:
+            os.environ["FASTPLS_DUAL"] = old
+
+
+@pytest.mark.parametrize("scaling", [1, 3])
+def test_dual_matches_primal_fp64(lib, wide, scaling):
+    d = wide
+    outer, inner = double_cv_folds(d["y"], d["groups"], 4, 3, seed=5)
+    nc = np.arange(1, 13)
+    run = lambda: lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], scaling=scaling,
+                                seed=1, precision="fp64", return_inner=True)
+    dual = _with_env("1", run)
+    primal = _with_env("0", run)
+    assert np.array_equal(dual["best_comp"], primal["best_comp"])
+    assert np.max(np.abs(dual["inner_accuracy"] - primal["inner_accuracy"])) < 1e-12
+    assert np.array_equal(dual["pred"], primal["pred"])
+    assert np.mean(dual["inner_pred"] == primal["inner_pred"]) > 0.9995
+
+
+def test_dual_cv_predict_matches_oracle(lib, wide):
+    d = wide
+    rng = np.random.default_rng(4)
+    fold = stratified_group_folds(d["y"], d["groups"], 5, rng)
+    nc = np.arange(1, 11)
+    got = lib.cv_predict(d["X"], d["y"], fold, nc, d["n_classes"], seed=7, batched=True)
+    ref = ocv.pls_cv_predict_compiled(d["X"].astype(np.float64), d["y"], fold, nc, d["n_classes"],
+                                      seed=7)
+    assert np.array_equal(got["status"], ref["status"])
+    assert np.mean(np.asarray(got["class_pred"]) == np.asarray(ref["class_pred"])) >= 0.999
+
+
+def test_dual_bf16x3_close_to_fp64(lib, wide):
+    d = wide
+    outer, inner = double_cv_folds(d["y"], d["groups"], 4, 3, seed=5)
+    nc = np.arange(1, 13)
+    a = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], seed=1, precision="fp64")
+    b = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], seed=1, precision="bf16x3")
+    assert np.allclose(a["inner_accuracy"], b["inner_accuracy"], atol=5e-3)
+    assert np.mean(a["pred"] == b["pred"]) >= 0.99

@@ -282,17 +282,22 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
     b.dY = d_dY;
     b.omega = d_om;
     b.m1_mode = (m == 1);
+    // Fold column sums X^T D_f 1 centre the response in S_f; divided by the
+    // fold sizes they are the fold offsets delta_f when X is centred.
+    double* Mtr = ar.alloc_n<double>((size_t)Fa * n);
+    double* colsum = ar.alloc_n<double>((size_t)Fa * p);
+    mask_to_double_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(d_tr, (size_t)Fa * n, Mtr); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    xop->t_times(Mtr, Fa, colsum);
     double* delta = nullptr;
     if (center) {
-      double* Mtr = ar.alloc_n<double>((size_t)Fa * n);
       delta = ar.alloc_n<double>((size_t)Fa * p);
-      mask_to_double_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(d_tr, (size_t)Fa * n, Mtr); ::fpls::note_launch();
-      FPLS_CHECK_LAUNCH();
-      xop->t_times(Mtr, Fa, delta);
+      d2d(delta, colsum, (size_t)Fa * p * sizeof(double));
       scale_cols_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(delta, p, Fa, d_inv); ::fpls::note_launch();
       FPLS_CHECK_LAUNCH();
     }
     b.delta = delta;
+    b.colsum = colsum;
     pt.mark("fold means");
     b.S = ar.alloc_n<double>((size_t)Fa * p * m);
     simpls_batch_crosscov(b, X, d_nt);

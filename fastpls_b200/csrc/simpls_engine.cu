@@ -22,6 +22,7 @@ struct Eng {
   const double* mY_all;
   const uint8_t* mask;
   const double* delta;
+  const double* colsum;
   const double* colscale;
   const double* dY;
   double* S;
@@ -417,7 +418,7 @@ __global__ void k_masked_response(Eng e, double* M) {
   }
 }
 
-__global__ void k_crosscov_finish(Eng e, const double* P, const int* n_train) {
+__global__ void k_crosscov_finish(Eng e, const double* P) {
   const size_t total = (size_t)e.F * e.p * e.m;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
        t += (size_t)gridDim.x * blockDim.x) {
@@ -425,11 +426,11 @@ __global__ void k_crosscov_finish(Eng e, const double* P, const int* n_train) {
     const size_t col = t / e.p;
     const int f = static_cast<int>(col / e.m), j = static_cast<int>(col % e.m);
     double v = P[i + col * e.p];
-    if (e.delta) {
+    if (e.colsum) {
       double off = 0.0;
       if (e.labels) off += e.mY_all[j];
       if (e.dY) off += e.dY[(size_t)f * e.m + j];
-      v -= static_cast<double>(n_train[f]) * e.delta[(size_t)f * e.p + i] * off;
+      v -= e.colsum[(size_t)f * e.p + i] * off;
     }
     if (e.colscale) v *= e.colscale[(size_t)f * e.p + i];
     e.S[(size_t)f * e.p * e.m + i + (size_t)j * e.p] = v;
@@ -449,6 +450,7 @@ Eng make_eng(const SimplsBatch& b) {
   e.szn = ceil_div(b.n, e.cn);
   e.cn = ceil_div(b.n, e.szn);
   e.Yg = b.Yg; e.labels = b.labels; e.mY_all = b.mY_all; e.mask = b.mask; e.delta = b.delta;
+  e.colsum = b.colsum;
   e.colscale = b.colscale; e.dY = b.dY; e.S = b.S; e.omega = b.omega; e.m1_mode = b.m1_mode;
   e.iters = b.m1_mode ? 0 : std::max(b.power_iters, 0);
   e.R = b.R; e.Q = b.Q; e.V = b.V; e.tnorm = b.tnorm; e.Tkeep = b.Tkeep;
@@ -470,7 +472,7 @@ void XOperatorF64::t_times(const double* T, int F, double* P) {
 
 void XOperatorF64::gram(double* K) { gemm(false, true, n, n, p, 1.0, Xc, n, Xc, n, 0.0, K, n); }
 
-void simpls_batch_crosscov(const SimplsBatch& b, const double* /*Xc*/, const int* n_train) {
+void simpls_batch_crosscov(const SimplsBatch& b, const double* /*Xc*/, const int* /*n_train*/) {
   Context& ctx = Context::get();
   Eng e = make_eng(b);
   double* M = ctx.arena.alloc_n<double>((size_t)b.n * b.F * b.m);
@@ -478,7 +480,7 @@ void simpls_batch_crosscov(const SimplsBatch& b, const double* /*Xc*/, const int
   k_masked_response<<<2 * ctx.sm_count, kThreads, 0, ctx.stream>>>(e, M); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   b.X->t_times(M, b.F * b.m, P);
-  k_crosscov_finish<<<2 * ctx.sm_count, kThreads, 0, ctx.stream>>>(e, P, n_train); ::fpls::note_launch();
+  k_crosscov_finish<<<2 * ctx.sm_count, kThreads, 0, ctx.stream>>>(e, P); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 

@@ -52,6 +52,7 @@ struct SimplsBatch {
   const double* mY_all = nullptr;            // m (labels mode)
   const uint8_t* mask = nullptr;             // F x n train masks, null = all rows
   const double* delta = nullptr;             // F x p fold offsets, null = zero
+  const double* colsum = nullptr;            // F x p fold column sums X^T D_f 1 (response centring)
   const double* colscale = nullptr;          // F x p (1/vX), null = ones
   const double* dY = nullptr;                // F x m response offsets, null = zero
   double* S = nullptr;                       // F x p x m cross-covariances (deflated in place)
@@ -70,8 +71,9 @@ struct SimplsBatch {
 // Runs K components for all fits.  Device pointers throughout; launches only.
 void simpls_batch_run(const SimplsBatch& b);
 
-// S_f = diag(colscale_f) [ Xc^T D_f Yg - n_f delta_f dY_f^T ] for all fits
-// (the masked cross-covariances), via one GEMM Xc^T [D_1 Yg ... D_F Yg].
+// S_f = diag(colscale_f) [ Xc^T D_f Y - colsum_f off_f^T ] for all fits (the
+// masked cross-covariances with the fold-centred response, off_f the fold's
+// response means), via one GEMM Xc^T [D_1 Y ... D_F Y].
 void simpls_batch_crosscov(const SimplsBatch& b, const double* Xc, const int* n_train);
 
 }  // namespace fpls

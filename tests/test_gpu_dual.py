@@ -64,3 +64,17 @@ def test_dual_bf16x3_close_to_fp64(lib, wide):
     b = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], seed=1, precision="bf16x3")
     assert np.allclose(a["inner_accuracy"], b["inner_accuracy"], atol=5e-3)
     assert np.mean(a["pred"] == b["pred"]) >= 0.99
+
+
+@pytest.mark.parametrize("dual", ["1", "0"])
+def test_uncentred_predictors_match_oracle(lib, wide, dual):
+    # scaling 3: X is not centred but the response still is (fold means)
+    d = wide
+    rng = np.random.default_rng(6)
+    fold = stratified_group_folds(d["y"], d["groups"], 4, rng)
+    nc = np.arange(1, 9)
+    got = _with_env(dual, lambda: lib.cv_predict(d["X"], d["y"], fold, nc, d["n_classes"], scaling=3,
+                                                 seed=3, batched=True))
+    ref = ocv.pls_cv_predict_compiled(d["X"].astype(np.float64), d["y"], fold, nc, d["n_classes"],
+                                      scaling=3, seed=3)
+    assert np.mean(np.asarray(got["class_pred"]) == np.asarray(ref["class_pred"])) >= 0.999

@@ -41,24 +41,43 @@ struct DualEng {
   int* status;
 };
 
-// out[j] = sum_i M[i + j*ld] * xs[i] for j < ncols, xs in shared memory; warps
-// take columns.  Ends with a barrier.
+constexpr int kRows = kMaxN / kThreads;   // rows of an n-vector held per thread
+
+// out[j] = sum_i M[i + j*ld] * xs[i] for j < ncols, xs in shared memory.  With
+// fewer columns than warps, several warps split the rows of one column; every
+// lane keeps four independent partial sums.  Ends with a barrier.
 __device__ void dots_smem(const double* __restrict__ M, size_t ld, int ncols, const double* xs, int rows,
                           double* out) {
+  __shared__ double red[kWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int j = warp; j < ncols; j += kWarps) {
-    const double* col = M + (size_t)j * ld;
-    double a0 = 0.0, a1 = 0.0;
-    int r = lane;
-    for (; r + 32 < rows; r += 64) {
-      a0 += col[r] * xs[r];
-      a1 += col[r + 32] * xs[r + 32];
+  const int g = ncols >= kWarps ? 1 : kWarps / max(ncols, 1);   // warps per column
+  const int cols_per_pass = kWarps / g;
+  for (int j0 = 0; j0 < ncols; j0 += cols_per_pass) {
+    const int j = j0 + warp / g, sub = warp % g;
+    double acc = 0.0;
+    if (j < ncols && warp / g < cols_per_pass) {
+      const double* col = M + (size_t)j * ld;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      const int step = 32 * g;
+      int r = sub * 32 + lane;
+      for (; r + 3 * step < rows; r += 4 * step) {
+        a0 += col[r] * xs[r];
+        a1 += col[r + step] * xs[r + step];
+        a2 += col[r + 2 * step] * xs[r + 2 * step];
+        a3 += col[r + 3 * step] * xs[r + 3 * step];
+      }
+      for (; r < rows; r += step) a0 += col[r] * xs[r];
+      acc = warp_sum((a0 + a1) + (a2 + a3));
     }
-    if (r < rows) a0 += col[r] * xs[r];
-    const double s = warp_sum(a0 + a1);
-    if (lane == 0) out[j] = s;
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x < cols_per_pass && j0 + threadIdx.x < ncols) {
+      double t = 0.0;
+      for (int u = 0; u < g; ++u) t += red[threadIdx.x * g + u];
+      out[j0 + threadIdx.x] = t;
+    }
+    __syncthreads();
   }
-  __syncthreads();
 }
 
 // Block sum of up to 4 values per thread; result broadcast to every thread.
@@ -126,15 +145,30 @@ __global__ void __launch_bounds__(kThreads) k_dual_a(DualEng e, int a) {
     dots_smem(CS, n, m, vk, n, z);
   }
   for (int it = 0; it < steps; ++it) {
-    // y = S z: c_y = C_S z, K c_y = (K C_S) z
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      double c = 0.0, k = 0.0;
-      for (int j = 0; j < m; ++j) {
-        c += CS[i + (size_t)j * n] * z[j];
-        k += KCS[i + (size_t)j * n] * z[j];
+    // y = S z: c_y = C_S z, K c_y = (K C_S) z (rows held in registers)
+    double c[kRows], k[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) c[r] = k[r] = 0.0;
+    for (int j = 0; j < m; ++j) {
+      const double zj = z[j];
+      const double* cs = CS + (size_t)j * n;
+      const double* ks = KCS + (size_t)j * n;
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const int i = threadIdx.x + r * kThreads;
+        if (i < n) {
+          c[r] += cs[i] * zj;
+          k[r] += ks[i] * zj;
+        }
       }
-      vy[i] = c;
-      vk[i] = k;
+    }
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const int i = threadIdx.x + r * kThreads;
+      if (i < n) {
+        vy[i] = c[r];
+        vk[i] = k[r];
+      }
     }
     __syncthreads();
     if (it + 1 < steps) dots_smem(CS, n, m, vk, n, z);
@@ -213,16 +247,35 @@ __global__ void __launch_bounds__(kThreads) k_dual_b(DualEng e, int a) {
   }
   __syncthreads();
   if (a > 0) dots_smem(CV, n, a, g, n, w);   // V^T p = C_V^T K c_p
-  double s[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double cv = c[i], kv = g[i];
-    for (int l = 0; l < a; ++l) {
-      cv -= CV[i + (size_t)l * n] * w[l];
-      kv -= KCV[i + (size_t)l * n] * w[l];
+  double cv[kRows], kv[kRows];
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    const int i = threadIdx.x + r * kThreads;
+    cv[r] = i < n ? c[i] : 0.0;
+    kv[r] = i < n ? g[i] : 0.0;
+  }
+  for (int l = 0; l < a; ++l) {
+    const double wl = w[l];
+    const double* vc = CV + (size_t)l * n;
+    const double* vk = KCV + (size_t)l * n;
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const int i = threadIdx.x + r * kThreads;
+      if (i < n) {
+        cv[r] -= vc[i] * wl;
+        kv[r] -= vk[i] * wl;
+      }
     }
-    c[i] = cv;
-    g[i] = kv;
-    s[0] += cv * kv;
+  }
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    const int i = threadIdx.x + r * kThreads;
+    if (i < n) {
+      c[i] = cv[r];
+      g[i] = kv[r];
+      s[0] += cv[r] * kv[r];
+    }
   }
   block_sum4(s, 1);
   const double vn = sqrt(s[0]);
@@ -238,11 +291,17 @@ __global__ void __launch_bounds__(kThreads) k_dual_b(DualEng e, int a) {
   }
   __syncthreads();
   dots_smem(CS, n, m, g, n, vs);             // S^T v = C_S^T K c_v
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double ci = c[i], gi = g[i];
-    for (int j = 0; j < m; ++j) {
-      CS[i + (size_t)j * n] -= ci * vs[j];
-      KCS[i + (size_t)j * n] -= gi * vs[j];
+  for (int j = 0; j < m; ++j) {
+    const double vj = vs[j];
+    double* cs = CS + (size_t)j * n;
+    double* ks = KCS + (size_t)j * n;
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const int i = threadIdx.x + r * kThreads;
+      if (i < n) {
+        cs[i] -= c[i] * vj;
+        ks[i] -= g[i] * vj;
+      }
     }
   }
   const double tn = e.scal[2 * f], st = e.scal[2 * f + 1];

@@ -65,11 +65,12 @@ template <bool TA, bool TB>
 __global__ void __launch_bounds__(GEMM_THREADS)
 gemm_f64_dmma(int M, int N, int K, double alpha, const double* __restrict__ A, int lda,
               const double* __restrict__ B, int ldb, double beta, double* __restrict__ C, int ldc,
-              int k_per_split, int use_atomic) {
+              int k_per_split, int use_atomic, int upper) {
   __shared__ double As[2][BK][BM + PAD];
   __shared__ double Bs[2][BK][BN + PAD];
   const int bm = blockIdx.x * BM;
   const int bn = blockIdx.y * BN;
+  if (upper && bm >= bn + BN) return;  // tile entirely below the diagonal
   const int kbeg = blockIdx.z * k_per_split;
   const int kend = min(K, kbeg + k_per_split);
   const int warp = threadIdx.x >> 5;
@@ -345,14 +346,47 @@ void gemm(bool transA, bool transB, int M, int N, int K, double alpha, const dou
   }
   dim3 grid(gm, gn, splits);
   if (!transA && !transB)
-    gemm_f64_dmma<false, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic);
+    gemm_f64_dmma<false, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic, 0);
   else if (transA && !transB)
-    gemm_f64_dmma<true, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic);
+    gemm_f64_dmma<true, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic, 0);
   else if (!transA && transB)
-    gemm_f64_dmma<false, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic);
+    gemm_f64_dmma<false, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic, 0);
   else
-    gemm_f64_dmma<true, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic);
+    gemm_f64_dmma<true, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic, 0);
   ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+__global__ void mirror_upper_f64_kernel(double* K, int n, int ldk) {
+  const size_t total = (size_t)n * n;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = static_cast<int>(t % n), j = static_cast<int>(t / n);
+    if (i > j) K[i + (size_t)j * ldk] = K[j + (size_t)i * ldk];
+  }
+}
+
+void gram_f64(const double* X, int n, int p, int ldx, double* K, int ldk) {
+  if (n <= 0) return;
+  Context& ctx = Context::get();
+  cudaStream_t st = ctx.stream;
+  const int g = ceil_div(n, BM);
+  int splits = 1;
+  const int tiles = g * (g + 1) / 2;
+  const int target = 2 * ctx.sm_count;
+  if (tiles < target && p >= 4 * BK) splits = std::max(1, std::min(ceil_div(target, tiles), ceil_div(p, 8 * BK)));
+  int kps = ceil_div(ceil_div(p, splits), BK) * BK;
+  splits = ceil_div(p, kps);
+  const int use_atomic = splits > 1 ? 1 : 0;
+  if (use_atomic || p <= 0) {
+    scale_matrix_kernel<<<grid_for((size_t)n * n, 256), 256, 0, st>>>(K, n, n, ldk, 0.0); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+  }
+  if (p > 0) {
+    gemm_f64_dmma<false, true><<<dim3(g, g, splits), GEMM_THREADS, 0, st>>>(n, n, p, 1.0, X, ldx, X, ldx, 0.0, K,
+                                                                         ldk, kps, use_atomic, 1); ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+  }
+  mirror_upper_f64_kernel<<<grid_for((size_t)n * n, 256), 256, 0, st>>>(K, n, ldk); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 

@@ -14,6 +14,10 @@ void gemm(bool transA, bool transB, int M, int N, int K, double alpha,
           const double* A, int lda, const double* B, int ldb, double beta,
           double* C, int ldc);
 
+// K (n x n) = X X^T for X n x p: the upper-triangle tiles by FP64 tensor-core
+// MMA, the lower triangle mirrored (K exactly symmetric).
+void gram_f64(const double* X, int n, int p, int ldx, double* K, int ldk);
+
 // y = alpha * op(A) * x + beta * y.  A is rows x cols (lda).
 void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda,
           const double* x, double beta, double* y);

@@ -246,7 +246,6 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   if (dual) {
     double* Kg = ar.alloc_n<double>((size_t)n * n);
     xop->gram(Kg);
-    symmetrize(Kg, n);
     std::unique_ptr<XOperator> kop;
     if (opt.precision == 1) kop = make_split_operator(Kg, n, n, false);
     else kop.reset(new XOperatorF64(Kg, n, n));

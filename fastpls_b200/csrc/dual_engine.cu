@@ -116,14 +116,13 @@ __global__ void k_dual_cs0(DualEng e) {
 // Refresh (power iterations of S S^T from the sketch or the warm start),
 // Householder normalisation, scores t = X_f r, q = Y^T t, and the loading
 // coefficients c_p for the K product.
-__global__ void __launch_bounds__(kThreads) k_dual_a(DualEng e, int a) {
-  extern __shared__ double sm[];
+__device__ bool dual_a(const DualEng& e, int a, double* sm) {
   double* vy = sm;            // n: c_y, later t
   double* vk = sm + e.n;      // n: K c_y, later K c_r
   __shared__ double z[kMaxM];
   __shared__ double zq[kMaxM];
   const int f = blockIdx.x;
-  if (e.status[f]) return;
+  if (e.status[f]) return false;
   const int n = e.n, m = e.m;
   const double* CS = e.CS + (size_t)f * n * m;
   const double* KCS = e.KCS + (size_t)f * n * m;
@@ -183,7 +182,7 @@ __global__ void __launch_bounds__(kThreads) k_dual_a(DualEng e, int a) {
   const double nrm = sqrt(s[0]);
   if (!(nrm > 0.0) || !isfinite(nrm)) {
     if (threadIdx.x == 0) e.status[f] = 1;
-    return;
+    return false;
   }
   const double sg = ((s[1] >= 0.0) ? -1.0 : 1.0) / nrm;
   const double nf = static_cast<double>(e.ntrain[f]);
@@ -213,7 +212,7 @@ __global__ void __launch_bounds__(kThreads) k_dual_a(DualEng e, int a) {
   const double st = t2[1];
   if (!(tn > 0.0) || !isfinite(tn)) {
     if (threadIdx.x == 0) e.status[f] = 1;
-    return;
+    return false;
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     e.cp[(size_t)f * n + i] = (vy[i] - ((e.center && mk[i]) ? st / nf : 0.0)) / tn;
@@ -224,18 +223,18 @@ __global__ void __launch_bounds__(kThreads) k_dual_a(DualEng e, int a) {
     e.scal[2 * f] = tn;
     e.scal[2 * f + 1] = st;
   }
+  return true;
 }
 
 // Gram-Schmidt of the loading against the earlier ones in K-coordinates,
 // normalisation, rank-1 deflation of C_S and K C_S, and the component outputs.
-__global__ void __launch_bounds__(kThreads) k_dual_b(DualEng e, int a) {
-  extern __shared__ double sm[];
+__device__ bool dual_b(const DualEng& e, int a, double* sm) {
   double* g = sm;             // n: K c_p, then K c_v
   double* c = sm + e.n;       // n: c_p, then c_v
   __shared__ double w[kMaxK];
   __shared__ double vs[kMaxM];
   const int f = blockIdx.x;
-  if (e.status[f]) return;
+  if (e.status[f]) return false;
   const int n = e.n, m = e.m, K = e.K;
   double* CV = e.CV + (size_t)f * n * K;
   double* KCV = e.KCV + (size_t)f * n * K;
@@ -281,7 +280,7 @@ __global__ void __launch_bounds__(kThreads) k_dual_b(DualEng e, int a) {
   const double vn = sqrt(s[0]);
   if (!(vn > 0.0) || !isfinite(vn)) {
     if (threadIdx.x == 0) e.status[f] = 1;
-    return;
+    return false;
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     c[i] /= vn;
@@ -313,6 +312,18 @@ __global__ void __launch_bounds__(kThreads) k_dual_b(DualEng e, int a) {
   if (threadIdx.x == 0) {
     e.tnorm[(size_t)f * K + a] = tn;
     e.ncomp_done[f] = a + 1;
+  }
+  return true;
+}
+
+// One launch per component boundary: the Gram-Schmidt / deflation of
+// component a - 1 and then the refresh / scores of component a, per fit.
+__global__ void __launch_bounds__(kThreads) k_dual_step(DualEng e, int a) {
+  extern __shared__ double sm[];
+  if (a > 0 && !dual_b(e, a - 1, sm)) return;
+  if (a < e.K) {
+    __syncthreads();
+    dual_a(e, a, sm);
   }
 }
 
@@ -375,20 +386,17 @@ void dual_simpls_run(const DualBatch& b) {
   const size_t smem = 2 * n * sizeof(double);
   static bool attr = false;
   if (!attr) {
-    FPLS_CUDA(cudaFuncSetAttribute(k_dual_a, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMaxN * 8));
-    FPLS_CUDA(cudaFuncSetAttribute(k_dual_b, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMaxN * 8));
+    FPLS_CUDA(cudaFuncSetAttribute(k_dual_step, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMaxN * 8));
     attr = true;
   }
   PhaseTimer pt("dual SIMPLS engine");
-  for (int a = 0; a < b.K; ++a) {
-    k_dual_a<<<b.F, kThreads, smem, st>>>(e, a); ::fpls::note_launch();
+  for (int a = 0; a <= b.K; ++a) {
+    k_dual_step<<<b.F, kThreads, smem, st>>>(e, a); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
-    pt.mark("refresh + scores");
+    pt.mark("per-fit steps");
+    if (a == b.K) break;
     b.Kop->times(e.cp, b.F, e.Gp);
     pt.mark("K products");
-    k_dual_b<<<b.F, kThreads, smem, st>>>(e, a); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
-    pt.mark("orth + deflate");
   }
   pt.report();
 }

@@ -470,7 +470,7 @@ void XOperatorF64::t_times(const double* T, int F, double* P) {
   else gemm(true, false, p, F, n, 1.0, Xc, n, T, n, 0.0, P, p);
 }
 
-void XOperatorF64::gram(double* K) { gemm(false, true, n, n, p, 1.0, Xc, n, Xc, n, 0.0, K, n); }
+void XOperatorF64::gram(double* K) { gram_f64(Xc, n, p, n, K, n); }
 
 void simpls_batch_crosscov(const SimplsBatch& b, const double* /*Xc*/, const int* /*n_train*/) {
   Context& ctx = Context::get();

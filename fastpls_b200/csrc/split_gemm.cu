@@ -392,21 +392,28 @@ struct GemmPlan {
   std::vector<int> cta_begin, tile_begin;
 };
 
-GemmPlan plan_gemm(int M, int N, int K, int sm_count) {
+// Stream-K plan over the output tiles.  With `upper` only the tiles that
+// reach the upper triangle (tile row start < tile column end) are planned, for
+// symmetric products whose lower triangle is mirrored afterwards.
+GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false) {
   GemmPlan g;
   const int mt = (M + BM - 1) / BM;
   g.ntn = (N + BN - 1) / BN;
   g.tiles = mt * g.ntn;
+  std::vector<int> inc;
+  inc.reserve(g.tiles);
+  for (int t = 0; t < g.tiles; ++t)
+    if (!upper || (t / g.ntn) * BM < ((t % g.ntn) + 1) * BN) inc.push_back(t);
   const int kbt = (K + BK - 1) / BK;
-  const long long total = static_cast<long long>(g.tiles) * kbt;
-  g.ctas = static_cast<int>(std::min<long long>(sm_count, total));
+  const long long total = static_cast<long long>(inc.size()) * kbt;
+  g.ctas = static_cast<int>(std::max<long long>(1, std::min<long long>(sm_count, total)));
   g.cta_begin.assign(g.ctas + 1, 0);
   g.tile_begin.assign(g.tiles + 1, 0);
   for (int c = 0; c < g.ctas; ++c) {
     g.cta_begin[c] = static_cast<int>(g.segs.size());
     long long a = total * c / g.ctas, e = total * (c + 1) / g.ctas;
     while (a < e) {
-      const int t = static_cast<int>(a / kbt);
+      const int t = inc[static_cast<size_t>(a / kbt)];
       const int kb0 = static_cast<int>(a % kbt);
       const int kb1 = static_cast<int>(std::min<long long>(kbt, kb0 + (e - a)));
       g.segs.push_back(make_int4(t, kb0, kb1, 0));
@@ -503,18 +510,18 @@ struct CachedPlan {
   char* dev = nullptr;
   GemmScratch s;
 };
-std::map<std::array<int, 4>, CachedPlan>& plan_cache() {
-  static std::map<std::array<int, 4>, CachedPlan> cache;
+std::map<std::array<int, 5>, CachedPlan>& plan_cache() {
+  static std::map<std::array<int, 5>, CachedPlan> cache;
   return cache;
 }
 
-const CachedPlan& cached_plan(int M, int N, int K, int sm_count, cudaStream_t st) {
+const CachedPlan& cached_plan(int M, int N, int K, int sm_count, cudaStream_t st, bool upper = false) {
   auto& cache = plan_cache();
-  const std::array<int, 4> key{M, N, K, sm_count};
+  const std::array<int, 5> key{M, N, K, sm_count, upper ? 1 : 0};
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
   CachedPlan c;
-  c.g = plan_gemm(M, N, K, sm_count);
+  c.g = plan_gemm(M, N, K, sm_count, upper);
   FPLS_CUDA(cudaMalloc(&c.dev, gemm_scratch_bytes(c.g)));
   c.s = carve_gemm_scratch(c.g, c.dev);
   upload_plan_tables(c.g, c.s, st);
@@ -522,11 +529,26 @@ const CachedPlan& cached_plan(int M, int N, int K, int sm_count, cudaStream_t st
 }
 
 void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,
-                double beta, double* C, int ldc) {
+                double beta, double* C, int ldc, bool upper = false) {
   Context& ctx = Context::get();
-  const CachedPlan& c = cached_plan(M, N, K, ctx.sm_count, ctx.stream);
+  const CachedPlan& c = cached_plan(M, N, K, ctx.sm_count, ctx.stream, upper);
   split_gemm_run(A, B, M, N, K, alpha, beta, C, ldc, c.g, c.s, ctx.d_status + 16, ctx.stream,
                  ctx.profile ? &ctx : nullptr);
+}
+
+__global__ void mirror_upper_kernel(double* K, int n) {
+  const size_t total = (size_t)n * n;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = static_cast<int>(t % n), j = static_cast<int>(t / n);
+    if (i > j) K[t] = K[j + (size_t)i * n];
+  }
+}
+
+// K[i, j] = K[j, i] for i > j (n x n).
+void mirror_upper(double* K, int n) {
+  Context& ctx = Context::get();
+  mirror_upper_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(K, n); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
 }
 
 void split_cols_on(const double* X, int rows, int cols, int ld, const SplitPair& out, cudaStream_t st,
@@ -569,7 +591,11 @@ struct XOperatorSplit : public XOperator {
     split_cols(Rhat, p, F, p, b);
     split_gemm(xr, b, n, F, p, 1.0, 0.0, U, n);
   }
-  void gram(double* K) override { split_gemm(xr, xr, n, n, p, 1.0, 0.0, K, n); }
+  void gram(double* K) override {
+    // upper-triangle tiles only; the lower triangle is mirrored
+    split_gemm(xr, xr, n, n, p, 1.0, 0.0, K, n, true);
+    mirror_upper(K, n);
+  }
   void t_times(const double* T, int F, double* P) override {
     FPLS_REQUIRE(has_t, "split operator built without its transposed copy");
     SplitPair b = alloc_pair(F, n);

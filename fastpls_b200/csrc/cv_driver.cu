@@ -244,11 +244,14 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   int* ncd = ar.alloc_n<int>(Fa);
   int* sto = ar.alloc_n<int>(Fa);
   if (dual) {
+    // The Gram contracts over all p columns (BF16x3 on the tensor cores in the
+    // mixed mode); the per-component products with the L2-resident K stay
+    // FP64: the K-coordinate Gram-Schmidt carries K C_V and K C_S forward, and
+    // split-precision products there drift from one component to the next.
     double* Kg = ar.alloc_n<double>((size_t)n * n);
     xop->gram(Kg);
-    std::unique_ptr<XOperator> kop;
-    if (opt.precision == 1) kop = make_split_operator(Kg, n, n, false);
-    else kop.reset(new XOperatorF64(Kg, n, n));
+    XOperatorF64 kop_f64(Kg, n, n);
+    XOperator* kop = &kop_f64;
     pt.mark("row gram");
     FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0));
     double* XOm = ar.alloc_n<double>((size_t)n * Fa);
@@ -259,7 +262,7 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
     db.power_iters = opt.power_iters;
     db.m1_mode = (m == 1);
     db.center = center;
-    db.Kop = kop.get();
+    db.Kop = kop;
     db.x0 = X;
     db.XOmega = XOm;
     db.mask = d_tr;

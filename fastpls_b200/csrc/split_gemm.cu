@@ -395,6 +395,8 @@ struct GemmPlan {
 // Stream-K plan over the output tiles.  With `upper` only the tiles that
 // reach the upper triangle (tile row start < tile column end) are planned, for
 // symmetric products whose lower triangle is mirrored afterwards.
+constexpr int kSymSegBlocks = 16;
+
 GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false) {
   GemmPlan g;
   const int mt = (M + BM - 1) / BM;
@@ -405,6 +407,10 @@ GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false) {
   for (int t = 0; t < g.tiles; ++t)
     if (!upper || (t / g.ntn) * BM < ((t % g.ntn) + 1) * BN) inc.push_back(t);
   const int kbt = (K + BK - 1) / BK;
+  // A symmetric (Gram) product sums the whole contraction of each tile in one
+  // CTA; cutting it into segments of at most kSymSegBlocks K-blocks keeps each
+  // FP32 accumulation short and adds the segments in FP64.
+  const int kseg = upper ? kSymSegBlocks : kbt;
   const long long total = static_cast<long long>(inc.size()) * kbt;
   g.ctas = static_cast<int>(std::max<long long>(1, std::min<long long>(sm_count, total)));
   g.cta_begin.assign(g.ctas + 1, 0);
@@ -415,7 +421,8 @@ GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false) {
     while (a < e) {
       const int t = inc[static_cast<size_t>(a / kbt)];
       const int kb0 = static_cast<int>(a % kbt);
-      const int kb1 = static_cast<int>(std::min<long long>(kbt, kb0 + (e - a)));
+      int kb1 = static_cast<int>(std::min<long long>(kbt, kb0 + (e - a)));
+      kb1 = std::min(kb1, (kb0 / kseg + 1) * kseg);
       g.segs.push_back(make_int4(t, kb0, kb1, 0));
       a += kb1 - kb0;
     }

@@ -63,7 +63,8 @@ def test_dual_bf16x3_close_to_fp64(lib, wide):
     a = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], seed=1, precision="fp64")
     b = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], seed=1, precision="bf16x3")
     assert np.allclose(a["inner_accuracy"], b["inner_accuracy"], atol=5e-3)
-    assert np.mean(a["pred"] == b["pred"]) >= 0.99
+    assert np.array_equal(a["best_comp"], b["best_comp"])
+    assert np.mean(a["pred"] == b["pred"]) >= 0.995
 
 
 @pytest.mark.parametrize("dual", ["1", "0"])

@@ -7,11 +7,13 @@
 #include "blas_f64.cuh"
 #include "context.cuh"
 
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
 namespace fpls {
 namespace {
 
-constexpr int kThreads = 512;
-constexpr int kWarps = kThreads / 32;
 constexpr int kMaxN = 8192;     // n-vectors staged in shared memory
 constexpr int kMaxM = 128;
 constexpr int kMaxK = 256;
@@ -41,60 +43,86 @@ struct DualEng {
   int* status;
 };
 
-constexpr int kRows = kMaxN / kThreads;   // rows of an n-vector held per thread
+// Each fit is handled by a cluster of kCl CTAs; CTA r of the cluster owns rows
+// [r * rows_per, (r + 1) * rows_per) of every n-vector of the fit and keeps
+// them in registers (kLR rows per thread).  Reductions over the n rows are
+// per-CTA (warp shuffles, shared memory) and then across the cluster through
+// distributed shared memory, summed in rank order so every CTA of the cluster
+// sees bit-identical results and takes the same branches.
+constexpr int kCl = 4;
+constexpr int kT = 256;
+constexpr int kW = kT / 32;
+constexpr int kLR = kMaxN / kCl / kT;     // 8 rows per thread
+constexpr int kRedMax = kMaxK > kMaxM + 2 ? kMaxK : kMaxM + 2;
 
-// out[j] = sum_i M[i + j*ld] * xs[i] for j < ncols, xs in shared memory.  With
-// fewer columns than warps, several warps split the rows of one column; every
-// lane keeps four independent partial sums.  Ends with a barrier.
-__device__ void dots_smem(const double* __restrict__ M, size_t ld, int ncols, const double* xs, int rows,
-                          double* out) {
-  __shared__ double red[kWarps];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = ncols >= kWarps ? 1 : kWarps / max(ncols, 1);   // warps per column
-  const int cols_per_pass = kWarps / g;
-  for (int j0 = 0; j0 < ncols; j0 += cols_per_pass) {
-    const int j = j0 + warp / g, sub = warp % g;
-    double acc = 0.0;
-    if (j < ncols && warp / g < cols_per_pass) {
-      const double* col = M + (size_t)j * ld;
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      const int step = 32 * g;
-      int r = sub * 32 + lane;
-      for (; r + 3 * step < rows; r += 4 * step) {
-        a0 += col[r] * xs[r];
-        a1 += col[r + step] * xs[r + step];
-        a2 += col[r + 2 * step] * xs[r + 2 * step];
-        a3 += col[r + 3 * step] * xs[r + 3 * step];
-      }
-      for (; r < rows; r += step) a0 += col[r] * xs[r];
-      acc = warp_sum((a0 + a1) + (a2 + a3));
-    }
-    if (lane == 0) red[warp] = acc;
-    __syncthreads();
-    if (threadIdx.x < cols_per_pass && j0 + threadIdx.x < ncols) {
-      double t = 0.0;
-      for (int u = 0; u < g; ++u) t += red[threadIdx.x * g + u];
-      out[j0 + threadIdx.x] = t;
-    }
-    __syncthreads();
+struct ClusterRed {
+  double warp[kW][kRedMax];
+  double part[2][kRedMax];
+  double res[kRedMax];
+  int buf;
+};
+
+struct Rows {
+  int r0, nl;  // first owned row, owned row count
+  __device__ __forceinline__ bool ok(int k) const { return (int)threadIdx.x + k * kT < nl; }
+  __device__ __forceinline__ int row(int k) const { return r0 + (int)threadIdx.x + k * kT; }
+};
+
+// part[buf][0..count) holds this CTA's partials (after a barrier): sum them
+// over the cluster into res[0..count); ends with res visible to the CTA.
+__device__ void cluster_exchange(ClusterRed& R, int count) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int b = R.buf;
+  cl.sync();
+  for (int k = threadIdx.x; k < count; k += kT) {
+    double s = 0.0;
+    for (int r = 0; r < kCl; ++r) s += cl.map_shared_rank(&R.part[b][0], r)[k];
+    R.res[k] = s;
   }
+  __syncthreads();
+  if (threadIdx.x == 0) R.buf = b ^ 1;
+  __syncthreads();
 }
 
-// Block sum of up to 4 values per thread; result broadcast to every thread.
-__device__ void block_sum4(double (&v)[4], int count) {
-  __shared__ double red[kWarps][4];
+// res[0..count) = cluster sums of the per-thread values v[0..count) (count <= 4).
+__device__ void cluster_sum(ClusterRed& R, double (&v)[4], int count) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int k = 0; k < count; ++k) {
     const double w = warp_sum(v[k]);
-    if (lane == 0) red[warp][k] = w;
+    if (lane == 0) R.warp[warp][k] = w;
   }
   __syncthreads();
-  for (int k = 0; k < count; ++k) {
+  if (threadIdx.x < count) {
     double s = 0.0;
-    for (int w = 0; w < kWarps; ++w) s += red[w][k];
-    v[k] = s;
+    for (int w = 0; w < kW; ++w) s += R.warp[w][threadIdx.x];
+    R.part[R.buf][threadIdx.x] = s;
   }
   __syncthreads();
+  cluster_exchange(R, count);
+}
+
+// res[j] = sum over the fit's rows of M[i + j*n] * x_i for j < ncols, with x
+// given by the owned rows in registers.
+__device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M, int n, int ncols, const Rows& rw,
+                             const double (&x)[kLR]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int j = 0; j < ncols; ++j) {
+    const double* col = M + (size_t)j * n;
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < kLR; ++k)
+      if (rw.ok(k)) acc += col[rw.row(k)] * x[k];
+    acc = warp_sum(acc);
+    if (lane == 0) R.warp[warp][j] = acc;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < ncols; j += kT) {
+    double s = 0.0;
+    for (int w = 0; w < kW; ++w) s += R.warp[w][j];
+    R.part[R.buf][j] = s;
+  }
+  __syncthreads();
+  cluster_exchange(R, ncols);
 }
 
 // C_S of every fit: mask_f * (onehot(label) - (mY_all + dY_f)).
@@ -116,215 +144,221 @@ __global__ void k_dual_cs0(DualEng e) {
 // Refresh (power iterations of S S^T from the sketch or the warm start),
 // Householder normalisation, scores t = X_f r, q = Y^T t, and the loading
 // coefficients c_p for the K product.
-__device__ bool dual_a(const DualEng& e, int a, double* sm) {
-  double* vy = sm;            // n: c_y, later t
-  double* vk = sm + e.n;      // n: K c_y, later K c_r
-  __shared__ double z[kMaxM];
-  __shared__ double zq[kMaxM];
-  const int f = blockIdx.x;
-  if (e.status[f]) return false;
+__device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank) {
+  __shared__ double zloc[kMaxM + 2];
+  const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m;
   const double* CS = e.CS + (size_t)f * n * m;
   const double* KCS = e.KCS + (size_t)f * n * m;
   const uint8_t* mk = e.mask + (size_t)f * n;
+  double cy[kLR], ky[kLR];
   int steps = e.iters;
   if (e.m1) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      vy[i] = CS[i];
-      vk[i] = KCS[i];
+#pragma unroll
+    for (int k = 0; k < kLR; ++k) {
+      cy[k] = rw.ok(k) ? CS[rw.row(k)] : 0.0;
+      ky[k] = rw.ok(k) ? KCS[rw.row(k)] : 0.0;
     }
-    __syncthreads();
     steps = 0;
   } else {
     // z = S^T (start): the sketch through X Omega at the first component,
     // else the warm start r_{a-1} through its K image.
     const double* src = (a == 0) ? e.XOmega + (size_t)f * n : e.Kcy + (size_t)f * n;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) vk[i] = src[i];
-    __syncthreads();
-    dots_smem(CS, n, m, vk, n, z);
+#pragma unroll
+    for (int k = 0; k < kLR; ++k) ky[k] = rw.ok(k) ? src[rw.row(k)] : 0.0;
+    cluster_dots(R, CS, n, m, rw, ky);
   }
   for (int it = 0; it < steps; ++it) {
-    // y = S z: c_y = C_S z, K c_y = (K C_S) z (rows held in registers)
-    double c[kRows], k[kRows];
+    // y = S z: c_y = C_S z, K c_y = (K C_S) z, z in R.res
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) c[r] = k[r] = 0.0;
+    for (int k = 0; k < kLR; ++k) cy[k] = ky[k] = 0.0;
     for (int j = 0; j < m; ++j) {
-      const double zj = z[j];
+      const double zj = R.res[j];
       const double* cs = CS + (size_t)j * n;
       const double* ks = KCS + (size_t)j * n;
 #pragma unroll
-      for (int r = 0; r < kRows; ++r) {
-        const int i = threadIdx.x + r * kThreads;
-        if (i < n) {
-          c[r] += cs[i] * zj;
-          k[r] += ks[i] * zj;
+      for (int k = 0; k < kLR; ++k)
+        if (rw.ok(k)) {
+          cy[k] += cs[rw.row(k)] * zj;
+          ky[k] += ks[rw.row(k)] * zj;
         }
-      }
     }
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-      const int i = threadIdx.x + r * kThreads;
-      if (i < n) {
-        vy[i] = c[r];
-        vk[i] = k[r];
-      }
-    }
-    __syncthreads();
-    if (it + 1 < steps) dots_smem(CS, n, m, vk, n, z);
+    if (it + 1 < steps) cluster_dots(R, CS, n, m, rw, ky);
   }
-  // ||y||^2 = c_y^T K c_y, y[0] = Xc[:,0]^T c_y, and the train-row count
+  // ||y||^2 = c_y^T K c_y and y[0] = Xc[:,0]^T c_y
   double s[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    s[0] += vy[i] * vk[i];
-    s[1] += e.x0[i] * vy[i];
-  }
-  block_sum4(s, 2);
-  const double nrm = sqrt(s[0]);
+#pragma unroll
+  for (int k = 0; k < kLR; ++k)
+    if (rw.ok(k)) {
+      s[0] += cy[k] * ky[k];
+      s[1] += e.x0[rw.row(k)] * cy[k];
+    }
+  cluster_sum(R, s, 2);
+  const double nrm = sqrt(R.res[0]);
+  const double y0 = R.res[1];
   if (!(nrm > 0.0) || !isfinite(nrm)) {
-    if (threadIdx.x == 0) e.status[f] = 1;
+    if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
     return false;
   }
-  const double sg = ((s[1] >= 0.0) ? -1.0 : 1.0) / nrm;
+  const double sg = ((y0 >= 0.0) ? -1.0 : 1.0) / nrm;
   const double nf = static_cast<double>(e.ntrain[f]);
-  // U = X r = sg * K c_y; c = mean of U over the train rows
+  // U = X r = sg * K c_y; its mean over the train rows centres the scores
   double u[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int i = threadIdx.x; i < n; i += blockDim.x)
-    if (mk[i]) u[0] += sg * vk[i];
-  block_sum4(u, 1);
-  const double cmean = e.center ? u[0] / nf : 0.0;
-  double* keep = e.Tkeep ? e.Tkeep + ((size_t)f * e.K + a) * n : nullptr;
-  for (int j = threadIdx.x; j < m; j += blockDim.x) zq[j] = 0.0;
-  __syncthreads();
-  double t2[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double U = sg * vk[i];
-    const double uc = U - cmean;
-    const double t = mk[i] ? uc : 0.0;
-    if (keep) keep[i] = uc;
-    t2[0] += t * t;
-    t2[1] += t;
-    if (t != 0.0) atomicAdd(&zq[e.labels[i]], t);
-    vk[i] = U;
-    vy[i] = t;
+#pragma unroll
+  for (int k = 0; k < kLR; ++k) {
+    ky[k] *= sg;
+    if (rw.ok(k) && mk[rw.row(k)]) u[0] += ky[k];
   }
-  block_sum4(t2, 2);
-  const double tn = sqrt(t2[0]);
-  const double st = t2[1];
+  cluster_sum(R, u, 1);
+  const double cmean = e.center ? R.res[0] / nf : 0.0;
+  double* keep = e.Tkeep ? e.Tkeep + ((size_t)f * e.K + a) * n : nullptr;
+  for (int j = threadIdx.x; j < m + 2; j += kT) zloc[j] = 0.0;
+  __syncthreads();
+  double t2[2] = {0.0, 0.0};
+  double t[kLR];
+#pragma unroll
+  for (int k = 0; k < kLR; ++k) {
+    t[k] = 0.0;
+    if (!rw.ok(k)) continue;
+    const int i = rw.row(k);
+    const double uc = ky[k] - cmean;
+    if (keep) keep[i] = uc;
+    if (mk[i]) {
+      t[k] = uc;
+      t2[0] += uc * uc;
+      t2[1] += uc;
+      if (uc != 0.0) atomicAdd(&zloc[e.labels[i]], uc);
+    }
+  }
+  {
+    const double a0 = warp_sum(t2[0]), a1 = warp_sum(t2[1]);
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&zloc[m], a0);
+      atomicAdd(&zloc[m + 1], a1);
+    }
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < m + 2; j += kT) R.part[R.buf][j] = zloc[j];
+  __syncthreads();
+  cluster_exchange(R, m + 2);
+  const double tn = sqrt(R.res[m]);
+  const double st = R.res[m + 1];
   if (!(tn > 0.0) || !isfinite(tn)) {
-    if (threadIdx.x == 0) e.status[f] = 1;
+    if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
     return false;
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    e.cp[(size_t)f * n + i] = (vy[i] - ((e.center && mk[i]) ? st / nf : 0.0)) / tn;
-    e.Kcy[(size_t)f * n + i] = vk[i] / tn;
+#pragma unroll
+  for (int k = 0; k < kLR; ++k) {
+    if (!rw.ok(k)) continue;
+    const int i = rw.row(k);
+    e.cp[(size_t)f * n + i] = (t[k] - ((e.center && mk[i]) ? st / nf : 0.0)) / tn;
+    e.Kcy[(size_t)f * n + i] = ky[k] / tn;
   }
-  for (int j = threadIdx.x; j < m; j += blockDim.x) e.qs[(size_t)f * m + j] = zq[j];
-  if (threadIdx.x == 0) {
-    e.scal[2 * f] = tn;
-    e.scal[2 * f + 1] = st;
+  if (rank == 0) {
+    for (int j = threadIdx.x; j < m; j += kT) e.qs[(size_t)f * m + j] = R.res[j];
+    if (threadIdx.x == 0) {
+      e.scal[2 * f] = tn;
+      e.scal[2 * f + 1] = st;
+    }
   }
   return true;
 }
 
 // Gram-Schmidt of the loading against the earlier ones in K-coordinates,
 // normalisation, rank-1 deflation of C_S and K C_S, and the component outputs.
-__device__ bool dual_b(const DualEng& e, int a, double* sm) {
-  double* g = sm;             // n: K c_p, then K c_v
-  double* c = sm + e.n;       // n: c_p, then c_v
-  __shared__ double w[kMaxK];
-  __shared__ double vs[kMaxM];
-  const int f = blockIdx.x;
-  if (e.status[f]) return false;
+__device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank) {
+  const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m, K = e.K;
   double* CV = e.CV + (size_t)f * n * K;
   double* KCV = e.KCV + (size_t)f * n * K;
   double* CS = e.CS + (size_t)f * n * m;
   double* KCS = e.KCS + (size_t)f * n * m;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    g[i] = e.Gp[(size_t)f * n + i];
-    c[i] = e.cp[(size_t)f * n + i];
-  }
-  __syncthreads();
-  if (a > 0) dots_smem(CV, n, a, g, n, w);   // V^T p = C_V^T K c_p
-  double cv[kRows], kv[kRows];
+  double cv[kLR], kv[kLR];
 #pragma unroll
-  for (int r = 0; r < kRows; ++r) {
-    const int i = threadIdx.x + r * kThreads;
-    cv[r] = i < n ? c[i] : 0.0;
-    kv[r] = i < n ? g[i] : 0.0;
+  for (int k = 0; k < kLR; ++k) {
+    cv[k] = rw.ok(k) ? e.cp[(size_t)f * n + rw.row(k)] : 0.0;
+    kv[k] = rw.ok(k) ? e.Gp[(size_t)f * n + rw.row(k)] : 0.0;
   }
-  for (int l = 0; l < a; ++l) {
-    const double wl = w[l];
-    const double* vc = CV + (size_t)l * n;
-    const double* vk = KCV + (size_t)l * n;
+  if (a > 0) {
+    cluster_dots(R, CV, n, a, rw, kv);   // V^T p = C_V^T K c_p
+    for (int l = 0; l < a; ++l) {
+      const double wl = R.res[l];
+      const double* vc = CV + (size_t)l * n;
+      const double* vk = KCV + (size_t)l * n;
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-      const int i = threadIdx.x + r * kThreads;
-      if (i < n) {
-        cv[r] -= vc[i] * wl;
-        kv[r] -= vk[i] * wl;
-      }
+      for (int k = 0; k < kLR; ++k)
+        if (rw.ok(k)) {
+          cv[k] -= vc[rw.row(k)] * wl;
+          kv[k] -= vk[rw.row(k)] * wl;
+        }
     }
   }
   double s[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-  for (int r = 0; r < kRows; ++r) {
-    const int i = threadIdx.x + r * kThreads;
-    if (i < n) {
-      c[i] = cv[r];
-      g[i] = kv[r];
-      s[0] += cv[r] * kv[r];
-    }
-  }
-  block_sum4(s, 1);
-  const double vn = sqrt(s[0]);
+  for (int k = 0; k < kLR; ++k) s[0] += cv[k] * kv[k];
+  cluster_sum(R, s, 1);
+  const double vn = sqrt(R.res[0]);
   if (!(vn > 0.0) || !isfinite(vn)) {
-    if (threadIdx.x == 0) e.status[f] = 1;
+    if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
     return false;
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    c[i] /= vn;
-    g[i] /= vn;
-    CV[i + (size_t)a * n] = c[i];
-    KCV[i + (size_t)a * n] = g[i];
+#pragma unroll
+  for (int k = 0; k < kLR; ++k) {
+    cv[k] /= vn;
+    kv[k] /= vn;
+    if (rw.ok(k)) {
+      CV[rw.row(k) + (size_t)a * n] = cv[k];
+      KCV[rw.row(k) + (size_t)a * n] = kv[k];
+    }
   }
-  __syncthreads();
-  dots_smem(CS, n, m, g, n, vs);             // S^T v = C_S^T K c_v
+  cluster_dots(R, CS, n, m, rw, kv);     // S^T v = C_S^T K c_v
   for (int j = 0; j < m; ++j) {
-    const double vj = vs[j];
+    const double vj = R.res[j];
     double* cs = CS + (size_t)j * n;
     double* ks = KCS + (size_t)j * n;
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-      const int i = threadIdx.x + r * kThreads;
-      if (i < n) {
-        cs[i] -= c[i] * vj;
-        ks[i] -= g[i] * vj;
+    for (int k = 0; k < kLR; ++k)
+      if (rw.ok(k)) {
+        cs[rw.row(k)] -= cv[k] * vj;
+        ks[rw.row(k)] -= kv[k] * vj;
       }
+  }
+  if (rank == 0) {
+    const double tn = e.scal[2 * f], st = e.scal[2 * f + 1];
+    double* Qcol = e.Q + ((size_t)f * K + a) * m;
+    for (int j = threadIdx.x; j < m; j += kT) {
+      const double off = e.mY_all[j] + (e.dY ? e.dY[(size_t)f * m + j] : 0.0);
+      Qcol[j] = (e.qs[(size_t)f * m + j] - off * st) / tn;
     }
-  }
-  const double tn = e.scal[2 * f], st = e.scal[2 * f + 1];
-  double* Qcol = e.Q + ((size_t)f * K + a) * m;
-  for (int j = threadIdx.x; j < m; j += blockDim.x) {
-    const double off = e.mY_all[j] + (e.dY ? e.dY[(size_t)f * m + j] : 0.0);
-    Qcol[j] = (e.qs[(size_t)f * m + j] - off * st) / tn;
-  }
-  if (threadIdx.x == 0) {
-    e.tnorm[(size_t)f * K + a] = tn;
-    e.ncomp_done[f] = a + 1;
+    if (threadIdx.x == 0) {
+      e.tnorm[(size_t)f * K + a] = tn;
+      e.ncomp_done[f] = a + 1;
+    }
   }
   return true;
 }
 
 // One launch per component boundary: the Gram-Schmidt / deflation of
 // component a - 1 and then the refresh / scores of component a, per fit.
-__global__ void __launch_bounds__(kThreads) k_dual_step(DualEng e, int a) {
-  extern __shared__ double sm[];
-  if (a > 0 && !dual_b(e, a - 1, sm)) return;
-  if (a < e.K) {
-    __syncthreads();
-    dual_a(e, a, sm);
-  }
+__global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kT) k_dual_step(DualEng e, int a) {
+  __shared__ ClusterRed R;
+  const int f = blockIdx.x / kCl;
+  const int rank = static_cast<int>(cg::this_cluster().block_rank());
+  if (e.status[f]) return;   // set only in earlier launches: uniform over the cluster, before any remote access
+  if (threadIdx.x == 0) R.buf = 0;
+  __syncthreads();
+  const int rows_per = (e.n + kCl - 1) / kCl;
+  Rows rw;
+  rw.r0 = rank * rows_per;
+  rw.nl = max(0, min(e.n, rw.r0 + rows_per) - rw.r0);
+  // Every CTA of the cluster takes the same branches (they follow the
+  // cluster-wide sums, identical in all CTAs), and all of them end on the same
+  // cluster barrier, which also keeps each CTA's shared memory alive until the
+  // last remote read of it.
+  bool ok = true;
+  if (a > 0) ok = dual_b(e, a - 1, R, rw, rank);
+  if (ok && a < e.K) dual_a(e, a, R, rw, rank);
+  cg::this_cluster().sync();
 }
 
 __global__ void symmetrize_kernel(double* K, int n) {
@@ -383,15 +417,9 @@ void dual_simpls_run(const DualBatch& b) {
   k_dual_cs0<<<2 * ctx.sm_count, 256, 0, st>>>(e); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   b.Kop->times(e.CS, static_cast<int>(F * m), e.KCS);   // K C_S for every fit
-  const size_t smem = 2 * n * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    FPLS_CUDA(cudaFuncSetAttribute(k_dual_step, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMaxN * 8));
-    attr = true;
-  }
   PhaseTimer pt("dual SIMPLS engine");
   for (int a = 0; a <= b.K; ++a) {
-    k_dual_step<<<b.F, kThreads, smem, st>>>(e, a); ::fpls::note_launch();
+    k_dual_step<<<b.F * kCl, kT, 0, st>>>(e, a); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     pt.mark("per-fit steps");
     if (a == b.K) break;

@@ -115,22 +115,63 @@ class Clocks:
 
 
 def measured_peaks():
+    """HBM GB/s and dense BF16 TFLOP/s denominators (burst figures: the kernels
+    are timed inside a step of a few milliseconds)."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
         d = json.load(open(path))
-        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
-    return 6650.0, "fallback 6.65 TB/s"
+        return dict(hbm=(float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"),
+                    bf16=(float(d["bf16_tflops"]), "measured (MEASURED_PEAKS.json bf16_tflops, burst)"),
+                    fp64=(40.0, "nominal B200 FP64 tensor 40 TFLOP/s (no measured FP64 figure)"))
+    return dict(hbm=(6650.0, "fallback 6.65 TB/s"), bf16=(1590.0, "fallback 1.59 PFLOP/s"),
+                fp64=(40.0, "nominal B200 FP64 tensor 40 TFLOP/s (no measured FP64 figure)"))
 
 
-def profile_traffic():
-    """Per-launch DRAM traffic of the split GEMM from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "split_gemm_c4_traffic.json")
+# kernel class -> (roofline bound, peak key, kernel description, ncu traffic file)
+KERNEL_CLASSES = {
+    "dual_step": ("hbm", "hbm", "k_dual_step (per-fit SIMPLS steps in row space, 4-CTA clusters)",
+                  "k_dual_step_c4_traffic.json"),
+    "k_products_f64": ("tensor", "fp64", "gemm_f64_dmma (batched K products, FP64 DMMA)", None),
+    "gram_bf16x3": ("tensor", "bf16", "split_gemm_kernel (tcgen05 BF16x3 row Gram, upper tiles)", None),
+    "split_gemm_bf16x3": ("hbm", "hbm", "split_gemm_kernel (tcgen05 BF16x3 skinny GEMM)",
+                          "split_gemm_c4_traffic.json"),
+}
+
+
+def profile_traffic(fname):
+    """Per-launch DRAM traffic of a kernel from its committed ncu summary."""
+    if not fname:
+        return None
+    path = os.path.join(ROOT, "profiles", fname)
     if os.path.exists(path):
         try:
             return json.load(open(path)).get("traffic_bytes_per_launch_full_size")
         except (OSError, ValueError):
             return None
     return None
+
+
+def kernel_rooflines(classes, peaks):
+    """Achieved bandwidth or throughput of each profiled kernel class against
+    its roofline; the class with the most device time is the dominant one."""
+    out = []
+    for c in classes:
+        bound, key, desc, tfile = KERNEL_CLASSES.get(c["name"], ("hbm", "hbm", c["name"], None))
+        per_ms = c["ms"] / max(c["launches"], 1)
+        peak, src = peaks[key]
+        if bound == "hbm":
+            ach = (c["bytes"] / max(c["launches"], 1)) / (per_ms / 1e3) / 1e9 if per_ms > 0 else None
+            unit = "GB/s"
+        else:
+            ach = (c["flops"] / max(c["launches"], 1)) / (per_ms / 1e3) / 1e12 if per_ms > 0 else None
+            unit = "TFLOP/s"
+        out.append(dict(bound=bound, achieved=ach, peak=peak, unit=unit, frac=(ach / peak) if ach else None,
+                        traffic=profile_traffic(tfile), kernel=desc, launches=c["launches"],
+                        total_ms=c["ms"], avg_launch_ms=per_ms,
+                        algorithmic_bytes_per_launch=c["bytes"] / max(c["launches"], 1),
+                        algorithmic_flops_per_launch=c["flops"] / max(c["launches"], 1), peak_source=src))
+    out.sort(key=lambda r: -r["total_ms"])
+    return out
 
 
 def cpu_baseline(d, max_seconds=30.0):
@@ -238,7 +279,8 @@ def run_ours(args):
         for _ in range(args.steps):
             r_mixed, ms = step_value()
             times.append(ms)
-    prof = lib.profile_end()
+    lib.profile_end()
+    kernels = kernel_rooflines(lib.profile_classes(), measured_peaks())
     launches = lib.launch_count() - launches0
     clocks = clk.summary()
     barrier(pg)
@@ -270,10 +312,6 @@ def run_ours(args):
         r_plain, plain_ms = step_value("fp64", False)
     barrier(pg)
 
-    peak, peak_src = measured_peaks()
-    per_launch_bytes = prof["bytes"] / max(prof["launches"], 1)
-    per_launch_ms = prof["ms"] / max(prof["launches"], 1)
-    achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else None
     agree = float(np.mean(r_mixed["pred"] == r64["pred"]))
     rows_per_fit = np.mean([np.sum((d["outer"] != o) & (d["inner"][:, o] != i))
                             for o in range(10) for i in range(5)])
@@ -287,11 +325,8 @@ def run_ours(args):
         x_rows_per_s=world * rows_per_fit * 50 * args.steps / (total_ms / 1e3),
         e2e=dict(value=e2e_value, unit="fits/s", h2d_bytes_per_step=int(h2d),
                  d2h_bytes_per_step=int(d2h), ms_per_step=e2e_ms / args.steps),
-        roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s",
-                      frac=(achieved / peak) if achieved else None, traffic=profile_traffic(),
-                      kernel="split_gemm_kernel (tcgen05 BF16x3 skinny GEMM)",
-                      launches=prof["launches"], avg_launch_ms=per_launch_ms,
-                      algorithmic_bytes_per_launch=per_launch_bytes, peak_source=peak_src),
+        roofline=kernels[0] if kernels else None,
+        kernel_rooflines=kernels[1:],
         clocks=clocks, gpu_launches=int(launches),
         fp64_batched=dict(ms_per_step=fp64_batched_ms, fits_per_s=FITS_PER_RUN / (fp64_batched_ms / 1e3)),
         parity=dict(outer_pred_agreement_bf16x3_vs_fp64=agree,

@@ -77,6 +77,8 @@ SIGNATURES = {
                                _I, _I, _I, _I, _D, _D, _I, _I, _IP, _DP, _C, _S], ctypes.c_int),
     "fpls_label_aware_cknn_resident": ([_I, _IP, _I, _I, _I, _I, _I, _I, _I, _I, _I, _D, _D, _I, _I,
                                         _IP, _DP, _C, _S], ctypes.c_int),
+    "fpls_profile_class": ([_I, ctypes.c_char_p, _S, _DP, ctypes.POINTER(ctypes.c_longlong), _DP, _DP,
+                            _C, _S], ctypes.c_int),
     "fpls_host_register": ([ctypes.c_void_p, _S, _C, _S], ctypes.c_int),
     "fpls_host_unregister": ([ctypes.c_void_p, _C, _S], ctypes.c_int),
     "fpls_gaussian_sketch": ([_I, _I, ctypes.c_uint, _DP, _C, _S], ctypes.c_int),
@@ -529,6 +531,26 @@ def profile_end():
     by = ctypes.c_double(0.0)
     _call("fpls_profile", 0, ctypes.byref(ms), ctypes.byref(cnt), ctypes.byref(by))
     return dict(ms=ms.value, launches=cnt.value, bytes=by.value)
+
+
+def profile_classes():
+    """Per-kernel-class timings of the last closed profiling window."""
+    out = []
+    idx = 0
+    lib = load()
+    while True:
+        name = ctypes.create_string_buffer(64)
+        ms, by, fl = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
+        cnt = ctypes.c_longlong(0)
+        err = ctypes.create_string_buffer(256)
+        rc = lib.fpls_profile_class(idx, name, 64, ctypes.byref(ms), ctypes.byref(cnt), ctypes.byref(by),
+                                    ctypes.byref(fl), err, 256)
+        if rc != 0:
+            break
+        out.append(dict(name=name.value.decode(), ms=ms.value, launches=cnt.value, bytes=by.value,
+                        flops=fl.value))
+        idx += 1
+    return out
 
 
 def gaussian_y_encode(Y, projection):

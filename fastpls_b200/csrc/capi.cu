@@ -910,25 +910,53 @@ int fpls_profile(int enable, double* gemm_ms, long long* gemm_launches, double* 
   return guarded(err, errlen, [&] {
     Context& ctx = Context::get();
     if (enable) {
-      for (cudaEvent_t e : ctx.prof_events) cudaEventDestroy(e);
-      ctx.prof_events.clear();
-      ctx.prof_bytes = 0.0;
+      for (auto& c : ctx.prof_classes)
+        for (cudaEvent_t e : c.events) cudaEventDestroy(e);
+      ctx.prof_classes.clear();
       ctx.profile = true;
       return;
     }
     ctx.profile = false;
     ctx.sync();
-    double total = 0.0;
-    for (size_t i = 0; i + 1 < ctx.prof_events.size(); i += 2) {
-      float ms = 0.f;
-      FPLS_CUDA(cudaEventElapsedTime(&ms, ctx.prof_events[i], ctx.prof_events[i + 1]));
-      total += ms;
+    double total = 0.0, bytes = 0.0;
+    long long launches = 0;
+    for (auto& c : ctx.prof_classes) {
+      if (c.name.rfind("split_gemm", 0) != 0 && c.name.rfind("gram_bf16x3", 0) != 0) continue;
+      for (size_t i = 0; i + 1 < c.events.size(); i += 2) {
+        float ms = 0.f;
+        FPLS_CUDA(cudaEventElapsedTime(&ms, c.events[i], c.events[i + 1]));
+        total += ms;
+      }
+      launches += static_cast<long long>(c.events.size() / 2);
+      bytes += c.bytes;
     }
     if (gemm_ms) *gemm_ms = total;
-    if (gemm_launches) *gemm_launches = static_cast<long long>(ctx.prof_events.size() / 2);
-    if (gemm_bytes) *gemm_bytes = ctx.prof_bytes;
-    for (cudaEvent_t e : ctx.prof_events) cudaEventDestroy(e);
-    ctx.prof_events.clear();
+    if (gemm_launches) *gemm_launches = launches;
+    if (gemm_bytes) *gemm_bytes = bytes;
+  });
+}
+
+int fpls_profile_class(int index, char* name, size_t namelen, double* ms, long long* launches,
+                       double* bytes, double* flops, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    Context& ctx = Context::get();
+    FPLS_REQUIRE(index >= 0 && index < static_cast<int>(ctx.prof_classes.size()),
+                 "profile_class: no kernel class with this index");
+    const auto& c = ctx.prof_classes[index];
+    double total = 0.0;
+    for (size_t i = 0; i + 1 < c.events.size(); i += 2) {
+      float t = 0.f;
+      FPLS_CUDA(cudaEventElapsedTime(&t, c.events[i], c.events[i + 1]));
+      total += t;
+    }
+    if (name && namelen) {
+      std::strncpy(name, c.name.c_str(), namelen - 1);
+      name[namelen - 1] = '\0';
+    }
+    if (ms) *ms = total;
+    if (launches) *launches = static_cast<long long>(c.events.size() / 2);
+    if (bytes) *bytes = c.bytes;
+    if (flops) *flops = c.flops;
   });
 }
 

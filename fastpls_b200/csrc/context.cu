@@ -195,3 +195,35 @@ void PhaseTimer::report() {
 }
 
 }  // namespace fpls
+
+namespace fpls {
+
+int Context::prof_begin(const char* cls, cudaStream_t st) {
+  if (!profile) return -1;
+  int slot = -1;
+  for (size_t i = 0; i < prof_classes.size(); ++i)
+    if (prof_classes[i].name == cls) slot = static_cast<int>(i);
+  if (slot < 0) {
+    prof_classes.push_back(ProfClass{});
+    prof_classes.back().name = cls;
+    slot = static_cast<int>(prof_classes.size()) - 1;
+  }
+  cudaEvent_t ev;
+  FPLS_CUDA(cudaEventCreate(&ev));
+  FPLS_CUDA(cudaEventRecord(ev, st));
+  prof_classes[slot].events.push_back(ev);
+  return slot;
+}
+
+void Context::prof_end(int slot, cudaStream_t st, double bytes, double flops) {
+  if (slot < 0 || !profile) return;
+  cudaEvent_t ev;
+  FPLS_CUDA(cudaEventCreate(&ev));
+  FPLS_CUDA(cudaEventRecord(ev, st));
+  ProfClass& c = prof_classes[slot];
+  c.events.push_back(ev);
+  c.bytes += bytes;
+  c.flops += flops;
+}
+
+}  // namespace fpls

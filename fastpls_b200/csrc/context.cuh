@@ -4,6 +4,7 @@
 // thread and released by fpls_reset_workspace().
 #pragma once
 
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -47,10 +48,20 @@ struct Context {
   cudaEvent_t call_start = nullptr, call_stop = nullptr;
   bool call_started = false;
   double last_call_ms = 0.0;
-  // Optional profiling window of the tensor-core GEMM (events around each launch).
+  // Optional profiling window: CUDA events around the launches of the main
+  // kernels, grouped by kernel class, with each launch's algorithmic bytes and
+  // flops (the figures a roofline divides by the measured time).
   bool profile = false;
-  std::vector<cudaEvent_t> prof_events;   // start/stop pairs
-  double prof_bytes = 0.0;                // algorithmic bytes of the profiled launches
+  struct ProfClass {
+    std::string name;
+    std::vector<cudaEvent_t> events;      // start/stop pairs
+    double bytes = 0.0, flops = 0.0;
+  };
+  std::vector<ProfClass> prof_classes;
+  // Records the start event of one launch of `cls` on `st` (no-op unless
+  // profiling); prof_end() records the stop event and adds bytes / flops.
+  int prof_begin(const char* cls, cudaStream_t st);
+  void prof_end(int slot, cudaStream_t st, double bytes, double flops);
   std::vector<ResidentX> resident;
 
   static Context& get();       // initialises the device on first use

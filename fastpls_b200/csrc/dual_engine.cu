@@ -418,12 +418,23 @@ void dual_simpls_run(const DualBatch& b) {
   FPLS_CHECK_LAUNCH();
   b.Kop->times(e.CS, static_cast<int>(F * m), e.KCS);   // K C_S for every fit
   PhaseTimer pt("dual SIMPLS engine");
+  const double nd = static_cast<double>(n), md = static_cast<double>(m), Fd = static_cast<double>(F);
+  const double it = static_cast<double>(e.iters);
   for (int a = 0; a <= b.K; ++a) {
+    // algorithmic bytes of one step launch (all fits): the Gram-Schmidt and
+    // deflation of component a - 1 and the refresh / scores of component a
+    double words = 0.0;
+    if (a > 0) words += (4.0 + 3.0 * (a - 1) + 5.0 * md) * nd;
+    if (a < b.K) words += (5.0 + md + 2.0 * it * md + std::max(it - 1.0, 0.0) * md) * nd;
+    const int slot = ctx.prof_begin("dual_step", st);
     k_dual_step<<<b.F * kCl, kT, 0, st>>>(e, a); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    ctx.prof_end(slot, st, Fd * (8.0 * words + (a < b.K ? 5.0 * nd : 0.0)), 0.0);
     pt.mark("per-fit steps");
     if (a == b.K) break;
+    const int ks = ctx.prof_begin("k_products_f64", st);
     b.Kop->times(e.cp, b.F, e.Gp);
+    ctx.prof_end(ks, st, 8.0 * (nd * nd + 2.0 * nd * Fd), 2.0 * nd * nd * Fd);
     pt.mark("K products");
   }
   pt.report();

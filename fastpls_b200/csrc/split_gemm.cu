@@ -437,6 +437,16 @@ GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false) {
   return g;
 }
 
+// Number of output tiles that received at least one segment.
+int planned_tiles(const GemmPlan& g) {
+  int c = 0;
+  for (int t = 0; t < g.tiles; ++t) c += g.tile_begin[t + 1] > g.tile_begin[t];
+  return c;
+}
+
+// True when the plan skips tiles (a symmetric, upper-triangle plan).
+bool upper_hint(const GemmPlan& g) { return planned_tiles(g) < g.tiles; }
+
 // Device scratch of one GEMM: segment tables and the FP32 stream-K partials.
 struct GemmScratch {
   int4* segs = nullptr;
@@ -488,22 +498,20 @@ void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K,
   const CUtensorMap mAlo = make_map(A.lo, M, K, A.ld, BM);
   const CUtensorMap mBhi = make_map(B.hi, N, K, B.ld, BN);
   const CUtensorMap mBlo = make_map(B.lo, N, K, B.ld, BN);
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  if (prof) {
-    FPLS_CUDA(cudaEventCreate(&ev0));
-    FPLS_CUDA(cudaEventCreate(&ev1));
-    FPLS_CUDA(cudaEventRecord(ev0, st));
-  }
+  const bool upper_plan = g.tiles > 0 && static_cast<int>(g.tile_begin.size()) == g.tiles + 1 &&
+                          g.tile_begin[g.tiles] > 0 && upper_hint(g);
+  const int slot = prof ? prof->prof_begin(upper_plan ? "gram_bf16x3" : "split_gemm_bf16x3", st) : -1;
   split_gemm_kernel<<<g.ctas, NUM_THREADS, SMEM_BYTES, st>>>(mAhi, mAlo, mBhi, mBlo, s.segs, s.cta_begin,
                                                              g.ntn, s.part, err); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   if (prof) {
-    FPLS_CUDA(cudaEventRecord(ev1, st));
-    prof->prof_events.push_back(ev0);
-    prof->prof_events.push_back(ev1);
-    // Algorithmic bytes: both BF16 halves of A and B once, the FP64 result once.
-    prof->prof_bytes += 4.0 * (static_cast<double>(M) * K + static_cast<double>(N) * K) +
-                        8.0 * static_cast<double>(M) * N;
+    // Algorithmic bytes: both BF16 halves of A and B once, the FP64 result once;
+    // flops: three products over the planned tiles.
+    const double tiles_frac = static_cast<double>(planned_tiles(g)) / g.tiles;
+    prof->prof_end(slot, st,
+                   4.0 * (static_cast<double>(M) * K + static_cast<double>(N) * K) +
+                       8.0 * static_cast<double>(M) * N * tiles_frac,
+                   3.0 * 2.0 * static_cast<double>(M) * N * K * tiles_frac);
   }
   split_reduce_kernel<<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, g.ntn, M, N, alpha, beta, C, ldc); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();

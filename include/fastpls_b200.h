@@ -386,6 +386,14 @@ double fpls_last_call_ms(void);
 int fpls_profile(int enable, double* gemm_ms, long long* gemm_launches, double* gemm_bytes,
                  char* err, size_t errlen);
 
+/* Per-class view of the same profiling window: the index-th kernel class
+ * recorded ("dual_step", "k_products_f64", "gram_bf16x3", "split_gemm_bf16x3"),
+ * its summed launch time in ms (CUDA events around each launch), launch count
+ * and the algorithmic bytes and flops of those launches.  Call after the
+ * window is closed; an index past the last class returns FPLS_ERR_ARGUMENT. */
+int fpls_profile_class(int index, char* name, size_t namelen, double* ms, long long* launches,
+                       double* bytes, double* flops, char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -106,14 +106,22 @@ __device__ void cluster_sum(ClusterRed& R, double (&v)[4], int count) {
 __device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M, int n, int ncols, const Rows& rw,
                              const double (&x)[kLR]) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int j = 0; j < ncols; ++j) {
-    const double* col = M + (size_t)j * n;
-    double acc = 0.0;
+  // four columns per pass: their loads are independent and issued together
+  for (int j0 = 0; j0 < ncols; j0 += 4) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int k = 0; k < kLR; ++k)
-      if (rw.ok(k)) acc += col[rw.row(k)] * x[k];
-    acc = warp_sum(acc);
-    if (lane == 0) R.warp[warp][j] = acc;
+    for (int jj = 0; jj < 4; ++jj) {
+      if (j0 + jj >= ncols) break;
+      const double* col = M + (size_t)(j0 + jj) * n;
+#pragma unroll
+      for (int k = 0; k < kLR; ++k)
+        if (rw.ok(k)) acc[jj] += col[rw.row(k)] * x[k];
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const double w = warp_sum(acc[jj]);
+      if (lane == 0 && j0 + jj < ncols) R.warp[warp][j0 + jj] = w;
+    }
   }
   __syncthreads();
   for (int j = threadIdx.x; j < ncols; j += kT) {
@@ -172,6 +180,7 @@ __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, i
     // y = S z: c_y = C_S z, K c_y = (K C_S) z, z in R.res
 #pragma unroll
     for (int k = 0; k < kLR; ++k) cy[k] = ky[k] = 0.0;
+#pragma unroll 4
     for (int j = 0; j < m; ++j) {
       const double zj = R.res[j];
       const double* cs = CS + (size_t)j * n;
@@ -281,6 +290,7 @@ __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, i
   }
   if (a > 0) {
     cluster_dots(R, CV, n, a, rw, kv);   // V^T p = C_V^T K c_p
+#pragma unroll 4
     for (int l = 0; l < a; ++l) {
       const double wl = R.res[l];
       const double* vc = CV + (size_t)l * n;

@@ -79,6 +79,8 @@ SIGNATURES = {
                                         _IP, _DP, _C, _S], ctypes.c_int),
     "fpls_profile_class": ([_I, ctypes.c_char_p, _S, _DP, ctypes.POINTER(ctypes.c_longlong), _DP, _DP,
                             _C, _S], ctypes.c_int),
+    "fpls_set_precision": ([_I, _C, _S], ctypes.c_int),
+    "fpls_get_precision": ([], ctypes.c_int),
     "fpls_host_register": ([ctypes.c_void_p, _S, _C, _S], ctypes.c_int),
     "fpls_host_unregister": ([ctypes.c_void_p, _C, _S], ctypes.c_int),
     "fpls_gaussian_sketch": ([_I, _I, ctypes.c_uint, _DP, _C, _S], ctypes.c_int),
@@ -411,7 +413,7 @@ def lda_project_predict(X, R, offset, lda, return_scores=False):
     return dict(pred=lab, scores=sc) if return_scores else dict(pred=lab)
 
 
-PREC = {"fp64": 0, "bf16x3": 1}
+PREC = {"fp64": 0, "bf16x3": 1, "bf16x6": 2}
 
 
 def bf16x3_gemm(A, B):
@@ -719,3 +721,12 @@ def host_register(a):
 
 def host_unregister(a):
     _call("fpls_host_unregister", ctypes.c_void_p(a.ctypes.data))
+
+
+def set_precision(precision):
+    """Session precision of single fits and predictions: "fp64", "bf16x3" or "bf16x6"."""
+    _call("fpls_set_precision", PREC[precision] if isinstance(precision, str) else int(precision))
+
+
+def get_precision():
+    return {v: k for k, v in PREC.items()}[int(load().fpls_get_precision())]

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "gaussian.cuh"
@@ -318,8 +319,12 @@ int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, 
     double* dvX = ctx.arena.alloc_n<double>(p);
     double* dmY = ctx.arena.alloc_n<double>(m);
     center_scale_xy(dX, n, p, dYc, m, scaling, dmX, dvX, dmY);
-    // Single fit on all rows: S = Xc^T Yc as the reference (fastPLS.cpp:2499).
-    XOperatorF64 xop(dX, n, p);
+    // Single fit on all rows: S = Xc^T Yc as the reference (fastPLS.cpp:2499);
+    // the two predictor passes per component run FP64 or, in the mixed
+    // session precision, as BF16x3 tensor-core products.
+    std::unique_ptr<XOperator> xop;
+    if (ctx.precision >= 1) xop = make_split_operator(dX, n, p, true, ctx.precision == 2 ? 3 : 2);
+    else xop.reset(new XOperatorF64(dX, n, p));
     SimplsBatch b;
     b.n = n; b.p = p; b.m = m; b.F = 1; b.K = K;
     int iters = 2;
@@ -329,10 +334,10 @@ int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, 
       if (endp != e) iters = static_cast<int>(std::min(6L, std::max(1L, v)));
     }
     b.power_iters = iters;
-    b.X = &xop;
+    b.X = xop.get();
     b.Yg = dYc;
     b.S = ctx.arena.alloc_n<double>((size_t)p * m);
-    gemm(true, false, p, m, n, 1.0, dX, n, dYc, n, 0.0, b.S, p);
+    xgemm(true, p, m, n, dX, n, dYc, n, b.S, p);
     double* om = ctx.arena.alloc_n<double>(p);
     device_gaussian(om, p, static_cast<unsigned int>(seed));
     b.omega = om;
@@ -562,7 +567,7 @@ int fpls_lda_project_train_prefix(const double* X, int n, int p, const double* R
     const double* dX = upload(X, (size_t)n * p);
     const double* dR = upload(R, (size_t)p * k);
     double* dT = ctx.arena.alloc_n<double>((size_t)n * k);
-    gemm(false, false, n, k, p, 1.0, dX, n, dR, p, 0.0, dT, n);
+    xgemm(false, n, k, p, dX, n, dR, p, dT, n);
     if (offset) {
       double* doff = upload(offset, k);
       scale_vec(doff, k, -1.0);
@@ -631,7 +636,7 @@ int fpls_lda_project_predict(const double* X, int w, int p, const double* R, int
     if (direct_ops < 0.5 * latent_ops) {
       double* dW = ctx.arena.alloc_n<double>((size_t)p * n_classes);
       gemm(false, true, p, n_classes, k, 1.0, dR, p, dL, n_classes, 0.0, dW, p);
-      gemm(false, false, w, n_classes, p, 1.0, dX, w, dW, p, 0.0, dS, w);
+      xgemm(false, w, n_classes, p, dX, w, dW, p, dS, w);
     } else {
       double* dT = ctx.arena.alloc_n<double>((size_t)w * k);
       gemm(false, false, w, k, p, 1.0, dX, w, dR, p, 0.0, dT, w);
@@ -862,6 +867,17 @@ int fpls_x_free(int handle, char* err, size_t errlen) {
     ctx.resident[handle] = ResidentX();
   });
 }
+
+int fpls_set_precision(int precision, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(precision == FPLS_PREC_FP64 || precision == FPLS_PREC_BF16X3 ||
+                     precision == FPLS_PREC_BF16X6,
+                 "precision must be FPLS_PREC_FP64 (0), FPLS_PREC_BF16X3 (1) or FPLS_PREC_BF16X6 (2)");
+    Context::get().precision = precision;
+  });
+}
+
+int fpls_get_precision(void) { return Context::get().precision; }
 
 int fpls_host_register(void* ptr, size_t bytes, char* err, size_t errlen) {
   return guarded(err, errlen, [&] {

@@ -44,6 +44,7 @@ struct Context {
   Arena arena;
   int* d_status = nullptr;     // device-side failure flag (0 = ok)
   int sm_count = kSMCount;
+  int precision = 0;           // session precision of single fits: 0 FP64, 1 BF16x3 (predictor GEMMs)
   // Timing of the last ABI call (events on `stream`, bracketing the whole call).
   cudaEvent_t call_start = nullptr, call_stop = nullptr;
   bool call_started = false;

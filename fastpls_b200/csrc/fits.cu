@@ -1,3 +1,4 @@
+#include "xop_split.cuh"
 #include "gaussian.cuh"
 #include "blas_f64.cuh"
 #include "context.cuh"
@@ -154,7 +155,7 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
   double* S = nullptr;
   if (!opt.xprod) {
     S = ctx.arena.alloc_n<double>((size_t)p * m);
-    gemm(true, false, p, m, n, 1.0, X, n, Y, n, 0.0, S, p);
+    xgemm(true, p, m, n, X, n, Y, n, S, p);
   }
   int thr = 32;
   if (const char* e = std::getenv("FASTPLS_PLSSVD_SMALL_EXACT_MAX_RANK")) {
@@ -175,7 +176,7 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
   int keff = std::min(K0, sr.rank);
   FPLS_REQUIRE(keff >= 1, "plssvd effective rank is < 1 after SVD");
   dzero(out.T, (size_t)n * K0 * sizeof(double));
-  gemm(false, false, n, keff, p, 1.0, X, n, out.R, p, 0.0, out.T, n);
+  xgemm(false, n, keff, p, X, n, out.R, p, out.T, n);
   double* G = ctx.arena.alloc_n<double>((size_t)keff * keff);
   gemm(true, false, keff, keff, n, 1.0, out.T, n, out.T, n, 0.0, G, keff);
   dzero(out.C_latent, (size_t)K0 * K0 * L * sizeof(double));
@@ -225,7 +226,7 @@ int simpls_classic_fit(const double* X, int n, int p, const double* Y, int m, co
   int max_ncomp = 0;
   for (int i = 0; i < L; ++i) max_ncomp = std::max(max_ncomp, ncomp[i]);
   double* S = ctx.arena.alloc_n<double>((size_t)p * m);
-  gemm(true, false, p, m, n, 1.0, X, n, Y, n, 0.0, S, p);
+  xgemm(true, p, m, n, X, n, Y, n, S, p);
   double* V = ctx.arena.alloc_n<double>((size_t)p * max_ncomp);
   double* t = ctx.arena.alloc_n<double>(n);
   double* pp = ctx.arena.alloc_n<double>(p);

@@ -1,3 +1,4 @@
+#include "xop_split.cuh"
 #include "blas_f64.cuh"
 #include "context.cuh"
 #include "heads.cuh"
@@ -150,7 +151,7 @@ __global__ void lda_constants_kernel(const double* M, const double* Lin, int C, 
 void lowrank_predict(const double* Xs, int w, int p, const double* R, int kmax, const double* W,
                      int m, const int* ncomp_host, int L, const double* mY, double* T,
                      double* Ypred) {
-  gemm(false, false, w, kmax, p, 1.0, Xs, w, R, p, 0.0, T, w);
+  xgemm(false, w, kmax, p, Xs, w, R, p, T, w);
   for (int a = 0; a < L; ++a) {
     const int mc = ncomp_host[a];
     double* Ya = Ypred + (size_t)a * w * m;

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <vector>
 
+#include "xop_split.cuh"
 #include "blas_f64.cuh"
 #include "capi_util.cuh"
 #include "cknn.cuh"
@@ -286,7 +287,7 @@ LabelAwareFit label_aware_fit(const void* dX, bool f32, int n, int p, const int*
 
   // T = X~ R (n x K), G = T^T T
   f.T = ctx.arena.alloc_n<double>((size_t)n * K);
-  gemm(true, false, n, K, p, 1.0, f.Xt, p, f.R, p, 0.0, f.T, n);
+  xgemm(true, n, K, p, f.Xt, p, f.R, p, f.T, n);
   f.G = ctx.arena.alloc_n<double>((size_t)K * K);
   gemm(true, false, K, K, n, 1.0, f.T, n, f.T, n, 0.0, f.G, K);
   pt.mark("scores + gram");

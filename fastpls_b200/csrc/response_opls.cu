@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 
+#include "xop_split.cuh"
 #include "gaussian.cuh"
 #include "blas_f64.cuh"
 #include "capi_util.cuh"
@@ -169,13 +170,13 @@ int fpls_gaussian_y_encode(const double* Y, int n, int q, const double* projecti
     col_mean(dY, n, q, n, dmu);
     center_scale(dY, n, q, n, dmu, nullptr);
     double* dZ = ctx.arena.alloc_n<double>((size_t)n * d);
-    gemm(false, false, n, d, q, 1.0, dY, n, dG, q, 0.0, dZ, n);
+    xgemm(false, n, d, q, dY, n, dG, q, dZ, n);
     // decoder = (Z^T Z + 1e-8 mean(diag) I)^{-1} Z^T Yc
     double* ztz = ctx.arena.alloc_n<double>((size_t)d * d);
     double* rhs = ctx.arena.alloc_n<double>((size_t)d * q);
     double* dec = ctx.arena.alloc_n<double>((size_t)d * q);
     gemm(true, false, d, d, n, 1.0, dZ, n, dZ, n, 0.0, ztz, d);
-    gemm(true, false, d, q, n, 1.0, dZ, n, dY, n, 0.0, rhs, d);
+    xgemm(true, d, q, n, dZ, n, dY, n, rhs, d);
     spd_solve(d, ztz, d, q, rhs, d, dec, d, ctx.d_status + 6, 1e-8);
     d2h(Z, dZ, (size_t)n * d * sizeof(double));
     d2h(y_center, dmu, q * sizeof(double));
@@ -267,7 +268,7 @@ int fpls_opls_filter(const double* X, int n, int p, const double* Y, int q, int 
     double* dP = ctx.arena.alloc_n<double>((size_t)p * std::max(north, 1));
     int k = 0;
     for (int a = 0; a < north; ++a) {
-      gemm(true, false, p, q, n, 1.0, dX, n, dY, n, 0.0, S, p);
+      xgemm(true, p, q, n, dX, n, dY, n, S, p);
       leading_left_vector(S, p, q, u, 1234567u + a);
       dot2_kernel<<<1, 512, 0, ctx.stream>>>(u, u, p, sc); ::fpls::note_launch();
       FPLS_CHECK_LAUNCH();

@@ -38,12 +38,17 @@ namespace {
 constexpr int BM = 128;
 constexpr int BN = 64;
 constexpr int BK = 64;
-constexpr int STAGES = 4;
 constexpr int A_TILE = BM * BK * 2;                 // 16 KB
 constexpr int B_TILE = BN * BK * 2;                 // 8 KB
-constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;  // 48 KB
 constexpr int BAR_BYTES = 256;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
+// NP BF16 planes per operand: 2 (hi, lo: 48 KB stages, 4 deep) or 3 (hi, mid,
+// lo: 72 KB stages, 3 deep).
+template <int NP> struct Planes {
+  static constexpr int STAGES = NP == 2 ? 4 : 3;
+  static constexpr int STAGE_BYTES = NP * (A_TILE + B_TILE);
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
+};
+static_assert(Planes<3>::SMEM_BYTES <= 227 * 1024, "three-plane stages exceed shared memory");
 constexpr int NUM_THREADS = 192;
 constexpr int TMEM_COLS = 2 * BN;
 constexpr long long kWaitBudget = 1ll << 33;        // ~4 s at 2 GHz
@@ -135,11 +140,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+template <int NP>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
-split_gemm_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
-                  const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo,
+split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
+                  const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
+                  const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2,
                   const int4* __restrict__ segs, const int* __restrict__ cta_seg_begin,
                   int n_tiles_n, float* __restrict__ part, int* err) {
+  constexpr int STAGES = Planes<NP>::STAGES;
+  constexpr int STAGE_BYTES = Planes<NP>::STAGE_BYTES;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~static_cast<uintptr_t>(1023));
@@ -199,10 +208,12 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constan
         const uint32_t fb = smem_u32(&full[s]);
         mbar_expect_tx(fb, STAGE_BYTES);
         uint8_t* st = smem + s * STAGE_BYTES;
-        tma_load_2d(&mAhi, smem_u32(st), fb, kb * BK, mt * BM);
-        tma_load_2d(&mAlo, smem_u32(st + A_TILE), fb, kb * BK, mt * BM);
-        tma_load_2d(&mBhi, smem_u32(st + 2 * A_TILE), fb, kb * BK, nt * BN);
-        tma_load_2d(&mBlo, smem_u32(st + 2 * A_TILE + B_TILE), fb, kb * BK, nt * BN);
+        tma_load_2d(&mA0, smem_u32(st), fb, kb * BK, mt * BM);
+        tma_load_2d(&mA1, smem_u32(st + A_TILE), fb, kb * BK, mt * BM);
+        if (NP == 3) tma_load_2d(&mA2, smem_u32(st + 2 * A_TILE), fb, kb * BK, mt * BM);
+        tma_load_2d(&mB0, smem_u32(st + NP * A_TILE), fb, kb * BK, nt * BN);
+        tma_load_2d(&mB1, smem_u32(st + NP * A_TILE + B_TILE), fb, kb * BK, nt * BN);
+        if (NP == 3) tma_load_2d(&mB2, smem_u32(st + NP * A_TILE + 2 * B_TILE), fb, kb * BK, nt * BN);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -221,18 +232,24 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constan
         const uint32_t ph = (it / STAGES) & 1;
         if (!mbar_wait(smem_u32(&full[s]), ph, err)) { ok = false; break; }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a_hi = smem_u32(smem + s * STAGE_BYTES);
-        const uint32_t a_lo = a_hi + A_TILE;
-        const uint32_t b_hi = a_hi + 2 * A_TILE;
-        const uint32_t b_lo = b_hi + B_TILE;
+        const uint32_t a0 = smem_u32(smem + s * STAGE_BYTES);
+        const uint32_t b0 = a0 + NP * A_TILE;
 #pragma unroll
         for (int k = 0; k < BK / 16; ++k) {
           const uint32_t off = k * 32;  // 16 BF16 = 32 bytes along K inside the swizzle atom
-          const uint64_t dah = sw128_desc(a_hi + off), dal = sw128_desc(a_lo + off);
-          const uint64_t dbh = sw128_desc(b_hi + off), dbl = sw128_desc(b_lo + off);
-          umma_bf16(acc, dah, dbh, (kb > seg.y || k > 0) ? 1u : 0u);
-          umma_bf16(acc, dah, dbl, 1u);
-          umma_bf16(acc, dal, dbh, 1u);
+          const uint64_t da0 = sw128_desc(a0 + off), da1 = sw128_desc(a0 + A_TILE + off);
+          const uint64_t db0 = sw128_desc(b0 + off), db1 = sw128_desc(b0 + B_TILE + off);
+          // products down to 2^-16 (two planes) or 2^-24 (three planes) of hi*hi
+          umma_bf16(acc, da0, db0, (kb > seg.y || k > 0) ? 1u : 0u);
+          umma_bf16(acc, da0, db1, 1u);
+          umma_bf16(acc, da1, db0, 1u);
+          if (NP == 3) {
+            const uint64_t da2 = sw128_desc(a0 + 2 * A_TILE + off);
+            const uint64_t db2 = sw128_desc(b0 + 2 * B_TILE + off);
+            umma_bf16(acc, da0, db2, 1u);
+            umma_bf16(acc, da2, db0, 1u);
+            umma_bf16(acc, da1, db1, 1u);
+          }
         }
         umma_commit(smem_u32(&empty[s]));
       }
@@ -294,18 +311,33 @@ __global__ void split_reduce_kernel(const float* __restrict__ part, const int* _
 
 // hi/lo split of a column-major FP64 matrix (rows x cols, ld) written as
 // cols x ldo row-major BF16 pairs (row j = column j), zero padded to ldo.
+// Two planes: hi = bf16(x), lo = bf16(x - hi).  Three planes (mid non-null):
+// hi = bf16(x), mid = bf16(x - hi), lo = bf16(x - hi - mid).
+__device__ __forceinline__ void split_value(double x, __nv_bfloat16& h, __nv_bfloat16* m, __nv_bfloat16& l) {
+  h = __double2bfloat16(x);
+  const double r = x - static_cast<double>(__bfloat162float(h));
+  if (m) {
+    *m = __double2bfloat16(r);
+    l = __double2bfloat16(r - static_cast<double>(__bfloat162float(*m)));
+  } else {
+    l = __double2bfloat16(r);
+  }
+}
+
 __global__ void split_cols_kernel(const double* __restrict__ X, int rows, int cols, int ld,
                                   __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
-                                  int ldo) {
+                                  int ldo, __nv_bfloat16* __restrict__ mid) {
   const size_t total = static_cast<size_t>(cols) * ldo;
   for (size_t t = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<size_t>(gridDim.x) * blockDim.x) {
     const int i = static_cast<int>(t % ldo);
     const int j = static_cast<int>(t / ldo);
     double x = (i < rows) ? X[i + static_cast<size_t>(j) * ld] : 0.0;
-    const __nv_bfloat16 h = __double2bfloat16(x);
+    __nv_bfloat16 h, l, md;
+    split_value(x, h, mid ? &md : nullptr, l);
     hi[t] = h;
-    lo[t] = __double2bfloat16(x - static_cast<double>(__bfloat162float(h)));
+    lo[t] = l;
+    if (mid) mid[t] = md;
   }
 }
 
@@ -313,7 +345,7 @@ __global__ void split_cols_kernel(const double* __restrict__ X, int rows, int co
 // row-major pairs (row i holds X[i, :]), zero padded.  32 x 32 tiles via smem.
 __global__ void split_rows_kernel(const double* __restrict__ X, int rows, int cols, int ld,
                                   __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
-                                  int ldo) {
+                                  int ldo, __nv_bfloat16* __restrict__ mid) {
   __shared__ double tile[32][33];
   const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
@@ -326,9 +358,11 @@ __global__ void split_rows_kernel(const double* __restrict__ X, int rows, int co
     const int i = i0 + r, j = j0 + tx;
     if (i < rows && j < ldo) {
       const double x = tile[tx][r];
-      const __nv_bfloat16 h = __double2bfloat16(x);
+      __nv_bfloat16 h, l, md;
+      split_value(x, h, mid ? &md : nullptr, l);
       hi[static_cast<size_t>(i) * ldo + j] = h;
-      lo[static_cast<size_t>(i) * ldo + j] = __double2bfloat16(x - static_cast<double>(__bfloat162float(h)));
+      lo[static_cast<size_t>(i) * ldo + j] = l;
+      if (mid) mid[static_cast<size_t>(i) * ldo + j] = md;
     }
   }
 }
@@ -362,26 +396,33 @@ CUtensorMap make_map(const __nv_bfloat16* base, int rows, int k, int ld, int box
 
 int round_up(int x, int a) { return (x + a - 1) / a * a; }
 
+// BF16 planes of one operand (hi, lo and, with three planes, mid), each
+// rows x ld K-contiguous, stored one after the other.
 struct SplitPair {
   __nv_bfloat16* hi = nullptr;
   __nv_bfloat16* lo = nullptr;
-  int rows = 0, k = 0, ld = 0;
+  __nv_bfloat16* mid = nullptr;
+  int rows = 0, k = 0, ld = 0, np = 2;
 };
 
-SplitPair pair_at(__nv_bfloat16* base, int rows, int k) {
+SplitPair pair_at(__nv_bfloat16* base, int rows, int k, int np = 2) {
   SplitPair s;
   s.rows = rows;
   s.k = k;
+  s.np = np;
   s.ld = round_up(std::max(k, 1), BK);
   s.hi = base;
   s.lo = base + static_cast<size_t>(rows) * s.ld;
+  if (np == 3) s.mid = base + 2 * static_cast<size_t>(rows) * s.ld;
   return s;
 }
 
-size_t pair_elems(int rows, int k) { return 2 * static_cast<size_t>(rows) * round_up(std::max(k, 1), BK); }
+size_t pair_elems(int rows, int k, int np = 2) {
+  return np * static_cast<size_t>(rows) * round_up(std::max(k, 1), BK);
+}
 
-SplitPair alloc_pair(int rows, int k) {
-  return pair_at(Context::get().arena.alloc_n<__nv_bfloat16>(pair_elems(rows, k)), rows, k);
+SplitPair alloc_pair(int rows, int k, int np = 2) {
+  return pair_at(Context::get().arena.alloc_n<__nv_bfloat16>(pair_elems(rows, k, np)), rows, k, np);
 }
 
 // Stream-K work plan: CTA c covers iterations [c*total/ctas, (c+1)*total/ctas)
@@ -396,8 +437,11 @@ struct GemmPlan {
 // reach the upper triangle (tile row start < tile column end) are planned, for
 // symmetric products whose lower triangle is mirrored afterwards.
 constexpr int kSymSegBlocks = 16;
+// Products that take the split path in the mixed precision mode.
+constexpr int kMixedMinK = 256;
+constexpr double kMixedMinWork = 1e7;
 
-GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false) {
+GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false, bool short_segments = false) {
   GemmPlan g;
   const int mt = (M + BM - 1) / BM;
   g.ntn = (N + BN - 1) / BN;
@@ -408,9 +452,10 @@ GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false) {
     if (!upper || (t / g.ntn) * BM < ((t % g.ntn) + 1) * BN) inc.push_back(t);
   const int kbt = (K + BK - 1) / BK;
   // A symmetric (Gram) product sums the whole contraction of each tile in one
-  // CTA; cutting it into segments of at most kSymSegBlocks K-blocks keeps each
-  // FP32 accumulation short and adds the segments in FP64.
-  const int kseg = upper ? kSymSegBlocks : kbt;
+  // CTA; cutting it (and every three-plane product) into segments of at most
+  // kSymSegBlocks K-blocks keeps each FP32 accumulation short and adds the
+  // segments in FP64.
+  const int kseg = (upper || short_segments) ? kSymSegBlocks : kbt;
   const long long total = static_cast<long long>(inc.size()) * kbt;
   g.ctas = static_cast<int>(std::max<long long>(1, std::min<long long>(sm_count, total)));
   g.cta_begin.assign(g.ctas + 1, 0);
@@ -474,10 +519,12 @@ GemmScratch carve_gemm_scratch(const GemmPlan& g, char* base) {
   return s;
 }
 
+template <int NP>
 void ensure_smem_attr() {
   static bool attr = false;
   if (!attr) {
-    FPLS_CUDA(cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    FPLS_CUDA(cudaFuncSetAttribute(split_gemm_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Planes<NP>::SMEM_BYTES));
     attr = true;
   }
 }
@@ -493,25 +540,39 @@ void upload_plan_tables(const GemmPlan& g, const GemmScratch& s, cudaStream_t st
 void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,
                     double beta, double* C, int ldc, const GemmPlan& g, const GemmScratch& s,
                     int* err, cudaStream_t st, Context* prof) {
-  ensure_smem_attr();
-  const CUtensorMap mAhi = make_map(A.hi, M, K, A.ld, BM);
-  const CUtensorMap mAlo = make_map(A.lo, M, K, A.ld, BM);
-  const CUtensorMap mBhi = make_map(B.hi, N, K, B.ld, BN);
-  const CUtensorMap mBlo = make_map(B.lo, N, K, B.ld, BN);
+  FPLS_REQUIRE(A.np == B.np && (A.np == 2 || A.np == 3), "split GEMM: operands with different plane counts");
+  const CUtensorMap mA0 = make_map(A.hi, M, K, A.ld, BM);
+  const CUtensorMap mA1 = make_map(A.np == 3 ? A.mid : A.lo, M, K, A.ld, BM);
+  const CUtensorMap mA2 = make_map(A.lo, M, K, A.ld, BM);
+  const CUtensorMap mB0 = make_map(B.hi, N, K, B.ld, BN);
+  const CUtensorMap mB1 = make_map(B.np == 3 ? B.mid : B.lo, N, K, B.ld, BN);
+  const CUtensorMap mB2 = make_map(B.lo, N, K, B.ld, BN);
   const bool upper_plan = g.tiles > 0 && static_cast<int>(g.tile_begin.size()) == g.tiles + 1 &&
                           g.tile_begin[g.tiles] > 0 && upper_hint(g);
-  const int slot = prof ? prof->prof_begin(upper_plan ? "gram_bf16x3" : "split_gemm_bf16x3", st) : -1;
-  split_gemm_kernel<<<g.ctas, NUM_THREADS, SMEM_BYTES, st>>>(mAhi, mAlo, mBhi, mBlo, s.segs, s.cta_begin,
-                                                             g.ntn, s.part, err); ::fpls::note_launch();
+  const int slot = prof ? prof->prof_begin(upper_plan ? (A.np == 3 ? "gram_bf16x6" : "gram_bf16x3")
+                                                      : (A.np == 3 ? "split_gemm_bf16x6" : "split_gemm_bf16x3"),
+                                           st)
+                        : -1;
+  if (A.np == 3) {
+    ensure_smem_attr<3>();
+    split_gemm_kernel<3><<<g.ctas, NUM_THREADS, Planes<3>::SMEM_BYTES, st>>>(mA0, mA1, mA2, mB0, mB1, mB2, s.segs,
+                                                                           s.cta_begin, g.ntn, s.part, err);
+  } else {
+    ensure_smem_attr<2>();
+    split_gemm_kernel<2><<<g.ctas, NUM_THREADS, Planes<2>::SMEM_BYTES, st>>>(mA0, mA1, mA2, mB0, mB1, mB2, s.segs,
+                                                                           s.cta_begin, g.ntn, s.part, err);
+  }
+  ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   if (prof) {
-    // Algorithmic bytes: both BF16 halves of A and B once, the FP64 result once;
-    // flops: three products over the planned tiles.
+    // Algorithmic bytes: every BF16 plane of A and B once, the FP64 result once;
+    // flops: three (two planes) or six (three planes) products over the planned tiles.
     const double tiles_frac = static_cast<double>(planned_tiles(g)) / g.tiles;
+    const double planes = A.np, products = A.np == 3 ? 6.0 : 3.0;
     prof->prof_end(slot, st,
-                   4.0 * (static_cast<double>(M) * K + static_cast<double>(N) * K) +
+                   2.0 * planes * (static_cast<double>(M) * K + static_cast<double>(N) * K) +
                        8.0 * static_cast<double>(M) * N * tiles_frac,
-                   3.0 * 2.0 * static_cast<double>(M) * N * K * tiles_frac);
+                   products * 2.0 * static_cast<double>(M) * N * K * tiles_frac);
   }
   split_reduce_kernel<<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, g.ntn, M, N, alpha, beta, C, ldc); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
@@ -525,18 +586,19 @@ struct CachedPlan {
   char* dev = nullptr;
   GemmScratch s;
 };
-std::map<std::array<int, 5>, CachedPlan>& plan_cache() {
-  static std::map<std::array<int, 5>, CachedPlan> cache;
+std::map<std::array<int, 6>, CachedPlan>& plan_cache() {
+  static std::map<std::array<int, 6>, CachedPlan> cache;
   return cache;
 }
 
-const CachedPlan& cached_plan(int M, int N, int K, int sm_count, cudaStream_t st, bool upper = false) {
+const CachedPlan& cached_plan(int M, int N, int K, int sm_count, cudaStream_t st, bool upper = false,
+                              bool short_segments = false) {
   auto& cache = plan_cache();
-  const std::array<int, 5> key{M, N, K, sm_count, upper ? 1 : 0};
+  const std::array<int, 6> key{M, N, K, sm_count, upper ? 1 : 0, short_segments ? 1 : 0};
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
   CachedPlan c;
-  c.g = plan_gemm(M, N, K, sm_count, upper);
+  c.g = plan_gemm(M, N, K, sm_count, upper, short_segments);
   FPLS_CUDA(cudaMalloc(&c.dev, gemm_scratch_bytes(c.g)));
   c.s = carve_gemm_scratch(c.g, c.dev);
   upload_plan_tables(c.g, c.s, st);
@@ -546,7 +608,7 @@ const CachedPlan& cached_plan(int M, int N, int K, int sm_count, cudaStream_t st
 void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,
                 double beta, double* C, int ldc, bool upper = false) {
   Context& ctx = Context::get();
-  const CachedPlan& c = cached_plan(M, N, K, ctx.sm_count, ctx.stream, upper);
+  const CachedPlan& c = cached_plan(M, N, K, ctx.sm_count, ctx.stream, upper, A.np == 3);
   split_gemm_run(A, B, M, N, K, alpha, beta, C, ldc, c.g, c.s, ctx.d_status + 16, ctx.stream,
                  ctx.profile ? &ctx : nullptr);
 }
@@ -568,13 +630,13 @@ void mirror_upper(double* K, int n) {
 
 void split_cols_on(const double* X, int rows, int cols, int ld, const SplitPair& out, cudaStream_t st,
                    int sm_count) {
-  split_cols_kernel<<<4 * sm_count, 256, 0, st>>>(X, rows, cols, ld, out.hi, out.lo, out.ld); ::fpls::note_launch();
+  split_cols_kernel<<<4 * sm_count, 256, 0, st>>>(X, rows, cols, ld, out.hi, out.lo, out.ld, out.mid); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
 void split_rows_on(const double* X, int rows, int cols, int ld, const SplitPair& out, cudaStream_t st) {
   dim3 grid((out.ld + 31) / 32, (rows + 31) / 32);
-  split_rows_kernel<<<grid, dim3(32, 8), 0, st>>>(X, rows, cols, ld, out.hi, out.lo, out.ld); ::fpls::note_launch();
+  split_rows_kernel<<<grid, dim3(32, 8), 0, st>>>(X, rows, cols, ld, out.hi, out.lo, out.ld, out.mid); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -591,18 +653,19 @@ struct XOperatorSplit : public XOperator {
   SplitPair xr;   // n x p  (A of X * R)
   SplitPair xc;   // p x n  (A of X^T * T)
   bool has_t = true;
-  XOperatorSplit(const double* X, int n_, int p_, bool need_t) : has_t(need_t) {
+  int np = 2;
+  XOperatorSplit(const double* X, int n_, int p_, bool need_t, int np_) : has_t(need_t), np(np_) {
     n = n_;
     p = p_;
-    xr = alloc_pair(n, p);
+    xr = alloc_pair(n, p, np);
     split_rows(X, n, p, n, xr);
     if (has_t) {
-      xc = alloc_pair(p, n);
+      xc = alloc_pair(p, n, np);
       split_cols(X, n, p, n, xc);
     }
   }
   void times(const double* Rhat, int F, double* U) override {
-    SplitPair b = alloc_pair(F, p);
+    SplitPair b = alloc_pair(F, p, np);
     split_cols(Rhat, p, F, p, b);
     split_gemm(xr, b, n, F, p, 1.0, 0.0, U, n);
   }
@@ -613,7 +676,7 @@ struct XOperatorSplit : public XOperator {
   }
   void t_times(const double* T, int F, double* P) override {
     FPLS_REQUIRE(has_t, "split operator built without its transposed copy");
-    SplitPair b = alloc_pair(F, n);
+    SplitPair b = alloc_pair(F, n, np);
     split_cols(T, n, F, n, b);
     split_gemm(xc, b, p, F, n, 1.0, 0.0, P, p);
   }
@@ -621,13 +684,33 @@ struct XOperatorSplit : public XOperator {
 
 }  // namespace
 
+void xgemm(bool transA, int M, int N, int K, const double* A, int lda, const double* B, int ldb, double* C,
+           int ldc) {
+  Context& ctx = Context::get();
+  const bool mixed = ctx.precision >= 1 && K >= kMixedMinK &&
+                     static_cast<double>(M) * N * K >= kMixedMinWork;
+  const int np = ctx.precision == 2 ? 3 : 2;
+  if (!mixed) {
+    gemm(transA, false, M, N, K, 1.0, A, lda, B, ldb, 0.0, C, ldc);
+    return;
+  }
+  // A operand as M x K K-contiguous rows: op(A) = A (M x K col-major) needs
+  // the row split, op(A) = A^T (A is K x M) is already K-contiguous per row.
+  SplitPair a = alloc_pair(M, K, np);
+  if (transA) split_cols(A, K, M, lda, a);
+  else split_rows(A, M, K, lda, a);
+  SplitPair b = alloc_pair(N, K, np);
+  split_cols(B, K, N, ldb, b);
+  split_gemm(a, b, M, N, K, 1.0, 0.0, C, ldc);
+}
+
 void split_gemm_release_cache() {
   for (auto& kv : plan_cache()) cudaFree(kv.second.dev);
   plan_cache().clear();
 }
 
-std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p, bool need_t) {
-  return std::unique_ptr<XOperator>(new XOperatorSplit(X, n, p, need_t));
+std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p, bool need_t, int planes) {
+  return std::unique_ptr<XOperator>(new XOperatorSplit(X, n, p, need_t, planes));
 }
 
 void split_gemm_test(const double* A, const double* B, int M, int N, int K, double* C) {

@@ -14,8 +14,20 @@ namespace fpls {
 void split_gemm_release_cache();
 
 // Builds the split operator from an FP64 device matrix (n x p, ld n); without
-// need_t only the row-major copy (for times() and gram()) is kept.
-std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p, bool need_t = true);
+// need_t only the row-major copy (for times() and gram()) is kept.  planes: 2
+// (BF16x3: hi, lo, three products) or 3 (BF16x6: hi, mid, lo, six products).
+std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p, bool need_t = true,
+                                               int planes = 2);
+
+// C (M x N) = op(A) B with op(A) = A (M x K) or A^T (A is K x M), B K x N,
+// column-major device matrices.  In the mixed precision modes (session setting
+// FPLS_PREC_BF16X3 or FPLS_PREC_BF16X6) products with a contraction of at
+// least 256 and 1e7 multiply-adds run as the split BF16 tensor-core GEMM (two
+// or three planes per operand, FP32 accumulation in segments, FP64
+// reduction); everything else, and every product in the FP64 mode, runs the
+// FP64 GEMM.
+void xgemm(bool transA, int M, int N, int K, const double* A, int lda, const double* B, int ldb, double* C,
+           int ldc);
 
 // Plain C = A (M x K) * B^T (N x K) with A, B given as FP64 and split on the fly
 // into BF16 hi/lo; used by tests of the tensor-core kernel.  C is M x N (ld M).

@@ -6,6 +6,7 @@
 //                                     refresh of :936-1000 (k_block = 1)
 //
 // X (n x p) and Y (n x m) are the centred (scaled) device matrices.
+#include "xop_split.cuh"
 #include "gaussian.cuh"
 #include "xprod.cuh"
 
@@ -103,12 +104,12 @@ SvdResult truncated_rsvd_crossprod_device(const double* X, int n, int p, const d
   double* Qp = ctx.arena.alloc_n<double>((size_t)p * l);
   double* Qm = ctx.arena.alloc_n<double>((size_t)m * l);
   auto a_times = [&](const double* M, double* out) {  // (m x l) -> (p x l)
-    gemm(false, false, n, l, m, 1.0, Y, n, M, m, 0.0, T, n);
-    gemm(true, false, p, l, n, 1.0, X, n, T, n, 0.0, out, p);
+    xgemm(false, n, l, m, Y, n, M, m, T, n);
+    xgemm(true, p, l, n, X, n, T, n, out, p);
   };
   auto at_times = [&](const double* M, double* out) {  // (p x l) -> (m x l)
-    gemm(false, false, n, l, p, 1.0, X, n, M, p, 0.0, T, n);
-    gemm(true, false, m, l, n, 1.0, Y, n, T, n, 0.0, out, m);
+    xgemm(false, n, l, p, X, n, M, p, T, n);
+    xgemm(true, m, l, n, Y, n, T, n, out, m);
   };
   device_gaussian(Zm, (long long)m * l, seed);
   a_times(Zm, Ys);
@@ -126,8 +127,8 @@ SvdResult truncated_rsvd_crossprod_device(const double* X, int n, int p, const d
   qr_orthonormalize(p, l, Ys, p, Qp, p);
   // B = (X Q)^T Y  (l x m), then svd_econ(B)
   double* B = ctx.arena.alloc_n<double>((size_t)l * m);
-  gemm(false, false, n, l, p, 1.0, X, n, Qp, p, 0.0, T, n);
-  gemm(true, false, l, m, n, 1.0, T, n, Y, n, 0.0, B, l);
+  xgemm(false, n, l, p, X, n, Qp, p, T, n);
+  xgemm(true, l, m, n, T, n, Y, n, B, l);
   const int r = std::min(l, m);
   double* Ub = ctx.arena.alloc_n<double>((size_t)l * r);
   double* sb = ctx.arena.alloc_n<double>(r);

@@ -39,7 +39,11 @@ enum fpls_status {
 };
 
 /* Precision of the predictor passes in the batched CV grid. */
-enum fpls_precision { FPLS_PREC_FP64 = 0, FPLS_PREC_BF16X3 = 1 };
+/* FP64: the drop-in.  BF16X3: operands split into two BF16 planes (hi, lo),
+ * three tensor-core products (~2^-16 relative per product).  BF16X6: three
+ * planes (hi, mid, lo), six products (~2^-24), FP32 accumulation in short
+ * segments, FP64 sums. */
+enum fpls_precision { FPLS_PREC_FP64 = 0, FPLS_PREC_BF16X3 = 1, FPLS_PREC_BF16X6 = 2 };
 
 /* 1 when a B200 (sm_100a) device is usable.
  * Replaces _fastPLS_has_cuda (RcppExports.cpp:87; fastPLS.cpp:1607-1609). */
@@ -360,6 +364,20 @@ int fpls_bf16x3_gemm_noalloc(const double* A, int M, int K, const double* B, int
 int fpls_x_upload(const void* X, int x_is_float32, int n, int p, int* handle, char* err,
                   size_t errlen);
 int fpls_x_free(int handle, char* err, size_t errlen);
+
+/* Session precision of the single-fit and prediction entry points
+ * (fpls_pls_model1[_xprod], fpls_pls_model2_fast[_xprod], fpls_pls_model2's
+ * cross-covariance, fpls_predict_*, the LDA projections, Gaussian-Y, OPLS,
+ * label-aware PLSSVD): FPLS_PREC_FP64 (default, the drop-in), FPLS_PREC_BF16X3
+ * or FPLS_PREC_BF16X6, where the products with the predictor block (XᵀY, X·R,
+ * Xᵀ·T, the matrix-free operator passes, the response projections) with a
+ * contraction of at least 256 run as split-BF16 tensor-core GEMMs with FP32
+ * accumulation and FP64 sums of the partials, while the small core
+ * (sketch of S, QR, eigen/SVD, Cholesky, Gram–Schmidt, LDA) stays FP64.  The
+ * CV entry points take their precision as an argument instead.  No reference
+ * counterpart (the reference's CUDA backend is FP64 only). */
+int fpls_set_precision(int precision, char* err, size_t errlen);
+int fpls_get_precision(void);
 
 /* Page-locks (pins) an existing host buffer so that the host-buffer entry
  * points copy it to and from the device at full link speed, e.g. an R matrix

@@ -225,31 +225,18 @@ def run_reference(args):
 
 
 def dist_init(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    os.environ["FASTPLS_DEVICE"] = str(local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
-        pg = dist
-    return world, rank, local, pg
+    from fastpls_b200 import replicas
+    return replicas.init_from_env()
 
 
 def reduce_max(pg, v):
-    if pg is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64)
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+    from fastpls_b200 import replicas
+    return replicas.reduce_max(pg, v)
 
 
 def barrier(pg):
-    if pg is not None:
-        pg.barrier()
+    from fastpls_b200 import replicas
+    replicas.barrier(pg)
 
 
 def run_ours(args):

@@ -122,9 +122,12 @@ def measured_peaks():
         d = json.load(open(path))
         return dict(hbm=(float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"),
                     bf16=(float(d["bf16_tflops"]), "measured (MEASURED_PEAKS.json bf16_tflops, burst)"),
-                    fp64=(40.0, "nominal B200 FP64 tensor 40 TFLOP/s (no measured FP64 figure)"))
+                    fp64=(40.0, "nominal B200 FP64 tensor 40 TFLOP/s (no measured FP64 figure)"),
+                    int8=(2.0 * float(d["bf16_tflops"]),
+                          "2 x measured BF16 burst (dense INT8 tensor rate is twice BF16; no measured INT8 figure)"))
     return dict(hbm=(6650.0, "fallback 6.65 TB/s"), bf16=(1590.0, "fallback 1.59 PFLOP/s"),
-                fp64=(40.0, "nominal B200 FP64 tensor 40 TFLOP/s (no measured FP64 figure)"))
+                fp64=(40.0, "nominal B200 FP64 tensor 40 TFLOP/s (no measured FP64 figure)"),
+                int8=(3180.0, "2 x fallback BF16 1.59 PFLOP/s"))
 
 
 # kernel class -> (roofline bound, peak key, kernel description, ncu traffic file)
@@ -132,6 +135,8 @@ KERNEL_CLASSES = {
     "dual_step": ("hbm", "hbm", "k_dual_step (per-fit SIMPLS steps in row space, 4-CTA clusters)",
                   "k_dual_step_c4_traffic.json"),
     "k_products_f64": ("tensor", "fp64", "gemm_f64_dmma (batched K products, FP64 DMMA)", None),
+    "k_products_int8": ("tensor", "int8", "ozaki_gemm_kernel (batched K products on INT8 tcgen05 digit planes, "
+                        "with the per-product digit split and partial reduction; TOP/s of int8 plane products)", None),
     "gram_bf16x3": ("tensor", "bf16", "split_gemm_kernel (tcgen05 BF16x3 row Gram, upper tiles)", None),
     "split_gemm_bf16x3": ("hbm", "hbm", "split_gemm_kernel (tcgen05 BF16x3 skinny GEMM)",
                           "split_gemm_c4_traffic.json"),

@@ -59,6 +59,7 @@ SIGNATURES = {
     "fpls_lda_project_predict": ([_DP, _I, _I, _DP, _I, _DP, _DP, _DP, _I, _IP, _DP, _C, _S],
                                  ctypes.c_int),
     "fpls_bf16x3_gemm": ([_DP, _I, _I, _DP, _I, _DP, _C, _S], ctypes.c_int),
+    "fpls_int8_emulated_gemm": ([_DP, _I, _I, _DP, _I, _I, _DP, _C, _S], ctypes.c_int),
     "fpls_cv_predict": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I, _I, _I,
                          _I, _IP, _IP, _C, _S], ctypes.c_int),
     "fpls_double_cv": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I,
@@ -422,6 +423,15 @@ def bf16x3_gemm(A, B):
     B = _f64(B)
     C = _out(A.shape[0], B.shape[1])
     _call("fpls_bf16x3_gemm", _p(A), A.shape[0], A.shape[1], _p(B), B.shape[1], _p(C))
+    return C
+
+
+def int8_emulated_gemm(A, B, slices=7):
+    """C = A B through the INT8 tensor-core (Ozaki digit-plane) product."""
+    A = _f64(A)
+    B = _f64(B)
+    C = _out(A.shape[0], B.shape[1])
+    _call("fpls_int8_emulated_gemm", _p(A), A.shape[0], A.shape[1], _p(B), B.shape[1], int(slices), _p(C))
     return C
 
 

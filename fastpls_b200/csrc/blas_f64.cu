@@ -200,15 +200,18 @@ __global__ void gemv_t_kernel(int K, int N, double alpha, const double* __restri
   if (lane == 0) y[n] = (beta == 0.0) ? alpha * acc : alpha * acc + beta * y[n];
 }
 
-__global__ void col_mean_kernel(const double* __restrict__ X, int n, int p, int ldx,
+// FP64 column means; single-precision input is summed in FP64 in the same
+// order, so its means equal those of the widened FP64 copy bit for bit.
+template <typename T>
+__global__ void col_mean_kernel(const T* __restrict__ X, int n, int p, int ldx,
                                 double* __restrict__ out) {
   const int warps_per_block = blockDim.x >> 5;
   const int j = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (j >= p) return;
-  const double* xp = X + (size_t)j * ldx;
+  const T* xp = X + (size_t)j * ldx;
   double s = 0.0;
-  for (int i = lane; i < n; i += 32) s += xp[i];
+  for (int i = lane; i < n; i += 32) s += static_cast<double>(xp[i]);
   s = warp_sum(s);
   if (lane == 0) out[j] = s / static_cast<double>(n);
 }
@@ -421,7 +424,13 @@ void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda
 
 void col_mean(const double* X, int n, int p, int ldx, double* out) {
   if (p <= 0) return;
-  col_mean_kernel<<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, out); ::fpls::note_launch();
+  col_mean_kernel<double><<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, out); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+void col_mean(const float* X, int n, int p, int ldx, double* out) {
+  if (p <= 0) return;
+  col_mean_kernel<float><<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, out); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 

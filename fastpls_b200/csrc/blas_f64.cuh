@@ -24,6 +24,7 @@ void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda
 
 // Column means of X (n x p).  out[p].
 void col_mean(const double* X, int n, int p, int ldx, double* out);
+void col_mean(const float* X, int n, int p, int ldx, double* out);
 // Column standard deviation (n-1) of an already centred X.
 void col_sd_centered(const double* X, int n, int p, int ldx, double* out);
 // X[:, j] = (X[:, j] - mean[j]) / scale[j]   (mean or scale may be null).

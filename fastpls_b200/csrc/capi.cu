@@ -14,6 +14,7 @@
 #include "cv_driver.cuh"
 #include "fits.cuh"
 #include "heads.cuh"
+#include "ozaki_gemm.cuh"
 #include "simpls_engine.cuh"
 #include "svd.cuh"
 #include "xop_split.cuh"
@@ -102,6 +103,7 @@ int fpls_reset_workspace(char* err, size_t errlen) {
   return guarded(err, errlen, [&] {
     Context::get().sync();
     split_gemm_release_cache();
+    ozaki_release_cache();
     Context::get().release();
   });
 }
@@ -664,6 +666,33 @@ int fpls_bf16x3_gemm(const double* A, int M, int K, const double* B, int N, doub
     double* dC = ctx.arena.alloc_n<double>((size_t)M * N);
     dzero(ctx.d_status + 16, sizeof(int));
     split_gemm_test(dA, dB, M, N, K, dC);
+    download(C, dC, (size_t)M * N);
+    int e = 0;
+    d2h(&e, ctx.d_status + 16, sizeof(int));
+    ctx.sync();
+    if (e) throw Error(FPLS_ERR_CUDA, "tensor-core pipeline wait timed out");
+  });
+}
+
+int fpls_int8_emulated_gemm(const double* A, int M, int K, const double* B, int N, int slices, double* C,
+                            char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(M > 0 && N > 0 && K > 0, "int8_emulated_gemm: dimensions must be positive");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    // Rows of A are K-contiguous in A^T (K x M, column-major).
+    std::vector<double> At((size_t)K * M);
+    for (int k = 0; k < K; ++k)
+      for (int m = 0; m < M; ++m) At[k + (size_t)m * K] = A[m + (size_t)k * M];
+    const double* dAt = upload(At.data(), At.size());
+    const double* dB = upload(B, (size_t)K * N);
+    double* dC = ctx.arena.alloc_n<double>((size_t)M * N);
+    dzero(ctx.d_status + 16, sizeof(int));
+    OzakiPlanes pa = ozaki_alloc(M, K, slices);
+    OzakiPlanes pb = ozaki_alloc(N, K, slices);
+    ozaki_split(dAt, K, pa);
+    ozaki_split(dB, K, pb);
+    ozaki_gemm(pa, pb, dC, M);
     download(C, dC, (size_t)M * N);
     int e = 0;
     d2h(&e, ctx.d_status + 16, sizeof(int));

@@ -5,13 +5,16 @@
 #include "gaussian.cuh"
 #include "fits.cuh"
 #include "heads.cuh"
+#include "ozaki_gemm.cuh"
 #include "simpls_engine.cuh"
 #include "svd.cuh"
 #include "xop_split.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <memory>
 #include <numeric>
+#include <string>
 #include <thread>
 
 namespace fpls {
@@ -19,10 +22,33 @@ namespace {
 
 constexpr int kMaxClassesCv = 128;
 
-__global__ void widen_f32_kernel(const float* __restrict__ src, double* __restrict__ dst, size_t n) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    dst[i] = static_cast<double>(src[i]);
+// dst (n x p, ld n) = src - mean (per column; mean may be null), widened to
+// FP64: the centred working copy in one pass over the caller's matrix.
+template <typename T>
+__global__ void load_centered_kernel(const T* __restrict__ src, int n, int p, const double* __restrict__ mean,
+                                     double* __restrict__ dst) {
+  const size_t total = (size_t)n * p;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    double v = static_cast<double>(src[idx]);
+    if (mean) v -= mean[idx / n];
+    dst[idx] = v;
+  }
+}
+
+// The mixed-mode row-space products run on the INT8 tensor cores unless
+// FASTPLS_KPROD=fp64 asks for FP64 DMMA.
+bool int8_k_products() {
+  const char* e = std::getenv("FASTPLS_KPROD");
+  return !(e && std::string(e) == "fp64");
+}
+
+void load_centered(const double* x64, const float* x32, int n, int p, const double* mean, double* dst) {
+  Context& ctx = Context::get();
+  if (x64) load_centered_kernel<double><<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(x64, n, p, mean, dst);
+  else load_centered_kernel<float><<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(x32, n, p, mean, dst);
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
 }
 
 __global__ void mask_to_double_kernel(const uint8_t* __restrict__ mask, size_t total,
@@ -167,7 +193,7 @@ void fill_special_predictions(const CvFitSet& fs, const int* y, const std::vecto
   }
 }
 
-void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, int L,
+void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const int* y, const int* ncomp, int L,
                  const CvGridOptions& opt, const std::vector<int>& status,
                  const std::vector<double>& counts, double* d_om, CvGridResult& res) {
   Context& ctx = Context::get();
@@ -185,18 +211,34 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
   PhaseTimer pt("CV grid (batched)");
   // Global centring (scaling < 3): Xc = X - mean(X); folds shift by delta_f.
   const bool center = opt.scaling < 3;
+  double* mall = nullptr;
   if (center) {
-    double* mall = ar.alloc_n<double>(p);
-    col_mean(X, n, p, n, mall);
-    center_scale(X, n, p, n, mall, nullptr);
+    mall = ar.alloc_n<double>(p);
+    if (x64) col_mean(x64, n, p, n, mall);
+    else col_mean(x32, n, p, n, mall);
   }
-  pt.mark("centre");
+  pt.mark("column means");
   // Short, wide predictor blocks run the loop in the row space of X (the
   // row Gram K = Xc Xc^T); otherwise in the predictor space.
   const bool dual = dual_engine_applies(n, p, m, K);
+  // The mixed row-space loop needs only the BF16 planes of Xc, split straight
+  // from the caller's matrix; every other combination works on a centred FP64
+  // copy.  x0 is the first column of Xc (the Householder sign of the sketch).
+  const bool planes_only = opt.precision == 1 && dual;
+  double* X = nullptr;
+  double* x0 = nullptr;
   std::unique_ptr<XOperator> xop;
-  if (opt.precision == 1) xop = make_split_operator(X, n, p, !dual);
-  else xop.reset(new XOperatorF64(X, n, p));
+  if (planes_only) {
+    x0 = ar.alloc_n<double>(n);
+    load_centered(x64, x32, n, 1, mall, x0);
+    xop = make_split_operator_centered(x64, x32, mall, n, p);
+  } else {
+    X = ar.alloc_n<double>((size_t)n * p);
+    load_centered(x64, x32, n, p, mall, X);
+    x0 = X;
+    if (opt.precision == 1) xop = make_split_operator(X, n, p, !dual);
+    else xop.reset(new XOperatorF64(X, n, p));
+  }
   pt.mark("operator");
   std::vector<uint8_t> tr((size_t)Fa * n), te((size_t)Fa * n);
   std::vector<int> grp(Fa), ntrain(Fa);
@@ -252,6 +294,15 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
     xop->gram(Kg);
     XOperatorF64 kop_f64(Kg, n, n);
     XOperator* kop = &kop_f64;
+    // Mixed mode: the K products on the INT8 tensor cores (digit planes of K
+    // split once, FP64-level accuracy); FP64 mode: FP64 DMMA.
+    std::unique_ptr<XOperator> kop_int8;
+    int kop_slices = 0;
+    if (opt.precision == 1 && int8_k_products()) {
+      kop_slices = ozaki_default_slices();
+      kop_int8 = make_ozaki_sym_operator(Kg, n, kop_slices);
+      kop = kop_int8.get();
+    }
     pt.mark("row gram");
     FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0));
     double* XOm = ar.alloc_n<double>((size_t)n * Fa);
@@ -263,7 +314,8 @@ void run_batched(const CvFitSet& fs, double* X, const int* y, const int* ncomp, 
     db.m1_mode = (m == 1);
     db.center = center;
     db.Kop = kop;
-    db.x0 = X;
+    db.kop_int8_slices = kop_slices;
+    db.x0 = x0;
     db.XOmega = XOm;
     db.mask = d_tr;
     db.labels = d_lab;
@@ -457,16 +509,18 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
   } else {
     dzero(res.d_pred, npred * sizeof(int));
   }
-  // Working FP64 copy of X (the batched path centres it in place).
-  double* X = ctx.arena.alloc_n<double>((size_t)fs.n * fs.p);
-  if (x64) {
-    d2d(X, x64, (size_t)fs.n * fs.p * sizeof(double));
-  } else {
-    widen_f32_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(x32, X, (size_t)fs.n * fs.p); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
+  if (batched) {
+    run_batched(fs, x64, x32, labels_host, ncomp, L, opt, status, counts, d_om, res);
+    return;
   }
-  if (batched) run_batched(fs, X, labels_host, ncomp, L, opt, status, counts, d_om, res);
-  else run_sequential(fs, X, labels_host, ncomp, L, opt, status, res);
+  // The per-fit path reads X in FP64 (widened once when the caller's is FP32).
+  const double* X = x64;
+  if (!X) {
+    double* w = ctx.arena.alloc_n<double>((size_t)fs.n * fs.p);
+    load_centered(nullptr, x32, fs.n, fs.p, nullptr, w);
+    X = w;
+  }
+  run_sequential(fs, X, labels_host, ncomp, L, opt, status, res);
 }
 
 void cv_prediction_counts(const int* d_pred, int G, int L, int n, const int* d_labels,

@@ -442,9 +442,18 @@ void dual_simpls_run(const DualBatch& b) {
     ctx.prof_end(slot, st, Fd * (8.0 * words + (a < b.K ? 5.0 * nd : 0.0)), 0.0);
     pt.mark("per-fit steps");
     if (a == b.K) break;
-    const int ks = ctx.prof_begin("k_products_f64", st);
-    b.Kop->times(e.cp, b.F, e.Gp);
-    ctx.prof_end(ks, st, 8.0 * (nd * nd + 2.0 * nd * Fd), 2.0 * nd * nd * Fd);
+    if (b.kop_int8_slices > 0) {
+      // digit planes of K and of the F coefficient columns, the FP64 columns in
+      // and out; the S (S + 1) / 2 int8 plane products
+      const double S = b.kop_int8_slices;
+      const int ks = ctx.prof_begin("k_products_int8", st);
+      b.Kop->times(e.cp, b.F, e.Gp);
+      ctx.prof_end(ks, st, S * nd * nd + S * nd * Fd + 16.0 * nd * Fd, 0.5 * S * (S + 1.0) * 2.0 * nd * nd * Fd);
+    } else {
+      const int ks = ctx.prof_begin("k_products_f64", st);
+      b.Kop->times(e.cp, b.F, e.Gp);
+      ctx.prof_end(ks, st, 8.0 * (nd * nd + 2.0 * nd * Fd), 2.0 * nd * nd * Fd);
+    }
     pt.mark("K products");
   }
   pt.report();

@@ -33,6 +33,7 @@ struct DualBatch {
   bool m1_mode = false;
   bool center = true;                // fold centring of the predictors (scaling < 3)
   XOperator* Kop = nullptr;          // K = Xc Xc^T (n x n), times() only
+  int kop_int8_slices = 0;           // > 0: Kop is the INT8 digit-plane product with these slices
   const double* x0 = nullptr;        // n: first column of Xc (Householder sign)
   const double* XOmega = nullptr;    // n x F: Xc Omega_f (first refresh step)
   const uint8_t* mask = nullptr;     // F x n train masks

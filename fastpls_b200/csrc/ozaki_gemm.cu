@@ -1,0 +1,560 @@
+// FP64-accurate products on the sm_100a INT8 tensor cores.
+//
+//   C (M x N, FP64) = A (M x K) * B (N x K)^T
+//
+// Method: the error-free slice splitting of Ozaki, Ogita and Oishi ("Error-free
+// transformations of matrix multiplication by using fast routines of matrix
+// multiplication and its applications", Numer. Algorithms 59, 2012) in its
+// integer form (Ootomo, Ozaki and Yokota, "DGEMM on integer matrix
+// multiplication unit", IJHPCA 2024).  Each row r of A and of B (both
+// K-contiguous) is scaled by 2^-e_r, e_r the binary exponent of its largest
+// magnitude (so every scaled entry is below 1 in magnitude), and written as S
+// signed 7-bit digits,
+//     x = 2^e * sum_{s=1..S} d_s 2^{-7s} + r,   |d_s| <= 127,  |r| < 2^{e-7S},
+// each digit taken exactly in FP64 (multiply by 128, truncate, subtract).  A
+// product of two digit planes is exact in int32 (at most K * 127^2 per pair).
+// The pairs with s + t <= S + 1 are summed per level l = s + t into their own
+// int32 TMEM accumulator (several pairs share a level), and the levels are
+// combined in FP64:
+//     (A B^T)_ij = 2^{eA_i + eB_j} sum_l 2^{-7l} Acc_l(i, j) + error,
+//     |error| <~ 3 K 2^{eA_i + eB_j - 7S}.
+//
+// Kernel (persistent, one CTA per SM, 6 warps; stream-K over (tile, K block)):
+//   warp 0 lane 0  TMA producer.  Per 128-wide K block: the S digit planes of
+//                  the 64-row B tile (8 KB each) into one of two B sets, and
+//                  the S planes of the 128-row A tile (16 KB each) into S
+//                  single-plane slots, each refilled as soon as its last MMA
+//                  of the previous K block is done;
+//   warp 1 lane 0  MMA issuer: for A plane s, the pairs with B planes
+//                  t <= S + 1 - s, four tcgen05.mma (M128 N64 K32, kind::i8)
+//                  each, into the level accumulator s + t (S x 64 TMEM columns);
+//   warps 2..5     epilogue: tcgen05.ld of the S level accumulators, FP64
+//                  combination with the row and column scales, written as an
+//                  FP64 stream-K partial; a second kernel sums each tile's
+//                  partials in a fixed order (deterministic).
+// Every mbarrier wait is bounded (error flag, no endless spin); the copies and
+// MMAs in flight are drained before the CTA releases TMEM and exits.  No
+// cluster multicast is used.
+#include "ozaki_gemm.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdlib>
+#include <map>
+#include <vector>
+
+#include "context.cuh"
+#include "tc_util.cuh"
+
+namespace fpls {
+namespace {
+
+using tc::mbar_arrive;
+using tc::mbar_expect_tx;
+using tc::mbar_init;
+using tc::mbar_wait;
+using tc::smem_u32;
+using tc::sw128_desc;
+using tc::tma_load_2d;
+using tc::umma_commit;
+
+constexpr int OBM = 128;                 // A rows per tile
+constexpr int OBN = 64;                  // B rows per tile
+constexpr int OBK = 128;                 // K per block (one 128-byte swizzle row of int8)
+constexpr int A_PLANE = OBM * OBK;       // 16 KB
+constexpr int B_PLANE = OBN * OBK;       // 8 KB
+constexpr int kThreads = 192;
+constexpr int kTmemCols = 512;
+// int32 headroom: one level sums at most S pairs over one segment, so
+// S * (64 * 128) * 127^2 < 2^31 for S <= 7.
+constexpr int kMaxSegBlocks = 64;
+constexpr int kReducePieces = 8;
+
+template <int S>
+struct OzLayout {
+  static constexpr int A_BYTES = S * A_PLANE;
+  static constexpr int B_SET = S * B_PLANE;
+  static constexpr int BAR_OFF = A_BYTES + 2 * B_SET;
+  static constexpr int SMEM_BYTES = BAR_OFF + 256 + 1024;
+};
+static_assert(OzLayout<kOzakiMaxSlices>::SMEM_BYTES <= 227 * 1024, "digit planes exceed shared memory");
+static_assert(kOzakiMaxSlices * OBN <= kTmemCols, "level accumulators exceed TMEM");
+
+// Instruction descriptor: D S32, A/B signed 8-bit, both K-major, N = 64, M = 128.
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(OBN >> 3) << 17) |
+                              (uint32_t(OBM >> 4) << 24);
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdescI8), "r"(accumulate)
+      : "memory");
+}
+
+// 2^e as a double, for -1022 <= e <= 1023.
+__host__ __device__ __forceinline__ double pow2i(int e) {
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double(static_cast<long long>(1023 + e) << 52);
+#else
+  return std::ldexp(1.0, e);
+#endif
+}
+
+template <int S>
+__global__ void __launch_bounds__(kThreads, 1)
+ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB,
+                  int a_rows_pad, int b_rows_pad, const double* __restrict__ sA,
+                  const double* __restrict__ sB, const int4* __restrict__ segs,
+                  const int* __restrict__ cta_seg_begin, int n_tiles_n, double* __restrict__ part,
+                  int* err) {
+  using L = OzLayout<S>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~static_cast<uintptr_t>(1023));
+  uint8_t* sa = smem;                  // S single-plane A slots
+  uint8_t* sb = smem + L::A_BYTES;     // two sets of S B planes
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
+  uint64_t* fullA = bars;
+  uint64_t* emptyA = bars + S;
+  uint64_t* fullB = bars + 2 * S;
+  uint64_t* emptyB = bars + 2 * S + 2;
+  uint64_t* tfull = bars + 2 * S + 4;
+  uint64_t* tempty = bars + 2 * S + 5;
+  uint64_t* done = bars + 2 * S + 6;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 7);
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int sbeg = cta_seg_begin[blockIdx.x];
+  const int send = cta_seg_begin[blockIdx.x + 1];
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(smem_u32(&fullA[s]), 1);
+      mbar_init(smem_u32(&emptyA[s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&fullB[b]), 1);
+      mbar_init(smem_u32(&emptyB[b]), 1);
+    }
+    mbar_init(smem_u32(tfull), 1);
+    mbar_init(smem_u32(tempty), 128);
+    mbar_init(smem_u32(done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------------------------------------------------- producer
+    int it = 0;         // K blocks of this CTA so far
+    int b_loads = 0;    // B sets issued (iterations 0 .. b_loads - 1)
+    int a_last[S];      // last iteration whose plane s was issued, or -1
+#pragma unroll
+    for (int s = 0; s < S; ++s) a_last[s] = -1;
+    bool ok = true;
+    for (int sg = sbeg; sg < send && ok; ++sg) {
+      const int4 seg = segs[sg];
+      const int mt = seg.x / n_tiles_n, nt = seg.x % n_tiles_n;
+      for (int kb = seg.y; kb < seg.z && ok; ++kb, ++it) {
+        const int b = it & 1;
+        if (!mbar_wait(smem_u32(&emptyB[b]), ((it >> 1) & 1) ^ 1, err)) { ok = false; break; }
+        const uint32_t fb = smem_u32(&fullB[b]);
+        mbar_expect_tx(fb, S * B_PLANE);
+#pragma unroll
+        for (int t = 0; t < S; ++t)
+          tma_load_2d(&mB, smem_u32(sb + b * L::B_SET + t * B_PLANE), fb, kb * OBK, t * b_rows_pad + nt * OBN);
+        b_loads = it + 1;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          if (!ok) break;
+          if (!mbar_wait(smem_u32(&emptyA[s]), (it & 1) ^ 1, err)) { ok = false; break; }
+          const uint32_t fa = smem_u32(&fullA[s]);
+          mbar_expect_tx(fa, A_PLANE);
+          tma_load_2d(&mA, smem_u32(sa + s * A_PLANE), fa, kb * OBK, s * a_rows_pad + mt * OBM);
+          a_last[s] = it;
+        }
+      }
+    }
+    // Drain: the last copy issued into every slot has landed before the CTA
+    // can exit (bounded waits that ignore the error flag).
+    for (int d = 1; d <= 2 && b_loads - d >= 0; ++d) {
+      const int u = b_loads - d;
+      mbar_wait(smem_u32(&fullB[u & 1]), (u >> 1) & 1, err, false);
+    }
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+      if (a_last[s] >= 0) mbar_wait(smem_u32(&fullA[s]), a_last[s] & 1, err, false);
+  } else if (warp == 1 && lane == 0) {
+    // ---------------------------------------------------------- MMA issuer
+    int it = 0, j = 0;
+    bool ok = true;
+    for (int sg = sbeg; sg < send && ok; ++sg, ++j) {
+      const int4 seg = segs[sg];
+      if (!mbar_wait(smem_u32(tempty), (j & 1) ^ 1, err)) { ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t inited = 0;   // level accumulators written in this segment
+      for (int kb = seg.y; kb < seg.z && ok; ++kb, ++it) {
+        const int b = it & 1;
+        if (!mbar_wait(smem_u32(&fullB[b]), (it >> 1) & 1, err)) { ok = false; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t b0 = smem_u32(sb + b * L::B_SET);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          if (!mbar_wait(smem_u32(&fullA[s]), it & 1, err)) { ok = false; break; }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a0 = smem_u32(sa + s * A_PLANE);
+#pragma unroll
+          for (int t = 0; t + s < S; ++t) {
+            const int l = s + t;
+            const uint32_t acc = tmem + static_cast<uint32_t>(l * OBN);
+#pragma unroll
+            for (int k = 0; k < OBK / 32; ++k) {
+              const uint32_t off = k * 32;  // 32 int8 along K per MMA inside the swizzle row
+              umma_i8(acc, sw128_desc(a0 + off), sw128_desc(b0 + t * B_PLANE + off),
+                      (k > 0 || ((inited >> l) & 1u)) ? 1u : 0u);
+            }
+            inited |= 1u << l;
+          }
+          umma_commit(smem_u32(&emptyA[s]));
+        }
+        if (!ok) break;
+        umma_commit(smem_u32(&emptyB[b]));
+      }
+      if (!ok) break;
+      umma_commit(smem_u32(tfull));
+    }
+    // Every MMA issued by this thread has completed before TMEM is released.
+    umma_commit(smem_u32(done));
+    mbar_wait(smem_u32(done), 0, err, false);
+  } else if (warp >= 2) {
+    // ---------------------------------------------------------- epilogue
+    const int q = warp & 3;  // TMEM lane quarter accessible to this warp
+    int j = 0;
+    for (int sg = sbeg; sg < send; ++sg, ++j) {
+      const int4 seg = segs[sg];
+      const int mt = seg.x / n_tiles_n, nt = seg.x % n_tiles_n;
+      const bool ok = mbar_wait(smem_u32(tfull), j & 1, err);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (!ok) {
+        mbar_arrive(smem_u32(tempty));
+        break;
+      }
+      const double rs = sA[mt * OBM + q * 32 + lane];
+      const double* cs = sB + nt * OBN;
+      double* dst = part + static_cast<size_t>(sg) * OBN * OBM + q * 32 + lane;
+      const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16);
+#pragma unroll 1
+      for (int c = 0; c < OBN / 16; ++c) {
+        uint32_t v[S][16];
+#pragma unroll
+        for (int l = 0; l < S; ++l) tc::tmem_ld16_raw(base + static_cast<uint32_t>(l * OBN + c * 16), v[l]);
+        tc::tmem_wait_ld();
+        double acc[16];
+#pragma unroll
+        for (int x = 0; x < 16; ++x) acc[x] = 0.0;
+        // smallest level first
+#pragma unroll
+        for (int l = S - 1; l >= 0; --l) {
+          const double w = pow2i(-7 * (l + 2));
+#pragma unroll
+          for (int x = 0; x < 16; ++x) acc[x] += static_cast<double>(static_cast<int32_t>(v[l][x])) * w;
+        }
+#pragma unroll
+        for (int x = 0; x < 16; ++x) dst[static_cast<size_t>(c * 16 + x) * OBM] = acc[x] * rs * cs[c * 16 + x];
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(smem_u32(tempty));
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+// C[m + n*ldc] = sum of the tile's partials, in segment order.
+__global__ void ozaki_reduce_kernel(const double* __restrict__ part, const int* __restrict__ tile_seg,
+                                    int n_tiles_n, int M, int N, double* __restrict__ C, int ldc) {
+  const int tile = blockIdx.x / kReducePieces;
+  const int piece = blockIdx.x % kReducePieces;
+  const int mt = tile / n_tiles_n, nt = tile % n_tiles_n;
+  const int s0 = tile_seg[tile], s1 = tile_seg[tile + 1];
+  const int e0 = piece * (OBM * OBN / kReducePieces), e1 = e0 + OBM * OBN / kReducePieces;
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const int mm = e % OBM, nn = e / OBM;
+    const int m = mt * OBM + mm, n = nt * OBN + nn;
+    if (m >= M || n >= N) continue;
+    double acc = 0.0;
+    for (int s = s0; s < s1; ++s) acc += part[(static_cast<size_t>(s) * OBN + nn) * OBM + mm];
+    C[m + static_cast<size_t>(n) * ldc] = acc;
+  }
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// One block per plane row j: the scale exponent from the largest |X[:, j]|,
+// then the S digits of every entry (zeros in the padding).
+__global__ void ozaki_split_kernel(const double* __restrict__ X, int klen, int cols, int ldx,
+                                   int8_t* __restrict__ P, int ldk, size_t plane_stride, int S,
+                                   double* __restrict__ scale) {
+  __shared__ double red[32];
+  __shared__ int bad_any;
+  const int j = blockIdx.x;
+  const double* x = X + static_cast<size_t>(j) * ldx;
+  if (threadIdx.x == 0) bad_any = 0;
+  double m = 0.0;
+  bool bad = false;
+  if (j < cols)
+    for (int i = threadIdx.x; i < klen; i += blockDim.x) {
+      const double v = x[i];
+      if (!isfinite(v)) bad = true;
+      else m = fmax(m, fabs(v));
+    }
+  m = warp_max(m);
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  __syncthreads();
+  if (bad) bad_any = 1;
+  if (ln == 0) red[w] = m;
+  __syncthreads();
+  if (w == 0) {
+    double r = ln < (int)(blockDim.x >> 5) ? red[ln] : 0.0;
+    r = warp_max(r);
+    if (ln == 0) red[0] = r;
+  }
+  __syncthreads();
+  m = red[0];
+  int e = 0;
+  if (m > 0.0) frexp(m, &e);       // m = f 2^e with 1/2 <= f < 1, so |x| 2^-e < 1
+  if (e > 1000 && threadIdx.x == 0) bad_any = 1;   // beyond the scale range: NaN column
+  e = max(-1000, min(1000, e));
+  const double inv = pow2i(-e);
+  if (threadIdx.x == 0) scale[j] = bad_any ? __longlong_as_double(0x7ff8000000000000ll) : pow2i(e);
+  int8_t* row = P + static_cast<size_t>(j) * ldk;
+  for (int i = threadIdx.x; i < ldk; i += blockDim.x) {
+    double a = (j < cols && i < klen) ? x[i] * inv : 0.0;
+    if (!isfinite(a)) a = 0.0;
+    for (int s = 0; s < S; ++s) {
+      a *= 128.0;
+      const double d = trunc(a);
+      a -= d;
+      row[static_cast<size_t>(s) * plane_stride + i] = static_cast<int8_t>(static_cast<int>(d));
+    }
+  }
+}
+
+int round_up(int x, int a) { return (x + a - 1) / a * a; }
+
+struct OzPlan {
+  int tiles = 0, ntn = 0, ctas = 0;
+  std::vector<int4> segs;
+  std::vector<int> cta_begin, tile_begin;
+};
+
+// Stream-K plan: CTA c covers iterations [c*total/ctas, (c+1)*total/ctas) of
+// the (tile, K block) space, cut into per-tile segments of at most
+// kMaxSegBlocks K blocks.
+OzPlan plan_ozaki(int M, int N, int K, int sm_count) {
+  OzPlan g;
+  const int mt = (M + OBM - 1) / OBM;
+  g.ntn = (N + OBN - 1) / OBN;
+  g.tiles = mt * g.ntn;
+  const int kbt = (K + OBK - 1) / OBK;
+  const long long total = static_cast<long long>(g.tiles) * kbt;
+  g.ctas = static_cast<int>(std::max<long long>(1, std::min<long long>(sm_count, total)));
+  g.cta_begin.assign(g.ctas + 1, 0);
+  g.tile_begin.assign(g.tiles + 1, 0);
+  for (int c = 0; c < g.ctas; ++c) {
+    g.cta_begin[c] = static_cast<int>(g.segs.size());
+    long long a = total * c / g.ctas, e = total * (c + 1) / g.ctas;
+    while (a < e) {
+      const int t = static_cast<int>(a / kbt);
+      const int kb0 = static_cast<int>(a % kbt);
+      int kb1 = static_cast<int>(std::min<long long>(kbt, kb0 + (e - a)));
+      kb1 = std::min(kb1, kb0 + kMaxSegBlocks);
+      g.segs.push_back(make_int4(t, kb0, kb1, 0));
+      a += kb1 - kb0;
+    }
+  }
+  g.cta_begin[g.ctas] = static_cast<int>(g.segs.size());
+  int s = 0;
+  for (int t = 0; t < g.tiles; ++t) {
+    g.tile_begin[t] = s;
+    while (s < static_cast<int>(g.segs.size()) && g.segs[s].x == t) ++s;
+  }
+  g.tile_begin[g.tiles] = s;
+  return g;
+}
+
+struct OzCached {
+  OzPlan g;
+  char* dev = nullptr;
+  int4* segs = nullptr;
+  int* cta_begin = nullptr;
+  int* tile_begin = nullptr;
+  double* part = nullptr;
+};
+
+std::map<std::array<int, 4>, OzCached>& oz_cache() {
+  static std::map<std::array<int, 4>, OzCached> cache;
+  return cache;
+}
+
+// Plans, their device tables and the partial buffers are kept per shape, so
+// the repeated products of an iteration issue no host-to-device copy.
+const OzCached& oz_plan(int M, int N, int K, int sm_count, cudaStream_t st) {
+  auto& cache = oz_cache();
+  const std::array<int, 4> key{M, N, K, sm_count};
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  OzCached c;
+  c.g = plan_ozaki(M, N, K, sm_count);
+  auto up = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  const size_t b_segs = up(c.g.segs.size() * sizeof(int4));
+  const size_t b_cta = up(c.g.cta_begin.size() * sizeof(int));
+  const size_t b_tile = up(c.g.tile_begin.size() * sizeof(int));
+  const size_t b_part = c.g.segs.size() * static_cast<size_t>(OBM) * OBN * sizeof(double);
+  FPLS_CUDA(cudaMalloc(&c.dev, b_segs + b_cta + b_tile + b_part));
+  c.segs = reinterpret_cast<int4*>(c.dev);
+  c.cta_begin = reinterpret_cast<int*>(c.dev + b_segs);
+  c.tile_begin = reinterpret_cast<int*>(c.dev + b_segs + b_cta);
+  c.part = reinterpret_cast<double*>(c.dev + b_segs + b_cta + b_tile);
+  FPLS_CUDA(cudaMemcpyAsync(c.segs, c.g.segs.data(), c.g.segs.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+  FPLS_CUDA(cudaMemcpyAsync(c.cta_begin, c.g.cta_begin.data(), c.g.cta_begin.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, st));
+  FPLS_CUDA(cudaMemcpyAsync(c.tile_begin, c.g.tile_begin.data(), c.g.tile_begin.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, st));
+  return cache.emplace(key, std::move(c)).first->second;
+}
+
+// 2-D int8 tensor map over all planes stacked (rows_pad * slices rows of ldk bytes).
+CUtensorMap make_plane_map(const OzakiPlanes& p, int box_rows) {
+  CUtensorMap m;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(p.ldk), static_cast<cuuint64_t>(p.rows_pad) * p.slices};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(p.ldk)};
+  cuuint32_t box[2] = {static_cast<cuuint32_t>(OBK), static_cast<cuuint32_t>(box_rows)};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = tc::encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, p.data, dims, strides, box, estr,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(kErrCuda, "cuTensorMapEncodeTiled failed (digit planes)");
+  return m;
+}
+
+template <int S>
+void launch_ozaki(const CUtensorMap& mA, const CUtensorMap& mB, const OzakiPlanes& A, const OzakiPlanes& B,
+                  const OzCached& c, int* err, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    FPLS_CUDA(cudaFuncSetAttribute(ozaki_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   OzLayout<S>::SMEM_BYTES));
+    attr = true;
+  }
+  ozaki_gemm_kernel<S><<<c.g.ctas, kThreads, OzLayout<S>::SMEM_BYTES, st>>>(
+      mA, mB, A.rows_pad, B.rows_pad, A.scale, B.scale, c.segs, c.cta_begin, c.g.ntn, c.part, err);
+}
+
+struct XOperatorOzakiSym : public XOperator {
+  OzakiPlanes kp;
+  int slices;
+  XOperatorOzakiSym(const double* K, int n_, int s) : slices(s) {
+    n = n_;
+    p = n_;
+    kp = ozaki_alloc(n, n, slices);
+    ozaki_split(K, n, kp);   // row j of the planes = column j of K = row j (K symmetric)
+  }
+  void times(const double* M, int F, double* U) override {
+    OzakiPlanes b = ozaki_alloc(F, n, slices);
+    ozaki_split(M, n, b);
+    ozaki_gemm(kp, b, U, n);
+  }
+  void t_times(const double* M, int F, double* U) override { times(M, F, U); }
+  void gram(double*) override { throw Error(kErrArgument, "the INT8 product operator has no Gram"); }
+};
+
+}  // namespace
+
+OzakiPlanes ozaki_alloc(int rows, int k, int slices) {
+  FPLS_REQUIRE(slices >= kOzakiMinSlices && slices <= kOzakiMaxSlices, "INT8 products: slices must be in 4..7");
+  FPLS_REQUIRE(rows >= 1 && k >= 1, "INT8 products: empty operand");
+  OzakiPlanes p;
+  p.rows = rows;
+  p.k = k;
+  p.slices = slices;
+  p.rows_pad = round_up(rows, OBM);
+  p.ldk = round_up(k, OBK);
+  Arena& ar = Context::get().arena;
+  p.data = ar.alloc_n<int8_t>(static_cast<size_t>(slices) * p.rows_pad * p.ldk);
+  p.scale = ar.alloc_n<double>(p.rows_pad);
+  return p;
+}
+
+void ozaki_split(const double* X, int ldx, const OzakiPlanes& out) {
+  Context& ctx = Context::get();
+  ozaki_split_kernel<<<out.rows_pad, 256, 0, ctx.stream>>>(X, out.k, out.rows, ldx, out.data, out.ldk,
+                                                           static_cast<size_t>(out.rows_pad) * out.ldk,
+                                                           out.slices, out.scale);
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc) {
+  FPLS_REQUIRE(A.slices == B.slices && A.k == B.k && A.ldk == B.ldk, "INT8 products: operands do not match");
+  Context& ctx = Context::get();
+  cudaStream_t st = ctx.stream;
+  const int M = A.rows, N = B.rows, K = A.k;
+  const OzCached& c = oz_plan(M, N, K, ctx.sm_count, st);
+  const CUtensorMap mA = make_plane_map(A, OBM);
+  const CUtensorMap mB = make_plane_map(B, OBN);
+  int* err = ctx.d_status + 16;
+  const int S = A.slices;
+  switch (S) {
+    case 4: launch_ozaki<4>(mA, mB, A, B, c, err, st); break;
+    case 5: launch_ozaki<5>(mA, mB, A, B, c, err, st); break;
+    case 6: launch_ozaki<6>(mA, mB, A, B, c, err, st); break;
+    default: launch_ozaki<7>(mA, mB, A, B, c, err, st); break;
+  }
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  ozaki_reduce_kernel<<<c.g.tiles * kReducePieces, 256, 0, st>>>(c.part, c.tile_begin, c.g.ntn, M, N, C, ldc);
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+void ozaki_release_cache() {
+  for (auto& kv : oz_cache()) cudaFree(kv.second.dev);
+  oz_cache().clear();
+}
+
+std::unique_ptr<XOperator> make_ozaki_sym_operator(const double* K, int n, int slices) {
+  return std::unique_ptr<XOperator>(new XOperatorOzakiSym(K, n, slices));
+}
+
+int ozaki_default_slices() {
+  if (const char* e = std::getenv("FASTPLS_OZAKI_SLICES")) {
+    const int v = std::atoi(e);
+    if (v >= kOzakiMinSlices && v <= kOzakiMaxSlices) return v;
+  }
+  return 7;
+}
+
+}  // namespace fpls

@@ -1,0 +1,53 @@
+// FP64-accurate matrix products on the INT8 tensor cores: the operands are
+// split into signed 7-bit digit planes with a power-of-two scale per row, the
+// plane pairs are multiplied exactly (tcgen05.mma kind::i8, int32 in TMEM) and
+// recombined in FP64 (Ozaki, Ogita and Oishi 2012, integer form of Ootomo,
+// Ozaki and Yokota 2024).
+#pragma once
+
+#include <cstdint>
+#include <memory>
+
+#include "simpls_engine.cuh"
+
+namespace fpls {
+
+// Digit planes of one operand: `rows` rows of the contraction length k, each
+// row scaled by scale[r] = 2^e_r and held as `slices` int8 planes (plane s at
+// data + s * rows_pad * ldk), rows_pad and ldk padded to 128 with zeros.
+struct OzakiPlanes {
+  int8_t* data = nullptr;
+  double* scale = nullptr;
+  int rows = 0, rows_pad = 0, k = 0, ldk = 0, slices = 0;
+};
+
+// Slices per operand accepted by the kernel.
+constexpr int kOzakiMinSlices = 4;
+constexpr int kOzakiMaxSlices = 7;
+
+OzakiPlanes ozaki_alloc(int rows, int k, int slices);
+
+// Planes of the columns of the column-major FP64 matrix X (k x rows, ld ldx):
+// row j of the planes is column j of X.  A non-finite column gets a NaN scale,
+// so that its products are NaN.
+void ozaki_split(const double* X, int ldx, const OzakiPlanes& out);
+
+// C (M x N, ld ldc, FP64) = A B^T with A (M x k) and B (N x k) given as planes
+// with the same slice count and contraction length.  The digit pairs whose
+// levels s + t exceed slices + 1 are dropped; the result differs from the
+// exact product by at most about 3 k 2^(eA_i + eB_j - 7 slices) per entry.
+void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc);
+
+// Releases the cached stream-K plans (fpls_reset_workspace).
+void ozaki_release_cache();
+
+// Operator over a symmetric n x n FP64 matrix K, split once into planes:
+// times() and t_times() are K * M through the INT8 tensor cores; gram() is not
+// provided.
+std::unique_ptr<XOperator> make_ozaki_sym_operator(const double* K, int n, int slices);
+
+// Slice count of the mixed-precision row-space products (environment
+// FASTPLS_OZAKI_SLICES, else 7).
+int ozaki_default_slices();
+
+}  // namespace fpls

@@ -30,10 +30,28 @@
 
 #include "blas_f64.cuh"
 #include "context.cuh"
+#include "tc_util.cuh"
 #include "xop_split.cuh"
 
 namespace fpls {
 namespace {
+
+using tc::encode_fn;
+using tc::mbar_arrive;
+using tc::mbar_expect_tx;
+using tc::mbar_init;
+using tc::mbar_wait;
+using tc::smem_u32;
+using tc::sw128_desc;
+using tc::tma_load_2d;
+using tc::umma_commit;
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  tc::tmem_ld16_raw(taddr, r);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
 
 constexpr int BM = 128;
 constexpr int BN = 64;
@@ -51,68 +69,11 @@ template <int NP> struct Planes {
 static_assert(Planes<3>::SMEM_BYTES <= 227 * 1024, "three-plane stages exceed shared memory");
 constexpr int NUM_THREADS = 192;
 constexpr int TMEM_COLS = 2 * BN;
-constexpr long long kWaitBudget = 1ll << 33;        // ~4 s at 2 GHz
 
 // Instruction descriptor: D F32, A/B BF16, both K-major, N = 64, M = 128.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
                             (uint32_t(BN >> 3) << 17) | (uint32_t(BM >> 4) << 24);
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
-
-// Bounded parity wait: returns false (and raises *err) when the budget runs out
-// or an error was already raised by another thread.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err,
-                                          bool stop_on_error = true) {
-  const long long t0 = clock64();
-  for (uint32_t spin = 0;; ++spin) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if (stop_on_error && (spin & 63) == 63 && *(volatile int*)err) return false;
-    if (clock64() - t0 > kWaitBudget) {
-      atomicExch(err, 1);
-      return false;
-    }
-  }
-}
-
-__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint32_t dst, uint32_t bar,
-                                            int x, int y) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-      : "memory");
-}
-
-// UMMA shared-memory descriptor: K-major, SWIZZLE_128B, 8-row core groups 1024 B apart.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-  uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
-  d |= static_cast<uint64_t>(1) << 16;              // leading byte offset (unused for SW128 K-major)
-  d |= static_cast<uint64_t>(1024 >> 4) << 32;      // stride byte offset
-  d |= static_cast<uint64_t>(1) << 46;              // descriptor version for sm_100
-  d |= static_cast<uint64_t>(2) << 61;              // SWIZZLE_128B
-  return d;
-}
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
                                           uint32_t accumulate) {
@@ -123,22 +84,6 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint6
       : "memory");
 }
 
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
 
 template <int NP>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
@@ -343,15 +288,25 @@ __global__ void split_cols_kernel(const double* __restrict__ X, int rows, int co
 
 // hi/lo split with transpose: X (rows x cols col-major, ld) -> rows x ldo
 // row-major pairs (row i holds X[i, :]), zero padded.  32 x 32 tiles via smem.
-__global__ void split_rows_kernel(const double* __restrict__ X, int rows, int cols, int ld,
+// With `mean` the column means are subtracted (in FP64) before the split, so a
+// single-precision or uncentred caller matrix is centred and split in one pass
+// with the same values as centring an FP64 copy first.
+template <typename T>
+__global__ void split_rows_kernel(const T* __restrict__ X, int rows, int cols, int ld,
                                   __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
-                                  int ldo, __nv_bfloat16* __restrict__ mid) {
+                                  int ldo, __nv_bfloat16* __restrict__ mid,
+                                  const double* __restrict__ mean) {
   __shared__ double tile[32][33];
   const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
   for (int r = ty; r < 32; r += 8) {
     const int i = i0 + tx, j = j0 + r;
-    tile[r][tx] = (i < rows && j < cols) ? X[i + static_cast<size_t>(j) * ld] : 0.0;
+    double v = 0.0;
+    if (i < rows && j < cols) {
+      v = static_cast<double>(X[i + static_cast<size_t>(j) * ld]);
+      if (mean) v -= mean[j];
+    }
+    tile[r][tx] = v;
   }
   __syncthreads();
   for (int r = ty; r < 32; r += 8) {
@@ -367,18 +322,6 @@ __global__ void split_rows_kernel(const double* __restrict__ X, int rows, int co
   }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    FPLS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
-    if (!p || q != cudaDriverEntryPointSuccess)
-      throw Error(kErrCuda, "cuTensorMapEncodeTiled is unavailable");
-    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
-  return fn;
-}
 
 // 2-D BF16 tensor map: `rows` rows of `k` elements, row pitch ld elements.
 CUtensorMap make_map(const __nv_bfloat16* base, int rows, int k, int ld, int box_rows) {
@@ -634,9 +577,11 @@ void split_cols_on(const double* X, int rows, int cols, int ld, const SplitPair&
   FPLS_CHECK_LAUNCH();
 }
 
-void split_rows_on(const double* X, int rows, int cols, int ld, const SplitPair& out, cudaStream_t st) {
+template <typename T>
+void split_rows_on(const T* X, int rows, int cols, int ld, const SplitPair& out, cudaStream_t st,
+                   const double* mean = nullptr) {
   dim3 grid((out.ld + 31) / 32, (rows + 31) / 32);
-  split_rows_kernel<<<grid, dim3(32, 8), 0, st>>>(X, rows, cols, ld, out.hi, out.lo, out.ld, out.mid); ::fpls::note_launch();
+  split_rows_kernel<T><<<grid, dim3(32, 8), 0, st>>>(X, rows, cols, ld, out.hi, out.lo, out.ld, out.mid, mean); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -663,6 +608,15 @@ struct XOperatorSplit : public XOperator {
       xc = alloc_pair(p, n, np);
       split_cols(X, n, p, n, xc);
     }
+  }
+  // Row-major planes only, split straight from the caller's matrix with the
+  // column means (or none) subtracted on the way.
+  template <typename T>
+  XOperatorSplit(const T* X, const double* mean, int n_, int p_, int np_) : has_t(false), np(np_) {
+    n = n_;
+    p = p_;
+    xr = alloc_pair(n, p, np);
+    split_rows_on(X, n, p, n, xr, Context::get().stream, mean);
   }
   void times(const double* Rhat, int F, double* U) override {
     SplitPair b = alloc_pair(F, p, np);
@@ -711,6 +665,12 @@ void split_gemm_release_cache() {
 
 std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p, bool need_t, int planes) {
   return std::unique_ptr<XOperator>(new XOperatorSplit(X, n, p, need_t, planes));
+}
+
+std::unique_ptr<XOperator> make_split_operator_centered(const double* x64, const float* x32, const double* mean,
+                                                        int n, int p, int planes) {
+  if (x64) return std::unique_ptr<XOperator>(new XOperatorSplit(x64, mean, n, p, planes));
+  return std::unique_ptr<XOperator>(new XOperatorSplit(x32, mean, n, p, planes));
 }
 
 void split_gemm_test(const double* A, const double* B, int M, int N, int K, double* C) {

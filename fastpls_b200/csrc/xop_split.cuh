@@ -19,6 +19,13 @@ void split_gemm_release_cache();
 std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p, bool need_t = true,
                                                int planes = 2);
 
+// Row-major planes only (times() and gram()), split straight from the
+// caller's n x p matrix (ld n; x64 or, when x64 is null, x32) with the column
+// means `mean` (or nothing, when null) subtracted in FP64 on the way: the same
+// planes as centring an FP64 copy and splitting it, without the copy.
+std::unique_ptr<XOperator> make_split_operator_centered(const double* x64, const float* x32, const double* mean,
+                                                        int n, int p, int planes = 2);
+
 // C (M x N) = op(A) B with op(A) = A (M x K) or A^T (A is K x M), B K x N,
 // column-major device matrices.  In the mixed precision modes (session setting
 // FPLS_PREC_BF16X3 or FPLS_PREC_BF16X6) products with a contraction of at

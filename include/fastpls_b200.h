@@ -193,6 +193,18 @@ int fpls_lda_project_predict(const double* X, int w, int p, const double* R, int
 int fpls_bf16x3_gemm(const double* A, int M, int K, const double* B, int N, double* C,
                      char* err, size_t errlen);
 
+/* C (M x N) = A (M x K) * B (K x N) through the FP64-accurate INT8 tensor-core
+ * product: every row of A and column of B is scaled by a power of two and
+ * split into `slices` (4..7) signed 7-bit digit planes, the plane pairs with
+ * s + t <= slices + 1 are multiplied exactly (tcgen05 kind::i8, int32
+ * accumulation) and recombined in FP64 (Ozaki scheme).  Entry (i, j) differs
+ * from the exact product by at most about 3 K 2^(eA_i + eB_j - 7 slices),
+ * 2^e the scale of row i of A or column j of B.  The mixed-precision CV grids
+ * use it for their row-space products; a diagnostic with no counterpart in
+ * the reference. */
+int fpls_int8_emulated_gemm(const double* A, int M, int K, const double* B, int N, int slices,
+                            double* C, char* err, size_t errlen);
+
 /* Cross-validated class predictions with the argmax classifier for method 3
  * (simpls_fast).  X is n x p, FP64 (x_is_float32 = 0) or FP32 (= 1); y are
  * 1-based labels; fold holds 0-based fold ids (drawn by the caller, as the R

@@ -6,6 +6,7 @@
 
 #include "blas_f64.cuh"
 #include "context.cuh"
+#include "ozaki_gemm.cuh"
 
 #include <cooperative_groups.h>
 
@@ -34,6 +35,12 @@ struct DualEng {
   double* Kcy;   // F x n   K image of the warm start r / ||t|| of the last component
   double* cp;    // n x F   loading coefficients (input of the K product)
   double* Gp;    // n x F   K cp
+  // K cp as INT8-product partials (when kpart is set): entry (i, f) is the sum
+  // over segments s of tile (i / 128) * kntn + f / 64 of
+  // kpart[(s * 64 + f % 64) * 128 + i % 128], in segment order.
+  const double* kpart;
+  const int* kseg;
+  int kntn;
   double* scal;  // F x 2   ||t||, sum(t)
   double* qs;    // F x m   Y^T t
   double* Q;
@@ -286,7 +293,19 @@ __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, i
 #pragma unroll
   for (int k = 0; k < kLR; ++k) {
     cv[k] = rw.ok(k) ? e.cp[(size_t)f * n + rw.row(k)] : 0.0;
-    kv[k] = rw.ok(k) ? e.Gp[(size_t)f * n + rw.row(k)] : 0.0;
+    kv[k] = 0.0;
+    if (!rw.ok(k)) continue;
+    const int i = rw.row(k);
+    if (e.kpart) {
+      const int tile = (i >> 7) * e.kntn + (f >> 6);
+      const int s1 = e.kseg[tile + 1];
+      const double* pp = e.kpart + (size_t)(f & 63) * 128 + (i & 127);
+      double v = 0.0;
+      for (int sg = e.kseg[tile]; sg < s1; ++sg) v += pp[(size_t)sg * 64 * 128];
+      kv[k] = v;
+    } else {
+      kv[k] = e.Gp[(size_t)f * n + i];
+    }
   }
   if (a > 0) {
     cluster_dots(R, CV, n, a, rw, kv);   // V^T p = C_V^T K c_p
@@ -444,10 +463,14 @@ void dual_simpls_run(const DualBatch& b) {
     if (a == b.K) break;
     if (b.kop_int8_slices > 0) {
       // digit planes of K and of the F coefficient columns, the FP64 columns in
-      // and out; the S (S + 1) / 2 int8 plane products
+      // and out; the S (S + 1) / 2 int8 plane products.  The next step sums
+      // the stream-K partials as it reads K c_p.
       const double S = b.kop_int8_slices;
       const int ks = ctx.prof_begin("k_products_int8", st);
-      b.Kop->times(e.cp, b.F, e.Gp);
+      const OzakiPartials pp = ozaki_sym_times_partials(*b.Kop, e.cp, b.F);
+      e.kpart = pp.part;
+      e.kseg = pp.tile_seg;
+      e.kntn = pp.n_tiles_n;
       ctx.prof_end(ks, st, S * nd * nd + S * nd * Fd + 16.0 * nd * Fd, 0.5 * S * (S + 1.0) * 2.0 * nd * nd * Fd);
     } else {
       const int ks = ctx.prof_begin("k_products_f64", st);

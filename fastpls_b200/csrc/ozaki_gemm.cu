@@ -26,12 +26,15 @@
 //                  single-plane slots, each refilled as soon as its last MMA
 //                  of the previous K block is done;
 //   warp 1 lane 0  MMA issuer: for A plane s, the pairs with B planes
-//                  t <= S + 1 - s, four tcgen05.mma (M128 N64 K32, kind::i8)
-//                  each, into the level accumulator s + t (S x 64 TMEM columns);
+//                  t <= S + 1 - s as tcgen05.mma (kind::i8, M128 K32) over the
+//                  B planes taken together (N = 64 per plane, up to 256): the
+//                  level accumulators s + t are 64 TMEM columns apart, so each
+//                  plane's block of D lands in its own level;
 //   warps 2..5     epilogue: tcgen05.ld of the S level accumulators, FP64
-//                  combination with the row and column scales, written as an
-//                  FP64 stream-K partial; a second kernel sums each tile's
-//                  partials in a fixed order (deterministic).
+//                  combination with the row and column scales, written to C
+//                  when the segment covers its whole tile, else as an FP64
+//                  stream-K partial; the CTA retiring a tile's last segment
+//                  sums that tile's partials in segment order (deterministic).
 // Every mbarrier wait is bounded (error flag, no endless spin); the copies and
 // MMAs in flight are drained before the CTA releases TMEM and exits.  No
 // cluster multicast is used.
@@ -72,7 +75,6 @@ constexpr int kTmemCols = 512;
 // int32 headroom: one level sums at most S pairs over one segment, so
 // S * (64 * 128) * 127^2 < 2^31 for S <= 7.
 constexpr int kMaxSegBlocks = 64;
-constexpr int kReducePieces = 8;
 
 template <int S>
 struct OzLayout {
@@ -84,15 +86,19 @@ struct OzLayout {
 static_assert(OzLayout<kOzakiMaxSlices>::SMEM_BYTES <= 227 * 1024, "digit planes exceed shared memory");
 static_assert(kOzakiMaxSlices * OBN <= kTmemCols, "level accumulators exceed TMEM");
 
-// Instruction descriptor: D S32, A/B signed 8-bit, both K-major, N = 64, M = 128.
-constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(OBN >> 3) << 17) |
-                              (uint32_t(OBM >> 4) << 24);
+// Instruction descriptor: D S32, A/B signed 8-bit, both K-major, M = 128, N = n.
+constexpr uint32_t idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(OBM >> 4) << 24);
+}
+// B planes per MMA: N = 64 * 4 = 256, the largest M = 128 int8 shape.
+constexpr int kPlanesPerMma = 4;
 
-__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n"
-      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdescI8), "r"(accumulate)
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
 
@@ -110,8 +116,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB,
                   int a_rows_pad, int b_rows_pad, const double* __restrict__ sA,
                   const double* __restrict__ sB, const int4* __restrict__ segs,
-                  const int* __restrict__ cta_seg_begin, int n_tiles_n, double* __restrict__ part,
-                  int* err) {
+                  const int* __restrict__ cta_seg_begin, const int* __restrict__ tile_seg, int n_tiles_n,
+                  double* __restrict__ part, double* __restrict__ C, int ldc, int M, int N, int* err) {
+  __shared__ int epi_fail;   // raised by any epilogue warp whose wait gave up
   using L = OzLayout<S>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
@@ -133,6 +140,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
   const int send = cta_seg_begin[blockIdx.x + 1];
 
   if (threadIdx.x == 0) {
+    epi_fail = 0;
     for (int s = 0; s < S; ++s) {
       mbar_init(smem_u32(&fullA[s]), 1);
       mbar_init(smem_u32(&emptyA[s]), 1);
@@ -205,7 +213,6 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
       const int4 seg = segs[sg];
       if (!mbar_wait(smem_u32(tempty), (j & 1) ^ 1, err)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      uint32_t inited = 0;   // level accumulators written in this segment
       for (int kb = seg.y; kb < seg.z && ok; ++kb, ++it) {
         const int b = it & 1;
         if (!mbar_wait(smem_u32(&fullB[b]), (it >> 1) & 1, err)) { ok = false; break; }
@@ -216,17 +223,21 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
           if (!mbar_wait(smem_u32(&fullA[s]), it & 1, err)) { ok = false; break; }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t a0 = smem_u32(sa + s * A_PLANE);
+          // B planes t = 0 .. S-1-s are consecutive 64-row tiles, i.e. one
+          // operand of 64 (S - s) rows; the D column block of plane t lands at
+          // TMEM column 64 (s + t), the accumulator of level s + t.  Plane s = 0
+          // touches every level and initialises them at a segment's first block.
 #pragma unroll
-          for (int t = 0; t + s < S; ++t) {
-            const int l = s + t;
-            const uint32_t acc = tmem + static_cast<uint32_t>(l * OBN);
+          for (int t0 = 0; t0 < S - s; t0 += kPlanesPerMma) {
+            const int np = (S - s - t0) < kPlanesPerMma ? (S - s - t0) : kPlanesPerMma;
+            const uint32_t idesc = idesc_i8(OBN * np);
+            const uint32_t acc = tmem + static_cast<uint32_t>((s + t0) * OBN);
 #pragma unroll
             for (int k = 0; k < OBK / 32; ++k) {
               const uint32_t off = k * 32;  // 32 int8 along K per MMA inside the swizzle row
-              umma_i8(acc, sw128_desc(a0 + off), sw128_desc(b0 + t * B_PLANE + off),
-                      (k > 0 || ((inited >> l) & 1u)) ? 1u : 0u);
+              umma_i8(acc, sw128_desc(a0 + off), sw128_desc(b0 + t0 * B_PLANE + off), idesc,
+                      (k > 0 || s > 0 || kb > seg.y) ? 1u : 0u);
             }
-            inited |= 1u << l;
           }
           umma_commit(smem_u32(&emptyA[s]));
         }
@@ -246,13 +257,19 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
     for (int sg = sbeg; sg < send; ++sg, ++j) {
       const int4 seg = segs[sg];
       const int mt = seg.x / n_tiles_n, nt = seg.x % n_tiles_n;
-      const bool ok = mbar_wait(smem_u32(tfull), j & 1, err);
+      if (!mbar_wait(smem_u32(tfull), j & 1, err)) atomicOr(&epi_fail, 1);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      if (!ok) {
+      // the four epilogue warps leave together (they share named barrier 1)
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      if (*(volatile int*)&epi_fail) {
         mbar_arrive(smem_u32(tempty));
         break;
       }
-      const double rs = sA[mt * OBM + q * 32 + lane];
+      const int tile = seg.x;
+      const int t0 = tile_seg[tile], t1 = tile_seg[tile + 1];
+      const bool whole = (t1 - t0) == 1;   // the tile's only segment: straight to C (when given)
+      const int row = mt * OBM + q * 32 + lane;
+      const double rs = sA[row];
       const double* cs = sB + nt * OBN;
       double* dst = part + static_cast<size_t>(sg) * OBN * OBM + q * 32 + lane;
       const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16);
@@ -272,8 +289,18 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
 #pragma unroll
           for (int x = 0; x < 16; ++x) acc[x] += static_cast<double>(static_cast<int32_t>(v[l][x])) * w;
         }
+        if (whole && C) {
+          if (row < M) {
 #pragma unroll
-        for (int x = 0; x < 16; ++x) dst[static_cast<size_t>(c * 16 + x) * OBM] = acc[x] * rs * cs[c * 16 + x];
+            for (int x = 0; x < 16; ++x) {
+              const int col = nt * OBN + c * 16 + x;
+              if (col < N) C[row + static_cast<size_t>(col) * ldc] = acc[x] * rs * cs[c * 16 + x];
+            }
+          }
+        } else {
+#pragma unroll
+          for (int x = 0; x < 16; ++x) dst[static_cast<size_t>(c * 16 + x) * OBM] = acc[x] * rs * cs[c * 16 + x];
+        }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(smem_u32(tempty));
@@ -288,13 +315,17 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
   }
 }
 
-// C[m + n*ldc] = sum of the tile's partials, in segment order.
+// C[m + n*ldc] = sum of the tile's partials in segment order; tiles with one
+// segment were written by the product kernel.
+constexpr int kReducePieces = 8;
+
 __global__ void ozaki_reduce_kernel(const double* __restrict__ part, const int* __restrict__ tile_seg,
                                     int n_tiles_n, int M, int N, double* __restrict__ C, int ldc) {
   const int tile = blockIdx.x / kReducePieces;
   const int piece = blockIdx.x % kReducePieces;
-  const int mt = tile / n_tiles_n, nt = tile % n_tiles_n;
   const int s0 = tile_seg[tile], s1 = tile_seg[tile + 1];
+  if (s1 - s0 <= 1) return;
+  const int mt = tile / n_tiles_n, nt = tile % n_tiles_n;
   const int e0 = piece * (OBM * OBN / kReducePieces), e1 = e0 + OBM * OBN / kReducePieces;
   for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
     const int mm = e % OBM, nn = e / OBM;
@@ -462,7 +493,7 @@ CUtensorMap make_plane_map(const OzakiPlanes& p, int box_rows) {
 
 template <int S>
 void launch_ozaki(const CUtensorMap& mA, const CUtensorMap& mB, const OzakiPlanes& A, const OzakiPlanes& B,
-                  const OzCached& c, int* err, cudaStream_t st) {
+                  const OzCached& c, double* C, int ldc, int* err, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
     FPLS_CUDA(cudaFuncSetAttribute(ozaki_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -470,7 +501,8 @@ void launch_ozaki(const CUtensorMap& mA, const CUtensorMap& mB, const OzakiPlane
     attr = true;
   }
   ozaki_gemm_kernel<S><<<c.g.ctas, kThreads, OzLayout<S>::SMEM_BYTES, st>>>(
-      mA, mB, A.rows_pad, B.rows_pad, A.scale, B.scale, c.segs, c.cta_begin, c.g.ntn, c.part, err);
+      mA, mB, A.rows_pad, B.rows_pad, A.scale, B.scale, c.segs, c.cta_begin, c.tile_begin, c.g.ntn, c.part,
+      C, ldc, A.rows, B.rows, err);
 }
 
 struct XOperatorOzakiSym : public XOperator {
@@ -488,6 +520,11 @@ struct XOperatorOzakiSym : public XOperator {
     ozaki_gemm(kp, b, U, n);
   }
   void t_times(const double* M, int F, double* U) override { times(M, F, U); }
+  OzakiPartials times_partials(const double* M, int F) {
+    OzakiPlanes b = ozaki_alloc(F, n, slices);
+    ozaki_split(M, n, b);
+    return ozaki_gemm_partials(kp, b);
+  }
   void gram(double*) override { throw Error(kErrArgument, "the INT8 product operator has no Gram"); }
 };
 
@@ -517,27 +554,46 @@ void ozaki_split(const double* X, int ldx, const OzakiPlanes& out) {
   FPLS_CHECK_LAUNCH();
 }
 
-void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc) {
+namespace {
+
+// Runs the product kernel: whole tiles straight to C (when C is given), the
+// others as partials in the cached plan.
+const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc) {
   FPLS_REQUIRE(A.slices == B.slices && A.k == B.k && A.ldk == B.ldk, "INT8 products: operands do not match");
   Context& ctx = Context::get();
   cudaStream_t st = ctx.stream;
-  const int M = A.rows, N = B.rows, K = A.k;
-  const OzCached& c = oz_plan(M, N, K, ctx.sm_count, st);
+  const OzCached& c = oz_plan(A.rows, B.rows, A.k, ctx.sm_count, st);
   const CUtensorMap mA = make_plane_map(A, OBM);
   const CUtensorMap mB = make_plane_map(B, OBN);
   int* err = ctx.d_status + 16;
-  const int S = A.slices;
-  switch (S) {
-    case 4: launch_ozaki<4>(mA, mB, A, B, c, err, st); break;
-    case 5: launch_ozaki<5>(mA, mB, A, B, c, err, st); break;
-    case 6: launch_ozaki<6>(mA, mB, A, B, c, err, st); break;
-    default: launch_ozaki<7>(mA, mB, A, B, c, err, st); break;
+  switch (A.slices) {
+    case 4: launch_ozaki<4>(mA, mB, A, B, c, C, ldc, err, st); break;
+    case 5: launch_ozaki<5>(mA, mB, A, B, c, C, ldc, err, st); break;
+    case 6: launch_ozaki<6>(mA, mB, A, B, c, C, ldc, err, st); break;
+    default: launch_ozaki<7>(mA, mB, A, B, c, C, ldc, err, st); break;
   }
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
-  ozaki_reduce_kernel<<<c.g.tiles * kReducePieces, 256, 0, st>>>(c.part, c.tile_begin, c.g.ntn, M, N, C, ldc);
+  return c;
+}
+
+}  // namespace
+
+void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc) {
+  const OzCached& c = run_ozaki(A, B, C, ldc);
+  ozaki_reduce_kernel<<<c.g.tiles * kReducePieces, 256, 0, Context::get().stream>>>(c.part, c.tile_begin, c.g.ntn,
+                                                                                 A.rows, B.rows, C, ldc);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+}
+
+OzakiPartials ozaki_gemm_partials(const OzakiPlanes& A, const OzakiPlanes& B) {
+  const OzCached& c = run_ozaki(A, B, nullptr, 0);
+  OzakiPartials p;
+  p.part = c.part;
+  p.tile_seg = c.tile_begin;
+  p.n_tiles_n = c.g.ntn;
+  return p;
 }
 
 void ozaki_release_cache() {
@@ -549,12 +605,20 @@ std::unique_ptr<XOperator> make_ozaki_sym_operator(const double* K, int n, int s
   return std::unique_ptr<XOperator>(new XOperatorOzakiSym(K, n, slices));
 }
 
+OzakiPartials ozaki_sym_times_partials(XOperator& op, const double* M, int F) {
+  auto* oz = dynamic_cast<XOperatorOzakiSym*>(&op);
+  FPLS_REQUIRE(oz != nullptr, "INT8 partial products need the INT8 operator");
+  return oz->times_partials(M, F);
+}
+
 int ozaki_default_slices() {
   if (const char* e = std::getenv("FASTPLS_OZAKI_SLICES")) {
     const int v = std::atoi(e);
     if (v >= kOzakiMinSlices && v <= kOzakiMaxSlices) return v;
   }
-  return 7;
+  // 2^-42 of the row scales: on the omics double-CV grid 5, 6 and 7 slices
+  // give the same predictions as FP64 products and 4 do not; 6 keeps a margin.
+  return 6;
 }
 
 }  // namespace fpls

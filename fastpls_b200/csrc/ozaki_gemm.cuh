@@ -38,6 +38,18 @@ void ozaki_split(const double* X, int ldx, const OzakiPlanes& out);
 // exact product by at most about 3 k 2^(eA_i + eB_j - 7 slices) per entry.
 void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc);
 
+// The same product left as FP64 stream-K partials for a consumer that sums
+// them (in segment order) while it reads C: entry (i, j) of C is
+//   sum_{s = tile_seg[t] .. tile_seg[t+1]-1} part[(s * 64 + j % 64) * 128 + i % 128],
+// t = (i / 128) * n_tiles_n + j / 64.  The buffers belong to the cached plan
+// of this shape and are overwritten by the next product of the same shape.
+struct OzakiPartials {
+  const double* part = nullptr;
+  const int* tile_seg = nullptr;
+  int n_tiles_n = 0;
+};
+OzakiPartials ozaki_gemm_partials(const OzakiPlanes& A, const OzakiPlanes& B);
+
 // Releases the cached stream-K plans (fpls_reset_workspace).
 void ozaki_release_cache();
 
@@ -45,9 +57,11 @@ void ozaki_release_cache();
 // times() and t_times() are K * M through the INT8 tensor cores; gram() is not
 // provided.
 std::unique_ptr<XOperator> make_ozaki_sym_operator(const double* K, int n, int slices);
+// K * M (n x F) of an operator made by make_ozaki_sym_operator, as partials.
+OzakiPartials ozaki_sym_times_partials(XOperator& op, const double* M, int F);
 
 // Slice count of the mixed-precision row-space products (environment
-// FASTPLS_OZAKI_SLICES, else 7).
+// FASTPLS_OZAKI_SLICES, else 6).
 int ozaki_default_slices();
 
 }  // namespace fpls

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <string>
 
 #include "blas_f64.cuh"
 #include "context.cuh"
@@ -41,6 +42,12 @@ struct DualEng {
   const double* kpart;
   const int* kseg;
   int kntn;
+  // Digit planes of cp written by the step (when cpd is set): plane sl, row f
+  // at cpd + sl * cpstride + f * cpldk, scale 2^e in cps[f].
+  int8_t* cpd;
+  double* cps;
+  int cpldk, cpS;
+  size_t cpstride;
   double* scal;  // F x 2   ||t||, sum(t)
   double* qs;    // F x m   Y^T t
   double* Q;
@@ -50,95 +57,7 @@ struct DualEng {
   int* status;
 };
 
-// Each fit is handled by a cluster of kCl CTAs; CTA r of the cluster owns rows
-// [r * rows_per, (r + 1) * rows_per) of every n-vector of the fit and keeps
-// them in registers (kLR rows per thread).  Reductions over the n rows are
-// per-CTA (warp shuffles, shared memory) and then across the cluster through
-// distributed shared memory, summed in rank order so every CTA of the cluster
-// sees bit-identical results and takes the same branches.
-constexpr int kCl = 4;
-constexpr int kT = 256;
-constexpr int kW = kT / 32;
-constexpr int kLR = kMaxN / kCl / kT;     // 8 rows per thread
-constexpr int kRedMax = kMaxK > kMaxM + 2 ? kMaxK : kMaxM + 2;
-
-struct ClusterRed {
-  double warp[kW][kRedMax];
-  double part[2][kRedMax];
-  double res[kRedMax];
-  int buf;
-};
-
-struct Rows {
-  int r0, nl;  // first owned row, owned row count
-  __device__ __forceinline__ bool ok(int k) const { return (int)threadIdx.x + k * kT < nl; }
-  __device__ __forceinline__ int row(int k) const { return r0 + (int)threadIdx.x + k * kT; }
-};
-
-// part[buf][0..count) holds this CTA's partials (after a barrier): sum them
-// over the cluster into res[0..count); ends with res visible to the CTA.
-__device__ void cluster_exchange(ClusterRed& R, int count) {
-  cg::cluster_group cl = cg::this_cluster();
-  const int b = R.buf;
-  cl.sync();
-  for (int k = threadIdx.x; k < count; k += kT) {
-    double s = 0.0;
-    for (int r = 0; r < kCl; ++r) s += cl.map_shared_rank(&R.part[b][0], r)[k];
-    R.res[k] = s;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) R.buf = b ^ 1;
-  __syncthreads();
-}
-
-// res[0..count) = cluster sums of the per-thread values v[0..count) (count <= 4).
-__device__ void cluster_sum(ClusterRed& R, double (&v)[4], int count) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int k = 0; k < count; ++k) {
-    const double w = warp_sum(v[k]);
-    if (lane == 0) R.warp[warp][k] = w;
-  }
-  __syncthreads();
-  if (threadIdx.x < count) {
-    double s = 0.0;
-    for (int w = 0; w < kW; ++w) s += R.warp[w][threadIdx.x];
-    R.part[R.buf][threadIdx.x] = s;
-  }
-  __syncthreads();
-  cluster_exchange(R, count);
-}
-
-// res[j] = sum over the fit's rows of M[i + j*n] * x_i for j < ncols, with x
-// given by the owned rows in registers.
-__device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M, int n, int ncols, const Rows& rw,
-                             const double (&x)[kLR]) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // four columns per pass: their loads are independent and issued together
-  for (int j0 = 0; j0 < ncols; j0 += 4) {
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      if (j0 + jj >= ncols) break;
-      const double* col = M + (size_t)(j0 + jj) * n;
-#pragma unroll
-      for (int k = 0; k < kLR; ++k)
-        if (rw.ok(k)) acc[jj] += col[rw.row(k)] * x[k];
-    }
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      const double w = warp_sum(acc[jj]);
-      if (lane == 0 && j0 + jj < ncols) R.warp[warp][j0 + jj] = w;
-    }
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < ncols; j += kT) {
-    double s = 0.0;
-    for (int w = 0; w < kW; ++w) s += R.warp[w][j];
-    R.part[R.buf][j] = s;
-  }
-  __syncthreads();
-  cluster_exchange(R, ncols);
-}
+constexpr int kRedMax = kMaxK > kMaxM + 3 ? kMaxK : kMaxM + 3;
 
 // C_S of every fit: mask_f * (onehot(label) - (mY_all + dY_f)).
 __global__ void k_dual_cs0(DualEng e) {
@@ -156,11 +75,126 @@ __global__ void k_dual_cs0(DualEng e) {
   }
 }
 
+// Each fit is handled by CL CTAs of T threads (a thread-block cluster when
+// CL > 1); CTA r owns rows [r * rows_per, (r + 1) * rows_per) of every
+// n-vector of the fit and keeps them in registers (LR rows per thread, so
+// n <= CL * T * LR).  Reductions over the n rows are per-CTA (warp shuffles,
+// shared memory) and then across the cluster through distributed shared
+// memory, summed in rank order so every CTA of the cluster sees bit-identical
+// results and takes the same branches.  With CL = 1 a fit lives in one CTA and
+// every reduction ends at a block barrier.
+template <int CL, int T, int LR>
+struct Step {
+static constexpr int kCl = CL;
+static constexpr int kT = T;
+static constexpr int kW = T / 32;
+static constexpr int kLR = LR;
+
+
+static constexpr int kDotChunk = 64;   // columns of one pass of per-warp dot partials
+static constexpr int kDotCols = LR <= 4 ? 8 : 4;   // columns whose loads are in flight together
+static constexpr int kColUnroll = LR <= 4 ? 8 : 4;
+struct ClusterRed {
+  double warp[kW][kDotChunk];
+  double part[2][kRedMax];           // this CTA's partials (alternating between exchanges)
+  double res[kRedMax];
+  int buf;
+};
+
+struct Rows {
+  int r0, nl;  // first owned row, owned row count
+  __device__ __forceinline__ bool ok(int k) const { return (int)threadIdx.x + k * kT < nl; }
+  __device__ __forceinline__ int row(int k) const { return r0 + (int)threadIdx.x + k * kT; }
+};
+
+// part[buf][0..count) holds this CTA's partials (after a barrier): combine
+// them over the cluster into res[0..count) (sums, or maxima for k >=
+// max_from), in rank order; ends with res visible to the CTA.  A peer reads
+// part[buf] after the cluster barrier, so the next exchange writes the other
+// buffer.
+static __device__ void cluster_exchange(ClusterRed& R, int count, int max_from = kRedMax) {
+  const int b = R.buf;
+  if constexpr (CL == 1) {
+    for (int k = threadIdx.x; k < count; k += kT) R.res[k] = R.part[b][k];
+    __syncthreads();
+  } else {
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    for (int k = threadIdx.x; k < count; k += kT) {
+      double v = cl.map_shared_rank(&R.part[b][0], 0)[k];
+      if (k >= max_from) {
+        for (int r = 1; r < kCl; ++r) v = fmax(v, cl.map_shared_rank(&R.part[b][0], r)[k]);
+      } else {
+        for (int r = 1; r < kCl; ++r) v += cl.map_shared_rank(&R.part[b][0], r)[k];
+      }
+      R.res[k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) R.buf = b ^ 1;
+    __syncthreads();
+  }
+}
+
+// res[0..count) = cluster sums of the per-thread values v[0..count) (count <= 4).
+static __device__ void cluster_sum(ClusterRed& R, double (&v)[4], int count) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int k = 0; k < count; ++k) {
+    const double w = warp_sum(v[k]);
+    if (lane == 0) R.warp[warp][k] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x < count) {
+    double s = 0.0;
+    for (int w = 0; w < kW; ++w) s += R.warp[w][threadIdx.x];
+    R.part[R.buf][threadIdx.x] = s;
+  }
+  __syncthreads();
+  cluster_exchange(R, count);
+}
+
+// res[j] = sum over the fit's rows of M[i + j*n] * x_i for j < ncols, with x
+// given by the owned rows in registers.
+static __device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M, int n, int ncols, const Rows& rw,
+                                    const double (&x)[kLR]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c0 = 0; c0 < ncols; c0 += kDotChunk) {
+    const int cn = min(kDotChunk, ncols - c0);
+    // kDotCols columns per pass, loads issued together (no data-dependent
+    // exit: a column past the end re-reads the last one and is discarded)
+    for (int j0 = 0; j0 < cn; j0 += kDotCols) {
+      double acc[kDotCols];
+#pragma unroll
+      for (int jj = 0; jj < kDotCols; ++jj) acc[jj] = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < kDotCols; ++jj) {
+        const int jc = min(j0 + jj, cn - 1);
+        const double* col = M + (size_t)(c0 + jc) * n;
+#pragma unroll
+        for (int k = 0; k < kLR; ++k)
+          if (rw.ok(k)) acc[jj] += col[rw.row(k)] * x[k];
+      }
+#pragma unroll
+      for (int jj = 0; jj < kDotCols; ++jj) {
+        const double w = warp_sum(acc[jj]);
+        if (lane == 0 && j0 + jj < cn) R.warp[warp][j0 + jj] = w;
+      }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < cn; j += kT) {
+      double s = 0.0;
+      for (int w = 0; w < kW; ++w) s += R.warp[w][j];
+      R.part[R.buf][c0 + j] = s;
+    }
+    __syncthreads();
+  }
+  cluster_exchange(R, ncols);
+}
+
 // Refresh (power iterations of S S^T from the sketch or the warm start),
 // Householder normalisation, scores t = X_f r, q = Y^T t, and the loading
 // coefficients c_p for the K product.
-__device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank) {
-  __shared__ double zloc[kMaxM + 2];
+static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank) {
+  __shared__ double zloc[kMaxM + 3];
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m;
   const double* CS = e.CS + (size_t)f * n * m;
@@ -201,15 +235,17 @@ __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, i
     }
     if (it + 1 < steps) cluster_dots(R, CS, n, m, rw, ky);
   }
-  // ||y||^2 = c_y^T K c_y and y[0] = Xc[:,0]^T c_y
+  // ||y||^2 = c_y^T K c_y, y[0] = Xc[:,0]^T c_y and the train-row sum of K c_y
+  // (the score mean, once the sign and norm are known)
   double s[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
   for (int k = 0; k < kLR; ++k)
     if (rw.ok(k)) {
       s[0] += cy[k] * ky[k];
       s[1] += e.x0[rw.row(k)] * cy[k];
+      if (mk[rw.row(k)]) s[2] += ky[k];
     }
-  cluster_sum(R, s, 2);
+  cluster_sum(R, s, 3);
   const double nrm = sqrt(R.res[0]);
   const double y0 = R.res[1];
   if (!(nrm > 0.0) || !isfinite(nrm)) {
@@ -219,17 +255,13 @@ __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, i
   const double sg = ((y0 >= 0.0) ? -1.0 : 1.0) / nrm;
   const double nf = static_cast<double>(e.ntrain[f]);
   // U = X r = sg * K c_y; its mean over the train rows centres the scores
-  double u[4] = {0.0, 0.0, 0.0, 0.0};
+  const double cmean = e.center ? sg * R.res[2] / nf : 0.0;
 #pragma unroll
-  for (int k = 0; k < kLR; ++k) {
-    ky[k] *= sg;
-    if (rw.ok(k) && mk[rw.row(k)]) u[0] += ky[k];
-  }
-  cluster_sum(R, u, 1);
-  const double cmean = e.center ? R.res[0] / nf : 0.0;
+  for (int k = 0; k < kLR; ++k) ky[k] *= sg;
   double* keep = e.Tkeep ? e.Tkeep + ((size_t)f * e.K + a) * n : nullptr;
-  for (int j = threadIdx.x; j < m + 2; j += kT) zloc[j] = 0.0;
+  for (int j = threadIdx.x; j < m + 3; j += kT) zloc[j] = 0.0;
   __syncthreads();
+  double umax = 0.0;   // largest |centred score| of the train rows
   double t2[2] = {0.0, 0.0};
   double t[kLR];
 #pragma unroll
@@ -243,32 +275,61 @@ __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, i
       t[k] = uc;
       t2[0] += uc * uc;
       t2[1] += uc;
+      umax = fmax(umax, fabs(uc));
       if (uc != 0.0) atomicAdd(&zloc[e.labels[i]], uc);
     }
   }
   {
     const double a0 = warp_sum(t2[0]), a1 = warp_sum(t2[1]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
     if ((threadIdx.x & 31) == 0) {
       atomicAdd(&zloc[m], a0);
       atomicAdd(&zloc[m + 1], a1);
+      // non-negative doubles order like their bit patterns
+      atomicMax(reinterpret_cast<unsigned long long*>(&zloc[m + 2]),
+                static_cast<unsigned long long>(__double_as_longlong(umax)));
     }
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < m + 2; j += kT) R.part[R.buf][j] = zloc[j];
+  for (int j = threadIdx.x; j < m + 3; j += kT) R.part[R.buf][j] = zloc[j];
   __syncthreads();
-  cluster_exchange(R, m + 2);
+  cluster_exchange(R, m + 3, m + 2);
   const double tn = sqrt(R.res[m]);
   const double st = R.res[m + 1];
   if (!(tn > 0.0) || !isfinite(tn)) {
     if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
     return false;
   }
+  // Digit planes of c_p for the INT8 K product: scale 2^ex above the bound
+  // (max |centred score| + |mean|) / ||t|| of every |c_p[i]|, then the signed
+  // 7-bit digits taken exactly (scale by 128, truncate, subtract).
+  double inv = 0.0;
+  if (e.cpd) {
+    const double bound = (R.res[m + 2] + (e.center ? fabs(st) / nf : 0.0)) / tn * (1.0 + 0x1p-30);
+    int ex = 0;
+    if (bound > 0.0) frexp(bound, &ex);
+    ex = max(-1000, min(1000, ex));
+    inv = __longlong_as_double(static_cast<long long>(1023 - ex) << 52);
+    if (rank == 0 && threadIdx.x == 0) e.cps[f] = __longlong_as_double(static_cast<long long>(1023 + ex) << 52);
+  }
 #pragma unroll
   for (int k = 0; k < kLR; ++k) {
     if (!rw.ok(k)) continue;
     const int i = rw.row(k);
-    e.cp[(size_t)f * n + i] = (t[k] - ((e.center && mk[i]) ? st / nf : 0.0)) / tn;
+    const double c = (t[k] - ((e.center && mk[i]) ? st / nf : 0.0)) / tn;
+    e.cp[(size_t)f * n + i] = c;
     e.Kcy[(size_t)f * n + i] = ky[k] / tn;
+    if (e.cpd) {
+      int8_t* d = e.cpd + (size_t)f * e.cpldk + i;
+      double x = c * inv;
+      for (int sl = 0; sl < e.cpS; ++sl) {
+        x *= 128.0;
+        const double dg = trunc(x);
+        x -= dg;
+        d[(size_t)sl * e.cpstride] = static_cast<int8_t>(static_cast<int>(dg));
+      }
+    }
   }
   if (rank == 0) {
     for (int j = threadIdx.x; j < m; j += kT) e.qs[(size_t)f * m + j] = R.res[j];
@@ -282,7 +343,7 @@ __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, i
 
 // Gram-Schmidt of the loading against the earlier ones in K-coordinates,
 // normalisation, rank-1 deflation of C_S and K C_S, and the component outputs.
-__device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank) {
+static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank) {
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m, K = e.K;
   double* CV = e.CV + (size_t)f * n * K;
@@ -309,7 +370,7 @@ __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, i
   }
   if (a > 0) {
     cluster_dots(R, CV, n, a, rw, kv);   // V^T p = C_V^T K c_p
-#pragma unroll 4
+#pragma unroll (kColUnroll)
     for (int l = 0; l < a; ++l) {
       const double wl = R.res[l];
       const double* vc = CV + (size_t)l * n;
@@ -341,6 +402,7 @@ __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, i
     }
   }
   cluster_dots(R, CS, n, m, rw, kv);     // S^T v = C_S^T K c_v
+#pragma unroll 4
   for (int j = 0; j < m; ++j) {
     const double vj = R.res[j];
     double* cs = CS + (size_t)j * n;
@@ -369,10 +431,11 @@ __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, i
 
 // One launch per component boundary: the Gram-Schmidt / deflation of
 // component a - 1 and then the refresh / scores of component a, per fit.
-__global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kT) k_dual_step(DualEng e, int a) {
+static __device__ void run(const DualEng& e, int a) {
   __shared__ ClusterRed R;
   const int f = blockIdx.x / kCl;
-  const int rank = static_cast<int>(cg::this_cluster().block_rank());
+  int rank = 0;
+  if constexpr (CL > 1) rank = static_cast<int>(cg::this_cluster().block_rank());
   if (e.status[f]) return;   // set only in earlier launches: uniform over the cluster, before any remote access
   if (threadIdx.x == 0) R.buf = 0;
   __syncthreads();
@@ -387,7 +450,13 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kT) k_dual_step(Du
   bool ok = true;
   if (a > 0) ok = dual_b(e, a - 1, R, rw, rank);
   if (ok && a < e.K) dual_a(e, a, R, rw, rank);
-  cg::this_cluster().sync();
+  if constexpr (CL > 1) cg::this_cluster().sync();
+}
+};  // struct Step
+
+template <int CL, int T, int LR>
+__global__ void __launch_bounds__(T) k_dual_step(DualEng e, int a) {
+  Step<CL, T, LR>::run(e, a);
 }
 
 __global__ void symmetrize_kernel(double* K, int n) {
@@ -409,6 +478,52 @@ void symmetrize(double* K, int n) {
   symmetrize_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(K, n); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
+
+namespace {
+
+template <int CL, int T, int LR>
+void launch_step_cfg(const DualEng& e, int a, int F, cudaStream_t st) {
+  if constexpr (CL == 1) {
+    k_dual_step<1, T, LR><<<F, T, 0, st>>>(e, a);
+  } else {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(F * CL);
+    lc.blockDim = dim3(T);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    FPLS_CUDA(cudaLaunchKernelEx(&lc, k_dual_step<CL, T, LR>, e, a));
+  }
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+// Step layouts (rows of a fit over a 4-CTA cluster): 512 threads with up to 2
+// rows each for n <= 4096, 256 threads with up to 8 rows each for n <= 8192.
+// On the 3000-row omics grid the 512-thread layout beat one CTA per fit
+// (768 threads), 2-CTA clusters, 8-CTA clusters and 1024-thread CTAs: the
+// step is bound by the loads each SM keeps in flight, and more CTAs per
+// cluster cost more in the cluster reductions than they add.
+enum StepLayout { kStepWide = 0, kStepDeep = 1 };
+
+int choose_step_layout(int n) {
+  if (const char* v = std::getenv("FASTPLS_DUAL_STEP"))
+    if (std::string(v) == "deep") return kStepDeep;
+  return n <= 4 * 512 * 2 ? kStepWide : kStepDeep;
+}
+
+void launch_step(int layout, const DualEng& e, int a, int F, cudaStream_t st) {
+  if (layout == kStepWide) launch_step_cfg<4, 512, 2>(e, a, F, st);
+  else launch_step_cfg<4, 256, 8>(e, a, F, st);
+}
+
+}  // namespace
 
 bool dual_engine_applies(int n, int p, int m, int K) {
   if (const char* e = std::getenv("FASTPLS_DUAL"))
@@ -438,11 +553,23 @@ void dual_simpls_run(const DualBatch& b) {
   e.scal = ar.alloc_n<double>(2 * F);
   e.qs = ar.alloc_n<double>(F * m);
   e.ntrain = b.ntrain;
+  OzakiPlanes cpP;
+  if (b.kop_int8_slices > 0) {
+    cpP = ozaki_alloc(b.F, b.n, b.kop_int8_slices);
+    dzero(cpP.data, (size_t)cpP.slices * cpP.rows_pad * cpP.ldk);
+    dzero(cpP.scale, (size_t)cpP.rows_pad * sizeof(double));
+    e.cpd = cpP.data;
+    e.cps = cpP.scale;
+    e.cpldk = cpP.ldk;
+    e.cpS = cpP.slices;
+    e.cpstride = (size_t)cpP.rows_pad * cpP.ldk;
+  }
   dzero(b.status, F * sizeof(int));
   dzero(b.ncomp_done, F * sizeof(int));
   dzero(b.Q, F * m * K * sizeof(double));
   dzero(b.tnorm, F * K * sizeof(double));
   cudaStream_t st = ctx.stream;
+  const int cfg = choose_step_layout(b.n);
   k_dual_cs0<<<2 * ctx.sm_count, 256, 0, st>>>(e); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   b.Kop->times(e.CS, static_cast<int>(F * m), e.KCS);   // K C_S for every fit
@@ -456,8 +583,7 @@ void dual_simpls_run(const DualBatch& b) {
     if (a > 0) words += (4.0 + 3.0 * (a - 1) + 5.0 * md) * nd;
     if (a < b.K) words += (5.0 + md + 2.0 * it * md + std::max(it - 1.0, 0.0) * md) * nd;
     const int slot = ctx.prof_begin("dual_step", st);
-    k_dual_step<<<b.F * kCl, kT, 0, st>>>(e, a); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
+    launch_step(cfg, e, a, b.F, st);
     ctx.prof_end(slot, st, Fd * (8.0 * words + (a < b.K ? 5.0 * nd : 0.0)), 0.0);
     pt.mark("per-fit steps");
     if (a == b.K) break;
@@ -467,7 +593,7 @@ void dual_simpls_run(const DualBatch& b) {
       // the stream-K partials as it reads K c_p.
       const double S = b.kop_int8_slices;
       const int ks = ctx.prof_begin("k_products_int8", st);
-      const OzakiPartials pp = ozaki_sym_times_partials(*b.Kop, e.cp, b.F);
+      const OzakiPartials pp = ozaki_sym_partials_from_planes(*b.Kop, cpP);
       e.kpart = pp.part;
       e.kseg = pp.tile_seg;
       e.kntn = pp.n_tiles_n;

@@ -605,6 +605,12 @@ std::unique_ptr<XOperator> make_ozaki_sym_operator(const double* K, int n, int s
   return std::unique_ptr<XOperator>(new XOperatorOzakiSym(K, n, slices));
 }
 
+OzakiPartials ozaki_sym_partials_from_planes(XOperator& op, const OzakiPlanes& b) {
+  auto* oz = dynamic_cast<XOperatorOzakiSym*>(&op);
+  FPLS_REQUIRE(oz != nullptr, "INT8 partial products need the INT8 operator");
+  return ozaki_gemm_partials(oz->kp, b);
+}
+
 OzakiPartials ozaki_sym_times_partials(XOperator& op, const double* M, int F) {
   auto* oz = dynamic_cast<XOperatorOzakiSym*>(&op);
   FPLS_REQUIRE(oz != nullptr, "INT8 partial products need the INT8 operator");

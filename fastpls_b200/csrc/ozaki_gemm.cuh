@@ -59,6 +59,8 @@ void ozaki_release_cache();
 std::unique_ptr<XOperator> make_ozaki_sym_operator(const double* K, int n, int slices);
 // K * M (n x F) of an operator made by make_ozaki_sym_operator, as partials.
 OzakiPartials ozaki_sym_times_partials(XOperator& op, const double* M, int F);
+// The same with the planes of M already made (rows = the F columns, k = n).
+OzakiPartials ozaki_sym_partials_from_planes(XOperator& op, const OzakiPlanes& b);
 
 // Slice count of the mixed-precision row-space products (environment
 // FASTPLS_OZAKI_SLICES, else 6).

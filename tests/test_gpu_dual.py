@@ -79,3 +79,25 @@ def test_uncentred_predictors_match_oracle(lib, wide, dual):
     ref = ocv.pls_cv_predict_compiled(d["X"].astype(np.float64), d["y"], fold, nc, d["n_classes"],
                                       scaling=3, seed=3)
     assert np.mean(np.asarray(got["class_pred"]) == np.asarray(ref["class_pred"])) >= 0.999
+
+
+def test_step_layouts_agree(lib):
+    # the 512-thread step layout (default for n <= 4096) against the 256-thread
+    # layout with 8 rows per thread (FP64, same folds and sketches)
+    d = synthetic.c4_omics(seed=12, n=500, p=1600, n_informative=20)
+    outer, inner = double_cv_folds(d["y"], d["groups"], 4, 3, seed=7)
+    nc = np.arange(1, 11)
+
+    def run(lay):
+        if lay:
+            os.environ["FASTPLS_DUAL_STEP"] = lay
+        try:
+            return lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], seed=2,
+                                 precision="fp64", return_inner=True)
+        finally:
+            os.environ.pop("FASTPLS_DUAL_STEP", None)
+
+    a, b = run(None), run("deep")
+    assert np.array_equal(a["best_comp"], b["best_comp"])
+    assert np.mean(a["inner_pred"] == b["inner_pred"]) >= 0.9999
+    assert np.nanmax(np.abs(a["inner_accuracy"] - b["inner_accuracy"])) <= 1e-3

@@ -27,6 +27,8 @@
 #include <map>
 #include <memory>
 #include <vector>
+#include <string>
+#include <cstdlib>
 
 #include "blas_f64.cuh"
 #include "context.cuh"
@@ -54,46 +56,49 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 constexpr int BM = 128;
-constexpr int BN = 64;
+constexpr int BN = 64;     // N tile of the general products
+constexpr int BN_SYM = 128;  // N tile of the symmetric (Gram) products
 constexpr int BK = 64;
 constexpr int A_TILE = BM * BK * 2;                 // 16 KB
-constexpr int B_TILE = BN * BK * 2;                 // 8 KB
 constexpr int BAR_BYTES = 256;
-// NP BF16 planes per operand: 2 (hi, lo: 48 KB stages, 4 deep) or 3 (hi, mid,
-// lo: 72 KB stages, 3 deep).
-template <int NP> struct Planes {
-  static constexpr int STAGES = NP == 2 ? 4 : 3;
-  static constexpr int STAGE_BYTES = NP * (A_TILE + B_TILE);
+// NP BF16 planes per operand, TN columns per output tile.  TN = 64: 48 KB
+// (two planes) or 72 KB (three) stages, 4 or 3 deep; TN = 128: 64 KB or 96 KB
+// stages, 3 or 2 deep.
+template <int NP, int TN> struct Planes {
+  static constexpr int B_BYTES = TN * BK * 2;
+  static constexpr int STAGES = TN == 64 ? (NP == 2 ? 4 : 3) : (NP == 2 ? 3 : 2);
+  static constexpr int STAGE_BYTES = NP * (A_TILE + B_BYTES);
   static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
+  static constexpr int TMEM_COLS = 2 * TN;
+  // Instruction descriptor: D F32, A/B BF16, both K-major, N = TN, M = 128.
+  static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) |
+                                    (uint32_t(TN >> 3) << 17) | (uint32_t(BM >> 4) << 24);
 };
-static_assert(Planes<3>::SMEM_BYTES <= 227 * 1024, "three-plane stages exceed shared memory");
+static_assert(Planes<3, 64>::SMEM_BYTES <= 227 * 1024, "three-plane stages exceed shared memory");
+static_assert(Planes<2, 128>::SMEM_BYTES <= 227 * 1024, "wide-tile stages exceed shared memory");
 constexpr int NUM_THREADS = 192;
-constexpr int TMEM_COLS = 2 * BN;
 
-// Instruction descriptor: D F32, A/B BF16, both K-major, N = 64, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
-                            (uint32_t(BN >> 3) << 17) | (uint32_t(BM >> 4) << 24);
-
-
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                           uint32_t accumulate) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
 
 
-template <int NP>
+template <int NP, int TN>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
 split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
                   const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
                   const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2,
                   const int4* __restrict__ segs, const int* __restrict__ cta_seg_begin,
                   int n_tiles_n, float* __restrict__ part, int* err) {
-  constexpr int STAGES = Planes<NP>::STAGES;
-  constexpr int STAGE_BYTES = Planes<NP>::STAGE_BYTES;
+  using P = Planes<NP, TN>;
+  constexpr int STAGES = P::STAGES;
+  constexpr int STAGE_BYTES = P::STAGE_BYTES;
+  constexpr int B_T = P::B_BYTES;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~static_cast<uintptr_t>(1023));
@@ -121,7 +126,7 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(TMEM_COLS)
+                 "r"(P::TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -156,9 +161,9 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant
         tma_load_2d(&mA0, smem_u32(st), fb, kb * BK, mt * BM);
         tma_load_2d(&mA1, smem_u32(st + A_TILE), fb, kb * BK, mt * BM);
         if (NP == 3) tma_load_2d(&mA2, smem_u32(st + 2 * A_TILE), fb, kb * BK, mt * BM);
-        tma_load_2d(&mB0, smem_u32(st + NP * A_TILE), fb, kb * BK, nt * BN);
-        tma_load_2d(&mB1, smem_u32(st + NP * A_TILE + B_TILE), fb, kb * BK, nt * BN);
-        if (NP == 3) tma_load_2d(&mB2, smem_u32(st + NP * A_TILE + 2 * B_TILE), fb, kb * BK, nt * BN);
+        tma_load_2d(&mB0, smem_u32(st + NP * A_TILE), fb, kb * BK, nt * TN);
+        tma_load_2d(&mB1, smem_u32(st + NP * A_TILE + B_T), fb, kb * BK, nt * TN);
+        if (NP == 3) tma_load_2d(&mB2, smem_u32(st + NP * A_TILE + 2 * B_T), fb, kb * BK, nt * TN);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -171,7 +176,7 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant
       const uint32_t jph = (j >> 1) & 1;
       if (!mbar_wait(smem_u32(&tempty[b]), jph ^ 1, err)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t acc = tmem + static_cast<uint32_t>(b * BN);
+      const uint32_t acc = tmem + static_cast<uint32_t>(b * TN);
       for (int kb = seg.y; kb < seg.z; ++kb, ++it) {
         const int s = it % STAGES;
         const uint32_t ph = (it / STAGES) & 1;
@@ -183,17 +188,17 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant
         for (int k = 0; k < BK / 16; ++k) {
           const uint32_t off = k * 32;  // 16 BF16 = 32 bytes along K inside the swizzle atom
           const uint64_t da0 = sw128_desc(a0 + off), da1 = sw128_desc(a0 + A_TILE + off);
-          const uint64_t db0 = sw128_desc(b0 + off), db1 = sw128_desc(b0 + B_TILE + off);
+          const uint64_t db0 = sw128_desc(b0 + off), db1 = sw128_desc(b0 + B_T + off);
           // products down to 2^-16 (two planes) or 2^-24 (three planes) of hi*hi
-          umma_bf16(acc, da0, db0, (kb > seg.y || k > 0) ? 1u : 0u);
-          umma_bf16(acc, da0, db1, 1u);
-          umma_bf16(acc, da1, db0, 1u);
+          umma_bf16(acc, da0, db0, P::IDESC, (kb > seg.y || k > 0) ? 1u : 0u);
+          umma_bf16(acc, da0, db1, P::IDESC, 1u);
+          umma_bf16(acc, da1, db0, P::IDESC, 1u);
           if (NP == 3) {
             const uint64_t da2 = sw128_desc(a0 + 2 * A_TILE + off);
-            const uint64_t db2 = sw128_desc(b0 + 2 * B_TILE + off);
-            umma_bf16(acc, da0, db2, 1u);
-            umma_bf16(acc, da2, db0, 1u);
-            umma_bf16(acc, da1, db1, 1u);
+            const uint64_t db2 = sw128_desc(b0 + 2 * B_T + off);
+            umma_bf16(acc, da0, db2, P::IDESC, 1u);
+            umma_bf16(acc, da2, db0, P::IDESC, 1u);
+            umma_bf16(acc, da1, db1, P::IDESC, 1u);
           }
         }
         umma_commit(smem_u32(&empty[s]));
@@ -209,24 +214,24 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant
       const uint32_t jph = (j >> 1) & 1;
       const bool ok = mbar_wait(smem_u32(&tfull[b]), jph, err);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      float v[BN];
-      const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(b * BN);
+      float v[TN];
+      const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(b * TN);
 #pragma unroll
-      for (int c = 0; c < BN / 16; ++c) tmem_ld16(base + c * 16, v + c * 16);
+      for (int c = 0; c < TN / 16; ++c) tmem_ld16(base + c * 16, v + c * 16);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(smem_u32(&tempty[b]));
       if (!ok) break;
-      float* dst = part + static_cast<size_t>(sg) * BN * BM + q * 32 + lane;
+      float* dst = part + static_cast<size_t>(sg) * TN * BM + q * 32 + lane;
 #pragma unroll
-      for (int c = 0; c < BN; ++c) dst[static_cast<size_t>(c) * BM] = v[c];
+      for (int c = 0; c < TN; ++c) dst[static_cast<size_t>(c) * BM] = v[c];
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P::TMEM_COLS)
                  : "memory");
   }
 }
@@ -234,9 +239,11 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant
 // C[m + n*ldc] = alpha * sum_{segments of the tile} part + beta * C   (FP64)
 constexpr int kReduceSplit = 8;
 
+template <int TN>
 __global__ void split_reduce_kernel(const float* __restrict__ part, const int* __restrict__ tile_seg,
                                     int n_tiles_n, int M, int N, double alpha, double beta,
                                     double* __restrict__ C, int ldc) {
+  constexpr int BN = TN;
   // kReduceSplit blocks per tile, each covering BN / kReduceSplit columns.
   const int tile = blockIdx.x / kReduceSplit;
   const int part_idx = blockIdx.x % kReduceSplit;
@@ -372,6 +379,7 @@ SplitPair alloc_pair(int rows, int k, int np = 2) {
 // of the (tile, K block) space, cut into per-tile segments.
 struct GemmPlan {
   int tiles = 0, ntn = 0, ctas = 0;
+  int bn = BN;   // output tile width (64, or 128 for symmetric products)
   std::vector<int4> segs;
   std::vector<int> cta_begin, tile_begin;
 };
@@ -384,15 +392,17 @@ constexpr int kSymSegBlocks = 16;
 constexpr int kMixedMinK = 256;
 constexpr double kMixedMinWork = 1e7;
 
-GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false, bool short_segments = false) {
+GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false, bool short_segments = false,
+                   int bn = BN) {
   GemmPlan g;
+  g.bn = bn;
   const int mt = (M + BM - 1) / BM;
-  g.ntn = (N + BN - 1) / BN;
+  g.ntn = (N + bn - 1) / bn;
   g.tiles = mt * g.ntn;
   std::vector<int> inc;
   inc.reserve(g.tiles);
   for (int t = 0; t < g.tiles; ++t)
-    if (!upper || (t / g.ntn) * BM < ((t % g.ntn) + 1) * BN) inc.push_back(t);
+    if (!upper || (t / g.ntn) * BM < ((t % g.ntn) + 1) * bn) inc.push_back(t);
   const int kbt = (K + BK - 1) / BK;
   // A symmetric (Gram) product sums the whole contraction of each tile in one
   // CTA; cutting it (and every three-plane product) into segments of at most
@@ -446,7 +456,7 @@ struct GemmScratch {
 size_t gemm_scratch_bytes(const GemmPlan& g) {
   auto up = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
   return up(g.segs.size() * sizeof(int4)) + up(g.cta_begin.size() * sizeof(int)) +
-         up(g.tile_begin.size() * sizeof(int)) + up(g.segs.size() * static_cast<size_t>(BM) * BN * sizeof(float));
+         up(g.tile_begin.size() * sizeof(int)) + up(g.segs.size() * static_cast<size_t>(BM) * g.bn * sizeof(float));
 }
 
 GemmScratch carve_gemm_scratch(const GemmPlan& g, char* base) {
@@ -462,14 +472,22 @@ GemmScratch carve_gemm_scratch(const GemmPlan& g, char* base) {
   return s;
 }
 
-template <int NP>
+template <int NP, int TN>
 void ensure_smem_attr() {
   static bool attr = false;
   if (!attr) {
-    FPLS_CUDA(cudaFuncSetAttribute(split_gemm_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   Planes<NP>::SMEM_BYTES));
+    FPLS_CUDA(cudaFuncSetAttribute(split_gemm_kernel<NP, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Planes<NP, TN>::SMEM_BYTES));
     attr = true;
   }
+}
+
+template <int NP, int TN>
+void launch_split_kernel(const CUtensorMap (&m)[6], const GemmPlan& g, const GemmScratch& s, int* err,
+                         cudaStream_t st) {
+  ensure_smem_attr<NP, TN>();
+  split_gemm_kernel<NP, TN><<<g.ctas, NUM_THREADS, Planes<NP, TN>::SMEM_BYTES, st>>>(
+      m[0], m[1], m[2], m[3], m[4], m[5], s.segs, s.cta_begin, g.ntn, s.part, err);
 }
 
 // C (M x N) = alpha * A B^T + beta C on stream `st` with the given scratch; no allocation.
@@ -484,27 +502,22 @@ void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K,
                     double beta, double* C, int ldc, const GemmPlan& g, const GemmScratch& s,
                     int* err, cudaStream_t st, Context* prof) {
   FPLS_REQUIRE(A.np == B.np && (A.np == 2 || A.np == 3), "split GEMM: operands with different plane counts");
-  const CUtensorMap mA0 = make_map(A.hi, M, K, A.ld, BM);
-  const CUtensorMap mA1 = make_map(A.np == 3 ? A.mid : A.lo, M, K, A.ld, BM);
-  const CUtensorMap mA2 = make_map(A.lo, M, K, A.ld, BM);
-  const CUtensorMap mB0 = make_map(B.hi, N, K, B.ld, BN);
-  const CUtensorMap mB1 = make_map(B.np == 3 ? B.mid : B.lo, N, K, B.ld, BN);
-  const CUtensorMap mB2 = make_map(B.lo, N, K, B.ld, BN);
+  FPLS_REQUIRE(g.bn == BN || (g.bn == BN_SYM && A.np == 2), "split GEMM: unsupported tile width");
+  const CUtensorMap maps[6] = {make_map(A.hi, M, K, A.ld, BM),
+                               make_map(A.np == 3 ? A.mid : A.lo, M, K, A.ld, BM),
+                               make_map(A.lo, M, K, A.ld, BM),
+                               make_map(B.hi, N, K, B.ld, g.bn),
+                               make_map(B.np == 3 ? B.mid : B.lo, N, K, B.ld, g.bn),
+                               make_map(B.lo, N, K, B.ld, g.bn)};
   const bool upper_plan = g.tiles > 0 && static_cast<int>(g.tile_begin.size()) == g.tiles + 1 &&
                           g.tile_begin[g.tiles] > 0 && upper_hint(g);
   const int slot = prof ? prof->prof_begin(upper_plan ? (A.np == 3 ? "gram_bf16x6" : "gram_bf16x3")
                                                       : (A.np == 3 ? "split_gemm_bf16x6" : "split_gemm_bf16x3"),
                                            st)
                         : -1;
-  if (A.np == 3) {
-    ensure_smem_attr<3>();
-    split_gemm_kernel<3><<<g.ctas, NUM_THREADS, Planes<3>::SMEM_BYTES, st>>>(mA0, mA1, mA2, mB0, mB1, mB2, s.segs,
-                                                                           s.cta_begin, g.ntn, s.part, err);
-  } else {
-    ensure_smem_attr<2>();
-    split_gemm_kernel<2><<<g.ctas, NUM_THREADS, Planes<2>::SMEM_BYTES, st>>>(mA0, mA1, mA2, mB0, mB1, mB2, s.segs,
-                                                                           s.cta_begin, g.ntn, s.part, err);
-  }
+  if (A.np == 3) launch_split_kernel<3, BN>(maps, g, s, err, st);
+  else if (g.bn == BN_SYM) launch_split_kernel<2, BN_SYM>(maps, g, s, err, st);
+  else launch_split_kernel<2, BN>(maps, g, s, err, st);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   if (prof) {
@@ -517,7 +530,11 @@ void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K,
                        8.0 * static_cast<double>(M) * N * tiles_frac,
                    products * 2.0 * static_cast<double>(M) * N * K * tiles_frac);
   }
-  split_reduce_kernel<<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, g.ntn, M, N, alpha, beta, C, ldc); ::fpls::note_launch();
+  if (g.bn == BN_SYM)
+    split_reduce_kernel<BN_SYM><<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, g.ntn, M, N, alpha, beta, C, ldc);
+  else
+    split_reduce_kernel<BN><<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, g.ntn, M, N, alpha, beta, C, ldc);
+  ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -529,29 +546,38 @@ struct CachedPlan {
   char* dev = nullptr;
   GemmScratch s;
 };
-std::map<std::array<int, 6>, CachedPlan>& plan_cache() {
-  static std::map<std::array<int, 6>, CachedPlan> cache;
+std::map<std::array<int, 7>, CachedPlan>& plan_cache() {
+  static std::map<std::array<int, 7>, CachedPlan> cache;
   return cache;
 }
 
 const CachedPlan& cached_plan(int M, int N, int K, int sm_count, cudaStream_t st, bool upper = false,
-                              bool short_segments = false) {
+                              bool short_segments = false, int bn = BN) {
   auto& cache = plan_cache();
-  const std::array<int, 6> key{M, N, K, sm_count, upper ? 1 : 0, short_segments ? 1 : 0};
+  const std::array<int, 7> key{M, N, K, sm_count, upper ? 1 : 0, short_segments ? 1 : 0, bn};
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
   CachedPlan c;
-  c.g = plan_gemm(M, N, K, sm_count, upper, short_segments);
+  c.g = plan_gemm(M, N, K, sm_count, upper, short_segments, bn);
   FPLS_CUDA(cudaMalloc(&c.dev, gemm_scratch_bytes(c.g)));
   c.s = carve_gemm_scratch(c.g, c.dev);
   upload_plan_tables(c.g, c.s, st);
   return cache.emplace(key, std::move(c)).first->second;
 }
 
+bool sym_wide_tiles() {
+  const char* e = std::getenv("FASTPLS_GRAM_TILE");
+  return !(e && std::string(e) == "64");
+}
+
 void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,
                 double beta, double* C, int ldc, bool upper = false) {
   Context& ctx = Context::get();
-  const CachedPlan& c = cached_plan(M, N, K, ctx.sm_count, ctx.stream, upper, A.np == 3);
+  // Symmetric two-plane products (the row Gram) on 128 x 128 tiles: half the
+  // B re-reads of the 128 x 64 tiles and twice the MACs per operand byte read
+  // by the tensor core.
+  const int bn = (upper && A.np == 2 && sym_wide_tiles()) ? BN_SYM : BN;
+  const CachedPlan& c = cached_plan(M, N, K, ctx.sm_count, ctx.stream, upper, A.np == 3, bn);
   split_gemm_run(A, B, M, N, K, alpha, beta, C, ldc, c.g, c.s, ctx.d_status + 16, ctx.stream,
                  ctx.profile ? &ctx : nullptr);
 }

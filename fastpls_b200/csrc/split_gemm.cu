@@ -239,10 +239,12 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant
 // C[m + n*ldc] = alpha * sum_{segments of the tile} part + beta * C   (FP64)
 constexpr int kReduceSplit = 8;
 
+// tile_segs (when not null) lists each tile's segment ids in contraction
+// order; otherwise a tile's segments are the consecutive ids s0 .. s1 - 1.
 template <int TN>
 __global__ void split_reduce_kernel(const float* __restrict__ part, const int* __restrict__ tile_seg,
-                                    int n_tiles_n, int M, int N, double alpha, double beta,
-                                    double* __restrict__ C, int ldc) {
+                                    const int* __restrict__ tile_segs, int n_tiles_n, int M, int N,
+                                    double alpha, double beta, double* __restrict__ C, int ldc) {
   constexpr int BN = TN;
   // kReduceSplit blocks per tile, each covering BN / kReduceSplit columns.
   const int tile = blockIdx.x / kReduceSplit;
@@ -255,7 +257,10 @@ __global__ void split_reduce_kernel(const float* __restrict__ part, const int* _
     const int m = mt * BM + mm, n = nt * BN + nn;
     if (m >= M || n >= N) continue;
     double acc = 0.0;
-    for (int s = s0; s < s1; ++s) acc += static_cast<double>(part[(static_cast<size_t>(s) * BN + nn) * BM + mm]);
+    for (int j = s0; j < s1; ++j) {
+      const int s = tile_segs ? tile_segs[j] : j;
+      acc += static_cast<double>(part[(static_cast<size_t>(s) * BN + nn) * BM + mm]);
+    }
     double* cp = C + m + static_cast<size_t>(n) * ldc;
     *cp = (beta == 0.0) ? alpha * acc : alpha * acc + beta * *cp;
   }
@@ -382,12 +387,16 @@ struct GemmPlan {
   int bn = BN;   // output tile width (64, or 128 for symmetric products)
   std::vector<int4> segs;
   std::vector<int> cta_begin, tile_begin;
+  // Segment ids of each tile (tile t: tile_segs[tile_begin[t] .. tile_begin[t+1])),
+  // in contraction order; empty when the segments are already grouped by tile.
+  std::vector<int> tile_segs;
 };
 
 // Stream-K plan over the output tiles.  With `upper` only the tiles that
 // reach the upper triangle (tile row start < tile column end) are planned, for
 // symmetric products whose lower triangle is mirrored afterwards.
 constexpr int kSymSegBlocks = 16;
+constexpr int kSymChunkBlocks = 64;   // K-blocks per chunk of a symmetric plan (a multiple of kSymSegBlocks)
 // Products that take the split path in the mixed precision mode.
 constexpr int kMixedMinK = 256;
 constexpr double kMixedMinWork = 1e7;
@@ -413,25 +422,52 @@ GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false, bool s
   g.ctas = static_cast<int>(std::max<long long>(1, std::min<long long>(sm_count, total)));
   g.cta_begin.assign(g.ctas + 1, 0);
   g.tile_begin.assign(g.tiles + 1, 0);
+  // A symmetric plan walks the contraction in chunks of kSymChunkBlocks
+  // K-blocks and gives every CTA an equal share of each chunk, chunk after
+  // chunk, so that the CTAs running at the same time read the same K-panel of
+  // both operands (it stays in L2) instead of the whole operands.
+  const int kc = upper ? kSymChunkBlocks : kbt;
+  const int nchunks = (kbt + kc - 1) / kc;
+  const long long ninc = static_cast<long long>(inc.size());
   for (int c = 0; c < g.ctas; ++c) {
     g.cta_begin[c] = static_cast<int>(g.segs.size());
-    long long a = total * c / g.ctas, e = total * (c + 1) / g.ctas;
-    while (a < e) {
-      const int t = inc[static_cast<size_t>(a / kbt)];
-      const int kb0 = static_cast<int>(a % kbt);
-      int kb1 = static_cast<int>(std::min<long long>(kbt, kb0 + (e - a)));
-      kb1 = std::min(kb1, (kb0 / kseg + 1) * kseg);
-      g.segs.push_back(make_int4(t, kb0, kb1, 0));
-      a += kb1 - kb0;
+    for (int q = 0; q < nchunks; ++q) {
+      const int w = std::min(kc, kbt - q * kc);
+      const long long tq = ninc * w;   // (tile, K block) pairs of chunk q
+      long long a = tq * c / g.ctas, e = tq * (c + 1) / g.ctas;
+      while (a < e) {
+        const int t = inc[static_cast<size_t>(a / w)];
+        const int kb0 = q * kc + static_cast<int>(a % w);
+        int kb1 = static_cast<int>(std::min<long long>(q * kc + w, kb0 + (e - a)));
+        kb1 = std::min(kb1, (kb0 / kseg + 1) * kseg);
+        g.segs.push_back(make_int4(t, kb0, kb1, 0));
+        a += kb1 - kb0;
+      }
     }
   }
   g.cta_begin[g.ctas] = static_cast<int>(g.segs.size());
-  int s = 0;
-  for (int t = 0; t < g.tiles; ++t) {
-    g.tile_begin[t] = s;
-    while (s < static_cast<int>(g.segs.size()) && g.segs[s].x == t) ++s;
+  if (kc == kbt) {
+    int s = 0;
+    for (int t = 0; t < g.tiles; ++t) {
+      g.tile_begin[t] = s;
+      while (s < static_cast<int>(g.segs.size()) && g.segs[s].x == t) ++s;
+    }
+    g.tile_begin[g.tiles] = s;
+  } else {
+    // group the segment ids by tile, each tile's in contraction order
+    std::vector<int> ids(g.segs.size());
+    for (size_t i = 0; i < ids.size(); ++i) ids[i] = static_cast<int>(i);
+    std::stable_sort(ids.begin(), ids.end(), [&](int x, int y) {
+      return g.segs[x].x != g.segs[y].x ? g.segs[x].x < g.segs[y].x : g.segs[x].y < g.segs[y].y;
+    });
+    g.tile_segs = ids;
+    int s = 0;
+    for (int t = 0; t < g.tiles; ++t) {
+      g.tile_begin[t] = s;
+      while (s < static_cast<int>(ids.size()) && g.segs[ids[s]].x == t) ++s;
+    }
+    g.tile_begin[g.tiles] = s;
   }
-  g.tile_begin[g.tiles] = s;
   return g;
 }
 
@@ -450,13 +486,15 @@ struct GemmScratch {
   int4* segs = nullptr;
   int* cta_begin = nullptr;
   int* tile_begin = nullptr;
+  int* tile_segs = nullptr;   // null when the plan has no per-tile segment list
   float* part = nullptr;
 };
 
 size_t gemm_scratch_bytes(const GemmPlan& g) {
   auto up = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
   return up(g.segs.size() * sizeof(int4)) + up(g.cta_begin.size() * sizeof(int)) +
-         up(g.tile_begin.size() * sizeof(int)) + up(g.segs.size() * static_cast<size_t>(BM) * g.bn * sizeof(float));
+         up(g.tile_begin.size() * sizeof(int)) + up(g.tile_segs.size() * sizeof(int)) +
+         up(g.segs.size() * static_cast<size_t>(BM) * g.bn * sizeof(float));
 }
 
 GemmScratch carve_gemm_scratch(const GemmPlan& g, char* base) {
@@ -468,6 +506,10 @@ GemmScratch carve_gemm_scratch(const GemmPlan& g, char* base) {
   base += up(g.cta_begin.size() * sizeof(int));
   s.tile_begin = reinterpret_cast<int*>(base);
   base += up(g.tile_begin.size() * sizeof(int));
+  if (!g.tile_segs.empty()) {
+    s.tile_segs = reinterpret_cast<int*>(base);
+    base += up(g.tile_segs.size() * sizeof(int));
+  }
   s.part = reinterpret_cast<float*>(base);
   return s;
 }
@@ -495,6 +537,9 @@ void upload_plan_tables(const GemmPlan& g, const GemmScratch& s, cudaStream_t st
   FPLS_CUDA(cudaMemcpyAsync(s.segs, g.segs.data(), g.segs.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
   FPLS_CUDA(cudaMemcpyAsync(s.cta_begin, g.cta_begin.data(), g.cta_begin.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   FPLS_CUDA(cudaMemcpyAsync(s.tile_begin, g.tile_begin.data(), g.tile_begin.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  if (!g.tile_segs.empty())
+    FPLS_CUDA(cudaMemcpyAsync(s.tile_segs, g.tile_segs.data(), g.tile_segs.size() * sizeof(int), cudaMemcpyHostToDevice,
+                              st));
 }
 
 // Launches the GEMM and its reduction; the plan tables must already be in `s`.
@@ -531,9 +576,11 @@ void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K,
                    products * 2.0 * static_cast<double>(M) * N * K * tiles_frac);
   }
   if (g.bn == BN_SYM)
-    split_reduce_kernel<BN_SYM><<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, g.ntn, M, N, alpha, beta, C, ldc);
+    split_reduce_kernel<BN_SYM><<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, s.tile_segs, g.ntn, M, N,
+                                                                         alpha, beta, C, ldc);
   else
-    split_reduce_kernel<BN><<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, g.ntn, M, N, alpha, beta, C, ldc);
+    split_reduce_kernel<BN><<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, s.tile_segs, g.ntn, M, N,
+                                                                     alpha, beta, C, ldc);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }

@@ -115,11 +115,19 @@ struct Rows {
 static __device__ void cluster_exchange(ClusterRed& R, int count, int max_from = kRedMax) {
   const int b = R.buf;
   if constexpr (CL == 1) {
+    __syncthreads();
     for (int k = threadIdx.x; k < count; k += kT) R.res[k] = R.part[b][k];
     __syncthreads();
+    if (threadIdx.x == 0) R.buf = b ^ 1;
+    __syncthreads();
   } else {
+    // The cluster barrier also orders this CTA's own partial writes (every
+    // thread of every CTA arrives with release semantics), and every thread
+    // has read buf before it, so the flip can follow at once; the closing
+    // block barrier publishes res and the new buf.
     cg::cluster_group cl = cg::this_cluster();
     cl.sync();
+    if (threadIdx.x == 0) R.buf = b ^ 1;
     for (int k = threadIdx.x; k < count; k += kT) {
       double v = cl.map_shared_rank(&R.part[b][0], 0)[k];
       if (k >= max_from) {
@@ -129,8 +137,6 @@ static __device__ void cluster_exchange(ClusterRed& R, int count, int max_from =
       }
       R.res[k] = v;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) R.buf = b ^ 1;
     __syncthreads();
   }
 }
@@ -148,7 +154,6 @@ static __device__ void cluster_sum(ClusterRed& R, double (&v)[4], int count) {
     for (int w = 0; w < kW; ++w) s += R.warp[w][threadIdx.x];
     R.part[R.buf][threadIdx.x] = s;
   }
-  __syncthreads();
   cluster_exchange(R, count);
 }
 
@@ -185,7 +190,7 @@ static __device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M,
       for (int w = 0; w < kW; ++w) s += R.warp[w][j];
       R.part[R.buf][c0 + j] = s;
     }
-    __syncthreads();
+    if (c0 + kDotChunk < ncols) __syncthreads();   // before the next chunk reuses warp[][]
   }
   cluster_exchange(R, ncols);
 }
@@ -293,7 +298,6 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
   }
   __syncthreads();
   for (int j = threadIdx.x; j < m + 3; j += kT) R.part[R.buf][j] = zloc[j];
-  __syncthreads();
   cluster_exchange(R, m + 3, m + 2);
   const double tn = sqrt(R.res[m]);
   const double st = R.res[m + 1];

@@ -8,6 +8,7 @@
 #include "blas_f64.cuh"
 #include "context.cuh"
 #include "ozaki_gemm.cuh"
+#include "tc_util.cuh"
 
 #include <cooperative_groups.h>
 
@@ -440,6 +441,8 @@ static __device__ void run(const DualEng& e, int a) {
   const int f = blockIdx.x / kCl;
   int rank = 0;
   if constexpr (CL > 1) rank = static_cast<int>(cg::this_cluster().block_rank());
+  tc::grid_dep_wait();     // the previous product / step has completed
+  tc::grid_dep_launch();
   if (e.status[f]) return;   // set only in earlier launches: uniform over the cluster, before any remote access
   if (threadIdx.x == 0) R.buf = 0;
   __syncthreads();
@@ -495,13 +498,15 @@ void launch_step_cfg(const DualEng& e, int a, int F, cudaStream_t st) {
     lc.blockDim = dim3(T);
     lc.dynamicSmemBytes = 0;
     lc.stream = st;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = CL;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     lc.attrs = attr;
-    lc.numAttrs = 1;
+    lc.numAttrs = tc::pdl_enabled() ? 2 : 1;
     FPLS_CUDA(cudaLaunchKernelEx(&lc, k_dual_step<CL, T, LR>, e, a));
   }
   ::fpls::note_launch();

@@ -164,6 +164,10 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
+  // The set-up above overlaps the previous kernel; its outputs (the B planes
+  // and scales) are read only after it has completed.
+  tc::grid_dep_wait();
+  tc::grid_dep_launch();
 
   if (warp == 0 && lane == 0) {
     // ---------------------------------------------------------- producer
@@ -500,9 +504,21 @@ void launch_ozaki(const CUtensorMap& mA, const CUtensorMap& mB, const OzakiPlane
                                    OzLayout<S>::SMEM_BYTES));
     attr = true;
   }
-  ozaki_gemm_kernel<S><<<c.g.ctas, kThreads, OzLayout<S>::SMEM_BYTES, st>>>(
-      mA, mB, A.rows_pad, B.rows_pad, A.scale, B.scale, c.segs, c.cta_begin, c.tile_begin, c.g.ntn, c.part,
-      C, ldc, A.rows, B.rows, err);
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(c.g.ctas);
+  lc.blockDim = dim3(kThreads);
+  lc.dynamicSmemBytes = OzLayout<S>::SMEM_BYTES;
+  lc.stream = st;
+  cudaLaunchAttribute pdl[1];
+  pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  pdl[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = pdl;
+  lc.numAttrs = tc::pdl_enabled() ? 1 : 0;
+  const int a_rows_pad = A.rows_pad, b_rows_pad = B.rows_pad, ntn = c.g.ntn, m_rows = A.rows, n_rows = B.rows;
+  FPLS_CUDA(cudaLaunchKernelEx(&lc, ozaki_gemm_kernel<S>, mA, mB, a_rows_pad, b_rows_pad,
+                               static_cast<const double*>(A.scale), static_cast<const double*>(B.scale),
+                               static_cast<const int4*>(c.segs), static_cast<const int*>(c.cta_begin),
+                               static_cast<const int*>(c.tile_begin), ntn, c.part, C, ldc, m_rows, n_rows, err));
 }
 
 struct XOperatorOzakiSym : public XOperator {

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
 #include "context.cuh"
 
@@ -96,6 +97,21 @@ __device__ __forceinline__ void tmem_ld16_raw(uint32_t taddr, uint32_t (&r)[16])
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Programmatic dependent launch: wait until the grid this one depends on has
+// completed and its writes are visible (a no-op for a grid launched without
+// programmatic stream serialisation), and allow the next grid on the stream to
+// be scheduled.  Every kernel chained this way fits on the GPU in one wave, so
+// a dependent waiting early never holds an SM its predecessor still needs.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Launch attribute for programmatic stream serialisation (FASTPLS_PDL=0 turns
+// it off).
+inline bool pdl_enabled() {
+  const char* e = std::getenv("FASTPLS_PDL");
+  return !(e && e[0] == '0');
+}
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point.
 inline PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {

@@ -775,6 +775,7 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     FPLS_REQUIRE(kfold_outer >= 1 && kfold_inner >= 1 && L >= 1, "fold counts and ncomp must be >= 1");
     Context& ctx = Context::get();
     ctx.begin_call();
+    PhaseTimer pt("double CV call");
     const int Ko = kfold_outer, Ki = kfold_inner;
     std::vector<int> nc(ncomp, ncomp + L);
     for (int& c : nc) c = std::max(1, c);
@@ -785,45 +786,86 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     fs.group.assign(fs.F, 0);
     fs.seeds.resize(fs.F);
     std::vector<int> outer_classes(Ko, 0), fallback(Ko, 1);
+    const int m = n_classes;
+    FPLS_REQUIRE(m >= 1, "n_classes must be >= 1");
+    for (int i = 0; i < n; ++i)
+      FPLS_REQUIRE(y[i] >= 1 && y[i] <= m, "labels must be in 1..n_classes");
+    // Fold masks and training-row class counts from per-fold histograms: the
+    // rows outside outer fold o, split by inner fold id and class, give every
+    // inner fit's counts by subtraction (no pass per fit over the masks).
+    fs.train_class_counts.assign((size_t)fs.F * m, 0);
+    fs.n_train.assign(fs.F, 0);
+    fs.n_test.assign(fs.F, 0);
+    std::vector<uint8_t> keep(n);
+    std::vector<int> outer_cnt(m), inner_cnt((size_t)Ki * m);
     for (int o = 0; o < Ko; ++o) {
-      std::vector<int> cnt(n_classes, 0);
-      for (int i = 0; i < n; ++i)
-        if (outer_fold[i] != o) cnt[y[i] - 1]++;
+      const int* inner_o = inner_fold + (size_t)o * n;
+      std::fill(outer_cnt.begin(), outer_cnt.end(), 0);
+      std::fill(inner_cnt.begin(), inner_cnt.end(), 0);
+      for (int i = 0; i < n; ++i) {
+        keep[i] = outer_fold[i] != o;
+        if (keep[i]) {
+          ++outer_cnt[y[i] - 1];
+          const int fi = inner_o[i];
+          if (fi >= 0 && fi < Ki) ++inner_cnt[(size_t)fi * m + (y[i] - 1)];
+        }
+      }
       int best = 0;
-      for (int c = 0; c < n_classes; ++c) {
-        if (cnt[c] > 0) outer_classes[o]++;
-        if (cnt[c] > cnt[best]) best = c;
+      for (int c = 0; c < m; ++c) {
+        if (outer_cnt[c] > 0) outer_classes[o]++;
+        if (outer_cnt[c] > outer_cnt[best]) best = c;
       }
       fallback[o] = best + 1;
-    }
-    for (int o = 0; o < Ko; ++o) {
       const bool skip = outer_classes[o] < 2;  // pls.double.cv's single-class fallback
       for (int i0 = 0; i0 < Ki; ++i0) {
         const int f = o * Ki + i0;
         fs.group[f] = o;
         fs.seeds[f] = static_cast<unsigned>(seed + 1000 * run + (o + 1) + i0);
         if (skip) continue;
+        uint8_t* tr = fs.train.data() + (size_t)f * n;
+        uint8_t* te = fs.test.data() + (size_t)f * n;
         for (int i = 0; i < n; ++i) {
-          if (outer_fold[i] == o) continue;
-          const int fi = inner_fold[i + (size_t)o * n];
-          if (fi == i0) fs.test[(size_t)f * n + i] = 1;
-          else fs.train[(size_t)f * n + i] = 1;
+          const uint8_t in = inner_o[i] == i0;
+          tr[i] = keep[i] & static_cast<uint8_t>(!in);
+          te[i] = keep[i] & in;
         }
+        int ntr = 0, nte = 0;
+        for (int c = 0; c < m; ++c) {
+          const int t = inner_cnt[(size_t)i0 * m + c];
+          fs.train_class_counts[(size_t)f * m + c] = outer_cnt[c] - t;
+          ntr += outer_cnt[c] - t;
+          nte += t;
+        }
+        fs.n_train[f] = ntr;
+        fs.n_test[f] = nte;
       }
       const int f = Ko * Ki + o;
       fs.group[f] = Ko;
       fs.seeds[f] = static_cast<unsigned>(seed + 2000 * run + (o + 1));
       if (skip) continue;
-      for (int i = 0; i < n; ++i) (outer_fold[i] == o ? fs.test : fs.train)[(size_t)f * n + i] = 1;
+      uint8_t* tr = fs.train.data() + (size_t)f * n;
+      uint8_t* te = fs.test.data() + (size_t)f * n;
+      int ntr = 0;
+      for (int i = 0; i < n; ++i) {
+        tr[i] = keep[i];
+        te[i] = !keep[i];
+        ntr += keep[i];
+      }
+      for (int c = 0; c < m; ++c) fs.train_class_counts[(size_t)f * m + c] = outer_cnt[c];
+      fs.n_train[f] = ntr;
+      fs.n_test[f] = n - ntr;
     }
     CvGridResult res;
+    pt.mark("folds (host)");
     run_cv_grid(fs, X, x_is_float32, x_on_device, y, nc.data(), L, scaling, precision, batched, res);
+    pt.mark("grid");
     // Inner accuracy per (outer fold, ncomp) on the device; the chosen ncomp is the
     // first maximum (.cv_best_index); only counts and the outer predictions return.
     const int* d_y = upload(y, n);
     const int* d_outer = upload(outer_fold, n);
     std::vector<long long> cnts;
     cv_prediction_counts(res.d_pred, Ko, L, n, d_y, d_outer, cnts);
+    pt.mark("counts");
     std::vector<int> best_slice(Ko, 0), fb(Ko, 0);
     for (int o = 0; o < Ko; ++o) {
       int bi = 0;
@@ -847,6 +889,7 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     FPLS_CHECK_LAUNCH();
     download(outer_pred, d_out, n);
     if (inner_pred) download(inner_pred, res.d_pred, (size_t)Ko * L * n);
+    pt.mark("ncomp + outer");
     ctx.sync();
     if (fit_status) std::copy(res.status.begin(), res.status.end(), fit_status);
     }

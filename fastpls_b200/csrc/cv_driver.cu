@@ -159,14 +159,24 @@ void classify_fits(const CvFitSet& fs, const int* y, std::vector<int>& status,
   status.assign(fs.F, 1);
   fallback.assign(fs.F, 1);
   counts.assign((size_t)fs.F * fs.m, 0.0);
+  const bool given = !fs.train_class_counts.empty();
+  std::vector<int> cnt(fs.m);
   for (int f = 0; f < fs.F; ++f) {
     int ntest = 0, ntrain = 0;
-    for (int i = 0; i < fs.n; ++i) {
-      if (fs.test[(size_t)f * fs.n + i]) ++ntest;
-      if (fs.train[(size_t)f * fs.n + i]) {
-        ++ntrain;
-        counts[(size_t)f * fs.m + (y[i] - 1)] += 1.0;
+    if (given) {
+      ntest = fs.n_test[f];
+      ntrain = fs.n_train[f];
+      for (int c = 0; c < fs.m; ++c) counts[(size_t)f * fs.m + c] = fs.train_class_counts[(size_t)f * fs.m + c];
+    } else {
+      std::fill(cnt.begin(), cnt.end(), 0);
+      const uint8_t* te = fs.test.data() + (size_t)f * fs.n;
+      const uint8_t* tr = fs.train.data() + (size_t)f * fs.n;
+      for (int i = 0; i < fs.n; ++i) {
+        ntest += te[i];
+        ntrain += tr[i];
+        cnt[y[i] - 1] += tr[i];
       }
+      for (int c = 0; c < fs.m; ++c) counts[(size_t)f * fs.m + c] = cnt[c];
     }
     if (ntest == 0) { status[f] = 2; continue; }
     if (ntrain == 0) { status[f] = 3; continue; }
@@ -250,7 +260,12 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
     std::copy(fs.test.begin() + (size_t)f * n, fs.test.begin() + (size_t)(f + 1) * n, te.begin() + (size_t)a * n);
     grp[a] = fs.group[f];
     int nt = 0;
-    for (int i = 0; i < n; ++i) nt += fs.train[(size_t)f * n + i];
+    if (!fs.n_train.empty()) {
+      nt = fs.n_train[f];
+    } else {
+      const uint8_t* trf = fs.train.data() + (size_t)f * n;
+      for (int i = 0; i < n; ++i) nt += trf[i];
+    }
     ntrain[a] = nt;
     inv_nf[a] = 1.0 / nt;
     for (int c = 0; c < m; ++c) {
@@ -469,6 +484,7 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
                       const int* labels_host, const int* ncomp, int L,
                       const CvGridOptions& opt, CvGridResult& res) {
   Context& ctx = Context::get();
+  PhaseTimer pt("CV grid set-up");
   FPLS_REQUIRE(L >= 1, "ncomp must contain at least one value");
   for (int s = 0; s < L; ++s) FPLS_REQUIRE(ncomp[s] >= 1, "ncomp values must be >= 1");
   for (int i = 0; i < fs.n; ++i)
@@ -497,6 +513,7 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
       FPLS_CUDA(cudaEventRecord(ctx.side_done, ctx.side));
     }
   }
+  pt.mark("classify + sketches");
   const size_t npred = (size_t)fs.G * L * fs.n;
   res.d_pred = ctx.arena.alloc_n<int>(npred);
   bool special = false;
@@ -509,6 +526,8 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
   } else {
     dzero(res.d_pred, npred * sizeof(int));
   }
+  pt.mark("prediction buffers");
+  pt.report();
   if (batched) {
     run_batched(fs, x64, x32, labels_host, ncomp, L, opt, status, counts, d_om, res);
     return;

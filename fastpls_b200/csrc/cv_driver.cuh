@@ -19,6 +19,10 @@ struct CvFitSet {
   std::vector<uint8_t> test;        // F x n
   std::vector<int> group;           // F: prediction group of each fit
   std::vector<unsigned> seeds;      // F
+  // Optional, filled by builders that know the fold structure: training-row
+  // class counts (F x m) and training / test row counts (F); empty otherwise.
+  std::vector<int> train_class_counts;
+  std::vector<int> n_train, n_test;
 };
 
 struct CvGridOptions {

@@ -3,6 +3,7 @@ import numpy as np
 import pytest
 
 from oracle import cv as ocv
+from oracle import pls as opls
 from fastpls_b200 import synthetic
 from fastpls_b200.folds import double_cv_folds, stratified_group_folds
 from parity_utils import rel_err
@@ -78,3 +79,49 @@ def test_double_cv_bf16x3_close_to_fp64(lib, c4_small):
     b = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], seed=1, precision="bf16x3")
     assert np.allclose(a["inner_accuracy"], b["inner_accuracy"], atol=5e-3)
     assert _labels_agree(a["pred"], b["pred"], 0.99)
+
+
+def test_double_cv_fold_edge_cases(lib):
+    # Outer fold 0 leaves only class 1 in its training rows (single-class
+    # fallback: every fit of that fold is skipped, its rows get the majority
+    # class of the outer training rows, best ncomp = the smallest), and inner
+    # fold id 2 of outer fold 1 is never used (that inner fit has no test rows).
+    # The other folds follow the oracle's double CV loop.
+    rng = np.random.default_rng(11)
+    n, p, m = 240, 300, 3
+    y = np.repeat(np.arange(1, m + 1), n // m).astype(np.int32)
+    X = rng.standard_normal((n, p)) + 0.8 * y[:, None] * (np.arange(p) < 10)[None, :]
+    outer = np.where(y > 1, 0, 1 + rng.integers(0, 2, n)).astype(np.int32)
+    idx1 = np.where(y == 1)[0]
+    outer[idx1[:60]] = 1 + (np.arange(60) % 2)
+    outer[idx1[60:]] = 0
+    # outer 0 holds classes 2, 3 and 20 rows of class 1 -> its training rows are class 1 only
+    Ko, Ki = 3, 4
+    inner = np.full((n, Ko), -1, dtype=np.int32)
+    for o in range(Ko):
+        rows = np.where(outer != o)[0]
+        ids = np.arange(rows.size) % Ki
+        if o == 1:
+            ids[ids == 2] = 3
+        inner[rows, o] = ids
+    nc = np.arange(1, 6)
+    got = lib.double_cv(X, y, outer, inner, nc, m, seed=3)
+    st = got["fit_status"]
+    assert np.all(st[0:Ki] == 2) and st[Ko * Ki + 0] == 2
+    assert st[1 * Ki + 2] == 2
+    tr0 = outer != 0
+    fb = np.bincount(y[tr0], minlength=m + 1)[1:].argmax() + 1
+    assert got["best_comp"][0] == nc.min()
+    assert np.all(got["pred"][outer == 0] == fb)
+    Xd = X.astype(np.float64)
+    for o in (1, 2):
+        test = np.where(outer == o)[0]
+        train = np.where(outer != o)[0]
+        inn = ocv.pls_cv_predict_compiled(Xd[train], y[train], inner[train, o], nc, m, seed=3 + 1000 + o + 1)
+        acc = ocv.accuracy_table(inn["class_pred"], y[train])
+        assert np.allclose(got["inner_accuracy"][o], acc, atol=2e-3)
+        best = int(nc[ocv.best_index(acc)])
+        assert got["best_comp"][o] == best
+        model = opls.pls_model2_fast(Xd[train], ocv.response_rows(y, train, m), [best], seed=3 + 2000 + o + 1)
+        ref = opls.pls_predict_classes_compact(model, Xd[test])[:, 0]
+        assert np.mean(got["pred"][test] == ref) >= 0.99

@@ -717,12 +717,14 @@ static void run_cv_grid(const CvFitSet& fs, const void* X, int x_is_float32, boo
   }
   const size_t np = (size_t)fs.n * fs.p;
   dzero(ctx.d_status + 16, sizeof(int));
+  // Host X: the driver uploads it (overlapped with its first passes where it can).
+  const void* xh = x_on_device ? nullptr : X;
   if (x_is_float32) {
-    const float* d = x_on_device ? static_cast<const float*>(X) : upload(static_cast<const float*>(X), np);
-    cv_grid_classify(fs, nullptr, d, y, ncomp, L, opt, res);
+    const float* d = x_on_device ? static_cast<const float*>(X) : ctx.arena.alloc_n<float>(np);
+    cv_grid_classify(fs, nullptr, d, y, ncomp, L, opt, res, xh);
   } else {
-    const double* d = x_on_device ? static_cast<const double*>(X) : upload(static_cast<const double*>(X), np);
-    cv_grid_classify(fs, d, nullptr, y, ncomp, L, opt, res);
+    const double* d = x_on_device ? static_cast<const double*>(X) : ctx.arena.alloc_n<double>(np);
+    cv_grid_classify(fs, d, nullptr, y, ncomp, L, opt, res, xh);
   }
   int e = 0;
   d2h(&e, ctx.d_status + 16, sizeof(int));

@@ -79,6 +79,7 @@ Context& Context::get() {
     FPLS_CUDA(cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking));
     FPLS_CUDA(cudaStreamCreateWithFlags(&ctx.side, cudaStreamNonBlocking));
     FPLS_CUDA(cudaEventCreateWithFlags(&ctx.side_done, cudaEventDisableTiming));
+    FPLS_CUDA(cudaStreamCreateWithFlags(&ctx.copy, cudaStreamNonBlocking));
     FPLS_CUDA(cudaMalloc(&ctx.d_status, 64 * sizeof(int)));
     FPLS_CUDA(cudaMemset(ctx.d_status, 0, 64 * sizeof(int)));
     ctx.device = dev;
@@ -123,9 +124,19 @@ int Context::read_status() {
 
 void Context::sync() { FPLS_CUDA(cudaStreamSynchronize(stream)); }
 
+cudaEvent_t Context::copy_event(int i) {
+  while (static_cast<int>(copy_events.size()) <= i) {
+    cudaEvent_t ev;
+    FPLS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    copy_events.push_back(ev);
+  }
+  return copy_events[i];
+}
+
 void Context::release() {
   if (device < 0) return;
   cudaStreamSynchronize(side);
+  if (copy) cudaStreamSynchronize(copy);
   cudaStreamSynchronize(stream);
   arena.release();
 }

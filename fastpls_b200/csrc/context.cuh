@@ -41,6 +41,9 @@ struct Context {
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;   // second stream for work that overlaps `stream` (joined by events)
   cudaEvent_t side_done = nullptr;
+  cudaStream_t copy = nullptr;   // host-to-device copies that overlap `stream` (joined by copy_event(i))
+  std::vector<cudaEvent_t> copy_events;
+  cudaEvent_t copy_event(int i);   // i-th event of the copy stream (created on first use)
   Arena arena;
   int* d_status = nullptr;     // device-side failure flag (0 = ok)
   int sm_count = kSMCount;

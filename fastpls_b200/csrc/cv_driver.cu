@@ -203,9 +203,13 @@ void fill_special_predictions(const CvFitSet& fs, const int* y, const std::vecto
   }
 }
 
+// Columns per chunk of the overlapped upload of X.
+constexpr int kUploadChunkCols = 4096;
+
 void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const int* y, const int* ncomp, int L,
                  const CvGridOptions& opt, const std::vector<int>& status,
-                 const std::vector<double>& counts, double* d_om, CvGridResult& res) {
+                 const std::vector<double>& counts, double* d_om, CvGridResult& res,
+                 const void* x_host) {
   Context& ctx = Context::get();
   Arena& ar = ctx.arena;
   const int n = fs.n, p = fs.p, m = fs.m;
@@ -221,13 +225,6 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
   PhaseTimer pt("CV grid (batched)");
   // Global centring (scaling < 3): Xc = X - mean(X); folds shift by delta_f.
   const bool center = opt.scaling < 3;
-  double* mall = nullptr;
-  if (center) {
-    mall = ar.alloc_n<double>(p);
-    if (x64) col_mean(x64, n, p, n, mall);
-    else col_mean(x32, n, p, n, mall);
-  }
-  pt.mark("column means");
   // Short, wide predictor blocks run the loop in the row space of X (the
   // row Gram K = Xc Xc^T); otherwise in the predictor space.
   const bool dual = dual_engine_applies(n, p, m, K);
@@ -235,19 +232,69 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
   // from the caller's matrix; every other combination works on a centred FP64
   // copy.  x0 is the first column of Xc (the Householder sign of the sketch).
   const bool planes_only = opt.precision == 1 && dual;
+  FPLS_REQUIRE(!x_host || planes_only, "chunked upload outside the mixed row-space path");
+  double* mall = center ? ar.alloc_n<double>(p) : nullptr;
+  double* Kg = dual ? ar.alloc_n<double>((size_t)n * n) : nullptr;
+  bool gram_done = false;
   double* X = nullptr;
   double* x0 = nullptr;
   std::unique_ptr<XOperator> xop;
-  if (planes_only) {
+  if (x_host) {
+    // X arrives in column chunks on the copy stream; each chunk's column means,
+    // BF16 planes and row-Gram contribution run as soon as it has landed, while
+    // the next chunk is in flight (copies and compute are enqueued in turn, so
+    // a pageable host buffer overlaps too).
+    const size_t esz = x64 ? sizeof(double) : sizeof(float);
+    char* dst = x64 ? reinterpret_cast<char*>(const_cast<double*>(x64)) : reinterpret_cast<char*>(const_cast<float*>(x32));
+    const char* src = static_cast<const char*>(x_host);
+    const int nch = (p + kUploadChunkCols - 1) / kUploadChunkCols;
+    xop = make_split_operator_chunked(n, p);
     x0 = ar.alloc_n<double>(n);
-    load_centered(x64, x32, n, 1, mall, x0);
-    xop = make_split_operator_centered(x64, x32, mall, n, p);
+    // the copies follow this call's earlier work on the main stream (an event
+    // of their own: side_done marks the sketches, awaited later)
+    FPLS_CUDA(cudaEventRecord(ctx.copy_event(nch), ctx.stream));
+    FPLS_CUDA(cudaStreamWaitEvent(ctx.copy, ctx.copy_event(nch), 0));
+    auto chunk_work = [&](int c) {
+      const int j0 = c * kUploadChunkCols, j1 = std::min(p, j0 + kUploadChunkCols);
+      FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.copy_event(c), 0));
+      const double* c64 = x64 ? x64 + (size_t)j0 * n : nullptr;
+      const float* c32 = x32 ? x32 + (size_t)j0 * n : nullptr;
+      if (center) {
+        if (c64) col_mean(c64, n, j1 - j0, n, mall + j0);
+        else col_mean(c32, n, j1 - j0, n, mall + j0);
+      }
+      split_operator_fill_columns(*xop, c64, c32, center ? mall + j0 : nullptr, j0, j1);
+      if (c == 0) load_centered(x64, x32, n, 1, mall, x0);
+      split_operator_gram_columns(*xop, Kg, j0, j1, c > 0);
+    };
+    for (int c = 0; c < nch; ++c) {
+      const int j0 = c * kUploadChunkCols, j1 = std::min(p, j0 + kUploadChunkCols);
+      FPLS_CUDA(cudaMemcpyAsync(dst + (size_t)j0 * n * esz, src + (size_t)j0 * n * esz, (size_t)(j1 - j0) * n * esz,
+                                cudaMemcpyHostToDevice, ctx.copy));
+      FPLS_CUDA(cudaEventRecord(ctx.copy_event(c), ctx.copy));
+      if (c > 0) chunk_work(c - 1);
+    }
+    chunk_work(nch - 1);
+    mirror_upper_triangle(Kg, n);
+    gram_done = true;
+    pt.mark("upload + split + row gram");
   } else {
-    X = ar.alloc_n<double>((size_t)n * p);
-    load_centered(x64, x32, n, p, mall, X);
-    x0 = X;
-    if (opt.precision == 1) xop = make_split_operator(X, n, p, !dual);
-    else xop.reset(new XOperatorF64(X, n, p));
+    if (center) {
+      if (x64) col_mean(x64, n, p, n, mall);
+      else col_mean(x32, n, p, n, mall);
+    }
+    pt.mark("column means");
+    if (planes_only) {
+      x0 = ar.alloc_n<double>(n);
+      load_centered(x64, x32, n, 1, mall, x0);
+      xop = make_split_operator_centered(x64, x32, mall, n, p);
+    } else {
+      X = ar.alloc_n<double>((size_t)n * p);
+      load_centered(x64, x32, n, p, mall, X);
+      x0 = X;
+      if (opt.precision == 1) xop = make_split_operator(X, n, p, !dual);
+      else xop.reset(new XOperatorF64(X, n, p));
+    }
   }
   pt.mark("operator");
   std::vector<uint8_t> tr((size_t)Fa * n), te((size_t)Fa * n);
@@ -305,8 +352,7 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
     // mixed mode); the per-component products with the L2-resident K stay
     // FP64: the K-coordinate Gram-Schmidt carries K C_V and K C_S forward, and
     // split-precision products there drift from one component to the next.
-    double* Kg = ar.alloc_n<double>((size_t)n * n);
-    xop->gram(Kg);
+    if (!gram_done) xop->gram(Kg);
     XOperatorF64 kop_f64(Kg, n, n);
     XOperator* kop = &kop_f64;
     // Mixed mode: the K products on the INT8 tensor cores (digit planes of K
@@ -482,7 +528,7 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
 
 void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
                       const int* labels_host, const int* ncomp, int L,
-                      const CvGridOptions& opt, CvGridResult& res) {
+                      const CvGridOptions& opt, CvGridResult& res, const void* x_host) {
   Context& ctx = Context::get();
   PhaseTimer pt("CV grid set-up");
   FPLS_REQUIRE(L >= 1, "ncomp must contain at least one value");
@@ -528,8 +574,16 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
   }
   pt.mark("prediction buffers");
   pt.report();
+  // Overlapped upload only where the loop needs just the BF16 planes and the
+  // row Gram of X; otherwise X is copied whole before use.
+  const int Kmax = *std::max_element(ncomp, ncomp + L);
+  const bool chunked = x_host && batched && opt.precision == 1 && dual_engine_applies(fs.n, fs.p, fs.m, Kmax);
+  if (x_host && !chunked) {
+    if (x64) h2d(const_cast<double*>(x64), x_host, (size_t)fs.n * fs.p * sizeof(double));
+    else h2d(const_cast<float*>(x32), x_host, (size_t)fs.n * fs.p * sizeof(float));
+  }
   if (batched) {
-    run_batched(fs, x64, x32, labels_host, ncomp, L, opt, status, counts, d_om, res);
+    run_batched(fs, x64, x32, labels_host, ncomp, L, opt, status, counts, d_om, res, chunked ? x_host : nullptr);
     return;
   }
   // The per-fit path reads X in FP64 (widened once when the caller's is FP32).

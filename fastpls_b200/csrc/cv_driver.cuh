@@ -46,9 +46,12 @@ void cv_prediction_counts(const int* d_pred, int G, int L, int n, const int* d_l
                           const int* d_exclude, std::vector<long long>& counts);
 
 // X: device predictor matrix n x p, FP64 (x64) or FP32 (x32, exactly widened).
-// labels_host: 1-based class labels.  ncomp: L values (host).
+// labels_host: 1-based class labels.  ncomp: L values (host).  With x_host the
+// device buffer is empty and x_host holds the same matrix in host memory: the
+// driver uploads it, in column chunks overlapped with the column means, the
+// BF16 split and the row Gram on the mixed row-space path, else in one copy.
 void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
                       const int* labels_host, const int* ncomp, int L,
-                      const CvGridOptions& opt, CvGridResult& res);
+                      const CvGridOptions& opt, CvGridResult& res, const void* x_host = nullptr);
 
 }  // namespace fpls

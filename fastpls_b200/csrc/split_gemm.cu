@@ -299,7 +299,9 @@ __global__ void split_cols_kernel(const double* __restrict__ X, int rows, int co
 }
 
 // hi/lo split with transpose: X (rows x cols col-major, ld) -> rows x ldo
-// row-major pairs (row i holds X[i, :]), zero padded.  32 x 32 tiles via smem.
+// row-major pairs (row i holds X[i, :]), columns [cols, wcols) written as zero
+// padding (wcols <= ldo; a column chunk of a wider matrix writes just its
+// columns).  32 x 32 tiles via smem.
 // With `mean` the column means are subtracted (in FP64) before the split, so a
 // single-precision or uncentred caller matrix is centred and split in one pass
 // with the same values as centring an FP64 copy first.
@@ -307,7 +309,7 @@ template <typename T>
 __global__ void split_rows_kernel(const T* __restrict__ X, int rows, int cols, int ld,
                                   __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
                                   int ldo, __nv_bfloat16* __restrict__ mid,
-                                  const double* __restrict__ mean) {
+                                  const double* __restrict__ mean, int wcols) {
   __shared__ double tile[32][33];
   const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
@@ -323,7 +325,7 @@ __global__ void split_rows_kernel(const T* __restrict__ X, int rows, int cols, i
   __syncthreads();
   for (int r = ty; r < 32; r += 8) {
     const int i = i0 + r, j = j0 + tx;
-    if (i < rows && j < ldo) {
+    if (i < rows && j < wcols) {
       const double x = tile[tx][r];
       __nv_bfloat16 h, l, md;
       split_value(x, h, mid ? &md : nullptr, l);
@@ -652,9 +654,12 @@ void split_cols_on(const double* X, int rows, int cols, int ld, const SplitPair&
 
 template <typename T>
 void split_rows_on(const T* X, int rows, int cols, int ld, const SplitPair& out, cudaStream_t st,
-                   const double* mean = nullptr) {
-  dim3 grid((out.ld + 31) / 32, (rows + 31) / 32);
-  split_rows_kernel<T><<<grid, dim3(32, 8), 0, st>>>(X, rows, cols, ld, out.hi, out.lo, out.ld, out.mid, mean); ::fpls::note_launch();
+                   const double* mean = nullptr, int col0 = 0, int wcols = -1) {
+  if (wcols < 0) wcols = out.ld - col0;
+  dim3 grid((wcols + 31) / 32, (rows + 31) / 32);
+  split_rows_kernel<T><<<grid, dim3(32, 8), 0, st>>>(X, rows, cols, ld, out.hi + col0, out.lo + col0, out.ld,
+                                                     out.mid ? out.mid + col0 : nullptr, mean, wcols);
+  ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
@@ -690,6 +695,28 @@ struct XOperatorSplit : public XOperator {
     p = p_;
     xr = alloc_pair(n, p, np);
     split_rows_on(X, n, p, n, xr, Context::get().stream, mean);
+  }
+  // Row-major planes allocated only; filled column chunk by column chunk.
+  XOperatorSplit(int n_, int p_, int np_) : has_t(false), np(np_) {
+    n = n_;
+    p = p_;
+    xr = alloc_pair(n, p, np);
+  }
+  // Columns [j0, j1) of the planes from the chunk X (n x (j1 - j0), ld n) minus
+  // mean[0 .. j1-j0) (or nothing); the last chunk also writes the zero padding.
+  template <typename T>
+  void fill_columns(const T* X, const double* mean, int j0, int j1) {
+    const int w = (j1 >= p) ? xr.ld - j0 : j1 - j0;
+    split_rows_on(X, n, j1 - j0, n, xr, Context::get().stream, mean, j0, w);
+  }
+  // K (upper tiles) = Xc[:, j0:j1] Xc[:, j0:j1]^T, added to K when accumulate.
+  void gram_columns(double* K, int j0, int j1, bool accumulate) {
+    SplitPair v = xr;
+    v.hi = xr.hi + j0;
+    v.lo = xr.lo + j0;
+    if (v.mid) v.mid = xr.mid + j0;
+    v.k = j1 - j0;
+    split_gemm(v, v, n, n, j1 - j0, 1.0, accumulate ? 1.0 : 0.0, K, n, true);
   }
   void times(const double* Rhat, int F, double* U) override {
     SplitPair b = alloc_pair(F, p, np);
@@ -739,6 +766,28 @@ void split_gemm_release_cache() {
 std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p, bool need_t, int planes) {
   return std::unique_ptr<XOperator>(new XOperatorSplit(X, n, p, need_t, planes));
 }
+
+std::unique_ptr<XOperator> make_split_operator_chunked(int n, int p, int planes) {
+  return std::unique_ptr<XOperator>(new XOperatorSplit(n, p, planes));
+}
+
+void split_operator_fill_columns(XOperator& op, const double* x64, const float* x32, const double* mean, int j0,
+                                 int j1) {
+  auto* sp = dynamic_cast<XOperatorSplit*>(&op);
+  FPLS_REQUIRE(sp != nullptr, "column chunks need the split operator");
+  FPLS_REQUIRE(j0 % 8 == 0 && j0 >= 0 && j1 > j0 && j1 <= sp->p, "column chunk out of range");
+  if (x64) sp->fill_columns(x64, mean, j0, j1);
+  else sp->fill_columns(x32, mean, j0, j1);
+}
+
+void split_operator_gram_columns(XOperator& op, double* K, int j0, int j1, bool accumulate) {
+  auto* sp = dynamic_cast<XOperatorSplit*>(&op);
+  FPLS_REQUIRE(sp != nullptr, "column chunks need the split operator");
+  FPLS_REQUIRE(j0 % 8 == 0 && j0 >= 0 && j1 > j0 && j1 <= sp->p, "column chunk out of range");
+  sp->gram_columns(K, j0, j1, accumulate);
+}
+
+void mirror_upper_triangle(double* K, int n) { mirror_upper(K, n); }
 
 std::unique_ptr<XOperator> make_split_operator_centered(const double* x64, const float* x32, const double* mean,
                                                         int n, int p, int planes) {

@@ -26,6 +26,19 @@ std::unique_ptr<XOperator> make_split_operator(const double* X, int n, int p, bo
 std::unique_ptr<XOperator> make_split_operator_centered(const double* x64, const float* x32, const double* mean,
                                                         int n, int p, int planes = 2);
 
+// The same operator filled column chunk by column chunk (so that the upload
+// of X overlaps its split and its row Gram): planes allocated only;
+// split_operator_fill_columns writes columns [j0, j1) (j0 a multiple of 8) from
+// the chunk X[:, j0:j1] (device, ld n) minus mean[0 .. j1-j0) (or nothing);
+// split_operator_gram_columns sets (accumulate false) or adds to the upper
+// tiles of K (n x n) the chunk's X[:, j0:j1] X[:, j0:j1]^T; the lower triangle
+// is filled by mirror_upper_triangle once all chunks are in.
+std::unique_ptr<XOperator> make_split_operator_chunked(int n, int p, int planes = 2);
+void split_operator_fill_columns(XOperator& op, const double* x64, const float* x32, const double* mean, int j0,
+                                 int j1);
+void split_operator_gram_columns(XOperator& op, double* K, int j0, int j1, bool accumulate);
+void mirror_upper_triangle(double* K, int n);
+
 // C (M x N) = op(A) B with op(A) = A (M x K) or A^T (A is K x M), B K x N,
 // column-major device matrices.  In the mixed precision modes (session setting
 // FPLS_PREC_BF16X3 or FPLS_PREC_BF16X6) products with a contraction of at

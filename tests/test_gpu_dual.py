@@ -101,3 +101,34 @@ def test_step_layouts_agree(lib):
     assert np.array_equal(a["best_comp"], b["best_comp"])
     assert np.mean(a["inner_pred"] == b["inner_pred"]) >= 0.9999
     assert np.nanmax(np.abs(a["inner_accuracy"] - b["inner_accuracy"])) <= 1e-3
+
+
+def test_host_buffer_chunked_upload_matches_resident(lib):
+    # The host-buffer call uploads X in 4096-column chunks overlapped with the
+    # column means, the BF16 split and the row Gram (three chunks here, the last
+    # one partial); its predictions match the resident call's.  The chunked row
+    # Gram sums its FP32 segments over different stream-K cuts, so the check is
+    # agreement, not bit equality.
+    d = synthetic.c4_omics(seed=21, n=400, p=9000, n_informative=25)
+    outer, inner = double_cv_folds(d["y"], d["groups"], 4, 3, seed=3)
+    nc = np.arange(1, 13)
+    host = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], seed=5, precision="bf16x3",
+                         return_inner=True)
+    h = lib.x_upload(d["X"])
+    try:
+        res = lib.double_cv_resident(h, d["X"].shape[0], d["y"], outer, inner, nc, d["n_classes"], seed=5,
+                                     precision="bf16x3", return_inner=True)
+    finally:
+        lib.x_free(h)
+    assert np.array_equal(host["best_comp"], res["best_comp"])
+    assert np.mean(host["inner_pred"] == res["inner_pred"]) >= 0.999
+    assert np.mean(host["pred"] == res["pred"]) >= 0.99
+    # FP64 runs the single upload: identical to the resident call
+    a = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], seed=5, precision="fp64")
+    h = lib.x_upload(d["X"])
+    try:
+        b = lib.double_cv_resident(h, d["X"].shape[0], d["y"], outer, inner, nc, d["n_classes"], seed=5,
+                                   precision="fp64")
+    finally:
+        lib.x_free(h)
+    assert np.array_equal(a["pred"], b["pred"]) and np.array_equal(a["inner_accuracy"], b["inner_accuracy"])

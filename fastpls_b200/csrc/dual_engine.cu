@@ -200,7 +200,7 @@ static __device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M,
 // Householder normalisation, scores t = X_f r, q = Y^T t, and the loading
 // coefficients c_p for the K product.
 static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank) {
-  __shared__ double zloc[kMaxM + 3];
+  __shared__ double wcls[kW][kMaxM + 3];   // per-warp class sums, sum of squares, sum, max
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m;
   const double* CS = e.CS + (size_t)f * n * m;
@@ -265,40 +265,58 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
 #pragma unroll
   for (int k = 0; k < kLR; ++k) ky[k] *= sg;
   double* keep = e.Tkeep ? e.Tkeep + ((size_t)f * e.K + a) * n : nullptr;
-  for (int j = threadIdx.x; j < m + 3; j += kT) zloc[j] = 0.0;
-  __syncthreads();
-  double umax = 0.0;   // largest |centred score| of the train rows
-  double t2[2] = {0.0, 0.0};
+  // Class sums of the centred train scores, sum of squares, sum and the
+  // largest magnitude: each warp reduces its rows label by label (segmented
+  // warp sums) into its own row of wcls, and the rows are combined in warp
+  // order (no shared atomics: no contention on the few class slots, and the
+  // same rounding on every run).
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* wrow = wcls[warp];
+  for (int c = lane; c < m + 3; c += 32) wrow[c] = 0.0;
+  __syncwarp();
+  double t2a = 0.0, t2b = 0.0, umax = 0.0;   // sum of squares, sum, largest |centred score|
   double t[kLR];
 #pragma unroll
   for (int k = 0; k < kLR; ++k) {
     t[k] = 0.0;
-    if (!rw.ok(k)) continue;
-    const int i = rw.row(k);
-    const double uc = ky[k] - cmean;
-    if (keep) keep[i] = uc;
-    if (mk[i]) {
-      t[k] = uc;
-      t2[0] += uc * uc;
-      t2[1] += uc;
-      umax = fmax(umax, fabs(uc));
-      if (uc != 0.0) atomicAdd(&zloc[e.labels[i]], uc);
+    int lab = -1;
+    double uc = 0.0;
+    if (rw.ok(k)) {
+      const int i = rw.row(k);
+      uc = ky[k] - cmean;
+      if (keep) keep[i] = uc;
+      if (mk[i]) {
+        t[k] = uc;
+        t2a += uc * uc;
+        t2b += uc;
+        umax = fmax(umax, fabs(uc));
+        if (uc != 0.0) lab = e.labels[i];
+      }
+    }
+    unsigned pending = __ballot_sync(0xffffffffu, lab >= 0);
+    while (pending) {
+      const int c = __shfl_sync(0xffffffffu, lab, __ffs(pending) - 1);
+      const bool mine = lab == c;
+      const double v = warp_sum(mine ? uc : 0.0);
+      if (lane == 0) wrow[c] += v;
+      pending &= ~__ballot_sync(0xffffffffu, mine);
     }
   }
-  {
-    const double a0 = warp_sum(t2[0]), a1 = warp_sum(t2[1]);
+  t2a = warp_sum(t2a);
+  t2b = warp_sum(t2b);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
-    if ((threadIdx.x & 31) == 0) {
-      atomicAdd(&zloc[m], a0);
-      atomicAdd(&zloc[m + 1], a1);
-      // non-negative doubles order like their bit patterns
-      atomicMax(reinterpret_cast<unsigned long long*>(&zloc[m + 2]),
-                static_cast<unsigned long long>(__double_as_longlong(umax)));
-    }
+  for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+  if (lane == 0) {
+    wrow[m] = t2a;
+    wrow[m + 1] = t2b;
+    wrow[m + 2] = umax;
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < m + 3; j += kT) R.part[R.buf][j] = zloc[j];
+  for (int j = threadIdx.x; j < m + 3; j += kT) {
+    double v = wcls[0][j];
+    for (int w = 1; w < kW; ++w) v = (j == m + 2) ? fmax(v, wcls[w][j]) : v + wcls[w][j];
+    R.part[R.buf][j] = v;
+  }
   cluster_exchange(R, m + 3, m + 2);
   const double tn = sqrt(R.res[m]);
   const double st = R.res[m + 1];
@@ -407,17 +425,33 @@ static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows
     }
   }
   cluster_dots(R, CS, n, m, rw, kv);     // S^T v = C_S^T K c_v
-#pragma unroll 4
-  for (int j = 0; j < m; ++j) {
-    const double vj = R.res[j];
-    double* cs = CS + (size_t)j * n;
-    double* ks = KCS + (size_t)j * n;
+  // Rank-1 deflation of C_S and K C_S, four columns at a time: every load of
+  // a chunk is issued before its stores (the stores could alias later loads,
+  // which would otherwise serialise each column's read-modify-write).
+  for (int j0 = 0; j0 < m; j0 += 4) {
+    double csv[4][kLR], ksv[4][kLR];
 #pragma unroll
-    for (int k = 0; k < kLR; ++k)
-      if (rw.ok(k)) {
-        cs[rw.row(k)] -= cv[k] * vj;
-        ks[rw.row(k)] -= kv[k] * vj;
+    for (int jj = 0; jj < 4; ++jj) {
+      const int j = min(j0 + jj, m - 1);
+#pragma unroll
+      for (int k = 0; k < kLR; ++k) {
+        csv[jj][k] = rw.ok(k) ? CS[(size_t)j * n + rw.row(k)] : 0.0;
+        ksv[jj][k] = rw.ok(k) ? KCS[(size_t)j * n + rw.row(k)] : 0.0;
       }
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      if (j0 + jj >= m) break;
+      const double vj = R.res[j0 + jj];
+      double* cs = CS + (size_t)(j0 + jj) * n;
+      double* ks = KCS + (size_t)(j0 + jj) * n;
+#pragma unroll
+      for (int k = 0; k < kLR; ++k)
+        if (rw.ok(k)) {
+          cs[rw.row(k)] = csv[jj][k] - cv[k] * vj;
+          ks[rw.row(k)] = ksv[jj][k] - kv[k] * vj;
+        }
+    }
   }
   if (rank == 0) {
     const double tn = e.scal[2 * f], st = e.scal[2 * f + 1];

@@ -366,7 +366,8 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
 
 // Gram-Schmidt of the loading against the earlier ones in K-coordinates,
 // normalisation, rank-1 deflation of C_S and K C_S, and the component outputs.
-static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank) {
+static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank,
+                              const int (&ks0)[kLR], const int (&ks1)[kLR]) {
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m, K = e.K;
   double* CV = e.CV + (size_t)f * n * K;
@@ -381,11 +382,9 @@ static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows
     if (!rw.ok(k)) continue;
     const int i = rw.row(k);
     if (e.kpart) {
-      const int tile = (i >> 7) * e.kntn + (f >> 6);
-      const int s1 = e.kseg[tile + 1];
       const double* pp = e.kpart + (size_t)(f & 63) * 128 + (i & 127);
       double v = 0.0;
-      for (int sg = e.kseg[tile]; sg < s1; ++sg) v += pp[(size_t)sg * 64 * 128];
+      for (int sg = ks0[k]; sg < ks1[k]; ++sg) v += pp[(size_t)sg * 64 * 128];
       kv[k] = v;
     } else {
       kv[k] = e.Gp[(size_t)f * n + i];
@@ -475,28 +474,42 @@ static __device__ void run(const DualEng& e, int a) {
   const int f = blockIdx.x / kCl;
   int rank = 0;
   if constexpr (CL > 1) rank = static_cast<int>(cg::this_cluster().block_rank());
+  const int rows_per = (e.n + kCl - 1) / kCl;
+  Rows rw;
+  rw.r0 = rank * rows_per;
+  rw.nl = max(0, min(e.n, rw.r0 + rows_per) - rw.r0);
+  // Segment ranges of the K-product partials of this thread's rows: the plan's
+  // table was written when the plan was made, so it is read before the wait.
+  int ks0[kLR], ks1[kLR];
+#pragma unroll
+  for (int k = 0; k < kLR; ++k) {
+    ks0[k] = ks1[k] = 0;
+    if (a > 0 && e.kpart && rw.ok(k)) {
+      const int tile = (rw.row(k) >> 7) * e.kntn + (f >> 6);
+      ks0[k] = e.kseg[tile];
+      ks1[k] = e.kseg[tile + 1];
+    }
+  }
   tc::grid_dep_wait();     // the previous product / step has completed
   tc::grid_dep_launch();
   if (e.status[f]) return;   // set only in earlier launches: uniform over the cluster, before any remote access
   if (threadIdx.x == 0) R.buf = 0;
   __syncthreads();
-  const int rows_per = (e.n + kCl - 1) / kCl;
-  Rows rw;
-  rw.r0 = rank * rows_per;
-  rw.nl = max(0, min(e.n, rw.r0 + rows_per) - rw.r0);
   // Every CTA of the cluster takes the same branches (they follow the
   // cluster-wide sums, identical in all CTAs), and all of them end on the same
   // cluster barrier, which also keeps each CTA's shared memory alive until the
   // last remote read of it.
   bool ok = true;
-  if (a > 0) ok = dual_b(e, a - 1, R, rw, rank);
+  if (a > 0) ok = dual_b(e, a - 1, R, rw, rank, ks0, ks1);
   if (ok && a < e.K) dual_a(e, a, R, rw, rank);
   if constexpr (CL > 1) cg::this_cluster().sync();
 }
 };  // struct Step
 
+// 512-thread CTAs are held to 64 registers so that two fit on an SM and the
+// 240 CTAs of a 60-fit grid run in one wave.
 template <int CL, int T, int LR>
-__global__ void __launch_bounds__(T) k_dual_step(DualEng e, int a) {
+__global__ void __launch_bounds__(T, T >= 512 ? 2 : 1) k_dual_step(DualEng e, int a) {
   Step<CL, T, LR>::run(e, a);
 }
 

@@ -132,12 +132,13 @@ def measured_peaks():
 
 # kernel class -> (roofline bound, peak key, kernel description, ncu traffic file)
 KERNEL_CLASSES = {
-    "dual_step": ("hbm", "hbm", "k_dual_step (per-fit SIMPLS steps in row space, 4-CTA clusters)",
+    "dual_step": ("hbm", "hbm", "k_dual_step<4, 512, 2> (per-fit SIMPLS steps in row space, 4-CTA clusters)",
                   "k_dual_step_c4_traffic.json"),
     "k_products_f64": ("tensor", "fp64", "gemm_f64_dmma (batched K products, FP64 DMMA)", None),
-    "k_products_int8": ("tensor", "int8", "ozaki_gemm_kernel (batched K products on INT8 tcgen05 digit planes, "
-                        "with the per-product digit split and partial reduction; TOP/s of int8 plane products)", None),
-    "gram_bf16x3": ("tensor", "bf16", "split_gemm_kernel (tcgen05 BF16x3 row Gram, upper tiles)", None),
+    "k_products_int8": ("tensor", "int8", "ozaki_gemm_kernel<6> (batched K products on INT8 tcgen05 digit planes; "
+                        "TOP/s of int8 plane products)", "ozaki_gemm_c4_traffic.json"),
+    "gram_bf16x3": ("tensor", "bf16", "split_gemm_kernel<2, 128> (tcgen05 BF16x3 row Gram, upper tiles)",
+                    "gram_bf16x3_c4_traffic.json"),
     "split_gemm_bf16x3": ("hbm", "hbm", "split_gemm_kernel (tcgen05 BF16x3 skinny GEMM)",
                           "split_gemm_c4_traffic.json"),
 }

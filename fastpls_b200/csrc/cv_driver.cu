@@ -383,6 +383,14 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
     db.mY_all = d_mYall;
     db.dY = d_dY;
     db.ntrain = d_nt;
+    {
+      std::vector<double> cc((size_t)Fa * m);
+      for (int a = 0; a < Fa; ++a)
+        for (int c = 0; c < m; ++c) cc[(size_t)a * m + c] = counts[(size_t)act[a] * m + c];
+      double* d_cc = ar.alloc_n<double>(cc.size());
+      h2d(d_cc, cc.data(), cc.size() * sizeof(double));
+      db.class_cnt = d_cc;
+    }
     db.Q = Qo; db.tnorm = tno; db.Tkeep = Tko; db.ncomp_done = ncd; db.status = sto;
     dual_simpls_run(db);
     pt.mark("simpls");

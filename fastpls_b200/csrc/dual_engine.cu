@@ -30,6 +30,7 @@ struct DualEng {
   const double* mY_all;
   const double* dY;
   const int* ntrain;
+  const double* class_cnt;   // F x m train rows per class
   double* CS;    // F x n x m
   double* KCS;   // F x n x m
   double* CV;    // F x n x K
@@ -97,6 +98,7 @@ static constexpr int kDotCols = LR <= 4 ? 8 : 4;   // columns whose loads are in
 static constexpr int kColUnroll = LR <= 4 ? 8 : 4;
 struct ClusterRed {
   double warp[kW][kDotChunk];
+  double xw[kW];                     // per-warp sums of an extra scalar reduced with the dots
   double part[2][kRedMax];           // this CTA's partials (alternating between exchanges)
   double res[kRedMax];
   int buf;
@@ -160,9 +162,14 @@ static __device__ void cluster_sum(ClusterRed& R, double (&v)[4], int count) {
 
 // res[j] = sum over the fit's rows of M[i + j*n] * x_i for j < ncols, with x
 // given by the owned rows in registers.
+// With has_extra, res[ncols] is also the cluster sum of the per-thread value extra.
 static __device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M, int n, int ncols, const Rows& rw,
-                                    const double (&x)[kLR]) {
+                                    const double (&x)[kLR], bool has_extra = false, double extra = 0.0) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (has_extra) {
+    const double w = warp_sum(extra);
+    if (lane == 0) R.xw[warp] = w;
+  }
   for (int c0 = 0; c0 < ncols; c0 += kDotChunk) {
     const int cn = min(kDotChunk, ncols - c0);
     // kDotCols columns per pass, loads issued together (no data-dependent
@@ -191,16 +198,21 @@ static __device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M,
       for (int w = 0; w < kW; ++w) s += R.warp[w][j];
       R.part[R.buf][c0 + j] = s;
     }
+    if (has_extra && c0 == 0 && threadIdx.x == kT - 1) {
+      double v = 0.0;
+      for (int w = 0; w < kW; ++w) v += R.xw[w];
+      R.part[R.buf][ncols] = v;
+    }
     if (c0 + kDotChunk < ncols) __syncthreads();   // before the next chunk reuses warp[][]
   }
-  cluster_exchange(R, ncols);
+  cluster_exchange(R, has_extra ? ncols + 1 : ncols);
 }
 
 // Refresh (power iterations of S S^T from the sketch or the warm start),
 // Householder normalisation, scores t = X_f r, q = Y^T t, and the loading
 // coefficients c_p for the K product.
 static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank) {
-  __shared__ double wcls[kW][kMaxM + 3];   // per-warp class sums, sum of squares, sum, max
+  __shared__ double wcls[kW][kMaxM + 5];   // per-warp class sums and the reduction's scalars
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m;
   const double* CS = e.CS + (size_t)f * n * m;
@@ -241,95 +253,115 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
     }
     if (it + 1 < steps) cluster_dots(R, CS, n, m, rw, ky);
   }
-  // ||y||^2 = c_y^T K c_y, y[0] = Xc[:,0]^T c_y and the train-row sum of K c_y
-  // (the score mean, once the sign and norm are known)
-  double s[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-  for (int k = 0; k < kLR; ++k)
-    if (rw.ok(k)) {
-      s[0] += cy[k] * ky[k];
-      s[1] += e.x0[rw.row(k)] * cy[k];
-      if (mk[rw.row(k)]) s[2] += ky[k];
-    }
-  cluster_sum(R, s, 3);
-  const double nrm = sqrt(R.res[0]);
-  const double y0 = R.res[1];
-  if (!(nrm > 0.0) || !isfinite(nrm)) {
-    if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
-    return false;
-  }
-  const double sg = ((y0 >= 0.0) ? -1.0 : 1.0) / nrm;
-  const double nf = static_cast<double>(e.ntrain[f]);
-  // U = X r = sg * K c_y; its mean over the train rows centres the scores
-  const double cmean = e.center ? sg * R.res[2] / nf : 0.0;
-#pragma unroll
-  for (int k = 0; k < kLR; ++k) ky[k] *= sg;
-  double* keep = e.Tkeep ? e.Tkeep + ((size_t)f * e.K + a) * n : nullptr;
-  // Class sums of the centred train scores, sum of squares, sum and the
-  // largest magnitude: each warp reduces its rows label by label (segmented
-  // warp sums) into its own row of wcls, and the rows are combined in warp
-  // order (no shared atomics: no contention on the few class slots, and the
-  // same rounding on every run).
+  // One reduction for the refresh result and its scores: ||y||^2 = c_y^T K c_y
+  // (all rows), y[0] = Xc[:,0]^T c_y, and over the train rows the class sums,
+  // the sum S, the sum of squares Q and the largest magnitude of K c_y (per
+  // warp, label-segmented warp sums, warps combined in order).  The scores
+  // u = sg K c_y - cmean are then known row by row, and their class sums, sum
+  // and norm follow with the exact class counts n_c: sum_c u = sg S_c - cmean n_c,
+  // ||u||^2 = sg^2 (Q - S^2 / n_f) when centred (sg^2 Q otherwise).  When the
+  // centred sum of squares falls below 1e-6 Q (the train mean dominates the
+  // spread) it is taken by a second, exact pass instead.
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* wrow = wcls[warp];
-  for (int c = lane; c < m + 3; c += 32) wrow[c] = 0.0;
+  for (int c = lane; c < m + 5; c += 32) wrow[c] = 0.0;
   __syncwarp();
-  double t2a = 0.0, t2b = 0.0, umax = 0.0;   // sum of squares, sum, largest |centred score|
-  double t[kLR];
+  double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0, kmax = 0.0;
 #pragma unroll
   for (int k = 0; k < kLR; ++k) {
-    t[k] = 0.0;
     int lab = -1;
-    double uc = 0.0;
+    double kt = 0.0;
     if (rw.ok(k)) {
       const int i = rw.row(k);
-      uc = ky[k] - cmean;
-      if (keep) keep[i] = uc;
+      r0 += cy[k] * ky[k];
+      r1 += e.x0[i] * cy[k];
       if (mk[i]) {
-        t[k] = uc;
-        t2a += uc * uc;
-        t2b += uc;
-        umax = fmax(umax, fabs(uc));
-        if (uc != 0.0) lab = e.labels[i];
+        kt = ky[k];
+        r2 += kt;
+        r3 += kt * kt;
+        kmax = fmax(kmax, fabs(kt));
+        lab = e.labels[i];
       }
     }
     unsigned pending = __ballot_sync(0xffffffffu, lab >= 0);
     while (pending) {
       const int c = __shfl_sync(0xffffffffu, lab, __ffs(pending) - 1);
       const bool mine = lab == c;
-      const double v = warp_sum(mine ? uc : 0.0);
+      const double v = warp_sum(mine ? kt : 0.0);
       if (lane == 0) wrow[c] += v;
       pending &= ~__ballot_sync(0xffffffffu, mine);
     }
   }
-  t2a = warp_sum(t2a);
-  t2b = warp_sum(t2b);
+  r0 = warp_sum(r0);
+  r1 = warp_sum(r1);
+  r2 = warp_sum(r2);
+  r3 = warp_sum(r3);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+  for (int o = 16; o > 0; o >>= 1) kmax = fmax(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
   if (lane == 0) {
-    wrow[m] = t2a;
-    wrow[m + 1] = t2b;
-    wrow[m + 2] = umax;
+    wrow[m] = r0;
+    wrow[m + 1] = r1;
+    wrow[m + 2] = r2;
+    wrow[m + 3] = r3;
+    wrow[m + 4] = kmax;
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < m + 3; j += kT) {
+  for (int j = threadIdx.x; j < m + 5; j += kT) {
     double v = wcls[0][j];
-    for (int w = 1; w < kW; ++w) v = (j == m + 2) ? fmax(v, wcls[w][j]) : v + wcls[w][j];
+    for (int w = 1; w < kW; ++w) v = (j == m + 4) ? fmax(v, wcls[w][j]) : v + wcls[w][j];
     R.part[R.buf][j] = v;
   }
-  cluster_exchange(R, m + 3, m + 2);
-  const double tn = sqrt(R.res[m]);
-  const double st = R.res[m + 1];
+  cluster_exchange(R, m + 5, m + 4);
+  const double nrm = sqrt(R.res[m]);
+  const double y0 = R.res[m + 1];
+  if (!(nrm > 0.0) || !isfinite(nrm)) {
+    if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
+    return false;
+  }
+  const double sg = ((y0 >= 0.0) ? -1.0 : 1.0) / nrm;
+  const double nf = static_cast<double>(e.ntrain[f]);
+  const double S = R.res[m + 2], Q = R.res[m + 3];
+  // U = X r = sg * K c_y; its mean over the train rows centres the scores
+  const double cmean = e.center ? sg * S / nf : 0.0;
+  const double var = e.center ? Q - S * S / nf : Q;
+  const double kmax_all = R.res[m + 4];
+  // q = Y^T t: class sums of the centred scores (written now: the exact
+  // fallback below reuses the reduction buffer)
+  if (rank == 0)
+    for (int j = threadIdx.x; j < m; j += kT)
+      e.qs[(size_t)f * m + j] = sg * R.res[j] - cmean * e.class_cnt[(size_t)f * m + j];
+#pragma unroll
+  for (int k = 0; k < kLR; ++k) ky[k] *= sg;
+  double tn2, st;
+  if (var > 1e-6 * Q) {
+    tn2 = sg * sg * var;
+    st = sg * S - (e.center ? nf * cmean : 0.0);
+  } else {
+    double s2[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < kLR; ++k)
+      if (rw.ok(k) && mk[rw.row(k)]) {
+        const double uc = ky[k] - cmean;
+        s2[0] += uc * uc;
+        s2[1] += uc;
+      }
+    cluster_sum(R, s2, 2);
+    tn2 = R.res[0];
+    st = R.res[1];
+  }
+  const double tn = sqrt(tn2);
   if (!(tn > 0.0) || !isfinite(tn)) {
     if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
     return false;
   }
+  double* keep = e.Tkeep ? e.Tkeep + ((size_t)f * e.K + a) * n : nullptr;
   // Digit planes of c_p for the INT8 K product: scale 2^ex above the bound
-  // (max |centred score| + |mean|) / ||t|| of every |c_p[i]|, then the signed
-  // 7-bit digits taken exactly (scale by 128, truncate, subtract).
+  // (|sg| max |K c_y| + |cmean| + |mean|) / ||t|| of every |c_p[i]|, then the
+  // signed 7-bit digits taken exactly (scale by 128, truncate, subtract).
   double inv = 0.0;
   if (e.cpd) {
-    const double bound = (R.res[m + 2] + (e.center ? fabs(st) / nf : 0.0)) / tn * (1.0 + 0x1p-30);
+    const double bound = (fabs(sg) * kmax_all + fabs(cmean) + (e.center ? fabs(st) / nf : 0.0)) / tn *
+                         (1.0 + 0x1p-30);
     int ex = 0;
     if (bound > 0.0) frexp(bound, &ex);
     ex = max(-1000, min(1000, ex));
@@ -340,7 +372,9 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
   for (int k = 0; k < kLR; ++k) {
     if (!rw.ok(k)) continue;
     const int i = rw.row(k);
-    const double c = (t[k] - ((e.center && mk[i]) ? st / nf : 0.0)) / tn;
+    const double uc = ky[k] - cmean;
+    if (keep) keep[i] = uc;
+    const double c = mk[i] ? (uc - (e.center ? st / nf : 0.0)) / tn : 0.0;
     e.cp[(size_t)f * n + i] = c;
     e.Kcy[(size_t)f * n + i] = ky[k] / tn;
     if (e.cpd) {
@@ -355,7 +389,6 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
     }
   }
   if (rank == 0) {
-    for (int j = threadIdx.x; j < m; j += kT) e.qs[(size_t)f * m + j] = R.res[j];
     if (threadIdx.x == 0) {
       e.scal[2 * f] = tn;
       e.scal[2 * f + 1] = st;
@@ -405,11 +438,13 @@ static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows
         }
     }
   }
-  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  // ||v||^2 = c_v^T K c_v and S^T v = C_S^T K c_v in one reduction (the
+  // normalisation only rescales the dots)
+  double vv = 0.0;
 #pragma unroll
-  for (int k = 0; k < kLR; ++k) s[0] += cv[k] * kv[k];
-  cluster_sum(R, s, 1);
-  const double vn = sqrt(R.res[0]);
+  for (int k = 0; k < kLR; ++k) vv += cv[k] * kv[k];
+  cluster_dots(R, CS, n, m, rw, kv, true, vv);
+  const double vn = sqrt(R.res[m]);
   if (!(vn > 0.0) || !isfinite(vn)) {
     if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
     return false;
@@ -423,7 +458,6 @@ static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows
       KCV[rw.row(k) + (size_t)a * n] = kv[k];
     }
   }
-  cluster_dots(R, CS, n, m, rw, kv);     // S^T v = C_S^T K c_v
   // Rank-1 deflation of C_S and K C_S, four columns at a time: every load of
   // a chunk is issued before its stores (the stores could alias later loads,
   // which would otherwise serialise each column's read-modify-write).
@@ -441,7 +475,7 @@ static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj) {
       if (j0 + jj >= m) break;
-      const double vj = R.res[j0 + jj];
+      const double vj = R.res[j0 + jj] / vn;
       double* cs = CS + (size_t)(j0 + jj) * n;
       double* ks = KCS + (size_t)(j0 + jj) * n;
 #pragma unroll
@@ -609,6 +643,8 @@ void dual_simpls_run(const DualBatch& b) {
   e.scal = ar.alloc_n<double>(2 * F);
   e.qs = ar.alloc_n<double>(F * m);
   e.ntrain = b.ntrain;
+  FPLS_REQUIRE(b.class_cnt != nullptr, "dual SIMPLS: class counts missing");
+  e.class_cnt = b.class_cnt;
   OzakiPlanes cpP;
   if (b.kop_int8_slices > 0) {
     cpP = ozaki_alloc(b.F, b.n, b.kop_int8_slices);

@@ -41,6 +41,7 @@ struct DualBatch {
   const double* mY_all = nullptr;    // m
   const double* dY = nullptr;        // F x m fold offsets of the class proportions
   const int* ntrain = nullptr;       // F train-row counts
+  const double* class_cnt = nullptr; // F x m train rows per class (exact integers)
   // Outputs (as SimplsBatch)
   double* Q = nullptr;               // F x m x K
   double* tnorm = nullptr;           // F x K

@@ -60,6 +60,12 @@ SIGNATURES = {
                                  ctypes.c_int),
     "fpls_bf16x3_gemm": ([_DP, _I, _I, _DP, _I, _DP, _C, _S], ctypes.c_int),
     "fpls_int8_emulated_gemm": ([_DP, _I, _I, _DP, _I, _I, _DP, _C, _S], ctypes.c_int),
+    "fpls_kernel_matrix": ([_DP, _I, _DP, _I, _I, _I, _D, _I, _D, _DP, _C, _S], ctypes.c_int),
+    "fpls_center_kernel_train": ([_DP, _I, _DP, _DP, _DP, _C, _S], ctypes.c_int),
+    "fpls_center_kernel_test": ([_DP, _I, _I, _DP, _D, _DP, _C, _S], ctypes.c_int),
+    "fpls_kernel_pls_model2_fast": ([_DP, _I, _I, _DP, _I, _IP, _I, _I, _I, _D, _I, _D, _I, _I, _DP, _DP, _DP,
+                                     _DP, _DP, _DP, _DP, _DP, _IP, _DP, _DP, _DP, _DP, _DP, _C, _S],
+                                    ctypes.c_int),
     "fpls_cv_predict": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I, _I, _I,
                          _I, _IP, _IP, _C, _S], ctypes.c_int),
     "fpls_double_cv": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I,
@@ -433,6 +439,73 @@ def int8_emulated_gemm(A, B, slices=7):
     C = _out(A.shape[0], B.shape[1])
     _call("fpls_int8_emulated_gemm", _p(A), A.shape[0], A.shape[1], _p(B), B.shape[1], int(slices), _p(C))
     return C
+
+
+KERNEL_IDS = {"linear": 1, "rbf": 2, "poly": 3}
+
+
+def kernel_matrix(X1, X2, kernel="rbf", gamma=None, degree=3, coef0=1.0):
+    """kernel_matrix_cpp on the device (X1 n1 x p, X2 n2 x p)."""
+    X1 = _f64(X1)
+    X2 = X1 if X2 is None else _f64(X2)
+    kid = KERNEL_IDS[kernel] if isinstance(kernel, str) else int(kernel)
+    g = 1.0 / max(1, X1.shape[1]) if gamma is None else float(gamma)
+    K = _out(X1.shape[0], X2.shape[0])
+    _call("fpls_kernel_matrix", _p(X1), X1.shape[0], _p(X2), X2.shape[0], X1.shape[1], kid, g, int(degree),
+          float(coef0), _p(K))
+    return K
+
+
+def center_kernel_train(K):
+    K = _f64(K)
+    n = K.shape[0]
+    Kc = _out(n, n)
+    cm = np.zeros(n)
+    g = np.zeros(1)
+    _call("fpls_center_kernel_train", _p(K), n, _p(Kc), _p(cm), _p(g))
+    return dict(K=Kc, col_means=cm, grand_mean=float(g[0]))
+
+
+def center_kernel_test(Ktest, col_means, grand_mean):
+    Kt = _f64(Ktest)
+    Kc = _out(*Kt.shape)
+    _call("fpls_center_kernel_test", _p(Kt), Kt.shape[0], Kt.shape[1], _p(_f64(np.asarray(col_means))),
+          float(grand_mean), _p(Kc))
+    return Kc
+
+
+def kernel_pls_model2_fast(X, Y, ncomp, kernel="rbf", gamma=None, degree=3, coef0=1.0, scaling=1, fit=False,
+                           seed=1):
+    """Kernel PLS fit in one device call (preprocess, kernel, centre, fast SIMPLS)."""
+    X = _f64(X)
+    Y = _f64(np.asarray(Y, dtype=np.float64).reshape(X.shape[0], -1))
+    n, p = X.shape
+    m = Y.shape[1]
+    nc = _i32(np.atleast_1d(ncomp))
+    L = nc.size
+    K = int(nc.max())
+    R = _out(n, K)
+    Q = _out(m, K)
+    mK, vK, mY = np.zeros(n), np.zeros(n), np.zeros(m)
+    B = np.zeros((n, m, L), order="F")
+    Yfit = np.zeros((n, m, L), order="F") if fit else None
+    R2Y = np.zeros(L)
+    ncd = ctypes.c_int(0)
+    mX, vX, cm = np.zeros(p), np.zeros(p), np.zeros(n)
+    g = np.zeros(1)
+    gu = np.zeros(1)
+    kid = KERNEL_IDS[kernel] if isinstance(kernel, str) else int(kernel)
+    _call("fpls_kernel_pls_model2_fast", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), kid,
+          -1.0 if gamma is None else float(gamma), int(degree), float(coef0), int(bool(fit)), int(seed),
+          _p(R), _p(Q), _p(mK), _p(vK), _p(mY), _p(B), None if Yfit is None else _p(Yfit), _p(R2Y),
+          ctypes.byref(ncd), _p(mX), _p(vX), _p(cm), _p(g), _p(gu))
+    inner = dict(R=R, Q=Q, mX=mK.reshape(1, n), vX=vK.reshape(1, n), mY=mY.reshape(1, m), B=B, R2Y=R2Y,
+                 ncomp=nc, p=n, m=m, pls_method="simpls", n_components=ncd.value, B_stored=True,
+                 compact_prediction=False)
+    if fit:
+        inner["Yfit"] = Yfit
+    return dict(inner=inner, mX=mX, vX=vX, col_means=cm, grand_mean=float(g[0]), gamma=float(gu[0]),
+                kernel_id=kid, degree=int(degree), coef0=float(coef0))
 
 
 def _x_arg(X):

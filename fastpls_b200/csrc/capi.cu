@@ -14,6 +14,7 @@
 #include "cv_driver.cuh"
 #include "fits.cuh"
 #include "heads.cuh"
+#include "kernel_pls.cuh"
 #include "ozaki_gemm.cuh"
 #include "simpls_engine.cuh"
 #include "svd.cuh"
@@ -299,11 +300,11 @@ int fpls_pls_model2_fast_xprod(const double* X, int n, int p, const double* Y, i
   });
 }
 
-int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
-                         int L, int scaling, int fit, int seed, double* R, double* Q, double* mX,
-                         double* vX, double* mY, double* B, double* Yfit, double* R2Y,
-                         int* n_components, char* err, size_t errlen) {
-  return guarded(err, errlen, [&] {
+// Fast SIMPLS (pls_model2_fast) on device copies of X (n x p) and Y (n x m),
+// both centred / scaled in place; host outputs as fpls_pls_model2_fast.
+static void simpls_fast_on_device(double* dX, int n, int p, double* dYc, int m, const int* ncomp, int L,
+                                  int scaling, int fit, int seed, double* R, double* Q, double* mX, double* vX,
+                                  double* mY, double* B, double* Yfit, double* R2Y, int* n_components) {
     FPLS_REQUIRE(n > 0 && p > 0 && m > 0, "pls_model2_fast requires non-empty X and Y");
     FPLS_REQUIRE(L >= 1 && ncomp, "ncomp must contain at least one value");
     FPLS_REQUIRE(!(fit && !Yfit), "fit = 1 requires a Yfit buffer");
@@ -311,12 +312,9 @@ int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, 
                  "pls_model2_fast with <= 5 predictors and several responses is not supported on "
                  "the GPU path");
     Context& ctx = Context::get();
-    ctx.begin_call();
     std::vector<int> nc(ncomp, ncomp + L);
     for (int& c : nc) c = std::max(1, c);
     const int K = max_of(nc.data(), L);
-    double* dX = upload(X, (size_t)n * p);
-    double* dYc = upload(Y, (size_t)n * m);
     double* dmX = ctx.arena.alloc_n<double>(p);
     double* dvX = ctx.arena.alloc_n<double>(p);
     double* dmY = ctx.arena.alloc_n<double>(m);
@@ -403,6 +401,103 @@ int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, 
         R2Y[i] = (fit && filled[i]) ? 1.0 - hrq[2 * i] / hrq[2 * i + 1] : 0.0;
     }
     if (n_components) *n_components = done;
+}
+
+int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
+                         int L, int scaling, int fit, int seed, double* R, double* Q, double* mX,
+                         double* vX, double* mY, double* B, double* Yfit, double* R2Y,
+                         int* n_components, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && m > 0, "pls_model2_fast requires non-empty X and Y");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    double* dX = upload(X, (size_t)n * p);
+    double* dYc = upload(Y, (size_t)n * m);
+    simpls_fast_on_device(dX, n, p, dYc, m, ncomp, L, scaling, fit, seed, R, Q, mX, vX, mY, B, Yfit, R2Y,
+                          n_components);
+  });
+}
+
+int fpls_kernel_matrix(const double* X1, int n1, const double* X2, int n2, int p, int kernel, double gamma,
+                       int degree, double coef0, double* K, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n1 > 0 && n2 > 0 && p > 0, "X1 and X2 must be non-empty");
+    FPLS_REQUIRE(kernel >= 1 && kernel <= 3, "Unknown kernel id");
+    FPLS_REQUIRE(kernel == 1 || (std::isfinite(gamma) && gamma > 0.0), "gamma must be a finite positive number");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const double* d1 = upload(X1, (size_t)n1 * p);
+    const double* d2 = (X2 == X1 && n2 == n1) ? d1 : upload(X2, (size_t)n2 * p);
+    double* dK = ctx.arena.alloc_n<double>((size_t)n1 * n2);
+    kernel_matrix_device(d1, n1, d2, n2, p, kernel, gamma, degree, coef0, dK);
+    download(K, dK, (size_t)n1 * n2);
+    ctx.sync();
+  });
+}
+
+int fpls_center_kernel_train(const double* K, int n, double* Kc, double* col_means, double* grand_mean, char* err,
+                             size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0, "K must be non-empty");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    double* dK = upload(K, (size_t)n * n);
+    double* dcm = ctx.arena.alloc_n<double>(n);
+    double* dg = ctx.arena.alloc_n<double>(1);
+    center_kernel_train_device(dK, n, dcm, dg);
+    download(Kc, dK, (size_t)n * n);
+    download(col_means, dcm, n);
+    download(grand_mean, dg, 1);
+    ctx.sync();
+  });
+}
+
+int fpls_center_kernel_test(const double* Ktest, int nt, int n, const double* col_means, double grand_mean,
+                            double* Kc, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(nt > 0 && n > 0, "Ktest must be non-empty");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    double* dK = upload(Ktest, (size_t)nt * n);
+    const double* dcm = upload(col_means, n);
+    const double* dg = upload(&grand_mean, 1);
+    center_kernel_test_device(dK, nt, n, dcm, dg);
+    download(Kc, dK, (size_t)nt * n);
+    ctx.sync();
+  });
+}
+
+int fpls_kernel_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, const int* ncomp, int L,
+                                int scaling, int kernel, double gamma, int degree, double coef0, int fit,
+                                int seed, double* R, double* Q, double* mK, double* vK, double* mY, double* B,
+                                double* Yfit, double* R2Y, int* n_components, double* mX, double* vX,
+                                double* col_means, double* grand_mean, double* gamma_used, char* err,
+                                size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && m > 0, "kernel PLS requires non-empty X and Y");
+    FPLS_REQUIRE(kernel >= 1 && kernel <= 3, "Unknown kernel id");
+    FPLS_REQUIRE(scaling >= 1 && scaling <= 3, "scaling must be 1, 2 or 3");
+    const double g = gamma > 0.0 ? gamma : 1.0 / std::max(1, p);   // .kernel_pls_gamma: NULL -> 1 / p
+    FPLS_REQUIRE(std::isfinite(g), "gamma must be a finite positive number");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    double* dX = upload(X, (size_t)n * p);
+    double* dmX = ctx.arena.alloc_n<double>(p);
+    double* dvX = ctx.arena.alloc_n<double>(p);
+    preprocess_kernel_x_device(dX, n, p, scaling, dmX, dvX);
+    double* dK = ctx.arena.alloc_n<double>((size_t)n * n);
+    kernel_matrix_device(dX, n, dX, n, p, kernel, g, degree, coef0, dK);
+    double* dcm = ctx.arena.alloc_n<double>(n);
+    double* dg = ctx.arena.alloc_n<double>(1);
+    center_kernel_train_device(dK, n, dcm, dg);
+    download(mX, dmX, p);
+    download(vX, dvX, p);
+    download(col_means, dcm, n);
+    download(grand_mean, dg, 1);
+    if (gamma_used) *gamma_used = g;
+    double* dY = upload(Y, (size_t)n * m);
+    // The inner fit runs on the centred kernel with scaling "none" (R/main.R:2875-2891).
+    simpls_fast_on_device(dK, n, n, dY, m, ncomp, L, 3, fit, seed, R, Q, mK, vK, mY, B, Yfit, R2Y, n_components);
   });
 }
 

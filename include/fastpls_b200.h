@@ -186,6 +186,42 @@ int fpls_lda_project_predict(const double* X, int w, int p, const double* R, int
                              const double* constants, int n_classes, int* labels,
                              double* scores, char* err, size_t errlen);
 
+/* Kernel matrix K (n1 x n2) between the rows of X1 (n1 x p) and X2 (n2 x p):
+ * kernel 1 linear x.y; 2 RBF exp(-gamma |x - y|^2) (tiny negative distances
+ * above -1e-10 set to 0); 3 polynomial (gamma x.y + coef0)^degree.  FP64; the
+ * dot products run on the FP64 tensor cores.
+ * Replaces kernel_matrix_cpp (RcppExports.cpp; fastPLS.cpp:4314-4340). */
+int fpls_kernel_matrix(const double* X1, int n1, const double* X2, int n2, int p, int kernel, double gamma,
+                       int degree, double coef0, double* K, char* err, size_t errlen);
+
+/* Double centring of a training kernel K (n x n): Kc = ((K - col_means) -
+ * row_means) + grand_mean, with col_means (n) and grand_mean returned.
+ * Replaces center_kernel_train_cpp (fastPLS.cpp:4344-4357). */
+int fpls_center_kernel_train(const double* K, int n, double* Kc, double* col_means, double* grand_mean,
+                             char* err, size_t errlen);
+
+/* Centring of a test kernel Ktest (nt x n) with the training col_means and
+ * grand_mean and its own row means.
+ * Replaces center_kernel_test_cpp (fastPLS.cpp:4360-4375). */
+int fpls_center_kernel_test(const double* Ktest, int nt, int n, const double* col_means, double grand_mean,
+                            double* Kc, char* err, size_t errlen);
+
+/* Kernel PLS fit on the device in one call: the preprocessing of X (scaling
+ * 1 centre, 2 autoscale with sd 0 -> 1, 3 none; mX, vX (p) returned), the
+ * kernel matrix of the preprocessed rows (gamma <= 0 selects 1 / p, the value
+ * used is returned), its double centring (col_means (n), grand_mean), and the
+ * fast SIMPLS fit on the centred kernel with scaling "none" (outputs as
+ * fpls_pls_model2_fast with p = n: R (n x kmax), Q, mK, vK (n), mY, B, Yfit,
+ * R2Y, n_components).  The R route .kernel_pls_fit (R/main.R:2826-2917) calls
+ * kernel_matrix_cpp, center_kernel_train_cpp and the GPU fit one after another
+ * through host memory. */
+int fpls_kernel_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, const int* ncomp, int L,
+                                int scaling, int kernel, double gamma, int degree, double coef0, int fit,
+                                int seed, double* R, double* Q, double* mK, double* vK, double* mY, double* B,
+                                double* Yfit, double* R2Y, int* n_components, double* mX, double* vX,
+                                double* col_means, double* grand_mean, double* gamma_used, char* err,
+                                size_t errlen);
+
 /* C (M x N) = A (M x K) * B (K x N) through the BF16 split-precision tensor-core
  * path (hi/lo three-product tcgen05 GEMM, FP32 accumulation, FP64 reduction of
  * the K-split partials).  A diagnostic of the mixed-precision kernel; it has no

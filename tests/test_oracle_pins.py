@@ -229,3 +229,19 @@ def test_xprod_oracle_equals_materialized():
     c = ox.pls_model2_fast_xprod(X, Y, [2, 5, 9], seed=3)
     e = opls.pls_model2_fast(X, Y, [2, 5, 9], seed=3)
     assert np.linalg.norm(c["B"] - e["B"]) < 1e-10 * np.linalg.norm(e["B"])
+
+
+def test_kernel_oracle_properties():
+    # centring a linear kernel equals the Gram of the column-centred rows; an
+    # RBF kernel has a unit diagonal and is symmetric; centred test kernels of
+    # the training rows reproduce the centred training kernel
+    from oracle import kernel as ok
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((40, 7))
+    Xc = X - X.mean(axis=0)
+    kc = ok.center_kernel_train(ok.kernel_matrix(X, X, 1, 1.0, 1, 0.0))
+    assert np.allclose(kc["K"], Xc @ Xc.T, atol=1e-12)
+    K = ok.kernel_matrix(X, X, 2, 0.2, 3, 1.0)
+    assert np.allclose(np.diag(K), 1.0) and np.allclose(K, K.T)
+    kc = ok.center_kernel_train(K)
+    assert np.allclose(ok.center_kernel_test(K, kc["col_means"], kc["grand_mean"]), kc["K"], atol=1e-12)

@@ -117,7 +117,8 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
                   int a_rows_pad, int b_rows_pad, const double* __restrict__ sA,
                   const double* __restrict__ sB, const int4* __restrict__ segs,
                   const int* __restrict__ cta_seg_begin, const int* __restrict__ tile_seg, int n_tiles_n,
-                  double* __restrict__ part, double* __restrict__ C, int ldc, int M, int N, int* err) {
+                  double* __restrict__ part, double* __restrict__ C, int ldc, int M, int N, int* err,
+                  int a_static) {
   __shared__ int epi_fail;   // raised by any epilogue warp whose wait gave up
   using L = OzLayout<S>;
   extern __shared__ uint8_t smem_raw[];
@@ -164,6 +165,19 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
+  // With a_static the A planes were written before the previous kernel ran,
+  // so the first K block's A planes are requested before waiting for it.
+  const bool pre_a = a_static && warp == 0 && lane == 0 && sbeg < send;
+  if (pre_a) {
+    const int4 seg = segs[sbeg];
+    const int mt = seg.x / n_tiles_n;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const uint32_t fa = smem_u32(&fullA[s]);
+      mbar_expect_tx(fa, A_PLANE);
+      tma_load_2d(&mA, smem_u32(sa + s * A_PLANE), fa, seg.y * OBK, s * a_rows_pad + mt * OBM);
+    }
+  }
   // The set-up above overlaps the previous kernel; its outputs (the B planes
   // and scales) are read only after it has completed.
   tc::grid_dep_wait();
@@ -175,7 +189,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
     int b_loads = 0;    // B sets issued (iterations 0 .. b_loads - 1)
     int a_last[S];      // last iteration whose plane s was issued, or -1
 #pragma unroll
-    for (int s = 0; s < S; ++s) a_last[s] = -1;
+    for (int s = 0; s < S; ++s) a_last[s] = pre_a ? 0 : -1;
     bool ok = true;
     for (int sg = sbeg; sg < send && ok; ++sg) {
       const int4 seg = segs[sg];
@@ -191,7 +205,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
         b_loads = it + 1;
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-          if (!ok) break;
+          if (!ok || (pre_a && it == 0)) break;   // first block's A planes already requested
           if (!mbar_wait(smem_u32(&emptyA[s]), (it & 1) ^ 1, err)) { ok = false; break; }
           const uint32_t fa = smem_u32(&fullA[s]);
           mbar_expect_tx(fa, A_PLANE);
@@ -283,15 +297,24 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
 #pragma unroll
         for (int l = 0; l < S; ++l) tc::tmem_ld16_raw(base + static_cast<uint32_t>(l * OBN + c * 16), v[l]);
         tc::tmem_wait_ld();
+        // Levels three at a time, exactly in int64 (v_l 2^14 + v_{l+1} 2^7 +
+        // v_{l+2} < 2^46), then one conversion and one scaling per group,
+        // smallest group first.
         double acc[16];
 #pragma unroll
         for (int x = 0; x < 16; ++x) acc[x] = 0.0;
-        // smallest level first
 #pragma unroll
-        for (int l = S - 1; l >= 0; --l) {
-          const double w = pow2i(-7 * (l + 2));
+        for (int g = (S - 1) / 3; g >= 0; --g) {
+          const int l0 = 3 * g, l1 = (3 * g + 2 < S - 1) ? 3 * g + 2 : S - 1;
+          const double w = pow2i(-7 * (l1 + 2));
 #pragma unroll
-          for (int x = 0; x < 16; ++x) acc[x] += static_cast<double>(static_cast<int32_t>(v[l][x])) * w;
+          for (int x = 0; x < 16; ++x) {
+            long long q = 0;
+#pragma unroll
+            for (int l = l0; l <= l1; ++l)
+              q += static_cast<long long>(static_cast<int32_t>(v[l][x])) << (7 * (l1 - l));
+            acc[x] += static_cast<double>(q) * w;
+          }
         }
         if (whole && C) {
           if (row < M) {
@@ -497,7 +520,7 @@ CUtensorMap make_plane_map(const OzakiPlanes& p, int box_rows) {
 
 template <int S>
 void launch_ozaki(const CUtensorMap& mA, const CUtensorMap& mB, const OzakiPlanes& A, const OzakiPlanes& B,
-                  const OzCached& c, double* C, int ldc, int* err, cudaStream_t st) {
+                  const OzCached& c, double* C, int ldc, int* err, cudaStream_t st, bool a_static) {
   static bool attr = false;
   if (!attr) {
     FPLS_CUDA(cudaFuncSetAttribute(ozaki_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -518,7 +541,8 @@ void launch_ozaki(const CUtensorMap& mA, const CUtensorMap& mB, const OzakiPlane
   FPLS_CUDA(cudaLaunchKernelEx(&lc, ozaki_gemm_kernel<S>, mA, mB, a_rows_pad, b_rows_pad,
                                static_cast<const double*>(A.scale), static_cast<const double*>(B.scale),
                                static_cast<const int4*>(c.segs), static_cast<const int*>(c.cta_begin),
-                               static_cast<const int*>(c.tile_begin), ntn, c.part, C, ldc, m_rows, n_rows, err));
+                               static_cast<const int*>(c.tile_begin), ntn, c.part, C, ldc, m_rows, n_rows, err,
+                               a_static ? 1 : 0));
 }
 
 struct XOperatorOzakiSym : public XOperator {
@@ -533,13 +557,13 @@ struct XOperatorOzakiSym : public XOperator {
   void times(const double* M, int F, double* U) override {
     OzakiPlanes b = ozaki_alloc(F, n, slices);
     ozaki_split(M, n, b);
-    ozaki_gemm(kp, b, U, n);
+    ozaki_gemm(kp, b, U, n, true);
   }
   void t_times(const double* M, int F, double* U) override { times(M, F, U); }
   OzakiPartials times_partials(const double* M, int F) {
     OzakiPlanes b = ozaki_alloc(F, n, slices);
     ozaki_split(M, n, b);
-    return ozaki_gemm_partials(kp, b);
+    return ozaki_gemm_partials(kp, b, true);
   }
   void gram(double*) override { throw Error(kErrArgument, "the INT8 product operator has no Gram"); }
 };
@@ -574,7 +598,7 @@ namespace {
 
 // Runs the product kernel: whole tiles straight to C (when C is given), the
 // others as partials in the cached plan.
-const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc) {
+const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc, bool a_static) {
   FPLS_REQUIRE(A.slices == B.slices && A.k == B.k && A.ldk == B.ldk, "INT8 products: operands do not match");
   Context& ctx = Context::get();
   cudaStream_t st = ctx.stream;
@@ -583,10 +607,10 @@ const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C,
   const CUtensorMap mB = make_plane_map(B, OBN);
   int* err = ctx.d_status + 16;
   switch (A.slices) {
-    case 4: launch_ozaki<4>(mA, mB, A, B, c, C, ldc, err, st); break;
-    case 5: launch_ozaki<5>(mA, mB, A, B, c, C, ldc, err, st); break;
-    case 6: launch_ozaki<6>(mA, mB, A, B, c, C, ldc, err, st); break;
-    default: launch_ozaki<7>(mA, mB, A, B, c, C, ldc, err, st); break;
+    case 4: launch_ozaki<4>(mA, mB, A, B, c, C, ldc, err, st, a_static); break;
+    case 5: launch_ozaki<5>(mA, mB, A, B, c, C, ldc, err, st, a_static); break;
+    case 6: launch_ozaki<6>(mA, mB, A, B, c, C, ldc, err, st, a_static); break;
+    default: launch_ozaki<7>(mA, mB, A, B, c, C, ldc, err, st, a_static); break;
   }
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
@@ -595,16 +619,16 @@ const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C,
 
 }  // namespace
 
-void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc) {
-  const OzCached& c = run_ozaki(A, B, C, ldc);
+void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc, bool a_static) {
+  const OzCached& c = run_ozaki(A, B, C, ldc, a_static);
   ozaki_reduce_kernel<<<c.g.tiles * kReducePieces, 256, 0, Context::get().stream>>>(c.part, c.tile_begin, c.g.ntn,
                                                                                  A.rows, B.rows, C, ldc);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 
-OzakiPartials ozaki_gemm_partials(const OzakiPlanes& A, const OzakiPlanes& B) {
-  const OzCached& c = run_ozaki(A, B, nullptr, 0);
+OzakiPartials ozaki_gemm_partials(const OzakiPlanes& A, const OzakiPlanes& B, bool a_static) {
+  const OzCached& c = run_ozaki(A, B, nullptr, 0, a_static);
   OzakiPartials p;
   p.part = c.part;
   p.tile_seg = c.tile_begin;
@@ -624,7 +648,7 @@ std::unique_ptr<XOperator> make_ozaki_sym_operator(const double* K, int n, int s
 OzakiPartials ozaki_sym_partials_from_planes(XOperator& op, const OzakiPlanes& b) {
   auto* oz = dynamic_cast<XOperatorOzakiSym*>(&op);
   FPLS_REQUIRE(oz != nullptr, "INT8 partial products need the INT8 operator");
-  return ozaki_gemm_partials(oz->kp, b);
+  return ozaki_gemm_partials(oz->kp, b, true);
 }
 
 OzakiPartials ozaki_sym_times_partials(XOperator& op, const double* M, int F) {

@@ -36,7 +36,9 @@ void ozaki_split(const double* X, int ldx, const OzakiPlanes& out);
 // with the same slice count and contraction length.  The digit pairs whose
 // levels s + t exceed slices + 1 are dropped; the result differs from the
 // exact product by at most about 3 k 2^(eA_i + eB_j - 7 slices) per entry.
-void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc);
+// a_static: A's planes were written before the kernel launched just before
+// this product (so their loads may start before waiting for that kernel).
+void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc, bool a_static = false);
 
 // The same product left as FP64 stream-K partials for a consumer that sums
 // them (in segment order) while it reads C: entry (i, j) of C is
@@ -48,7 +50,7 @@ struct OzakiPartials {
   const int* tile_seg = nullptr;
   int n_tiles_n = 0;
 };
-OzakiPartials ozaki_gemm_partials(const OzakiPlanes& A, const OzakiPlanes& B);
+OzakiPartials ozaki_gemm_partials(const OzakiPlanes& A, const OzakiPlanes& B, bool a_static = false);
 
 // Releases the cached stream-K plans (fpls_reset_workspace).
 void ozaki_release_cache();

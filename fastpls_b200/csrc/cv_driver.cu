@@ -120,6 +120,8 @@ __global__ void pred_counts_kernel(const int* __restrict__ pred, int L, int n, c
 
 // Class predictions of the test rows of every fit for every ncomp slice from the
 // kept scores: y_a = sum_{b<=a} (t_b[i] / ||t_b||) q_b + mY_f, label = first argmax.
+// MB bounds the class count so that the running scores stay in registers.
+template <int MB>
 __global__ void cv_predict_kernel(int F, int n, int m, int K, int L, const int* __restrict__ ncomp,
                                   const uint8_t* __restrict__ test, const int* __restrict__ group,
                                   const double* __restrict__ Tkeep, const double* __restrict__ tnorm,
@@ -130,20 +132,26 @@ __global__ void cv_predict_kernel(int F, int n, int m, int K, int L, const int* 
   if (i >= n || !test[(size_t)f * n + i]) return;
   const int done = ncomp_done[f];
   const int g = group[f];
-  double y[kMaxClassesCv];
-  for (int j = 0; j < m; ++j) y[j] = 0.0;
+  double y[MB];
+#pragma unroll
+  for (int j = 0; j < MB; ++j) y[j] = 0.0;
   const double* Qf = Q + (size_t)f * m * K;
+  const double* mf = mYf + (size_t)f * m;
   for (int a = 0; a < K; ++a) {
     if (a < done) {
       const double c = Tkeep[((size_t)f * K + a) * n + i] / tnorm[(size_t)f * K + a];
-      for (int j = 0; j < m; ++j) y[j] += c * Qf[j + (size_t)a * m];
+#pragma unroll
+      for (int j = 0; j < MB; ++j)
+        if (j < m) y[j] += c * Qf[j + (size_t)a * m];
     }
     for (int s = 0; s < L; ++s) {
       if (ncomp[s] != a + 1) continue;
       int best = 0;
-      double bv = y[0] + mYf[(size_t)f * m];
-      for (int j = 1; j < m; ++j) {
-        const double v = y[j] + mYf[(size_t)f * m + j];
+      double bv = y[0] + mf[0];
+#pragma unroll
+      for (int j = 1; j < MB; ++j) {
+        if (j >= m) break;
+        const double v = y[j] + mf[j];
         if (v > bv) { bv = v; best = j; }
       }
       pred[((size_t)g * L + s) * n + i] = best + 1;
@@ -438,8 +446,15 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
     pt.mark("simpls");
   }
   int* d_pred = res.d_pred;
-  cv_predict_kernel<<<dim3(ceil_div(n, 128), Fa), 128, 0, ctx.stream>>>(
-      Fa, n, m, K, L, d_nc, d_te, d_grp, Tko, tno, Qo, ncd, d_mYf, d_pred); ::fpls::note_launch();
+  const dim3 pgrid(ceil_div(n, 128), Fa);
+  if (m <= 8)
+    cv_predict_kernel<8><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_te, d_grp, Tko, tno, Qo, ncd, d_mYf, d_pred);
+  else if (m <= 32)
+    cv_predict_kernel<32><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_te, d_grp, Tko, tno, Qo, ncd, d_mYf, d_pred);
+  else
+    cv_predict_kernel<kMaxClassesCv><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_te, d_grp, Tko, tno, Qo, ncd,
+                                                                    d_mYf, d_pred);
+  ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   pt.mark("predict");
   std::vector<int> done(Fa);

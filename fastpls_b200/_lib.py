@@ -100,6 +100,11 @@ SIGNATURES = {
     "fpls_x_free": ([_I, _C, _S], ctypes.c_int),
     "fpls_double_cv_resident": ([_I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I, _I, _I, _I,
                                  _IP, _DP, _IP, _IP, _IP, _C, _S], ctypes.c_int),
+    "fpls_double_cv_outer_subset": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _IP, _I,
+                                     _IP, _I, _I, _I, _I, _I, _I, _IP, _DP, _IP, _IP, _IP, _C, _S],
+                                    ctypes.c_int),
+    "fpls_double_cv_resident_outer_subset": ([_I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I, _I,
+                                              _I, _I, _IP, _DP, _IP, _IP, _IP, _C, _S], ctypes.c_int),
     "fpls_launch_count": ([], ctypes.c_longlong),
     "fpls_last_call_ms": ([], ctypes.c_double),
     "fpls_profile": ([_I, _DP, ctypes.POINTER(ctypes.c_longlong), _DP, _C, _S], ctypes.c_int),
@@ -533,11 +538,7 @@ def cv_predict(X, y, fold, ncomp, n_classes, method=3, scaling=1, seed=1, precis
     return dict(class_pred=cp, status=st)
 
 
-def double_cv(X, y, outer_fold, inner_fold, ncomp, n_classes, scaling=1, seed=1, run=1,
-              precision="fp64", batched=True, return_inner=False):
-    """Double CV of SIMPLS PLS-DA over the supplied outer/inner folds (0-based)."""
-    Xa, is32 = _x_arg(X)
-    n, p = Xa.shape
+def _double_cv_args(n, y, outer_fold, inner_fold, ncomp, return_inner, outer_ids):
     yy = _i32(y)
     of = _i32(outer_fold)
     inf_ = np.asfortranarray(np.asarray(inner_fold, dtype=np.int32))
@@ -545,20 +546,43 @@ def double_cv(X, y, outer_fold, inner_fold, ncomp, n_classes, scaling=1, seed=1,
     Ki = int(inf_.max()) + 1
     nc = _i32(np.atleast_1d(ncomp))
     L = nc.size
-    best = np.zeros(Ko, dtype=np.int32)
-    acc = _out(Ko, L)
-    pred = np.zeros(n, dtype=np.int32)
-    inner = np.zeros((n, L, Ko), dtype=np.int32, order="F") if return_inner else None
-    fst = np.zeros(Ko * Ki + Ko, dtype=np.int32)
-    _call("fpls_double_cv", Xa.ctypes.data, is32, n, p, _p(yy), int(n_classes), _p(of), Ko,
-          inf_.ctypes.data_as(_c_int_p), Ki, _p(nc), L, int(scaling), int(seed), int(run),
-          PREC[precision], int(bool(batched)), _p(best), _p(acc), _p(pred),
-          None if inner is None else inner.ctypes.data_as(_c_int_p), _p(fst))
-    out = dict(best_comp=best, inner_accuracy=acc, pred=pred, fit_status=fst,
-               accuracy=float(np.mean(pred == yy)))
+    ids = None if outer_ids is None else _i32(outer_ids)
+    outs = dict(best_comp=np.zeros(Ko, dtype=np.int32), inner_accuracy=_out(Ko, L),
+                pred=np.zeros(n, dtype=np.int32), fit_status=np.zeros(Ko * Ki + Ko, dtype=np.int32))
     if return_inner:
-        out["inner_pred"] = inner
-    return out
+        outs["inner_pred"] = np.zeros((n, L, Ko), dtype=np.int32, order="F")
+    return yy, of, inf_, Ko, Ki, nc, L, ids, outs
+
+
+def _double_cv_result(outs, yy, ids, of):
+    pred = outs["pred"]
+    rows = np.ones(pred.size, dtype=bool) if ids is None else np.isin(of, ids)
+    outs["accuracy"] = float(np.mean(pred[rows] == yy[rows])) if rows.any() else float("nan")
+    return outs
+
+
+def double_cv(X, y, outer_fold, inner_fold, ncomp, n_classes, scaling=1, seed=1, run=1,
+              precision="fp64", batched=True, return_inner=False, outer_ids=None):
+    """Double CV of SIMPLS PLS-DA over the supplied outer/inner folds (0-based).
+
+    outer_ids restricts the call to those outer folds (fpls_double_cv_outer_subset):
+    only their entries of the outputs are written, the rest stay zero, and
+    `accuracy` is taken over their rows."""
+    Xa, is32 = _x_arg(X)
+    n, p = Xa.shape
+    yy, of, inf_, Ko, Ki, nc, L, ids, o = _double_cv_args(n, y, outer_fold, inner_fold, ncomp,
+                                                          return_inner, outer_ids)
+    inner = o.get("inner_pred")
+    tail = (_p(nc), L, int(scaling), int(seed), int(run), PREC[precision], int(bool(batched)),
+            _p(o["best_comp"]), _p(o["inner_accuracy"]), _p(o["pred"]),
+            None if inner is None else inner.ctypes.data_as(_c_int_p), _p(o["fit_status"]))
+    head = (Xa.ctypes.data, is32, n, p, _p(yy), int(n_classes), _p(of), Ko,
+            inf_.ctypes.data_as(_c_int_p), Ki)
+    if ids is None:
+        _call("fpls_double_cv", *head, *tail)
+    else:
+        _call("fpls_double_cv_outer_subset", *head, _p(ids), ids.size, *tail)
+    return _double_cv_result(o, yy, ids, of)
 
 
 def x_upload(X):
@@ -574,28 +598,20 @@ def x_free(handle):
 
 
 def double_cv_resident(handle, n, y, outer_fold, inner_fold, ncomp, n_classes, scaling=1, seed=1,
-                       run=1, precision="fp64", batched=True, return_inner=False):
-    yy = _i32(y)
-    of = _i32(outer_fold)
-    inf_ = np.asfortranarray(np.asarray(inner_fold, dtype=np.int32))
-    Ko = int(of.max()) + 1
-    Ki = int(inf_.max()) + 1
-    nc = _i32(np.atleast_1d(ncomp))
-    L = nc.size
-    best = np.zeros(Ko, dtype=np.int32)
-    acc = _out(Ko, L)
-    pred = np.zeros(n, dtype=np.int32)
-    inner = np.zeros((n, L, Ko), dtype=np.int32, order="F") if return_inner else None
-    fst = np.zeros(Ko * Ki + Ko, dtype=np.int32)
-    _call("fpls_double_cv_resident", int(handle), _p(yy), int(n_classes), _p(of), Ko,
-          inf_.ctypes.data_as(_c_int_p), Ki, _p(nc), L, int(scaling), int(seed), int(run),
-          PREC[precision], int(bool(batched)), _p(best), _p(acc), _p(pred),
-          None if inner is None else inner.ctypes.data_as(_c_int_p), _p(fst))
-    out = dict(best_comp=best, inner_accuracy=acc, pred=pred, fit_status=fst,
-               accuracy=float(np.mean(pred == yy)))
-    if return_inner:
-        out["inner_pred"] = inner
-    return out
+                       run=1, precision="fp64", batched=True, return_inner=False, outer_ids=None):
+    """double_cv on a registered predictor matrix (x_upload)."""
+    yy, of, inf_, Ko, Ki, nc, L, ids, o = _double_cv_args(n, y, outer_fold, inner_fold, ncomp,
+                                                          return_inner, outer_ids)
+    inner = o.get("inner_pred")
+    tail = (_p(nc), L, int(scaling), int(seed), int(run), PREC[precision], int(bool(batched)),
+            _p(o["best_comp"]), _p(o["inner_accuracy"]), _p(o["pred"]),
+            None if inner is None else inner.ctypes.data_as(_c_int_p), _p(o["fit_status"]))
+    head = (int(handle), _p(yy), int(n_classes), _p(of), Ko, inf_.ctypes.data_as(_c_int_p), Ki)
+    if ids is None:
+        _call("fpls_double_cv_resident", *head, *tail)
+    else:
+        _call("fpls_double_cv_resident_outer_subset", *head, _p(ids), ids.size, *tail)
+    return _double_cv_result(o, yy, ids, of)
 
 
 def launch_count():

@@ -861,32 +861,57 @@ int fpls_cv_predict(const void* X, int x_is_float32, int n, int p, const int* y,
   });
 }
 
+// One double CV over the outer folds in outer_ids (all of them, in order, when
+// outer_ids is null).  Slot s of the batched grid runs outer fold ids[s]: its
+// inner fits are s*Ki .. s*Ki + Ki-1, its refit S*Ki + s, and every output is
+// written at the outer fold's own index, so the outputs of disjoint fold lists
+// are disjoint and the union of their calls equals one call over all folds.
 static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, int n, int p,
                            const int* y, int n_classes, const int* outer_fold, int kfold_outer,
-                           const int* inner_fold, int kfold_inner, const int* ncomp, int L,
-                           int scaling, int seed, int run, int precision, int batched,
-                           int* best_comp, double* inner_accuracy, int* outer_pred,
+                           const int* inner_fold, int kfold_inner, const int* outer_ids, int n_ids,
+                           const int* ncomp, int L, int scaling, int seed, int run, int precision,
+                           int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
                            int* inner_pred, int* fit_status) {
   {
     FPLS_REQUIRE(n >= 2 && p > 0, "Xdata must contain at least two samples");
     FPLS_REQUIRE(kfold_outer >= 1 && kfold_inner >= 1 && L >= 1, "fold counts and ncomp must be >= 1");
+    const int Ko = kfold_outer, Ki = kfold_inner;
+    std::vector<int> ids;
+    if (outer_ids) {
+      FPLS_REQUIRE(n_ids >= 1 && n_ids <= Ko, "outer fold list must hold 1..kfold_outer ids");
+      std::vector<uint8_t> seen(Ko, 0);
+      for (int s = 0; s < n_ids; ++s) {
+        const int o = outer_ids[s];
+        FPLS_REQUIRE(o >= 0 && o < Ko, "outer fold ids must be in 0..kfold_outer-1");
+        FPLS_REQUIRE(!seen[o], "outer fold list holds a fold twice");
+        seen[o] = 1;
+        ids.push_back(o);
+      }
+    } else {
+      for (int o = 0; o < Ko; ++o) ids.push_back(o);
+    }
+    const int S = static_cast<int>(ids.size());
     Context& ctx = Context::get();
     ctx.begin_call();
     PhaseTimer pt("double CV call");
-    const int Ko = kfold_outer, Ki = kfold_inner;
     std::vector<int> nc(ncomp, ncomp + L);
     for (int& c : nc) c = std::max(1, c);
     CvFitSet fs;
-    fs.n = n; fs.p = p; fs.m = n_classes; fs.F = Ko * Ki + Ko; fs.G = Ko + 1;
+    fs.n = n; fs.p = p; fs.m = n_classes; fs.F = S * Ki + S; fs.G = S + 1;
     fs.train.assign((size_t)fs.F * n, 0);
     fs.test.assign((size_t)fs.F * n, 0);
     fs.group.assign(fs.F, 0);
     fs.seeds.resize(fs.F);
-    std::vector<int> outer_classes(Ko, 0), fallback(Ko, 1);
+    std::vector<int> outer_classes(S, 0), fallback(S, 1);
     const int m = n_classes;
     FPLS_REQUIRE(m >= 1, "n_classes must be >= 1");
     for (int i = 0; i < n; ++i)
       FPLS_REQUIRE(y[i] >= 1 && y[i] <= m, "labels must be in 1..n_classes");
+    // Slot of every row: s when the row belongs to outer fold ids[s], else -1.
+    std::vector<int> slot_of_fold(Ko, -1), row_slot(n, -1);
+    for (int s = 0; s < S; ++s) slot_of_fold[ids[s]] = s;
+    for (int i = 0; i < n; ++i)
+      if (outer_fold[i] >= 0 && outer_fold[i] < Ko) row_slot[i] = slot_of_fold[outer_fold[i]];
     // Fold masks and training-row class counts from per-fold histograms: the
     // rows outside outer fold o, split by inner fold id and class, give every
     // inner fit's counts by subtraction (no pass per fit over the masks).
@@ -895,7 +920,8 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     fs.n_test.assign(fs.F, 0);
     std::vector<uint8_t> keep(n);
     std::vector<int> outer_cnt(m), inner_cnt((size_t)Ki * m);
-    for (int o = 0; o < Ko; ++o) {
+    for (int s = 0; s < S; ++s) {
+      const int o = ids[s];
       const int* inner_o = inner_fold + (size_t)o * n;
       std::fill(outer_cnt.begin(), outer_cnt.end(), 0);
       std::fill(inner_cnt.begin(), inner_cnt.end(), 0);
@@ -909,14 +935,14 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
       }
       int best = 0;
       for (int c = 0; c < m; ++c) {
-        if (outer_cnt[c] > 0) outer_classes[o]++;
+        if (outer_cnt[c] > 0) outer_classes[s]++;
         if (outer_cnt[c] > outer_cnt[best]) best = c;
       }
-      fallback[o] = best + 1;
-      const bool skip = outer_classes[o] < 2;  // pls.double.cv's single-class fallback
+      fallback[s] = best + 1;
+      const bool skip = outer_classes[s] < 2;  // pls.double.cv's single-class fallback
       for (int i0 = 0; i0 < Ki; ++i0) {
-        const int f = o * Ki + i0;
-        fs.group[f] = o;
+        const int f = s * Ki + i0;
+        fs.group[f] = s;
         fs.seeds[f] = static_cast<unsigned>(seed + 1000 * run + (o + 1) + i0);
         if (skip) continue;
         uint8_t* tr = fs.train.data() + (size_t)f * n;
@@ -936,8 +962,8 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
         fs.n_train[f] = ntr;
         fs.n_test[f] = nte;
       }
-      const int f = Ko * Ki + o;
-      fs.group[f] = Ko;
+      const int f = S * Ki + s;
+      fs.group[f] = S;
       fs.seeds[f] = static_cast<unsigned>(seed + 2000 * run + (o + 1));
       if (skip) continue;
       uint8_t* tr = fs.train.data() + (size_t)f * n;
@@ -959,36 +985,53 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     // Inner accuracy per (outer fold, ncomp) on the device; the chosen ncomp is the
     // first maximum (.cv_best_index); only counts and the outer predictions return.
     const int* d_y = upload(y, n);
-    const int* d_outer = upload(outer_fold, n);
+    const int* d_slot = upload(row_slot.data(), n);
     std::vector<long long> cnts;
-    cv_prediction_counts(res.d_pred, Ko, L, n, d_y, d_outer, cnts);
+    cv_prediction_counts(res.d_pred, S, L, n, d_y, d_slot, cnts);
     pt.mark("counts");
-    std::vector<int> best_slice(Ko, 0), fb(Ko, 0);
-    for (int o = 0; o < Ko; ++o) {
+    std::vector<int> best_slice(S, 0), fb(S, 0);
+    for (int s = 0; s < S; ++s) {
+      const int o = ids[s];
       int bi = 0;
       double bv = -1.0;
       bool any = false;
-      for (int s = 0; s < L; ++s) {
-        const long long ok = cnts[2 * ((size_t)o * L + s)], tot = cnts[2 * ((size_t)o * L + s) + 1];
+      for (int l = 0; l < L; ++l) {
+        const long long ok = cnts[2 * ((size_t)s * L + l)], tot = cnts[2 * ((size_t)s * L + l) + 1];
         const double acc = tot ? static_cast<double>(ok) / tot : std::nan("");
-        if (inner_accuracy) inner_accuracy[o + (size_t)s * Ko] = acc;
-        if (std::isfinite(acc) && (!any || acc > bv)) { bv = acc; bi = s; any = true; }
+        if (inner_accuracy) inner_accuracy[o + (size_t)l * Ko] = acc;
+        if (std::isfinite(acc) && (!any || acc > bv)) { bv = acc; bi = l; any = true; }
       }
-      const bool skip = outer_classes[o] < 2;
-      best_slice[o] = bi;
-      fb[o] = skip ? fallback[o] : 0;
+      const bool skip = outer_classes[s] < 2;
+      best_slice[s] = bi;
+      fb[s] = skip ? fallback[s] : 0;
       if (best_comp) best_comp[o] = skip ? *std::min_element(nc.begin(), nc.end()) : nc[bi];
     }
-    int* d_best = upload(best_slice.data(), Ko);
-    int* d_fb = upload(fb.data(), Ko);
+    int* d_best = upload(best_slice.data(), S);
+    int* d_fb = upload(fb.data(), S);
     int* d_out = ctx.arena.alloc_n<int>(n);
-    gather_outer_pred_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(res.d_pred, d_outer, d_best, d_fb, Ko, L, n, d_out); ::fpls::note_launch();
+    gather_outer_pred_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(res.d_pred, d_slot, d_best, d_fb, S, L, n, d_out); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
-    download(outer_pred, d_out, n);
-    if (inner_pred) download(inner_pred, res.d_pred, (size_t)Ko * L * n);
+    std::vector<int> pred_all;
+    if (outer_ids) {
+      pred_all.resize(n);
+      download(pred_all.data(), d_out, n);
+      if (inner_pred)
+        for (int s = 0; s < S; ++s)
+          download(inner_pred + (size_t)ids[s] * L * n, res.d_pred + (size_t)s * L * n, (size_t)L * n);
+    } else {
+      download(outer_pred, d_out, n);
+      if (inner_pred) download(inner_pred, res.d_pred, (size_t)Ko * L * n);
+    }
     pt.mark("ncomp + outer");
     ctx.sync();
-    if (fit_status) std::copy(res.status.begin(), res.status.end(), fit_status);
+    if (outer_ids)
+      for (int i = 0; i < n; ++i)
+        if (row_slot[i] >= 0) outer_pred[i] = pred_all[i];
+    if (fit_status)
+      for (int s = 0; s < S; ++s) {
+        for (int i0 = 0; i0 < Ki; ++i0) fit_status[(size_t)ids[s] * Ki + i0] = res.status[(size_t)s * Ki + i0];
+        fit_status[(size_t)Ko * Ki + ids[s]] = res.status[(size_t)S * Ki + s];
+      }
     }
 }
 
@@ -999,8 +1042,23 @@ int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, 
                    int* inner_pred, int* fit_status, char* err, size_t errlen) {
   return guarded(err, errlen, [&] {
     double_cv_impl(X, x_is_float32, false, n, p, y, n_classes, outer_fold, kfold_outer, inner_fold,
-                   kfold_inner, ncomp, L, scaling, seed, run, precision, batched, best_comp,
+                   kfold_inner, nullptr, 0, ncomp, L, scaling, seed, run, precision, batched, best_comp,
                    inner_accuracy, outer_pred, inner_pred, fit_status);
+  });
+}
+
+int fpls_double_cv_outer_subset(const void* X, int x_is_float32, int n, int p, const int* y,
+                                int n_classes, const int* outer_fold, int kfold_outer,
+                                const int* inner_fold, int kfold_inner, const int* outer_ids,
+                                int n_outer_ids, const int* ncomp, int L, int scaling, int seed, int run,
+                                int precision, int batched, int* best_comp, double* inner_accuracy,
+                                int* outer_pred, int* inner_pred, int* fit_status, char* err,
+                                size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(outer_ids, "outer fold list is null");
+    double_cv_impl(X, x_is_float32, false, n, p, y, n_classes, outer_fold, kfold_outer, inner_fold,
+                   kfold_inner, outer_ids, n_outer_ids, ncomp, L, scaling, seed, run, precision, batched,
+                   best_comp, inner_accuracy, outer_pred, inner_pred, fit_status);
   });
 }
 
@@ -1075,8 +1133,26 @@ int fpls_double_cv_resident(int handle, const int* y, int n_classes, const int* 
                      ctx.resident[handle].ptr, "double_cv_resident: unknown handle");
     const ResidentX r = ctx.resident[handle];
     double_cv_impl(r.ptr, r.f32 ? 1 : 0, true, r.n, r.p, y, n_classes, outer_fold, kfold_outer,
-                   inner_fold, kfold_inner, ncomp, L, scaling, seed, run, precision, batched,
+                   inner_fold, kfold_inner, nullptr, 0, ncomp, L, scaling, seed, run, precision, batched,
                    best_comp, inner_accuracy, outer_pred, inner_pred, fit_status);
+  });
+}
+
+int fpls_double_cv_resident_outer_subset(int handle, const int* y, int n_classes, const int* outer_fold,
+                                         int kfold_outer, const int* inner_fold, int kfold_inner,
+                                         const int* outer_ids, int n_outer_ids, const int* ncomp, int L,
+                                         int scaling, int seed, int run, int precision, int batched,
+                                         int* best_comp, double* inner_accuracy, int* outer_pred,
+                                         int* inner_pred, int* fit_status, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(outer_ids, "outer fold list is null");
+    Context& ctx = Context::get();
+    FPLS_REQUIRE(handle >= 0 && handle < static_cast<int>(ctx.resident.size()) &&
+                     ctx.resident[handle].ptr, "double_cv_resident: unknown handle");
+    const ResidentX r = ctx.resident[handle];
+    double_cv_impl(r.ptr, r.f32 ? 1 : 0, true, r.n, r.p, y, n_classes, outer_fold, kfold_outer,
+                   inner_fold, kfold_inner, outer_ids, n_outer_ids, ncomp, L, scaling, seed, run,
+                   precision, batched, best_comp, inner_accuracy, outer_pred, inner_pred, fit_status);
   });
 }
 

@@ -1,11 +1,10 @@
 """Host plumbing for N independent double-CV replicas, one process per GPU.
 
-The CV grid does not shard across GPUs (every fit needs the whole predictor
-block and the fits of one grid are batched on one device), so `bench.py
---gpus N` runs N weak-scaled replicas: rank r uses device LOCAL_RANK and its
-own seeded workload, the ranks meet only at barriers, and the job's time is the
-maximum of the ranks' device times (gloo all-reduce of one float; no data-path
-collective).
+`bench.py --gpus N` runs N weak-scaled replicas: rank r uses device LOCAL_RANK
+and its own seeded workload, the ranks meet only at barriers, and the job's time
+is the maximum of the ranks' device times (gloo all-reduce of one float; no
+data-path collective).  Splitting ONE double CV across the ranks by outer fold
+is fold_shards.double_cv_sharded.
 """
 import datetime
 import os

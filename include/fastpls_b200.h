@@ -275,6 +275,27 @@ int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, 
                    int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
                    int* inner_pred, int* fit_status, char* err, size_t errlen);
 
+/* fpls_double_cv over the outer folds listed in outer_ids (n_outer_ids distinct
+ * 0-based ids) only, for fold-sharded grids: the caller splits the outer folds
+ * of one double CV across processes or GPUs (X replicated) and merges.  The
+ * inner and refit seeds are those of the full call (they depend on the fold id,
+ * not on its position in the list), and every output is written at the listed
+ * folds' own entries only: best_comp[o], inner_accuracy[o + l kfold_outer],
+ * outer_pred[i] for the rows of the listed folds, inner_pred[(o L + l) n + i],
+ * fit_status[o kfold_inner + i0] and fit_status[kfold_outer kfold_inner + o].
+ * Everything else is left as the caller set it, so disjoint lists covering all
+ * folds give, merged, the outputs of one fpls_double_cv call.  The per-call row
+ * Gram of the whole X is computed by every call (it does not depend on the
+ * folds).  Invalid lists (empty, an id out of range, a repeated id) return
+ * FPLS_ERR_ARGUMENT. */
+int fpls_double_cv_outer_subset(const void* X, int x_is_float32, int n, int p, const int* y,
+                                int n_classes, const int* outer_fold, int kfold_outer,
+                                const int* inner_fold, int kfold_inner, const int* outer_ids,
+                                int n_outer_ids, const int* ncomp, int L, int scaling, int seed, int run,
+                                int precision, int batched, int* best_comp, double* inner_accuracy,
+                                int* outer_pred, int* inner_pred, int* fit_status, char* err,
+                                size_t errlen);
+
 /* Gaussian response compression, regression branch: Yc = Y - colMeans(Y),
  * Z = Yc * projection (projection q x d is drawn by the caller, as R draws it
  * with rnorm), decoder = (ZᵀZ + 1e-8·mean(diag(ZᵀZ)) I)⁻¹ ZᵀYc.
@@ -439,6 +460,14 @@ int fpls_double_cv_resident(int handle, const int* y, int n_classes, const int* 
                             const int* ncomp, int L, int scaling, int seed, int run, int precision,
                             int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
                             int* inner_pred, int* fit_status, char* err, size_t errlen);
+
+/* fpls_double_cv_outer_subset on a registered predictor matrix. */
+int fpls_double_cv_resident_outer_subset(int handle, const int* y, int n_classes, const int* outer_fold,
+                                         int kfold_outer, const int* inner_fold, int kfold_inner,
+                                         const int* outer_ids, int n_outer_ids, const int* ncomp, int L,
+                                         int scaling, int seed, int run, int precision, int batched,
+                                         int* best_comp, double* inner_accuracy, int* outer_pred,
+                                         int* inner_pred, int* fit_status, char* err, size_t errlen);
 
 /* Instrumentation: number of kernels this library has launched since load, and
  * the device time (CUDA events on the library stream) of the last call,

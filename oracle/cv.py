@@ -73,8 +73,12 @@ def best_index(acc):
     return int(np.argmax(np.where(finite, acc, -np.inf)))
 
 
-def double_cv(X, y, outer_fold, inner_folds, ncomp, n_classes, scaling=1, seed=1, run=1):
+def double_cv(X, y, outer_fold, inner_folds, ncomp, n_classes, scaling=1, seed=1, run=1,
+              outer_ids=None):
     """pls.double.cv for one run with method simpls, argmax classifier.
+
+    outer_ids (optional) restricts the loop to those outer folds; the entries of
+    the other folds stay zero (the fold-sharded layout of the library's outputs).
 
     outer_fold: n 0-based outer fold ids.  inner_folds: n x kfold_outer matrix of
     inner fold ids of each row within outer fold o (-1 for the rows of fold o).
@@ -88,7 +92,7 @@ def double_cv(X, y, outer_fold, inner_folds, ncomp, n_classes, scaling=1, seed=1
     best = np.zeros(K_out, dtype=np.int32)
     inner_acc = np.zeros((K_out, ncomp.size))
     pred = np.zeros(n, dtype=np.int32)
-    for o in range(K_out):
+    for o in (range(K_out) if outer_ids is None else outer_ids):
         test = np.where(outer_fold == o)[0]
         train = np.where(outer_fold != o)[0]
         inner = pls_cv_predict_compiled(X[train], y[train], inner_folds[train, o], ncomp,

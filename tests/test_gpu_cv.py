@@ -125,3 +125,83 @@ def test_double_cv_fold_edge_cases(lib):
         model = opls.pls_model2_fast(Xd[train], ocv.response_rows(y, train, m), [best], seed=3 + 2000 + o + 1)
         ref = opls.pls_predict_classes_compact(model, Xd[test])[:, 0]
         assert np.mean(got["pred"][test] == ref) >= 0.99
+
+
+def _same_outputs(a, b, exact=True):
+    assert np.array_equal(a["best_comp"], b["best_comp"])
+    assert np.array_equal(a["fit_status"], b["fit_status"])
+    if exact:
+        assert np.array_equal(a["pred"], b["pred"])
+        assert np.array_equal(a["inner_accuracy"], b["inner_accuracy"], equal_nan=True)
+        assert np.array_equal(a["inner_pred"], b["inner_pred"])
+    else:
+        assert _labels_agree(a["pred"], b["pred"], 0.995)
+        assert np.allclose(a["inner_accuracy"], b["inner_accuracy"], atol=3e-3)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+@pytest.mark.parametrize("world", [2, 3])
+def test_fold_sharded_double_cv_merges_to_the_full_call(lib, c4_small, precision, world):
+    # Each shard runs only its outer folds (own fit set, same seeds); merged, the
+    # shards give the outputs of one call.  FP64 fits do not depend on which
+    # other fits share the batch, so the merge is exact there.
+    from fastpls_b200 import fold_shards
+    d = c4_small
+    outer, inner = double_cv_folds(d["y"], d["groups"], 5, 3, seed=5)
+    nc = np.arange(1, 9)
+    kw = dict(seed=1, precision=precision, return_inner=True)
+    full = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)
+    plan = fold_shards.assign_outer_folds(outer, world)
+    parts = [lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], outer_ids=ids, **kw)
+             for ids in plan]
+    for ids, part in zip(plan, parts):
+        rows = np.isin(outer, ids)
+        assert np.all(part["pred"][~rows] == 0) and np.all(part["pred"][rows] >= 1)
+        assert np.all(part["best_comp"][np.setdiff1d(np.arange(5), ids)] == 0)
+    _same_outputs(fold_shards.merge_outputs(parts), full, exact=precision == "fp64")
+
+
+def test_fold_sharded_resident_and_single_rank_driver(lib, c4_small):
+    from fastpls_b200 import fold_shards
+    d = c4_small
+    outer, inner = double_cv_folds(d["y"], d["groups"], 4, 3, seed=8)
+    nc = np.arange(1, 7)
+    kw = dict(seed=4, precision="fp64", return_inner=True)
+    full = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)
+    one = fold_shards.double_cv_sharded(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)
+    assert one["plan"] == [[0, 1, 2, 3]]
+    _same_outputs(one, full)
+    assert one["accuracy"] == full["accuracy"]
+    h = lib.x_upload(d["X"])
+    try:
+        parts = [lib.double_cv_resident(h, d["X"].shape[0], d["y"], outer, inner, nc, d["n_classes"],
+                                        outer_ids=ids, **kw) for ids in ([3, 0], [2], [1])]
+    finally:
+        lib.x_free(h)
+    _same_outputs(fold_shards.merge_outputs(parts), full)
+
+
+def test_fold_sharded_edge_folds(lib):
+    # A single-class outer fold and an unused inner fold id, split across shards.
+    from fastpls_b200 import fold_shards
+    rng = np.random.default_rng(11)
+    n, p, m = 240, 300, 3
+    y = np.repeat(np.arange(1, m + 1), n // m).astype(np.int32)
+    X = rng.standard_normal((n, p)) + 0.8 * y[:, None] * (np.arange(p) < 10)[None, :]
+    outer = np.where(y > 1, 0, 1 + rng.integers(0, 2, n)).astype(np.int32)
+    idx1 = np.where(y == 1)[0]
+    outer[idx1[:60]] = 1 + (np.arange(60) % 2)
+    outer[idx1[60:]] = 0
+    Ko, Ki = 3, 4
+    inner = np.full((n, Ko), -1, dtype=np.int32)
+    for o in range(Ko):
+        rows = np.where(outer != o)[0]
+        ids = np.arange(rows.size) % Ki
+        if o == 1:
+            ids[ids == 2] = 3
+        inner[rows, o] = ids
+    nc = np.arange(1, 6)
+    full = lib.double_cv(X, y, outer, inner, nc, m, seed=3, return_inner=True)
+    parts = [lib.double_cv(X, y, outer, inner, nc, m, seed=3, return_inner=True, outer_ids=ids)
+             for ids in ([0], [1, 2])]
+    _same_outputs(fold_shards.merge_outputs(parts), full)

@@ -211,8 +211,22 @@ void fill_special_predictions(const CvFitSet& fs, const int* y, const std::vecto
   }
 }
 
-// Columns per chunk of the overlapped upload of X.
+// Column chunks of the overlapped upload of X: 4096 columns each, except that
+// the work of the LAST chunk (its means, split and Gram) follows the last copy
+// instead of overlapping one, so the end of X goes in a narrow chunk of about
+// kUploadTailCols columns.  Chunk starts are multiples of 64 (one K-block of
+// the Gram).  Returns the nch + 1 column boundaries.
 constexpr int kUploadChunkCols = 4096;
+constexpr int kUploadTailCols = 1024;
+
+std::vector<int> upload_chunks(int p) {
+  std::vector<int> b{0};
+  while (p - b.back() > kUploadChunkCols + kUploadTailCols) b.push_back(b.back() + kUploadChunkCols);
+  const int tail0 = (p - kUploadTailCols) / 64 * 64;
+  if (tail0 - b.back() >= kUploadTailCols / 2) b.push_back(tail0);
+  b.push_back(p);
+  return b;
+}
 
 void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const int* y, const int* ncomp, int L,
                  const CvGridOptions& opt, const std::vector<int>& status,
@@ -255,7 +269,8 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
     const size_t esz = x64 ? sizeof(double) : sizeof(float);
     char* dst = x64 ? reinterpret_cast<char*>(const_cast<double*>(x64)) : reinterpret_cast<char*>(const_cast<float*>(x32));
     const char* src = static_cast<const char*>(x_host);
-    const int nch = (p + kUploadChunkCols - 1) / kUploadChunkCols;
+    const std::vector<int> bounds = upload_chunks(p);
+    const int nch = static_cast<int>(bounds.size()) - 1;
     xop = make_split_operator_chunked(n, p);
     x0 = ar.alloc_n<double>(n);
     // the copies follow this call's earlier work on the main stream (an event
@@ -263,7 +278,7 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
     FPLS_CUDA(cudaEventRecord(ctx.copy_event(nch), ctx.stream));
     FPLS_CUDA(cudaStreamWaitEvent(ctx.copy, ctx.copy_event(nch), 0));
     auto chunk_work = [&](int c) {
-      const int j0 = c * kUploadChunkCols, j1 = std::min(p, j0 + kUploadChunkCols);
+      const int j0 = bounds[c], j1 = bounds[c + 1];
       FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.copy_event(c), 0));
       const double* c64 = x64 ? x64 + (size_t)j0 * n : nullptr;
       const float* c32 = x32 ? x32 + (size_t)j0 * n : nullptr;
@@ -276,7 +291,7 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
       split_operator_gram_columns(*xop, Kg, j0, j1, c > 0);
     };
     for (int c = 0; c < nch; ++c) {
-      const int j0 = c * kUploadChunkCols, j1 = std::min(p, j0 + kUploadChunkCols);
+      const int j0 = bounds[c], j1 = bounds[c + 1];
       FPLS_CUDA(cudaMemcpyAsync(dst + (size_t)j0 * n * esz, src + (size_t)j0 * n * esz, (size_t)(j1 - j0) * n * esz,
                                 cudaMemcpyHostToDevice, ctx.copy));
       FPLS_CUDA(cudaEventRecord(ctx.copy_event(c), ctx.copy));

@@ -23,6 +23,7 @@ constexpr int kMaxK = 256;
 
 struct DualEng {
   int n, m, F, K, iters, m1, center;
+  int merge;     // refresh merged into the previous component's reduction (m <= kFuseM)
   const double* x0;
   const double* XOmega;
   const uint8_t* mask;
@@ -60,6 +61,10 @@ struct DualEng {
 };
 
 constexpr int kRedMax = kMaxK > kMaxM + 3 ? kMaxK : kMaxM + 3;
+// Class counts up to which a step launch merges the refresh of component a
+// into the Gram-Schmidt of component a - 1 (its 3m + m^2 + 2 dots fit one
+// pass of per-warp partials).
+constexpr int kFuseM = 6;
 
 // C_S of every fit: mask_f * (onehot(label) - (mY_all + dY_f)).
 __global__ void k_dual_cs0(DualEng e) {
@@ -101,6 +106,8 @@ struct ClusterRed {
   double xw[kW];                     // per-warp sums of an extra scalar reduced with the dots
   double part[2][kRedMax];           // this CTA's partials (alternating between exchanges)
   double res[kRedMax];
+  double fv[kFuseM];                 // merged launch: S'^T v / |v| and the refresh start z
+  double fz[2][kFuseM];
   int buf;
 };
 
@@ -208,10 +215,123 @@ static __device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M,
   cluster_exchange(R, has_extra ? ncols + 1 : ncols);
 }
 
+// The one reduction of a merged launch (m <= kFuseM), over the fit's rows, with
+// c_v, K c_v the Gram-Schmidt result of component a - 1 (unnormalised) and k_y
+// the warm start K c_y of component a:
+//   res[j]            = C_S[:,j] . K c_v      res[m + j]  = C_S[:,j] . k_y
+//   res[2m + j]       = K C_S[:,j] . c_v      res[3m + jm + k] = C_S[:,j] . K C_S[:,k]
+//   res[3m + m^2]     = c_v . K c_v           res[3m + m^2 + 1] = c_v . k_y
+static __device__ void fused_dots(ClusterRed& R, const double* __restrict__ CS, const double* __restrict__ KCS,
+                                  int n, int m, const Rows& rw, const double (&cv)[kLR], const double (&kv)[kLR],
+                                  const double (&ky)[kLR]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q0 = 3 * m + m * m;
+  {
+    double sv = 0.0, sy = 0.0;
+#pragma unroll
+    for (int r = 0; r < kLR; ++r) {
+      sv += cv[r] * kv[r];
+      sy += cv[r] * ky[r];
+    }
+    sv = warp_sum(sv);
+    sy = warp_sum(sy);
+    if (lane == 0) {
+      R.warp[warp][q0] = sv;
+      R.warp[warp][q0 + 1] = sy;
+    }
+  }
+  for (int j = 0; j < m; ++j) {
+    const double* cs = CS + (size_t)j * n;
+    double d2 = 0.0, d1 = 0.0;
+#pragma unroll
+    for (int r = 0; r < kLR; ++r)
+      if (rw.ok(r)) {
+        const double c = cs[rw.row(r)];
+        d2 += c * kv[r];
+        d1 += c * ky[r];
+      }
+    d2 = warp_sum(d2);
+    d1 = warp_sum(d1);
+    if (lane == 0) {
+      R.warp[warp][j] = d2;
+      R.warp[warp][m + j] = d1;
+    }
+  }
+  // K C_S columns one at a time against c_v and every C_S column (those
+  // re-reads hit L1)
+  for (int k = 0; k < m; ++k) {
+    double ks[kLR];
+#pragma unroll
+    for (int r = 0; r < kLR; ++r) ks[r] = rw.ok(r) ? KCS[(size_t)k * n + rw.row(r)] : 0.0;
+    double ek = 0.0;
+#pragma unroll
+    for (int r = 0; r < kLR; ++r) ek += ks[r] * cv[r];
+    ek = warp_sum(ek);
+    if (lane == 0) R.warp[warp][2 * m + k] = ek;
+    for (int j = 0; j < m; ++j) {
+      const double* cs = CS + (size_t)j * n;
+      double mjk = 0.0;
+#pragma unroll
+      for (int r = 0; r < kLR; ++r)
+        if (rw.ok(r)) mjk += cs[rw.row(r)] * ks[r];
+      mjk = warp_sum(mjk);
+      if (lane == 0) R.warp[warp][3 * m + j * m + k] = mjk;
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < q0 + 2; q += kT) {
+    double v = 0.0;
+    for (int w = 0; w < kW; ++w) v += R.warp[w][q];
+    R.part[R.buf][q] = v;
+  }
+  cluster_exchange(R, q0 + 2);
+}
+
+// After fused_dots and the normalisation by vn = |v|: fv[j] = S^T v / |v| (the
+// deflation coefficients) and fz[zb][..] = the refresh direction after `iters`
+// power iterations from the warm start (lanes j < m of warp 0; every thread
+// sees the result after the closing block barrier).  Returns zb.
+static __device__ int fused_refresh(ClusterRed& R, int m, int iters, double vn) {
+  const int q0 = 3 * m + m * m;
+  int zb = 0;
+  if (threadIdx.x < 32) {
+    const int j = threadIdx.x;
+    const double vv = R.res[q0], cky = R.res[q0 + 1] / vn;
+    double vj = 0.0;
+    if (j < m) {
+      vj = R.res[j] / vn;
+      R.fv[j] = vj;
+      R.fz[0][j] = R.res[m + j] - cky * vj;
+    }
+    __syncwarp();
+    const double vvn = vv / (vn * vn);
+    for (int it = 1; it < iters; ++it) {
+      if (j < m) {
+        double t = 0.0;
+        for (int k = 0; k < m; ++k) {
+          const double vk = R.fv[k];
+          const double mjk = R.res[3 * m + j * m + k] - vj * vk - vj * (R.res[2 * m + k] / vn) + vj * vk * vvn;
+          t += mjk * R.fz[zb][k];
+        }
+        R.fz[zb ^ 1][j] = t;
+      }
+      zb ^= 1;
+      __syncwarp();
+    }
+  } else {
+    for (int it = 1; it < iters; ++it) zb ^= 1;
+  }
+  __syncthreads();
+  return zb;
+}
+
 // Refresh (power iterations of S S^T from the sketch or the warm start),
 // Householder normalisation, scores t = X_f r, q = Y^T t, and the loading
 // coefficients c_p for the K product.
-static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank) {
+// With `pre` the refresh was already run by the merged launch (c_y, K c_y in
+// pre_cy, pre_ky) and only the scores part follows.
+static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank,
+                              const double (&pre_cy)[kLR], const double (&pre_ky)[kLR], bool pre) {
   __shared__ double wcls[kW][kMaxM + 5];   // per-warp class sums and the reduction's scalars
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m;
@@ -220,7 +340,14 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
   const uint8_t* mk = e.mask + (size_t)f * n;
   double cy[kLR], ky[kLR];
   int steps = e.iters;
-  if (e.m1) {
+  if (pre) {
+#pragma unroll
+    for (int k = 0; k < kLR; ++k) {
+      cy[k] = pre_cy[k];
+      ky[k] = pre_ky[k];
+    }
+    steps = 0;
+  } else if (e.m1) {
 #pragma unroll
     for (int k = 0; k < kLR; ++k) {
       cy[k] = rw.ok(k) ? CS[rw.row(k)] : 0.0;
@@ -399,8 +526,17 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
 
 // Gram-Schmidt of the loading against the earlier ones in K-coordinates,
 // normalisation, rank-1 deflation of C_S and K C_S, and the component outputs.
+// With fuse (m <= kFuseM, launches between the first and the last) the
+// refresh of component a + 1 rides on this component's reduction: the merged
+// dots give z0 = C_S'^T k_y for the deflated C_S' and the m x m matrix
+// M' = C_S'^T K C_S' = S'^T S' in closed form (M' = M - v v^T - v e^T / |v|
+// + v v^T c_v.Kc_v / |v|^2), the power iterations z <- M' z run on it, and the
+// deflation pass accumulates c_y = C_S' z and K c_y = K C_S' z (into fcy, fky)
+// as it writes C_S' and K C_S'.  This saves two cluster reductions and one pass
+// over C_S and K C_S per launch.
 static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank,
-                              const int (&ks0)[kLR], const int (&ks1)[kLR]) {
+                              const int (&ks0)[kLR], const int (&ks1)[kLR], bool fuse, double (&fcy)[kLR],
+                              double (&fky)[kLR]) {
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m, K = e.K;
   double* CV = e.CV + (size_t)f * n * K;
@@ -438,52 +574,111 @@ static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows
         }
     }
   }
-  // ||v||^2 = c_v^T K c_v and S^T v = C_S^T K c_v in one reduction (the
-  // normalisation only rescales the dots)
-  double vv = 0.0;
+  if (fuse) {
+    double kyw[kLR];
 #pragma unroll
-  for (int k = 0; k < kLR; ++k) vv += cv[k] * kv[k];
-  cluster_dots(R, CS, n, m, rw, kv, true, vv);
-  const double vn = sqrt(R.res[m]);
-  if (!(vn > 0.0) || !isfinite(vn)) {
-    if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
-    return false;
-  }
-#pragma unroll
-  for (int k = 0; k < kLR; ++k) {
-    cv[k] /= vn;
-    kv[k] /= vn;
-    if (rw.ok(k)) {
-      CV[rw.row(k) + (size_t)a * n] = cv[k];
-      KCV[rw.row(k) + (size_t)a * n] = kv[k];
+    for (int k = 0; k < kLR; ++k) kyw[k] = rw.ok(k) ? e.Kcy[(size_t)f * n + rw.row(k)] : 0.0;
+    fused_dots(R, CS, KCS, n, m, rw, cv, kv, kyw);
+    const int q0 = 3 * m + m * m;
+    const double vv = R.res[q0];
+    const double vn = sqrt(vv);
+    if (!(vn > 0.0) || !isfinite(vn)) {
+      if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
+      return false;
     }
-  }
-  // Rank-1 deflation of C_S and K C_S, four columns at a time: every load of
-  // a chunk is issued before its stores (the stores could alias later loads,
-  // which would otherwise serialise each column's read-modify-write).
-  for (int j0 = 0; j0 < m; j0 += 4) {
-    double csv[4][kLR], ksv[4][kLR];
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      const int j = min(j0 + jj, m - 1);
-#pragma unroll
-      for (int k = 0; k < kLR; ++k) {
-        csv[jj][k] = rw.ok(k) ? CS[(size_t)j * n + rw.row(k)] : 0.0;
-        ksv[jj][k] = rw.ok(k) ? KCS[(size_t)j * n + rw.row(k)] : 0.0;
+    for (int k = 0; k < kLR; ++k) {
+      cv[k] /= vn;
+      kv[k] /= vn;
+      if (rw.ok(k)) {
+        CV[rw.row(k) + (size_t)a * n] = cv[k];
+        KCV[rw.row(k) + (size_t)a * n] = kv[k];
       }
     }
+    const int zb = fused_refresh(R, m, e.iters, vn);
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      if (j0 + jj >= m) break;
-      const double vj = R.res[j0 + jj] / vn;
-      double* cs = CS + (size_t)(j0 + jj) * n;
-      double* ks = KCS + (size_t)(j0 + jj) * n;
+    for (int k = 0; k < kLR; ++k) fcy[k] = fky[k] = 0.0;
+    // (kFC columns per chunk: two in the register-capped 512-thread layout)
+    constexpr int kFC = kLR <= 2 ? 2 : 4;
 #pragma unroll
-      for (int k = 0; k < kLR; ++k)
-        if (rw.ok(k)) {
-          cs[rw.row(k)] = csv[jj][k] - cv[k] * vj;
-          ks[rw.row(k)] = ksv[jj][k] - kv[k] * vj;
+    for (int j0 = 0; j0 < kFuseM; j0 += kFC) {
+      if (j0 >= m) break;
+      double csv[kFC][kLR], ksv[kFC][kLR];
+#pragma unroll
+      for (int jj = 0; jj < kFC; ++jj) {
+        const int j = min(j0 + jj, m - 1);
+#pragma unroll
+        for (int k = 0; k < kLR; ++k) {
+          csv[jj][k] = rw.ok(k) ? CS[(size_t)j * n + rw.row(k)] : 0.0;
+          ksv[jj][k] = rw.ok(k) ? KCS[(size_t)j * n + rw.row(k)] : 0.0;
         }
+      }
+#pragma unroll
+      for (int jj = 0; jj < kFC; ++jj) {
+        if (j0 + jj >= m || j0 + jj >= kFuseM) break;
+        const double vj = R.fv[j0 + jj], zj = R.fz[zb][j0 + jj];
+        double* cs = CS + (size_t)(j0 + jj) * n;
+        double* ks = KCS + (size_t)(j0 + jj) * n;
+#pragma unroll
+        for (int k = 0; k < kLR; ++k)
+          if (rw.ok(k)) {
+            const double cn = csv[jj][k] - cv[k] * vj;
+            const double kn = ksv[jj][k] - kv[k] * vj;
+            cs[rw.row(k)] = cn;
+            ks[rw.row(k)] = kn;
+            fcy[k] += cn * zj;
+            fky[k] += kn * zj;
+          }
+      }
+    }
+  } else {
+    // ||v||^2 = c_v^T K c_v and S^T v = C_S^T K c_v in one reduction (the
+    // normalisation only rescales the dots)
+    double vv = 0.0;
+#pragma unroll
+    for (int k = 0; k < kLR; ++k) vv += cv[k] * kv[k];
+    cluster_dots(R, CS, n, m, rw, kv, true, vv);
+    const double vn = sqrt(R.res[m]);
+    if (!(vn > 0.0) || !isfinite(vn)) {
+      if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
+      return false;
+    }
+#pragma unroll
+    for (int k = 0; k < kLR; ++k) {
+      cv[k] /= vn;
+      kv[k] /= vn;
+      if (rw.ok(k)) {
+        CV[rw.row(k) + (size_t)a * n] = cv[k];
+        KCV[rw.row(k) + (size_t)a * n] = kv[k];
+      }
+    }
+    // Rank-1 deflation of C_S and K C_S, four columns at a time: every load of
+    // a chunk is issued before its stores (the stores could alias later loads,
+    // which would otherwise serialise each column's read-modify-write).
+    for (int j0 = 0; j0 < m; j0 += 4) {
+      double csv[4][kLR], ksv[4][kLR];
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const int j = min(j0 + jj, m - 1);
+#pragma unroll
+        for (int k = 0; k < kLR; ++k) {
+          csv[jj][k] = rw.ok(k) ? CS[(size_t)j * n + rw.row(k)] : 0.0;
+          ksv[jj][k] = rw.ok(k) ? KCS[(size_t)j * n + rw.row(k)] : 0.0;
+        }
+      }
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        if (j0 + jj >= m) break;
+        const double vj = R.res[j0 + jj] / vn;
+        double* cs = CS + (size_t)(j0 + jj) * n;
+        double* ks = KCS + (size_t)(j0 + jj) * n;
+#pragma unroll
+        for (int k = 0; k < kLR; ++k)
+          if (rw.ok(k)) {
+            cs[rw.row(k)] = csv[jj][k] - cv[k] * vj;
+            ks[rw.row(k)] = ksv[jj][k] - kv[k] * vj;
+          }
+      }
     }
   }
   if (rank == 0) {
@@ -534,8 +729,10 @@ static __device__ void run(const DualEng& e, int a) {
   // cluster barrier, which also keeps each CTA's shared memory alive until the
   // last remote read of it.
   bool ok = true;
-  if (a > 0) ok = dual_b(e, a - 1, R, rw, rank, ks0, ks1);
-  if (ok && a < e.K) dual_a(e, a, R, rw, rank);
+  const bool fuse = e.merge && a > 0 && a < e.K;
+  double fcy[kLR], fky[kLR];
+  if (a > 0) ok = dual_b(e, a - 1, R, rw, rank, ks0, ks1, fuse, fcy, fky);
+  if (ok && a < e.K) dual_a(e, a, R, rw, rank, fcy, fky, fuse);
   if constexpr (CL > 1) cg::this_cluster().sync();
 }
 };  // struct Step
@@ -615,6 +812,13 @@ void launch_step(int layout, const DualEng& e, int a, int F, cudaStream_t st) {
 
 }  // namespace
 
+// FASTPLS_DUAL_MERGE=0 runs the refresh of every component in its own
+// reductions (the unmerged launch) instead.
+static bool dual_merge_enabled() {
+  const char* v = std::getenv("FASTPLS_DUAL_MERGE");
+  return !(v && v[0] == '0');
+}
+
 bool dual_engine_applies(int n, int p, int m, int K) {
   if (const char* e = std::getenv("FASTPLS_DUAL"))
     if (e[0] == '0') return false;
@@ -630,6 +834,7 @@ void dual_simpls_run(const DualBatch& b) {
   e.iters = b.m1_mode ? 0 : std::max(b.power_iters, 0);
   e.m1 = b.m1_mode ? 1 : 0;
   e.center = b.center ? 1 : 0;
+  e.merge = (!e.m1 && e.iters >= 1 && e.m <= kFuseM && dual_merge_enabled()) ? 1 : 0;
   e.x0 = b.x0; e.XOmega = b.XOmega; e.mask = b.mask; e.labels = b.labels; e.mY_all = b.mY_all; e.dY = b.dY;
   e.Q = b.Q; e.tnorm = b.tnorm; e.Tkeep = b.Tkeep; e.ncomp_done = b.ncomp_done; e.status = b.status;
   const size_t F = b.F, n = b.n, m = b.m, K = b.K;

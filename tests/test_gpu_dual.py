@@ -104,9 +104,9 @@ def test_step_layouts_agree(lib):
 
 
 def test_host_buffer_chunked_upload_matches_resident(lib):
-    # The host-buffer call uploads X in 4096-column chunks overlapped with the
-    # column means, the BF16 split and the row Gram (three chunks here, the last
-    # one partial); its predictions match the resident call's.  The chunked row
+    # The host-buffer call uploads X in column chunks overlapped with the column
+    # means, the BF16 split and the row Gram (4096, 3840 and a narrow final chunk
+    # of 1064 columns here); its predictions match the resident call's.  The chunked row
     # Gram sums its FP32 segments over different stream-K cuts, so the check is
     # agreement, not bit equality.
     d = synthetic.c4_omics(seed=21, n=400, p=9000, n_informative=25)

@@ -90,7 +90,7 @@ __global__ void k_dual_cs0(DualEng e) {
 // memory, summed in rank order so every CTA of the cluster sees bit-identical
 // results and takes the same branches.  With CL = 1 a fit lives in one CTA and
 // every reduction ends at a block barrier.
-template <int CL, int T, int LR>
+template <int CL, int T, int LR, bool MG>
 struct Step {
 static constexpr int kCl = CL;
 static constexpr int kT = T;
@@ -328,10 +328,10 @@ static __device__ int fused_refresh(ClusterRed& R, int m, int iters, double vn) 
 // Refresh (power iterations of S S^T from the sketch or the warm start),
 // Householder normalisation, scores t = X_f r, q = Y^T t, and the loading
 // coefficients c_p for the K product.
-// With `pre` the refresh was already run by the merged launch (c_y, K c_y in
+// In the merged launch (MG) the refresh was already run by dual_b (c_y, K c_y in
 // pre_cy, pre_ky) and only the scores part follows.
 static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank,
-                              const double (&pre_cy)[kLR], const double (&pre_ky)[kLR], bool pre) {
+                              const double (&pre_cy)[kLR], const double (&pre_ky)[kLR]) {
   __shared__ double wcls[kW][kMaxM + 5];   // per-warp class sums and the reduction's scalars
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m;
@@ -340,7 +340,7 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
   const uint8_t* mk = e.mask + (size_t)f * n;
   double cy[kLR], ky[kLR];
   int steps = e.iters;
-  if (pre) {
+  if constexpr (MG) {
 #pragma unroll
     for (int k = 0; k < kLR; ++k) {
       cy[k] = pre_cy[k];
@@ -526,16 +526,16 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
 
 // Gram-Schmidt of the loading against the earlier ones in K-coordinates,
 // normalisation, rank-1 deflation of C_S and K C_S, and the component outputs.
-// With fuse (m <= kFuseM, launches between the first and the last) the
-// refresh of component a + 1 rides on this component's reduction: the merged
-// dots give z0 = C_S'^T k_y for the deflated C_S' and the m x m matrix
+// In the merged launch (MG: m <= kFuseM, launches between the first and the
+// last) the refresh of component a + 1 rides on this component's reduction:
+// the merged dots give z0 = C_S'^T k_y for the deflated C_S' and the m x m matrix
 // M' = C_S'^T K C_S' = S'^T S' in closed form (M' = M - v v^T - v e^T / |v|
 // + v v^T c_v.Kc_v / |v|^2), the power iterations z <- M' z run on it, and the
 // deflation pass accumulates c_y = C_S' z and K c_y = K C_S' z (into fcy, fky)
 // as it writes C_S' and K C_S'.  This saves two cluster reductions and one pass
 // over C_S and K C_S per launch.
 static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank,
-                              const int (&ks0)[kLR], const int (&ks1)[kLR], bool fuse, double (&fcy)[kLR],
+                              const int (&ks0)[kLR], const int (&ks1)[kLR], double (&fcy)[kLR],
                               double (&fky)[kLR]) {
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m, K = e.K;
@@ -574,7 +574,7 @@ static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows
         }
     }
   }
-  if (fuse) {
+  if constexpr (MG) {
     double kyw[kLR];
 #pragma unroll
     for (int k = 0; k < kLR; ++k) kyw[k] = rw.ok(k) ? e.Kcy[(size_t)f * n + rw.row(k)] : 0.0;
@@ -728,20 +728,21 @@ static __device__ void run(const DualEng& e, int a) {
   // cluster-wide sums, identical in all CTAs), and all of them end on the same
   // cluster barrier, which also keeps each CTA's shared memory alive until the
   // last remote read of it.
+  // MG (the merged launch) is chosen by the host for 0 < a < K when the fit
+  // set allows it (e.merge).
   bool ok = true;
-  const bool fuse = e.merge && a > 0 && a < e.K;
   double fcy[kLR], fky[kLR];
-  if (a > 0) ok = dual_b(e, a - 1, R, rw, rank, ks0, ks1, fuse, fcy, fky);
-  if (ok && a < e.K) dual_a(e, a, R, rw, rank, fcy, fky, fuse);
+  if (a > 0) ok = dual_b(e, a - 1, R, rw, rank, ks0, ks1, fcy, fky);
+  if (ok && a < e.K) dual_a(e, a, R, rw, rank, fcy, fky);
   if constexpr (CL > 1) cg::this_cluster().sync();
 }
 };  // struct Step
 
 // 512-thread CTAs are held to 64 registers so that two fit on an SM and the
 // 240 CTAs of a 60-fit grid run in one wave.
-template <int CL, int T, int LR>
+template <int CL, int T, int LR, bool MG>
 __global__ void __launch_bounds__(T, T >= 512 ? 2 : 1) k_dual_step(DualEng e, int a) {
-  Step<CL, T, LR>::run(e, a);
+  Step<CL, T, LR, MG>::run(e, a);
 }
 
 __global__ void symmetrize_kernel(double* K, int n) {
@@ -766,10 +767,10 @@ void symmetrize(double* K, int n) {
 
 namespace {
 
-template <int CL, int T, int LR>
+template <int CL, int T, int LR, bool MG>
 void launch_step_cfg(const DualEng& e, int a, int F, cudaStream_t st) {
   if constexpr (CL == 1) {
-    k_dual_step<1, T, LR><<<F, T, 0, st>>>(e, a);
+    k_dual_step<1, T, LR, MG><<<F, T, 0, st>>>(e, a);
   } else {
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3(F * CL);
@@ -785,7 +786,7 @@ void launch_step_cfg(const DualEng& e, int a, int F, cudaStream_t st) {
     attr[1].val.programmaticStreamSerializationAllowed = 1;
     lc.attrs = attr;
     lc.numAttrs = tc::pdl_enabled() ? 2 : 1;
-    FPLS_CUDA(cudaLaunchKernelEx(&lc, k_dual_step<CL, T, LR>, e, a));
+    FPLS_CUDA(cudaLaunchKernelEx(&lc, k_dual_step<CL, T, LR, MG>, e, a));
   }
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
@@ -806,8 +807,14 @@ int choose_step_layout(int n) {
 }
 
 void launch_step(int layout, const DualEng& e, int a, int F, cudaStream_t st) {
-  if (layout == kStepWide) launch_step_cfg<4, 512, 2>(e, a, F, st);
-  else launch_step_cfg<4, 256, 8>(e, a, F, st);
+  const bool mg = e.merge && a > 0 && a < e.K;
+  if (layout == kStepWide) {
+    if (mg) launch_step_cfg<4, 512, 2, true>(e, a, F, st);
+    else launch_step_cfg<4, 512, 2, false>(e, a, F, st);
+  } else {
+    if (mg) launch_step_cfg<4, 256, 8, true>(e, a, F, st);
+    else launch_step_cfg<4, 256, 8, false>(e, a, F, st);
+  }
 }
 
 }  // namespace

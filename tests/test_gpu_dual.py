@@ -132,3 +132,38 @@ def test_host_buffer_chunked_upload_matches_resident(lib):
     finally:
         lib.x_free(h)
     assert np.array_equal(a["pred"], b["pred"]) and np.array_equal(a["inner_accuracy"], b["inner_accuracy"])
+
+
+@pytest.mark.parametrize("props", [(0.5, 0.3, 0.2), (0.25, 0.2, 0.2, 0.15, 0.1, 0.1),
+                                   (0.2, 0.15, 0.15, 0.1, 0.1, 0.1, 0.1, 0.1)])
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_merged_refresh_matches_separate_reductions(lib, props, precision):
+    # Up to 6 classes a step launch takes the refresh of component a from the
+    # Gram-Schmidt reduction of a - 1 (power iterations on S'^T S'); with
+    # FASTPLS_DUAL_MERGE=0 every refresh runs its own reductions.  Same folds
+    # and sketches: the two agree to rounding (8 classes never merge).
+    d = synthetic.c4_omics(seed=14, n=420, p=1500, n_informative=30, props=props)
+    outer, inner = double_cv_folds(d["y"], d["groups"], 4, 3, seed=9)
+    nc = np.arange(1, 16)
+
+    def run(merge):
+        if merge is not None:
+            os.environ["FASTPLS_DUAL_MERGE"] = merge
+        try:
+            return lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], seed=4,
+                                 precision=precision, return_inner=True)
+        finally:
+            os.environ.pop("FASTPLS_DUAL_MERGE", None)
+
+    a, b = run(None), run("0")
+    assert np.array_equal(a["fit_status"], b["fit_status"])
+    assert np.array_equal(a["best_comp"], b["best_comp"])
+    assert np.nanmax(np.abs(a["inner_accuracy"] - b["inner_accuracy"])) <= 1e-3
+    assert np.mean(a["inner_pred"] == b["inner_pred"]) >= 0.999
+    assert np.mean(a["pred"] == b["pred"]) >= 0.995
+    if len(props) > 6:
+        assert np.array_equal(a["inner_pred"], b["inner_pred"])
+    if precision == "fp64":
+        ref = ocv.double_cv(d["X"].astype(np.float64), d["y"], outer, inner, nc, d["n_classes"], seed=4)
+        assert np.array_equal(a["best_comp"], ref["best_comp"])
+        assert np.allclose(a["inner_accuracy"], ref["inner_accuracy"], atol=2e-3)

@@ -10,12 +10,6 @@ constexpr int BK = 16;
 constexpr int PAD = 4;  // row stride of 68 doubles keeps the DMMA fragment loads conflict-free
 constexpr int GEMM_THREADS = 128;
 
-__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
-}
-
 // Tile loader: fetches the BK x BM slice of op(A) (or BK x BN of op(B)) for the
 // k-block starting at k0 into registers; out-of-range elements read as zero.
 template <bool KContig>

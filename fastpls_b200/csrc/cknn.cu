@@ -40,12 +40,6 @@ constexpr int kTileThreads = 128;
 constexpr int kMaxChunks = 64;   // chunk lists merged per pair
 constexpr int kMinChunkRows = 2048;
 
-__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
-}
-
 // Strict '>' insertion into a descending list of length k (earlier entries win
 // ties), list entries strided by `stride` (src/fastPLS.cpp:1249-1267).
 template <typename V, typename I>

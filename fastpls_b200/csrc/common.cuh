@@ -63,6 +63,15 @@ __device__ __forceinline__ float warp_sum_f(float v) {
   return v;
 }
 
+// D (8 x 8) += A (8 x 4) B (4 x 8) on the FP64 tensor cores (mma.sync m8n8k4):
+// lane l holds a = A[l / 4][l % 4], b = B[l % 4][l / 4] and the accumulators
+// c0, c1 = D[l / 4][2 (l % 4)], D[l / 4][2 (l % 4) + 1].
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
 // Block-wide sum; `scratch` needs blockDim.x/32 doubles. Result valid in all threads.
 __device__ __forceinline__ double block_sum(double v, double* scratch) {
   const int lane = threadIdx.x & 31;

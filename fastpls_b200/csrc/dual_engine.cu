@@ -62,8 +62,8 @@ struct DualEng {
 
 constexpr int kRedMax = kMaxK > kMaxM + 3 ? kMaxK : kMaxM + 3;
 // Class counts up to which a step launch merges the refresh of component a
-// into the Gram-Schmidt of component a - 1 (its 3m + m^2 + 2 dots fit one
-// pass of per-warp partials).
+// into the Gram-Schmidt of component a - 1 (the merged reduction's columns,
+// m + 1 and m + 2 of them, fit one 8 x 8 FP64 MMA tile).
 constexpr int kFuseM = 6;
 
 // C_S of every fit: mask_f * (onehot(label) - (mY_all + dY_f)).
@@ -215,76 +215,46 @@ static __device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M,
   cluster_exchange(R, has_extra ? ncols + 1 : ncols);
 }
 
-// The one reduction of a merged launch (m <= kFuseM), over the fit's rows, with
-// c_v, K c_v the Gram-Schmidt result of component a - 1 (unnormalised) and k_y
-// the warm start K c_y of component a:
-//   res[j]            = C_S[:,j] . K c_v      res[m + j]  = C_S[:,j] . k_y
-//   res[2m + j]       = K C_S[:,j] . c_v      res[3m + jm + k] = C_S[:,j] . K C_S[:,k]
-//   res[3m + m^2]     = c_v . K c_v           res[3m + m^2 + 1] = c_v . k_y
-static __device__ void fused_dots(ClusterRed& R, const double* __restrict__ CS, const double* __restrict__ KCS,
-                                  int n, int m, const Rows& rw, const double (&cv)[kLR], const double (&kv)[kLR],
-                                  const double (&ky)[kLR]) {
+// The one reduction of a merged launch (m <= kFuseM) as a single 8 x 8 product
+// over the fit's rows on the FP64 tensor cores: D = A^T B with the columns
+// A = [C_S (m) | c_v] and B = [K C_S (m) | K c_v | k_y], where c_v, K c_v are
+// the Gram-Schmidt result of component a - 1 (unnormalised, stored in cvb, kvb
+// by this CTA before a block barrier) and k_y the warm start K c_y of component
+// a.  Each warp takes 4-row chunks of the CTA's rows (one m8n8k4 per chunk:
+// lane l loads column l / 4 of A and of B at row l % 4), the warps' tiles are
+// summed in order and then over the cluster: res[8 g + h] = A[:,g] . B[:,h], so
+//   res[8 j + k] = C_S[:,j] . K C_S[:,k]   res[8 j + m] = C_S[:,j] . K c_v
+//   res[8 j + m + 1] = C_S[:,j] . k_y      res[8 m + k] = c_v . K C_S[:,k]
+//   res[8 m + m] = c_v . K c_v             res[8 m + m + 1] = c_v . k_y
+static __device__ void fused_dots(ClusterRed& R, const double* CS, const double* KCS, const double* cvb,
+                                  const double* kvb, const double* kyb, int n, int m, const Rows& rw) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int q0 = 3 * m + m * m;
-  {
-    double sv = 0.0, sy = 0.0;
+  const int g = lane >> 2, t = lane & 3;
+  const double* colA = g < m ? CS + (size_t)g * n : (g == m ? cvb : nullptr);
+  const double* colB = g < m ? KCS + (size_t)g * n : (g == m ? kvb : (g == m + 1 ? kyb : nullptr));
+  double d0 = 0.0, d1 = 0.0;
+  const int nch = (rw.nl + 3) >> 2;
+  for (int c0 = warp; c0 < nch; c0 += 4 * kW) {
+    double av[4], bv[4];
 #pragma unroll
-    for (int r = 0; r < kLR; ++r) {
-      sv += cv[r] * kv[r];
-      sy += cv[r] * ky[r];
+    for (int u = 0; u < 4; ++u) {
+      const int r = (c0 + u * kW) * 4 + t;
+      const bool ok = r < rw.nl;
+      av[u] = (ok && colA) ? colA[rw.r0 + r] : 0.0;
+      bv[u] = (ok && colB) ? colB[rw.r0 + r] : 0.0;
     }
-    sv = warp_sum(sv);
-    sy = warp_sum(sy);
-    if (lane == 0) {
-      R.warp[warp][q0] = sv;
-      R.warp[warp][q0 + 1] = sy;
-    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) dmma_8x8x4(d0, d1, av[u], bv[u]);
   }
-  for (int j = 0; j < m; ++j) {
-    const double* cs = CS + (size_t)j * n;
-    double d2 = 0.0, d1 = 0.0;
-#pragma unroll
-    for (int r = 0; r < kLR; ++r)
-      if (rw.ok(r)) {
-        const double c = cs[rw.row(r)];
-        d2 += c * kv[r];
-        d1 += c * ky[r];
-      }
-    d2 = warp_sum(d2);
-    d1 = warp_sum(d1);
-    if (lane == 0) {
-      R.warp[warp][j] = d2;
-      R.warp[warp][m + j] = d1;
-    }
-  }
-  // K C_S columns one at a time against c_v and every C_S column (those
-  // re-reads hit L1)
-  for (int k = 0; k < m; ++k) {
-    double ks[kLR];
-#pragma unroll
-    for (int r = 0; r < kLR; ++r) ks[r] = rw.ok(r) ? KCS[(size_t)k * n + rw.row(r)] : 0.0;
-    double ek = 0.0;
-#pragma unroll
-    for (int r = 0; r < kLR; ++r) ek += ks[r] * cv[r];
-    ek = warp_sum(ek);
-    if (lane == 0) R.warp[warp][2 * m + k] = ek;
-    for (int j = 0; j < m; ++j) {
-      const double* cs = CS + (size_t)j * n;
-      double mjk = 0.0;
-#pragma unroll
-      for (int r = 0; r < kLR; ++r)
-        if (rw.ok(r)) mjk += cs[rw.row(r)] * ks[r];
-      mjk = warp_sum(mjk);
-      if (lane == 0) R.warp[warp][3 * m + j * m + k] = mjk;
-    }
-  }
+  R.warp[warp][8 * g + 2 * t] = d0;
+  R.warp[warp][8 * g + 2 * t + 1] = d1;
   __syncthreads();
-  for (int q = threadIdx.x; q < q0 + 2; q += kT) {
+  for (int q = threadIdx.x; q < 64; q += kT) {
     double v = 0.0;
     for (int w = 0; w < kW; ++w) v += R.warp[w][q];
     R.part[R.buf][q] = v;
   }
-  cluster_exchange(R, q0 + 2);
+  cluster_exchange(R, 64);
 }
 
 // After fused_dots and the normalisation by vn = |v|: fv[j] = S^T v / |v| (the
@@ -292,16 +262,15 @@ static __device__ void fused_dots(ClusterRed& R, const double* __restrict__ CS, 
 // power iterations from the warm start (lanes j < m of warp 0; every thread
 // sees the result after the closing block barrier).  Returns zb.
 static __device__ int fused_refresh(ClusterRed& R, int m, int iters, double vn) {
-  const int q0 = 3 * m + m * m;
   int zb = 0;
   if (threadIdx.x < 32) {
     const int j = threadIdx.x;
-    const double vv = R.res[q0], cky = R.res[q0 + 1] / vn;
+    const double vv = R.res[8 * m + m], cky = R.res[8 * m + m + 1] / vn;
     double vj = 0.0;
     if (j < m) {
-      vj = R.res[j] / vn;
+      vj = R.res[8 * j + m] / vn;
       R.fv[j] = vj;
-      R.fz[0][j] = R.res[m + j] - cky * vj;
+      R.fz[0][j] = R.res[8 * j + m + 1] - cky * vj;
     }
     __syncwarp();
     const double vvn = vv / (vn * vn);
@@ -310,7 +279,7 @@ static __device__ int fused_refresh(ClusterRed& R, int m, int iters, double vn) 
         double t = 0.0;
         for (int k = 0; k < m; ++k) {
           const double vk = R.fv[k];
-          const double mjk = R.res[3 * m + j * m + k] - vj * vk - vj * (R.res[2 * m + k] / vn) + vj * vk * vvn;
+          const double mjk = R.res[8 * j + k] - vj * vk - vj * (R.res[8 * m + k] / vn) + vj * vk * vvn;
           t += mjk * R.fz[zb][k];
         }
         R.fz[zb ^ 1][j] = t;
@@ -575,12 +544,17 @@ static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows
     }
   }
   if constexpr (MG) {
-    double kyw[kLR];
+    // the unnormalised c_v, K c_v go to this component's columns first: the
+    // reduction reads them across the CTA's threads
 #pragma unroll
-    for (int k = 0; k < kLR; ++k) kyw[k] = rw.ok(k) ? e.Kcy[(size_t)f * n + rw.row(k)] : 0.0;
-    fused_dots(R, CS, KCS, n, m, rw, cv, kv, kyw);
-    const int q0 = 3 * m + m * m;
-    const double vv = R.res[q0];
+    for (int k = 0; k < kLR; ++k)
+      if (rw.ok(k)) {
+        CV[rw.row(k) + (size_t)a * n] = cv[k];
+        KCV[rw.row(k) + (size_t)a * n] = kv[k];
+      }
+    __syncthreads();
+    fused_dots(R, CS, KCS, CV + (size_t)a * n, KCV + (size_t)a * n, e.Kcy + (size_t)f * n, n, m, rw);
+    const double vv = R.res[8 * m + m];
     const double vn = sqrt(vv);
     if (!(vn > 0.0) || !isfinite(vn)) {
       if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;

@@ -111,6 +111,17 @@ struct ClusterRed {
   int buf;
 };
 
+// Per-fit data that no launch changes, staged in shared memory before the
+// dependency wait: x0 and the label of every owned row (-1 outside the fit's
+// training rows) at slot k * T + thread, the class counts and the training
+// row count.
+struct Fixed {
+  double x0[kT * kLR];
+  signed char lab[kT * kLR];
+  double cnt[kMaxM];
+  double nf;
+};
+
 struct Rows {
   int r0, nl;  // first owned row, owned row count
   __device__ __forceinline__ bool ok(int k) const { return (int)threadIdx.x + k * kT < nl; }
@@ -170,6 +181,9 @@ static __device__ void cluster_sum(ClusterRed& R, double (&v)[4], int count) {
 // res[j] = sum over the fit's rows of M[i + j*n] * x_i for j < ncols, with x
 // given by the owned rows in registers.
 // With has_extra, res[ncols] is also the cluster sum of the per-thread value extra.
+// With CG the columns are read through L2 only (ld.global.cg): for data of an
+// earlier grid read before this grid's dependency wait.
+template <bool CG = false>
 static __device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M, int n, int ncols, const Rows& rw,
                                     const double (&x)[kLR], bool has_extra = false, double extra = 0.0) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -191,7 +205,7 @@ static __device__ void cluster_dots(ClusterRed& R, const double* __restrict__ M,
         const double* col = M + (size_t)(c0 + jc) * n;
 #pragma unroll
         for (int k = 0; k < kLR; ++k)
-          if (rw.ok(k)) acc[jj] += col[rw.row(k)] * x[k];
+          if (rw.ok(k)) acc[jj] += (CG ? __ldcg(col + rw.row(k)) : col[rw.row(k)]) * x[k];
       }
 #pragma unroll
       for (int jj = 0; jj < kDotCols; ++jj) {
@@ -299,14 +313,13 @@ static __device__ int fused_refresh(ClusterRed& R, int m, int iters, double vn) 
 // coefficients c_p for the K product.
 // In the merged launch (MG) the refresh was already run by dual_b (c_y, K c_y in
 // pre_cy, pre_ky) and only the scores part follows.
-static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank,
+static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Fixed& P, const Rows& rw, int rank,
                               const double (&pre_cy)[kLR], const double (&pre_ky)[kLR]) {
   __shared__ double wcls[kW][kMaxM + 5];   // per-warp class sums and the reduction's scalars
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m;
   const double* CS = e.CS + (size_t)f * n * m;
   const double* KCS = e.KCS + (size_t)f * n * m;
-  const uint8_t* mk = e.mask + (size_t)f * n;
   double cy[kLR], ky[kLR];
   int steps = e.iters;
   if constexpr (MG) {
@@ -368,15 +381,15 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
     int lab = -1;
     double kt = 0.0;
     if (rw.ok(k)) {
-      const int i = rw.row(k);
+      const int sl = k * kT + threadIdx.x;
       r0 += cy[k] * ky[k];
-      r1 += e.x0[i] * cy[k];
-      if (mk[i]) {
+      r1 += P.x0[sl] * cy[k];
+      if (P.lab[sl] >= 0) {
         kt = ky[k];
         r2 += kt;
         r3 += kt * kt;
         kmax = fmax(kmax, fabs(kt));
-        lab = e.labels[i];
+        lab = P.lab[sl];
       }
     }
     unsigned pending = __ballot_sync(0xffffffffu, lab >= 0);
@@ -415,7 +428,7 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
     return false;
   }
   const double sg = ((y0 >= 0.0) ? -1.0 : 1.0) / nrm;
-  const double nf = static_cast<double>(e.ntrain[f]);
+  const double nf = P.nf;
   const double S = R.res[m + 2], Q = R.res[m + 3];
   // U = X r = sg * K c_y; its mean over the train rows centres the scores
   const double cmean = e.center ? sg * S / nf : 0.0;
@@ -425,7 +438,7 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
   // fallback below reuses the reduction buffer)
   if (rank == 0)
     for (int j = threadIdx.x; j < m; j += kT)
-      e.qs[(size_t)f * m + j] = sg * R.res[j] - cmean * e.class_cnt[(size_t)f * m + j];
+      e.qs[(size_t)f * m + j] = sg * R.res[j] - cmean * P.cnt[j];
 #pragma unroll
   for (int k = 0; k < kLR; ++k) ky[k] *= sg;
   double tn2, st;
@@ -436,7 +449,7 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
     double s2[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int k = 0; k < kLR; ++k)
-      if (rw.ok(k) && mk[rw.row(k)]) {
+      if (rw.ok(k) && P.lab[k * kT + threadIdx.x] >= 0) {
         const double uc = ky[k] - cmean;
         s2[0] += uc * uc;
         s2[1] += uc;
@@ -470,7 +483,7 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
     const int i = rw.row(k);
     const double uc = ky[k] - cmean;
     if (keep) keep[i] = uc;
-    const double c = mk[i] ? (uc - (e.center ? st / nf : 0.0)) / tn : 0.0;
+    const double c = P.lab[k * kT + threadIdx.x] >= 0 ? (uc - (e.center ? st / nf : 0.0)) / tn : 0.0;
     e.cp[(size_t)f * n + i] = c;
     e.Kcy[(size_t)f * n + i] = ky[k] / tn;
     if (e.cpd) {
@@ -503,33 +516,42 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Rows
 // deflation pass accumulates c_y = C_S' z and K c_y = K C_S' z (into fcy, fky)
 // as it writes C_S' and K C_S'.  This saves two cluster reductions and one pass
 // over C_S and K C_S per launch.
+// On entry cv holds c_p of component a (this thread's rows) and, for a > 0,
+// R.res[0 .. a) the Gram-Schmidt coefficients C_V^T K c_p (taken by run()
+// before the dependency wait).
 static __device__ bool dual_b(const DualEng& e, int a, ClusterRed& R, const Rows& rw, int rank,
-                              const int (&ks0)[kLR], const int (&ks1)[kLR], double (&fcy)[kLR],
-                              double (&fky)[kLR]) {
+                              const int (&ks0)[kLR], const int (&ks1)[kLR], double (&cv)[kLR],
+                              double (&fcy)[kLR], double (&fky)[kLR]) {
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m, K = e.K;
   double* CV = e.CV + (size_t)f * n * K;
   double* KCV = e.KCV + (size_t)f * n * K;
   double* CS = e.CS + (size_t)f * n * m;
   double* KCS = e.KCS + (size_t)f * n * m;
-  double cv[kLR], kv[kLR];
+  double kv[kLR];
 #pragma unroll
   for (int k = 0; k < kLR; ++k) {
-    cv[k] = rw.ok(k) ? e.cp[(size_t)f * n + rw.row(k)] : 0.0;
     kv[k] = 0.0;
     if (!rw.ok(k)) continue;
     const int i = rw.row(k);
     if (e.kpart) {
+      // the tile's segments in order, eight loads in flight at a time
       const double* pp = e.kpart + (size_t)(f & 63) * 128 + (i & 127);
       double v = 0.0;
-      for (int sg = ks0[k]; sg < ks1[k]; ++sg) v += pp[(size_t)sg * 64 * 128];
+      for (int s0 = ks0[k]; s0 < ks1[k]; s0 += 8) {
+        double t[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) t[u] = s0 + u < ks1[k] ? pp[(size_t)(s0 + u) * 64 * 128] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (s0 + u < ks1[k]) v += t[u];
+      }
       kv[k] = v;
     } else {
       kv[k] = e.Gp[(size_t)f * n + i];
     }
   }
   if (a > 0) {
-    cluster_dots(R, CV, n, a, rw, kv);   // V^T p = C_V^T K c_p
 #pragma unroll (kColUnroll)
     for (int l = 0; l < a; ++l) {
       const double wl = R.res[l];
@@ -693,11 +715,34 @@ static __device__ void run(const DualEng& e, int a) {
       ks1[k] = e.kseg[tile + 1];
     }
   }
-  tc::grid_dep_wait();     // the previous product / step has completed
-  tc::grid_dep_launch();
-  if (e.status[f]) return;   // set only in earlier launches: uniform over the cluster, before any remote access
+  __shared__ Fixed P;
+#pragma unroll
+  for (int k = 0; k < kLR; ++k)
+    if (rw.ok(k)) {
+      const int i = rw.row(k);
+      P.x0[k * kT + threadIdx.x] = e.x0[i];
+      P.lab[k * kT + threadIdx.x] = e.mask[(size_t)f * e.n + i] ? static_cast<signed char>(e.labels[i]) : -1;
+    }
+  for (int j = threadIdx.x; j < e.m; j += kT) P.cnt[j] = e.class_cnt[(size_t)f * e.m + j];
+  if (threadIdx.x == 0) P.nf = static_cast<double>(e.ntrain[f]);
+  // The product this grid depends on releases it only after its own wait, so
+  // the step launch before it has completed: its outputs (c_p, K C_V, the fit
+  // status) are read through L2 before this grid's wait, and the Gram-Schmidt
+  // coefficients of component a - 1, C_V^T K c_p = (K C_V)^T c_p (K is
+  // symmetric), are reduced while the product finishes.
+  if (__ldcg(e.status + f)) return;   // set only in earlier launches: uniform over the cluster
   if (threadIdx.x == 0) R.buf = 0;
   __syncthreads();
+  double cv[kLR];
+#pragma unroll
+  for (int k = 0; k < kLR; ++k) cv[k] = 0.0;
+  if (a > 0) {
+#pragma unroll
+    for (int k = 0; k < kLR; ++k) cv[k] = rw.ok(k) ? __ldcg(e.cp + (size_t)f * e.n + rw.row(k)) : 0.0;
+    if (a > 1) cluster_dots<true>(R, e.KCV + (size_t)f * e.n * e.K, e.n, a - 1, rw, cv);
+  }
+  tc::grid_dep_wait();     // the previous product has completed
+  tc::grid_dep_launch();
   // Every CTA of the cluster takes the same branches (they follow the
   // cluster-wide sums, identical in all CTAs), and all of them end on the same
   // cluster barrier, which also keeps each CTA's shared memory alive until the
@@ -706,8 +751,8 @@ static __device__ void run(const DualEng& e, int a) {
   // set allows it (e.merge).
   bool ok = true;
   double fcy[kLR], fky[kLR];
-  if (a > 0) ok = dual_b(e, a - 1, R, rw, rank, ks0, ks1, fcy, fky);
-  if (ok && a < e.K) dual_a(e, a, R, rw, rank, fcy, fky);
+  if (a > 0) ok = dual_b(e, a - 1, R, rw, rank, ks0, ks1, cv, fcy, fky);
+  if (ok && a < e.K) dual_a(e, a, R, P, rw, rank, fcy, fky);
   if constexpr (CL > 1) cg::this_cluster().sync();
 }
 };  // struct Step

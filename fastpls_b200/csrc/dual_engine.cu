@@ -902,9 +902,16 @@ void dual_simpls_run(const DualBatch& b) {
   for (int a = 0; a <= b.K; ++a) {
     // algorithmic bytes of one step launch (all fits): the Gram-Schmidt and
     // deflation of component a - 1 and the refresh / scores of component a
+    // (merged launch: c_p, K c_p, the 3 (a - 1) Gram-Schmidt columns, c_v and
+    // K c_v stored twice, the 8 x 8 product's 2m + 3 columns, the deflation's
+    // 4m, and x0, t, c_p, K c_y of the scores part)
     double words = 0.0;
-    if (a > 0) words += (4.0 + 3.0 * (a - 1) + 5.0 * md) * nd;
-    if (a < b.K) words += (5.0 + md + 2.0 * it * md + std::max(it - 1.0, 0.0) * md) * nd;
+    if (e.merge && a > 0 && a < b.K) {
+      words = (13.0 + 3.0 * (a - 1) + 6.0 * md) * nd;
+    } else {
+      if (a > 0) words += (4.0 + 3.0 * (a - 1) + 5.0 * md) * nd;
+      if (a < b.K) words += (5.0 + md + 2.0 * it * md + std::max(it - 1.0, 0.0) * md) * nd;
+    }
     const int slot = ctx.prof_begin("dual_step", st);
     launch_step(cfg, e, a, b.F, st);
     ctx.prof_end(slot, st, Fd * (8.0 * words + (a < b.K ? 5.0 * nd : 0.0)), 0.0);

@@ -337,6 +337,62 @@ __global__ void split_rows_kernel(const T* __restrict__ X, int rows, int cols, i
 }
 
 
+// The same split with TR x 64 tiles (TR rows of X, 64 columns): each warp reads
+// columns of the tile as TR / 32 runs of 128 bytes, and writes rows of the
+// planes as BF16 pairs (128 bytes per warp and plane).  Needs ldo and the
+// column offset of hi / lo / mid even (4-byte pairs).
+template <typename T, int TR>
+__global__ void __launch_bounds__(256) split_rows_tile_kernel(const T* __restrict__ X, int rows, int cols, int ld,
+                                                               __nv_bfloat16* __restrict__ hi,
+                                                               __nv_bfloat16* __restrict__ lo, int ldo,
+                                                               __nv_bfloat16* __restrict__ mid,
+                                                               const double* __restrict__ mean, int wcols) {
+  __shared__ T tile[64][TR + 1];   // tile[column][row] of the block
+  const int i0 = blockIdx.y * TR, j0 = blockIdx.x * 64;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int jj = warp + 8 * c, j = j0 + jj;
+    T v[TR / 32];
+#pragma unroll
+    for (int u = 0; u < TR / 32; ++u) v[u] = T(0);
+    if (j < cols) {
+      const T* col = X + static_cast<size_t>(j) * ld + i0;
+#pragma unroll
+      for (int u = 0; u < TR / 32; ++u)
+        if (i0 + lane + 32 * u < rows) v[u] = col[lane + 32 * u];
+    }
+#pragma unroll
+    for (int u = 0; u < TR / 32; ++u) tile[jj][lane + 32 * u] = v[u];
+  }
+  __syncthreads();
+  const int jj = 2 * lane, j = j0 + jj;
+  if (j >= wcols) return;
+  const double m0 = (mean && j < cols) ? mean[j] : 0.0;
+  const double m1 = (mean && j + 1 < cols) ? mean[j + 1] : 0.0;
+  const bool pair = j + 1 < wcols;
+#pragma unroll 4
+  for (int r = 0; r < TR / 8; ++r) {
+    const int ii = warp + 8 * r, i = i0 + ii;
+    if (i >= rows) break;
+    const double x0 = j < cols ? static_cast<double>(tile[jj][ii]) - m0 : 0.0;
+    const double x1 = j + 1 < cols ? static_cast<double>(tile[jj + 1][ii]) - m1 : 0.0;
+    __nv_bfloat16 h0, l0, d0, h1, l1, d1;
+    split_value(x0, h0, mid ? &d0 : nullptr, l0);
+    split_value(x1, h1, mid ? &d1 : nullptr, l1);
+    const size_t o = static_cast<size_t>(i) * ldo + j;
+    if (pair) {
+      *reinterpret_cast<__nv_bfloat162*>(hi + o) = __halves2bfloat162(h0, h1);
+      *reinterpret_cast<__nv_bfloat162*>(lo + o) = __halves2bfloat162(l0, l1);
+      if (mid) *reinterpret_cast<__nv_bfloat162*>(mid + o) = __halves2bfloat162(d0, d1);
+    } else {
+      hi[o] = h0;
+      lo[o] = l0;
+      if (mid) mid[o] = d0;
+    }
+  }
+}
+
 // 2-D BF16 tensor map: `rows` rows of `k` elements, row pitch ld elements.
 CUtensorMap make_map(const __nv_bfloat16* base, int rows, int k, int ld, int box_rows) {
   CUtensorMap m;
@@ -398,7 +454,11 @@ struct GemmPlan {
 // reach the upper triangle (tile row start < tile column end) are planned, for
 // symmetric products whose lower triangle is mirrored afterwards.
 constexpr int kSymSegBlocks = 16;
-constexpr int kSymChunkBlocks = 64;   // K-blocks per chunk of a symmetric plan (a multiple of kSymSegBlocks)
+// Segments of the symmetric (row Gram) plan: 32 K-blocks (2048 terms in FP32;
+// sqrt(2) more rounding than 16 blocks, still far below the BF16 split error)
+// halve the FP32 partials written and summed.
+constexpr int kGramSegBlocks = 32;
+constexpr int kSymChunkBlocks = 64;   // K-blocks per chunk of a symmetric plan (a multiple of kGramSegBlocks)
 // Products that take the split path in the mixed precision mode.
 constexpr int kMixedMinK = 256;
 constexpr double kMixedMinWork = 1e7;
@@ -416,10 +476,10 @@ GemmPlan plan_gemm(int M, int N, int K, int sm_count, bool upper = false, bool s
     if (!upper || (t / g.ntn) * BM < ((t % g.ntn) + 1) * bn) inc.push_back(t);
   const int kbt = (K + BK - 1) / BK;
   // A symmetric (Gram) product sums the whole contraction of each tile in one
-  // CTA; cutting it (and every three-plane product) into segments of at most
-  // kSymSegBlocks K-blocks keeps each FP32 accumulation short and adds the
-  // segments in FP64.
-  const int kseg = (upper || short_segments) ? kSymSegBlocks : kbt;
+  // CTA; cutting it into segments of at most kGramSegBlocks K-blocks (every
+  // three-plane product into kSymSegBlocks) keeps each FP32 accumulation short
+  // and adds the segments in FP64.
+  const int kseg = upper ? kGramSegBlocks : (short_segments ? kSymSegBlocks : kbt);
   const long long total = static_cast<long long>(inc.size()) * kbt;
   g.ctas = static_cast<int>(std::max<long long>(1, std::min<long long>(sm_count, total)));
   g.cta_begin.assign(g.ctas + 1, 0);
@@ -656,9 +716,17 @@ template <typename T>
 void split_rows_on(const T* X, int rows, int cols, int ld, const SplitPair& out, cudaStream_t st,
                    const double* mean = nullptr, int col0 = 0, int wcols = -1) {
   if (wcols < 0) wcols = out.ld - col0;
-  dim3 grid((wcols + 31) / 32, (rows + 31) / 32);
-  split_rows_kernel<T><<<grid, dim3(32, 8), 0, st>>>(X, rows, cols, ld, out.hi + col0, out.lo + col0, out.ld,
-                                                     out.mid ? out.mid + col0 : nullptr, mean, wcols);
+  if (((out.ld | col0) & 1) == 0) {
+    // 128-row tiles for FP32 (33 KB of shared memory), 64-row tiles for FP64
+    constexpr int TR = sizeof(T) == 4 ? 128 : 64;
+    dim3 grid((wcols + 63) / 64, (rows + TR - 1) / TR);
+    split_rows_tile_kernel<T, TR><<<grid, 256, 0, st>>>(X, rows, cols, ld, out.hi + col0, out.lo + col0, out.ld,
+                                                        out.mid ? out.mid + col0 : nullptr, mean, wcols);
+  } else {
+    dim3 grid((wcols + 31) / 32, (rows + 31) / 32);
+    split_rows_kernel<T><<<grid, dim3(32, 8), 0, st>>>(X, rows, cols, ld, out.hi + col0, out.lo + col0, out.ld,
+                                                       out.mid ? out.mid + col0 : nullptr, mean, wcols);
+  }
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }

@@ -796,10 +796,25 @@ int fpls_int8_emulated_gemm(const double* A, int M, int K, const double* B, int 
   });
 }
 
-static void run_cv_grid(const CvFitSet& fs, const void* X, int x_is_float32, bool x_on_device,
-                        const int* y, const int* ncomp, int L, int scaling, int precision,
-                        int batched, CvGridResult& res) {
+// X of a CV call on the device: the caller's matrix when resident, else an
+// arena buffer that the driver fills from the host matrix.
+struct CvX {
+  const double* x64 = nullptr;
+  const float* x32 = nullptr;
+  const void* host = nullptr;
+};
+
+static CvX cv_x(const void* X, int x_is_float32, bool x_on_device, int n, int p) {
   Context& ctx = Context::get();
+  CvX c;
+  const size_t np = (size_t)n * p;
+  c.host = x_on_device ? nullptr : X;
+  if (x_is_float32) c.x32 = x_on_device ? static_cast<const float*>(X) : ctx.arena.alloc_n<float>(np);
+  else c.x64 = x_on_device ? static_cast<const double*>(X) : ctx.arena.alloc_n<double>(np);
+  return c;
+}
+
+static CvGridOptions cv_options(int scaling, int precision, int batched) {
   FPLS_REQUIRE(precision == FPLS_PREC_FP64 || precision == FPLS_PREC_BF16X3, "unknown precision");
   CvGridOptions opt;
   opt.scaling = scaling;
@@ -810,17 +825,15 @@ static void run_cv_grid(const CvFitSet& fs, const void* X, int x_is_float32, boo
     long v = std::strtol(e, &endp, 10);
     if (endp != e) opt.power_iters = static_cast<int>(std::min(6L, std::max(1L, v)));
   }
-  const size_t np = (size_t)fs.n * fs.p;
+  return opt;
+}
+
+// prep: the X-side work already enqueued by the caller (batched grids), or null.
+static void run_cv_grid(const CvFitSet& fs, const CvX& x, const int* y, const int* ncomp, int L,
+                        const CvGridOptions& opt, CvGridResult& res, CvPreparedX* prep = nullptr) {
+  Context& ctx = Context::get();
   dzero(ctx.d_status + 16, sizeof(int));
-  // Host X: the driver uploads it (overlapped with its first passes where it can).
-  const void* xh = x_on_device ? nullptr : X;
-  if (x_is_float32) {
-    const float* d = x_on_device ? static_cast<const float*>(X) : ctx.arena.alloc_n<float>(np);
-    cv_grid_classify(fs, nullptr, d, y, ncomp, L, opt, res, xh);
-  } else {
-    const double* d = x_on_device ? static_cast<const double*>(X) : ctx.arena.alloc_n<double>(np);
-    cv_grid_classify(fs, d, nullptr, y, ncomp, L, opt, res, xh);
-  }
+  cv_grid_classify(fs, x.x64, x.x32, y, ncomp, L, opt, res, prep ? nullptr : x.host, prep);
   int e = 0;
   d2h(&e, ctx.d_status + 16, sizeof(int));
   ctx.sync();
@@ -854,7 +867,8 @@ int fpls_cv_predict(const void* X, int x_is_float32, int n, int p, const int* y,
     std::vector<int> nc(ncomp, ncomp + L);
     for (int& c : nc) c = std::max(1, c);
     CvGridResult res;
-    run_cv_grid(fs, X, x_is_float32, false, y, nc.data(), L, scaling, precision, batched, res);
+    const CvGridOptions opt = cv_options(scaling, precision, batched);
+    run_cv_grid(fs, cv_x(X, x_is_float32, false, n, p), y, nc.data(), L, opt, res);
     download(class_pred, res.d_pred, (size_t)n * L);
     ctx.sync();
     if (status) std::copy(res.status.begin(), res.status.end(), status);
@@ -898,15 +912,24 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     for (int& c : nc) c = std::max(1, c);
     CvFitSet fs;
     fs.n = n; fs.p = p; fs.m = n_classes; fs.F = S * Ki + S; fs.G = S + 1;
-    fs.train.assign((size_t)fs.F * n, 0);
-    fs.test.assign((size_t)fs.F * n, 0);
-    fs.group.assign(fs.F, 0);
-    fs.seeds.resize(fs.F);
     std::vector<int> outer_classes(S, 0), fallback(S, 1);
     const int m = n_classes;
     FPLS_REQUIRE(m >= 1, "n_classes must be >= 1");
     for (int i = 0; i < n; ++i)
       FPLS_REQUIRE(y[i] >= 1 && y[i] <= m, "labels must be in 1..n_classes");
+    // The X-side work of the grid (upload, column means, BF16 planes, row Gram)
+    // does not depend on the folds: enqueued first, it runs on the GPU while
+    // the fold set-up below runs on the host.
+    const CvGridOptions opt = cv_options(scaling, precision, batched);
+    const CvX cx = cv_x(X, x_is_float32, x_on_device, n, p);
+    std::unique_ptr<CvPreparedX> prep;
+    if (opt.batched && opt.scaling != 2 && fs.p > 5)
+      prep = cv_prepare_x(cx.x64, cx.x32, n, p, m, *std::max_element(nc.begin(), nc.end()), opt, cx.host);
+    pt.mark("X preparation (enqueue)");
+    fs.train.assign((size_t)fs.F * n, 0);
+    fs.test.assign((size_t)fs.F * n, 0);
+    fs.group.assign(fs.F, 0);
+    fs.seeds.resize(fs.F);
     // Slot of every row: s when the row belongs to outer fold ids[s], else -1.
     std::vector<int> slot_of_fold(Ko, -1), row_slot(n, -1);
     for (int s = 0; s < S; ++s) slot_of_fold[ids[s]] = s;
@@ -980,7 +1003,7 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     }
     CvGridResult res;
     pt.mark("folds (host)");
-    run_cv_grid(fs, X, x_is_float32, x_on_device, y, nc.data(), L, scaling, precision, batched, res);
+    run_cv_grid(fs, cx, y, nc.data(), L, opt, res, prep.get());
     pt.mark("grid");
     // Inner accuracy per (outer fold, ncomp) on the device; the chosen ncomp is the
     // first maximum (.cv_best_index); only counts and the outer predictions return.

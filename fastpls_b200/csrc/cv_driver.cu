@@ -228,39 +228,39 @@ std::vector<int> upload_chunks(int p) {
   return b;
 }
 
-void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const int* y, const int* ncomp, int L,
-                 const CvGridOptions& opt, const std::vector<int>& status,
-                 const std::vector<double>& counts, double* d_om, CvGridResult& res,
-                 const void* x_host) {
+}  // namespace
+
+std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, int n, int p, int m, int kmax,
+                                          const CvGridOptions& opt, const void* x_host) {
   Context& ctx = Context::get();
   Arena& ar = ctx.arena;
-  const int n = fs.n, p = fs.p, m = fs.m;
-  const int K = *std::max_element(ncomp, ncomp + L);
-  FPLS_REQUIRE(m <= kMaxClassesCv, "batched CV supports at most 128 classes");
-  // Active fits only (status 1) go to the engine.
-  std::vector<int> act;
-  for (int f = 0; f < fs.F; ++f)
-    if (status[f] == 1) act.push_back(f);
-  const int Fa = static_cast<int>(act.size());
-  res.ncomp_done.assign(fs.F, 0);
-  if (Fa == 0) return;
-  PhaseTimer pt("CV grid (batched)");
+  FPLS_REQUIRE(opt.batched && opt.scaling != 2, "X preparation is for batched grids");
+  std::unique_ptr<CvPreparedX> px(new CvPreparedX());
+  px->n = n; px->p = p; px->m = m; px->kmax = kmax; px->precision = opt.precision;
+  PhaseTimer pt("CV grid X preparation");
   // Global centring (scaling < 3): Xc = X - mean(X); folds shift by delta_f.
-  const bool center = opt.scaling < 3;
+  const bool center = px->center = opt.scaling < 3;
   // Short, wide predictor blocks run the loop in the row space of X (the
   // row Gram K = Xc Xc^T); otherwise in the predictor space.
-  const bool dual = dual_engine_applies(n, p, m, K);
+  const bool dual = px->dual = dual_engine_applies(n, p, m, kmax);
   // The mixed row-space loop needs only the BF16 planes of Xc, split straight
   // from the caller's matrix; every other combination works on a centred FP64
   // copy.  x0 is the first column of Xc (the Householder sign of the sketch).
   const bool planes_only = opt.precision == 1 && dual;
-  FPLS_REQUIRE(!x_host || planes_only, "chunked upload outside the mixed row-space path");
-  double* mall = center ? ar.alloc_n<double>(p) : nullptr;
-  double* Kg = dual ? ar.alloc_n<double>((size_t)n * n) : nullptr;
+  // A host X goes up in overlapped column chunks on the mixed row-space path,
+  // else in one copy first.
+  if (x_host && !planes_only) {
+    if (x64) h2d(const_cast<double*>(x64), x_host, (size_t)n * p * sizeof(double));
+    else h2d(const_cast<float*>(x32), x_host, (size_t)n * p * sizeof(float));
+    x_host = nullptr;
+  }
+  double* mall = px->mall = center ? ar.alloc_n<double>(p) : nullptr;
+  double* Kg = px->Kg = dual ? ar.alloc_n<double>((size_t)n * n) : nullptr;
   bool gram_done = false;
   double* X = nullptr;
   double* x0 = nullptr;
   std::unique_ptr<XOperator> xop;
+
   if (x_host) {
     // X arrives in column chunks on the copy stream; each chunk's column means,
     // BF16 planes and row-Gram contribution run as soon as it has landed, while
@@ -320,6 +320,52 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
     }
   }
   pt.mark("operator");
+  // The Gram contracts over all p columns (BF16x3 on the tensor cores in the
+  // mixed mode); the per-component products with the L2-resident K stay
+  // FP64-accurate: the K-coordinate Gram-Schmidt carries K C_V and K C_S
+  // forward, and split-precision products there drift from one component to
+  // the next.  Mixed mode: the K products on the INT8 tensor cores (digit
+  // planes of K split once); FP64 mode: FP64 DMMA.
+  if (dual) {
+    if (!gram_done) xop->gram(Kg);
+    px->kop_f64.reset(new XOperatorF64(Kg, n, n));
+    if (opt.precision == 1 && int8_k_products()) {
+      px->kop_slices = ozaki_default_slices();
+      px->kop_int8 = make_ozaki_sym_operator(Kg, n, px->kop_slices);
+    }
+    pt.mark("row gram");
+  }
+  px->X = X;
+  px->x0 = x0;
+  px->xop = std::move(xop);
+  pt.report();
+  return px;
+}
+
+namespace {
+
+void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, const CvGridOptions& opt,
+                 const std::vector<int>& status, const std::vector<double>& counts, double* d_om,
+                 CvGridResult& res, CvPreparedX& px) {
+  Context& ctx = Context::get();
+  Arena& ar = ctx.arena;
+  const int n = fs.n, p = fs.p, m = fs.m;
+  const int K = *std::max_element(ncomp, ncomp + L);
+  FPLS_REQUIRE(m <= kMaxClassesCv, "batched CV supports at most 128 classes");
+  FPLS_REQUIRE(px.n == n && px.p == p && px.m == m && px.kmax == K && px.precision == opt.precision,
+               "prepared X does not match the grid");
+  // Active fits only (status 1) go to the engine.
+  std::vector<int> act;
+  for (int f = 0; f < fs.F; ++f)
+    if (status[f] == 1) act.push_back(f);
+  const int Fa = static_cast<int>(act.size());
+  res.ncomp_done.assign(fs.F, 0);
+  if (Fa == 0) return;
+  PhaseTimer pt("CV grid (batched)");
+  const bool center = px.center, dual = px.dual;
+  double* X = px.X;
+  double* x0 = px.x0;
+  std::unique_ptr<XOperator>& xop = px.xop;
   std::vector<uint8_t> tr((size_t)Fa * n), te((size_t)Fa * n);
   std::vector<int> grp(Fa), ntrain(Fa);
   std::vector<double> inv_nf(Fa), mYf((size_t)Fa * m), mYall(m, 0.0), dY((size_t)Fa * m);
@@ -371,23 +417,9 @@ void run_batched(const CvFitSet& fs, const double* x64, const float* x32, const 
   int* ncd = ar.alloc_n<int>(Fa);
   int* sto = ar.alloc_n<int>(Fa);
   if (dual) {
-    // The Gram contracts over all p columns (BF16x3 on the tensor cores in the
-    // mixed mode); the per-component products with the L2-resident K stay
-    // FP64: the K-coordinate Gram-Schmidt carries K C_V and K C_S forward, and
-    // split-precision products there drift from one component to the next.
-    if (!gram_done) xop->gram(Kg);
-    XOperatorF64 kop_f64(Kg, n, n);
-    XOperator* kop = &kop_f64;
-    // Mixed mode: the K products on the INT8 tensor cores (digit planes of K
-    // split once, FP64-level accuracy); FP64 mode: FP64 DMMA.
-    std::unique_ptr<XOperator> kop_int8;
-    int kop_slices = 0;
-    if (opt.precision == 1 && int8_k_products()) {
-      kop_slices = ozaki_default_slices();
-      kop_int8 = make_ozaki_sym_operator(Kg, n, kop_slices);
-      kop = kop_int8.get();
-    }
-    pt.mark("row gram");
+    XOperator* kop = px.kop_int8 ? px.kop_int8.get() : px.kop_f64.get();
+    const int kop_slices = px.kop_slices;
+    pt.mark("fold set-up");
     FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0));
     double* XOm = ar.alloc_n<double>((size_t)n * Fa);
     xop->times(d_om, Fa, XOm);
@@ -566,7 +598,7 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
 
 void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
                       const int* labels_host, const int* ncomp, int L,
-                      const CvGridOptions& opt, CvGridResult& res, const void* x_host) {
+                      const CvGridOptions& opt, CvGridResult& res, const void* x_host, CvPreparedX* prep) {
   Context& ctx = Context::get();
   PhaseTimer pt("CV grid set-up");
   FPLS_REQUIRE(L >= 1, "ncomp must contain at least one value");
@@ -589,8 +621,15 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
     if (!seeds.empty()) {
       unsigned int* d_seeds = ctx.arena.alloc_n<unsigned int>(seeds.size());
       d_om = ctx.arena.alloc_n<double>(seeds.size() * (size_t)fs.p);
-      FPLS_CUDA(cudaEventRecord(ctx.side_done, ctx.stream));  // arena reuse: after earlier work
-      FPLS_CUDA(cudaStreamWaitEvent(ctx.side, ctx.side_done, 0));
+      // The sketch buffers are fresh arena memory of this call, so the side
+      // stream only follows the work of earlier calls (the call's start event),
+      // not the X-side work of this call enqueued before it.
+      if (ctx.call_started) {
+        FPLS_CUDA(cudaStreamWaitEvent(ctx.side, ctx.call_start, 0));
+      } else {
+        FPLS_CUDA(cudaEventRecord(ctx.side_done, ctx.stream));
+        FPLS_CUDA(cudaStreamWaitEvent(ctx.side, ctx.side_done, 0));
+      }
       FPLS_CUDA(cudaMemcpyAsync(d_seeds, seeds.data(), seeds.size() * sizeof(unsigned), cudaMemcpyHostToDevice,
                                 ctx.side));
       device_gaussian_streams(d_om, fs.p, fs.p, d_seeds, static_cast<int>(seeds.size()), ctx.side);
@@ -612,17 +651,19 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
   }
   pt.mark("prediction buffers");
   pt.report();
-  // Overlapped upload only where the loop needs just the BF16 planes and the
-  // row Gram of X; otherwise X is copied whole before use.
-  const int Kmax = *std::max_element(ncomp, ncomp + L);
-  const bool chunked = x_host && batched && opt.precision == 1 && dual_engine_applies(fs.n, fs.p, fs.m, Kmax);
-  if (x_host && !chunked) {
+  if (batched) {
+    // the X-side work (and a host X's upload), unless the caller enqueued it
+    std::unique_ptr<CvPreparedX> own;
+    if (!prep) {
+      own = cv_prepare_x(x64, x32, fs.n, fs.p, fs.m, *std::max_element(ncomp, ncomp + L), opt, x_host);
+      prep = own.get();
+    }
+    run_batched(fs, labels_host, ncomp, L, opt, status, counts, d_om, res, *prep);
+    return;
+  }
+  if (x_host) {
     if (x64) h2d(const_cast<double*>(x64), x_host, (size_t)fs.n * fs.p * sizeof(double));
     else h2d(const_cast<float*>(x32), x_host, (size_t)fs.n * fs.p * sizeof(float));
-  }
-  if (batched) {
-    run_batched(fs, x64, x32, labels_host, ncomp, L, opt, status, counts, d_om, res, chunked ? x_host : nullptr);
-    return;
   }
   // The per-fit path reads X in FP64 (widened once when the caller's is FP32).
   const double* X = x64;

@@ -4,9 +4,11 @@
 // of the same passes (no extra pass over X).
 #pragma once
 
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
+#include "simpls_engine.cuh"
 
 namespace fpls {
 
@@ -45,6 +47,30 @@ struct CvGridResult {
 void cv_prediction_counts(const int* d_pred, int G, int L, int n, const int* d_labels,
                           const int* d_exclude, std::vector<long long>& counts);
 
+// The fold-independent X-side work of a batched CV grid: the column means, the
+// BF16 planes of Xc (mixed row-space path) or a centred FP64 copy of X, its
+// first centred column x0 and, on the row-space path, the row Gram
+// K = Xc Xc^T with the operator of the per-component K products.
+// cv_prepare_x enqueues it on the library stream (a host X is uploaded first,
+// or in overlapped column chunks on the mixed row-space path);
+// cv_grid_classify does the same itself unless it is given one prepared for
+// the same X, class count, largest ncomp and options.
+struct CvPreparedX {
+  bool center = false, dual = false;
+  int n = 0, p = 0, m = 0, kmax = 0, precision = 0;
+  double* mall = nullptr;   // p column means when centred
+  double* Kg = nullptr;     // n x n row Gram (row-space path)
+  double* X = nullptr;      // centred FP64 copy (every path but the mixed row-space one)
+  double* x0 = nullptr;     // first centred column
+  std::unique_ptr<XOperator> xop, kop_f64, kop_int8;
+  int kop_slices = 0;
+};
+
+// Batched grids only (opt.batched with scaling != 2); x64 / x32 as in
+// cv_grid_classify (the device buffer to fill when x_host is given).
+std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, int n, int p, int m, int kmax,
+                                          const CvGridOptions& opt, const void* x_host);
+
 // X: device predictor matrix n x p, FP64 (x64) or FP32 (x32, exactly widened).
 // labels_host: 1-based class labels.  ncomp: L values (host).  With x_host the
 // device buffer is empty and x_host holds the same matrix in host memory: the
@@ -52,6 +78,7 @@ void cv_prediction_counts(const int* d_pred, int G, int L, int n, const int* d_l
 // BF16 split and the row Gram on the mixed row-space path, else in one copy.
 void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
                       const int* labels_host, const int* ncomp, int L,
-                      const CvGridOptions& opt, CvGridResult& res, const void* x_host = nullptr);
+                      const CvGridOptions& opt, CvGridResult& res, const void* x_host = nullptr,
+                      CvPreparedX* prep = nullptr);
 
 }  // namespace fpls

@@ -135,7 +135,7 @@ KERNEL_CLASSES = {
     "dual_step": ("hbm", "hbm", "k_dual_step<4, 512, 2, *> (per-fit SIMPLS steps in row space, 4-CTA clusters; "
                   "merged launches for 0 < a < K)", "k_dual_step_c4_traffic.json"),
     "k_products_f64": ("tensor", "fp64", "gemm_f64_dmma (batched K products, FP64 DMMA)", None),
-    "k_products_int8": ("tensor", "int8", "ozaki_gemm_kernel<6> (batched K products on INT8 tcgen05 digit planes; "
+    "k_products_int8": ("tensor", "int8", "ozaki_gemm_kernel<5> (batched K products on INT8 tcgen05 digit planes; "
                         "TOP/s of int8 plane products)", "ozaki_gemm_c4_traffic.json"),
     "gram_bf16x3": ("tensor", "bf16", "split_gemm_kernel<2, 128> (tcgen05 BF16x3 row Gram, upper tiles)",
                     "gram_bf16x3_c4_traffic.json"),

@@ -662,9 +662,11 @@ int ozaki_default_slices() {
     const int v = std::atoi(e);
     if (v >= kOzakiMinSlices && v <= kOzakiMaxSlices) return v;
   }
-  // 2^-42 of the row scales: on the omics double-CV grid 5, 6 and 7 slices
-  // give the same predictions as FP64 products and 4 do not; 6 keeps a margin.
-  return 6;
+  // 2^-35 of the row scales, about four orders of magnitude below the error
+  // the BF16x3 row Gram already carries: on the omics double-CV grid 5, 6 and 7
+  // slices give the same predictions as FP64 products (5 and 6 the same to the
+  // last inner prediction) and 4 do not.
+  return 5;
 }
 
 }  // namespace fpls

@@ -77,6 +77,35 @@ __global__ void gather_outer_pred_kernel(const int* __restrict__ pred, const int
   out[i] = fb[o] ? fb[o] : pred[((size_t)Ko * L + best_slice[o]) * n + i];
 }
 
+// Slot s of a double CV (outer fold ids[s]): the inner accuracy of every ncomp
+// slice from the prediction counts (NaN when no row was predicted), the first
+// slice of maximal finite accuracy (.cv_best_index) and the chosen ncomp (the
+// smallest one for a single-class fold, fb[s] != 0, whose rows get the
+// fallback class).
+__global__ void select_ncomp_kernel(const long long* __restrict__ counts, int S, int L, const int* __restrict__ ids,
+                                    int Ko, const int* __restrict__ nc, const int* __restrict__ fb, int nc_min,
+                                    double* __restrict__ acc_out, int* __restrict__ best_slice,
+                                    int* __restrict__ best_comp) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  const int o = ids[s];
+  int bi = 0;
+  double bv = -1.0;
+  bool any = false;
+  for (int l = 0; l < L; ++l) {
+    const long long ok = counts[2 * ((size_t)s * L + l)], tot = counts[2 * ((size_t)s * L + l) + 1];
+    const double acc = tot ? static_cast<double>(ok) / static_cast<double>(tot) : nan("");
+    acc_out[o + (size_t)l * Ko] = acc;
+    if (isfinite(acc) && (!any || acc > bv)) {
+      bv = acc;
+      bi = l;
+      any = true;
+    }
+  }
+  best_slice[s] = bi;
+  best_comp[o] = fb[s] ? nc_min : nc[bi];
+}
+
 void lda_outputs_to_host(const LdaModelsDev& d, int C, int kmax, int L, double* means,
                          double* linear, double* constants, double* priors) {
   download(means, d.means, (size_t)C * kmax * L);
@@ -1009,28 +1038,26 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     // first maximum (.cv_best_index); only counts and the outer predictions return.
     const int* d_y = upload(y, n);
     const int* d_slot = upload(row_slot.data(), n);
-    std::vector<long long> cnts;
-    cv_prediction_counts(res.d_pred, S, L, n, d_y, d_slot, cnts);
-    pt.mark("counts");
-    std::vector<int> best_slice(S, 0), fb(S, 0);
-    for (int s = 0; s < S; ++s) {
-      const int o = ids[s];
-      int bi = 0;
-      double bv = -1.0;
-      bool any = false;
-      for (int l = 0; l < L; ++l) {
-        const long long ok = cnts[2 * ((size_t)s * L + l)], tot = cnts[2 * ((size_t)s * L + l) + 1];
-        const double acc = tot ? static_cast<double>(ok) / tot : std::nan("");
-        if (inner_accuracy) inner_accuracy[o + (size_t)l * Ko] = acc;
-        if (std::isfinite(acc) && (!any || acc > bv)) { bv = acc; bi = l; any = true; }
-      }
-      const bool skip = outer_classes[s] < 2;
-      best_slice[s] = bi;
-      fb[s] = skip ? fallback[s] : 0;
-      if (best_comp) best_comp[o] = skip ? *std::min_element(nc.begin(), nc.end()) : nc[bi];
-    }
-    int* d_best = upload(best_slice.data(), S);
+    // Accuracies, the chosen ncomp and the outer predictions on the device;
+    // one download and one synchronisation at the end.
+    const long long* d_cnt = cv_prediction_counts_device(res.d_pred, S, L, n, d_y, d_slot);
+    std::vector<int> fb(S, 0);
+    for (int s = 0; s < S; ++s) fb[s] = outer_classes[s] < 2 ? fallback[s] : 0;
     int* d_fb = upload(fb.data(), S);
+    const int* d_ids = upload(ids.data(), S);
+    const int* d_nc = upload(nc.data(), L);
+    double* d_acc = ctx.arena.alloc_n<double>((size_t)Ko * L);
+    int* d_best = ctx.arena.alloc_n<int>(S);
+    int* d_bcomp = ctx.arena.alloc_n<int>(Ko);
+    select_ncomp_kernel<<<ceil_div(S, 128), 128, 0, ctx.stream>>>(d_cnt, S, L, d_ids, Ko, d_nc, d_fb,
+                                                                  *std::min_element(nc.begin(), nc.end()), d_acc,
+                                                                  d_best, d_bcomp);
+    ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    std::vector<double> acc_all((size_t)Ko * L);
+    std::vector<int> bcomp_all(Ko);
+    download(acc_all.data(), d_acc, (size_t)Ko * L);
+    download(bcomp_all.data(), d_bcomp, Ko);
     int* d_out = ctx.arena.alloc_n<int>(n);
     gather_outer_pred_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(res.d_pred, d_slot, d_best, d_fb, S, L, n, d_out); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
@@ -1047,6 +1074,12 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     }
     pt.mark("ncomp + outer");
     ctx.sync();
+    for (int s = 0; s < S; ++s) {
+      const int o = ids[s];
+      if (best_comp) best_comp[o] = bcomp_all[o];
+      if (inner_accuracy)
+        for (int l = 0; l < L; ++l) inner_accuracy[o + (size_t)l * Ko] = acc_all[o + (size_t)l * Ko];
+    }
     if (outer_ids)
       for (int i = 0; i < n; ++i)
         if (row_slot[i] >= 0) outer_pred[i] = pred_all[i];

@@ -123,10 +123,11 @@ __global__ void pred_counts_kernel(const int* __restrict__ pred, int L, int n, c
 // MB bounds the class count so that the running scores stay in registers.
 template <int MB>
 __global__ void cv_predict_kernel(int F, int n, int m, int K, int L, const int* __restrict__ ncomp,
-                                  const uint8_t* __restrict__ test, const int* __restrict__ group,
-                                  const double* __restrict__ Tkeep, const double* __restrict__ tnorm,
-                                  const double* __restrict__ Q, const int* __restrict__ ncomp_done,
-                                  const double* __restrict__ mYf, int* __restrict__ pred) {
+                                  const int* __restrict__ order, const uint8_t* __restrict__ test,
+                                  const int* __restrict__ group, const double* __restrict__ Tkeep,
+                                  const double* __restrict__ tnorm, const double* __restrict__ Q,
+                                  const int* __restrict__ ncomp_done, const double* __restrict__ mYf,
+                                  int* __restrict__ pred) {
   const int f = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !test[(size_t)f * n + i]) return;
@@ -137,24 +138,38 @@ __global__ void cv_predict_kernel(int F, int n, int m, int K, int L, const int* 
   for (int j = 0; j < MB; ++j) y[j] = 0.0;
   const double* Qf = Q + (size_t)f * m * K;
   const double* mf = mYf + (size_t)f * m;
-  for (int a = 0; a < K; ++a) {
-    if (a < done) {
-      const double c = Tkeep[((size_t)f * K + a) * n + i] / tnorm[(size_t)f * K + a];
+  const double* tk = Tkeep + (size_t)f * K * n + i;
+  // the slices in increasing ncomp (order), each written once y holds its
+  // components; the scores of four components are loaded together
+  int next = 0;
+  int nc_next = L > 0 ? ncomp[order[0]] : 0;
+  for (int a0 = 0; a0 < K; a0 += 4) {
+    double t[4];
 #pragma unroll
-      for (int j = 0; j < MB; ++j)
-        if (j < m) y[j] += c * Qf[j + (size_t)a * m];
-    }
-    for (int s = 0; s < L; ++s) {
-      if (ncomp[s] != a + 1) continue;
-      int best = 0;
-      double bv = y[0] + mf[0];
+    for (int u = 0; u < 4; ++u) t[u] = a0 + u < done ? tk[(size_t)(a0 + u) * n] : 0.0;
 #pragma unroll
-      for (int j = 1; j < MB; ++j) {
-        if (j >= m) break;
-        const double v = y[j] + mf[j];
-        if (v > bv) { bv = v; best = j; }
+    for (int u = 0; u < 4; ++u) {
+      const int a = a0 + u;
+      if (a >= K) break;
+      if (a < done) {
+        const double c = t[u] / tnorm[(size_t)f * K + a];
+#pragma unroll
+        for (int j = 0; j < MB; ++j)
+          if (j < m) y[j] += c * Qf[j + (size_t)a * m];
       }
-      pred[((size_t)g * L + s) * n + i] = best + 1;
+      while (next < L && nc_next == a + 1) {
+        const int s = order[next];
+        int best = 0;
+        double bv = y[0] + mf[0];
+#pragma unroll
+        for (int j = 1; j < MB; ++j) {
+          if (j >= m) break;
+          const double v = y[j] + mf[j];
+          if (v > bv) { bv = v; best = j; }
+        }
+        pred[((size_t)g * L + s) * n + i] = best + 1;
+        if (++next < L) nc_next = ncomp[order[next]];
+      }
     }
   }
 }
@@ -359,7 +374,6 @@ void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, cons
   for (int f = 0; f < fs.F; ++f)
     if (status[f] == 1) act.push_back(f);
   const int Fa = static_cast<int>(act.size());
-  res.ncomp_done.assign(fs.F, 0);
   if (Fa == 0) return;
   PhaseTimer pt("CV grid (batched)");
   const bool center = px.center, dual = px.dual;
@@ -411,6 +425,12 @@ void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, cons
   h2d(d_dY, dY.data(), dY.size() * sizeof(double));
   h2d(d_lab, lab0.data(), n * sizeof(int));
   h2d(d_nc, ncomp, L * sizeof(int));
+  // slice indices in increasing ncomp (ties in slice order) for the predictions
+  std::vector<int> order(L);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int u, int v) { return ncomp[u] < ncomp[v]; });
+  int* d_order = ar.alloc_n<int>(L);
+  h2d(d_order, order.data(), L * sizeof(int));
   double* Qo = ar.alloc_n<double>((size_t)Fa * m * K);
   double* tno = ar.alloc_n<double>((size_t)Fa * K);
   double* Tko = ar.alloc_n<double>((size_t)Fa * n * K);
@@ -495,20 +515,17 @@ void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, cons
   int* d_pred = res.d_pred;
   const dim3 pgrid(ceil_div(n, 128), Fa);
   if (m <= 8)
-    cv_predict_kernel<8><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_te, d_grp, Tko, tno, Qo, ncd, d_mYf, d_pred);
+    cv_predict_kernel<8><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_te, d_grp, Tko, tno, Qo, ncd,
+                                                        d_mYf, d_pred);
   else if (m <= 32)
-    cv_predict_kernel<32><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_te, d_grp, Tko, tno, Qo, ncd, d_mYf, d_pred);
+    cv_predict_kernel<32><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_te, d_grp, Tko, tno, Qo, ncd,
+                                                         d_mYf, d_pred);
   else
-    cv_predict_kernel<kMaxClassesCv><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_te, d_grp, Tko, tno, Qo, ncd,
-                                                                    d_mYf, d_pred);
+    cv_predict_kernel<kMaxClassesCv><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_te, d_grp, Tko,
+                                                                    tno, Qo, ncd, d_mYf, d_pred);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   pt.mark("predict");
-  std::vector<int> done(Fa);
-  d2h(done.data(), ncd, Fa * sizeof(int));
-  ctx.sync();
-  for (int a = 0; a < Fa; ++a) res.ncomp_done[act[a]] = done[a];
-  pt.mark("d2h");
   pt.report();
 }
 
@@ -518,7 +535,6 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
   Arena& ar = ctx.arena;
   const int n = fs.n, p = fs.p, m = fs.m;
   const int K = *std::max_element(ncomp, ncomp + L);
-  res.ncomp_done.assign(fs.F, 0);
   // Per-fit buffers sized for the largest fold, reused fit after fit.
   double* Xf = ar.alloc_n<double>((size_t)n * p);
   double* Xt = ar.alloc_n<double>((size_t)n * p);
@@ -574,10 +590,7 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
     simpls_batch_run(b);
     // Compact class prediction of the test rows (pls_predict_classes_compact_cuda).
     d2h(Qh.data(), Q, (size_t)m * K * sizeof(double));
-    int done = 0;
-    d2h(&done, ncd, sizeof(int));
     ctx.sync();
-    res.ncomp_done[f] = done;
     std::fill(Wh.begin(), Wh.end(), 0.0);
     for (int s = 0; s < L; ++s)
       for (int a = 0; a < ncomp[s]; ++a)
@@ -675,12 +688,19 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
   run_sequential(fs, X, labels_host, ncomp, L, opt, status, res);
 }
 
-void cv_prediction_counts(const int* d_pred, int G, int L, int n, const int* d_labels,
-                          const int* d_exclude, std::vector<long long>& counts) {
+long long* cv_prediction_counts_device(const int* d_pred, int G, int L, int n, const int* d_labels,
+                                      const int* d_exclude) {
   Context& ctx = Context::get();
   long long* d_counts = ctx.arena.alloc_n<long long>(2 * (size_t)G * L);
   pred_counts_kernel<<<G * L, 256, 0, ctx.stream>>>(d_pred, L, n, d_labels, d_exclude, d_counts); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+  return d_counts;
+}
+
+void cv_prediction_counts(const int* d_pred, int G, int L, int n, const int* d_labels,
+                          const int* d_exclude, std::vector<long long>& counts) {
+  Context& ctx = Context::get();
+  long long* d_counts = cv_prediction_counts_device(d_pred, G, L, n, d_labels, d_exclude);
   counts.assign(2 * (size_t)G * L, 0);
   d2h(counts.data(), d_counts, counts.size() * sizeof(long long));
   ctx.sync();

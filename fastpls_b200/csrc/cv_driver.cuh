@@ -37,13 +37,15 @@ struct CvGridOptions {
 struct CvGridResult {
   int* d_pred = nullptr;            // device G x L x n (0 where the row is not predicted);
                                     // valid until the next call resets the arena
-  std::vector<int> ncomp_done;      // F
   std::vector<int> status;          // F: 1 ok, 2 empty test, 3 no train, 4 degenerate
 };
 
 // Per (group g, slice s): counts[2*(g*L+s)] = correct predictions and
 // counts[2*(g*L+s)+1] = predicted rows, over the rows where exclude[i] != g
 // (exclude may be null).  Device buffers in, host vector out.
+// The same counts left on the device (no synchronisation).
+long long* cv_prediction_counts_device(const int* d_pred, int G, int L, int n, const int* d_labels,
+                                      const int* d_exclude);
 void cv_prediction_counts(const int* d_pred, int G, int L, int n, const int* d_labels,
                           const int* d_exclude, std::vector<long long>& counts);
 

@@ -205,3 +205,32 @@ def test_fold_sharded_edge_folds(lib):
     parts = [lib.double_cv(X, y, outer, inner, nc, m, seed=3, return_inner=True, outer_ids=ids)
              for ids in ([0], [1, 2])]
     _same_outputs(fold_shards.merge_outputs(parts), full)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_ncomp_list_order_and_repeats(lib, c4_small, precision):
+    # The predictions of a slice depend only on its ncomp value: an unsorted
+    # list with repeats gives, slice by slice, the predictions of the sorted
+    # list without repeats (same folds, same sketches).
+    d = c4_small
+    outer, inner = double_cv_folds(d["y"], d["groups"], 4, 3, seed=5)
+    mixed = np.array([7, 2, 9, 2, 5])
+    base = np.array([2, 5, 7, 9])
+    kw = dict(seed=1, precision=precision, return_inner=True)
+    a = lib.double_cv(d["X"], d["y"], outer, inner, mixed, d["n_classes"], **kw)
+    b = lib.double_cv(d["X"], d["y"], outer, inner, base, d["n_classes"], **kw)
+    for s, c in enumerate(mixed):
+        t = int(np.where(base == c)[0][0])
+        assert np.array_equal(a["inner_pred"][:, s, :], b["inner_pred"][:, t, :])
+        assert np.array_equal(a["inner_accuracy"][:, s], b["inner_accuracy"][:, t], equal_nan=True)
+    # first maximum: the chosen ncomp follows the list order on ties
+    for o in range(a["best_comp"].size):
+        acc = a["inner_accuracy"][o]
+        assert a["best_comp"][o] == mixed[int(np.nanargmax(acc))]
+    rng = np.random.default_rng(2)
+    fold = stratified_group_folds(d["y"], d["groups"], 5, rng)
+    pa = lib.cv_predict(d["X"], d["y"], fold, mixed, d["n_classes"], seed=3, precision=precision)
+    pb = lib.cv_predict(d["X"], d["y"], fold, base, d["n_classes"], seed=3, precision=precision)
+    for s, c in enumerate(mixed):
+        t = int(np.where(base == c)[0][0])
+        assert np.array_equal(np.asarray(pa["class_pred"])[:, s], np.asarray(pb["class_pred"])[:, t])

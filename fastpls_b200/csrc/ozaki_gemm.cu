@@ -70,7 +70,11 @@ constexpr int OBN = 64;                  // B rows per tile
 constexpr int OBK = 128;                 // K per block (one 128-byte swizzle row of int8)
 constexpr int A_PLANE = OBM * OBK;       // 16 KB
 constexpr int B_PLANE = OBN * OBK;       // 8 KB
-constexpr int kThreads = 192;
+// Warp 0 loads, warp 1 issues the MMAs, warps 2..9 are the epilogue: two warps
+// per TMEM lane quarter (warp w reaches lanes 32 (w % 4) ..), each taking half
+// of the tile's columns.
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr int kTmemCols = 512;
 // int32 headroom: one level sums at most S pairs over one segment, so
 // S * (64 * 128) * 127^2 < 2^31 for S <= 7.
@@ -151,7 +155,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
       mbar_init(smem_u32(&emptyB[b]), 1);
     }
     mbar_init(smem_u32(tfull), 1);
-    mbar_init(smem_u32(tempty), 128);
+    mbar_init(smem_u32(tempty), 32 * kEpiWarps);
     mbar_init(smem_u32(done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -167,9 +171,16 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
   const uint32_t tmem = *tmem_slot;
   // With a_static the A planes were written before the previous kernel ran,
   // so the first K block's A planes are requested before waiting for it.
+  if (warp == 0 && lane == 0) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mA)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mB)) : "memory");
+  }
+  // the segment table is written when the plan is made: read before the wait
+  int4 seg0 = make_int4(0, 0, 0, 0);
+  if (lane == 0 && warp < 2 && sbeg < send) seg0 = segs[sbeg];
   const bool pre_a = a_static && warp == 0 && lane == 0 && sbeg < send;
   if (pre_a) {
-    const int4 seg = segs[sbeg];
+    const int4 seg = seg0;
     const int mt = seg.x / n_tiles_n;
 #pragma unroll
     for (int s = 0; s < S; ++s) {
@@ -192,7 +203,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
     for (int s = 0; s < S; ++s) a_last[s] = pre_a ? 0 : -1;
     bool ok = true;
     for (int sg = sbeg; sg < send && ok; ++sg) {
-      const int4 seg = segs[sg];
+      const int4 seg = sg == sbeg ? seg0 : segs[sg];
       const int mt = seg.x / n_tiles_n, nt = seg.x % n_tiles_n;
       for (int kb = seg.y; kb < seg.z && ok; ++kb, ++it) {
         const int b = it & 1;
@@ -228,7 +239,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
     int it = 0, j = 0;
     bool ok = true;
     for (int sg = sbeg; sg < send && ok; ++sg, ++j) {
-      const int4 seg = segs[sg];
+      const int4 seg = sg == sbeg ? seg0 : segs[sg];
       if (!mbar_wait(smem_u32(tempty), (j & 1) ^ 1, err)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       for (int kb = seg.y; kb < seg.z && ok; ++kb, ++it) {
@@ -271,14 +282,15 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
   } else if (warp >= 2) {
     // ---------------------------------------------------------- epilogue
     const int q = warp & 3;  // TMEM lane quarter accessible to this warp
+    const int half = (warp - 2) / 4;   // which half of the tile's columns
     int j = 0;
     for (int sg = sbeg; sg < send; ++sg, ++j) {
       const int4 seg = segs[sg];
       const int mt = seg.x / n_tiles_n, nt = seg.x % n_tiles_n;
       if (!mbar_wait(smem_u32(tfull), j & 1, err)) atomicOr(&epi_fail, 1);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      // the four epilogue warps leave together (they share named barrier 1)
-      asm volatile("bar.sync 1, 128;" ::: "memory");
+      // the epilogue warps leave together (they share named barrier 1)
+      asm volatile("bar.sync 1, %0;" ::"r"(32 * kEpiWarps) : "memory");
       if (*(volatile int*)&epi_fail) {
         mbar_arrive(smem_u32(tempty));
         break;
@@ -292,7 +304,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
       double* dst = part + static_cast<size_t>(sg) * OBN * OBM + q * 32 + lane;
       const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16);
 #pragma unroll 1
-      for (int c = 0; c < OBN / 16; ++c) {
+      for (int c = half * (OBN / 32); c < (half + 1) * (OBN / 32); ++c) {
         uint32_t v[S][16];
 #pragma unroll
         for (int l = 0; l < S; ++l) tc::tmem_ld16_raw(base + static_cast<uint32_t>(l * OBN + c * 16), v[l]);

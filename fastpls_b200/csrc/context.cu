@@ -79,6 +79,7 @@ Context& Context::get() {
     FPLS_CUDA(cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking));
     FPLS_CUDA(cudaStreamCreateWithFlags(&ctx.side, cudaStreamNonBlocking));
     FPLS_CUDA(cudaEventCreateWithFlags(&ctx.side_done, cudaEventDisableTiming));
+    FPLS_CUDA(cudaEventCreateWithFlags(&ctx.planes_ready, cudaEventDisableTiming));
     FPLS_CUDA(cudaStreamCreateWithFlags(&ctx.copy, cudaStreamNonBlocking));
     FPLS_CUDA(cudaMalloc(&ctx.d_status, 64 * sizeof(int)));
     FPLS_CUDA(cudaMemset(ctx.d_status, 0, 64 * sizeof(int)));

@@ -41,6 +41,7 @@ struct Context {
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;   // second stream for work that overlaps `stream` (joined by events)
   cudaEvent_t side_done = nullptr;
+  cudaEvent_t planes_ready = nullptr;   // the operator of a CV grid's X is complete on `stream`
   cudaStream_t copy = nullptr;   // host-to-device copies that overlap `stream` (joined by copy_event(i))
   std::vector<cudaEvent_t> copy_events;
   cudaEvent_t copy_event(int i);   // i-th event of the copy stream (created on first use)
@@ -78,6 +79,17 @@ struct Context {
 
 // Opt-in phase timer (FASTPLS_TRACE=1): CUDA events on the context stream
 // between named marks; the sums per name are printed to stderr by report().
+// Makes the launches of a scope go to another stream of the context (every
+// launch site uses ctx.stream), e.g. the side stream; restores the main one.
+struct StreamSwap {
+  Context& ctx;
+  cudaStream_t saved;
+  StreamSwap(Context& c, cudaStream_t s) : ctx(c), saved(c.stream) { c.stream = s; }
+  ~StreamSwap() { ctx.stream = saved; }
+  StreamSwap(const StreamSwap&) = delete;
+  StreamSwap& operator=(const StreamSwap&) = delete;
+};
+
 class PhaseTimer {
  public:
   explicit PhaseTimer(const char* title);

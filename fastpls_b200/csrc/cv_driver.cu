@@ -303,6 +303,7 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
       }
       split_operator_fill_columns(*xop, c64, c32, center ? mall + j0 : nullptr, j0, j1);
       if (c == 0) load_centered(x64, x32, n, 1, mall, x0);
+      if (c == nch - 1) FPLS_CUDA(cudaEventRecord(ctx.planes_ready, ctx.stream));
       split_operator_gram_columns(*xop, Kg, j0, j1, c > 0);
     };
     for (int c = 0; c < nch; ++c) {
@@ -333,6 +334,7 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
       if (opt.precision == 1) xop = make_split_operator(X, n, p, !dual);
       else xop.reset(new XOperatorF64(X, n, p));
     }
+    FPLS_CUDA(cudaEventRecord(ctx.planes_ready, ctx.stream));
   }
   pt.mark("operator");
   // The Gram contracts over all p columns (BF16x3 on the tensor cores in the
@@ -441,8 +443,11 @@ void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, cons
     const int kop_slices = px.kop_slices;
     pt.mark("fold set-up");
     FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0));
-    double* XOm = ar.alloc_n<double>((size_t)n * Fa);
-    xop->times(d_om, Fa, XOm);
+    double* XOm = px.XOm;
+    if (!XOm) {
+      XOm = ar.alloc_n<double>((size_t)n * Fa);
+      xop->times(d_om, Fa, XOm);
+    }
     pt.mark("sketch");
     DualBatch db;
     db.n = n; db.m = m; db.F = Fa; db.K = K;
@@ -624,6 +629,12 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
   classify_fits(fs, labels_host, status, fallback, counts);
   res.status = status;
   const bool batched = opt.batched && opt.scaling != 2;
+  // The X-side work (and a host X's upload) first, unless the caller enqueued it.
+  std::unique_ptr<CvPreparedX> own;
+  if (batched && !prep) {
+    own = cv_prepare_x(x64, x32, fs.n, fs.p, fs.m, *std::max_element(ncomp, ncomp + L), opt, x_host);
+    prep = own.get();
+  }
   // The per-fit sketches are drawn on the side stream, overlapping every
   // device step below until the SIMPLS loop needs them.
   double* d_om = nullptr;
@@ -646,6 +657,14 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
       FPLS_CUDA(cudaMemcpyAsync(d_seeds, seeds.data(), seeds.size() * sizeof(unsigned), cudaMemcpyHostToDevice,
                                 ctx.side));
       device_gaussian_streams(d_om, fs.p, fs.p, d_seeds, static_cast<int>(seeds.size()), ctx.side);
+      if (prep->dual) {
+        // X Omega of the row-space loop also on the side stream: it needs only
+        // the operator of X and the sketches, so it overlaps the row Gram.
+        FPLS_CUDA(cudaStreamWaitEvent(ctx.side, ctx.planes_ready, 0));
+        prep->XOm = ctx.arena.alloc_n<double>((size_t)fs.n * seeds.size());
+        StreamSwap on_side(ctx, ctx.side);
+        prep->xop->times(d_om, static_cast<int>(seeds.size()), prep->XOm);
+      }
       FPLS_CUDA(cudaEventRecord(ctx.side_done, ctx.side));
     }
   }
@@ -665,12 +684,6 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
   pt.mark("prediction buffers");
   pt.report();
   if (batched) {
-    // the X-side work (and a host X's upload), unless the caller enqueued it
-    std::unique_ptr<CvPreparedX> own;
-    if (!prep) {
-      own = cv_prepare_x(x64, x32, fs.n, fs.p, fs.m, *std::max_element(ncomp, ncomp + L), opt, x_host);
-      prep = own.get();
-    }
     run_batched(fs, labels_host, ncomp, L, opt, status, counts, d_om, res, *prep);
     return;
   }

@@ -66,6 +66,7 @@ struct CvPreparedX {
   double* x0 = nullptr;     // first centred column
   std::unique_ptr<XOperator> xop, kop_f64, kop_int8;
   int kop_slices = 0;
+  double* XOm = nullptr;    // X Omega of the row-space loop, when taken on the side stream
 };
 
 // Batched grids only (opt.batched with scaling != 2); x64 / x32 as in

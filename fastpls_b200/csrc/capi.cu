@@ -861,7 +861,8 @@ static CvGridOptions cv_options(int scaling, int precision, int batched) {
 static void run_cv_grid(const CvFitSet& fs, const CvX& x, const int* y, const int* ncomp, int L,
                         const CvGridOptions& opt, CvGridResult& res, CvPreparedX* prep = nullptr) {
   Context& ctx = Context::get();
-  dzero(ctx.d_status + 16, sizeof(int));
+  // (the error flag of the tensor-core kernels was cleared by begin_call; a
+  // flag raised by the X-side work enqueued before this point must survive)
   cv_grid_classify(fs, x.x64, x.x32, y, ncomp, L, opt, res, prep ? nullptr : x.host, prep);
   int e = 0;
   d2h(&e, ctx.d_status + 16, sizeof(int));

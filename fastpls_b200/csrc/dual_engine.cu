@@ -313,8 +313,11 @@ static __device__ int fused_refresh(ClusterRed& R, int m, int iters, double vn) 
 // coefficients c_p for the K product.
 // In the merged launch (MG) the refresh was already run by dual_b (c_y, K c_y in
 // pre_cy, pre_ky) and only the scores part follows.
+// The CTA arrives on the closing cluster barrier (arrived = true) once its
+// last read of a peer's shared memory is behind it, so that the writes of c_p
+// and its digit planes overlap the barrier.
 static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Fixed& P, const Rows& rw, int rank,
-                              const double (&pre_cy)[kLR], const double (&pre_ky)[kLR]) {
+                              const double (&pre_cy)[kLR], const double (&pre_ky)[kLR], bool& arrived) {
   __shared__ double wcls[kW][kMaxM + 5];   // per-warp class sums and the reduction's scalars
   const int f = blockIdx.x / kCl;
   const int n = e.n, m = e.m;
@@ -462,6 +465,10 @@ static __device__ bool dual_a(const DualEng& e, int a, ClusterRed& R, const Fixe
   if (!(tn > 0.0) || !isfinite(tn)) {
     if (rank == 0 && threadIdx.x == 0) e.status[f] = 1;
     return false;
+  }
+  if constexpr (CL > 1) {
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    arrived = true;
   }
   double* keep = e.Tkeep ? e.Tkeep + ((size_t)f * e.K + a) * n : nullptr;
   // Digit planes of c_p for the INT8 K product: scale 2^ex above the bound
@@ -752,8 +759,12 @@ static __device__ void run(const DualEng& e, int a) {
   bool ok = true;
   double fcy[kLR], fky[kLR];
   if (a > 0) ok = dual_b(e, a - 1, R, rw, rank, ks0, ks1, cv, fcy, fky);
-  if (ok && a < e.K) dual_a(e, a, R, P, rw, rank, fcy, fky);
-  if constexpr (CL > 1) cg::this_cluster().sync();
+  bool arrived = false;
+  if (ok && a < e.K) dual_a(e, a, R, P, rw, rank, fcy, fky, arrived);
+  if constexpr (CL > 1) {
+    if (!arrived) asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+  }
 }
 };  // struct Step
 

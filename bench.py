@@ -324,7 +324,8 @@ def run_ours(args):
     out = dict(
         metric="CV-grid fits/s", value=value, unit="fits/s", n_gpus=world, steps=args.steps,
         warmup=args.warmup, ms_per_step=ms_per_step, higher_is_better=True, scaling="weak",
-        vs_baseline=None, dtype="bf16x3 split (fp32 accumulate) + fp64", data="synthetic",
+        vs_baseline=None, dtype="bf16x3 split (fp32 accumulate) + int8 digit planes (exact int32) + fp64",
+        data="synthetic",
         config=dict(CONFIG, parallelism=f"{world} independent replicas" if world > 1 else "1 GPU",
                     precision="bf16x3", batched=True,
                     roofline_timing="per-kernel CUDA events over args.steps further steps run right after the "

@@ -12,8 +12,8 @@
 // which every GPU that loads the library keeps until the process exits.
 #include "../../include/fastpls_b200.h"
 
-#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "common.cuh"
@@ -35,19 +35,13 @@ struct DeviceSetup {
 };
 constexpr int kMaxDevices = 64;
 DeviceSetup g_setup[kMaxDevices];
+std::mutex g_setup_mutex;  // first calls from several host threads set up once
 
-// Once per device, with that device current: resolve the array's device address.
-DeviceSetup& setup_device() {
-  if (const char* e = std::getenv("FASTPLS_DEVICE")) {
-    char* endp = nullptr;
-    const long v = std::strtol(e, &endp, 10);
-    int n = 0;
-    if (endp != e && cudaGetDeviceCount(&n) == cudaSuccess && v >= 0 && v < n)
-      FPLS_CUDA(cudaSetDevice(static_cast<int>(v)));
-  }
-  int dev = 0;
-  FPLS_CUDA(cudaGetDevice(&dev));
+// Once per device, on the caller's current device (the call never changes it):
+// resolve the array's device address there.
+DeviceSetup& setup_device(int dev) {
   if (dev < 0 || dev >= kMaxDevices) throw fpls::Error(fpls::kErrArgument, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
   DeviceSetup& s = g_setup[dev];
   if (!s.ready) {
     void* p = nullptr;
@@ -61,6 +55,22 @@ DeviceSetup& setup_device() {
     s.ready = true;
   }
   return s;
+}
+
+// A, B and C must be memory of the current device (device or managed memory):
+// a host pointer, or another GPU's buffer, would fault inside the kernels, so
+// it is refused before anything is launched.
+void require_device_pointer(const void* ptr, int dev, const char* name) {
+  cudaPointerAttributes a{};
+  const cudaError_t e = cudaPointerGetAttributes(&a, ptr);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();  // the failed query's error is not a device fault: clear it
+    throw fpls::Error(fpls::kErrArgument, std::string("bf16x3_gemm_noalloc: ") + name + " is not a device pointer");
+  }
+  const bool on_device = a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (!on_device || (a.type == cudaMemoryTypeDevice && a.device != dev))
+    throw fpls::Error(fpls::kErrArgument, std::string("bf16x3_gemm_noalloc: ") + name +
+                                              " must be device memory of the current device");
 }
 
 void put_err(char* err, size_t errlen, const char* msg) {
@@ -77,7 +87,12 @@ extern "C" int fpls_bf16x3_gemm_noalloc(const double* A, int M, int K, const dou
   try {
     if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C)
       throw fpls::Error(fpls::kErrArgument, "bf16x3_gemm_noalloc: dimensions must be positive and pointers set");
-    DeviceSetup& s = setup_device();
+    int dev = 0;
+    FPLS_CUDA(cudaGetDevice(&dev));
+    require_device_pointer(A, dev, "A");
+    require_device_pointer(B, dev, "B");
+    require_device_pointer(C, dev, "C");
+    DeviceSetup& s = setup_device(dev);
     const size_t need = fpls::split_gemm_scratch_need(M, N, K, s.sms);
     if (need + kErrSlotBytes > kNoAllocScratchBytes) {
       throw fpls::Error(fpls::kErrArgument,

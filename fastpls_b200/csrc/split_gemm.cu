@@ -18,6 +18,7 @@
 // equal contiguous ranges per CTA; a second kernel sums each tile's partials in
 // FP64.  All mbarrier waits are bounded by a clock budget and raise an error
 // flag instead of spinning forever.  No cluster multicast is used.
+#include <atomic>
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -578,11 +579,19 @@ GemmScratch carve_gemm_scratch(const GemmPlan& g, char* base) {
 
 template <int NP, int TN>
 void ensure_smem_attr() {
-  static bool attr = false;
-  if (!attr) {
+  // The attribute applies to the device current when it is set: one flag per device.
+  static std::atomic<bool> attr[64];
+  int dev = 0;
+  FPLS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
     FPLS_CUDA(cudaFuncSetAttribute(split_gemm_kernel<NP, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    Planes<NP, TN>::SMEM_BYTES));
-    attr = true;
+    return;
+  }
+  if (!attr[dev].load(std::memory_order_acquire)) {
+    FPLS_CUDA(cudaFuncSetAttribute(split_gemm_kernel<NP, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Planes<NP, TN>::SMEM_BYTES));
+    attr[dev].store(true, std::memory_order_release);
   }
 }
 

@@ -413,8 +413,10 @@ int fpls_candidate_knn_predict(const double* Ttest_norm, int ntest, const double
  * for callers that cannot allocate device memory (a host that runs inside
  * another runtime's fixed memory pool, a stream callback, an allocation-free
  * loop).  No counterpart in the reference.  A, B and C are DEVICE pointers
- * (column-major, FP64) owned by the caller on the library's current device
- * (device 0, or FASTPLS_DEVICE).  The call allocates nothing: every temporary
+ * (column-major, FP64) owned by the caller on the calling thread's current
+ * device, where the work runs; the call never changes the current device, and
+ * a pointer that is not device (or managed) memory of that device is refused
+ * with FPLS_ERR_ARGUMENT before anything runs.  The call allocates nothing: every temporary
  * lives in one fixed 16 MiB device array that each GPU loading the library
  * holds until exit; shapes needing more (about (M + N) x K above 2.5 million
  * elements at N <= 64) are rejected with FPLS_ERR_ARGUMENT.  The first call on

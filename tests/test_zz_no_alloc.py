@@ -35,9 +35,11 @@ def test_noalloc_gemm_matches_allocating_entry_point(lib):
     torch = pytest.importorskip("torch")
     assert torch.cuda.is_available()
     rng = np.random.default_rng(2024)
-    M, K, N = 700, 1536, 48
-    results = []
-    for call in range(2):
+    # A large, block-aligned shape first, then a smaller one whose K is not a
+    # multiple of the 64-wide K-block: the second call reuses scratch that still
+    # holds the first call's planes and partials, so stale contents or padding
+    # that is not rewritten would show up in its result.
+    for M, K, N in ((700, 1536, 48), (333, 1000, 17)):
         A = rng.standard_normal((M, K))
         B = rng.standard_normal((K, N))
         # Column-major device copies (a transposed contiguous tensor is column-major).
@@ -45,15 +47,26 @@ def test_noalloc_gemm_matches_allocating_entry_point(lib):
         B_dev = torch.from_numpy(np.ascontiguousarray(B.T)).cuda()
         C_dev = torch.full((N, M), float("nan"), dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()
+        dev_before = torch.cuda.current_device()
         rc, msg = _call_noalloc(lib, A_dev.data_ptr(), M, K, B_dev.data_ptr(), N, C_dev.data_ptr())
         assert rc == 0, msg
+        assert torch.cuda.current_device() == dev_before
         C = C_dev.cpu().numpy().T
         ref = lib.bf16x3_gemm(A, B)
         assert np.all(np.isfinite(C))
         assert rel_err(C, ref) < SPLIT_REL_TOL
         assert rel_err(C, A @ B) < SPLIT_REL_TOL
-        results.append(C)
-    assert not np.array_equal(results[0], results[1])
+
+
+def test_noalloc_gemm_refuses_host_pointers(lib):
+    # A host buffer passed as an operand is refused before any kernel runs.
+    torch = pytest.importorskip("torch")
+    dev = torch.zeros(64 * 64, dtype=torch.float64, device="cuda")
+    host = np.zeros(64 * 64)
+    rc, msg = _call_noalloc(lib, host.ctypes.data, 64, 64, dev.data_ptr(), 64, dev.data_ptr())
+    assert rc == 1 and "device" in msg
+    rc, msg = _call_noalloc(lib, dev.data_ptr(), 64, 64, dev.data_ptr(), 64, host.ctypes.data)
+    assert rc == 1 and "device" in msg
 
 
 def test_noalloc_gemm_rejects_oversized_shapes(lib):

@@ -70,6 +70,10 @@ SIGNATURES = {
                          _I, _IP, _IP, _C, _S], ctypes.c_int),
     "fpls_double_cv": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I,
                         _I, _I, _I, _IP, _DP, _IP, _IP, _IP, _C, _S], ctypes.c_int),
+    "fpls_cv_predict_scores": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I, _I, _I,
+                                _I, _IP, _IP, _DP, _C, _S], ctypes.c_int),
+    "fpls_double_cv_scores": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I,
+                               _I, _I, _I, _IP, _DP, _IP, _IP, _IP, _DP, _DP, _C, _S], ctypes.c_int),
     "fpls_bf16x3_gemm_noalloc": ([ctypes.c_void_p, _I, _I, ctypes.c_void_p, _I, ctypes.c_void_p,
                                   _C, _S], ctypes.c_int),
     "fpls_gaussian_y_encode": ([_DP, _I, _I, _DP, _I, _DP, _DP, _DP, _C, _S], ctypes.c_int),
@@ -521,8 +525,10 @@ def _x_arg(X):
 
 
 def cv_predict(X, y, fold, ncomp, n_classes, method=3, scaling=1, seed=1, precision="fp64",
-               batched=True):
-    """Cross-validated class predictions (argmax classifier), folds 0-based."""
+               batched=True, return_scores=False):
+    """Cross-validated class predictions (argmax classifier), folds 0-based.
+    With return_scores, class_score (n x L x n_classes) holds the scores each
+    argmax read (fpls_cv_predict_scores)."""
     Xa, is32 = _x_arg(X)
     n, p = Xa.shape
     yy = _i32(y)
@@ -532,10 +538,15 @@ def cv_predict(X, y, fold, ncomp, n_classes, method=3, scaling=1, seed=1, precis
     kfold = int(fd.max()) + 1
     cp = np.zeros((n, L), dtype=np.int32, order="F")
     st = np.zeros(kfold, dtype=np.int32)
-    _call("fpls_cv_predict", Xa.ctypes.data, is32, n, p, _p(yy), int(n_classes), _p(fd), kfold,
-          _p(nc), L, int(method), int(scaling), int(seed), PREC[precision], int(bool(batched)),
-          cp.ctypes.data_as(_c_int_p), _p(st))
-    return dict(class_pred=cp, status=st)
+    args = (Xa.ctypes.data, is32, n, p, _p(yy), int(n_classes), _p(fd), kfold,
+            _p(nc), L, int(method), int(scaling), int(seed), PREC[precision], int(bool(batched)),
+            cp.ctypes.data_as(_c_int_p), _p(st))
+    if not return_scores:
+        _call("fpls_cv_predict", *args)
+        return dict(class_pred=cp, status=st)
+    sc = np.zeros((L, n, int(n_classes)))
+    _call("fpls_cv_predict_scores", *args, _p(sc))
+    return dict(class_pred=cp, status=st, class_score=np.ascontiguousarray(sc.transpose(1, 0, 2)))
 
 
 def _double_cv_args(n, y, outer_fold, inner_fold, ncomp, return_inner, outer_ids):
@@ -562,14 +573,21 @@ def _double_cv_result(outs, yy, ids, of):
 
 
 def double_cv(X, y, outer_fold, inner_fold, ncomp, n_classes, scaling=1, seed=1, run=1,
-              precision="fp64", batched=True, return_inner=False, outer_ids=None):
+              precision="fp64", batched=True, return_inner=False, outer_ids=None,
+              return_scores=False):
     """Double CV of SIMPLS PLS-DA over the supplied outer/inner folds (0-based).
 
     outer_ids restricts the call to those outer folds (fpls_double_cv_outer_subset):
     only their entries of the outputs are written, the rest stay zero, and
-    `accuracy` is taken over their rows."""
+    `accuracy` is taken over their rows.  return_scores (full calls only) adds
+    inner_score (kfold_outer x L x n x n_classes), outer_score (n x n_classes)
+    and inner_pred (fpls_double_cv_scores)."""
     Xa, is32 = _x_arg(X)
     n, p = Xa.shape
+    if return_scores:
+        if outer_ids is not None:
+            raise ValueError("return_scores needs the full fold list")
+        return_inner = True
     yy, of, inf_, Ko, Ki, nc, L, ids, o = _double_cv_args(n, y, outer_fold, inner_fold, ncomp,
                                                           return_inner, outer_ids)
     inner = o.get("inner_pred")
@@ -578,7 +596,11 @@ def double_cv(X, y, outer_fold, inner_fold, ncomp, n_classes, scaling=1, seed=1,
             None if inner is None else inner.ctypes.data_as(_c_int_p), _p(o["fit_status"]))
     head = (Xa.ctypes.data, is32, n, p, _p(yy), int(n_classes), _p(of), Ko,
             inf_.ctypes.data_as(_c_int_p), Ki)
-    if ids is None:
+    if return_scores:
+        o["inner_score"] = np.zeros((Ko, L, n, int(n_classes)))
+        o["outer_score"] = np.zeros((n, int(n_classes)))
+        _call("fpls_double_cv_scores", *head, *tail, _p(o["inner_score"]), _p(o["outer_score"]))
+    elif ids is None:
         _call("fpls_double_cv", *head, *tail)
     else:
         _call("fpls_double_cv_outer_subset", *head, _p(ids), ids.size, *tail)

@@ -77,6 +77,19 @@ __global__ void gather_outer_pred_kernel(const int* __restrict__ pred, const int
   out[i] = fb[o] ? fb[o] : pred[((size_t)Ko * L + best_slice[o]) * n + i];
 }
 
+// Class scores behind the outer predictions: row i of outer slot o takes the
+// refit's scores at the chosen slice (zeros for a fallback fold).
+__global__ void gather_outer_score_kernel(const double* __restrict__ score, const int* __restrict__ outer,
+                                          const int* __restrict__ best_slice, const int* __restrict__ fb,
+                                          int Ko, int L, int n, int m, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int o = outer[i];
+  const bool take = o >= 0 && o < Ko && !fb[o];
+  const double* src = take ? score + (((size_t)Ko * L + best_slice[o]) * n + i) * m : nullptr;
+  for (int j = 0; j < m; ++j) out[(size_t)i * m + j] = take ? src[j] : 0.0;
+}
+
 // Slot s of a double CV (outer fold ids[s]): the inner accuracy of every ncomp
 // slice from the prediction counts (NaN when no row was predicted), the first
 // slice of maximal finite accuracy (.cv_best_index) and the chosen ncomp (the
@@ -870,11 +883,11 @@ static void run_cv_grid(const CvFitSet& fs, const CvX& x, const int* y, const in
   if (e) throw Error(FPLS_ERR_CUDA, "tensor-core pipeline wait timed out");
 }
 
-int fpls_cv_predict(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
-                    const int* fold, int kfold, const int* ncomp, int L, int method, int scaling,
-                    int seed, int precision, int batched, int* class_pred, int* status,
-                    char* err, size_t errlen) {
-  return guarded(err, errlen, [&] {
+static void cv_predict_impl(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                            const int* fold, int kfold, const int* ncomp, int L, int method, int scaling,
+                            int seed, int precision, int batched, int* class_pred, int* status,
+                            double* class_score) {
+  {
     FPLS_REQUIRE(n >= 2 && p > 0, "Xdata must contain at least two samples");
     FPLS_REQUIRE(n_classes >= 1, "n_classes must be >= 1");
     FPLS_REQUIRE(method == 3 || method == 2, "the GPU CV grid runs method 3 (simpls_fast)");
@@ -897,11 +910,34 @@ int fpls_cv_predict(const void* X, int x_is_float32, int n, int p, const int* y,
     std::vector<int> nc(ncomp, ncomp + L);
     for (int& c : nc) c = std::max(1, c);
     CvGridResult res;
-    const CvGridOptions opt = cv_options(scaling, precision, batched);
+    CvGridOptions opt = cv_options(scaling, precision, batched);
+    opt.want_scores = class_score != nullptr;
     run_cv_grid(fs, cv_x(X, x_is_float32, false, n, p), y, nc.data(), L, opt, res);
     download(class_pred, res.d_pred, (size_t)n * L);
+    if (class_score) download(class_score, res.d_score, (size_t)n * L * n_classes);
     ctx.sync();
     if (status) std::copy(res.status.begin(), res.status.end(), status);
+  }
+}
+
+int fpls_cv_predict(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                    const int* fold, int kfold, const int* ncomp, int L, int method, int scaling,
+                    int seed, int precision, int batched, int* class_pred, int* status,
+                    char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    cv_predict_impl(X, x_is_float32, n, p, y, n_classes, fold, kfold, ncomp, L, method, scaling, seed, precision,
+                    batched, class_pred, status, nullptr);
+  });
+}
+
+int fpls_cv_predict_scores(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                           const int* fold, int kfold, const int* ncomp, int L, int method, int scaling,
+                           int seed, int precision, int batched, int* class_pred, int* status,
+                           double* class_score, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(class_score != nullptr, "class_score must be set");
+    cv_predict_impl(X, x_is_float32, n, p, y, n_classes, fold, kfold, ncomp, L, method, scaling, seed, precision,
+                    batched, class_pred, status, class_score);
   });
 }
 
@@ -915,7 +951,8 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
                            const int* inner_fold, int kfold_inner, const int* outer_ids, int n_ids,
                            const int* ncomp, int L, int scaling, int seed, int run, int precision,
                            int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
-                           int* inner_pred, int* fit_status) {
+                           int* inner_pred, int* fit_status, double* inner_score = nullptr,
+                           double* outer_score = nullptr) {
   {
     FPLS_REQUIRE(n >= 2 && p > 0, "Xdata must contain at least two samples");
     FPLS_REQUIRE(kfold_outer >= 1 && kfold_inner >= 1 && L >= 1, "fold counts and ncomp must be >= 1");
@@ -950,7 +987,8 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     // The X-side work of the grid (upload, column means, BF16 planes, row Gram)
     // does not depend on the folds: enqueued first, it runs on the GPU while
     // the fold set-up below runs on the host.
-    const CvGridOptions opt = cv_options(scaling, precision, batched);
+    CvGridOptions opt = cv_options(scaling, precision, batched);
+    opt.want_scores = inner_score != nullptr || outer_score != nullptr;
     const CvX cx = cv_x(X, x_is_float32, x_on_device, n, p);
     std::unique_ptr<CvPreparedX> prep;
     if (opt.batched && opt.scaling != 2 && fs.p > 5)
@@ -1062,6 +1100,24 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     int* d_out = ctx.arena.alloc_n<int>(n);
     gather_outer_pred_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(res.d_pred, d_slot, d_best, d_fb, S, L, n, d_out); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    double* d_oscore = nullptr;
+    if (outer_score) {
+      d_oscore = ctx.arena.alloc_n<double>((size_t)n * m);
+      gather_outer_score_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(res.d_score, d_slot, d_best, d_fb, S, L,
+                                                                          n, m, d_oscore);
+      ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+    }
+    std::vector<double> oscore_all;
+    if (outer_score && outer_ids) {
+      oscore_all.resize((size_t)n * m);
+      download(oscore_all.data(), d_oscore, (size_t)n * m);
+    } else if (outer_score) {
+      download(outer_score, d_oscore, (size_t)n * m);
+    }
+    if (inner_score)
+      for (int s = 0; s < S; ++s)
+        download(inner_score + (size_t)ids[s] * L * n * m, res.d_score + (size_t)s * L * n * m, (size_t)L * n * m);
     std::vector<int> pred_all;
     if (outer_ids) {
       pred_all.resize(n);
@@ -1083,7 +1139,11 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     }
     if (outer_ids)
       for (int i = 0; i < n; ++i)
-        if (row_slot[i] >= 0) outer_pred[i] = pred_all[i];
+        if (row_slot[i] >= 0) {
+          outer_pred[i] = pred_all[i];
+          if (outer_score)
+            for (int j = 0; j < m; ++j) outer_score[(size_t)i * m + j] = oscore_all[(size_t)i * m + j];
+        }
     if (fit_status)
       for (int s = 0; s < S; ++s) {
         for (int i0 = 0; i0 < Ki; ++i0) fit_status[(size_t)ids[s] * Ki + i0] = res.status[(size_t)s * Ki + i0];
@@ -1101,6 +1161,20 @@ int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, 
     double_cv_impl(X, x_is_float32, false, n, p, y, n_classes, outer_fold, kfold_outer, inner_fold,
                    kfold_inner, nullptr, 0, ncomp, L, scaling, seed, run, precision, batched, best_comp,
                    inner_accuracy, outer_pred, inner_pred, fit_status);
+  });
+}
+
+int fpls_double_cv_scores(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                          const int* outer_fold, int kfold_outer, const int* inner_fold, int kfold_inner,
+                          const int* ncomp, int L, int scaling, int seed, int run, int precision,
+                          int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
+                          int* inner_pred, int* fit_status, double* inner_score, double* outer_score,
+                          char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(inner_score || outer_score, "double_cv_scores: no score output requested");
+    double_cv_impl(X, x_is_float32, false, n, p, y, n_classes, outer_fold, kfold_outer, inner_fold,
+                   kfold_inner, nullptr, 0, ncomp, L, scaling, seed, run, precision, batched, best_comp,
+                   inner_accuracy, outer_pred, inner_pred, fit_status, inner_score, outer_score);
   });
 }
 

@@ -96,6 +96,18 @@ __global__ void scatter_pred_kernel(const int* __restrict__ lab, int nt, int L, 
   pred[((size_t)g * L + s) * n + rows[r]] = lab[t];
 }
 
+// Class scores of the test rows of one sequential fit (Yp: L slices of nt x m,
+// column-major) into the grid's score array at the rows' own indices.
+__global__ void scatter_score_kernel(const double* __restrict__ Yp, int nt, int m, int L,
+                                     const int* __restrict__ rows, int n, int g, double* __restrict__ score) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nt * m * L) return;
+  const int r = static_cast<int>(t % nt);
+  const int j = static_cast<int>((t / nt) % m);
+  const int s = static_cast<int>(t / ((long long)nt * m));
+  score[(((size_t)g * L + s) * n + rows[r]) * m + j] = Yp[t];
+}
+
 __global__ void pred_counts_kernel(const int* __restrict__ pred, int L, int n, const int* __restrict__ y,
                                    const int* __restrict__ exclude, long long* __restrict__ counts) {
   __shared__ double scratch[32];
@@ -127,7 +139,7 @@ __global__ void cv_predict_kernel(int F, int n, int m, int K, int L, const int* 
                                   const int* __restrict__ group, const double* __restrict__ Tkeep,
                                   const double* __restrict__ tnorm, const double* __restrict__ Q,
                                   const int* __restrict__ ncomp_done, const double* __restrict__ mYf,
-                                  int* __restrict__ pred) {
+                                  int* __restrict__ pred, double* __restrict__ score) {
   const int f = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !test[(size_t)f * n + i]) return;
@@ -168,6 +180,12 @@ __global__ void cv_predict_kernel(int F, int n, int m, int K, int L, const int* 
           if (v > bv) { bv = v; best = j; }
         }
         pred[((size_t)g * L + s) * n + i] = best + 1;
+        if (score) {
+          double* sc = score + (((size_t)g * L + s) * n + i) * m;
+#pragma unroll
+          for (int j = 0; j < MB; ++j)
+            if (j < m) sc[j] = y[j] + mf[j];
+        }
         if (++next < L) nc_next = ncomp[order[next]];
       }
     }
@@ -521,13 +539,13 @@ void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, cons
   const dim3 pgrid(ceil_div(n, 128), Fa);
   if (m <= 8)
     cv_predict_kernel<8><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_te, d_grp, Tko, tno, Qo, ncd,
-                                                        d_mYf, d_pred);
+                                                        d_mYf, d_pred, res.d_score);
   else if (m <= 32)
     cv_predict_kernel<32><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_te, d_grp, Tko, tno, Qo, ncd,
-                                                         d_mYf, d_pred);
+                                                         d_mYf, d_pred, res.d_score);
   else
     cv_predict_kernel<kMaxClassesCv><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_te, d_grp, Tko,
-                                                                    tno, Qo, ncd, d_mYf, d_pred);
+                                                                    tno, Qo, ncd, d_mYf, d_pred, res.d_score);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   pt.mark("predict");
@@ -609,6 +627,12 @@ void run_sequential(const CvFitSet& fs, const double* X, const int* y, const int
     for (int s = 0; s < L; ++s) row_argmax(Yp + (size_t)s * nt * m, nt, m, nullptr, lab + (size_t)s * nt);
     scatter_pred_kernel<<<ceil_div((long long)nt * L, 256), 256, 0, ctx.stream>>>(lab, nt, L, d_idx, n, fs.group[f], res.d_pred); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    if (res.d_score) {
+      scatter_score_kernel<<<ceil_div((long long)nt * m * L, 256), 256, 0, ctx.stream>>>(Yp, nt, m, L, d_idx, n,
+                                                                                          fs.group[f], res.d_score);
+      ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+    }
   }
 }
 
@@ -680,6 +704,11 @@ void cv_grid_classify(const CvFitSet& fs, const double* x64, const float* x32,
     ctx.sync();
   } else {
     dzero(res.d_pred, npred * sizeof(int));
+  }
+  if (opt.want_scores) {
+    const size_t nscore = npred * (size_t)fs.m;
+    res.d_score = ctx.arena.alloc_n<double>(nscore);
+    dzero(res.d_score, nscore * sizeof(double));
   }
   pt.mark("prediction buffers");
   pt.report();

@@ -32,11 +32,15 @@ struct CvGridOptions {
   int precision = 0;                // 0 FP64, 1 BF16x3 split
   bool batched = true;              // false: one fit after another (plain drop-in path)
   int power_iters = 2;              // FASTPLS_FAST_INC_ITERS
+  bool want_scores = false;         // also keep the class scores behind every prediction
 };
 
 struct CvGridResult {
   int* d_pred = nullptr;            // device G x L x n (0 where the row is not predicted);
                                     // valid until the next call resets the arena
+  double* d_score = nullptr;        // with opt.want_scores: device G x L x n x m class scores
+                                    // (classes fastest; 0 where the row is not predicted or
+                                    // its fold took a fallback class)
   std::vector<int> status;          // F: 1 ok, 2 empty test, 3 no train, 4 degenerate
 };
 

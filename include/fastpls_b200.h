@@ -256,6 +256,16 @@ int fpls_cv_predict(const void* X, int x_is_float32, int n, int p, const int* y,
                     int seed, int precision, int batched, int* class_pred, int* status,
                     char* err, size_t errlen);
 
+/* fpls_cv_predict that also returns class_score L x n x n_classes (entry
+ * (l n + i) n_classes + c), the Ypred rows the argmax of each prediction read
+ * (zeros where a fold took a fallback class or predicted nothing).  The
+ * reference's classifier-0 CV returns labels only; this is its score matrix
+ * for margin checks. */
+int fpls_cv_predict_scores(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                           const int* fold, int kfold, const int* ncomp, int L, int method, int scaling,
+                           int seed, int precision, int batched, int* class_pred, int* status,
+                           double* class_score, char* err, size_t errlen);
+
 /* Double cross-validation of SIMPLS PLS-DA (argmax classifier): for every outer
  * fold o, an inner CV over its training rows picks ncomp (first maximum of the
  * inner accuracy), then a refit on the outer training rows predicts fold o.
@@ -274,6 +284,23 @@ int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, 
                    const int* ncomp, int L, int scaling, int seed, int run, int precision,
                    int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
                    int* inner_pred, int* fit_status, char* err, size_t errlen);
+
+/* fpls_double_cv that also returns the class scores behind the labels, for
+ * margin checks and precision studies: inner_score kfold_outer x L x n x
+ * n_classes (entry ((o L + l) n + i) n_classes + c: the score of class c for
+ * training row i of outer fold o, predicted by its inner fold at ncomp slice
+ * l) and outer_score n x n_classes (row i's refit scores at the chosen ncomp,
+ * entry i n_classes + c); either may be null, not both.  Scores are the
+ * latent-route Ypred rows the argmax reads (pls_predict_classes_compact_cpu,
+ * fastPLS.cpp:4115-4154); rows that no fit predicts, or that took a
+ * single-class fallback, hold zeros.  No counterpart in the reference, whose
+ * classifier-0 CV returns labels only. */
+int fpls_double_cv_scores(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
+                          const int* outer_fold, int kfold_outer, const int* inner_fold, int kfold_inner,
+                          const int* ncomp, int L, int scaling, int seed, int run, int precision,
+                          int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
+                          int* inner_pred, int* fit_status, double* inner_score, double* outer_score,
+                          char* err, size_t errlen);
 
 /* fpls_double_cv over the outer folds listed in outer_ids (n_outer_ids distinct
  * 0-based ids) only, for fold-sharded grids: the caller splits the outer folds

@@ -22,8 +22,10 @@ def response_rows(y, idx, n_classes):
 
 def pls_cv_predict_compiled(X, y, fold, ncomp, n_classes, method=3, scaling=1, seed=1,
                             kfold=None):
-    """Classification CV with the argmax classifier (classifier 0, no score output).
-    Returns class_pred (n x L, 1-based) and the fold status vector."""
+    """Classification CV with the argmax classifier (classifier 0).
+    Returns class_pred (n x L, 1-based), the fold status vector and, for the
+    margin checks of the tests, class_score (n x L x m: the scores the argmax
+    read; zero for rows of skipped folds)."""
     X = np.asarray(X, dtype=np.float64)
     y = np.asarray(y)
     fold = np.asarray(fold)
@@ -32,6 +34,7 @@ def pls_cv_predict_compiled(X, y, fold, ncomp, n_classes, method=3, scaling=1, s
     n = X.shape[0]
     kfold = int(fold.max()) + 1 if kfold is None else kfold
     class_pred = np.zeros((n, L), dtype=np.int32)
+    class_score = np.zeros((n, L, n_classes))
     status = np.zeros(kfold, dtype=np.int32)
     for f in range(kfold):
         test = np.where(fold == f)[0]
@@ -56,9 +59,11 @@ def pls_cv_predict_compiled(X, y, fold, ncomp, n_classes, method=3, scaling=1, s
         else:
             model = opls.pls_model2_fast(X[train], Ytr, ncomp, scaling=scaling, fit=False,
                                          seed=seed + f)
-        class_pred[test, :] = opls.pls_predict_classes_compact(model, X[test])
+        lab, sc = opls.pls_predict_classes_compact(model, X[test], return_scores=True)
+        class_pred[test, :] = lab
+        class_score[test] = np.transpose(sc, (0, 2, 1))
         status[f] = 1
-    return dict(class_pred=class_pred, status=status, fold=fold + 1)
+    return dict(class_pred=class_pred, status=status, fold=fold + 1, class_score=class_score)
 
 
 def accuracy_table(class_pred, y):
@@ -92,6 +97,12 @@ def double_cv(X, y, outer_fold, inner_folds, ncomp, n_classes, scaling=1, seed=1
     best = np.zeros(K_out, dtype=np.int32)
     inner_acc = np.zeros((K_out, ncomp.size))
     pred = np.zeros(n, dtype=np.int32)
+    m = int(n_classes)
+    # class scores behind the labels: inner (kfold_outer x L x n x m, at the
+    # rows' own indices) and outer (n x m, at the chosen ncomp)
+    inner_pred = np.zeros((K_out, ncomp.size, n), dtype=np.int32)
+    inner_score = np.zeros((K_out, ncomp.size, n, m))
+    outer_score = np.zeros((n, m))
     for o in (range(K_out) if outer_ids is None else outer_ids):
         test = np.where(outer_fold == o)[0]
         train = np.where(outer_fold != o)[0]
@@ -100,10 +111,15 @@ def double_cv(X, y, outer_fold, inner_folds, ncomp, n_classes, scaling=1, seed=1
                                         seed=seed + 1000 * run + o + 1)
         acc = accuracy_table(inner["class_pred"], y[train])
         inner_acc[o] = acc
+        inner_pred[o][:, train] = inner["class_pred"].T
+        inner_score[o][:, train, :] = np.transpose(inner["class_score"], (1, 0, 2))
         best[o] = int(ncomp[best_index(acc)])
         Ytr = response_rows(y, train, n_classes)
         model = opls.pls_model2_fast(X[train], Ytr, [best[o]], scaling=scaling,
                                      seed=seed + 2000 * run + o + 1)
-        pred[test] = opls.pls_predict_classes_compact(model, X[test])[:, 0]
+        lab, sc = opls.pls_predict_classes_compact(model, X[test], return_scores=True)
+        pred[test] = lab[:, 0]
+        outer_score[test] = sc[:, :, 0]
     return dict(best_comp=best, inner_accuracy=inner_acc, pred=pred,
-                accuracy=float(np.mean(pred == y)))
+                accuracy=float(np.mean(pred == y)), inner_pred=inner_pred,
+                inner_score=inner_score, outer_score=outer_score)

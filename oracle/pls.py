@@ -461,7 +461,10 @@ def argmax_first(scores):
     return np.argmax(scores, axis=1).astype(np.int32) + 1
 
 
-def pls_predict_classes_compact(model, Xtest):
-    """pls_predict_classes_compact_cpu (fastPLS.cpp:4115-4154)."""
+def pls_predict_classes_compact(model, Xtest, return_scores=False):
+    """pls_predict_classes_compact_cpu (fastPLS.cpp:4115-4154).  With
+    return_scores the class scores the argmax reads (ntest x m x slices, the
+    latent-route Ypred) come back too."""
     pred = pls_predict(model, Xtest, use_B=False)["Ypred"]
-    return np.stack([argmax_first(pred[:, :, a]) for a in range(pred.shape[2])], axis=1)
+    labels = np.stack([argmax_first(pred[:, :, a]) for a in range(pred.shape[2])], axis=1)
+    return (labels, pred) if return_scores else labels

@@ -48,15 +48,7 @@ def parse():
 
 def workload(small=False, seed=1):
     from fastpls_b200 import synthetic
-    from fastpls_b200.folds import double_cv_folds
-    if small:
-        d = synthetic.c4_omics(seed=seed, n=1500, p=8000)
-    else:
-        d = synthetic.c4_omics(seed=seed)
-    outer, inner = double_cv_folds(d["y"], d["groups"], 10, 5, seed=seed)
-    d["outer"], d["inner"] = outer, inner
-    d["ncomp"] = np.arange(1, 31, dtype=np.int32)
-    return d
+    return synthetic.c4_double_cv(seed=seed, small=small)
 
 
 class Clocks:

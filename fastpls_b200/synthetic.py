@@ -80,6 +80,16 @@ def c4_omics(seed=1, n=3000, p=20000, n_informative=50, props=(0.4, 0.3, 0.2, 0.
                 groups=groups.astype(np.int32), n_classes=len(props))
 
 
+def c4_double_cv(seed=1, small=False):
+    """The double-CV benchmark workload: c4_omics (1500 x 8000 when small) with
+    10 outer x 5 inner stratified group folds and the ncomp grid 1..30."""
+    from .folds import double_cv_folds
+    d = c4_omics(seed=seed, n=1500, p=8000) if small else c4_omics(seed=seed)
+    d["outer"], d["inner"] = double_cv_folds(d["y"], d["groups"], 10, 5, seed=seed)
+    d["ncomp"] = np.arange(1, 31, dtype=np.int32)
+    return d
+
+
 def c5_lowrank(seed=1, n=50000, p=20000, q=5000, rank=40, n_test=10000):
     rng = np.random.default_rng(seed)
     nt = n + n_test

@@ -1,0 +1,65 @@
+"""Parity of the benchmark's double CV at its full size (3000 x 20000 FP32
+omics, 10 outer x 5 inner folds, ncomp 1..30: 1500 (fold, ncomp) fits).
+
+The FP64 batched grid (row-space engine, FP64 row Gram and K products) runs
+through the C ABI against the oracle's double CV (fastPLS.cpp:6805-7122 inside
+pls.double.cv, R/main.R:6586-6760) on the same input: chosen ncomp equal,
+labels identical wherever the oracle's decision margin exceeds 1e-8 of the
+score scale, class scores within relative 1e-9 in every (outer fold, ncomp)
+slice.  The mixed grid (BF16x3 row Gram, INT8 K products), the benchmarked
+form, is held to the FP64 grid beyond its own measured error: scores within
+1e-3 of a slice, labels identical beyond a 1e-3 margin, same chosen ncomp and
+outer predictions.  The oracle takes about 35 s of host time.
+"""
+import numpy as np
+import pytest
+
+from oracle import cv as ocv
+from fastpls_b200 import synthetic
+from parity_utils import REL_TOL, cv_labels_match, slice_score_rel_err
+
+pytestmark = pytest.mark.gpu
+
+MARGIN = 1e-8
+MIXED_TOL = 1e-3
+
+
+@pytest.fixture(scope="module")
+def full():
+    return synthetic.c4_double_cv(seed=1)
+
+
+@pytest.fixture(scope="module")
+def fp64_grid(lib, full):
+    w = full
+    return lib.double_cv(w["X"], w["y"], w["outer"], w["inner"], w["ncomp"], w["n_classes"], seed=1,
+                         precision="fp64", return_scores=True)
+
+
+def test_full_size_fp64_grid_matches_oracle(lib, full, fp64_grid):
+    w = full
+    ref = ocv.double_cv(w["X"].astype(np.float64), w["y"], w["outer"], w["inner"], w["ncomp"], w["n_classes"],
+                        seed=1)
+    got = fp64_grid
+    assert np.array_equal(got["best_comp"], ref["best_comp"])
+    assert np.all(got["fit_status"] == 1)
+    gi = np.transpose(got["inner_pred"], (2, 1, 0))
+    ok, nclear, bad, _ = cv_labels_match(gi, ref["inner_pred"], ref["inner_score"], MARGIN)
+    assert ok and nclear > 0.99 * gi.size, (bad, nclear)
+    assert cv_labels_match(got["pred"], ref["pred"], ref["outer_score"], MARGIN)[0]
+    assert slice_score_rel_err(got["inner_score"], ref["inner_score"]) < REL_TOL
+    assert slice_score_rel_err(got["outer_score"][None], ref["outer_score"][None]) < REL_TOL
+    assert np.allclose(got["inner_accuracy"], ref["inner_accuracy"], rtol=0, atol=1e-12)
+
+
+def test_full_size_mixed_grid_against_fp64(lib, full, fp64_grid):
+    w = full
+    a = fp64_grid
+    b = lib.double_cv(w["X"], w["y"], w["outer"], w["inner"], w["ncomp"], w["n_classes"], seed=1,
+                      precision="bf16x3", return_scores=True)
+    assert np.array_equal(a["best_comp"], b["best_comp"])
+    assert np.array_equal(a["pred"], b["pred"])
+    assert cv_labels_match(b["inner_pred"], a["inner_pred"], np.transpose(a["inner_score"], (2, 1, 0, 3)),
+                           MIXED_TOL)[0]
+    assert slice_score_rel_err(b["inner_score"], a["inner_score"]) < MIXED_TOL
+    assert slice_score_rel_err(b["outer_score"][None], a["outer_score"][None]) < 1e-5

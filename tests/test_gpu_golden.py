@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from golden.make_golden import C1_NCOMP, C2_NCOMP, C5_NCOMP, inputs_of
-from parity_utils import REL_TOL, cv_labels_match, labels_match_beyond_margin, rel_err
+from parity_utils import REL_TOL, cv_labels_match, labels_match_beyond_margin, rel_err, sign_align
 
 pytestmark = pytest.mark.gpu
 
@@ -59,7 +59,10 @@ def test_golden_c2_plssvd_lda(lib):
     lda = lib.lda_project_train_prefix(X, Rp, off, x["ytrain"], m, C2_NCOMP, ridge=1e-8)
     for kk in C2_NCOMP:
         g = lib.lda_project_predict(Xt, Rp[:, :kk], off[:kk], lda[str(kk)], return_scores=True)
-        assert rel_err(lda[str(kk)]["linear"], want[f"lda{kk}_linear"]) < REL_TOL
+        # each component of the rSVD is defined up to sign, and so is its LDA column
+        lin = sign_align(lda[str(kk)]["linear"], want[f"lda{kk}_linear"])
+        assert rel_err(lin, want[f"lda{kk}_linear"]) < REL_TOL
+        assert rel_err(lda[str(kk)]["constants"], want[f"lda{kk}_constants"]) < REL_TOL
         assert rel_err(g["scores"], want[f"lda{kk}_scores"]) < REL_TOL
         ok, nclear = labels_match_beyond_margin(g["pred"], want[f"lda{kk}_pred"], want[f"lda{kk}_scores"],
                                                 MARGIN)

@@ -145,7 +145,39 @@ def version():
 
 
 # ---------------------------------------------------------------- helpers ---
+class DeviceMatrix:
+    """A column-major FP64 matrix already in device memory, taken from any
+    object exposing __cuda_array_interface__ (for instance the transpose of a
+    contiguous torch CUDA tensor).  The matrix entry points accept it for X, Y,
+    Xtest, the response and the filtered-X output: the library then copies
+    within HBM instead of across PCIe (the C ABI tells host and device
+    pointers apart by unified addressing)."""
+
+    def __init__(self, obj):
+        cai = obj.__cuda_array_interface__
+        shape = tuple(int(v) for v in cai["shape"])
+        if cai["typestr"] != "<f8" or len(shape) not in (1, 2):
+            raise ValueError("device matrices must be float64 vectors or matrices")
+        if len(shape) == 1:
+            shape = (shape[0], 1)
+        rows, cols = shape
+        strides = cai.get("strides")
+        if strides is not None and len(cai["shape"]) == 2 and rows > 1 and cols > 1 and \
+                tuple(strides) != (8, 8 * rows):
+            raise ValueError("device matrices must be column-major and contiguous")
+        self.ptr = int(cai["data"][0])
+        self.shape = shape
+        self.dtype = np.dtype(np.float64)
+        self.owner = obj
+
+
+def _is_device(a):
+    return isinstance(a, DeviceMatrix) or hasattr(a, "__cuda_array_interface__")
+
+
 def _f64(a, shape=None):
+    if _is_device(a):
+        return a if isinstance(a, DeviceMatrix) else DeviceMatrix(a)
     a = np.asarray(a, dtype=np.float64)
     if shape is not None:
         a = a.reshape(shape)
@@ -159,6 +191,8 @@ def _i32(a):
 def _p(a):
     if a is None:
         return None
+    if isinstance(a, DeviceMatrix):
+        return ctypes.cast(ctypes.c_void_p(a.ptr), _c_double_p)
     if a.dtype == np.int32:
         return a.ctypes.data_as(_c_int_p)
     return a.ctypes.data_as(_c_double_p)
@@ -687,13 +721,13 @@ def gaussian_y_encode(Y, projection):
     return dict(Z=Z, y_center=mu, decoder=dec)
 
 
-def gaussian_y_decode(Z, decoder, y_center):
+def gaussian_y_decode(Z, decoder, y_center, out=None):
     Z = _f64(Z)
     D = _f64(decoder)
     mu = np.ascontiguousarray(y_center, dtype=np.float64).ravel()
     w, d = Z.shape
     q = D.shape[1]
-    Y = _out(w, q)
+    Y = _out(w, q) if out is None else _f64(out)
     _call("fpls_gaussian_y_decode", _p(Z), w, d, _p(D), _p(mu), q, _p(Y))
     return Y
 
@@ -706,12 +740,14 @@ def nearest_code_classes(Z, codes):
     return lab
 
 
-def opls_filter(X, Y, north, scaling=1):
+def opls_filter(X, Y, north, scaling=1, out=None):
+    """OPLS filter; `out` (optional, n x p, host or device) receives the filtered X."""
     X = _f64(X)
     Y = _f64(Y)
     n, p = X.shape
     q = Y.shape[1]
-    Xf, mX, vX = _out(n, p), np.zeros(p), np.zeros(p)
+    Xf = _out(n, p) if out is None else _f64(out)
+    mX, vX = np.zeros(p), np.zeros(p)
     W, P = _out(p, max(north, 1)), _out(p, max(north, 1))
     used = ctypes.c_int(0)
     _call("fpls_opls_filter", _p(X), n, p, _p(Y), q, int(north), int(scaling), _p(Xf), _p(mX),
@@ -720,12 +756,12 @@ def opls_filter(X, Y, north, scaling=1):
     return dict(X=Xf, mX=mX, vX=vX, W_orth=W[:, :k], P_orth=P[:, :k], north=k)
 
 
-def opls_apply_filter(X, mX, vX, W_orth, P_orth):
+def opls_apply_filter(X, mX, vX, W_orth, P_orth, out=None):
     X = _f64(X)
     w, p = X.shape
     W = _f64(W_orth)
     P = _f64(P_orth)
-    out = _out(w, p)
+    out = _out(w, p) if out is None else _f64(out)
     _call("fpls_opls_apply_filter", _p(X), w, p, _p(np.ascontiguousarray(mX, dtype=np.float64).ravel()),
           _p(np.ascontiguousarray(vX, dtype=np.float64).ravel()), _p(W), _p(P), W.shape[1], _p(out))
     return out

@@ -342,6 +342,8 @@ void gemm(bool transA, bool transB, int M, int N, int K, double alpha, const dou
     FPLS_CHECK_LAUNCH();
   }
   dim3 grid(gm, gn, splits);
+  Context& ctx = Context::get();
+  const int slot = ctx.prof_begin("gemm_f64_dmma", st);
   if (!transA && !transB)
     gemm_f64_dmma<false, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic, 0);
   else if (transA && !transB)
@@ -352,6 +354,8 @@ void gemm(bool transA, bool transB, int M, int N, int K, double alpha, const dou
     gemm_f64_dmma<true, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic, 0);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+  // algorithmic work: 2MNK flops; each operand and the result once
+  ctx.prof_end(slot, st, 8.0 * ((double)M * K + (double)K * N + (double)M * N), 2.0 * (double)M * N * K);
 }
 
 __global__ void mirror_upper_f64_kernel(double* K, int n, int ldk) {
@@ -389,7 +393,9 @@ void gram_f64(const double* X, int n, int p, int ldx, double* K, int ldk) {
 
 void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda, const double* x,
           double beta, double* y) {
-  cudaStream_t st = Context::get().stream;
+  Context& ctx = Context::get();
+  cudaStream_t st = ctx.stream;
+  const int slot = rows > 0 && cols > 0 ? ctx.prof_begin("gemv_f64", st) : -1;
   if (!trans) {
     if (rows <= 0) return;
     if (cols <= 0) {
@@ -414,6 +420,8 @@ void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda
     gemv_t_kernel<<<ceil_div(cols, 8), 256, 0, st>>>(rows, cols, alpha, A, lda, x, beta, y); ::fpls::note_launch();
   }
   FPLS_CHECK_LAUNCH();
+  // algorithmic bytes: the matrix once plus both vectors
+  ctx.prof_end(slot, st, 8.0 * ((double)rows * cols + rows + cols), 2.0 * (double)rows * cols);
 }
 
 void col_mean(const double* X, int n, int p, int ldx, double* out) {

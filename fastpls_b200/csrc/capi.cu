@@ -1205,7 +1205,7 @@ int fpls_x_upload(const void* X, int x_is_float32, int n, int p, int* handle, ch
     r.f32 = x_is_float32 != 0;
     const size_t bytes = (size_t)n * p * (r.f32 ? sizeof(float) : sizeof(double));
     FPLS_CUDA(cudaMalloc(&r.ptr, bytes));
-    FPLS_CUDA(cudaMemcpyAsync(r.ptr, X, bytes, cudaMemcpyHostToDevice, ctx.stream));
+    FPLS_CUDA(cudaMemcpyAsync(r.ptr, X, bytes, cudaMemcpyDefault, ctx.stream));
     ctx.sync();
     int h = -1;
     for (size_t i = 0; i < ctx.resident.size(); ++i)

@@ -569,9 +569,22 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
       attr_set = true;
     }
     FPLS_REQUIRE(items.size() < (1u << 31), "candidate-kNN: too many work items");
+    const int slot = ctx.prof_begin("cknn_tiles", ctx.stream);
     knn_tile_kernel<<<(unsigned)items.size(), kTileThreads, smem, ctx.stream>>>(
         ditems, ci, pairs, ntest, Tq, cr.Ts, kdim, use_k, part); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    if (slot >= 0) {
+      // algorithmic work: one kdim-long FP64 dot per (candidate pair, class row);
+      // bytes: every class's training rows once per 64-row tile of its pairs,
+      // the test rows once
+      double work = 0.0, bytes = 8.0 * (double)ntest * kdim;
+      for (int c = 0; c < C; ++c) {
+        const double rows = cr.offs[c + 1] - cr.offs[c];
+        work += (double)hp[c] * rows;
+        bytes += 8.0 * kdim * rows * (double)ceil_div(hp[c], kTileM);
+      }
+      ctx.prof_end(slot, ctx.stream, bytes, 2.0 * work * kdim);
+    }
   }
   pt.mark("similarity tiles");
   fill(cscore, (size_t)npairs, -INFINITY);

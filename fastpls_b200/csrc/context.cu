@@ -142,13 +142,16 @@ void Context::release() {
   arena.release();
 }
 
+// The caller's side of a copy may be host or device memory (unified
+// addressing tells them apart): a caller that already holds its matrices in
+// HBM passes device pointers and the copy stays on the device.
 void h2d(void* dst, const void* src, size_t bytes) {
   if (bytes == 0) return;
-  FPLS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, Context::get().stream));
+  FPLS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, Context::get().stream));
 }
 void d2h(void* dst, const void* src, size_t bytes) {
   if (bytes == 0) return;
-  FPLS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, Context::get().stream));
+  FPLS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, Context::get().stream));
 }
 void d2d(void* dst, const void* src, size_t bytes) {
   if (bytes == 0) return;

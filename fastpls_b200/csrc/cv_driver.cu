@@ -327,7 +327,7 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
     for (int c = 0; c < nch; ++c) {
       const int j0 = bounds[c], j1 = bounds[c + 1];
       FPLS_CUDA(cudaMemcpyAsync(dst + (size_t)j0 * n * esz, src + (size_t)j0 * n * esz, (size_t)(j1 - j0) * n * esz,
-                                cudaMemcpyHostToDevice, ctx.copy));
+                                cudaMemcpyDefault, ctx.copy));
       FPLS_CUDA(cudaEventRecord(ctx.copy_event(c), ctx.copy));
       if (c > 0) chunk_work(c - 1);
     }

@@ -97,7 +97,9 @@ def c5_lowrank(seed=1, n=50000, p=20000, q=5000, rank=40, n_test=10000):
     V = _orth(rng, p, rank).astype(np.float32)
     s = (20.0 * 0.9 ** np.arange(rank)).astype(np.float32)
     X = (U * s) @ V.T + rng.standard_normal((nt, p), dtype=np.float32)
-    Bs = (rng.standard_normal((p, rank), dtype=np.float32) @ rng.standard_normal((rank, q), dtype=np.float32)) / np.float32(np.sqrt(p * rank))
-    Y = X @ Bs + 0.1 * rng.standard_normal((nt, q), dtype=np.float32)
+    # B* = B1 B2 / sqrt(p rank) has rank 40; Y = (X B1) B2 never forms the p x q product
+    B1 = rng.standard_normal((p, rank), dtype=np.float32)
+    B2 = rng.standard_normal((rank, q), dtype=np.float32) / np.float32(np.sqrt(p * rank))
+    Y = (X @ B1) @ B2 + 0.1 * rng.standard_normal((nt, q), dtype=np.float32)
     return dict(Xtrain=np.asfortranarray(X[:n]), Ytrain=np.asfortranarray(Y[:n]),
                 Xtest=np.asfortranarray(X[n:]), Ytest=np.asfortranarray(Y[n:]))

@@ -9,9 +9,18 @@
  *  - Matrices are column-major double (R / Armadillo layout); "cubes" are
  *    rows x cols x slices, slice-major, as R arrays.
  *  - Class labels are int32, 1-based.  ncomp vectors are int32.
- *  - All pointers are HOST pointers owned by the caller; outputs are written
- *    into caller-allocated buffers of the documented sizes.  Optional outputs
- *    may be NULL.
+ *  - Pointers are owned by the caller; outputs are written into
+ *    caller-allocated buffers of the documented sizes.  Optional outputs may
+ *    be NULL.  Scalars' arrays (labels, folds, ncomp lists, R2Y and the other
+ *    per-component or per-class vectors) are HOST memory.  The matrices a call
+ *    copies whole (X, Y, Xtest, the response Z, the filtered X and the
+ *    prediction blocks of fpls_pls_model1, fpls_pls_model2_fast,
+ *    fpls_predict_lowrank, fpls_lda_project_train_prefix,
+ *    fpls_lda_project_predict, fpls_opls_filter, fpls_opls_apply_filter,
+ *    fpls_gaussian_y_encode / _decode and fpls_x_upload) may instead be device
+ *    memory of the library's device: unified addressing tells the two apart
+ *    and the copy then stays in HBM (no counterpart in the reference, whose
+ *    inputs are R objects in host memory).
  *  - Every function returns 0 on success or a non-zero fpls_status; on failure a
  *    NUL-terminated message is written to err[0..errlen-1] (err may be NULL).
  *    No exception crosses this boundary and there is no CPU fallback: without

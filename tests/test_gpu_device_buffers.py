@@ -1,0 +1,61 @@
+"""Matrix arguments already in HBM: the entry points that copy X, Y, Xtest, the
+response or the filtered X whole accept device pointers (unified addressing
+tells them from host pointers) and give the results of the host-buffer calls.
+The device buffers come from torch, standing in for a caller that keeps its
+data on the GPU."""
+import numpy as np
+import pytest
+
+from fastpls_b200 import synthetic
+from parity_utils import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(torch, a):
+    """Column-major device copy of a 2-D host array (transpose of a contiguous tensor)."""
+    a = np.asarray(a, dtype=np.float64)
+    return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().T
+
+
+def test_fits_and_predictions_from_device_buffers(lib):
+    torch = pytest.importorskip("torch")
+    d = synthetic.c5_lowrank(seed=6, n=600, p=300, q=80, rank=6, n_test=100)
+    X, Y, Xt = (d[k].astype(np.float64) for k in ("Xtrain", "Ytrain", "Xtest"))
+    Xd, Yd, Xtd = _dev(torch, X), _dev(torch, Y), _dev(torch, Xt)
+    torch.cuda.synchronize()
+    host = lib.pls_model2_fast(X, Y, [3, 7], seed=2)
+    dev = lib.pls_model2_fast(Xd, Yd, [3, 7], seed=2)
+    assert np.array_equal(host["B"], dev["B"]) and np.array_equal(host["R"], dev["R"])
+    m1h = lib.pls_model1(X, Y, [4], svd_method=4, seed=3)
+    m1d = lib.pls_model1(Xd, Yd, [4], svd_method=4, seed=3)
+    assert np.array_equal(m1h["B"], m1d["B"])
+    ph = lib.predict_lowrank(host, Xt)["Ypred"]
+    pd = lib.predict_lowrank(host, Xtd)["Ypred"]
+    assert np.array_equal(ph, pd)
+    # filtered X written straight into a device buffer
+    out = torch.empty((X.shape[1], X.shape[0]), dtype=torch.float64, device="cuda").T
+    fh = lib.opls_filter(X, Y, 2)
+    fd = lib.opls_filter(Xd, Yd, 2, out=out)
+    torch.cuda.synchronize()
+    assert np.array_equal(fh["X"], out.cpu().numpy())
+    assert np.array_equal(fh["W_orth"], fd["W_orth"])
+    outt = torch.empty((Xt.shape[1], Xt.shape[0]), dtype=torch.float64, device="cuda").T
+    lib.opls_apply_filter(Xtd, fd["mX"], fd["vX"], fd["W_orth"], fd["P_orth"], out=outt)
+    torch.cuda.synchronize()
+    assert np.array_equal(outt.cpu().numpy(),
+                          lib.opls_apply_filter(Xt, fh["mX"], fh["vX"], fh["W_orth"], fh["P_orth"]))
+    G = np.random.default_rng(1).standard_normal((Y.shape[1], 10)) / np.sqrt(10.0)
+    eh = lib.gaussian_y_encode(Y, G)
+    ed = lib.gaussian_y_encode(Yd, G)
+    assert np.array_equal(eh["Z"], ed["Z"]) and np.array_equal(eh["decoder"], ed["decoder"])
+    assert rel_err(lib.predict_lowrank(dev, Xtd)["Ypred"], ph) == 0.0
+
+
+def test_device_matrix_layout_is_checked(lib):
+    torch = pytest.importorskip("torch")
+    X = torch.zeros((50, 40), dtype=torch.float64, device="cuda")  # row-major: not column-major
+    with pytest.raises(ValueError):
+        lib.DeviceMatrix(X)
+    with pytest.raises(ValueError):
+        lib.DeviceMatrix(torch.zeros((50, 40), dtype=torch.float32, device="cuda").T)

@@ -161,9 +161,9 @@ class DeviceMatrix:
         if len(shape) == 1:
             shape = (shape[0], 1)
         rows, cols = shape
-        strides = cai.get("strides")
-        if strides is not None and len(cai["shape"]) == 2 and rows > 1 and cols > 1 and \
-                tuple(strides) != (8, 8 * rows):
+        strides = cai.get("strides")  # None: C-contiguous
+        if len(cai["shape"]) == 2 and rows > 1 and cols > 1 and \
+                (strides is None or tuple(strides) != (8, 8 * rows)):
             raise ValueError("device matrices must be column-major and contiguous")
         self.ptr = int(cai["data"][0])
         self.shape = shape

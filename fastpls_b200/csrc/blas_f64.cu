@@ -59,7 +59,7 @@ template <bool TA, bool TB>
 __global__ void __launch_bounds__(GEMM_THREADS)
 gemm_f64_dmma(int M, int N, int K, double alpha, const double* __restrict__ A, int lda,
               const double* __restrict__ B, int ldb, double beta, double* __restrict__ C, int ldc,
-              int k_per_split, int use_atomic, int upper) {
+              int k_per_split, long long split_stride, int upper) {
   __shared__ double As[2][BK][BM + PAD];
   __shared__ double Bs[2][BK][BN + PAD];
   const int bm = blockIdx.x * BM;
@@ -125,10 +125,12 @@ gemm_f64_dmma(int M, int N, int K, double alpha, const double* __restrict__ A, i
       for (int e = 0; e < 2; ++e) {
         const int n = bn + wn + j * 8 + tig * 2 + e;
         if (n >= N) continue;
-        double* cp = C + m + (size_t)n * ldc;
+        // split-K: each K range stores its own partial (summed in range order
+        // by splitk_reduce_kernel, so runs repeat bit for bit)
+        double* cp = C + (size_t)blockIdx.z * split_stride + m + (size_t)n * ldc;
         const double v = alpha * acc[i][j][e];
-        if (use_atomic) {
-          atomicAdd(cp, v);
+        if (split_stride) {
+          *cp = v;
         } else {
           *cp = (beta == 0.0) ? v : (v + beta * *cp);
         }
@@ -151,7 +153,7 @@ __global__ void scale_matrix_kernel(double* C, int M, int N, int ldc, double bet
 // y[m] = alpha * sum_k A[m + k*lda] x[k] (+ beta y) ; grid.y splits K, atomics combine.
 __global__ void gemv_n_kernel(int M, int K, double alpha, const double* __restrict__ A, int lda,
                               const double* __restrict__ x, double* __restrict__ y,
-                              int k_per_split, int use_atomic, double beta) {
+                              int k_per_split, long long split_stride, double beta) {
   __shared__ double xs[256];
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   const int kbeg = blockIdx.y * k_per_split;
@@ -175,8 +177,22 @@ __global__ void gemv_n_kernel(int M, int K, double alpha, const double* __restri
     }
   }
   if (m < M) {
-    if (use_atomic) atomicAdd(y + m, alpha * acc);
+    if (split_stride) y[(size_t)blockIdx.y * split_stride + m] = alpha * acc;
     else y[m] = (beta == 0.0) ? alpha * acc : alpha * acc + beta * y[m];
+  }
+}
+
+// C (M x N, ldc) = beta C + sum_{z < splits} W_z, W_z = W + z stride (ld ldw):
+// the split-K partials added in K-range order.
+__global__ void splitk_reduce_kernel(const double* __restrict__ W, int splits, long long stride, int M, int N,
+                                     int ldw, double beta, double* __restrict__ C, int ldc) {
+  const size_t total = (size_t)M * N;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int m = static_cast<int>(t % M), n = static_cast<int>(t / M);
+    double acc = 0.0;
+    for (int z = 0; z < splits; ++z) acc += W[(size_t)z * stride + m + (size_t)n * ldw];
+    double* cp = C + m + (size_t)n * ldc;
+    *cp = (beta == 0.0) ? acc : acc + beta * *cp;
   }
 }
 
@@ -336,24 +352,34 @@ void gemm(bool transA, bool transB, int M, int N, int K, double alpha, const dou
   int kps = ceil_div(K, splits);
   kps = ceil_div(kps, BK) * BK;
   splits = ceil_div(K, kps);
-  const int use_atomic = splits > 1 ? 1 : 0;
-  if (use_atomic) {
-    scale_matrix_kernel<<<grid_for((size_t)M * N, 256), 256, 0, st>>>(C, M, N, ldc, beta); ::fpls::note_launch();
-    FPLS_CHECK_LAUNCH();
+  // split-K partials go to a per-stream workspace and are summed in order
+  double* dst = C;
+  int ldd = ldc;
+  long long stride = 0;
+  if (splits > 1) {
+    stride = (long long)M * N;
+    dst = Context::get().splitk_workspace(st, (size_t)splits * M * N);
+    ldd = M;
   }
+  const double beta_k = splits > 1 ? 0.0 : beta;
   dim3 grid(gm, gn, splits);
   Context& ctx = Context::get();
   const int slot = ctx.prof_begin("gemm_f64_dmma", st);
   if (!transA && !transB)
-    gemm_f64_dmma<false, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic, 0);
+    gemm_f64_dmma<false, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta_k, dst, ldd, kps, stride, 0);
   else if (transA && !transB)
-    gemm_f64_dmma<true, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic, 0);
+    gemm_f64_dmma<true, false><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta_k, dst, ldd, kps, stride, 0);
   else if (!transA && transB)
-    gemm_f64_dmma<false, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic, 0);
+    gemm_f64_dmma<false, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta_k, dst, ldd, kps, stride, 0);
   else
-    gemm_f64_dmma<true, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kps, use_atomic, 0);
+    gemm_f64_dmma<true, true><<<grid, GEMM_THREADS, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta_k, dst, ldd, kps, stride, 0);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+  if (splits > 1) {
+    splitk_reduce_kernel<<<grid_for((size_t)M * N, 256), 256, 0, st>>>(dst, splits, stride, M, N, ldd, beta, C, ldc);
+    ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+  }
   // algorithmic work: 2MNK flops; each operand and the result once
   ctx.prof_end(slot, st, 8.0 * ((double)M * K + (double)K * N + (double)M * N), 2.0 * (double)M * N * K);
 }
@@ -377,15 +403,28 @@ void gram_f64(const double* X, int n, int p, int ldx, double* K, int ldk) {
   if (tiles < target && p >= 4 * BK) splits = std::max(1, std::min(ceil_div(target, tiles), ceil_div(p, 8 * BK)));
   int kps = ceil_div(ceil_div(p, splits), BK) * BK;
   splits = ceil_div(p, kps);
-  const int use_atomic = splits > 1 ? 1 : 0;
-  if (use_atomic || p <= 0) {
+  if (p <= 0) {
     scale_matrix_kernel<<<grid_for((size_t)n * n, 256), 256, 0, st>>>(K, n, n, ldk, 0.0); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
   if (p > 0) {
-    gemm_f64_dmma<false, true><<<dim3(g, g, splits), GEMM_THREADS, 0, st>>>(n, n, p, 1.0, X, ldx, X, ldx, 0.0, K,
-                                                                         ldk, kps, use_atomic, 1); ::fpls::note_launch();
+    double* dst = K;
+    int ldd = ldk;
+    long long stride = 0;
+    if (splits > 1) {  // partials of the K ranges, summed in order (lower tiles stay unused)
+      stride = (long long)n * n;
+      dst = ctx.splitk_workspace(st, (size_t)splits * n * n);
+      ldd = n;
+    }
+    gemm_f64_dmma<false, true><<<dim3(g, g, splits), GEMM_THREADS, 0, st>>>(n, n, p, 1.0, X, ldx, X, ldx, 0.0, dst,
+                                                                         ldd, kps, stride, 1); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    if (splits > 1) {
+      splitk_reduce_kernel<<<grid_for((size_t)n * n, 256), 256, 0, st>>>(dst, splits, stride, n, n, ldd, 0.0, K,
+                                                                        ldk);
+      ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+    }
   }
   mirror_upper_f64_kernel<<<grid_for((size_t)n * n, 256), 256, 0, st>>>(K, n, ldk); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
@@ -409,12 +448,17 @@ void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda
     if (gx < target) splits = std::max(1, std::min(ceil_div(target, gx), ceil_div(cols, 256)));
     int kps = ceil_div(cols, splits);
     splits = ceil_div(cols, kps);
-    const int use_atomic = splits > 1 ? 1 : 0;
-    if (use_atomic) {
-      scale_matrix_kernel<<<grid_for(rows, 256), 256, 0, st>>>(y, rows, 1, rows, beta); ::fpls::note_launch();
+    if (splits > 1) {
+      // partials of the column ranges, summed in order (runs repeat bit for bit)
+      double* ws = ctx.splitk_workspace(st, (size_t)splits * rows);
+      gemv_n_kernel<<<dim3(gx, splits), 256, 0, st>>>(rows, cols, alpha, A, lda, x, ws, kps, (long long)rows, 0.0);
+      ::fpls::note_launch();
       FPLS_CHECK_LAUNCH();
+      splitk_reduce_kernel<<<grid_for(rows, 256), 256, 0, st>>>(ws, splits, rows, rows, 1, rows, beta, y, rows);
+    } else {
+      gemv_n_kernel<<<dim3(gx, splits), 256, 0, st>>>(rows, cols, alpha, A, lda, x, y, kps, 0ll, beta);
     }
-    gemv_n_kernel<<<dim3(gx, splits), 256, 0, st>>>(rows, cols, alpha, A, lda, x, y, kps, use_atomic, beta); ::fpls::note_launch();
+    ::fpls::note_launch();
   } else {
     if (cols <= 0) return;
     gemv_t_kernel<<<ceil_div(cols, 8), 256, 0, st>>>(rows, cols, alpha, A, lda, x, beta, y); ::fpls::note_launch();

@@ -675,7 +675,6 @@ int fpls_lda_train_prefix(const double* T, int n, int kmax, const int* y, int n_
     Context& ctx = Context::get();
     ctx.begin_call();
     const double* dT = upload(T, (size_t)n * kmax);
-    const int* dy = upload(y, n);
     LdaModelsDev d;
     d.means = ctx.arena.alloc_n<double>((size_t)n_classes * km * L);
     d.linear = ctx.arena.alloc_n<double>((size_t)n_classes * km * L);
@@ -683,7 +682,7 @@ int fpls_lda_train_prefix(const double* T, int n, int kmax, const int* y, int n_
     d.priors = ctx.arena.alloc_n<double>(n_classes);
     std::vector<double> lam(L);
     d.lambda = lam.data();
-    lda_train_prefix(dT, n, km, dy, n_classes, ncomp, L, ridge, d);
+    lda_train_prefix(dT, n, km, y, n_classes, ncomp, L, ridge, d);
     lda_outputs_to_host(d, n_classes, km, L, means, linear, constants, priors);
     ctx.sync();
     if (lambda) std::copy(lam.begin(), lam.end(), lambda);
@@ -712,7 +711,6 @@ int fpls_lda_project_train_prefix(const double* X, int n, int p, const double* R
       scale_vec(doff, k, -1.0);
       add_row_vector(dT, n, k, n, doff);
     }
-    const int* dy = upload(y, n);
     LdaModelsDev d;
     d.means = ctx.arena.alloc_n<double>((size_t)n_classes * km * L);
     d.linear = ctx.arena.alloc_n<double>((size_t)n_classes * km * L);
@@ -720,7 +718,7 @@ int fpls_lda_project_train_prefix(const double* X, int n, int p, const double* R
     d.priors = ctx.arena.alloc_n<double>(n_classes);
     std::vector<double> lam(L);
     d.lambda = lam.data();
-    lda_train_prefix(dT, n, km, dy, n_classes, ncomp, L, ridge, d);
+    lda_train_prefix(dT, n, km, y, n_classes, ncomp, L, ridge, d);
     lda_outputs_to_host(d, n_classes, km, L, means, linear, constants, priors);
     ctx.sync();
     if (lambda) std::copy(lam.begin(), lam.end(), lambda);

@@ -140,6 +140,25 @@ void Context::release() {
   if (copy) cudaStreamSynchronize(copy);
   cudaStreamSynchronize(stream);
   arena.release();
+  for (auto& b : splitk) cudaFree(b.ptr);
+  splitk.clear();
+}
+
+double* Context::splitk_workspace(cudaStream_t st, size_t elems) {
+  for (auto& b : splitk) {
+    if (b.stream != st) continue;
+    if (b.cap >= elems) return b.ptr;
+    // grow: earlier products on this stream may still read the old buffer
+    FPLS_CUDA(cudaStreamSynchronize(st));
+    FPLS_CUDA(cudaFree(b.ptr));
+    b.cap = std::max(elems, 2 * b.cap);
+    FPLS_CUDA(cudaMalloc(&b.ptr, b.cap * sizeof(double)));
+    return b.ptr;
+  }
+  StreamBuffer b{st, nullptr, std::max<size_t>(elems, 1 << 20)};
+  FPLS_CUDA(cudaMalloc(&b.ptr, b.cap * sizeof(double)));
+  splitk.push_back(b);
+  return b.ptr;
 }
 
 // The caller's side of a copy may be host or device memory (unified

@@ -68,6 +68,12 @@ struct Context {
   int prof_begin(const char* cls, cudaStream_t st);
   void prof_end(int slot, cudaStream_t st, double bytes, double flops);
   std::vector<ResidentX> resident;
+  // Split-K partials of the FP64 products, one buffer per stream (grown on
+  // demand, kept across calls): partial sums are added in K-range order
+  // instead of by atomics, so FP64 results repeat bit for bit.
+  struct StreamBuffer { cudaStream_t stream; double* ptr; size_t cap; };
+  std::vector<StreamBuffer> splitk;
+  double* splitk_workspace(cudaStream_t st, size_t elems);
 
   static Context& get();       // initialises the device on first use
   void begin_call();           // resets the arena and the status flag, starts the call timer

@@ -52,32 +52,22 @@ __global__ void topk_kernel(const double* __restrict__ S, int w, int C, const do
   }
 }
 
-// Per-column class sums of T (n x kmax) into sums (C x kmax); block j handles column j.
-__global__ void class_sums_kernel(const double* __restrict__ T, int n, int kmax, const int* y,
-                                  int C, double* sums, double* counts, int* bad) {
-  extern __shared__ double bins[];
-  const int j = blockIdx.x;
-  for (int c = threadIdx.x; c < C; c += blockDim.x) bins[c] = 0.0;
-  __syncthreads();
+// Class sums of the score columns (T n x kmax into sums C x kmax) in a fixed
+// order: warp w takes (class c, column j) = (w % C, w / C) and walks that
+// class's rows in class-sorted order perm[off[c] .. off[c+1]) lane-strided,
+// then a fixed shuffle tree -- the same rounding on every run (no atomics).
+__global__ void class_sums_sorted_kernel(const double* __restrict__ T, int n, int kmax,
+                                         const int* __restrict__ perm, const int* __restrict__ off, int C,
+                                         double* __restrict__ sums) {
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= (long long)C * kmax) return;  // whole warps leave together
+  const int c = static_cast<int>(w % C), j = static_cast<int>(w / C);
   const double* tc = T + (size_t)j * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const int cls = y[i] - 1;
-    if (cls < 0 || cls >= C) { atomicExch(bad, 1); continue; }
-    atomicAdd(&bins[cls], tc[i]);
-  }
-  __syncthreads();
-  for (int c = threadIdx.x; c < C; c += blockDim.x) sums[c + (size_t)j * C] = bins[c];
-  if (j == 0 && counts) {
-    __syncthreads();
-    for (int c = threadIdx.x; c < C; c += blockDim.x) bins[c] = 0.0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const int cls = y[i] - 1;
-      if (cls >= 0 && cls < C) atomicAdd(&bins[cls], 1.0);
-    }
-    __syncthreads();
-    for (int c = threadIdx.x; c < C; c += blockDim.x) counts[c] = bins[c];
-  }
+  double acc = 0.0;
+  for (int i = off[c] + lane; i < off[c + 1]; i += 32) acc += tc[perm[i]];
+  acc = warp_sum(acc);
+  if (lane == 0) sums[c + (size_t)j * C] = acc;
 }
 
 __global__ void means_from_sums_kernel(double* M, int C, int k, const double* counts,
@@ -174,26 +164,41 @@ void row_topk(const double* S, int w, int C, const double* bias, int top_k, int*
   FPLS_CHECK_LAUNCH();
 }
 
-void lda_train_prefix(const double* T, int n, int kmax, const int* y, int C,
+void lda_train_prefix(const double* T, int n, int kmax, const int* y_host, int C,
                       const int* ncomp_host, int L, double ridge, LdaModelsDev out) {
   Context& ctx = Context::get();
   FPLS_REQUIRE(n > 0 && kmax > 0, "lda_train_prefix requires a non-empty score matrix");
   FPLS_REQUIRE(C >= 2, "lda_train_prefix requires at least two classes");
+  // class counts and a stable class-sorted row order (host, O(n))
+  std::vector<int> off(C + 1, 0), perm(n);
+  for (int i = 0; i < n; ++i) {
+    const int cls = y_host[i] - 1;
+    if (cls < 0 || cls >= C) throw Error(kErrArgument, "lda_train_prefix labels must be encoded as 1..n_classes");
+    ++off[cls + 1];
+  }
+  std::vector<double> hc(C);
+  for (int c = 0; c < C; ++c) {
+    if (off[c + 1] <= 0) throw Error(kErrArgument, "lda_train_prefix received an empty class");
+    hc[c] = off[c + 1];
+    off[c + 1] += off[c];
+  }
+  {
+    std::vector<int> cur(off.begin(), off.end() - 1);
+    for (int i = 0; i < n; ++i) perm[cur[y_host[i] - 1]++] = i;
+  }
   double* M = ctx.arena.alloc_n<double>((size_t)C * kmax);
   double* Mw = ctx.arena.alloc_n<double>((size_t)C * kmax);
   double* counts = ctx.arena.alloc_n<double>(C);
-  int* bad = ctx.d_status + 4;
-  dzero(bad, sizeof(int));
-  class_sums_kernel<<<kmax, 256, C * sizeof(double), ctx.stream>>>(T, n, kmax, y, C, M, counts, bad); ::fpls::note_launch();
+  int* d_perm = ctx.arena.alloc_n<int>(n);
+  int* d_off = ctx.arena.alloc_n<int>(C + 1);
+  h2d(counts, hc.data(), C * sizeof(double));
+  h2d(d_perm, perm.data(), n * sizeof(int));
+  h2d(d_off, off.data(), (C + 1) * sizeof(int));
+  const long long warps = (long long)C * kmax;
+  class_sums_sorted_kernel<<<static_cast<unsigned>((warps + 7) / 8), 256, 0, ctx.stream>>>(T, n, kmax, d_perm,
+                                                                                        d_off, C, M);
+  ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
-  std::vector<double> hc(C);
-  int hbad = 0;
-  d2h(hc.data(), counts, C * sizeof(double));
-  d2h(&hbad, bad, sizeof(int));
-  ctx.sync();
-  if (hbad) throw Error(kErrArgument, "lda_train_prefix labels must be encoded as 1..n_classes");
-  for (int c = 0; c < C; ++c)
-    if (hc[c] <= 0.0) throw Error(kErrArgument, "lda_train_prefix received an empty class");
   means_from_sums_kernel<<<ceil_div(C * kmax, 256), 256, 0, ctx.stream>>>(M, C, kmax, counts, Mw); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   double* P = ctx.arena.alloc_n<double>((size_t)kmax * kmax);

@@ -27,8 +27,9 @@ struct LdaModelsDev {
 };
 
 // lda_train_prefix_cpp (src/fastPLS.cpp:1817-1927) on scores T (n x kmax, ld n)
-// with 1-based labels y.  Throws on an empty class or out-of-range label.
-void lda_train_prefix(const double* T, int n, int kmax, const int* y, int C,
+// with 1-based host labels y_host.  Throws on an empty class or out-of-range
+// label.  Class sums run in a fixed order (no atomics): runs repeat bit for bit.
+void lda_train_prefix(const double* T, int n, int kmax, const int* y_host, int C,
                       const int* ncomp_host, int L, double ridge, LdaModelsDev out);
 
 }  // namespace fpls

@@ -95,7 +95,7 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant
                   const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
                   const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2,
                   const int4* __restrict__ segs, const int* __restrict__ cta_seg_begin,
-                  int n_tiles_n, float* __restrict__ part, int* err) {
+                  int n_tiles_n, float* __restrict__ part, int* err, int withhold_loads) {
   using P = Planes<NP, TN>;
   constexpr int STAGES = P::STAGES;
   constexpr int STAGE_BYTES = P::STAGE_BYTES;
@@ -139,7 +139,9 @@ split_gemm_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant
   if (warp == 0 && lane == 0) {
     // ---------------------------------------------------------- producer
     int it = 0;
-    bool ok = true;
+    bool ok = !withhold_loads;  // test hook: no stage is ever filled, so the MMA
+                                // issuer's first wait runs out its budget while
+                                // no copy or MMA is in flight
     for (int sg = sbeg; sg < send && ok; ++sg) {
       const int4 seg = segs[sg];
       const int mt = seg.x / n_tiles_n, nt = seg.x % n_tiles_n;
@@ -599,8 +601,13 @@ template <int NP, int TN>
 void launch_split_kernel(const CUtensorMap (&m)[6], const GemmPlan& g, const GemmScratch& s, int* err,
                          cudaStream_t st) {
   ensure_smem_attr<NP, TN>();
+  // FASTPLS_TEST_WITHHOLD_LOADS=1 (tests of the timeout path only): the
+  // producer issues no load, the pipeline's bounded wait expires and the call
+  // returns FPLS_ERR_CUDA with the tensor memory released.
+  const char* w = std::getenv("FASTPLS_TEST_WITHHOLD_LOADS");
+  const int withhold = (w && w[0] == '1') ? 1 : 0;
   split_gemm_kernel<NP, TN><<<g.ctas, NUM_THREADS, Planes<NP, TN>::SMEM_BYTES, st>>>(
-      m[0], m[1], m[2], m[3], m[4], m[5], s.segs, s.cta_begin, g.ntn, s.part, err);
+      m[0], m[1], m[2], m[3], m[4], m[5], s.segs, s.cta_begin, g.ntn, s.part, err, withhold);
 }
 
 // C (M x N) = alpha * A B^T + beta C on stream `st` with the given scratch; no allocation.

@@ -205,3 +205,24 @@ def test_errors_are_status_codes(lib):
         lib.lda_train_prefix(np.ones((4, 2)), np.array([1, 1, 1, 1], dtype=np.int32), 2, [1])
     with pytest.raises(FastPLSError):
         lib.lda_train_prefix(np.ones((4, 2)), np.array([1, 2, 3, 1], dtype=np.int32), 2, [1])
+
+
+def test_fp64_runs_repeat_bit_for_bit(lib, c1, c2_small):
+    # Split-K partial sums and LDA class sums are added in a fixed order (no
+    # atomics), so the FP64 drop-in gives identical bits on every run.
+    X, Y = c1["Xtrain"], c1["Ytrain"]
+    a = lib.pls_model2_fast(X, Y, [3, 10], fit=True, seed=1)
+    b = lib.pls_model2_fast(X, Y, [3, 10], fit=True, seed=1)
+    assert np.array_equal(a["B"], b["B"]) and np.array_equal(a["Yfit"], b["Yfit"])
+    Xc = c2_small["Xtrain"].astype(np.float64)
+    y = c2_small["ytrain"]
+    m1 = lib.pls_model1(Xc, c2_small["Y"], [8], svd_method=4, power_iters=2, seed=1)
+    m2 = lib.pls_model1(Xc, c2_small["Y"], [8], svd_method=4, power_iters=2, seed=1)
+    assert np.array_equal(m1["B"], m2["B"])
+    Rp = m1["R"] / m1["vX"].T
+    off = (m1["mX"] @ Rp).ravel()
+    l1 = lib.lda_project_train_prefix(Xc, Rp, off, y, c2_small["n_classes"], [4, 8])
+    l2 = lib.lda_project_train_prefix(Xc, Rp, off, y, c2_small["n_classes"], [4, 8])
+    for kk in ("4", "8"):
+        assert np.array_equal(l1[kk]["linear"], l2[kk]["linear"])
+        assert np.array_equal(l1[kk]["constants"], l2[kk]["constants"])

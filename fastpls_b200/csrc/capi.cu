@@ -855,7 +855,8 @@ static CvX cv_x(const void* X, int x_is_float32, bool x_on_device, int n, int p)
 }
 
 static CvGridOptions cv_options(int scaling, int precision, int batched) {
-  FPLS_REQUIRE(precision == FPLS_PREC_FP64 || precision == FPLS_PREC_BF16X3, "unknown precision");
+  FPLS_REQUIRE(precision == FPLS_PREC_FP64 || precision == FPLS_PREC_BF16X3 || precision == FPLS_PREC_BF16X6,
+               "unknown precision");
   CvGridOptions opt;
   opt.scaling = scaling;
   opt.precision = precision;

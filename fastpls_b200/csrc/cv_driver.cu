@@ -279,7 +279,8 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
   // The mixed row-space loop needs only the BF16 planes of Xc, split straight
   // from the caller's matrix; every other combination works on a centred FP64
   // copy.  x0 is the first column of Xc (the Householder sign of the sketch).
-  const bool planes_only = opt.precision == 1 && dual;
+  const bool planes_only = opt.precision >= 1 && dual;
+  const int planes = opt.precision == 2 ? 3 : 2;  // BF16x6: hi, mid, lo planes
   // A host X goes up in overlapped column chunks on the mixed row-space path,
   // else in one copy first.
   if (x_host && !planes_only) {
@@ -304,7 +305,7 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
     const char* src = static_cast<const char*>(x_host);
     const std::vector<int> bounds = upload_chunks(p);
     const int nch = static_cast<int>(bounds.size()) - 1;
-    xop = make_split_operator_chunked(n, p);
+    xop = make_split_operator_chunked(n, p, planes);
     x0 = ar.alloc_n<double>(n);
     // the copies follow this call's earlier work on the main stream (an event
     // of their own: side_done marks the sketches, awaited later)
@@ -344,12 +345,12 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
     if (planes_only) {
       x0 = ar.alloc_n<double>(n);
       load_centered(x64, x32, n, 1, mall, x0);
-      xop = make_split_operator_centered(x64, x32, mall, n, p);
+      xop = make_split_operator_centered(x64, x32, mall, n, p, planes);
     } else {
       X = ar.alloc_n<double>((size_t)n * p);
       load_centered(x64, x32, n, p, mall, X);
       x0 = X;
-      if (opt.precision == 1) xop = make_split_operator(X, n, p, !dual);
+      if (opt.precision >= 1) xop = make_split_operator(X, n, p, !dual, planes);
       else xop.reset(new XOperatorF64(X, n, p));
     }
     FPLS_CUDA(cudaEventRecord(ctx.planes_ready, ctx.stream));
@@ -364,7 +365,7 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
   if (dual) {
     if (!gram_done) xop->gram(Kg);
     px->kop_f64.reset(new XOperatorF64(Kg, n, n));
-    if (opt.precision == 1 && int8_k_products()) {
+    if (opt.precision >= 1 && int8_k_products()) {
       px->kop_slices = ozaki_default_slices();
       px->kop_int8 = make_ozaki_sym_operator(Kg, n, px->kop_slices);
     }

@@ -29,7 +29,7 @@ struct CvFitSet {
 
 struct CvGridOptions {
   int scaling = 1;                  // 1 centre, 2 autoscale, 3 none
-  int precision = 0;                // 0 FP64, 1 BF16x3 split
+  int precision = 0;                // 0 FP64, 1 BF16x3 split, 2 BF16x6 split
   bool batched = true;              // false: one fit after another (plain drop-in path)
   int power_iters = 2;              // FASTPLS_FAST_INC_ITERS
   bool want_scores = false;         // also keep the class scores behind every prediction

@@ -254,8 +254,11 @@ int fpls_int8_emulated_gemm(const double* A, int M, int K, const double* B, int 
  * (simpls_fast).  X is n x p, FP64 (x_is_float32 = 0) or FP32 (= 1); y are
  * 1-based labels; fold holds 0-based fold ids (drawn by the caller, as the R
  * shim draws them with R's RNG); fit f uses seed + f.  All fold fits run in one
- * batched engine pass when batched = 1 (precision FPLS_PREC_FP64 or
- * FPLS_PREC_BF16X3), else one after another in FP64 (the plain drop-in path).
+ * batched engine pass when batched = 1 (precision FPLS_PREC_FP64,
+ * FPLS_PREC_BF16X3 or FPLS_PREC_BF16X6: the mixed forms build the row Gram
+ * from two BF16 planes and three products, or three planes and six, and keep
+ * the per-component products FP64-accurate on the INT8 tensor cores), else one
+ * after another in FP64 (the plain drop-in path).
  * class_pred n x L (1-based; 0 where not predicted), status kfold (1 ok,
  * 2 empty fold, 3 no training rows, 4 single-class training fold).
  * Replaces _fastPLS_pls_cv_predict_compiled (RcppExports.cpp:731;

@@ -273,3 +273,18 @@ def test_ncomp_list_order_and_repeats(lib, c4_small, precision):
     for s, c in enumerate(mixed):
         t = int(np.where(base == c)[0][0])
         assert np.array_equal(np.asarray(pa["class_pred"])[:, s], np.asarray(pb["class_pred"])[:, t])
+
+
+def test_double_cv_bf16x6_close_to_fp64(lib, c4_small):
+    # three BF16 planes and six products in the row Gram: the mixed grid's
+    # scores sit closer to FP64 than the two-plane form's
+    d = c4_small
+    outer, inner = double_cv_folds(d["y"], d["groups"], 4, 3, seed=5)
+    nc = np.arange(1, 9)
+    kw = dict(seed=1, return_scores=True)
+    a = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], precision="fp64", **kw)
+    b = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], precision="bf16x6", **kw)
+    c = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], precision="bf16x3", **kw)
+    _check_double_cv(b, _as_ref(a), margin=MIXED_TOL, score_tol=MIXED_TOL)
+    assert slice_score_rel_err(b["inner_score"], a["inner_score"]) < \
+        slice_score_rel_err(c["inner_score"], a["inner_score"])

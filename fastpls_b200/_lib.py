@@ -74,6 +74,9 @@ SIGNATURES = {
                                 _I, _IP, _IP, _DP, _C, _S], ctypes.c_int),
     "fpls_double_cv_scores": ([ctypes.c_void_p, _I, _I, _I, _IP, _I, _IP, _I, _IP, _I, _IP, _I, _I, _I,
                                _I, _I, _I, _IP, _DP, _IP, _IP, _IP, _DP, _DP, _C, _S], ctypes.c_int),
+    "fpls_pls_lda": ([ctypes.c_void_p, _I, _I, _I, _DP, _I, _IP, ctypes.c_void_p, _I, _IP, _I, _I, _I, _I, _I, _I,
+                      _I, _I, _D, _I, _D, _IP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _IP, _DP, _DP, _DP,
+                      _DP, _DP, _DP, _DP, _IP, _C, _S], ctypes.c_int),
     "fpls_bf16x3_gemm_noalloc": ([ctypes.c_void_p, _I, _I, ctypes.c_void_p, _I, ctypes.c_void_p,
                                   _C, _S], ctypes.c_int),
     "fpls_gaussian_y_encode": ([_DP, _I, _I, _DP, _I, _DP, _DP, _DP, _C, _S], ctypes.c_int),
@@ -639,6 +642,51 @@ def double_cv(X, y, outer_fold, inner_fold, ncomp, n_classes, scaling=1, seed=1,
     else:
         _call("fpls_double_cv_outer_subset", *head, _p(ids), ids.size, *tail)
     return _double_cv_result(o, yy, ids, of)
+
+
+def pls_lda(Xtrain, Ytrain, y, Xtest, ncomp, n_classes, method=1, scaling=1, xprod=False, fit=False,
+            oversample=10, power_iters=1, svds_tol=0.0, seed=1, lda_ridge=1e-8, store_B=True):
+    """Fused PLS + LDA (fpls_pls_lda): fit, one LDA per distinct ncomp, test labels.
+    Xtrain / Xtest: FP64 or FP32 (the same type for both)."""
+    f32 = np.asarray(Xtrain).dtype == np.float32
+    dt = np.float32 if f32 else np.float64
+    Xa = np.asfortranarray(Xtrain, dtype=dt)
+    n, p = Xa.shape
+    Xt = np.asfortranarray(np.zeros((0, p)) if Xtest is None else Xtest, dtype=dt)
+    Y = _f64(Ytrain)
+    m = Y.shape[1]
+    yy = _i32(y)
+    nc = _i32(np.maximum(np.atleast_1d(ncomp), 1))
+    L = nc.size
+    C = int(n_classes)
+    K0 = int(nc.max()) if method == 3 else min(int(nc.max()), min(n, p, m))
+    ntest = Xt.shape[0]
+    o = dict(ncomp=np.zeros(L, dtype=np.int32), R=_out(p, K0), Q=_out(m, K0), mX=_out(1, p), vX=_out(1, p),
+             mY=_out(1, m), B=_out(p, m, L) if store_B else None, Yfit=_out(n, m, L) if fit else None,
+             R2Y=np.zeros(L), unique_ncomp=np.zeros(L, dtype=np.int32), lda_means=_out(C, K0, L),
+             lda_linear=_out(C, K0, L), lda_constants=_out(C, L), lda_priors=np.zeros(C), lda_lambda=np.zeros(L),
+             R_predict=_out(p, K0), R_offset=np.zeros(K0),
+             pred_codes=np.zeros((max(ntest, 1), L), dtype=np.int32, order="F"))
+    U = ctypes.c_int(0)
+    _call("fpls_pls_lda", Xa.ctypes.data, int(f32), n, p, _p(Y), m, _p(yy),
+          Xt.ctypes.data if ntest else None, ntest, _p(nc), L, C, int(method), int(scaling), int(bool(xprod)),
+          int(bool(fit)), int(oversample), int(power_iters), float(svds_tol), int(seed), float(lda_ridge),
+          _p(o["ncomp"]), _p(o["R"]), _p(o["Q"]), _p(o["mX"]), _p(o["vX"]), _p(o["mY"]), _p(o["B"]),
+          _p(o["Yfit"]), _p(o["R2Y"]), ctypes.byref(U), _p(o["unique_ncomp"]), _p(o["lda_means"]),
+          _p(o["lda_linear"]), _p(o["lda_constants"]), _p(o["lda_priors"]), _p(o["lda_lambda"]),
+          _p(o["R_predict"]), _p(o["R_offset"]), _p(o["pred_codes"]) if ntest else None)
+    u = U.value
+    o["unique_ncomp"] = o["unique_ncomp"][:u]
+    for k in ("lda_means", "lda_linear"):
+        o[k] = o[k][:, :, :u]
+    o["lda_constants"] = o["lda_constants"][:, :u]
+    o["lda_lambda"] = o["lda_lambda"][:u]
+    if not ntest:
+        o.pop("pred_codes")
+    if not store_B:
+        o.pop("B")
+    o.update(p=p, m=m, method=int(method))
+    return o
 
 
 def x_upload(X):

@@ -748,6 +748,196 @@ int fpls_lda_predict(const double* T, int w, int k, const double* linear,
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+// LDA scores of raw rows X (w x p, device) through the projection R (p x k, ld
+// ldr) and offset: S = (X R - offset) linear^T + constants, by the direct or
+// the latent route as lda_project_predict_labels_cpp chooses
+// (fastPLS.cpp:2100-2147, CPU rule with the 0.5 factor); labels (device, w) and,
+// when scores is set, the full score matrix (device, w x C).  dc is modified.
+void lda_project_scores_device(const double* dX, int w, int p, const double* dR, int ldr, int k,
+                               const double* doff, const double* dL, int ldl, double* dc, int C, int* dlab,
+                               double* dS_out) {
+  Context& ctx = Context::get();
+  double* dS = dS_out ? dS_out : ctx.arena.alloc_n<double>((size_t)w * C);
+  // constants_adj = constants - offset linear^T
+  if (doff) gemv(false, C, k, -1.0, dL, ldl, doff, 1.0, dc);
+  const double nn = w, pp = p, kk = k, cc = C;
+  const double latent_ops = nn * kk * (pp + cc);
+  const double direct_ops = nn * pp * cc;
+  if (direct_ops < 0.5 * latent_ops) {
+    double* dW = ctx.arena.alloc_n<double>((size_t)p * C);
+    gemm(false, true, p, C, k, 1.0, dR, ldr, dL, ldl, 0.0, dW, p);
+    xgemm(false, w, C, p, dX, w, dW, p, dS, w);
+  } else {
+    double* dT = ctx.arena.alloc_n<double>((size_t)w * k);
+    gemm(false, false, w, k, p, 1.0, dX, w, dR, ldr, 0.0, dT, w);
+    gemm(false, true, w, C, k, 1.0, dT, w, dL, ldl, 0.0, dS, w);
+  }
+  row_argmax(dS, w, C, dc, dlab);
+  if (dS_out) add_row_vector(dS, w, C, w, dc);
+}
+
+__global__ void widen_f32_kernel(const float* __restrict__ src, size_t total, double* __restrict__ dst) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x)
+    dst[t] = static_cast<double>(src[t]);
+}
+
+// A caller's matrix (FP64, or FP32 widened exactly) as a fresh FP64 device copy.
+double* upload_widened(const void* X, bool f32, size_t count) {
+  Context& ctx = Context::get();
+  if (!f32) return upload(static_cast<const double*>(X), count);
+  const float* d32 = upload(static_cast<const float*>(X), count);
+  double* d = ctx.arena.alloc_n<double>(count ? count : 1);
+  if (count) {
+    widen_f32_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(d32, count, d);
+    ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+  }
+  return d;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const double* Ytrain, int m,
+                 const int* y, const void* Xtest, int ntest, const int* ncomp, int L, int n_classes,
+                 int method, int scaling, int xprod, int fit, int oversample, int power_iters,
+                 double svds_tol, int seed, double lda_ridge, int* ncomp_out, double* R, double* Q,
+                 double* mX, double* vX, double* mY, double* B, double* Yfit, double* R2Y, int* n_unique,
+                 int* unique_ncomp, double* lda_means, double* lda_linear, double* lda_constants,
+                 double* lda_priors, double* lda_lambda, double* R_predict, double* R_offset,
+                 int* pred_codes, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && m > 0 && Xtrain && Ytrain && y,
+                 "pls_lda requires compatible non-empty Xtrain and Ytrain");
+    FPLS_REQUIRE(n_classes >= 2, "pls_lda requires at least two classes");
+    FPLS_REQUIRE(L >= 1 && ncomp, "pls_lda requires at least one component count");
+    FPLS_REQUIRE(method == 1 || method == 3, "pls_lda supports method 1 (plssvd) or 3 (simpls)");
+    FPLS_REQUIRE(ntest == 0 || (Xtest && pred_codes), "pls_lda: Xtest rows need pred_codes");
+    FPLS_REQUIRE(!(fit && !Yfit), "fit = 1 requires a Yfit buffer");
+    const bool f32 = x_is_float32 != 0;
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    std::vector<int> nc(ncomp, ncomp + L);
+    for (int& c : nc) c = std::max(1, c);
+    // one upload of each matrix for the whole pipeline
+    double* dX = upload_widened(Xtrain, f32, (size_t)n * p);
+    double* dY = upload(Ytrain, (size_t)n * m);
+    int K0 = 0;
+    double* dR = nullptr;
+    double* dT = nullptr;   // training scores (X - mX) / vX R, n x K0
+    std::vector<double> hR, hmX(p), hvX(p);
+    if (method == 1) {
+      const int max_rank = std::min(n, std::min(p, m));
+      for (int& c : nc) c = std::min(c, max_rank);
+      K0 = std::min(max_of(nc.data(), L), max_rank);
+      double* dmX = ctx.arena.alloc_n<double>(p);
+      double* dvX = ctx.arena.alloc_n<double>(p);
+      double* dmY = ctx.arena.alloc_n<double>(m);
+      center_scale_xy(dX, n, p, dY, m, scaling, dmX, dvX, dmY);
+      FitOptions opt;
+      opt.scaling = scaling;
+      opt.fit = fit != 0;
+      opt.svd_method = kSvdCpuRsvd;
+      opt.oversample = std::max(oversample, 0);
+      opt.power_iters = std::max(power_iters, 0);
+      opt.svds_tol = std::max(svds_tol, 0.0);
+      opt.seed = static_cast<unsigned int>(seed);
+      opt.xprod = xprod != 0;
+      PlssvdOut o;
+      o.C_latent = ctx.arena.alloc_n<double>((size_t)K0 * K0 * L);
+      o.W_latent = ctx.arena.alloc_n<double>((size_t)K0 * m * L);
+      o.R = dR = ctx.arena.alloc_n<double>((size_t)p * K0);
+      o.Q = ctx.arena.alloc_n<double>((size_t)m * K0);
+      o.T = dT = ctx.arena.alloc_n<double>((size_t)n * K0);
+      o.s = ctx.arena.alloc_n<double>(K0);
+      o.B = B ? ctx.arena.alloc_n<double>((size_t)p * m * L) : nullptr;
+      o.Yfit = fit ? ctx.arena.alloc_n<double>((size_t)n * m * L) : nullptr;
+      std::vector<double> r2(L, 0.0);
+      o.R2Y = r2.data();
+      plssvd_fit_centered(dX, n, p, dY, m, nc.data(), L, K0, opt, dmY, o);
+      download(Q, o.Q, (size_t)m * K0);
+      download(mY, dmY, m);
+      if (B) download(B, o.B, (size_t)p * m * L);
+      if (fit) download(Yfit, o.Yfit, (size_t)n * m * L);
+      hR.resize((size_t)p * K0);
+      download(hR.data(), dR, (size_t)p * K0);
+      download(hmX.data(), dmX, p);
+      download(hvX.data(), dvX, p);
+      ctx.sync();
+      if (R2Y) std::copy(r2.begin(), r2.end(), R2Y);
+    } else {
+      K0 = max_of(nc.data(), L);
+      hR.resize((size_t)p * K0);
+      std::vector<double> hQ((size_t)m * K0), hmY(m);
+      int done = 0;
+      // centres / scales dX in place (the fit's own copy) and fits on it
+      simpls_fast_on_device(dX, n, p, dY, m, nc.data(), L, scaling, fit, seed, hR.data(), hQ.data(), hmX.data(),
+                            hvX.data(), hmY.data(), B, Yfit, R2Y, &done);
+      if (done < K0) throw Error(FPLS_ERR_NUMERICAL, "pls_lda has invalid effective component count");
+      if (Q) std::copy(hQ.begin(), hQ.end(), Q);
+      if (mY) std::copy(hmY.begin(), hmY.end(), mY);
+      dR = upload(hR.data(), (size_t)p * K0);
+      dT = ctx.arena.alloc_n<double>((size_t)n * K0);
+      xgemm(false, n, K0, p, dX, n, dR, p, dT, n);
+    }
+    if (R) std::copy(hR.begin(), hR.end(), R);
+    if (mX) std::copy(hmX.begin(), hmX.end(), mX);
+    if (vX) std::copy(hvX.begin(), hvX.end(), vX);
+    if (ncomp_out) std::copy(nc.begin(), nc.end(), ncomp_out);
+    // R_predict = R / vX (rows; a zero or non-finite scale counts as 1) and
+    // offset = mX R_predict (fastPLS.cpp:6321-6335)
+    std::vector<double> hRp((size_t)p * K0), hoff(K0, 0.0);
+    for (int a = 0; a < K0; ++a)
+      for (int j = 0; j < p; ++j) {
+        double sc = hvX[j];
+        if (!std::isfinite(sc) || sc == 0.0) sc = 1.0;
+        const double v = hR[j + (size_t)a * p] / sc;
+        hRp[j + (size_t)a * p] = v;
+        hoff[a] += hmX[j] * v;
+      }
+    if (R_predict) std::copy(hRp.begin(), hRp.end(), R_predict);
+    if (R_offset) std::copy(hoff.begin(), hoff.end(), R_offset);
+    // LDA on the fit's training scores, one model per distinct ncomp in
+    // increasing order (arma::unique)
+    std::vector<int> uq(nc);
+    std::sort(uq.begin(), uq.end());
+    uq.erase(std::unique(uq.begin(), uq.end()), uq.end());
+    const int U = static_cast<int>(uq.size());
+    LdaModelsDev d;
+    d.means = ctx.arena.alloc_n<double>((size_t)n_classes * K0 * U);
+    d.linear = ctx.arena.alloc_n<double>((size_t)n_classes * K0 * U);
+    d.constants = ctx.arena.alloc_n<double>((size_t)n_classes * U);
+    d.priors = ctx.arena.alloc_n<double>(n_classes);
+    std::vector<double> lam(U);
+    d.lambda = lam.data();
+    lda_train_prefix(dT, n, K0, y, n_classes, uq.data(), U, lda_ridge, d);
+    lda_outputs_to_host(d, n_classes, K0, U, lda_means, lda_linear, lda_constants, lda_priors);
+    if (ntest > 0) {
+      const double* dXt = upload_widened(Xtest, f32, (size_t)ntest * p);
+      const double* dRp = upload(hRp.data(), (size_t)p * K0);
+      const double* doff = upload(hoff.data(), K0);
+      int* dpred = ctx.arena.alloc_n<int>((size_t)ntest * L);
+      double* dc = ctx.arena.alloc_n<double>(n_classes);
+      for (int i = 0; i < L; ++i) {
+        const int u = static_cast<int>(std::lower_bound(uq.begin(), uq.end(), nc[i]) - uq.begin());
+        d2d(dc, d.constants + (size_t)u * n_classes, n_classes * sizeof(double));
+        lda_project_scores_device(dXt, ntest, p, dRp, p, nc[i], doff, d.linear + (size_t)u * n_classes * K0,
+                                  n_classes, dc, n_classes, dpred + (size_t)i * ntest, nullptr);
+      }
+      download(pred_codes, dpred, (size_t)ntest * L);
+    }
+    ctx.sync();
+    if (lda_lambda) std::copy(lam.begin(), lam.end(), lda_lambda);
+    if (n_unique) *n_unique = U;
+    if (unique_ncomp) std::copy(uq.begin(), uq.end(), unique_ncomp);
+  });
+}
+
 int fpls_lda_project_predict(const double* X, int w, int p, const double* R, int k,
                              const double* offset, const double* linear,
                              const double* constants, int n_classes, int* labels,
@@ -761,31 +951,12 @@ int fpls_lda_project_predict(const double* X, int w, int p, const double* R, int
     const double* dR = upload(R, (size_t)p * k);
     const double* dL = upload(linear, (size_t)n_classes * k);
     double* dc = upload(constants, n_classes);
-    double* dS = ctx.arena.alloc_n<double>((size_t)w * n_classes);
-    // constants_adj = constants - offset linear^T
-    if (offset) {
-      const double* doff = upload(offset, k);
-      gemv(false, n_classes, k, -1.0, dL, n_classes, doff, 1.0, dc);
-    }
-    const double nn = w, pp = p, kk = k, cc = n_classes;
-    const double latent_ops = nn * kk * (pp + cc);
-    const double direct_ops = nn * pp * cc;
-    if (direct_ops < 0.5 * latent_ops) {
-      double* dW = ctx.arena.alloc_n<double>((size_t)p * n_classes);
-      gemm(false, true, p, n_classes, k, 1.0, dR, p, dL, n_classes, 0.0, dW, p);
-      xgemm(false, w, n_classes, p, dX, w, dW, p, dS, w);
-    } else {
-      double* dT = ctx.arena.alloc_n<double>((size_t)w * k);
-      gemm(false, false, w, k, p, 1.0, dX, w, dR, p, 0.0, dT, w);
-      gemm(false, true, w, n_classes, k, 1.0, dT, w, dL, n_classes, 0.0, dS, w);
-    }
+    const double* doff = offset ? upload(offset, k) : nullptr;
+    double* dS = scores ? ctx.arena.alloc_n<double>((size_t)w * n_classes) : nullptr;
     int* dlab = ctx.arena.alloc_n<int>(w);
-    row_argmax(dS, w, n_classes, dc, dlab);
+    lda_project_scores_device(dX, w, p, dR, p, k, doff, dL, n_classes, dc, n_classes, dlab, dS);
     download(labels, dlab, w);
-    if (scores) {
-      add_row_vector(dS, w, n_classes, w, dc);
-      download(scores, dS, (size_t)w * n_classes);
-    }
+    if (scores) download(scores, dS, (size_t)w * n_classes);
     ctx.sync();
   });
 }

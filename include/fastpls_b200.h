@@ -278,6 +278,31 @@ int fpls_cv_predict_scores(const void* X, int x_is_float32, int n, int p, const 
                            int seed, int precision, int batched, int* class_pred, int* status,
                            double* class_score, char* err, size_t errlen);
 
+/* Fused PLS + LDA classifier: one call fits PLSSVD (method 1: seeded rSVD,
+ * or the matrix-free operator with xprod = 1) or fast SIMPLS (method 3) on
+ * Xtrain (n x p; FP64, or FP32 with x_is_float32 = 1, the same for Xtest) and
+ * the response Ytrain (n x m, FP64; the one-hot of y for PLS-DA), trains one
+ * LDA model per distinct ncomp on the fit's own training scores
+ * (X - mX) / vX R, and predicts the ntest rows of Xtest with each ncomp slice.
+ * X crosses to the device once.  Outputs (NULL to skip): ncomp_out (L, capped
+ * at min(n, p, m) for PLSSVD), R (p x K0), Q (m x K0), mX, vX (p), mY (m), B
+ * (p x m x L), Yfit (n x m x L, fit = 1), R2Y (L); n_unique = U and
+ * unique_ncomp (U, increasing); lda_means and lda_linear (n_classes x K0 x U,
+ * slice u filled in its first unique_ncomp[u] columns), lda_constants
+ * (n_classes x U), lda_priors (n_classes), lda_lambda (U); R_predict (p x K0,
+ * R with rows divided by vX) and R_offset (K0, mX R_predict); pred_codes
+ * (ntest x L, 1-based, required when ntest > 0).  K0 = max(ncomp_out).
+ * Replaces _fastPLS_pls_lda_gpu_native (RcppExports.cpp:706;
+ * fastPLS.cpp:6182-6443). */
+int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const double* Ytrain, int m,
+                 const int* y, const void* Xtest, int ntest, const int* ncomp, int L, int n_classes,
+                 int method, int scaling, int xprod, int fit, int oversample, int power_iters,
+                 double svds_tol, int seed, double lda_ridge, int* ncomp_out, double* R, double* Q,
+                 double* mX, double* vX, double* mY, double* B, double* Yfit, double* R2Y, int* n_unique,
+                 int* unique_ncomp, double* lda_means, double* lda_linear, double* lda_constants,
+                 double* lda_priors, double* lda_lambda, double* R_predict, double* R_offset,
+                 int* pred_codes, char* err, size_t errlen);
+
 /* Double cross-validation of SIMPLS PLS-DA (argmax classifier): for every outer
  * fold o, an inner CV over its training rows picks ncomp (first maximum of the
  * inner accuracy), then a refit on the outer training rows predicts fold o.

@@ -77,6 +77,8 @@ SIGNATURES = {
     "fpls_pls_lda": ([ctypes.c_void_p, _I, _I, _I, _DP, _I, _IP, ctypes.c_void_p, _I, _IP, _I, _I, _I, _I, _I, _I,
                       _I, _I, _D, _I, _D, _IP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _IP, _DP, _DP, _DP,
                       _DP, _DP, _DP, _DP, _IP, _C, _S], ctypes.c_int),
+    "fpls_set_autotune": ([_I, _C, _S], ctypes.c_int),
+    "fpls_autotune_report": ([ctypes.c_char_p, _S, ctypes.POINTER(ctypes.c_size_t), _C, _S], ctypes.c_int),
     "fpls_bf16x3_gemm_noalloc": ([ctypes.c_void_p, _I, _I, ctypes.c_void_p, _I, ctypes.c_void_p,
                                   _C, _S], ctypes.c_int),
     "fpls_gaussian_y_encode": ([_DP, _I, _I, _DP, _I, _DP, _DP, _DP, _C, _S], ctypes.c_int),
@@ -687,6 +689,21 @@ def pls_lda(Xtrain, Ytrain, y, Xtest, ncomp, n_classes, method=1, scaling=1, xpr
         o.pop("B")
     o.update(p=p, m=m, method=int(method))
     return o
+
+
+def set_autotune(on=True):
+    """Autotuning of the batched double-CV grids (fpls_set_autotune)."""
+    _call("fpls_set_autotune", int(bool(on)))
+
+
+def autotune_report():
+    """The tuned grid shapes: list of dicts (shape, chosen configuration, candidates)."""
+    import json
+    need = ctypes.c_size_t(0)
+    _call("fpls_autotune_report", None, 0, ctypes.byref(need))
+    buf = ctypes.create_string_buffer(max(int(need.value), 1))
+    _call("fpls_autotune_report", buf, ctypes.sizeof(buf), ctypes.byref(need))
+    return [json.loads(line) for line in buf.value.decode().splitlines() if line.strip()]
 
 
 def x_upload(X):

@@ -5,8 +5,11 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <sstream>
 #include <vector>
 
+#include "autotune.cuh"
+#include "dual_engine.cuh"
 #include "gaussian.cuh"
 #include "blas_f64.cuh"
 #include "capi_util.cuh"
@@ -1322,15 +1325,120 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
     }
 }
 
+}  // extern "C"
+
+namespace {
+
+// One double CV with the tuned configuration of its shape in force.  When
+// autotuning is on and the shape (device, n, p, fits, ncomp slices, largest
+// ncomp, classes, precision, scaling) has not been tuned, the candidates are
+// timed first on this call's own inputs: every candidate runs the whole grid
+// once to warm up and twice timed (the faster counts), and only candidates
+// whose chosen ncomp, outer predictions and inner accuracies equal the
+// default configuration's are eligible.  Only the batched row-space path has
+// knobs; other grids run as they are.
+template <typename Run>
+void run_double_cv_tuned(int n, int p, int n_classes, int kfold_outer, int kfold_inner, const int* ncomp, int L,
+                         int scaling, int precision, int batched, Run run) {
+  Context& ctx = Context::get();
+  const int K = std::max(1, max_of(ncomp, L));
+  const bool eligible = batched && scaling != 2 && p > 5 && dual_engine_applies(n, p, n_classes, K);
+  TuneKey key{ctx.device, n, p, kfold_outer * (kfold_inner + 1), L, K, n_classes, precision, scaling};
+  if (eligible && autotune_enabled() && !tuned_lookup(key)) {
+    struct Out {
+      std::vector<int> best, pred;
+      std::vector<double> acc;
+      double ms = 0.0;
+    };
+    auto measure = [&](const TuneConfig& c, Out& o) {
+      TuneScope scope(c);
+      o.best.assign(kfold_outer, 0);
+      o.pred.assign(n, 0);
+      o.acc.assign((size_t)kfold_outer * L, 0.0);
+      double best_ms = 1e300;
+      for (int r = 0; r < 3; ++r) {
+        run(o.best.data(), o.acc.data(), o.pred.data());
+        ctx.end_call();
+        if (r > 0) best_ms = std::min(best_ms, ctx.last_call_ms);
+      }
+      o.ms = best_ms;
+    };
+    std::vector<TuneConfig> cands;
+    const std::vector<int> tiles = precision == 1 ? std::vector<int>{128, 64} : std::vector<int>{0};
+    const std::vector<int> layouts = n <= 4096 ? std::vector<int>{0, 1} : std::vector<int>{1};
+    const std::vector<int> merges = n_classes <= 6 ? std::vector<int>{1, 0} : std::vector<int>{1};
+    const std::vector<int> slices = precision >= 1 ? std::vector<int>{5, 4, 6} : std::vector<int>{0};
+    for (int t : tiles)
+      for (int l : layouts)
+        for (int mg : merges)
+          for (int sl : slices) {
+            TuneConfig c;
+            c.gram_tile = t;
+            c.step_layout = l;
+            c.merge = mg;
+            c.ozaki_slices = sl;
+            cands.push_back(c);
+          }
+    Out ref;
+    measure(cands[0], ref);   // the default configuration, the reference of the equality gate
+    TuneConfig chosen = cands[0];
+    double chosen_ms = ref.ms;
+    std::ostringstream rep;
+    rep << "[{\"config\": " << cands[0].str() << ", \"ms\": " << ref.ms << ", \"same_results\": true}";
+    for (size_t i = 1; i < cands.size(); ++i) {
+      Out o;
+      measure(cands[i], o);
+      const bool same = o.best == ref.best && o.pred == ref.pred && o.acc == ref.acc;
+      rep << ", {\"config\": " << cands[i].str() << ", \"ms\": " << o.ms << ", \"same_results\": "
+          << (same ? "true" : "false") << "}";
+      if (same && o.ms < chosen_ms) {
+        chosen = cands[i];
+        chosen_ms = o.ms;
+      }
+    }
+    rep << "]";
+    tuned_store(key, chosen, rep.str());
+  }
+  const TuneConfig* t = autotune_enabled() ? tuned_lookup(key) : nullptr;
+  TuneScope scope(t ? *t : TuneConfig{});
+  run(nullptr, nullptr, nullptr);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fpls_set_autotune(int on, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] { set_autotune(on != 0); });
+}
+
+int fpls_autotune_report(char* buf, size_t len, size_t* needed, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    const std::string r = tune_report();
+    if (needed) *needed = r.size() + 1;
+    if (buf && len) {
+      const size_t k = std::min(len - 1, r.size());
+      std::memcpy(buf, r.data(), k);
+      buf[k] = '\0';
+    }
+  });
+}
+
 int fpls_double_cv(const void* X, int x_is_float32, int n, int p, const int* y, int n_classes,
                    const int* outer_fold, int kfold_outer, const int* inner_fold, int kfold_inner,
                    const int* ncomp, int L, int scaling, int seed, int run, int precision,
                    int batched, int* best_comp, double* inner_accuracy, int* outer_pred,
                    int* inner_pred, int* fit_status, char* err, size_t errlen) {
   return guarded(err, errlen, [&] {
-    double_cv_impl(X, x_is_float32, false, n, p, y, n_classes, outer_fold, kfold_outer, inner_fold,
-                   kfold_inner, nullptr, 0, ncomp, L, scaling, seed, run, precision, batched, best_comp,
-                   inner_accuracy, outer_pred, inner_pred, fit_status);
+    run_double_cv_tuned(n, p, n_classes, kfold_outer, kfold_inner, ncomp, L, scaling, precision, batched,
+                        [&](int* tb, double* ta, int* tp) {
+                          const bool probe = tb != nullptr;
+                          double_cv_impl(X, x_is_float32, false, n, p, y, n_classes, outer_fold, kfold_outer,
+                                         inner_fold, kfold_inner, nullptr, 0, ncomp, L, scaling, seed, run,
+                                         precision, batched, probe ? tb : best_comp, probe ? ta : inner_accuracy,
+                                         probe ? tp : outer_pred, probe ? nullptr : inner_pred,
+                                         probe ? nullptr : fit_status);
+                        });
   });
 }
 
@@ -1342,6 +1450,12 @@ int fpls_double_cv_scores(const void* X, int x_is_float32, int n, int p, const i
                           char* err, size_t errlen) {
   return guarded(err, errlen, [&] {
     FPLS_REQUIRE(inner_score || outer_score, "double_cv_scores: no score output requested");
+    // the configuration tuned for this shape, if any (no tuning from here)
+    Context& ctx = Context::get();
+    const TuneKey key{ctx.device, n, p, kfold_outer * (kfold_inner + 1), L, std::max(1, max_of(ncomp, L)),
+                      n_classes, precision, scaling};
+    const TuneConfig* t = autotune_enabled() ? tuned_lookup(key) : nullptr;
+    TuneScope scope(t ? *t : TuneConfig{});
     double_cv_impl(X, x_is_float32, false, n, p, y, n_classes, outer_fold, kfold_outer, inner_fold,
                    kfold_inner, nullptr, 0, ncomp, L, scaling, seed, run, precision, batched, best_comp,
                    inner_accuracy, outer_pred, inner_pred, fit_status, inner_score, outer_score);
@@ -1433,9 +1547,15 @@ int fpls_double_cv_resident(int handle, const int* y, int n_classes, const int* 
     FPLS_REQUIRE(handle >= 0 && handle < static_cast<int>(ctx.resident.size()) &&
                      ctx.resident[handle].ptr, "double_cv_resident: unknown handle");
     const ResidentX r = ctx.resident[handle];
-    double_cv_impl(r.ptr, r.f32 ? 1 : 0, true, r.n, r.p, y, n_classes, outer_fold, kfold_outer,
-                   inner_fold, kfold_inner, nullptr, 0, ncomp, L, scaling, seed, run, precision, batched,
-                   best_comp, inner_accuracy, outer_pred, inner_pred, fit_status);
+    run_double_cv_tuned(r.n, r.p, n_classes, kfold_outer, kfold_inner, ncomp, L, scaling, precision, batched,
+                        [&](int* tb, double* ta, int* tp) {
+                          const bool probe = tb != nullptr;
+                          double_cv_impl(r.ptr, r.f32 ? 1 : 0, true, r.n, r.p, y, n_classes, outer_fold,
+                                         kfold_outer, inner_fold, kfold_inner, nullptr, 0, ncomp, L, scaling, seed,
+                                         run, precision, batched, probe ? tb : best_comp,
+                                         probe ? ta : inner_accuracy, probe ? tp : outer_pred,
+                                         probe ? nullptr : inner_pred, probe ? nullptr : fit_status);
+                        });
   });
 }
 

@@ -5,6 +5,7 @@
 #include <cstdlib>
 #include <string>
 
+#include "autotune.cuh"
 #include "blas_f64.cuh"
 #include "context.cuh"
 #include "ozaki_gemm.cuh"
@@ -831,9 +832,11 @@ void launch_step_cfg(const DualEng& e, int a, int F, cudaStream_t st) {
 enum StepLayout { kStepWide = 0, kStepDeep = 1 };
 
 int choose_step_layout(int n) {
+  const bool wide_fits = n <= 4 * 512 * 2;
   if (const char* v = std::getenv("FASTPLS_DUAL_STEP"))
     if (std::string(v) == "deep") return kStepDeep;
-  return n <= 4 * 512 * 2 ? kStepWide : kStepDeep;
+  if (active_tune().step_layout == 1) return kStepDeep;
+  return wide_fits ? kStepWide : kStepDeep;
 }
 
 void launch_step(int layout, const DualEng& e, int a, int F, cudaStream_t st) {
@@ -852,8 +855,8 @@ void launch_step(int layout, const DualEng& e, int a, int F, cudaStream_t st) {
 // FASTPLS_DUAL_MERGE=0 runs the refresh of every component in its own
 // reductions (the unmerged launch) instead.
 static bool dual_merge_enabled() {
-  const char* v = std::getenv("FASTPLS_DUAL_MERGE");
-  return !(v && v[0] == '0');
+  if (const char* v = std::getenv("FASTPLS_DUAL_MERGE")) return v[0] != '0';
+  return active_tune().merge != 0;
 }
 
 bool dual_engine_applies(int n, int p, int m, int K) {

@@ -38,6 +38,7 @@
 // Every mbarrier wait is bounded (error flag, no endless spin); the copies and
 // MMAs in flight are drained before the CTA releases TMEM and exits.  No
 // cluster multicast is used.
+#include "autotune.cuh"
 #include "ozaki_gemm.cuh"
 
 #include <cuda.h>
@@ -674,6 +675,8 @@ int ozaki_default_slices() {
     const int v = std::atoi(e);
     if (v >= kOzakiMinSlices && v <= kOzakiMaxSlices) return v;
   }
+  const int t = active_tune().ozaki_slices;
+  if (t >= kOzakiMinSlices && t <= kOzakiMaxSlices) return t;
   // 2^-35 of the row scales, about four orders of magnitude below the error
   // the BF16x3 row Gram already carries: on the omics double-CV grid 5, 6 and 7
   // slices give the same predictions as FP64 products (5 and 6 the same to the

@@ -31,6 +31,7 @@
 #include <string>
 #include <cstdlib>
 
+#include "autotune.cuh"
 #include "blas_f64.cuh"
 #include "context.cuh"
 #include "tc_util.cuh"
@@ -691,8 +692,8 @@ const CachedPlan& cached_plan(int M, int N, int K, int sm_count, cudaStream_t st
 }
 
 bool sym_wide_tiles() {
-  const char* e = std::getenv("FASTPLS_GRAM_TILE");
-  return !(e && std::string(e) == "64");
+  if (const char* e = std::getenv("FASTPLS_GRAM_TILE")) return std::string(e) != "64";
+  return active_tune().gram_tile != 64;
 }
 
 void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, double alpha,

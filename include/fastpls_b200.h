@@ -492,6 +492,27 @@ int fpls_candidate_knn_predict(const double* Ttest_norm, int ntest, const double
 int fpls_bf16x3_gemm_noalloc(const double* A, int M, int K, const double* B, int N, double* C,
                              char* err, size_t errlen);
 
+/* Autotuning of the batched double-CV grids (off by default).  With on = 1,
+ * the first fpls_double_cv / fpls_double_cv_resident call of a grid shape
+ * (device, n, p, fit count, ncomp slices, largest ncomp, classes, precision,
+ * scaling) times the candidate kernel configurations on its own inputs --
+ * the row Gram's output tile width (128 or 64 columns), the row-space step
+ * layout (512 threads x 2 rows or 256 x 8 per CTA), the merged refresh, the
+ * INT8 digit slices of the K products -- each run whole, and caches for that
+ * shape the fastest configuration whose chosen ncomp, outer predictions and
+ * inner accuracies equal the default configuration's.  Later calls of the
+ * shape (fpls_double_cv_scores included) run with it while autotuning is on;
+ * with it off every call runs the default configuration.  The
+ * first call costs about 3 grid runs per candidate.  No counterpart in the
+ * reference. */
+int fpls_set_autotune(int on, char* err, size_t errlen);
+
+/* The tuned shapes as newline-separated JSON objects (shape, chosen
+ * configuration, every candidate's device ms and whether its results equaled
+ * the default's), NUL-terminated into buf (truncated to len); *needed gets
+ * the full size. */
+int fpls_autotune_report(char* buf, size_t len, size_t* needed, char* err, size_t errlen);
+
 /* Registers a predictor matrix (n x p, FP64 or FP32) in device memory for
  * repeated calls; *handle identifies it until fpls_x_free.  Lets a caller keep
  * X resident across CV runs instead of re-sending it (the reference re-uploads

@@ -413,31 +413,26 @@ def config_c1(lib, args, peaks, local):
 
 
 def config_c2(lib, args, peaks, local):
-    """PLSSVD PLS-DA with the LDA classifier: fit (rSVD), LDA on the projected
-    scores, prediction of the held-out rows; FP64 and BF16x3."""
+    """PLSSVD PLS-DA with the LDA classifier through the fused entry
+    (fpls_pls_lda): rSVD fit, LDA on the fit's training scores, prediction of
+    the held-out rows, X (FP32) sent once; FP64 and BF16x3."""
     from fastpls_b200 import synthetic
     from oracle import pls as opls
     torch = _torch_dev(local)
     d = synthetic.c2_plsda(seed=1)
-    X = np.asfortranarray(d["Xtrain"], dtype=np.float64)
-    Xt = np.asfortranarray(d["Xtest"], dtype=np.float64)
+    X, Xt = d["Xtrain"], d["Xtest"]          # FP32, column-major
     y, C, K = d["ytrain"], d["n_classes"], 50
     Y = opls.transformy(y)
     n, p = X.shape
     nt = Xt.shape[0]
-    Xd, Yd, Xtd = _dev(torch, X), _dev(torch, Y), _dev(torch, Xt)
+    Xd, Xtd = _dev(torch, X), _dev(torch, Xt)
     torch.cuda.synchronize()
+    kw = dict(method=1, oversample=10, power_iters=2, seed=1, store_B=False)
 
-    def step(Xa, Ya, Xta):
+    def step(Xa, Xta):
         def fn():
-            model = lib.pls_model1(Xa, Ya, [K], svd_method=4, oversample=10, power_iters=2, seed=1)
-            t = lib.last_call_ms()
-            Rp = model["R"] / model["vX"].T
-            off = (model["mX"] @ Rp).ravel()
-            lda = lib.lda_project_train_prefix(Xa, Rp, off, y, C, [K])
-            t += lib.last_call_ms()
-            r = lib.lda_project_predict(Xta, Rp, off, lda[str(K)], return_scores=True)
-            return r, t + lib.last_call_ms()
+            r = lib.pls_lda(Xa, Y, y, Xta, [K], C, **kw)
+            return r, lib.last_call_ms()
         return fn
 
     steps = min(args.steps, 10)
@@ -445,40 +440,46 @@ def config_c2(lib, args, peaks, local):
     for prec in ("fp64", "bf16x3"):
         lib.set_precision(prec)
         try:
-            r_d, ms_d, _ = _timed_calls(lib, step(Xd, Yd, Xtd), steps, max(args.warmup, 2))
+            r_d, ms_d, _ = _timed_calls(lib, step(Xd, Xtd), steps, max(args.warmup, 2))
             lib.host_register(X)
             lib.host_register(Xt)
             try:
-                r_h, ms_h, wall_h = _timed_calls(lib, step(X, Y, Xt), steps, 1)
+                r_h, ms_h, wall_h = _timed_calls(lib, step(X, Xt), steps, 1)
             finally:
                 lib.host_unregister(X)
                 lib.host_unregister(Xt)
-            kr = _profile_step(lib, step(Xd, Yd, Xtd), peaks)
+            kr = _profile_step(lib, step(Xd, Xtd), peaks)
         finally:
             lib.set_precision("fp64")
         res[prec] = (r_d, ms_d, ms_h, wall_h, kr)
     l = min(K + 10, p)
     F = (n * p + 2.0 * (1 + 2 * 2) * p * C * l + 2.0 * p * C * l + 4.0 * p * l * l + 2.0 * n * p * K
          + 4.0 * n * K * K + 2.0 * nt * p * K + 2.0 * nt * K * C)
-    B = 8.0 * (2.0 * n * p + nt * p)
+    B = 4.0 * (2.0 * n * p + nt * p)
     r64, r3 = res["fp64"][0], res["bf16x3"][0]
-    s64 = r64["scores"]
+    # LDA scores of the test rows under both fits (the labels' margins)
+    Rp64, off64 = r64["R_predict"], r64["R_offset"]
+    lin64, c64 = r64["lda_linear"][:, :K, 0], r64["lda_constants"][:, 0]
+    s64 = (Xt.astype(np.float64) @ Rp64 - off64) @ lin64.T + c64
     gap = np.sort(s64, axis=1)
     clear = (gap[:, -1] - gap[:, -2]) > 1e-5 * np.abs(gap).max(axis=1)
-    acc = dict(lda_score_rel_err_bf16x3_vs_fp64=float(np.linalg.norm(r3["scores"] - s64) / np.linalg.norm(s64)),
-               labels_equal_beyond_margin_1e5=bool(np.all(r3["pred"][clear] == r64["pred"][clear])),
+    p64, p3 = r64["pred_codes"][:, 0], r3["pred_codes"][:, 0]
+    s3 = (Xt.astype(np.float64) @ r3["R_predict"] - r3["R_offset"]) @ r3["lda_linear"][:, :K, 0].T + \
+        r3["lda_constants"][:, 0]
+    acc = dict(lda_score_rel_err_bf16x3_vs_fp64=float(np.linalg.norm(s3 - s64) / np.linalg.norm(s64)),
+               labels_equal_beyond_margin_1e5=bool(np.all(p3[clear] == p64[clear])),
                rows_beyond_margin=int(clear.sum()),
-               test_accuracy_fp64=float(np.mean(r64["pred"] == d["ytest"])),
-               test_accuracy_bf16x3=float(np.mean(r3["pred"] == d["ytest"])))
+               test_accuracy_fp64=float(np.mean(p64 == d["ytest"])),
+               test_accuracy_bf16x3=float(np.mean(p3 == d["ytest"])))
     _, ms_d, ms_h, wall_h, kr = res["bf16x3"]
-    out = dict(workload="C2 PLSSVD + LDA PLS-DA 20000x5000 (fp32 data, fp64 calls), 100 classes, ncomp 50, "
-                        "rSVD oversample 10 power 2, 5000 test rows",
+    out = dict(workload="C2 PLSSVD + LDA PLS-DA 20000x5000 fp32, 100 classes, ncomp 50, rSVD oversample 10 "
+                        "power 2, 5000 test rows, one fused call (fpls_pls_lda)",
                metric="X rows/s (fit + LDA + test prediction)", unit="rows/s", value=n / (ms_d / 1e3),
                fits_per_s=1e3 / ms_d, ms_per_step=ms_d, steps=steps, precision="bf16x3",
                dtype="bf16x3 split GEMMs (fp32 accumulate) + fp64",
                e2e=dict(value=n / (wall_h / 1e3), unit="rows/s", ms_per_step=wall_h, device_ms_per_step=ms_h,
-                        h2d_bytes_per_step=int(2 * X.nbytes + Y.nbytes + Xt.nbytes),
-                        d2h_bytes_per_step=int(8 * (p * K * 3 + nt * C) + 4 * nt)),
+                        h2d_bytes_per_step=int(X.nbytes + Y.nbytes + Xt.nbytes + y.nbytes),
+                        d2h_bytes_per_step=int(8 * (p * K * 3 + C * K * 2) + 4 * nt)),
                roofline=step_roofline(F, B, ms_d, peaks, "bf16x3"), kernel_rooflines=kr[:3],
                fp64=dict(ms_per_step=res["fp64"][1], rows_per_s=n / (res["fp64"][1] / 1e3),
                          e2e_ms_per_step=res["fp64"][3],
@@ -486,15 +487,12 @@ def config_c2(lib, args, peaks, local):
                          kernel_rooflines=res["fp64"][4][:3]),
                accuracy=acc)
     if not args.no_cpu_baseline:
-        from oracle import lda as olda
+        from oracle import pls_lda as opl
+        Xh, Xth = X.astype(np.float64), Xt.astype(np.float64)
 
         def sample():
             t0 = time.perf_counter()
-            model = opls.pls_model1(X, Y, [K], svd_method=4, rsvd_oversample=10, rsvd_power=2, seed=1)
-            Rp = model["R"] / model["vX"].T
-            off = (model["mX"] @ Rp).ravel()
-            lda = olda.lda_project_train_prefix(X, Rp, off, y, C, [K])
-            olda.lda_project_predict(Xt, Rp, off, lda[str(K)])
+            opl.pls_lda(Xh, Y, y, Xth, [K], C, method=1, oversample=10, power_iters=2, seed=1)
             return n, time.perf_counter() - t0
         cb = timed_cpu(sample)
         cb.update(unit="rows/s", kind="port", sample="the full C2 step (fit, LDA, 5000 test rows) per sample, "

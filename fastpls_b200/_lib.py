@@ -158,21 +158,23 @@ class DeviceMatrix:
     within HBM instead of across PCIe (the C ABI tells host and device
     pointers apart by unified addressing)."""
 
-    def __init__(self, obj):
+    def __init__(self, obj, allow_f32=False):
         cai = obj.__cuda_array_interface__
         shape = tuple(int(v) for v in cai["shape"])
-        if cai["typestr"] != "<f8" or len(shape) not in (1, 2):
+        ok_types = ("<f8", "<f4") if allow_f32 else ("<f8",)
+        if cai["typestr"] not in ok_types or len(shape) not in (1, 2):
             raise ValueError("device matrices must be float64 vectors or matrices")
+        esz = 4 if cai["typestr"] == "<f4" else 8
         if len(shape) == 1:
             shape = (shape[0], 1)
         rows, cols = shape
         strides = cai.get("strides")  # None: C-contiguous
         if len(cai["shape"]) == 2 and rows > 1 and cols > 1 and \
-                (strides is None or tuple(strides) != (8, 8 * rows)):
+                (strides is None or tuple(strides) != (esz, esz * rows)):
             raise ValueError("device matrices must be column-major and contiguous")
         self.ptr = int(cai["data"][0])
         self.shape = shape
-        self.dtype = np.dtype(np.float64)
+        self.dtype = np.dtype(np.float32 if esz == 4 else np.float64)
         self.owner = obj
 
 
@@ -650,11 +652,22 @@ def pls_lda(Xtrain, Ytrain, y, Xtest, ncomp, n_classes, method=1, scaling=1, xpr
             oversample=10, power_iters=1, svds_tol=0.0, seed=1, lda_ridge=1e-8, store_B=True):
     """Fused PLS + LDA (fpls_pls_lda): fit, one LDA per distinct ncomp, test labels.
     Xtrain / Xtest: FP64 or FP32 (the same type for both)."""
-    f32 = np.asarray(Xtrain).dtype == np.float32
-    dt = np.float32 if f32 else np.float64
-    Xa = np.asfortranarray(Xtrain, dtype=dt)
-    n, p = Xa.shape
-    Xt = np.asfortranarray(np.zeros((0, p)) if Xtest is None else Xtest, dtype=dt)
+    if _is_device(Xtrain):
+        Xa = Xtrain if isinstance(Xtrain, DeviceMatrix) else DeviceMatrix(Xtrain, allow_f32=True)
+        f32 = Xa.dtype == np.float32
+        n, p = Xa.shape
+        if Xtest is None:
+            Xt = np.zeros((0, p), dtype=Xa.dtype)
+        else:
+            Xt = Xtest if isinstance(Xtest, DeviceMatrix) else DeviceMatrix(Xtest, allow_f32=True)
+            if Xt.dtype != Xa.dtype:
+                raise ValueError("Xtrain and Xtest must have the same type")
+    else:
+        f32 = np.asarray(Xtrain).dtype == np.float32
+        dt = np.float32 if f32 else np.float64
+        Xa = np.asfortranarray(Xtrain, dtype=dt)
+        n, p = Xa.shape
+        Xt = np.asfortranarray(np.zeros((0, p)) if Xtest is None else Xtest, dtype=dt)
     Y = _f64(Ytrain)
     m = Y.shape[1]
     yy = _i32(y)
@@ -670,8 +683,9 @@ def pls_lda(Xtrain, Ytrain, y, Xtest, ncomp, n_classes, method=1, scaling=1, xpr
              R_predict=_out(p, K0), R_offset=np.zeros(K0),
              pred_codes=np.zeros((max(ntest, 1), L), dtype=np.int32, order="F"))
     U = ctypes.c_int(0)
-    _call("fpls_pls_lda", Xa.ctypes.data, int(f32), n, p, _p(Y), m, _p(yy),
-          Xt.ctypes.data if ntest else None, ntest, _p(nc), L, C, int(method), int(scaling), int(bool(xprod)),
+    xa_ptr = Xa.ptr if isinstance(Xa, DeviceMatrix) else Xa.ctypes.data
+    xt_ptr = (Xt.ptr if isinstance(Xt, DeviceMatrix) else Xt.ctypes.data) if ntest else None
+    _call("fpls_pls_lda", xa_ptr, int(f32), n, p, _p(Y), m, _p(yy), xt_ptr, ntest, _p(nc), L, C, int(method), int(scaling), int(bool(xprod)),
           int(bool(fit)), int(oversample), int(power_iters), float(svds_tol), int(seed), float(lda_ridge),
           _p(o["ncomp"]), _p(o["R"]), _p(o["Q"]), _p(o["mX"]), _p(o["vX"]), _p(o["mY"]), _p(o["B"]),
           _p(o["Yfit"]), _p(o["R2Y"]), ctypes.byref(U), _p(o["unique_ncomp"]), _p(o["lda_means"]),

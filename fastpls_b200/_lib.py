@@ -79,6 +79,7 @@ SIGNATURES = {
                       _DP, _DP, _DP, _DP, _IP, _C, _S], ctypes.c_int),
     "fpls_set_autotune": ([_I, _C, _S], ctypes.c_int),
     "fpls_autotune_report": ([ctypes.c_char_p, _S, ctypes.POINTER(ctypes.c_size_t), _C, _S], ctypes.c_int),
+    "fpls_int8_gram": ([ctypes.c_void_p, _I, _I, _I, _DP, _I, _DP, _C, _S], ctypes.c_int),
     "fpls_bf16x3_gemm_noalloc": ([ctypes.c_void_p, _I, _I, ctypes.c_void_p, _I, ctypes.c_void_p,
                                   _C, _S], ctypes.c_int),
     "fpls_gaussian_y_encode": ([_DP, _I, _I, _DP, _I, _DP, _DP, _DP, _C, _S], ctypes.c_int),
@@ -470,7 +471,7 @@ def lda_project_predict(X, R, offset, lda, return_scores=False):
     return dict(pred=lab, scores=sc) if return_scores else dict(pred=lab)
 
 
-PREC = {"fp64": 0, "bf16x3": 1, "bf16x6": 2}
+PREC = {"fp64": 0, "bf16x3": 1, "bf16x6": 2, "int8": 3}
 
 
 def bf16x3_gemm(A, B):
@@ -480,6 +481,17 @@ def bf16x3_gemm(A, B):
     C = _out(A.shape[0], B.shape[1])
     _call("fpls_bf16x3_gemm", _p(A), A.shape[0], A.shape[1], _p(B), B.shape[1], _p(C))
     return C
+
+
+def int8_gram(X, slices=4, mean=None):
+    """(X - mean)(X - mean)^T through INT8 digit planes of the rows (fpls_int8_gram)."""
+    f32 = np.asarray(X).dtype == np.float32
+    Xa = np.asfortranarray(X, dtype=np.float32 if f32 else np.float64)
+    n, p = Xa.shape
+    mu = None if mean is None else np.ascontiguousarray(mean, dtype=np.float64).ravel()
+    K = _out(n, n)
+    _call("fpls_int8_gram", Xa.ctypes.data, int(f32), n, p, _p(mu), int(slices), _p(K))
+    return K
 
 
 def int8_emulated_gemm(A, B, slices=7):

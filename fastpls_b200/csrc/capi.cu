@@ -983,6 +983,28 @@ int fpls_bf16x3_gemm(const double* A, int M, int K, const double* B, int N, doub
   });
 }
 
+int fpls_int8_gram(const void* X, int x_is_float32, int n, int p, const double* mean, int slices, double* K,
+                   char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && X && K, "int8_gram: empty matrix");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    const size_t np = (size_t)n * p;
+    const double* d64 = x_is_float32 ? nullptr : upload(static_cast<const double*>(X), np);
+    const float* d32 = x_is_float32 ? upload(static_cast<const float*>(X), np) : nullptr;
+    const double* dm = mean ? upload(mean, p) : nullptr;
+    double* dK = ctx.arena.alloc_n<double>((size_t)n * n);
+    dzero(ctx.d_status + 16, sizeof(int));
+    OzakiPlanes pl = ozaki_split_rows(d64, d32, n, p, dm, slices);
+    ozaki_gram(pl, dK, n);
+    download(K, dK, (size_t)n * n);
+    int e = 0;
+    d2h(&e, ctx.d_status + 16, sizeof(int));
+    ctx.sync();
+    if (e) throw Error(FPLS_ERR_CUDA, "tensor-core pipeline wait timed out");
+  });
+}
+
 int fpls_int8_emulated_gemm(const double* A, int M, int K, const double* B, int N, int slices, double* C,
                             char* err, size_t errlen) {
   return guarded(err, errlen, [&] {
@@ -1029,7 +1051,8 @@ static CvX cv_x(const void* X, int x_is_float32, bool x_on_device, int n, int p)
 }
 
 static CvGridOptions cv_options(int scaling, int precision, int batched) {
-  FPLS_REQUIRE(precision == FPLS_PREC_FP64 || precision == FPLS_PREC_BF16X3 || precision == FPLS_PREC_BF16X6,
+  FPLS_REQUIRE(precision == FPLS_PREC_FP64 || precision == FPLS_PREC_BF16X3 || precision == FPLS_PREC_BF16X6 ||
+                   precision == FPLS_PREC_INT8,
                "unknown precision");
   CvGridOptions opt;
   opt.scaling = scaling;

@@ -43,6 +43,17 @@ bool int8_k_products() {
   return !(e && std::string(e) == "fp64");
 }
 
+// Digit slices of the INT8 row Gram (FASTPLS_GRAM_SLICES, else 4: 28 bits of
+// every centred row against its largest entry, an error far below the FP32
+// rounding of the data).
+int int8_gram_slices() {
+  if (const char* e = std::getenv("FASTPLS_GRAM_SLICES")) {
+    const int v = std::atoi(e);
+    if (v >= kOzakiMinSlices && v <= kOzakiMaxSlices) return v;
+  }
+  return 4;
+}
+
 void load_centered(const double* x64, const float* x32, int n, int p, const double* mean, double* dst) {
   Context& ctx = Context::get();
   if (x64) load_centered_kernel<double><<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(x64, n, p, mean, dst);
@@ -279,7 +290,10 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
   // The mixed row-space loop needs only the BF16 planes of Xc, split straight
   // from the caller's matrix; every other combination works on a centred FP64
   // copy.  x0 is the first column of Xc (the Householder sign of the sketch).
-  const bool planes_only = opt.precision >= 1 && dual;
+  // INT8 grids build the row Gram (and the sketch product) from digit planes
+  // of the centred rows; off the row-space path they run in FP64.
+  const bool int8_gram = opt.precision == 3 && dual;
+  const bool planes_only = (opt.precision == 1 || opt.precision == 2) && dual;
   const int planes = opt.precision == 2 ? 3 : 2;  // BF16x6: hi, mid, lo planes
   // A host X goes up in overlapped column chunks on the mixed row-space path,
   // else in one copy first.
@@ -346,11 +360,15 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
       x0 = ar.alloc_n<double>(n);
       load_centered(x64, x32, n, 1, mall, x0);
       xop = make_split_operator_centered(x64, x32, mall, n, p, planes);
+    } else if (int8_gram) {
+      x0 = ar.alloc_n<double>(n);
+      load_centered(x64, x32, n, 1, mall, x0);
+      xop = make_ozaki_rows_operator(x64, x32, mall, n, p, int8_gram_slices());
     } else {
       X = ar.alloc_n<double>((size_t)n * p);
       load_centered(x64, x32, n, p, mall, X);
       x0 = X;
-      if (opt.precision >= 1) xop = make_split_operator(X, n, p, !dual, planes);
+      if (opt.precision == 1 || opt.precision == 2) xop = make_split_operator(X, n, p, !dual, planes);
       else xop.reset(new XOperatorF64(X, n, p));
     }
     FPLS_CUDA(cudaEventRecord(ctx.planes_ready, ctx.stream));
@@ -365,7 +383,7 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
   if (dual) {
     if (!gram_done) xop->gram(Kg);
     px->kop_f64.reset(new XOperatorF64(Kg, n, n));
-    if (opt.precision >= 1 && int8_k_products()) {
+    if ((opt.precision >= 1 && opt.precision <= 2 && int8_k_products()) || int8_gram) {
       px->kop_slices = ozaki_default_slices();
       px->kop_int8 = make_ozaki_sym_operator(Kg, n, px->kop_slices);
     }

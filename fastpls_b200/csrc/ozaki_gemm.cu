@@ -40,6 +40,7 @@
 // cluster multicast is used.
 #include "autotune.cuh"
 #include "ozaki_gemm.cuh"
+#include "xop_split.cuh"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -359,12 +360,15 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
 // segment were written by the product kernel.
 constexpr int kReducePieces = 8;
 
+// tile_segs (when not null) lists each tile's segment ids in contraction
+// order (plans whose segments of one tile are not consecutive).
 __global__ void ozaki_reduce_kernel(const double* __restrict__ part, const int* __restrict__ tile_seg,
-                                    int n_tiles_n, int M, int N, double* __restrict__ C, int ldc) {
+                                    const int* __restrict__ tile_segs, int n_tiles_n, int M, int N,
+                                    double* __restrict__ C, int ldc) {
   const int tile = blockIdx.x / kReducePieces;
   const int piece = blockIdx.x % kReducePieces;
   const int s0 = tile_seg[tile], s1 = tile_seg[tile + 1];
-  if (s1 - s0 <= 1) return;
+  if (s1 - s0 <= 1) return;   // a single segment went straight to C
   const int mt = tile / n_tiles_n, nt = tile % n_tiles_n;
   const int e0 = piece * (OBM * OBN / kReducePieces), e1 = e0 + OBM * OBN / kReducePieces;
   for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
@@ -372,7 +376,10 @@ __global__ void ozaki_reduce_kernel(const double* __restrict__ part, const int* 
     const int m = mt * OBM + mm, n = nt * OBN + nn;
     if (m >= M || n >= N) continue;
     double acc = 0.0;
-    for (int s = s0; s < s1; ++s) acc += part[(static_cast<size_t>(s) * OBN + nn) * OBM + mm];
+    for (int j = s0; j < s1; ++j) {
+      const int s = tile_segs ? tile_segs[j] : j;
+      acc += part[(static_cast<size_t>(s) * OBN + nn) * OBM + mm];
+    }
     C[m + static_cast<size_t>(n) * ldc] = acc;
   }
 }
@@ -433,13 +440,152 @@ __global__ void ozaki_split_kernel(const double* __restrict__ X, int klen, int c
   }
 }
 
+// Row exponents of a column-major matrix with the column means subtracted:
+// thread (row i, column range of the block) takes the largest |x_ij - mean_j|
+// and folds its binary exponent into rexp[i] by atomicMax (order-free);
+// a non-finite entry raises bad[i].
+template <typename T>
+__global__ void ozaki_row_exp_kernel(const T* __restrict__ X, int n, int p, int ld, const double* __restrict__ mean,
+                                     int cols_per_block, int* __restrict__ rexp, int* __restrict__ bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int j0 = blockIdx.y * cols_per_block, j1 = min(p, j0 + cols_per_block);
+  double m = 0.0;
+  bool b = false;
+  for (int j = j0; j < j1; ++j) {
+    const double v = static_cast<double>(X[i + static_cast<size_t>(j) * ld]) - (mean ? mean[j] : 0.0);
+    if (!isfinite(v)) b = true;
+    else m = fmax(m, fabs(v));
+  }
+  if (b) bad[i] = 1;
+  if (m > 0.0) {
+    int e = 0;
+    frexp(m, &e);
+    atomicMax(rexp + i, e);
+  }
+}
+
+__global__ void ozaki_row_scale_kernel(const int* __restrict__ rexp, const int* __restrict__ bad, int n, int rows_pad,
+                                       double* __restrict__ scale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows_pad) return;
+  if (i >= n) { scale[i] = 1.0; return; }
+  const int e = max(-1000, min(1000, rexp[i] < -1000 ? 0 : rexp[i]));
+  scale[i] = (bad[i] || rexp[i] > 1000) ? __longlong_as_double(0x7ff8000000000000ll) : pow2i(e);
+}
+
+// Digits of the rows of X - mean (n x p column-major) into the planes (row i of
+// plane s at P + s * plane_stride + i * ldk, zero padded to rows_pad x ldk):
+// tiles of 32 rows x 128 columns, read column by column (coalesced) into shared
+// memory, then each row's 128 columns cut into S signed 7-bit digits (exact
+// FP64 steps) and written as 16-byte runs.
+template <typename T>
+__global__ void __launch_bounds__(256) ozaki_split_rows_kernel(const T* __restrict__ X, int n, int p, int ld,
+                                                               const double* __restrict__ mean,
+                                                               const double* __restrict__ scale,
+                                                               int8_t* __restrict__ P, int ldk, size_t plane_stride,
+                                                               int S) {
+  __shared__ double tile[128][33];
+  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 128;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = warp; c < 128; c += 8) {
+    const int j = j0 + c, i = i0 + lane;
+    double v = 0.0;
+    if (j < p && i < n) v = static_cast<double>(X[i + static_cast<size_t>(j) * ld]) - (mean ? mean[j] : 0.0);
+    tile[c][lane] = v;
+  }
+  __syncthreads();
+  const int r = threadIdx.x >> 3, c0 = (threadIdx.x & 7) * 16;
+  const int i = i0 + r;
+  const double sc = scale[i];
+  const double inv = (isfinite(sc) && sc > 0.0) ? 1.0 / sc : 0.0;   // a power of two: exact
+  int8_t dg[kOzakiMaxSlices][16];
+#pragma unroll
+  for (int x = 0; x < 16; ++x) {
+    double a = tile[c0 + x][r] * inv;
+    if (!isfinite(a)) a = 0.0;
+#pragma unroll
+    for (int s = 0; s < kOzakiMaxSlices; ++s) {
+      if (s >= S) break;
+      a *= 128.0;
+      const double d = trunc(a);
+      a -= d;
+      dg[s][x] = static_cast<int8_t>(static_cast<int>(d));
+    }
+  }
+  for (int s = 0; s < S; ++s) {
+    int4 w;
+    memcpy(&w, dg[s], 16);
+    *reinterpret_cast<int4*>(P + static_cast<size_t>(s) * plane_stride + static_cast<size_t>(i) * ldk + j0 + c0) = w;
+  }
+}
+
 int round_up(int x, int a) { return (x + a - 1) / a * a; }
 
 struct OzPlan {
   int tiles = 0, ntn = 0, ctas = 0;
   std::vector<int4> segs;
   std::vector<int> cta_begin, tile_begin;
+  // Segment ids of each tile in contraction order (tile t: tile_segs[tile_begin[t]
+  // .. tile_begin[t+1])); empty when a tile's segments are consecutive.
+  std::vector<int> tile_segs;
 };
+
+// K blocks per chunk of a symmetric (Gram) plan: every CTA takes an equal share
+// of each chunk, chunk after chunk, so that the CTAs running together read the
+// same K-panel of the digit planes from L2 (32 blocks of 128 bytes per row and
+// plane: 4096 columns, ~60 MB of planes at 3000 rows and 5 slices).
+constexpr int kOzSymChunkBlocks = 32;
+
+// Upper-triangle plan of a symmetric product C = A A^T (n x n): the tiles that
+// reach the upper triangle, segments of at most kMaxSegBlocks K blocks cut at
+// the chunk boundaries.
+OzPlan plan_ozaki_sym(int n, int K, int sm_count) {
+  OzPlan g;
+  const int mt = (n + OBM - 1) / OBM;
+  g.ntn = (n + OBN - 1) / OBN;
+  g.tiles = mt * g.ntn;
+  std::vector<int> inc;
+  for (int t = 0; t < g.tiles; ++t)
+    if ((t / g.ntn) * OBM < ((t % g.ntn) + 1) * OBN) inc.push_back(t);
+  const int kbt = (K + OBK - 1) / OBK;
+  const int kc = kOzSymChunkBlocks;
+  const int nchunks = (kbt + kc - 1) / kc;
+  const long long ninc = static_cast<long long>(inc.size());
+  g.ctas = static_cast<int>(std::max<long long>(1, std::min<long long>(sm_count, ninc * kbt)));
+  g.cta_begin.assign(g.ctas + 1, 0);
+  g.tile_begin.assign(g.tiles + 1, 0);
+  for (int c = 0; c < g.ctas; ++c) {
+    g.cta_begin[c] = static_cast<int>(g.segs.size());
+    for (int q = 0; q < nchunks; ++q) {
+      const int w = std::min(kc, kbt - q * kc);
+      const long long tq = ninc * w;
+      long long a = tq * c / g.ctas, e = tq * (c + 1) / g.ctas;
+      while (a < e) {
+        const int t = inc[static_cast<size_t>(a / w)];
+        const int kb0 = q * kc + static_cast<int>(a % w);
+        int kb1 = static_cast<int>(std::min<long long>(q * kc + w, kb0 + (e - a)));
+        kb1 = std::min(kb1, kb0 + kMaxSegBlocks);
+        g.segs.push_back(make_int4(t, kb0, kb1, 0));
+        a += kb1 - kb0;
+      }
+    }
+  }
+  g.cta_begin[g.ctas] = static_cast<int>(g.segs.size());
+  std::vector<int> ids(g.segs.size());
+  for (size_t i = 0; i < ids.size(); ++i) ids[i] = static_cast<int>(i);
+  std::stable_sort(ids.begin(), ids.end(), [&](int x, int y) {
+    return g.segs[x].x != g.segs[y].x ? g.segs[x].x < g.segs[y].x : g.segs[x].y < g.segs[y].y;
+  });
+  g.tile_segs = ids;
+  int s = 0;
+  for (int t = 0; t < g.tiles; ++t) {
+    g.tile_begin[t] = s;
+    while (s < static_cast<int>(ids.size()) && g.segs[ids[s]].x == t) ++s;
+  }
+  g.tile_begin[g.tiles] = s;
+  return g;
+}
 
 // Stream-K plan: CTA c covers iterations [c*total/ctas, (c+1)*total/ctas) of
 // the (tile, K block) space, cut into per-tile segments of at most
@@ -482,38 +628,45 @@ struct OzCached {
   int4* segs = nullptr;
   int* cta_begin = nullptr;
   int* tile_begin = nullptr;
+  int* tile_segs = nullptr;   // null unless the plan lists each tile's segments
   double* part = nullptr;
 };
 
-std::map<std::array<int, 4>, OzCached>& oz_cache() {
-  static std::map<std::array<int, 4>, OzCached> cache;
+std::map<std::array<int, 5>, OzCached>& oz_cache() {
+  static std::map<std::array<int, 5>, OzCached> cache;
   return cache;
 }
 
-// Plans, their device tables and the partial buffers are kept per shape, so
-// the repeated products of an iteration issue no host-to-device copy.
-const OzCached& oz_plan(int M, int N, int K, int sm_count, cudaStream_t st) {
+// Plans, their device tables and the partial buffers are kept per shape (and
+// plan kind: general, or the upper tiles of a symmetric product), so the
+// repeated products of an iteration issue no host-to-device copy.
+const OzCached& oz_plan(int M, int N, int K, int sm_count, cudaStream_t st, bool sym = false) {
   auto& cache = oz_cache();
-  const std::array<int, 4> key{M, N, K, sm_count};
+  const std::array<int, 5> key{M, N, K, sm_count, sym ? 1 : 0};
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
   OzCached c;
-  c.g = plan_ozaki(M, N, K, sm_count);
+  c.g = sym ? plan_ozaki_sym(M, K, sm_count) : plan_ozaki(M, N, K, sm_count);
   auto up = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
   const size_t b_segs = up(c.g.segs.size() * sizeof(int4));
   const size_t b_cta = up(c.g.cta_begin.size() * sizeof(int));
   const size_t b_tile = up(c.g.tile_begin.size() * sizeof(int));
+  const size_t b_tsegs = up(std::max<size_t>(c.g.tile_segs.size(), 1) * sizeof(int));
   const size_t b_part = c.g.segs.size() * static_cast<size_t>(OBM) * OBN * sizeof(double);
-  FPLS_CUDA(cudaMalloc(&c.dev, b_segs + b_cta + b_tile + b_part));
+  FPLS_CUDA(cudaMalloc(&c.dev, b_segs + b_cta + b_tile + b_tsegs + b_part));
   c.segs = reinterpret_cast<int4*>(c.dev);
   c.cta_begin = reinterpret_cast<int*>(c.dev + b_segs);
   c.tile_begin = reinterpret_cast<int*>(c.dev + b_segs + b_cta);
-  c.part = reinterpret_cast<double*>(c.dev + b_segs + b_cta + b_tile);
+  c.tile_segs = c.g.tile_segs.empty() ? nullptr : reinterpret_cast<int*>(c.dev + b_segs + b_cta + b_tile);
+  c.part = reinterpret_cast<double*>(c.dev + b_segs + b_cta + b_tile + b_tsegs);
   FPLS_CUDA(cudaMemcpyAsync(c.segs, c.g.segs.data(), c.g.segs.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
   FPLS_CUDA(cudaMemcpyAsync(c.cta_begin, c.g.cta_begin.data(), c.g.cta_begin.size() * sizeof(int),
                             cudaMemcpyHostToDevice, st));
   FPLS_CUDA(cudaMemcpyAsync(c.tile_begin, c.g.tile_begin.data(), c.g.tile_begin.size() * sizeof(int),
                             cudaMemcpyHostToDevice, st));
+  if (c.tile_segs)
+    FPLS_CUDA(cudaMemcpyAsync(c.tile_segs, c.g.tile_segs.data(), c.g.tile_segs.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, st));
   return cache.emplace(key, std::move(c)).first->second;
 }
 
@@ -581,7 +734,61 @@ struct XOperatorOzakiSym : public XOperator {
   void gram(double*) override { throw Error(kErrArgument, "the INT8 product operator has no Gram"); }
 };
 
+// X as its centred rows' digit planes: times() (X M for a p x F block M, the
+// sketch product) and gram() (X X^T) on the INT8 tensor cores.
+struct XOperatorOzakiRows : public XOperator {
+  OzakiPlanes xp;
+  XOperatorOzakiRows(const double* x64, const float* x32, const double* mean, int n_, int p_, int slices) {
+    n = n_;
+    p = p_;
+    xp = ozaki_split_rows(x64, x32, n_, p_, mean, slices);
+  }
+  void times(const double* M, int F, double* U) override {
+    OzakiPlanes b = ozaki_alloc(F, p, xp.slices);
+    ozaki_split(M, p, b);
+    ozaki_gemm(xp, b, U, n);
+  }
+  void t_times(const double*, int, double*) override {
+    throw Error(kErrArgument, "the INT8 row operator has no transposed product");
+  }
+  void gram(double* K) override { ozaki_gram(xp, K, n); }
+};
+
 }  // namespace
+
+OzakiPlanes ozaki_split_rows(const double* x64, const float* x32, int n, int p, const double* mean, int slices) {
+  Context& ctx = Context::get();
+  OzakiPlanes pl = ozaki_alloc(n, p, slices);
+  int* rexp = ctx.arena.alloc_n<int>(n);
+  int* bad = ctx.arena.alloc_n<int>(n);
+  FPLS_CUDA(cudaMemsetAsync(rexp, 0x80, n * sizeof(int), ctx.stream));   // a very negative sentinel
+  dzero(bad, n * sizeof(int));
+  constexpr int kCols = 64;
+  const dim3 g1(ceil_div(n, 256), ceil_div(p, kCols));
+  if (x64) ozaki_row_exp_kernel<double><<<g1, 256, 0, ctx.stream>>>(x64, n, p, n, mean, kCols, rexp, bad);
+  else ozaki_row_exp_kernel<float><<<g1, 256, 0, ctx.stream>>>(x32, n, p, n, mean, kCols, rexp, bad);
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  ozaki_row_scale_kernel<<<ceil_div(pl.rows_pad, 256), 256, 0, ctx.stream>>>(rexp, bad, n, pl.rows_pad, pl.scale);
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  const dim3 g2(pl.ldk / 128, pl.rows_pad / 32);
+  const size_t stride = static_cast<size_t>(pl.rows_pad) * pl.ldk;
+  if (x64)
+    ozaki_split_rows_kernel<double><<<g2, 256, 0, ctx.stream>>>(x64, n, p, n, mean, pl.scale, pl.data, pl.ldk, stride,
+                                                                slices);
+  else
+    ozaki_split_rows_kernel<float><<<g2, 256, 0, ctx.stream>>>(x32, n, p, n, mean, pl.scale, pl.data, pl.ldk, stride,
+                                                               slices);
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  return pl;
+}
+
+std::unique_ptr<XOperator> make_ozaki_rows_operator(const double* x64, const float* x32, const double* mean, int n,
+                                                    int p, int slices) {
+  return std::unique_ptr<XOperator>(new XOperatorOzakiRows(x64, x32, mean, n, p, slices));
+}
 
 OzakiPlanes ozaki_alloc(int rows, int k, int slices) {
   FPLS_REQUIRE(slices >= kOzakiMinSlices && slices <= kOzakiMaxSlices, "INT8 products: slices must be in 4..7");
@@ -611,11 +818,12 @@ namespace {
 
 // Runs the product kernel: whole tiles straight to C (when C is given), the
 // others as partials in the cached plan.
-const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc, bool a_static) {
+const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc, bool a_static,
+                          bool sym = false) {
   FPLS_REQUIRE(A.slices == B.slices && A.k == B.k && A.ldk == B.ldk, "INT8 products: operands do not match");
   Context& ctx = Context::get();
   cudaStream_t st = ctx.stream;
-  const OzCached& c = oz_plan(A.rows, B.rows, A.k, ctx.sm_count, st);
+  const OzCached& c = oz_plan(A.rows, B.rows, A.k, ctx.sm_count, st, sym);
   const CUtensorMap mA = make_plane_map(A, OBM);
   const CUtensorMap mB = make_plane_map(B, OBN);
   int* err = ctx.d_status + 16;
@@ -634,10 +842,33 @@ const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C,
 
 void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc, bool a_static) {
   const OzCached& c = run_ozaki(A, B, C, ldc, a_static);
-  ozaki_reduce_kernel<<<c.g.tiles * kReducePieces, 256, 0, Context::get().stream>>>(c.part, c.tile_begin, c.g.ntn,
-                                                                                 A.rows, B.rows, C, ldc);
+  ozaki_reduce_kernel<<<c.g.tiles * kReducePieces, 256, 0, Context::get().stream>>>(c.part, c.tile_begin, nullptr,
+                                                                                 c.g.ntn, A.rows, B.rows, C, ldc);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+}
+
+void ozaki_gram(const OzakiPlanes& A, double* C, int ldc) {
+  FPLS_REQUIRE(ldc == A.rows, "INT8 Gram: the output must be n x n with ld n");
+  Context& ctx = Context::get();
+  const int slot = ctx.prof_begin("gram_int8", ctx.stream);
+  const OzCached& c = run_ozaki(A, A, C, ldc, false, true);
+  // the upper tiles' partials summed in contraction order (tiles with a single
+  // segment were written by the product kernel), then the lower triangle
+  ozaki_reduce_kernel<<<c.g.tiles * kReducePieces, 256, 0, ctx.stream>>>(c.part, c.tile_begin, c.tile_segs, c.g.ntn,
+                                                                         A.rows, A.rows, C, ldc);
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  if (slot >= 0) {
+    // algorithmic work: the S (S + 1) / 2 digit-plane pairs over the planned
+    // (upper) tiles; bytes: every plane of A once and C once
+    const double S = A.slices, n = A.rows, K = A.k;
+    int planned = 0;
+    for (int t = 0; t < c.g.tiles; ++t) planned += c.g.tile_begin[t + 1] > c.g.tile_begin[t];
+    const double frac = static_cast<double>(planned) / c.g.tiles;
+    ctx.prof_end(slot, ctx.stream, S * n * K + 8.0 * n * n * frac, 0.5 * S * (S + 1.0) * 2.0 * n * n * K * frac);
+  }
+  mirror_upper_triangle(C, A.rows);
 }
 
 OzakiPartials ozaki_gemm_partials(const OzakiPlanes& A, const OzakiPlanes& B, bool a_static) {

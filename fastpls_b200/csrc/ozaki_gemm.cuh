@@ -52,6 +52,24 @@ struct OzakiPartials {
 };
 OzakiPartials ozaki_gemm_partials(const OzakiPlanes& A, const OzakiPlanes& B, bool a_static = false);
 
+// Planes of the rows of a column-major n x p matrix (x64, or x32 widened
+// exactly) with the column means `mean` subtracted (none when null): row i of
+// the planes is row i of X - mean, scaled by the power of two above its largest
+// magnitude.  A row with a non-finite entry gets a NaN scale.
+OzakiPlanes ozaki_split_rows(const double* x64, const float* x32, int n, int p, const double* mean, int slices);
+
+// C (n x n, ld ldc) = A A^T for A given as planes: the upper tiles on an
+// L2-sharing stream-K plan (every CTA takes its share of each K chunk in turn),
+// the lower triangle mirrored.  Entry (i, j) is within about
+// 3 k 2^(eA_i + eA_j - 7 slices) of the exact product.
+void ozaki_gram(const OzakiPlanes& A, double* C, int ldc);
+
+// Operator over X (n x p) held as its centred rows' digit planes: times() is
+// X M (the sketch product of the row-space grids) and gram() is X X^T, both on
+// the INT8 tensor cores; no transposed product.
+std::unique_ptr<XOperator> make_ozaki_rows_operator(const double* x64, const float* x32, const double* mean, int n,
+                                                    int p, int slices);
+
 // Releases the cached stream-K plans (fpls_reset_workspace).
 void ozaki_release_cache();
 

@@ -52,7 +52,7 @@ enum fpls_status {
  * three tensor-core products (~2^-16 relative per product).  BF16X6: three
  * planes (hi, mid, lo), six products (~2^-24), FP32 accumulation in short
  * segments, FP64 sums. */
-enum fpls_precision { FPLS_PREC_FP64 = 0, FPLS_PREC_BF16X3 = 1, FPLS_PREC_BF16X6 = 2 };
+enum fpls_precision { FPLS_PREC_FP64 = 0, FPLS_PREC_BF16X3 = 1, FPLS_PREC_BF16X6 = 2, FPLS_PREC_INT8 = 3 };
 
 /* 1 when a B200 (sm_100a) device is usable.
  * Replaces _fastPLS_has_cuda (RcppExports.cpp:87; fastPLS.cpp:1607-1609). */
@@ -250,15 +250,30 @@ int fpls_bf16x3_gemm(const double* A, int M, int K, const double* B, int N, doub
 int fpls_int8_emulated_gemm(const double* A, int M, int K, const double* B, int N, int slices,
                             double* C, char* err, size_t errlen);
 
+/* K (n x n) = (X - mean)(X - mean)^T through the INT8 tensor cores: the rows
+ * of X (n x p, FP64 or FP32 with x_is_float32 = 1; mean p or null) cut into
+ * `slices` (4..7) signed 7-bit digit planes with a power-of-two scale per row,
+ * the plane pairs with s + t <= slices + 1 multiplied exactly (int32) on the
+ * upper tiles and combined in FP64, the lower triangle mirrored; entry (i, j)
+ * is within about 3 p 2^(e_i + e_j - 7 slices) of the exact product, 2^e_i the
+ * scale of row i.  The row Gram of the FPLS_PREC_INT8 CV grids; a diagnostic
+ * with no counterpart in the reference. */
+int fpls_int8_gram(const void* X, int x_is_float32, int n, int p, const double* mean, int slices, double* K,
+                   char* err, size_t errlen);
+
 /* Cross-validated class predictions with the argmax classifier for method 3
  * (simpls_fast).  X is n x p, FP64 (x_is_float32 = 0) or FP32 (= 1); y are
  * 1-based labels; fold holds 0-based fold ids (drawn by the caller, as the R
  * shim draws them with R's RNG); fit f uses seed + f.  All fold fits run in one
  * batched engine pass when batched = 1 (precision FPLS_PREC_FP64,
- * FPLS_PREC_BF16X3 or FPLS_PREC_BF16X6: the mixed forms build the row Gram
- * from two BF16 planes and three products, or three planes and six, and keep
- * the per-component products FP64-accurate on the INT8 tensor cores), else one
- * after another in FP64 (the plain drop-in path).
+ * FPLS_PREC_BF16X3, FPLS_PREC_BF16X6 or FPLS_PREC_INT8: the mixed forms build
+ * the row Gram from two BF16 planes and three products, three planes and six,
+ * or -- FPLS_PREC_INT8 -- from signed 7-bit digit planes of the centred rows
+ * multiplied exactly on the INT8 tensor cores (Ozaki scheme; the sketch
+ * product the same way), and all keep the per-component products
+ * FP64-accurate on the INT8 tensor cores; FPLS_PREC_INT8 grids that do not
+ * take the row-space engine run in FP64), else one after another in FP64
+ * (the plain drop-in path).
  * class_pred n x L (1-based; 0 where not predicted), status kfold (1 ok,
  * 2 empty fold, 3 no training rows, 4 single-class training fold).
  * Replaces _fastPLS_pls_cv_predict_compiled (RcppExports.cpp:731;

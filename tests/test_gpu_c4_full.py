@@ -9,7 +9,10 @@ score scale, class scores within relative 1e-9 in every (outer fold, ncomp)
 slice.  The mixed grid (BF16x3 row Gram, INT8 K products), the benchmarked
 form, is held to the FP64 grid beyond its own measured error: scores within
 1e-3 of a slice, labels identical beyond a 1e-3 margin, same chosen ncomp and
-outer predictions.  The oracle takes about 35 s of host time.
+outer predictions.  The INT8 grid (row Gram and sketch product from digit
+planes on the INT8 tensor cores) meets the 1e-5 relative score bound on every
+(outer fold, ncomp) slice, with labels identical beyond a 1e-5 margin.  The
+oracle takes about 35 s of host time.
 """
 import numpy as np
 import pytest
@@ -64,3 +67,16 @@ def test_full_size_mixed_grid_against_fp64(lib, full, fp64_grid):
                            MIXED_TOL)[0]
     assert slice_score_rel_err(b["inner_score"], a["inner_score"]) < MIXED_TOL
     assert slice_score_rel_err(b["outer_score"][None], a["outer_score"][None]) < 1e-5
+
+
+def test_full_size_int8_grid_within_1e5_of_fp64(lib, full, fp64_grid):
+    w = full
+    a = fp64_grid
+    b = lib.double_cv(w["X"], w["y"], w["outer"], w["inner"], w["ncomp"], w["n_classes"], seed=1,
+                      precision="int8", return_scores=True)
+    assert np.array_equal(a["best_comp"], b["best_comp"])
+    assert np.array_equal(a["pred"], b["pred"])
+    assert slice_score_rel_err(b["inner_score"], a["inner_score"]) < 1e-5
+    assert slice_score_rel_err(b["outer_score"][None], a["outer_score"][None]) < 1e-5
+    assert cv_labels_match(b["inner_pred"], a["inner_pred"], np.transpose(a["inner_score"], (2, 1, 0, 3)),
+                           1e-5)[0]

@@ -621,13 +621,26 @@ def config_c5(lib, args, peaks, local):
             kr = _profile_step(lib, step(Xd, Yd, Xtd, Xfd, Xtfd), peaks)
             e2e = None
             if prec == "bf16x6":
-                lib.host_register(X)
-                lib.host_register(Y)
+                # host buffers through the public API: each matrix crosses PCIe
+                # once (registered resident matrices, the filtered X kept in HBM)
+                for a in (X, Y, Xt):
+                    lib.host_register(a)
                 try:
-                    _, ms_h, wall_h = _timed_calls(lib, step(X, Y, Xt, None, None), 1, 0)
+                    def e2e_step():
+                        t0 = time.perf_counter()
+                        rx, ry, rt = lib.x_resident(X), lib.x_resident(Y), lib.x_resident(Xt)
+                        up_ms = 1e3 * (time.perf_counter() - t0)
+                        rf, rtf = lib.x_alloc(n, p), lib.x_alloc(nt, p)
+                        try:
+                            yp, dev_ms = step(rx, ry, rt, rf, rtf)()
+                        finally:
+                            for r in (rx, ry, rt, rf, rtf):
+                                r.free()
+                        return yp, up_ms + dev_ms
+                    _, ms_h, wall_h = _timed_calls(lib, e2e_step, 1, 0)
                 finally:
-                    lib.host_unregister(X)
-                    lib.host_unregister(Y)
+                    for a in (X, Y, Xt):
+                        lib.host_unregister(a)
                 e2e = (ms_h, wall_h)
         finally:
             lib.set_precision("fp64")
@@ -649,7 +662,9 @@ def config_c5(lib, args, peaks, local):
                precision="bf16x6", dtype="bf16x6 split GEMMs (fp32 accumulate) + fp64",
                e2e=dict(value=n / (wall_h / 1e3), unit="rows/s", ms_per_step=wall_h, device_ms_per_step=ms_h,
                         h2d_bytes_per_step=int(X.nbytes + Y.nbytes + Xt.nbytes + G.nbytes),
-                        d2h_bytes_per_step=int(n * p * 8 + nt * p * 8 + nt * q * 8)),
+                        d2h_bytes_per_step=int(nt * q * 8 + p * K * 8 * 2),
+                        note="X, Y and Xtest uploaded once as resident matrices (fpls_x_upload), the filtered "
+                             "matrices kept in HBM (fpls_x_alloc), the decoded test predictions returned"),
                roofline=step_roofline(F, B, res["bf16x6"][1], peaks, "bf16x3"),
                kernel_rooflines=res["bf16x6"][2][:3],
                other_precisions={pr: dict(ms_per_step=res[pr][1], rows_per_s=n / (res[pr][1] / 1e3),

@@ -80,6 +80,9 @@ SIGNATURES = {
     "fpls_set_autotune": ([_I, _C, _S], ctypes.c_int),
     "fpls_autotune_report": ([ctypes.c_char_p, _S, ctypes.POINTER(ctypes.c_size_t), _C, _S], ctypes.c_int),
     "fpls_int8_gram": ([ctypes.c_void_p, _I, _I, _I, _DP, _I, _DP, _C, _S], ctypes.c_int),
+    "fpls_x_alloc": ([_I, _I, _I, _IP, _C, _S], ctypes.c_int),
+    "fpls_x_device_pointer": ([_I, ctypes.POINTER(ctypes.c_void_p), _C, _S], ctypes.c_int),
+    "fpls_x_download": ([_I, ctypes.c_void_p, _C, _S], ctypes.c_int),
     "fpls_bf16x3_gemm_noalloc": ([ctypes.c_void_p, _I, _I, ctypes.c_void_p, _I, ctypes.c_void_p,
                                   _C, _S], ctypes.c_int),
     "fpls_gaussian_y_encode": ([_DP, _I, _I, _DP, _I, _DP, _DP, _DP, _C, _S], ctypes.c_int),
@@ -738,6 +741,47 @@ def x_upload(X):
     h = ctypes.c_int(-1)
     _call("fpls_x_upload", Xa.ctypes.data, is32, Xa.shape[0], Xa.shape[1], ctypes.byref(h))
     return h.value
+
+
+class ResidentMatrix:
+    """A registered device matrix seen as a column-major device matrix: pass it
+    where the entry points accept device memory (fpls_x_device_pointer)."""
+
+    def __init__(self, handle, n, p, f32=False):
+        self.handle = handle
+        ptr = ctypes.c_void_p(0)
+        _call("fpls_x_device_pointer", int(handle), ctypes.byref(ptr))
+        self.ptr = int(ptr.value)
+        self.shape = (int(n), int(p))
+        self.dtype = np.dtype(np.float32 if f32 else np.float64)
+
+    @property
+    def __cuda_array_interface__(self):
+        n, p = self.shape
+        esz = self.dtype.itemsize
+        return dict(shape=(n, p), typestr="<f4" if esz == 4 else "<f8", data=(self.ptr, False),
+                    strides=(esz, esz * n), version=3)
+
+    def download(self):
+        out = np.zeros(self.shape, dtype=self.dtype, order="F")
+        _call("fpls_x_download", int(self.handle), out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def free(self):
+        x_free(self.handle)
+
+
+def x_resident(X):
+    """Uploads X once and returns it as a ResidentMatrix."""
+    Xa, is32 = _x_arg(X)
+    return ResidentMatrix(x_upload(Xa), Xa.shape[0], Xa.shape[1], bool(is32))
+
+
+def x_alloc(n, p, f32=False):
+    """An empty resident matrix (zeros) for outputs that stay in HBM."""
+    h = ctypes.c_int(-1)
+    _call("fpls_x_alloc", int(n), int(p), int(bool(f32)), ctypes.byref(h))
+    return ResidentMatrix(h.value, n, p, f32)
 
 
 def x_free(handle):

@@ -1500,26 +1500,69 @@ int fpls_double_cv_outer_subset(const void* X, int x_is_float32, int n, int p, c
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+// A new resident matrix (n x p, FP32 or FP64), filled from X when X is set.
+int register_resident(const void* X, int x_is_float32, int n, int p) {
+  Context& ctx = Context::get();
+  ResidentX r;
+  r.n = n;
+  r.p = p;
+  r.f32 = x_is_float32 != 0;
+  const size_t bytes = (size_t)n * p * (r.f32 ? sizeof(float) : sizeof(double));
+  FPLS_CUDA(cudaMalloc(&r.ptr, bytes));
+  if (X) FPLS_CUDA(cudaMemcpyAsync(r.ptr, X, bytes, cudaMemcpyDefault, ctx.stream));
+  else FPLS_CUDA(cudaMemsetAsync(r.ptr, 0, bytes, ctx.stream));
+  ctx.sync();
+  int h = -1;
+  for (size_t i = 0; i < ctx.resident.size(); ++i)
+    if (!ctx.resident[i].ptr) { h = static_cast<int>(i); break; }
+  if (h < 0) { h = static_cast<int>(ctx.resident.size()); ctx.resident.push_back(r); }
+  else ctx.resident[h] = r;
+  return h;
+}
+
+}  // namespace
+
+extern "C" {
+
 int fpls_x_upload(const void* X, int x_is_float32, int n, int p, int* handle, char* err,
                   size_t errlen) {
   return guarded(err, errlen, [&] {
     FPLS_REQUIRE(n > 0 && p > 0 && X && handle, "x_upload: empty matrix");
+    Context::get().begin_call();
+    *handle = register_resident(X, x_is_float32, n, p);
+  });
+}
+
+int fpls_x_alloc(int n, int p, int x_is_float32, int* handle, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && handle, "x_alloc: empty matrix");
+    Context::get().begin_call();
+    *handle = register_resident(nullptr, x_is_float32, n, p);
+  });
+}
+
+int fpls_x_device_pointer(int handle, void** ptr, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
     Context& ctx = Context::get();
-    ctx.begin_call();
-    ResidentX r;
-    r.n = n;
-    r.p = p;
-    r.f32 = x_is_float32 != 0;
-    const size_t bytes = (size_t)n * p * (r.f32 ? sizeof(float) : sizeof(double));
-    FPLS_CUDA(cudaMalloc(&r.ptr, bytes));
-    FPLS_CUDA(cudaMemcpyAsync(r.ptr, X, bytes, cudaMemcpyDefault, ctx.stream));
+    FPLS_REQUIRE(ptr && handle >= 0 && handle < static_cast<int>(ctx.resident.size()) && ctx.resident[handle].ptr,
+                 "x_device_pointer: unknown handle");
+    *ptr = ctx.resident[handle].ptr;
+  });
+}
+
+int fpls_x_download(int handle, void* out, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    Context& ctx = Context::get();
+    FPLS_REQUIRE(out && handle >= 0 && handle < static_cast<int>(ctx.resident.size()) && ctx.resident[handle].ptr,
+                 "x_download: unknown handle");
+    const ResidentX& r = ctx.resident[handle];
+    const size_t bytes = (size_t)r.n * r.p * (r.f32 ? sizeof(float) : sizeof(double));
+    FPLS_CUDA(cudaMemcpyAsync(out, r.ptr, bytes, cudaMemcpyDefault, ctx.stream));
     ctx.sync();
-    int h = -1;
-    for (size_t i = 0; i < ctx.resident.size(); ++i)
-      if (!ctx.resident[i].ptr) { h = static_cast<int>(i); break; }
-    if (h < 0) { h = static_cast<int>(ctx.resident.size()); ctx.resident.push_back(r); }
-    else ctx.resident[h] = r;
-    *handle = h;
   });
 }
 

@@ -536,6 +536,17 @@ int fpls_x_upload(const void* X, int x_is_float32, int n, int p, int* handle, ch
                   size_t errlen);
 int fpls_x_free(int handle, char* err, size_t errlen);
 
+/* A registered device matrix created empty (zeros, n x p, FP32 or FP64), for
+ * outputs that should stay in HBM (e.g. the filtered X of fpls_opls_filter);
+ * fpls_x_device_pointer gives the device address of a registered matrix, to
+ * pass where the matrix entry points accept device memory, and
+ * fpls_x_download copies a registered matrix back (n x p, column-major).  With
+ * them a host caller sends X across PCIe once for a whole pipeline.  No
+ * counterpart in the reference. */
+int fpls_x_alloc(int n, int p, int x_is_float32, int* handle, char* err, size_t errlen);
+int fpls_x_device_pointer(int handle, void** ptr, char* err, size_t errlen);
+int fpls_x_download(int handle, void* out, char* err, size_t errlen);
+
 /* Session precision of the single-fit and prediction entry points
  * (fpls_pls_model1[_xprod], fpls_pls_model2_fast[_xprod], fpls_pls_model2's
  * cross-covariance, fpls_predict_*, the LDA projections, Gaussian-Y, OPLS,

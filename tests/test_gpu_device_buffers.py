@@ -61,3 +61,23 @@ def test_device_matrix_layout_is_checked(lib):
         lib.DeviceMatrix(X)
     with pytest.raises(ValueError):
         lib.DeviceMatrix(torch.zeros((50, 40), dtype=torch.float32, device="cuda").T)
+
+
+def test_resident_matrices_keep_a_pipeline_on_the_device(lib):
+    # X sent once (fpls_x_upload), the filtered X written to a resident matrix
+    # (fpls_x_alloc) and fed to the fit by its device pointer
+    d = synthetic.c5_lowrank(seed=7, n=500, p=240, q=60, rank=5, n_test=50)
+    X, Y = d["Xtrain"].astype(np.float64), d["Ytrain"].astype(np.float64)
+    rx, ry = lib.x_resident(X), lib.x_resident(Y)
+    rf = lib.x_alloc(*X.shape)
+    try:
+        fd = lib.opls_filter(rx, ry, 2, out=rf)
+        fh = lib.opls_filter(X, Y, 2)
+        assert rel_err(rf.download(), fh["X"]) <= TOL
+        md = lib.pls_model2_fast(rf, ry, [4], seed=1)
+        mh = lib.pls_model2_fast(fh["X"], Y, [4], seed=1)
+        assert rel_err(md["B"], mh["B"]) <= TOL
+        assert fd["north"] == 2
+    finally:
+        for r in (rx, ry, rf):
+            r.free()

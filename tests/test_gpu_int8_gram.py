@@ -52,5 +52,5 @@ def test_int8_double_cv_close_to_fp64(lib):
     b = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], precision="int8", **kw)
     assert np.array_equal(a["best_comp"], b["best_comp"])
     assert np.array_equal(a["pred"], b["pred"])
-    assert slice_score_rel_err(b["inner_score"], a["inner_score"]) < 1e-6
-    assert cv_labels_match(b["inner_pred"], a["inner_pred"], np.transpose(a["inner_score"], (2, 1, 0, 3)), 1e-6)[0]
+    assert slice_score_rel_err(b["inner_score"], a["inner_score"]) < 1e-5
+    assert cv_labels_match(b["inner_pred"], a["inner_pred"], np.transpose(a["inner_score"], (2, 1, 0, 3)), 1e-5)[0]

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <sstream>
@@ -66,6 +67,30 @@ double* centered_test_copy(const double* Xh, int w, int p, const double* mX_d, c
   center_copy_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(X, w, p, mX_d, vX_d, X); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   return X;
+}
+
+// Block results (rb x top_k, ld rb) into the full outputs (w x top_k, ld w) at row r0.
+__global__ void place_rows_kernel(const int* __restrict__ bi, const double* __restrict__ bs, int rb, int top_k, int w,
+                                  int r0, int* __restrict__ di, double* __restrict__ ds) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)rb * top_k) return;
+  const int i = static_cast<int>(t % rb), j = static_cast<int>(t / rb);
+  di[r0 + i + (size_t)j * w] = bi[t];
+  if (ds) ds[r0 + i + (size_t)j * w] = bs[t];
+}
+
+// Test rows per block of a class prediction: all of them while the scores of
+// every slice, the latent scores and the centred rows fit in 1 GiB, else
+// blocks that do (at least 128 rows); FASTPLS_PREDICT_BLOCK_ROWS sets it.
+int predict_block_rows(int w, int p, int kmax, int m, int L) {
+  if (const char* e = std::getenv("FASTPLS_PREDICT_BLOCK_ROWS")) {
+    const long v = std::strtol(e, nullptr, 10);
+    if (v >= 1) return static_cast<int>(std::min<long>(v, w));
+  }
+  const double per_row = 8.0 * (static_cast<double>(p) + kmax + static_cast<double>(m) * L + 2.0 * p);
+  const double budget = 1024.0 * 1024.0 * 1024.0;
+  if (per_row * w <= budget) return w;
+  return std::max(128, static_cast<int>(budget / per_row));
 }
 
 // outer_pred[i] = prediction of the refit of i's outer fold at the chosen slice
@@ -644,18 +669,61 @@ int fpls_predict_classes(const double* Xtest, int w, int p, const double* mX, co
     const double* dR = upload(R, (size_t)p * kmax);
     const double* dW = upload(W, (size_t)kmax * m * L);
     const double* dbias = class_bias ? upload(class_bias, m) : nullptr;
-    double* dX = centered_test_copy(Xtest, w, p, dmX, dvX);
-    double* dT = ctx.arena.alloc_n<double>((size_t)w * kmax);
-    double* dYp = ctx.arena.alloc_n<double>((size_t)w * m * L);
-    lowrank_predict(dX, w, p, dR, kmax, dW, m, ncomp, L, dmY, dT, dYp);
     int* didx = ctx.arena.alloc_n<int>((size_t)w * top_k * L);
     double* dsc = ctx.arena.alloc_n<double>((size_t)w * top_k * L);
-    for (int a = 0; a < L; ++a) {
-      const double* Ya = dYp + (size_t)a * w * m;
-      if (top_k == 1 && !top_score) {
-        row_argmax(Ya, w, m, dbias, didx + (size_t)a * w);
-      } else {
-        row_topk(Ya, w, m, dbias, top_k, didx + (size_t)a * w * top_k, dsc + (size_t)a * w * top_k);
+    const int B = predict_block_rows(w, p, kmax, m, L);
+    if (B >= w) {
+      double* dX = centered_test_copy(Xtest, w, p, dmX, dvX);
+      double* dT = ctx.arena.alloc_n<double>((size_t)w * kmax);
+      double* dYp = ctx.arena.alloc_n<double>((size_t)w * m * L);
+      lowrank_predict(dX, w, p, dR, kmax, dW, m, ncomp, L, dmY, dT, dYp);
+      for (int a = 0; a < L; ++a) {
+        const double* Ya = dYp + (size_t)a * w * m;
+        if (top_k == 1 && !top_score) {
+          row_argmax(Ya, w, m, dbias, didx + (size_t)a * w);
+        } else {
+          row_topk(Ya, w, m, dbias, top_k, didx + (size_t)a * w * top_k, dsc + (size_t)a * w * top_k);
+        }
+      }
+    } else {
+      // Streamed: row blocks of B test rows, the next block's copy (copy
+      // stream, double-buffered) in flight while this one is scored; device
+      // memory O(B (p + kmax + m L)) whatever the number of test rows.
+      double* xb[2] = {ctx.arena.alloc_n<double>((size_t)B * p), ctx.arena.alloc_n<double>((size_t)B * p)};
+      double* dT = ctx.arena.alloc_n<double>((size_t)B * kmax);
+      double* dYp = ctx.arena.alloc_n<double>((size_t)B * m * L);
+      int* bidx = ctx.arena.alloc_n<int>((size_t)B * top_k);
+      double* bsc = ctx.arena.alloc_n<double>((size_t)B * top_k);
+      FPLS_CUDA(cudaEventRecord(ctx.copy_event(4), ctx.stream));   // the buffers are this call's
+      FPLS_CUDA(cudaStreamWaitEvent(ctx.copy, ctx.copy_event(4), 0));
+      const int nblk = ceil_div(w, B);
+      auto issue_copy = [&](int blk) {
+        const int r0 = blk * B, rb = std::min(B, w - r0), b = blk & 1;
+        if (blk >= 2) FPLS_CUDA(cudaStreamWaitEvent(ctx.copy, ctx.copy_event(2 + b), 0));   // xb[b] is free
+        FPLS_CUDA(cudaMemcpy2DAsync(xb[b], (size_t)rb * sizeof(double), Xtest + r0, (size_t)w * sizeof(double),
+                                    (size_t)rb * sizeof(double), p, cudaMemcpyDefault, ctx.copy));
+        FPLS_CUDA(cudaEventRecord(ctx.copy_event(b), ctx.copy));
+      };
+      issue_copy(0);
+      for (int blk = 0; blk < nblk; ++blk) {
+        const int r0 = blk * B, rb = std::min(B, w - r0), b = blk & 1;
+        if (blk + 1 < nblk) issue_copy(blk + 1);
+        FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.copy_event(b), 0));
+        center_copy_kernel<<<2 * ctx.sm_count, 256, 0, ctx.stream>>>(xb[b], rb, p, dmX, dvX, xb[b]);
+        ::fpls::note_launch();
+        FPLS_CHECK_LAUNCH();
+        lowrank_predict(xb[b], rb, p, dR, kmax, dW, m, ncomp, L, dmY, dT, dYp);
+        FPLS_CUDA(cudaEventRecord(ctx.copy_event(2 + b), ctx.stream));   // xb[b] read by now
+        for (int a = 0; a < L; ++a) {
+          const double* Ya = dYp + (size_t)a * rb * m;
+          if (top_k == 1 && !top_score) row_argmax(Ya, rb, m, dbias, bidx);
+          else row_topk(Ya, rb, m, dbias, top_k, bidx, bsc);
+          place_rows_kernel<<<ceil_div((long long)rb * top_k, 256), 256, 0, ctx.stream>>>(
+              bidx, top_score ? bsc : nullptr, rb, top_k, w, r0, didx + (size_t)a * w * top_k,
+              top_score ? dsc + (size_t)a * w * top_k : nullptr);
+          ::fpls::note_launch();
+          FPLS_CHECK_LAUNCH();
+        }
       }
     }
     download(top_index, didx, (size_t)w * top_k * L);

@@ -152,6 +152,10 @@ int fpls_predict_lowrank(const double* Xtest, int w, int p, const double* mX, co
 /* Class prediction from the same low-rank model: per slice, the top_k classes
  * of Ypred + class_bias (first maximum wins ties).  class_bias: m or NULL.
  * top_index w x top_k x L (1-based), top_score w x top_k x L (optional).
+ * When the score cube of all rows would pass 1 GiB (large class counts or
+ * many test rows), the rows are scored in blocks, the next block's copy in
+ * flight, so device memory stays bounded (FASTPLS_PREDICT_BLOCK_ROWS sets the
+ * block).
  * Replaces _fastPLS_pls_class_predict_topk_cuda (RcppExports.cpp:468;
  * fastPLS.cpp:3863-4113) and pls_predict_classes_compact_cuda (fastPLS.cpp:4156-4201). */
 int fpls_predict_classes(const double* Xtest, int w, int p, const double* mX, const double* vX,

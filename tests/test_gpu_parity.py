@@ -226,3 +226,19 @@ def test_fp64_runs_repeat_bit_for_bit(lib, c1, c2_small):
     for kk in ("4", "8"):
         assert np.array_equal(l1[kk]["linear"], l2[kk]["linear"])
         assert np.array_equal(l1[kk]["constants"], l2[kk]["constants"])
+
+
+@pytest.mark.parametrize("top_k,scores", [(5, True), (1, False)])
+def test_class_prediction_streamed_in_row_blocks(lib, c2_small, monkeypatch, top_k, scores):
+    # test rows scored in blocks (the copy of the next block in flight) give the
+    # predictions of the one-block call
+    X = c2_small["Xtrain"].astype(np.float64)
+    model = lib.pls_model1(X, c2_small["Y"], [4, 8], svd_method=4, power_iters=2, seed=1)
+    Xt = c2_small["Xtest"].astype(np.float64)
+    bias = np.linspace(-0.02, 0.02, c2_small["Y"].shape[1])
+    one = lib.predict_classes(model, Xt, class_bias=bias, top_k=top_k, return_scores=scores)
+    monkeypatch.setenv("FASTPLS_PREDICT_BLOCK_ROWS", "37")
+    blk = lib.predict_classes(model, Xt, class_bias=bias, top_k=top_k, return_scores=scores)
+    assert np.array_equal(blk["top_index"], one["top_index"])
+    if scores:
+        assert np.max(np.abs(blk["top_score"] - one["top_score"])) < 1e-12

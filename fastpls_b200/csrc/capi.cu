@@ -1454,11 +1454,12 @@ void run_double_cv_tuned(int n, int p, int n_classes, int kfold_outer, int kfold
       }
       o.ms = best_ms;
     };
-    std::vector<TuneConfig> cands;
+    std::vector<TuneConfig> cands{TuneConfig{}};   // the default first: the equality gate's reference
     const std::vector<int> tiles = precision == 1 ? std::vector<int>{128, 64} : std::vector<int>{0};
     const std::vector<int> layouts = n <= 4096 ? std::vector<int>{0, 1} : std::vector<int>{1};
     const std::vector<int> merges = n_classes <= 6 ? std::vector<int>{1, 0} : std::vector<int>{1};
-    const std::vector<int> slices = precision >= 1 ? std::vector<int>{5, 4, 6} : std::vector<int>{0};
+    const std::vector<int> slices = precision == 3 ? std::vector<int>{6, 5, 7}
+                                    : (precision >= 1 ? std::vector<int>{5, 4, 6} : std::vector<int>{0});
     for (int t : tiles)
       for (int l : layouts)
         for (int mg : merges)

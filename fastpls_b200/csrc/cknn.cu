@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <limits>
 #include <vector>
@@ -339,6 +340,143 @@ knn_tile_kernel(const KnnItem* __restrict__ items, KnnClassInfo ci, const int* _
   }
 }
 
+// The same items with the whole contraction staged at once: the item's 64
+// test rows are copied into shared memory once (cp.async, rows of K doubles
+// at a stride S = K rounded up to 4 with S = 4 mod 16, so that the fragment
+// loads of a warp hit distinct banks), the class's training rows stream
+// through two 64-row buffers (the next tile's copy in flight while this one is
+// multiplied), eight warps each take a 32 x 16 block of the 64 x 64 tile
+// (FP64 m8n8k4), and the finished buffer holds the similarity tile for the
+// top-k epilogue.  Up to K = 116.
+constexpr int kV2Threads = 256;
+constexpr int kV2MaxStride = 116;
+
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(kV2Threads, 1)
+knn_tile_kernel_v2(const KnnItem* __restrict__ items, KnnClassInfo ci, const int* __restrict__ pairs,
+                   int ntest, const double* __restrict__ Tq, const double* __restrict__ Ts, int K, int KP, int S,
+                   int use_k, double* __restrict__ part) {
+  extern __shared__ double smem[];
+  // a training-row buffer also holds the 64 x 65 similarity tile
+  const int BS = max(S, kTileN + 1);
+  double* As = smem;                   // 64 x S (test rows)
+  double* Bb[2] = {smem + kTileM * S, smem + kTileM * S + kTileN * BS};   // 64 rows of stride S each
+  double* lv = smem + kTileM * S + 2 * kTileN * BS;                       // use_k x 128 lists
+  __shared__ int prow[kTileM];
+
+  const KnnItem it = items[blockIdx.x];
+  const int c = it.cls;
+  const int p0 = ci.pair_offs[c] + it.tile * kTileM;
+  const int np = min(kTileM, ci.pair_offs[c + 1] - p0);
+  const int cr = ci.chunk_rows[c];
+  const int r0 = ci.row_offs[c] + it.chunk * cr;
+  const int r1 = min(ci.row_offs[c + 1], r0 + cr);
+  const int tid = threadIdx.x;
+  if (tid < kTileM) prow[tid] = (tid < np) ? (int)(pairs[p0 + tid] % ntest) : -1;
+  if (tid < 2 * kTileM)
+    for (int e = 0; e < use_k; ++e) lv[e * (2 * kTileM) + tid] = -INFINITY;
+  double tail = -INFINITY;
+  __syncthreads();
+
+  const uint32_t sA = static_cast<uint32_t>(__cvta_generic_to_shared(As));
+  const uint32_t sB[2] = {static_cast<uint32_t>(__cvta_generic_to_shared(Bb[0])),
+                          static_cast<uint32_t>(__cvta_generic_to_shared(Bb[1]))};
+  for (int idx = tid; idx < kTileM * KP; idx += kV2Threads) {
+    const int r = idx / KP, k = idx % KP;
+    const int src = prow[r];
+    const bool ok = src >= 0 && k < K;
+    cp_async8(sA + 8u * (r * S + k), ok ? Tq + (size_t)src * K + k : Tq, ok);
+  }
+  auto copy_tile = [&](int n0, int b) {
+    for (int idx = tid; idx < kTileN * KP; idx += kV2Threads) {
+      const int r = idx / KP, k = idx % KP;
+      const bool ok = n0 + r < r1 && k < K;
+      cp_async8(sB[b] + 8u * (r * S + k), ok ? Ts + (size_t)(n0 + r) * K + k : Ts, ok);
+    }
+  };
+  copy_tile(r0, 0);
+  cp_async_commit();
+
+  const int warp = tid >> 5, lane = tid & 31, gid = lane >> 2, tig = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  int j = 0;
+  for (int n0 = r0; n0 < r1; n0 += kTileN, ++j) {
+    const int b = j & 1;
+    const bool more = n0 + kTileN < r1;
+    if (more) {
+      copy_tile(n0 + kTileN, b ^ 1);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double* Bs = Bb[b];
+    double acc[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) acc[i][q][0] = acc[i][q][1] = 0.0;
+    const double* ap = As + (wm + gid) * S + tig;
+    const double* bp = Bs + (wn + gid) * S + tig;
+#pragma unroll 5
+    for (int kk = 0; kk < KP; kk += 4) {
+      double a[4], bq[2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = ap[i * 8 * S + kk];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) bq[q] = bp[q * 8 * S + kk];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) dmma_8x8x4(acc[i][q][0], acc[i][q][1], a[i], bq[q]);
+    }
+    __syncthreads();   // every warp is done with this tile's training rows: the buffer holds the similarities
+    double* sim = Bb[b];   // 64 x 65
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) sim[(wm + i * 8 + gid) * (kTileN + 1) + wn + q * 8 + tig * 2 + e] = acc[i][q][e];
+    __syncthreads();
+    if (tid < 2 * kTileM) {
+      const int m = tid & (kTileM - 1), h = tid >> 6;
+      const int ncol = min(32, r1 - n0 - h * 32);
+      for (int cidx = 0; cidx < ncol; ++cidx) {
+        const double v = sim[m * (kTileN + 1) + h * 32 + cidx];
+        if (v > tail) {
+          insert_desc<double, int>(lv + tid, nullptr, use_k, 2 * kTileM, v, 0);
+          tail = lv[(use_k - 1) * (2 * kTileM) + tid];
+        }
+      }
+    }
+    __syncthreads();   // the buffer is refilled by the copy issued next
+  }
+
+  // Merge the two half-row lists of each test row; write the pair's list.
+  if (tid < kTileM && tid < np) {
+    const int q = p0 + tid - ci.pair_offs[c];
+    double* out = part + ci.part_base[c] + ((long long)q * ci.nchunks[c] + it.chunk) * use_k;
+    const double* la = lv + tid;
+    const double* lb = lv + tid + kTileM;
+    int ia = 0, ib = 0;
+    for (int e = 0; e < use_k; ++e) {
+      const double va = la[ia * (2 * kTileM)], vb = lb[ib * (2 * kTileM)];
+      if (!(vb > va)) { out[e] = va; ++ia; } else { out[e] = vb; ++ib; }
+    }
+  }
+}
+
 // Per pair: merge its chunk lists, smoothed class score (src/fastPLS.cpp:1287-1320,
 // src/lda_cuda_kernels.cu:225-242), add alpha * base + bias.
 __global__ void knn_merge_kernel(const int* __restrict__ pairs, long long total_pairs,
@@ -561,17 +699,36 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
   pt.mark("class rows + pair lists");
   if (!items.empty()) {
     const KnnItem* ditems = upload(items.data(), items.size());
-    const size_t smem = sizeof(double) * (2 * kBK * (kTileM + kPad) + 2 * kBK * (kTileN + kPad) +
-                                          kTileM * (kTileN + 1) + (size_t)kKnnMax * kTileThreads);
-    static bool attr_set = false;
-    if (!attr_set) {
-      FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr_set = true;
-    }
     FPLS_REQUIRE(items.size() < (1u << 31), "candidate-kNN: too many work items");
     const int slot = ctx.prof_begin("cknn_tiles", ctx.stream);
-    knn_tile_kernel<<<(unsigned)items.size(), kTileThreads, smem, ctx.stream>>>(
-        ditems, ci, pairs, ntest, Tq, cr.Ts, kdim, use_k, part); ::fpls::note_launch();
+    // stride of the staged rows: K rounded up to 4, then to 4 mod 16
+    const int KP = (kdim + 3) / 4 * 4;
+    const int S = KP + (4 - KP % 16 + 16) % 16;
+    const char* v1 = std::getenv("FASTPLS_CKNN_TILES");
+    if (S <= kV2MaxStride && !(v1 && v1[0] == '1')) {
+      const size_t smem = sizeof(double) * ((size_t)kTileM * S + 2 * (size_t)kTileN * std::max(S, kTileN + 1) +
+                                            (size_t)kKnnMax * 2 * kTileM);
+      static bool attr2 = false;
+      if (!attr2) {
+        FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel_v2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(double) * ((size_t)(kTileM + 2 * kTileN) * kV2MaxStride +
+                                                               (size_t)kKnnMax * 2 * kTileM))));
+        attr2 = true;
+      }
+      knn_tile_kernel_v2<<<(unsigned)items.size(), kV2Threads, smem, ctx.stream>>>(ditems, ci, pairs, ntest, Tq,
+                                                                                   cr.Ts, kdim, KP, S, use_k, part);
+    } else {
+      const size_t smem = sizeof(double) * (2 * kBK * (kTileM + kPad) + 2 * kBK * (kTileN + kPad) +
+                                            kTileM * (kTileN + 1) + (size_t)kKnnMax * kTileThreads);
+      static bool attr_set = false;
+      if (!attr_set) {
+        FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+      }
+      knn_tile_kernel<<<(unsigned)items.size(), kTileThreads, smem, ctx.stream>>>(
+          ditems, ci, pairs, ntest, Tq, cr.Ts, kdim, use_k, part);
+    }
+    ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     if (slot >= 0) {
       // algorithmic work: one kdim-long FP64 dot per (candidate pair, class row);

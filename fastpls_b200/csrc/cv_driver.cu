@@ -1,3 +1,4 @@
+#include "autotune.cuh"
 #include "blas_f64.cuh"
 #include "context.cuh"
 #include "cv_driver.cuh"
@@ -43,15 +44,31 @@ bool int8_k_products() {
   return !(e && std::string(e) == "fp64");
 }
 
-// Digit slices of the INT8 row Gram (FASTPLS_GRAM_SLICES, else 4: 28 bits of
-// every centred row against its largest entry, an error far below the FP32
-// rounding of the data).
+// Digit slices of the INT8 row Gram (FASTPLS_GRAM_SLICES, else 5: 35 bits of
+// every centred row against its largest entry).  With 4 slices the omics
+// double-CV grid's class scores sit within 4.1e-6 of the FP64 grid, with 5
+// within 6.2e-7 (FP64 itself moves by 8.6e-7 under a 2^-24 relative change of
+// X) for 0.06 ms more.
 int int8_gram_slices() {
   if (const char* e = std::getenv("FASTPLS_GRAM_SLICES")) {
     const int v = std::atoi(e);
     if (v >= kOzakiMinSlices && v <= kOzakiMaxSlices) return v;
   }
-  return 4;
+  return 5;
+}
+
+// Digit slices of the INT8 grids' K products: 6 unless set.  The row-space loop
+// amplifies product errors about 10^6-fold by the 30th component: with 5
+// slices (2^-35) the last components' scores drift to 6.3e-5 of FP64, with 6
+// and 7 they stay within the Gram's error.
+int int8_mode_kprod_slices() {
+  if (const char* e = std::getenv("FASTPLS_OZAKI_SLICES")) {
+    const int v = std::atoi(e);
+    if (v >= kOzakiMinSlices && v <= kOzakiMaxSlices) return v;
+  }
+  const int t = active_tune().ozaki_slices;
+  if (t >= kOzakiMinSlices && t <= kOzakiMaxSlices) return t;
+  return 6;
 }
 
 void load_centered(const double* x64, const float* x32, int n, int p, const double* mean, double* dst) {
@@ -384,7 +401,7 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
     if (!gram_done) xop->gram(Kg);
     px->kop_f64.reset(new XOperatorF64(Kg, n, n));
     if ((opt.precision >= 1 && opt.precision <= 2 && int8_k_products()) || int8_gram) {
-      px->kop_slices = ozaki_default_slices();
+      px->kop_slices = int8_gram ? int8_mode_kprod_slices() : ozaki_default_slices();
       px->kop_int8 = make_ozaki_sym_operator(Kg, n, px->kop_slices);
     }
     pt.mark("row gram");

@@ -274,10 +274,10 @@ int fpls_int8_gram(const void* X, int x_is_float32, int n, int p, const double* 
  * the row Gram from two BF16 planes and three products, three planes and six,
  * or -- FPLS_PREC_INT8 -- from signed 7-bit digit planes of the centred rows
  * multiplied exactly on the INT8 tensor cores (Ozaki scheme; the sketch
- * product the same way), and all keep the per-component products
- * FP64-accurate on the INT8 tensor cores; FPLS_PREC_INT8 grids that do not
- * take the row-space engine run in FP64), else one after another in FP64
- * (the plain drop-in path).
+ * product the same way; class scores within 1e-5 of the FP64 grid), and all
+ * keep the per-component products FP64-accurate on the INT8 tensor cores;
+ * FPLS_PREC_INT8 grids that do not take the row-space engine run in FP64),
+ * else one after another in FP64 (the plain drop-in path).
  * class_pred n x L (1-based; 0 where not predicted), status kfold (1 ok,
  * 2 empty fold, 3 no training rows, 4 single-class training fold).
  * Replaces _fastPLS_pls_cv_predict_compiled (RcppExports.cpp:731;

@@ -801,6 +801,11 @@ def run_ours(args):
                                    batched=batched, **kw)
         return r, lib.last_call_ms()
 
+    # the first call of the shape tunes it (one-time cost, outside the timed steps)
+    lib.set_autotune(True)
+    t_tune = time.perf_counter()
+    step_value()
+    tune_s = time.perf_counter() - t_tune
     # warm-up
     for _ in range(max(args.warmup, 3)):
         step_value()
@@ -873,7 +878,7 @@ def run_ours(args):
         vs_baseline=None, dtype="bf16x3 split (fp32 accumulate) + int8 digit planes (exact int32) + fp64",
         data="synthetic",
         config=dict(CONFIG, parallelism=f"{world} independent replicas" if world > 1 else "1 GPU",
-                    precision="bf16x3", batched=True,
+                    precision="bf16x3", batched=True, autotune=True,
                     roofline_timing="per-kernel CUDA events over args.steps further steps run right after the "
                                     "timed ones (the timed steps carry no per-kernel events)"),
         x_rows_per_s=world * rows_per_fit * 50 * args.steps / (total_ms / 1e3),
@@ -901,6 +906,13 @@ def run_ours(args):
         out["plain_fp64"] = dict(ms_per_step=plain_ms, fits_per_s=FITS_PER_RUN / (plain_ms / 1e3),
                                  best_comp_equal=bool(np.array_equal(r_plain["best_comp"], r64["best_comp"])))
         out["speedup_vs_plain_fp64"] = (plain_ms / ms_per_step)
+    rep = [r for r in lib.autotune_report() if r["n"] == n and r["p"] == p]
+    out["autotune"] = dict(first_call_seconds=tune_s, shapes=[
+        dict(precision=r["precision"], chosen=r["chosen"],
+             default_ms=r["candidates"][0]["ms"],
+             chosen_ms=min(c["ms"] for c in r["candidates"] if c["config"] == r["chosen"]),
+             candidates=len(r["candidates"]), eligible=sum(1 for c in r["candidates"] if c["same_results"]))
+        for r in rep])
     if rank == 0 and not args.small:
         out["accuracy"] = accuracy_clause(lib, d, kw)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -47,6 +47,12 @@ CONFIG = dict(workload="C4 double CV SIMPLS PLS-DA 3000x20000 fp32, 10x5 folds, 
               n=3000, p=20000, n_classes=4, kfold_outer=10, kfold_inner=5, ncomp_max=30,
               l2="inputs larger than L2 (X fp32 240 MB, its BF16 planes 240 MB; no flush needed)")
 OTHER_CONFIGS = ("c1", "c2", "c3", "c5")
+HEADLINE_DTYPE = {
+    "bf16x3": "bf16x3 split (fp32 accumulate) + int8 digit planes (exact int32) + fp64",
+    "bf16x6": "bf16x6 split (fp32 accumulate) + int8 digit planes (exact int32) + fp64",
+    "int8": "int8 digit planes (exact int32, Ozaki) + fp64",
+    "fp64": "f64",
+}
 
 
 def parse():
@@ -61,6 +67,9 @@ def parse():
     ap.add_argument("--only", default=None, help="run just this configuration (c1..c5), no C4 headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="headline without the autotuner (profiling captures)")
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "bf16x6", "int8", "fp64"],
+                    help="precision of the timed headline steps")
     return ap.parse_args()
 
 
@@ -505,7 +514,7 @@ def config_c3(lib, args, peaks, local):
     """Label-aware PLSSVD (class-sorted segmented class sums, rSVD) + candidate
     kNN at 1000 classes, FP64 arithmetic on FP32 features."""
     from fastpls_b200 import synthetic
-    d = synthetic.c3_prototypes(seed=1)
+    d = synthetic.c3_prototypes(seed=1, n=200_000, n_test=10_000) if args.small else synthetic.c3_prototypes(seed=1)
     X, Xt, y, C = d["Xtrain"], d["Xtest"], d["ytrain"], d["n_classes"]
     n, p = X.shape
     nt = Xt.shape[0]
@@ -802,13 +811,13 @@ def run_ours(args):
         return r, lib.last_call_ms()
 
     # the first call of the shape tunes it (one-time cost, outside the timed steps)
-    lib.set_autotune(True)
+    lib.set_autotune(not args.no_autotune)
     t_tune = time.perf_counter()
-    step_value()
+    step_value(args.precision)
     tune_s = time.perf_counter() - t_tune
     # warm-up
     for _ in range(max(args.warmup, 3)):
-        step_value()
+        step_value(args.precision)
     barrier(pg)
     launches0 = lib.launch_count()
     times = []
@@ -816,14 +825,14 @@ def run_ours(args):
         # timed steps: no per-kernel events (an event between two kernels
         # stops the next one's early launch and costs a record per launch)
         for _ in range(args.steps):
-            r_mixed, ms = step_value()
+            r_mixed, ms = step_value(args.precision)
             times.append(ms)
         launches = lib.launch_count() - launches0
         # the same number of steps again with CUDA events around every hot
         # kernel class on its stream: the per-kernel durations of the rooflines
         lib.profile_begin()
         for _ in range(args.steps):
-            step_value()
+            step_value(args.precision)
         lib.profile_end()
     kernels = kernel_rooflines(lib.profile_classes(), peaks)
     clocks = clk.summary()
@@ -834,11 +843,11 @@ def run_ours(args):
     # e2e through the host-buffer call, inputs in page-locked host memory
     lib.host_register(d["X"])
     for _ in range(2):
-        lib.double_cv(d["X"], d["y"], d["outer"], d["inner"], precision="bf16x3", **kw)
+        lib.double_cv(d["X"], d["y"], d["outer"], d["inner"], precision=args.precision, **kw)
     barrier(pg)
     e2e_times = []
     for _ in range(args.steps):
-        lib.double_cv(d["X"], d["y"], d["outer"], d["inner"], precision="bf16x3", **kw)
+        lib.double_cv(d["X"], d["y"], d["outer"], d["inner"], precision=args.precision, **kw)
         e2e_times.append(lib.last_call_ms())
     barrier(pg)
     # the FP64 batched grid through the same host-buffer call
@@ -875,10 +884,10 @@ def run_ours(args):
     out = dict(
         metric="CV-grid fits/s", value=value, unit="fits/s", n_gpus=world, steps=args.steps,
         warmup=args.warmup, ms_per_step=ms_per_step, higher_is_better=True, scaling="weak",
-        vs_baseline=None, dtype="bf16x3 split (fp32 accumulate) + int8 digit planes (exact int32) + fp64",
+        vs_baseline=None, dtype=HEADLINE_DTYPE[args.precision],
         data="synthetic",
         config=dict(CONFIG, parallelism=f"{world} independent replicas" if world > 1 else "1 GPU",
-                    precision="bf16x3", batched=True, autotune=True,
+                    precision=args.precision, batched=True, autotune=not args.no_autotune,
                     roofline_timing="per-kernel CUDA events over args.steps further steps run right after the "
                                     "timed ones (the timed steps carry no per-kernel events)"),
         x_rows_per_s=world * rows_per_fit * 50 * args.steps / (total_ms / 1e3),

@@ -704,8 +704,12 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
     // stride of the staged rows: K rounded up to 4, then to 4 mod 16
     const int KP = (kdim + 3) / 4 * 4;
     const int S = KP + (4 - KP % 16 + 16) % 16;
-    const char* v1 = std::getenv("FASTPLS_CKNN_TILES");
-    if (S <= kV2MaxStride && !(v1 && v1[0] == '1')) {
+    // The staged kernel (FASTPLS_CKNN_TILES=2) measured 162.6 ms against the
+    // 16-wide k-step kernel's 123.3 ms on the large-class workload: with one
+    // 8-warp CTA per SM the tensor pipe idles while half the warps run the
+    // top-k epilogue; the k-step kernel, two CTAs per SM, stays the default.
+    const char* tv = std::getenv("FASTPLS_CKNN_TILES");
+    if (S <= kV2MaxStride && tv && tv[0] == '2') {
       const size_t smem = sizeof(double) * ((size_t)kTileM * S + 2 * (size_t)kTileN * std::max(S, kTileN + 1) +
                                             (size_t)kKnnMax * 2 * kTileM);
       static bool attr2 = false;

@@ -905,7 +905,7 @@ def run_ours(args):
                                  "in the headline form"),
         int8_batched=dict(ms_per_step=i8_ms, fits_per_s=FITS_PER_RUN / (i8_ms / 1e3),
                           note="row Gram and sketch product from digit planes of the centred rows on the INT8 "
-                               "tensor cores (4 slices, exact int32 accumulation), K products on INT8"),
+                               "tensor cores (5 slices, exact int32 accumulation), K products on INT8 with 6 slices"),
         parity=dict(outer_pred_agreement_bf16x3_vs_fp64=agree,
                     best_comp_equal=bool(np.array_equal(r_mixed["best_comp"], r64["best_comp"])),
                     inner_accuracy_max_abs_diff=float(np.nanmax(np.abs(r_mixed["inner_accuracy"] - r64["inner_accuracy"]))),

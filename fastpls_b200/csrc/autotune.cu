@@ -22,7 +22,12 @@ std::string TuneConfig::str() const {
   std::ostringstream s;
   s << "{\"gram_tile\": " << (gram_tile ? gram_tile : 128) << ", \"step_layout\": \""
     << (step_layout == 1 ? "256x8" : (step_layout == 0 ? "512x2" : "default")) << "\", \"merge\": "
-    << (merge == 0 ? "false" : "true") << ", \"ozaki_slices\": " << (ozaki_slices ? ozaki_slices : 5) << "}";
+    << (merge == 0 ? "false" : "true") << ", \"ozaki_slices\": ";
+  if (ozaki_slices)
+    s << ozaki_slices;
+  else
+    s << "\"mode default\"";
+  s << "}";
   return s.str();
 }
 

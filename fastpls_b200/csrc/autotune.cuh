@@ -5,10 +5,12 @@
 //
 // Knobs: the row Gram's output tile width (128 x 128 or 128 x 64, two-plane
 // split), the row-space step layout (512 threads x 2 rows or 256 x 8 rows per
-// CTA of a 4-CTA cluster), the merged refresh (on / off) and the number of
-// INT8 digit slices of the K products.  A switch set in the environment
-// (FASTPLS_GRAM_TILE, FASTPLS_DUAL_STEP, FASTPLS_DUAL_MERGE,
-// FASTPLS_OZAKI_SLICES) wins over the tuned value.
+// CTA of a 4-CTA cluster) and the merged refresh (on / off).  The number of
+// INT8 digit slices of the K products is part of the configuration but is not
+// searched: it sets the accuracy of the products, so each precision mode keeps
+// its own.  A switch set in the environment (FASTPLS_GRAM_TILE,
+// FASTPLS_DUAL_STEP, FASTPLS_DUAL_MERGE, FASTPLS_OZAKI_SLICES) wins over the
+// tuned value.
 #pragma once
 
 #include <string>

@@ -361,7 +361,8 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-__global__ void __launch_bounds__(kV2Threads, 1)
+template <int NB>
+__global__ void __launch_bounds__(kV2Threads, NB == 1 ? 2 : 1)
 knn_tile_kernel_v2(const KnnItem* __restrict__ items, KnnClassInfo ci, const int* __restrict__ pairs,
                    int ntest, const double* __restrict__ Tq, const double* __restrict__ Ts, int K, int KP, int S,
                    int use_k, double* __restrict__ part) {
@@ -369,8 +370,11 @@ knn_tile_kernel_v2(const KnnItem* __restrict__ items, KnnClassInfo ci, const int
   // a training-row buffer also holds the 64 x 65 similarity tile
   const int BS = max(S, kTileN + 1);
   double* As = smem;                   // 64 x S (test rows)
-  double* Bb[2] = {smem + kTileM * S, smem + kTileM * S + kTileN * BS};   // 64 rows of stride S each
-  double* lv = smem + kTileM * S + 2 * kTileN * BS;                       // use_k x 128 lists
+  // NB = 2: two buffers, the next tile's copy in flight during this tile;
+  // NB = 1: one buffer (half the shared memory: two CTAs per SM, one CTA's
+  // epilogue overlapping the other's products)
+  double* Bb[2] = {smem + kTileM * S, smem + kTileM * S + (NB - 1) * kTileN * BS};   // rows of stride S
+  double* lv = smem + kTileM * S + NB * kTileN * BS;                                 // use_k x 128 lists
   __shared__ int prow[kTileM];
 
   const KnnItem it = items[blockIdx.x];
@@ -410,9 +414,9 @@ knn_tile_kernel_v2(const KnnItem* __restrict__ items, KnnClassInfo ci, const int
   const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
   int j = 0;
   for (int n0 = r0; n0 < r1; n0 += kTileN, ++j) {
-    const int b = j & 1;
+    const int b = NB == 2 ? (j & 1) : 0;
     const bool more = n0 + kTileN < r1;
-    if (more) {
+    if (NB == 2 && more) {
       copy_tile(n0 + kTileN, b ^ 1);
       cp_async_commit();
       cp_async_wait<1>();
@@ -461,6 +465,10 @@ knn_tile_kernel_v2(const KnnItem* __restrict__ items, KnnClassInfo ci, const int
       }
     }
     __syncthreads();   // the buffer is refilled by the copy issued next
+    if (NB == 1 && more) {
+      copy_tile(n0 + kTileN, 0);
+      cp_async_commit();
+    }
   }
 
   // Merge the two half-row lists of each test row; write the pair's list.
@@ -709,18 +717,26 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
     // 8-warp CTA per SM the tensor pipe idles while half the warps run the
     // top-k epilogue; the k-step kernel, two CTAs per SM, stays the default.
     const char* tv = std::getenv("FASTPLS_CKNN_TILES");
-    if (S <= kV2MaxStride && tv && tv[0] == '2') {
-      const size_t smem = sizeof(double) * ((size_t)kTileM * S + 2 * (size_t)kTileN * std::max(S, kTileN + 1) +
-                                            (size_t)kKnnMax * 2 * kTileM);
-      static bool attr2 = false;
-      if (!attr2) {
-        FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel_v2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(sizeof(double) * ((size_t)(kTileM + 2 * kTileN) * kV2MaxStride +
-                                                               (size_t)kKnnMax * 2 * kTileM))));
-        attr2 = true;
+    if (S <= kV2MaxStride && tv && (tv[0] == '2' || tv[0] == '3')) {
+      const int nb = tv[0] == '2' ? 2 : 1;
+      const size_t smem = sizeof(double) * ((size_t)kTileM * S + nb * (size_t)kTileN * std::max(S, kTileN + 1) +
+                                            (size_t)use_k * 2 * kTileM);
+      const int smem_max = (int)(sizeof(double) * ((size_t)(kTileM + nb * kTileN) * kV2MaxStride +
+                                                   (size_t)kKnnMax * 2 * kTileM));
+      static bool attr2[2] = {false, false};
+      if (!attr2[nb - 1]) {
+        if (nb == 2)
+          FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel_v2<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+        else
+          FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel_v2<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+        attr2[nb - 1] = true;
       }
-      knn_tile_kernel_v2<<<(unsigned)items.size(), kV2Threads, smem, ctx.stream>>>(ditems, ci, pairs, ntest, Tq,
-                                                                                   cr.Ts, kdim, KP, S, use_k, part);
+      if (nb == 2)
+        knn_tile_kernel_v2<2><<<(unsigned)items.size(), kV2Threads, smem, ctx.stream>>>(
+            ditems, ci, pairs, ntest, Tq, cr.Ts, kdim, KP, S, use_k, part);
+      else
+        knn_tile_kernel_v2<1><<<(unsigned)items.size(), kV2Threads, smem, ctx.stream>>>(
+            ditems, ci, pairs, ntest, Tq, cr.Ts, kdim, KP, S, use_k, part);
     } else {
       const size_t smem = sizeof(double) * (2 * kBK * (kTileM + kPad) + 2 * kBK * (kTileN + kPad) +
                                             kTileM * (kTileN + 1) + (size_t)kKnnMax * kTileThreads);

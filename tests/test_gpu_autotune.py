@@ -1,7 +1,9 @@
 """The double-CV autotuner: the first call of a grid shape times the candidate
-configurations (Gram tile width, step layout, merged refresh, INT8 digit
-slices) on its own inputs and caches the fastest one whose results equal the
-default configuration's; tuned calls then give the default's outputs."""
+configurations (Gram tile width, step layout, merged refresh) on its own
+inputs and caches the fastest one whose results equal the default
+configuration's; tuned calls then give the default's outputs.  The INT8 digit
+slices are not searched, so a tuned INT8 grid keeps the INT8 mode's class
+scores."""
 import numpy as np
 import pytest
 
@@ -18,7 +20,7 @@ def autotune(lib):
     lib.set_autotune(False)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3", "int8"])
 def test_tuned_grid_reproduces_default(lib, autotune, precision):
     d = synthetic.c4_omics(seed=31, n=330 if precision == "fp64" else 340, p=1400, n_informative=20)
     outer, inner = double_cv_folds(d["y"], d["groups"], 4, 3, seed=2)
@@ -40,3 +42,24 @@ def test_tuned_grid_reproduces_default(lib, autotune, precision):
         assert np.array_equal(res["best_comp"], default["best_comp"])
         assert np.array_equal(res["pred"], default["pred"])
         assert np.array_equal(res["inner_accuracy"], default["inner_accuracy"])
+
+
+def test_tuned_int8_grid_keeps_its_class_scores(lib, autotune):
+    """Every candidate keeps the INT8 mode's slice count, so the tuned grid's
+    class scores stay within the INT8 bound (1e-5 of the slice's scale) of the
+    untuned grid's."""
+    d = synthetic.c4_omics(seed=33, n=350, p=1500, n_informative=20)
+    outer, inner = double_cv_folds(d["y"], d["groups"], 4, 3, seed=3)
+    nc = np.arange(1, 9)
+    kw = dict(seed=1, precision="int8")
+    lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)   # tunes the shape
+    kw["return_scores"] = True
+    tuned = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)   # runs it tuned
+    r = [x for x in lib.autotune_report() if x["n"] == 350][0]
+    assert all(c["config"]["ozaki_slices"] == r["candidates"][0]["config"]["ozaki_slices"]
+               for c in r["candidates"])
+    lib.set_autotune(False)
+    default = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)
+    a, b = tuned["inner_score"], default["inner_score"]
+    scale = np.max(np.abs(b), axis=tuple(range(1, b.ndim)), keepdims=True)
+    assert np.max(np.abs(a - b) / scale) < 1e-5

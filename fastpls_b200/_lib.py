@@ -28,7 +28,16 @@ class FastPLSError(RuntimeError):
 # name -> argtypes (restype int unless noted)
 _D, _I, _DP, _IP, _S, _C = (ctypes.c_double, ctypes.c_int, _c_double_p, _c_int_p,
                             ctypes.c_size_t, ctypes.c_char_p)
+# int (*fpls_allreduce_fn)(double* buf, long long count, void* stream, void* user)
+ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
+                                ctypes.c_void_p)
+_VP = ctypes.c_void_p
 SIGNATURES = {
+    "fpls_pls_model1_rows": ([_DP, _I, _I, _DP, _I, _IP, _I, _I, _I, _I, _I, _I, _D, _I, ALLREDUCE_FN, _VP,
+                              _IP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S],
+                             ctypes.c_int),
+    "fpls_pls_model2_fast_rows": ([_DP, _I, _I, _DP, _I, _IP, _I, _I, _I, _I, ALLREDUCE_FN, _VP, _DP, _DP,
+                                   _DP, _DP, _DP, _DP, _DP, _DP, _IP, _C, _S], ctypes.c_int),
     "fpls_has_cuda": ([], ctypes.c_int),
     "fpls_version": ([], ctypes.c_char_p),
     "fpls_reset_workspace": ([_C, _S], ctypes.c_int),
@@ -249,16 +258,48 @@ def truncated_svd(A, k, svd_method=4, oversample=10, power_iters=1, svds_tol=0.0
     return dict(u=U[:, :r], d=s[:r], vt=None if Vt is None else Vt[:r, :])
 
 
+def allreduce_callback(fn):
+    """Wraps fn(buf_ptr, count, stream_ptr) -- a sum of `count` doubles of
+    device memory over the ranks, ordered on the library's stream -- as the
+    fpls_allreduce_fn of the row-sharded fits.  Returns (callback, errors): an
+    exception raised by fn is kept in errors and the library sees status 1."""
+    errors = []
+
+    def cb(buf, count, stream, user):
+        try:
+            fn(int(buf or 0), int(count), int(stream or 0))
+            return 0
+        except BaseException as e:   # never let an exception cross the C frames
+            errors.append(e)
+            return 1
+    return ALLREDUCE_FN(cb), errors
+
+
+def _call_sharded(errors, name, *args):
+    try:
+        _call(name, *args)
+    except FastPLSError as e:
+        if errors:
+            raise errors[0] from e
+        raise
+
+
 def pls_model1(X, Y, ncomp, scaling=1, fit=False, svd_method=4, oversample=10, power_iters=1,
-               svds_tol=0.0, seed=1, store_B=True, xprod=False):
-    """PLSSVD (fpls_pls_model1), or its matrix-free form with xprod=True."""
+               svds_tol=0.0, seed=1, store_B=True, xprod=False, allreduce=None, n_total=None):
+    """PLSSVD (fpls_pls_model1), or its matrix-free form with xprod=True.
+
+    Row-sharded (fpls_pls_model1_rows) when allreduce = fn(buf, count, stream)
+    is given: X and Y are this rank's rows, n_total the rows over all ranks
+    (see fastpls_b200.row_shards)."""
     X = _f64(X)
     Y = _f64(Y)
     n, p = X.shape
     m = Y.shape[1]
     nc = _i32(np.atleast_1d(ncomp))
     L = nc.size
-    max_rank = min(n, p, m)
+    if allreduce is not None and (xprod or n_total is None):
+        raise ValueError("a row-sharded PLSSVD forms S (xprod=False) and needs n_total")
+    max_rank = min(n if allreduce is None else int(n_total), p, m)
     K0 = min(int(np.clip(nc, 1, max_rank).max()), max_rank)
     out = dict(C_latent=_out(K0, K0, L), W_latent=_out(K0, m, L), Q=_out(m, K0), Ttrain=_out(n, K0),
                R=_out(p, K0), mX=_out(1, p), vX=_out(1, p), mY=_out(1, m),
@@ -266,13 +307,18 @@ def pls_model1(X, Y, ncomp, scaling=1, fit=False, svd_method=4, oversample=10, p
                R2Y=np.zeros(L), singular_values=np.zeros(K0))
     nco = np.zeros(L, dtype=np.int32)
     keff = ctypes.c_int(0)
+    errors = []
     if xprod:
         head = ("fpls_pls_model1_xprod", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling),
                 int(bool(fit)), int(oversample), int(power_iters), float(svds_tol), int(seed), 3)
+    elif allreduce is not None:
+        cb, errors = allreduce_callback(allreduce)
+        head = ("fpls_pls_model1_rows", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
+                int(svd_method), int(oversample), int(power_iters), float(svds_tol), int(seed), cb, None)
     else:
         head = ("fpls_pls_model1", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
                 int(svd_method), int(oversample), int(power_iters), float(svds_tol), int(seed))
-    _call(*head, _p(nco),
+    _call_sharded(errors, *head, _p(nco),
           _p(out["C_latent"]), _p(out["W_latent"]), _p(out["Q"]), _p(out["Ttrain"]), _p(out["R"]),
           _p(out["mX"]), _p(out["vX"]), _p(out["mY"]), _p(out["B"]), _p(out["Yfit"]),
           _p(out["R2Y"]), _p(out["singular_values"]), ctypes.byref(keff))
@@ -288,8 +334,13 @@ def pls_model1(X, Y, ncomp, scaling=1, fit=False, svd_method=4, oversample=10, p
     return out
 
 
-def pls_model2_fast(X, Y, ncomp, scaling=1, fit=False, seed=1, store_B=True, xprod=False):
-    """Fast SIMPLS (fpls_pls_model2_fast), or its matrix-free form with xprod=True."""
+def pls_model2_fast(X, Y, ncomp, scaling=1, fit=False, seed=1, store_B=True, xprod=False, allreduce=None):
+    """Fast SIMPLS (fpls_pls_model2_fast), or its matrix-free form with xprod=True.
+
+    Row-sharded (fpls_pls_model2_fast_rows) when allreduce = fn(buf, count,
+    stream) is given: X and Y are this rank's rows (see fastpls_b200.row_shards)."""
+    if allreduce is not None and xprod:
+        raise ValueError("a row-sharded fast SIMPLS forms S (xprod=False)")
     X = _f64(X)
     Y = _f64(Y)
     n, p = X.shape
@@ -301,11 +352,17 @@ def pls_model2_fast(X, Y, ncomp, scaling=1, fit=False, seed=1, store_B=True, xpr
                B=_out(p, m, L) if store_B else None, Yfit=_out(n, m, L) if fit else None,
                R2Y=np.zeros(L))
     ncmp = ctypes.c_int(0)
-    head = (("fpls_pls_model2_fast_xprod", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling),
-             int(bool(fit)), int(seed), 3) if xprod else
-            ("fpls_pls_model2_fast", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
-             int(seed)))
-    _call(*head, _p(out["R"]), _p(out["Q"]), _p(out["mX"]), _p(out["vX"]), _p(out["mY"]),
+    errors = []
+    if allreduce is not None:
+        cb, errors = allreduce_callback(allreduce)
+        head = ("fpls_pls_model2_fast_rows", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling),
+                int(bool(fit)), int(seed), cb, None)
+    else:
+        head = (("fpls_pls_model2_fast_xprod", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling),
+                 int(bool(fit)), int(seed), 3) if xprod else
+                ("fpls_pls_model2_fast", _p(X), n, p, _p(Y), m, _p(nc), L, int(scaling), int(bool(fit)),
+                 int(seed)))
+    _call_sharded(errors, *head, _p(out["R"]), _p(out["Q"]), _p(out["mX"]), _p(out["vX"]), _p(out["mY"]),
           _p(out["B"]), _p(out["Yfit"]), _p(out["R2Y"]), ctypes.byref(ncmp))
     out.update(ncomp=nc, p=p, m=m, pls_method="simpls", n_components=ncmp.value,
                B_stored=bool(store_B), compact_prediction=not store_B)

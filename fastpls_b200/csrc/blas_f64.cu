@@ -247,6 +247,45 @@ __global__ void col_sd_kernel(const double* __restrict__ X, int n, int p, int ld
   if (lane == 0) out[j] = sqrt(q / static_cast<double>(n - 1));
 }
 
+// Column sums (the loop and warp reduction of col_mean_kernel, without the
+// division): the partial sums of a row-sharded fit.
+__global__ void col_sum_kernel(const double* __restrict__ X, int n, int p, int ldx, double* __restrict__ out) {
+  const int warps_per_block = blockDim.x >> 5;
+  const int j = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= p) return;
+  const double* xp = X + (size_t)j * ldx;
+  double s = 0.0;
+  for (int i = lane; i < n; i += 32) s += xp[i];
+  s = warp_sum(s);
+  if (lane == 0) out[j] = s;
+}
+
+// Sums of squared deviations from mu (the second pass of col_sd_kernel).
+__global__ void col_sqdev_kernel(const double* __restrict__ X, int n, int p, int ldx, const double* __restrict__ mu,
+                                 double* __restrict__ out) {
+  const int warps_per_block = blockDim.x >> 5;
+  const int j = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= p) return;
+  const double* xp = X + (size_t)j * ldx;
+  const double m = mu[j];
+  double q = 0.0;
+  for (int i = lane; i < n; i += 32) {
+    const double d = xp[i] - m;
+    q += d * d;
+  }
+  q = warp_sum(q);
+  if (lane == 0) out[j] = q;
+}
+
+// out = in / d, or sqrt(in / d) when root is set.
+__global__ void div_vec_kernel(const double* __restrict__ in, size_t count, double d, int root,
+                               double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = root ? sqrt(in[i] / d) : in[i] / d;
+}
+
 __global__ void center_scale_kernel(double* X, int n, int p, int ldx, const double* mean,
                                     const double* scale) {
   const size_t total = (size_t)n * p;
@@ -282,16 +321,35 @@ __global__ void add_row_vector_kernel(double* X, int n, int p, int ldx, const do
   }
 }
 
-__global__ void rq_sums_kernel(const double* __restrict__ Y, const double* __restrict__ Yp,
-                               int n, int m, double* out2) {
+// Column sums of Y in the order rq_sums_kernel takes them (one block).
+__global__ void rq_col_sums_kernel(const double* __restrict__ Y, int n, int m, double* __restrict__ out) {
   __shared__ double scratch[32];
-  double press = 0.0, tss = 0.0;
   for (int j = 0; j < m; ++j) {
     const double* yc = Y + (size_t)j * n;
     double s = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) s += yc[i];
     s = block_sum(s, scratch);
-    const double mu = s / static_cast<double>(n);
+    if (threadIdx.x == 0) out[j] = s;
+  }
+}
+
+// PRESS and TSS of Y against Yp; the TSS about the column means of these rows,
+// or about mus (the means over all ranks' rows of a row-sharded fit).
+__global__ void rq_sums_kernel(const double* __restrict__ Y, const double* __restrict__ Yp,
+                               int n, int m, double* out2, const double* __restrict__ mus) {
+  __shared__ double scratch[32];
+  double press = 0.0, tss = 0.0;
+  for (int j = 0; j < m; ++j) {
+    const double* yc = Y + (size_t)j * n;
+    double mu;
+    if (mus) {
+      mu = mus[j];
+    } else {
+      double s = 0.0;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) s += yc[i];
+      s = block_sum(s, scratch);
+      mu = s / static_cast<double>(n);
+    }
     const double* pc = Yp + (size_t)j * n;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const double d = yc[i] - pc[i];
@@ -486,6 +544,24 @@ void col_sd_centered(const double* X, int n, int p, int ldx, double* out) {
   FPLS_CHECK_LAUNCH();
 }
 
+void col_sum(const double* X, int n, int p, int ldx, double* out) {
+  if (p <= 0) return;
+  col_sum_kernel<<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, out); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+void col_sqdev(const double* X, int n, int p, int ldx, const double* mu, double* out) {
+  if (p <= 0) return;
+  col_sqdev_kernel<<<ceil_div(p, 8), 256, 0, Context::get().stream>>>(X, n, p, ldx, mu, out); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
+void div_vec(const double* in, size_t count, double d, bool root, double* out) {
+  if (count == 0) return;
+  div_vec_kernel<<<grid_for(count, 256), 256, 0, Context::get().stream>>>(in, count, d, root ? 1 : 0, out); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+}
+
 void center_scale(double* X, int n, int p, int ldx, const double* mean, const double* scale) {
   if ((size_t)n * p == 0) return;
   center_scale_kernel<<<grid_for((size_t)n * p, 256), 256, 0, Context::get().stream>>>(X, n, p, ldx, mean, scale); ::fpls::note_launch();
@@ -504,9 +580,20 @@ void add_row_vector(double* X, int n, int p, int ldx, const double* v) {
   FPLS_CHECK_LAUNCH();
 }
 
-void rq_sums(const double* Y, const double* Yp, int n, int m, double* out2) {
-  rq_sums_kernel<<<1, 512, 0, Context::get().stream>>>(Y, Yp, n, m, out2); ::fpls::note_launch();
+void rq_sums(const double* Y, const double* Yp, int n, int m, double* out2, const double* mus) {
+  rq_sums_kernel<<<1, 512, 0, Context::get().stream>>>(Y, Yp, n, m, out2, mus); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+}
+
+const double* shard_rq_means(const double* Y, int n, int m) {
+  if (!sharded()) return nullptr;
+  Context& ctx = Context::get();
+  double* mu = ctx.arena.alloc_n<double>(m);
+  rq_col_sums_kernel<<<1, 512, 0, ctx.stream>>>(Y, n, m, mu); ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  shard_sum(mu, m);
+  div_vec(mu, m, static_cast<double>(shard_rows(n)), false, mu);
+  return mu;
 }
 
 void fill(double* x, size_t n, double v) {

@@ -27,6 +27,11 @@ void col_mean(const double* X, int n, int p, int ldx, double* out);
 void col_mean(const float* X, int n, int p, int ldx, double* out);
 // Column standard deviation (n-1) of an already centred X.
 void col_sd_centered(const double* X, int n, int p, int ldx, double* out);
+// Column sums; sums of squared deviations from mu; out = in / d (sqrt(in / d)
+// with root).  The pieces of col_mean / col_sd_centered for row-sharded fits.
+void col_sum(const double* X, int n, int p, int ldx, double* out);
+void col_sqdev(const double* X, int n, int p, int ldx, const double* mu, double* out);
+void div_vec(const double* in, size_t count, double d, bool root, double* out);
 // X[:, j] = (X[:, j] - mean[j]) / scale[j]   (mean or scale may be null).
 void center_scale(double* X, int n, int p, int ldx, const double* mean, const double* scale);
 // dst (n x p, ldd) = src (n x p, lds)
@@ -34,7 +39,10 @@ void copy_matrix(double* dst, int ldd, const double* src, int lds, int n, int p)
 // X[i, j] += v[j] for all i (row broadcast)
 void add_row_vector(double* X, int n, int p, int ldx, const double* v);
 // Frobenius-type sums for R2: out[0] = sum((Y - Yp)^2), out[1] = sum((Y - colmean(Y))^2)
-void rq_sums(const double* Y, const double* Yp, int n, int m, double* out2);
+void rq_sums(const double* Y, const double* Yp, int n, int m, double* out2, const double* mus = nullptr);
+// Row-sharded fits: the column means of Y over all ranks' rows, the TSS
+// centre of rq_sums (null when the fit is not sharded).
+const double* shard_rq_means(const double* Y, int n, int m);
 void fill(double* x, size_t n, double v);
 void scale_vec(double* x, size_t n, double a);
 

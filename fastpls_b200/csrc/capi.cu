@@ -236,14 +236,17 @@ int pls_model1_impl(const double* X, int n, int p, const double* Y, int m, const
                     double svds_tol, int seed, bool xprod, int* ncomp_out, double* C_latent,
                     double* W_latent, double* Q, double* Ttrain, double* R, double* mX, double* vX,
                     double* mY, double* B, double* Yfit, double* R2Y, double* s, int* k_eff, char* err,
-                    size_t errlen) {
+                    size_t errlen, fpls_allreduce_fn allreduce = nullptr, void* user = nullptr) {
   return guarded(err, errlen, [&] {
     FPLS_REQUIRE(n > 0 && p > 0 && m > 0, "pls_model1 requires non-empty X and Y");
     FPLS_REQUIRE(L >= 1 && ncomp, "ncomp must contain at least one value");
     FPLS_REQUIRE(!(fit && !Yfit), "fit = 1 requires a Yfit buffer");
+    FPLS_REQUIRE(!(allreduce && xprod), "row-sharded fits form S = X^T Y (no matrix-free operator)");
     Context& ctx = Context::get();
     ctx.begin_call();
-    const int max_rank = std::min(n, std::min(p, m));
+    std::unique_ptr<RowShardScope> shards;
+    if (allreduce) shards.reset(new RowShardScope(ctx, allreduce, user, n));
+    const int max_rank = static_cast<int>(std::min<long long>(shard_rows(n), std::min(p, m)));
     std::vector<int> nc(ncomp, ncomp + L);
     for (int& c : nc) c = std::max(1, std::min(c, max_rank));
     const int K0 = std::min(max_of(nc.data(), L), max_rank);
@@ -408,6 +411,7 @@ static void simpls_fast_on_device(double* dX, int n, int p, double* dYc, int m, 
     b.Yg = dYc;
     b.S = ctx.arena.alloc_n<double>((size_t)p * m);
     xgemm(true, p, m, n, dX, n, dYc, n, b.S, p);
+    shard_sum(b.S, (size_t)p * m);
     double* om = ctx.arena.alloc_n<double>(p);
     device_gaussian(om, p, static_cast<unsigned int>(seed));
     b.omega = om;
@@ -433,10 +437,12 @@ static void simpls_fast_on_device(double* dX, int n, int p, double* dYc, int m, 
     double* tcol = fit ? ctx.arena.alloc_n<double>(n) : nullptr;
     double* rq = fit ? ctx.arena.alloc_n<double>(2 * L) : nullptr;
     if (fit) {
+      dzero(rq, 2 * (size_t)L * sizeof(double));
       dzero(dYf, (size_t)n * m * L * sizeof(double));
       dzero(cur, (size_t)n * m * sizeof(double));
     }
     std::vector<int> filled(L, 0);
+    const double* rq_mu = fit ? shard_rq_means(dYc, n, m) : nullptr;
     int i_out = 0;
     for (int a = 0; a < done; ++a) {
       while (i_out < L && a == nc[i_out] - 1) {
@@ -445,7 +451,7 @@ static void simpls_fast_on_device(double* dX, int n, int p, double* dYc, int m, 
           scale_column_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(b.Tkeep + (size_t)a * n, n, 1.0 / tn[a], tcol); ::fpls::note_launch();
           FPLS_CHECK_LAUNCH();
           gemm(false, true, n, m, 1, 1.0, tcol, n, b.Q + (size_t)a * m, m, 1.0, cur, n);
-          rq_sums(dYc, cur, n, m, rq + 2 * i_out);
+          rq_sums(dYc, cur, n, m, rq + 2 * i_out, rq_mu);
           double* sl = dYf + (size_t)i_out * n * m;
           d2d(sl, cur, (size_t)n * m * sizeof(double));
           add_row_vector(sl, n, m, n, dmY);
@@ -462,6 +468,7 @@ static void simpls_fast_on_device(double* dX, int n, int p, double* dYc, int m, 
     if (B) download(B, dB, (size_t)p * m * L);
     std::vector<double> hrq(2 * L, 0.0);
     if (fit) {
+      shard_sum(rq, 2 * (size_t)L);
       download(Yfit, dYf, (size_t)n * m * L);
       download(hrq.data(), rq, 2 * (size_t)L);
     }
@@ -486,6 +493,38 @@ int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, 
     simpls_fast_on_device(dX, n, p, dYc, m, ncomp, L, scaling, fit, seed, R, Q, mX, vX, mY, B, Yfit, R2Y,
                           n_components);
   });
+}
+
+int fpls_pls_model2_fast_rows(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
+                              int L, int scaling, int fit, int seed, fpls_allreduce_fn allreduce, void* user,
+                              double* R, double* Q, double* mX, double* vX, double* mY, double* B,
+                              double* Yfit, double* R2Y, int* n_components, char* err, size_t errlen) {
+  return guarded(err, errlen, [&] {
+    FPLS_REQUIRE(n > 0 && p > 0 && m > 0, "pls_model2_fast requires non-empty X and Y");
+    FPLS_REQUIRE(allreduce != nullptr, "pls_model2_fast_rows: the all-reduce callback is null");
+    Context& ctx = Context::get();
+    ctx.begin_call();
+    RowShardScope shards(ctx, allreduce, user, n);
+    double* dX = upload(X, (size_t)n * p);
+    double* dYc = upload(Y, (size_t)n * m);
+    simpls_fast_on_device(dX, n, p, dYc, m, ncomp, L, scaling, fit, seed, R, Q, mX, vX, mY, B, Yfit, R2Y,
+                          n_components);
+  });
+}
+
+int fpls_pls_model1_rows(const double* X, int n, int p, const double* Y, int m, const int* ncomp, int L,
+                         int scaling, int fit, int svd_method, int oversample, int power_iters,
+                         double svds_tol, int seed, fpls_allreduce_fn allreduce, void* user, int* ncomp_out,
+                         double* C_latent, double* W_latent, double* Q, double* Ttrain, double* R, double* mX,
+                         double* vX, double* mY, double* B, double* Yfit, double* R2Y, double* s, int* k_eff,
+                         char* err, size_t errlen) {
+  if (!allreduce) {
+    capi::set_err(err, errlen, "pls_model1_rows: the all-reduce callback is null");
+    return FPLS_ERR_ARGUMENT;
+  }
+  return pls_model1_impl(X, n, p, Y, m, ncomp, L, scaling, fit, svd_method, oversample, power_iters,
+                         svds_tol, seed, false, ncomp_out, C_latent, W_latent, Q, Ttrain, R, mX, vX,
+                         mY, B, Yfit, R2Y, s, k_eff, err, errlen, allreduce, user);
 }
 
 int fpls_kernel_matrix(const double* X1, int n1, const double* X2, int n2, int p, int kernel, double gamma,

@@ -727,8 +727,12 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
       if (!attr2[nb - 1]) {
         if (nb == 2)
           FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel_v2<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
-        else
+        else {
           FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel_v2<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+          // all of the SM's unified memory as shared memory: two 113 KB CTAs at K = 100
+          FPLS_CUDA(cudaFuncSetAttribute(knn_tile_kernel_v2<1>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared));
+        }
         attr2[nb - 1] = true;
       }
       if (nb == 2)

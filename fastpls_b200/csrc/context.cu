@@ -181,6 +181,45 @@ void dzero(void* dst, size_t bytes) {
   FPLS_CUDA(cudaMemsetAsync(dst, 0, bytes, Context::get().stream));
 }
 
+void shard_sum(double* buf, size_t count) {
+  Context& ctx = Context::get();
+  if (!ctx.shards || count == 0) return;
+  const int rc = ctx.shards->fn(buf, static_cast<long long>(count), static_cast<void*>(ctx.stream),
+                                ctx.shards->user);
+  if (rc != 0)
+    throw Error(kErrCuda, "row-sharded fit: the all-reduce callback returned " + std::to_string(rc));
+}
+
+long long shard_rows(long long n_local) {
+  const Context& ctx = Context::get();
+  return ctx.shards ? ctx.shards->n_total : n_local;
+}
+
+bool sharded() { return Context::get().shards != nullptr; }
+
+RowShardScope::RowShardScope(Context& c, int (*fn)(double*, long long, void*, void*), void* user,
+                             long long n_local)
+    : ctx(c) {
+  FPLS_REQUIRE(fn != nullptr, "row-sharded fit: the all-reduce callback is null");
+  rs.fn = fn;
+  rs.user = user;
+  rs.n_total = n_local;
+  ctx.shards = &rs;
+  try {
+    double nd = static_cast<double>(n_local);
+    double* d = ctx.arena.alloc_n<double>(1);
+    h2d(d, &nd, sizeof(double));
+    shard_sum(d, 1);
+    d2h(&nd, d, sizeof(double));
+    ctx.sync();
+    rs.n_total = static_cast<long long>(nd + 0.5);
+    FPLS_REQUIRE(rs.n_total >= n_local, "row-sharded fit: the all-reduce did not sum the row counts");
+  } catch (...) {
+    ctx.shards = nullptr;   // the destructor does not run when the constructor throws
+    throw;
+  }
+}
+
 }  // namespace fpls
 
 namespace fpls {

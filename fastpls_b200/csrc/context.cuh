@@ -75,6 +75,15 @@ struct Context {
   std::vector<StreamBuffer> splitk;
   double* splitk_workspace(cudaStream_t st, size_t elems);
 
+  // Row-sharded fit in progress (null otherwise): the caller's all-reduce
+  // and the row count over all ranks.
+  struct RowShards {
+    int (*fn)(double* buf, long long count, void* stream, void* user) = nullptr;
+    void* user = nullptr;
+    long long n_total = 0;
+  };
+  RowShards* shards = nullptr;
+
   static Context& get();       // initialises the device on first use
   void begin_call();           // resets the arena and the status flag, starts the call timer
   void end_call();             // stops the call timer (after the final synchronisation)
@@ -109,6 +118,26 @@ class PhaseTimer {
   bool on_ = false;
   bool reported_ = false;
   std::vector<std::pair<const char*, cudaEvent_t>> marks_;
+};
+
+// Row-sharded fits: each rank holds a block of the rows of X and Y, and every
+// sum over rows (column sums, X^T Y, X^T t, t^T t, Y^T t, T^T T, residual sums)
+// is completed by the caller's all-reduce.  shard_sum() sums a device buffer
+// over the ranks in place, ordered on the context stream; it does nothing when
+// no sharded fit is active.  Every rank makes the same calls in the same order.
+void shard_sum(double* buf, size_t count);
+// Rows over all ranks (the local count when not sharded).
+long long shard_rows(long long n_local);
+bool sharded();
+struct RowShardScope {
+  Context::RowShards rs;
+  Context& ctx;
+  // Sets the callback and sums the local row count over the ranks (the first
+  // all-reduce of every sharded fit).
+  RowShardScope(Context& c, int (*fn)(double*, long long, void*, void*), void* user, long long n_local);
+  ~RowShardScope() { ctx.shards = nullptr; }
+  RowShardScope(const RowShardScope&) = delete;
+  RowShardScope& operator=(const RowShardScope&) = delete;
 };
 
 // Host <-> device copies on the context stream (synchronous w.r.t. the caller

@@ -127,8 +127,52 @@ double read_scalar(const double* d) {
 
 }  // namespace
 
+// Row-sharded centre / scale: the column sums, the sums of the centred
+// columns and their squared deviations are summed over the ranks, so every
+// rank centres and scales with the statistics of all rows.  With one rank the
+// results are those of the unsharded path bit for bit (same loops, same order).
+static void center_scale_xy_sharded(double* X, int n, int p, double* Y, int m, int scaling, double* mX,
+                                    double* vX, double* mY) {
+  Context& ctx = Context::get();
+  const double nt = static_cast<double>(shard_rows(n));
+  const int my = Y ? m : 0;
+  double* buf = ctx.arena.alloc_n<double>((size_t)p + my);
+  dzero(buf, ((size_t)p + my) * sizeof(double));
+  if (scaling < 3) col_sum(X, n, p, n, buf);
+  if (Y) col_sum(Y, n, m, n, buf + p);
+  shard_sum(buf, (size_t)p + my);
+  if (scaling < 3) {
+    div_vec(buf, p, nt, false, mX);
+    center_scale(X, n, p, n, mX, nullptr);
+  } else {
+    fill(mX, p, 0.0);
+  }
+  if (Y) {
+    div_vec(buf + p, m, nt, false, mY);
+    center_scale(Y, n, m, n, mY, nullptr);
+  }
+  if (scaling == 2) {
+    // sd of the centred columns: their mean (zero up to rounding), then the
+    // squared deviations from it, divided by n - 1 (two passes, as col_sd_centered)
+    double* mu = ctx.arena.alloc_n<double>(p);
+    col_sum(X, n, p, n, mu);
+    shard_sum(mu, p);
+    div_vec(mu, p, nt, false, mu);
+    col_sqdev(X, n, p, n, mu, vX);
+    shard_sum(vX, p);
+    div_vec(vX, p, nt - 1.0, true, vX);
+    center_scale(X, n, p, n, nullptr, vX);
+  } else {
+    fill(vX, p, 1.0);
+  }
+}
+
 void center_scale_xy(double* X, int n, int p, double* Y, int m, int scaling, double* mX,
                      double* vX, double* mY) {
+  if (sharded()) {
+    center_scale_xy_sharded(X, n, p, Y, m, scaling, mX, vX, mY);
+    return;
+  }
   // src/fastPLS.cpp:4817-4834: mX = mean, X -= mX, vX = sd(X centred), X /= vX
   if (scaling < 3) {
     col_mean(X, n, p, n, mX);
@@ -151,11 +195,12 @@ void center_scale_xy(double* X, int n, int p, double* Y, int m, int scaling, dou
 int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
                         int L, int K0, const FitOptions& opt, const double* mY, PlssvdOut out) {
   Context& ctx = Context::get();
-  const int max_rank = std::min(n, std::min(p, m));
+  const int max_rank = static_cast<int>(std::min<long long>(shard_rows(n), std::min(p, m)));
   double* S = nullptr;
   if (!opt.xprod) {
     S = ctx.arena.alloc_n<double>((size_t)p * m);
     xgemm(true, p, m, n, X, n, Y, n, S, p);
+    shard_sum(S, (size_t)p * m);
   }
   int thr = 32;
   if (const char* e = std::getenv("FASTPLS_PLSSVD_SMALL_EXACT_MAX_RANK")) {
@@ -179,6 +224,7 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
   xgemm(false, n, keff, p, X, n, out.R, p, out.T, n);
   double* G = ctx.arena.alloc_n<double>((size_t)keff * keff);
   gemm(true, false, keff, keff, n, 1.0, out.T, n, out.T, n, 0.0, G, keff);
+  shard_sum(G, (size_t)keff * keff);
   dzero(out.C_latent, (size_t)K0 * K0 * L * sizeof(double));
   dzero(out.W_latent, (size_t)K0 * m * L * sizeof(double));
   double* D = ctx.arena.alloc_n<double>((size_t)keff * keff);
@@ -186,6 +232,7 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
   double* Wa = ctx.arena.alloc_n<double>((size_t)keff * m);
   double* Yf = opt.fit ? ctx.arena.alloc_n<double>((size_t)n * m) : nullptr;
   double* rq = ctx.arena.alloc_n<double>(2 * L);
+  const double* rq_mu = opt.fit ? shard_rq_means(Y, n, m) : nullptr;
   for (int a = 0; a < L; ++a) {
     const int mc = std::min(ncomp[a], keff);
     diag_kernel<<<1, 256, 0, ctx.stream>>>(D, mc, out.s); ::fpls::note_launch();
@@ -199,12 +246,13 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
     if (out.B) gemm(false, false, p, m, mc, 1.0, out.R, p, Wa, mc, 0.0, out.B + (size_t)a * p * m, p);
     if (opt.fit) {
       gemm(false, false, n, m, mc, 1.0, out.T, n, Wa, mc, 0.0, Yf, n);
-      rq_sums(Y, Yf, n, m, rq + 2 * a);
+      rq_sums(Y, Yf, n, m, rq + 2 * a, rq_mu);
       add_row_vector(Yf, n, m, n, mY);
       d2d(out.Yfit + (size_t)a * n * m, Yf, (size_t)n * m * sizeof(double));
     }
   }
   if (opt.fit) {
+    shard_sum(rq, 2 * (size_t)L);
     std::vector<double> h(2 * L);
     d2h(h.data(), rq, 2 * L * sizeof(double));
     ctx.sync();

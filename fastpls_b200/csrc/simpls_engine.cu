@@ -437,6 +437,47 @@ __global__ void k_crosscov_finish(Eng e, const double* P) {
   }
 }
 
+// Row-sharded fits: after X^T T, the loading P (p x F), the score sums
+// (t^T t, sum t: F x 2) and Y^T t (F x m) are rank-local partial sums.  Pack
+// folds the row-chunk partials in chunk order into one buffer [P | t | q];
+// after the all-reduce, unpack puts the totals in chunk 0 (the other chunks
+// zero), so the kernels that follow read sums over all ranks' rows.
+__global__ void k_shard_pack(Eng e, double* __restrict__ red) {
+  const size_t np = (size_t)e.F * e.p, nt = (size_t)e.F * 2, nq = (size_t)e.F * e.m;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < np + nt + nq;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (i < np) {
+      red[i] = e.P[i];
+    } else if (i < np + nt) {
+      const size_t k = i - np, f = k / 2, c2 = k % 2;
+      double s = 0.0;
+      for (int c = 0; c < e.cn; ++c) s += e.tpart[(f * e.cn + c) * 2 + c2];
+      red[i] = s;
+    } else {
+      const size_t k = i - np - nt, f = k / e.m, j = k % e.m;
+      double s = 0.0;
+      for (int c = 0; c < e.cn; ++c) s += e.qpart[(f * e.cn + c) * e.m + j];
+      red[i] = s;
+    }
+  }
+}
+
+__global__ void k_shard_unpack(Eng e, const double* __restrict__ red) {
+  const size_t np = (size_t)e.F * e.p, nt = (size_t)e.F * e.cn * 2, nq = (size_t)e.F * e.cn * e.m;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < np + nt + nq;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (i < np) {
+      e.P[i] = red[i];
+    } else if (i < np + nt) {
+      const size_t k = i - np, f = k / (2 * (size_t)e.cn), c = (k / 2) % e.cn, c2 = k % 2;
+      e.tpart[k] = c == 0 ? red[np + f * 2 + c2] : 0.0;
+    } else {
+      const size_t k = i - np - nt, f = k / ((size_t)e.cn * e.m), c = (k / e.m) % e.cn, j = k % e.m;
+      e.qpart[k] = c == 0 ? red[np + (size_t)e.F * 2 + f * e.m + j] : 0.0;
+    }
+  }
+}
+
 Eng make_eng(const SimplsBatch& b) {
   Eng e{};
   e.n = b.n; e.p = b.p; e.m = b.m; e.F = b.F; e.K = b.K;
@@ -513,6 +554,13 @@ void simpls_batch_run(const SimplsBatch& b) {
   dzero(b.V, F * b.p * b.K * sizeof(double));
   dzero(b.tnorm, F * b.K * sizeof(double));
   const dim3 gp(e.cp, b.F), gn(e.cn, b.F);
+  // all-reduce buffer of a row-sharded fit: [P (F x p) | t^T t, sum t (F x 2) | Y^T t (F x m)]
+  const size_t shard_count = sharded() ? F * ((size_t)b.p + 2 + b.m) : 0;
+  double* shard_red = shard_count ? ar.alloc_n<double>(shard_count) : nullptr;
+  const unsigned shard_grid =
+      shard_count ? (unsigned)std::min<size_t>(ceil_div(F * ((size_t)b.p + e.cn * (2 + (size_t)b.m)), kThreads),
+                                               (size_t)ctx.sm_count * 8)
+                  : 1u;
   const size_t sm_m = std::max<size_t>(b.m, 1) * sizeof(double);
   const size_t sm_k = std::max<size_t>(b.K, 1) * sizeof(double);
   cudaStream_t st = ctx.stream;
@@ -549,6 +597,13 @@ void simpls_batch_run(const SimplsBatch& b) {
     FPLS_CHECK_LAUNCH();
     mark("scores");
     b.X->t_times(e.T, b.F, e.P);
+    if (shard_red) {
+      k_shard_pack<<<shard_grid, kThreads, 0, st>>>(e, shard_red); ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+      shard_sum(shard_red, shard_count);
+      k_shard_unpack<<<shard_grid, kThreads, 0, st>>>(e, shard_red); ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+    }
     mark("X^T*T");
     k_loading<<<gp, kThreads, 0, st>>>(e, a); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();

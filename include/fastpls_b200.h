@@ -129,6 +129,43 @@ int fpls_pls_model2_fast(const double* X, int n, int p, const double* Y, int m, 
                          double* vX, double* mY, double* B, double* Yfit, double* R2Y,
                          int* n_components, char* err, size_t errlen);
 
+/* Row-sharded fits (one process per GPU, each holding a block of the rows of
+ * X and Y).  Every sum over rows -- the column sums of the centring (and the
+ * sums of squares for scaling 2), S = XᵀY, per component Xᵀt, tᵀt and Yᵀt
+ * (fast SIMPLS) or TᵀT (PLSSVD), and the residual sums of R2Y -- is completed
+ * by `allreduce`, which must sum `count` doubles of device memory at `buf`
+ * over all ranks in place.  `stream` is the library's cudaStream_t: the sum
+ * must see the work already enqueued on it and finish before the work
+ * enqueued after it (enqueue the collective on that stream, or synchronise
+ * it).  Every rank calls the fit with the same p, m, ncomp, scaling, fit,
+ * seed and SVD options, and the library makes the same calls in the same
+ * order on every rank; the first sums the local row counts.  Return 0 on
+ * success; any other value fails the fit with FPLS_ERR_CUDA (the other ranks
+ * then wait in their next all-reduce: give the process group a timeout).
+ * With one rank the outputs are the unsharded fit's, bit for bit. */
+typedef int (*fpls_allreduce_fn)(double* buf, long long count, void* stream, void* user);
+
+/* fpls_pls_model1 over this rank's n rows.  The model (C_latent, W_latent, Q,
+ * R, mX, vX, mY, B, R2Y, s, ncomp_out, k_eff) is the fit of all ranks' rows
+ * and is the same on every rank; Ttrain and Yfit are this rank's rows.
+ * min(n, p, m) caps use the total row count.  Row sharding of
+ * fastPLS.cpp:4780-4986 (the S all-reduce and the T^T T all-reduce). */
+int fpls_pls_model1_rows(const double* X, int n, int p, const double* Y, int m, const int* ncomp, int L,
+                         int scaling, int fit, int svd_method, int oversample, int power_iters,
+                         double svds_tol, int seed, fpls_allreduce_fn allreduce, void* user, int* ncomp_out,
+                         double* C_latent, double* W_latent, double* Q, double* Ttrain, double* R, double* mX,
+                         double* vX, double* mY, double* B, double* Yfit, double* R2Y, double* s, int* k_eff,
+                         char* err, size_t errlen);
+
+/* fpls_pls_model2_fast over this rank's n rows: one all-reduce of
+ * [Xᵀt | tᵀt, Σt | Yᵀt] (p + 2 + m doubles) per component.  R, Q, mX, vX, mY,
+ * B, R2Y and n_components are the fit of all ranks' rows; Yfit is this
+ * rank's rows.  Row sharding of fastPLS.cpp:2454-2778. */
+int fpls_pls_model2_fast_rows(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
+                              int L, int scaling, int fit, int seed, fpls_allreduce_fn allreduce, void* user,
+                              double* R, double* Q, double* mX, double* vX, double* mY, double* B,
+                              double* Yfit, double* R2Y, int* n_components, char* err, size_t errlen);
+
 /* Classic SIMPLS with a fresh leading left singular vector per component
  * ("exact" mode when svd_method = 3).  K = max(ncomp).  Outputs: R p x K,
  * Q m x K, P p x K (optional), Ttrain n x K (optional; required when fit=1),

@@ -27,7 +27,9 @@ def test_tuned_grid_reproduces_default(lib, autotune, precision):
     nc = np.arange(1, 9)
     kw = dict(seed=1, precision=precision, return_inner=True)
     tuned = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)
-    rep = [r for r in lib.autotune_report() if r["n"] == d["X"].shape[0] and r["p"] == d["X"].shape[1]]
+    code = lib.PREC[precision]
+    rep = [r for r in lib.autotune_report()
+           if r["n"] == d["X"].shape[0] and r["p"] == d["X"].shape[1] and r["precision"] == code]
     assert len(rep) == 1
     r = rep[0]
     assert r["fits"] == 4 * (3 + 1) and r["kmax"] == 8
@@ -35,7 +37,8 @@ def test_tuned_grid_reproduces_default(lib, autotune, precision):
     chosen = [c for c in r["candidates"] if c["config"] == r["chosen"]]
     assert chosen and chosen[0]["same_results"]
     again = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)   # cached: no new entry
-    assert len([x for x in lib.autotune_report() if x["n"] == d["X"].shape[0]]) == 1
+    assert len([x for x in lib.autotune_report()
+                if x["n"] == d["X"].shape[0] and x["precision"] == code]) == 1
     lib.set_autotune(False)
     default = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)
     for res in (tuned, again):
@@ -55,7 +58,7 @@ def test_tuned_int8_grid_keeps_its_class_scores(lib, autotune):
     lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)   # tunes the shape
     kw["return_scores"] = True
     tuned = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], **kw)   # runs it tuned
-    r = [x for x in lib.autotune_report() if x["n"] == 350][0]
+    r = [x for x in lib.autotune_report() if x["n"] == 350 and x["precision"] == lib.PREC["int8"]][0]
     assert all(c["config"]["ozaki_slices"] == r["candidates"][0]["config"]["ozaki_slices"]
                for c in r["candidates"])
     lib.set_autotune(False)

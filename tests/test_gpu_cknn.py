@@ -82,11 +82,13 @@ def test_candidate_knn_wide_scores(lib):
     _check(got, ref)
 
 
+@pytest.mark.parametrize("buffers", ["2", "3"])
 @pytest.mark.parametrize("kdim", [9, 24, 100])
-def test_candidate_knn_staged_tiles_match_oracle(lib, monkeypatch, kdim):
-    # the staged similarity-tile kernel (FASTPLS_CKNN_TILES=2) gives the oracle's
-    # neighbours too, for odd, small and wide score spaces
-    monkeypatch.setenv("FASTPLS_CKNN_TILES", "2")
+def test_candidate_knn_staged_tiles_match_oracle(lib, monkeypatch, kdim, buffers):
+    # the staged similarity-tile kernel (FASTPLS_CKNN_TILES=2: two training-row
+    # buffers; 3: one buffer, two CTAs per SM) gives the oracle's neighbours too,
+    # for odd, small and wide score spaces
+    monkeypatch.setenv("FASTPLS_CKNN_TILES", buffers)
     Tr, y, Tt = _zipf_case(14 + kdim, 6000, 150, 30, kdim)
     cents = ok.centroids(Tr, y, 30)
     got = lib.candidate_knn_predict(Tt, Tr, y, cents, top_k=5, top_m=12, knn_k=10, tau=0.2, alpha=0.75)

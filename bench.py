@@ -171,7 +171,8 @@ KERNEL_CLASSES = {
     "split_gemm_bf16x6": ("bf16", "split_gemm_kernel<3, 64> (tcgen05 BF16x6 split GEMM)", None),
     "gemm_f64_dmma": ("fp64", "gemm_f64_dmma (FP64 DMMA m8n8k4 tiles)", None),
     "gemv_f64": (None, "gemv_n / gemv_t (FP64 matrix-vector passes over X)", None),
-    "cknn_tiles": ("fp64", "knn_tile_kernel (class-grouped 64x64 FP64 DMMA similarity tiles, top-k epilogue)",
+    "cknn_tiles": ("fp64", "knn_tile_kernel_v2<1> (class-grouped 64x64 FP64 DMMA similarity tiles, contraction "
+                           "staged in shared memory, two CTAs per SM, top-k epilogue)",
                    None),
 }
 

@@ -712,13 +712,18 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
     // stride of the staged rows: K rounded up to 4, then to 4 mod 16
     const int KP = (kdim + 3) / 4 * 4;
     const int S = KP + (4 - KP % 16 + 16) % 16;
-    // The staged kernel (FASTPLS_CKNN_TILES=2) measured 162.6 ms against the
-    // 16-wide k-step kernel's 123.3 ms on the large-class workload: with one
-    // 8-warp CTA per SM the tensor pipe idles while half the warps run the
-    // top-k epilogue; the k-step kernel, two CTAs per SM, stays the default.
+    // Kernel choice (FASTPLS_CKNN_TILES: 1 the 16-wide k-step kernel, 2 the
+    // staged kernel with two training-row buffers, 3 or unset the staged
+    // kernel with one buffer).  On the large-class workload (K = 100) the
+    // similarity tiles took 123.4 ms (k-step), 162.6 ms (two buffers: one
+    // 8-warp CTA per SM, the tensor pipe idles while the top-k epilogue runs)
+    // and 107.2 ms (one buffer: two CTAs per SM, one CTA's epilogue overlapping
+    // the other's products).  Staged rows wider than 116 doubles take the
+    // k-step kernel.
     const char* tv = std::getenv("FASTPLS_CKNN_TILES");
-    if (S <= kV2MaxStride && tv && (tv[0] == '2' || tv[0] == '3')) {
-      const int nb = tv[0] == '2' ? 2 : 1;
+    const char sel = (tv && tv[0]) ? tv[0] : '3';
+    if (S <= kV2MaxStride && (sel == '2' || sel == '3')) {
+      const int nb = sel == '2' ? 2 : 1;
       const size_t smem = sizeof(double) * ((size_t)kTileM * S + nb * (size_t)kTileN * std::max(S, kTileN + 1) +
                                             (size_t)use_k * 2 * kTileM);
       const int smem_max = (int)(sizeof(double) * ((size_t)(kTileM + nb * kTileN) * kV2MaxStride +

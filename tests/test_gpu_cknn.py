@@ -71,9 +71,11 @@ def test_candidate_knn_bias_small_classes_and_clamps(lib):
     _check(got, ref)
 
 
-def test_candidate_knn_wide_scores(lib):
-    # kdim > 16 * several K-blocks and a test count that is not a tile multiple
-    Tr, y, Tt = _zipf_case(13, 5000, 131, 25, 100)
+@pytest.mark.parametrize("kdim", [100, 150])
+def test_candidate_knn_wide_scores(lib, kdim):
+    # kdim > 16 * several K-blocks and a test count that is not a tile multiple;
+    # 150 is past the staged kernels' 116-wide rows (the k-step kernel runs)
+    Tr, y, Tt = _zipf_case(13, 5000, 131, 25, kdim)
     cents = ok.centroids(Tr, y, 25)
     got = lib.candidate_knn_predict(Tt, Tr, y, cents, top_k=5, top_m=10, knn_k=10, tau=0.2,
                                     alpha=0.75)
@@ -82,12 +84,13 @@ def test_candidate_knn_wide_scores(lib):
     _check(got, ref)
 
 
-@pytest.mark.parametrize("buffers", ["2", "3"])
+@pytest.mark.parametrize("buffers", ["1", "2", "3"])
 @pytest.mark.parametrize("kdim", [9, 24, 100])
 def test_candidate_knn_staged_tiles_match_oracle(lib, monkeypatch, kdim, buffers):
-    # the staged similarity-tile kernel (FASTPLS_CKNN_TILES=2: two training-row
-    # buffers; 3: one buffer, two CTAs per SM) gives the oracle's neighbours too,
-    # for odd, small and wide score spaces
+    # every similarity-tile kernel (FASTPLS_CKNN_TILES=1: 16-wide k-steps;
+    # 2: contraction staged, two training-row buffers; 3, the default: one
+    # buffer, two CTAs per SM) gives the oracle's neighbours, for odd, small
+    # and wide score spaces
     monkeypatch.setenv("FASTPLS_CKNN_TILES", buffers)
     Tr, y, Tt = _zipf_case(14 + kdim, 6000, 150, 30, kdim)
     cents = ok.centroids(Tr, y, 30)

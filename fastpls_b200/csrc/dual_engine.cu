@@ -59,6 +59,7 @@ struct DualEng {
   double* Tkeep;
   int* ncomp_done;
   int* status;
+  int prefetch;  // request the launch's later operands into L2 at its start
 };
 
 constexpr int kRedMax = kMaxK > kMaxM + 3 ? kMaxK : kMaxM + 3;
@@ -739,6 +740,18 @@ static __device__ void run(const DualEng& e, int a) {
   // coefficients of component a - 1, C_V^T K c_p = (K C_V)^T c_p (K is
   // symmetric), are reduced while the product finishes.
   if (__ldcg(e.status + f)) return;   // set only in earlier launches: uniform over the cluster
+  if (e.prefetch && a > 0) {
+    // This CTA's rows of the columns its later phases read (C_V for the
+    // Gram-Schmidt update, C_S and K C_S for the reduction and the
+    // deflation), requested into L2 while the coefficients are reduced.
+    const int ncv = a - 1, tot = ncv + 2 * e.m;
+    for (int q = threadIdx.x; q < tot; q += kT) {
+      const double* col = q < ncv ? e.CV + ((size_t)f * e.K + q) * e.n
+                                  : (q < ncv + e.m ? e.CS + ((size_t)f * e.m + (q - ncv)) * e.n
+                                                   : e.KCS + ((size_t)f * e.m + (q - ncv - e.m)) * e.n);
+      tc::l2_prefetch_range(col + rw.r0, (size_t)rw.nl * sizeof(double));
+    }
+  }
   if (threadIdx.x == 0) R.buf = 0;
   __syncthreads();
   double cv[kLR];
@@ -859,6 +872,65 @@ static bool dual_merge_enabled() {
   return active_tune().merge != 0;
 }
 
+// FASTPLS_LOOP_GRAPH=0 enqueues the component loop launch by launch instead of
+// as one CUDA graph.
+static bool loop_graph_enabled() {
+  static const int v = [] {
+    const char* e = std::getenv("FASTPLS_LOOP_GRAPH");
+    return e ? (e[0] != '0' ? 1 : 0) : 1;
+  }();
+  return v != 0;
+}
+
+// The executable graph of the last captured component loop.  Each call
+// captures its loop afresh and updates this graph in place when the topology
+// matches (same launches, new parameters), else instantiates a new one; an
+// update does not touch launches of the graph already in flight.
+static cudaGraphExec_t g_loop_exec = nullptr;
+
+template <typename Loop>
+static void launch_as_graph(cudaStream_t st, Loop&& loop) {
+  FPLS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaGraph_t graph = nullptr;
+  try {
+    loop();
+  } catch (...) {
+    cudaStreamEndCapture(st, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    throw;
+  }
+  FPLS_CUDA(cudaStreamEndCapture(st, &graph));
+  bool updated = false;
+  if (g_loop_exec) {
+    cudaGraphExecUpdateResultInfo info;
+    updated = cudaGraphExecUpdate(g_loop_exec, graph, &info) == cudaSuccess;
+    if (!updated) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(g_loop_exec);
+      g_loop_exec = nullptr;
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if (!updated) e = cudaGraphInstantiate(&g_loop_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    g_loop_exec = nullptr;
+    FPLS_CUDA(e);
+  }
+  FPLS_CUDA(cudaGraphLaunch(g_loop_exec, st));
+}
+
+// FASTPLS_STEP_PREFETCH=1: each step CTA requests the columns its later
+// phases read into L2 at the launch's start.
+static bool dual_prefetch_enabled() {
+  static const int v = [] {
+    const char* e = std::getenv("FASTPLS_STEP_PREFETCH");
+    return e ? (e[0] != '0' ? 1 : 0) : 0;
+  }();
+  return v != 0;
+}
+
 bool dual_engine_applies(int n, int p, int m, int K) {
   if (const char* e = std::getenv("FASTPLS_DUAL"))
     if (e[0] == '0') return false;
@@ -875,6 +947,7 @@ void dual_simpls_run(const DualBatch& b) {
   e.m1 = b.m1_mode ? 1 : 0;
   e.center = b.center ? 1 : 0;
   e.merge = (!e.m1 && e.iters >= 1 && e.m <= kFuseM && dual_merge_enabled()) ? 1 : 0;
+  e.prefetch = dual_prefetch_enabled() ? 1 : 0;
   e.x0 = b.x0; e.XOmega = b.XOmega; e.mask = b.mask; e.labels = b.labels; e.mY_all = b.mY_all; e.dY = b.dY;
   e.Q = b.Q; e.tnorm = b.tnorm; e.Tkeep = b.Tkeep; e.ncomp_done = b.ncomp_done; e.status = b.status;
   const size_t F = b.F, n = b.n, m = b.m, K = b.K;
@@ -913,6 +986,13 @@ void dual_simpls_run(const DualBatch& b) {
   PhaseTimer pt("dual SIMPLS engine");
   const double nd = static_cast<double>(n), md = static_cast<double>(m), Fd = static_cast<double>(F);
   const double it = static_cast<double>(e.iters);
+  // With INT8 K products the component loop is captured as one CUDA graph
+  // (not while the kernel-class profiler or the phase trace records events
+  // between its launches); the product's plan and kernel attribute are made
+  // before the capture, which then holds launches only.
+  const bool graph = b.kop_int8_slices > 0 && loop_graph_enabled() && !ctx.profile && !pt.enabled();
+  if (graph) ozaki_sym_prepare_partials(*b.Kop, cpP);
+  auto loop = [&]() {
   for (int a = 0; a <= b.K; ++a) {
     // algorithmic bytes of one step launch (all fits): the Gram-Schmidt and
     // deflation of component a - 1 and the refresh / scores of component a
@@ -949,7 +1029,15 @@ void dual_simpls_run(const DualBatch& b) {
     }
     pt.mark("K products");
   }
+  };
+  if (graph) launch_as_graph(st, loop);
+  else loop();
   pt.report();
+}
+
+void dual_release_graph() {
+  if (g_loop_exec) cudaGraphExecDestroy(g_loop_exec);
+  g_loop_exec = nullptr;
 }
 
 }  // namespace fpls

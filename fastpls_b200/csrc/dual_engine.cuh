@@ -53,6 +53,9 @@ struct DualBatch {
 // Runs K components for all fits; launches only (no host synchronisation).
 void dual_simpls_run(const DualBatch& b);
 
+// Frees the executable graph of the component loop (fpls_reset_workspace).
+void dual_release_graph();
+
 // True when the dual form applies to this shape (and fits its staging limits).
 bool dual_engine_applies(int n, int p, int m, int K);
 

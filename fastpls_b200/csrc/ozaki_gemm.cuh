@@ -81,9 +81,12 @@ std::unique_ptr<XOperator> make_ozaki_sym_operator(const double* K, int n, int s
 OzakiPartials ozaki_sym_times_partials(XOperator& op, const double* M, int F);
 // The same with the planes of M already made (rows = the F columns, k = n).
 OzakiPartials ozaki_sym_partials_from_planes(XOperator& op, const OzakiPlanes& b);
+// Makes the plan (and kernel attribute) of those partial products ahead of
+// time, so that later calls enqueue launches only (stream capture).
+void ozaki_sym_prepare_partials(XOperator& op, const OzakiPlanes& b);
 
 // Slice count of the mixed-precision row-space products (environment
-// FASTPLS_OZAKI_SLICES, else 6).
+// FASTPLS_OZAKI_SLICES, else the tuned or built-in default of 5).
 int ozaki_default_slices();
 
 }  // namespace fpls

@@ -59,7 +59,6 @@ struct DualEng {
   double* Tkeep;
   int* ncomp_done;
   int* status;
-  int prefetch;  // request the launch's later operands into L2 at its start
 };
 
 constexpr int kRedMax = kMaxK > kMaxM + 3 ? kMaxK : kMaxM + 3;
@@ -740,18 +739,6 @@ static __device__ void run(const DualEng& e, int a) {
   // coefficients of component a - 1, C_V^T K c_p = (K C_V)^T c_p (K is
   // symmetric), are reduced while the product finishes.
   if (__ldcg(e.status + f)) return;   // set only in earlier launches: uniform over the cluster
-  if (e.prefetch && a > 0) {
-    // This CTA's rows of the columns its later phases read (C_V for the
-    // Gram-Schmidt update, C_S and K C_S for the reduction and the
-    // deflation), requested into L2 while the coefficients are reduced.
-    const int ncv = a - 1, tot = ncv + 2 * e.m;
-    for (int q = threadIdx.x; q < tot; q += kT) {
-      const double* col = q < ncv ? e.CV + ((size_t)f * e.K + q) * e.n
-                                  : (q < ncv + e.m ? e.CS + ((size_t)f * e.m + (q - ncv)) * e.n
-                                                   : e.KCS + ((size_t)f * e.m + (q - ncv - e.m)) * e.n);
-      tc::l2_prefetch_range(col + rw.r0, (size_t)rw.nl * sizeof(double));
-    }
-  }
   if (threadIdx.x == 0) R.buf = 0;
   __syncthreads();
   double cv[kLR];
@@ -921,16 +908,6 @@ static void launch_as_graph(cudaStream_t st, Loop&& loop) {
   FPLS_CUDA(cudaGraphLaunch(g_loop_exec, st));
 }
 
-// FASTPLS_STEP_PREFETCH=1: each step CTA requests the columns its later
-// phases read into L2 at the launch's start.
-static bool dual_prefetch_enabled() {
-  static const int v = [] {
-    const char* e = std::getenv("FASTPLS_STEP_PREFETCH");
-    return e ? (e[0] != '0' ? 1 : 0) : 0;
-  }();
-  return v != 0;
-}
-
 bool dual_engine_applies(int n, int p, int m, int K) {
   if (const char* e = std::getenv("FASTPLS_DUAL"))
     if (e[0] == '0') return false;
@@ -947,7 +924,6 @@ void dual_simpls_run(const DualBatch& b) {
   e.m1 = b.m1_mode ? 1 : 0;
   e.center = b.center ? 1 : 0;
   e.merge = (!e.m1 && e.iters >= 1 && e.m <= kFuseM && dual_merge_enabled()) ? 1 : 0;
-  e.prefetch = dual_prefetch_enabled() ? 1 : 0;
   e.x0 = b.x0; e.XOmega = b.XOmega; e.mask = b.mask; e.labels = b.labels; e.mY_all = b.mY_all; e.dY = b.dY;
   e.Q = b.Q; e.tnorm = b.tnorm; e.Tkeep = b.Tkeep; e.ncomp_done = b.ncomp_done; e.status = b.status;
   const size_t F = b.F, n = b.n, m = b.m, K = b.K;

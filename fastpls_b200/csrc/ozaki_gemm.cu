@@ -124,7 +124,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
                   const double* __restrict__ sB, const int4* __restrict__ segs,
                   const int* __restrict__ cta_seg_begin, const int* __restrict__ tile_seg, int n_tiles_n,
                   double* __restrict__ part, double* __restrict__ C, int ldc, int M, int N, int* err,
-                  int a_static, int prefetch) {
+                  int a_static) {
   __shared__ int epi_fail;   // raised by any epilogue warp whose wait gave up
   using L = OzLayout<S>;
   extern __shared__ uint8_t smem_raw[];
@@ -180,20 +180,6 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
   // the segment table is written when the plan is made: read before the wait
   int4 seg0 = make_int4(0, 0, 0, 0);
   if (lane == 0 && warp < 2 && sbeg < send) seg0 = segs[sbeg];
-  // With prefetch (and static A planes), warp 0 asks for every A-plane tile of
-  // the CTA's later K blocks to be brought into L2 now, so that the loads of
-  // those blocks find them there instead of starting a DRAM round trip each.
-  if (prefetch && a_static && warp == 0) {
-    int idx = 0;
-    for (int sg = sbeg; sg < send; ++sg) {
-      const int4 seg = segs[sg];
-      const int mt = seg.x / n_tiles_n;
-      for (int kb = seg.y; kb < seg.z; ++kb)
-        for (int s = 0; s < S; ++s, ++idx)
-          if ((sg != sbeg || kb != seg.y) && (idx & 31) == lane)
-            tc::tma_prefetch_2d(&mA, kb * OBK, s * a_rows_pad + mt * OBM);
-    }
-  }
   const bool pre_a = a_static && warp == 0 && lane == 0 && sbeg < send;
   if (pre_a) {
     const int4 seg = seg0;
@@ -698,16 +684,6 @@ CUtensorMap make_plane_map(const OzakiPlanes& p, int box_rows) {
   return m;
 }
 
-// FASTPLS_OZ_PREFETCH=1: the product kernel requests the static A planes of
-// its later K blocks into L2 at its start.
-bool ozaki_prefetch_enabled() {
-  static const int v = [] {
-    const char* e = std::getenv("FASTPLS_OZ_PREFETCH");
-    return e ? (e[0] != '0' ? 1 : 0) : 0;
-  }();
-  return v != 0;
-}
-
 template <int S>
 void ensure_ozaki_attr() {
   static bool attr = false;
@@ -746,7 +722,7 @@ void launch_ozaki(const CUtensorMap& mA, const CUtensorMap& mB, const OzakiPlane
                                static_cast<const double*>(A.scale), static_cast<const double*>(B.scale),
                                static_cast<const int4*>(c.segs), static_cast<const int*>(c.cta_begin),
                                static_cast<const int*>(c.tile_begin), ntn, c.part, C, ldc, m_rows, n_rows, err,
-                               a_static ? 1 : 0, ozaki_prefetch_enabled() ? 1 : 0));
+                               a_static ? 1 : 0));
 }
 
 struct XOperatorOzakiSym : public XOperator {

@@ -68,24 +68,6 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint32_t dst
       : "memory");
 }
 
-// Asks for the tile a 2-D tensor-map load at (x, y) would copy to be brought
-// into L2 (no shared memory, no completion to wait for).
-__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
-  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];"
-               ::"l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y)
-               : "memory");
-}
-
-// Asks for the 16-byte aligned part of [p, p + bytes) to be brought into L2.
-__device__ __forceinline__ void l2_prefetch_range(const void* p, size_t bytes) {
-  const uintptr_t a = (reinterpret_cast<uintptr_t>(p) + 15) & ~static_cast<uintptr_t>(15);
-  const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + bytes) & ~static_cast<uintptr_t>(15);
-  if (e > a)
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(static_cast<uint64_t>(a)),
-                 "r"(static_cast<uint32_t>(e - a))
-                 : "memory");
-}
-
 // UMMA shared-memory descriptor: K-major, SWIZZLE_128B (128-byte rows), 8-row
 // core groups 1024 B apart.
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {

@@ -174,6 +174,9 @@ KERNEL_CLASSES = {
     "cknn_tiles": ("fp64", "knn_tile_kernel_v2<1> (class-grouped 64x64 FP64 DMMA similarity tiles, contraction "
                            "staged in shared memory, two CTAs per SM, top-k epilogue)",
                    None),
+    "cknn_filter": ("bf16", "knn_filter_kernel<1, 2> (class-grouped 128x128 tcgen05 BF16x3 similarity tiles: "
+                            "approximate top-k pass, bar per pair, pass with exact FP64 rescoring of the rows "
+                            "within the error bound; TFLOP/s of the BF16 products of both passes)", None),
 }
 
 
@@ -550,6 +553,11 @@ def config_c3(lib, args, peaks, local):
     k = kw["ncomp"]
     knn = next((c for c in kr if c["kernel"].startswith("knn_tile")), None)
     F_knn = knn["algorithmic_flops_per_launch"] if knn else 0.0
+    filt = next((c for c in kr if c["kernel"].startswith("knn_filter")), None)
+    if filt:
+        # FP64-equivalent work of the similarity tiles: one kdim-long dot per
+        # (candidate pair, class row), a sixth of the BF16 products counted
+        F_knn = filt["algorithmic_flops_per_launch"] / 6.0
     F = n * p + 2.0 * n * p * k + 2.0 * n * k * k + F_knn + 2.0 * nt * k * C + 2.0 * nt * p * k
     B = 2.0 * n * p * 4 + nt * p * 4
     out = dict(workload="C3 label-aware PLSSVD + cKNN 1.2Mx768 fp32, 1000 Zipf(1.1) classes, ncomp 100 (rSVD "

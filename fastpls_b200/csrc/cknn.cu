@@ -24,10 +24,13 @@
 #include <limits>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "blas_f64.cuh"
 #include "capi_util.cuh"
 #include "cknn.cuh"
 #include "context.cuh"
+#include "tc_util.cuh"
 
 namespace fpls {
 namespace {
@@ -485,6 +488,381 @@ knn_tile_kernel_v2(const KnnItem* __restrict__ items, KnnClassInfo ci, const int
   }
 }
 
+// ----------------------------------------------------- tensor-core filter
+// The same (class, pair tile, training chunk) items on the BF16 tensor cores,
+// with results equal to the FP64 tiles':
+//   pass 1  128 pairs x 128 training rows of approximate similarities per
+//           tile: both score rows split into BF16 planes hi = bf16(x),
+//           lo = bf16(x - hi), three products hi.hi + hi.lo + lo.hi
+//           (tcgen05.mma kind::f16, M128 N128 K16, FP32 accumulation in TMEM,
+//           double-buffered so the epilogue overlaps the next tile); each pair
+//           keeps the top k of its approximate values per chunk;
+//   bar     per pair, theta = the k-th largest approximate value over all its
+//           chunks.  Every approximate value is within
+//           eps = 2^-10 |x| max|y| of the exact dot (the dropped split terms
+//           are below 3 2^-18 |x||y| and the FP32 accumulation of 3 x 128
+//           products below 384 2^-23 sum|x_k y_k| <= 2^-14.4 |x||y|), so each
+//           row of the pair's exact top k has an approximate value of at least
+//           theta - 2 eps;
+//   pass 2  the same products again; every training row whose approximate
+//           value reaches that bar is scored exactly (FP64 dot of the two score
+//           rows) and folded into the pair's top-k list, which is what the
+//           FP64 tiles write and knn_merge_kernel reads.
+// Score rows up to 128 wide, neighbour lists up to 16 long.  Warp 0 loads
+// (TMA, SWIZZLE_128B boxes of 64 x 128 BF16: the A tile once, the B tiles
+// through two stages), warp 1 issues the MMAs, warps 2..5 are the epilogue
+// (one pair row per thread).  Every mbarrier wait is bounded; no cluster
+// multicast.
+constexpr int kFT = 128;                  // pairs per tile = training rows per tile
+constexpr int kFK = 128;                  // contraction width (rows zero padded)
+constexpr int kFBox = 64 * kFT * 2;       // one 64-wide box of 128 BF16 rows: 16 KB
+constexpr int kFOperand = 4 * kFBox;      // two planes x two boxes: 64 KB
+constexpr int kFEpiWarps = 8;             // two per TMEM lane quarter, half the columns each
+constexpr int kFThreads = 64 + 32 * kFEpiWarps;
+constexpr int kFBarOff = 3 * kFOperand;   // A, then two B stages
+constexpr int kFList = 16;                // list length the filter keeps (use_k <= 16)
+constexpr int kFCandOff = kFBarOff + 256;  // pass 2: 16 candidate rows per epilogue thread
+constexpr int kFSmem = kFCandOff + 16 * 32 * kFEpiWarps * 4 + 1024;
+constexpr uint32_t kFIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kFT >> 3) << 17) |
+                             (uint32_t(kFT >> 4) << 24);
+static_assert(kFSmem <= 227 * 1024, "filter tiles exceed shared memory");
+
+__device__ __forceinline__ void umma_bf16_f32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kFIdesc), "r"(acc)
+      : "memory");
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(kFThreads, 1)
+knn_filter_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                  const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
+                  const KnnItem* __restrict__ items, KnnClassInfo ci, const int* __restrict__ pairs, int ntest,
+                  const double* __restrict__ Tq, const double* __restrict__ Ts, int K, int use_k,
+                  float* __restrict__ apart, const float* __restrict__ bar, double* __restrict__ part,
+                  int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~static_cast<uintptr_t>(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kFBarOff);
+  uint64_t* fullA = bars;
+  uint64_t* full = bars + 1;     // [2]
+  uint64_t* empty = bars + 3;    // [2]
+  uint64_t* tfull = bars + 5;    // [2]
+  uint64_t* tempty = bars + 7;   // [2]
+  uint64_t* done = bars + 9;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  const KnnItem it = items[blockIdx.x];
+  const int c = it.cls;
+  const int p0 = ci.pair_offs[c] + it.tile * kFT;
+  const int np = min(kFT, ci.pair_offs[c + 1] - p0);
+  const int r0 = ci.row_offs[c] + it.chunk * ci.chunk_rows[c];
+  const int r1 = min(ci.row_offs[c + 1], r0 + ci.chunk_rows[c]);
+  const int ntiles = (r1 - r0 + kFT - 1) / kFT;
+
+  if (threadIdx.x == 0) {
+    tc::mbar_init(tc::smem_u32(fullA), 1);
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(tc::smem_u32(&full[b]), 1);
+      tc::mbar_init(tc::smem_u32(&empty[b]), 1);
+      tc::mbar_init(tc::smem_u32(&tfull[b]), 1);
+      tc::mbar_init(tc::smem_u32(&tempty[b]), 32 * kFEpiWarps);
+    }
+    tc::mbar_init(tc::smem_u32(done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(tmem_slot)),
+                 "r"(2 * kFT)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------------------------------------------------- producer
+    const uint32_t sa = tc::smem_u32(smem);
+    tc::mbar_expect_tx(tc::smem_u32(fullA), kFOperand);
+    tc::tma_load_2d(&mAh, sa, tc::smem_u32(fullA), 0, p0);
+    tc::tma_load_2d(&mAh, sa + kFBox, tc::smem_u32(fullA), 64, p0);
+    tc::tma_load_2d(&mAl, sa + 2 * kFBox, tc::smem_u32(fullA), 0, p0);
+    tc::tma_load_2d(&mAl, sa + 3 * kFBox, tc::smem_u32(fullA), 64, p0);
+    int issued = 0;
+    for (int t = 0; t < ntiles; ++t) {
+      const int s = t & 1;
+      if (!tc::mbar_wait(tc::smem_u32(&empty[s]), ((t >> 1) & 1) ^ 1, err)) break;
+      const uint32_t fb = tc::smem_u32(&full[s]);
+      const uint32_t sb = tc::smem_u32(smem + (1 + s) * kFOperand);
+      const int row = r0 + t * kFT;
+      tc::mbar_expect_tx(fb, kFOperand);
+      tc::tma_load_2d(&mBh, sb, fb, 0, row);
+      tc::tma_load_2d(&mBh, sb + kFBox, fb, 64, row);
+      tc::tma_load_2d(&mBl, sb + 2 * kFBox, fb, 0, row);
+      tc::tma_load_2d(&mBl, sb + 3 * kFBox, fb, 64, row);
+      issued = t + 1;
+    }
+    // the copies in flight land before the CTA exits (bounded waits)
+    tc::mbar_wait(tc::smem_u32(fullA), 0, err, false);
+    for (int d = 1; d <= 2 && issued - d >= 0; ++d) {
+      const int u = issued - d;
+      tc::mbar_wait(tc::smem_u32(&full[u & 1]), (u >> 1) & 1, err, false);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------------------------------------------------- MMA issuer
+    bool ok = tc::mbar_wait(tc::smem_u32(fullA), 0, err);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t sa = tc::smem_u32(smem);
+    for (int t = 0; t < ntiles && ok; ++t) {
+      const int b = t & 1;
+      if (!tc::mbar_wait(tc::smem_u32(&tempty[b]), ((t >> 1) & 1) ^ 1, err)) { ok = false; break; }
+      if (!tc::mbar_wait(tc::smem_u32(&full[b]), (t >> 1) & 1, err)) { ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t sb = tc::smem_u32(smem + (1 + b) * kFOperand);
+      const uint32_t acc = tmem + static_cast<uint32_t>(b * kFT);
+#pragma unroll
+      for (int kk = 0; kk < kFK / 16; ++kk) {
+        const uint32_t off = (kk >> 2) * kFBox + (kk & 3) * 32;   // box, then 32 bytes per K16 step
+        const uint64_t ah = tc::sw128_desc(sa + off), al = tc::sw128_desc(sa + 2 * kFBox + off);
+        const uint64_t bh = tc::sw128_desc(sb + off), bl = tc::sw128_desc(sb + 2 * kFBox + off);
+        umma_bf16_f32(acc, ah, bh, kk > 0 ? 1u : 0u);
+        umma_bf16_f32(acc, ah, bl, 1u);
+        umma_bf16_f32(acc, al, bh, 1u);
+      }
+      tc::umma_commit(tc::smem_u32(&empty[b]));
+      tc::umma_commit(tc::smem_u32(&tfull[b]));
+    }
+    // every MMA issued has completed before TMEM is released
+    tc::umma_commit(tc::smem_u32(done));
+    tc::mbar_wait(tc::smem_u32(done), 0, err, false);
+  } else if (warp >= 2) {
+    // ---------------------------------------------------------- epilogue
+    // Two warps per TMEM lane quarter, each with half of the tile's columns:
+    // thread (row r, half h) loads its 64 values in one round and releases
+    // the accumulator before scoring them.  Pass 1 keeps the top kFList
+    // approximate values of its half row in registers (a branch-free max/min
+    // insertion network); pass 2 notes the training rows that reach the bar
+    // and the warp scores them exactly, 32 lanes splitting each dot, into a
+    // register list of exact values.  The two half-row lists are merged at
+    // the end.
+    const int q = warp & 3;
+    const int h = (warp - 2) / 4;
+    const int r = q * 32 + lane;          // pair row of the tile (TMEM lane)
+    const bool row_ok = r < np;
+    const int tr = row_ok ? pairs[p0 + r] % ntest : 0;
+    const int et = (warp - 2) * 32 + lane;   // epilogue thread
+    float L[kFList];
+    double D[kFList];
+#pragma unroll
+    for (int e = 0; e < kFList; ++e) {
+      L[e] = -INFINITY;
+      D[e] = -INFINITY;
+    }
+    int* cand = reinterpret_cast<int*>(smem + kFCandOff);   // [slot * (32 kFEpiWarps) + et]
+    const float thr = (PASS == 2 && row_ok) ? bar[p0 + r] : INFINITY;
+    for (int t = 0; t < ntiles; ++t) {
+      const int b = t & 1;
+      const bool ok = tc::mbar_wait(tc::smem_u32(&tfull[b]), (t >> 1) & 1, err);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int n0 = r0 + t * kFT;
+      const int ncol = min(kFT, r1 - n0);
+      const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(b * kFT + h * 64);
+      uint32_t v[4][16];
+      __syncwarp();
+#pragma unroll
+      for (int c = 0; c < 4; ++c) tc::tmem_ld16_raw(base + c * 16, v[c]);
+      tc::tmem_wait_ld();
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      tc::mbar_arrive(tc::smem_u32(&tempty[b]));
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        // values past the class's last training row (or of an absent pair
+        // row) cannot enter a list
+        float f[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const bool in = ok && row_ok && h * 64 + g * 16 + i < ncol;
+          f[i] = in ? __uint_as_float(v[g][i]) : -INFINITY;
+        }
+        float gm = f[0];
+#pragma unroll
+        for (int i = 1; i < 16; ++i) gm = fmaxf(gm, f[i]);
+        if (PASS == 1) {
+          if (gm > L[kFList - 1]) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const float x = f[i];
+#pragma unroll
+              for (int e = kFList - 1; e > 0; --e) L[e] = fmaxf(L[e], fminf(x, L[e - 1]));
+              L[0] = fmaxf(L[0], x);
+            }
+          }
+        } else {
+          int nc = 0;
+          if (gm >= thr) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              if (f[i] >= thr) cand[(nc++) * (32 * kFEpiWarps) + et] = n0 + h * 64 + g * 16 + i;
+          }
+          // exact scores of the noted rows, one warp-wide dot each
+          unsigned pend = __ballot_sync(0xffffffffu, nc > 0);
+          while (pend) {
+            const int src = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const int ns = __shfl_sync(0xffffffffu, nc, src);
+            const int tsrc = __shfl_sync(0xffffffffu, tr, src);
+            const double* xr = Tq + (size_t)tsrc * K;
+            for (int u = 0; u < ns; ++u) {
+              const int gr = cand[u * (32 * kFEpiWarps) + (warp - 2) * 32 + src];
+              const double* yr = Ts + (size_t)gr * K;
+              double d = 0.0;
+              for (int k = lane; k < K; k += 32) d = fma(xr[k], yr[k], d);
+#pragma unroll
+              for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+              if (lane == src && d > D[kFList - 1]) {
+#pragma unroll
+                for (int e = kFList - 1; e > 0; --e) D[e] = fmax(D[e], fmin(d, D[e - 1]));
+                D[0] = fmax(D[0], d);
+              }
+            }
+          }
+        }
+      }
+      if (!ok) break;
+    }
+    // the half-row lists meet in the (now idle) A-tile buffer after the
+    // closing barrier below
+    if (PASS == 1) {
+      float* ls = reinterpret_cast<float*>(smem);
+#pragma unroll
+      for (int e = 0; e < kFList; ++e) ls[(h * kFList + e) * kFT + r] = L[e];
+    } else {
+      double* ls = reinterpret_cast<double*>(smem);
+#pragma unroll
+      for (int e = 0; e < kFList; ++e) ls[(h * kFList + e) * kFT + r] = D[e];
+    }
+  }
+  // every MMA has completed (the issuer waited for them) and every epilogue
+  // thread has stored its list: merge the two halves of each pair row
+  __syncthreads();
+  if (warp >= 2 && warp < 6) {
+    const int r = (warp & 3) * 32 + lane;
+    if (r < np) {
+      const int qi = p0 + r - ci.pair_offs[c];
+      const long long o = ci.part_base[c] + ((long long)qi * ci.nchunks[c] + it.chunk) * use_k;
+      int ia = 0, ib = 0;
+      if (PASS == 1) {
+        const float* ls = reinterpret_cast<const float*>(smem);
+        for (int e = 0; e < use_k; ++e) {
+          const float va = ls[ia * kFT + r], vb = ls[(kFList + ib) * kFT + r];
+          if (!(vb > va)) { apart[o + e] = va; ++ia; } else { apart[o + e] = vb; ++ib; }
+        }
+      } else {
+        const double* ls = reinterpret_cast<const double*>(smem);
+        for (int e = 0; e < use_k; ++e) {
+          const double va = ls[ia * kFT + r], vb = ls[(kFList + ib) * kFT + r];
+          if (!(vb > va)) { part[o + e] = va; ++ia; } else { part[o + e] = vb; ++ib; }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kFT) : "memory");
+  }
+}
+
+// Row i of the BF16 planes (rows_pad x kFK, zero padded) = the hi / lo split
+// of row src(i) of S (row-major, K doubles per row): src(i) = pairs[i] % ntest
+// when pairs is given (the test row of class-sorted pair i), else i.
+__global__ void knn_split_rows_kernel(const double* __restrict__ S, int rows, int K, const int* __restrict__ pairs,
+                                      int ntest, int rows_pad, __nv_bfloat16* __restrict__ hi,
+                                      __nv_bfloat16* __restrict__ lo) {
+  const size_t total = (size_t)rows_pad * kFK;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = static_cast<int>(t / kFK), k = static_cast<int>(t % kFK);
+    double x = 0.0;
+    if (i < rows && k < K) {
+      const int src = pairs ? pairs[i] % ntest : i;
+      x = S[(size_t)src * K + k];
+    }
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    hi[t] = h;
+    lo[t] = __double2bfloat16(x - static_cast<double>(__bfloat162float(h)));
+  }
+}
+
+// Largest row norm of S (rows x K, row-major) as float bits (non-negative
+// floats order as their bit patterns; a NaN norm wins and disables the filter).
+__global__ void knn_row_norm_max_kernel(const double* __restrict__ S, int rows, int K, unsigned* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows) return;
+  double s = 0.0;
+  for (int k = 0; k < K; ++k) s = fma(S[(size_t)i * K + k], S[(size_t)i * K + k], s);
+  atomicMax(out, __float_as_uint(__double2float_ru(sqrt(s))));
+}
+
+// Per class-sorted pair: theta = the k-th largest approximate similarity over
+// all its chunk lists, bar = theta - 2 eps (rounded down), -inf when the
+// class has fewer than k rows.
+__global__ void knn_filter_bar_kernel(const float* __restrict__ apart, KnnClassInfo ci, int C,
+                                      const int* __restrict__ pairs, long long total_pairs, int ntest,
+                                      const double* __restrict__ Tq, int K, int use_k,
+                                      const unsigned* __restrict__ ymax_bits, float* __restrict__ bar) {
+  const long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (P >= total_pairs) return;
+  int lo = 0, hi = C - 1;   // the last class whose pair offset is <= P
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (ci.pair_offs[mid] <= P) lo = mid;
+    else hi = mid - 1;
+  }
+  const int c = lo;
+  const long long qi = P - ci.pair_offs[c];
+  const int nch = ci.nchunks[c];
+  float lst[kKnnMax];
+  for (int e = 0; e < use_k; ++e) lst[e] = -INFINITY;
+  for (int s = 0; s < nch; ++s) {
+    const float* l = apart + ci.part_base[c] + (qi * nch + s) * use_k;
+    for (int e = 0; e < use_k; ++e) {
+      const float v = l[e];
+      if (!(v > lst[use_k - 1])) break;   // chunk lists are sorted
+      insert_desc<float, int>(lst, nullptr, use_k, 1, v, 0);
+    }
+  }
+  const float theta = lst[use_k - 1];
+  if (theta == -INFINITY) {
+    bar[P] = -INFINITY;
+    return;
+  }
+  const double* x = Tq + (size_t)(pairs[P] % ntest) * K;
+  double s2 = 0.0;
+  for (int k = 0; k < K; ++k) s2 = fma(x[k], x[k], s2);
+  const double eps = ldexp(sqrt(s2) * static_cast<double>(__uint_as_float(*ymax_bits)), -10);
+  bar[P] = __double2float_rd(static_cast<double>(theta) - 2.0 * eps);
+}
+
+CUtensorMap make_bf16_rows_map(const __nv_bfloat16* p, int rows_pad) {
+  CUtensorMap m;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(kFK), static_cast<cuuint64_t>(rows_pad)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(kFK) * 2};
+  cuuint32_t box[2] = {64, static_cast<cuuint32_t>(kFT)};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = tc::encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(p), dims, strides,
+                               box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(kErrCuda, "cuTensorMapEncodeTiled failed (cKNN score planes)");
+  return m;
+}
+
 // Per pair: merge its chunk lists, smoothed class score (src/fastPLS.cpp:1287-1320,
 // src/lda_cuda_kernels.cu:225-242), add alpha * base + bias.
 __global__ void knn_merge_kernel(const int* __restrict__ pairs, long long total_pairs,
@@ -660,6 +1038,15 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
   std::vector<int> hp(C);
   d2h(hp.data(), pcount, C * sizeof(int));
   ctx.sync();
+  // Tile kernel (FASTPLS_CKNN_TILES): 4 or unset the BF16 tensor-core filter
+  // with exact FP64 rescoring (score rows up to 128 wide), 1 the 16-wide
+  // k-step FP64 kernel, 2 / 3 the staged FP64 kernels with two / one
+  // training-row buffers.
+  const char* tv = std::getenv("FASTPLS_CKNN_TILES");
+  const char sel = (tv && tv[0]) ? tv[0] : '4';
+  const bool use_filter = sel == '4' && kdim <= kFK && use_k <= kFList;
+  const int tile_m = use_filter ? kFT : kTileM;   // pairs per item
+  const int gran = use_filter ? kFT : kTileN;     // chunk rows are a multiple of this
   std::vector<int> poffs(C + 1, 0), chunk_rows(C, 0), nchunks(C, 0);
   std::vector<long long> part_base(C, 0);
   std::vector<KnnItem> items;
@@ -670,7 +1057,7 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
     int S = 0, cr_rows = 0;
     if (rows > 0) {
       S = std::min(kMaxChunks, std::max(1, ceil_div(rows, kMinChunkRows)));
-      cr_rows = ceil_div(ceil_div(rows, S), kTileN) * kTileN;
+      cr_rows = ceil_div(ceil_div(rows, S), gran) * gran;
       S = ceil_div(rows, cr_rows);
     }
     chunk_rows[c] = cr_rows;
@@ -678,7 +1065,7 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
     part_base[c] = part_total;
     part_total += (long long)hp[c] * S * use_k;
     if (rows > 0 && hp[c] > 0) {
-      const int tiles = ceil_div(hp[c], kTileM);
+      const int tiles = ceil_div(hp[c], tile_m);
       for (int t = 0; t < tiles; ++t)
         for (int s = 0; s < S; ++s) items.push_back(KnnItem{c, t, s, 0});
     }
@@ -705,24 +1092,90 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
   double* part = ctx.arena.alloc_n<double>((size_t)std::max<long long>(part_total, 1));
   double* cscore = ctx.arena.alloc_n<double>((size_t)npairs);
   pt.mark("class rows + pair lists");
-  if (!items.empty()) {
+  if (!items.empty() && use_filter) {
+    const KnnItem* ditems = upload(items.data(), items.size());
+    FPLS_REQUIRE(items.size() < (1u << 31), "candidate-kNN: too many work items");
+    const int slot = ctx.prof_begin("cknn_filter", ctx.stream);
+    const int nvalid = cr.offs[C];
+    const long long a_rows = (total_pairs + kFT - 1) / kFT * kFT + kFT;
+    const long long b_rows = ((long long)nvalid + kFT - 1) / kFT * kFT + kFT;
+    FPLS_REQUIRE(a_rows < (1ll << 31) && b_rows < (1ll << 31), "candidate-kNN: too many rows for the filter");
+    __nv_bfloat16* ah = ctx.arena.alloc_n<__nv_bfloat16>((size_t)a_rows * kFK);
+    __nv_bfloat16* al = ctx.arena.alloc_n<__nv_bfloat16>((size_t)a_rows * kFK);
+    __nv_bfloat16* bh = ctx.arena.alloc_n<__nv_bfloat16>((size_t)b_rows * kFK);
+    __nv_bfloat16* bl = ctx.arena.alloc_n<__nv_bfloat16>((size_t)b_rows * kFK);
+    const int gs = 8 * ctx.sm_count;
+    knn_split_rows_kernel<<<gs, 256, 0, ctx.stream>>>(Tq, (int)total_pairs, kdim, pairs, ntest, (int)a_rows, ah, al);
+    ::fpls::note_launch();
+    knn_split_rows_kernel<<<gs, 256, 0, ctx.stream>>>(cr.Ts, nvalid, kdim, nullptr, 1, (int)b_rows, bh, bl);
+    ::fpls::note_launch();
+    unsigned* ymax = ctx.arena.alloc_n<unsigned>(1);
+    dzero(ymax, sizeof(unsigned));
+    if (nvalid > 0) {
+      knn_row_norm_max_kernel<<<ceil_div(nvalid, 256), 256, 0, ctx.stream>>>(cr.Ts, nvalid, kdim, ymax);
+      ::fpls::note_launch();
+    }
+    FPLS_CHECK_LAUNCH();
+    pt.mark("filter planes");
+    const CUtensorMap mAh = make_bf16_rows_map(ah, (int)a_rows), mAl = make_bf16_rows_map(al, (int)a_rows);
+    const CUtensorMap mBh = make_bf16_rows_map(bh, (int)b_rows), mBl = make_bf16_rows_map(bl, (int)b_rows);
+    float* apart = ctx.arena.alloc_n<float>((size_t)std::max<long long>(part_total, 1));
+    float* barv = ctx.arena.alloc_n<float>((size_t)std::max<long long>(total_pairs, 1));
+    int* ferr = ctx.d_status + 24;
+    dzero(ferr, sizeof(int));
+    static bool fattr = false;
+    if (!fattr) {
+      FPLS_CUDA(cudaFuncSetAttribute(knn_filter_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
+      FPLS_CUDA(cudaFuncSetAttribute(knn_filter_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
+      fattr = true;
+    }
+    const unsigned ng = (unsigned)items.size();
+    knn_filter_kernel<1><<<ng, kFThreads, kFSmem, ctx.stream>>>(mAh, mAl, mBh, mBl, ditems, ci, pairs, ntest, Tq,
+                                                               cr.Ts, kdim, use_k, apart, nullptr, nullptr, ferr);
+    ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    pt.mark("filter pass 1");
+    knn_filter_bar_kernel<<<(unsigned)ceil_div(total_pairs, 256), 256, 0, ctx.stream>>>(
+        apart, ci, C, pairs, total_pairs, ntest, Tq, kdim, use_k, ymax, barv);
+    ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    pt.mark("filter bar");
+    knn_filter_kernel<2><<<ng, kFThreads, kFSmem, ctx.stream>>>(mAh, mAl, mBh, mBl, ditems, ci, pairs, ntest, Tq,
+                                                               cr.Ts, kdim, use_k, nullptr, barv, part, ferr);
+    ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    pt.mark("filter pass 2");
+    if (slot >= 0) {
+      // algorithmic work: the three BF16 products of both passes over every
+      // (candidate pair, class row); bytes: the score planes of every class's
+      // training rows once per 128-pair tile and pass, the pair planes once
+      double work = 0.0, bytes = 2.0 * 4.0 * kFK * (double)total_pairs;
+      for (int c = 0; c < C; ++c) {
+        const double rows = cr.offs[c + 1] - cr.offs[c];
+        work += (double)hp[c] * rows;
+        bytes += 2.0 * 4.0 * kFK * rows * (double)ceil_div(hp[c], kFT);
+      }
+      ctx.prof_end(slot, ctx.stream, bytes, 2.0 * 3.0 * 2.0 * work * kdim);
+    }
+    int ferr_h = 0;
+    d2h(&ferr_h, ferr, sizeof(int));
+    ctx.sync();
+    if (ferr_h) throw Error(kErrCuda, "candidate-kNN: a filter tile's pipeline wait timed out");
+  } else if (!items.empty()) {
     const KnnItem* ditems = upload(items.data(), items.size());
     FPLS_REQUIRE(items.size() < (1u << 31), "candidate-kNN: too many work items");
     const int slot = ctx.prof_begin("cknn_tiles", ctx.stream);
     // stride of the staged rows: K rounded up to 4, then to 4 mod 16
     const int KP = (kdim + 3) / 4 * 4;
     const int S = KP + (4 - KP % 16 + 16) % 16;
-    // Kernel choice (FASTPLS_CKNN_TILES: 1 the 16-wide k-step kernel, 2 the
-    // staged kernel with two training-row buffers, 3 or unset the staged
-    // kernel with one buffer).  On the large-class workload (K = 100) the
+    // FP64 tile kernels: on the large-class workload (K = 100) the
     // similarity tiles took 123.4 ms (k-step), 162.6 ms (two buffers: one
     // 8-warp CTA per SM, the tensor pipe idles while the top-k epilogue runs)
     // and 107.2 ms (one buffer: two CTAs per SM, one CTA's epilogue overlapping
-    // the other's products).  Staged rows wider than 116 doubles take the
-    // k-step kernel.
-    const char* tv = std::getenv("FASTPLS_CKNN_TILES");
-    const char sel = (tv && tv[0]) ? tv[0] : '3';
-    if (S <= kV2MaxStride && (sel == '2' || sel == '3')) {
+    // the other's products).  The filter takes score rows up to 128 wide and
+    // lists up to 16 long; past that the staged kernel runs, and rows wider
+    // than 116 doubles take the k-step kernel.
+    if (S <= kV2MaxStride && sel != '1') {
       const int nb = sel == '2' ? 2 : 1;
       const size_t smem = sizeof(double) * ((size_t)kTileM * S + nb * (size_t)kTileN * std::max(S, kTileN + 1) +
                                             (size_t)use_k * 2 * kTileM);

@@ -84,16 +84,33 @@ def test_candidate_knn_wide_scores(lib, kdim):
     _check(got, ref)
 
 
-@pytest.mark.parametrize("buffers", ["1", "2", "3"])
-@pytest.mark.parametrize("kdim", [9, 24, 100])
+@pytest.mark.parametrize("buffers", ["1", "2", "3", "4"])
+@pytest.mark.parametrize("kdim", [9, 24, 100, 128])
 def test_candidate_knn_staged_tiles_match_oracle(lib, monkeypatch, kdim, buffers):
     # every similarity-tile kernel (FASTPLS_CKNN_TILES=1: 16-wide k-steps;
-    # 2: contraction staged, two training-row buffers; 3, the default: one
-    # buffer, two CTAs per SM) gives the oracle's neighbours, for odd, small
-    # and wide score spaces
+    # 2: contraction staged, two training-row buffers; 3: one buffer, two
+    # CTAs per SM; 4, the default: BF16 tensor-core filter with exact FP64
+    # rescoring) gives the oracle's neighbours, for odd, small and wide score
+    # spaces (128 is the filter's widest; the staged kernels hand it to the
+    # k-step kernel)
     monkeypatch.setenv("FASTPLS_CKNN_TILES", buffers)
     Tr, y, Tt = _zipf_case(14 + kdim, 6000, 150, 30, kdim)
     cents = ok.centroids(Tr, y, 30)
     got = lib.candidate_knn_predict(Tt, Tr, y, cents, top_k=5, top_m=12, knn_k=10, tau=0.2, alpha=0.75)
     ref = ok.candidate_knn_predict(Tt, Tr, y, cents, top_k=5, top_m=12, knn_k=10, tau=0.2, alpha=0.75)
+    _check(got, ref)
+
+
+def test_candidate_knn_filter_near_ties(lib, monkeypatch):
+    # training rows that are copies of one another up to 1e-7: many
+    # approximate similarities fall inside the filter's error bar around a
+    # pair's k-th neighbour, so the exact rescoring decides the list
+    monkeypatch.setenv("FASTPLS_CKNN_TILES", "4")
+    rng = np.random.default_rng(21)
+    base, y, Tt = _zipf_case(22, 400, 90, 6, 32)
+    Tr = ok.row_l2(np.repeat(base, 8, axis=0) + 1e-7 * rng.standard_normal((3200, 32)))
+    y = np.repeat(y, 8).astype(np.int32)
+    cents = ok.centroids(Tr, y, 6)
+    got = lib.candidate_knn_predict(Tt, Tr, y, cents, top_k=3, top_m=4, knn_k=12, tau=0.2, alpha=0.75)
+    ref = ok.candidate_knn_predict(Tt, Tr, y, cents, top_k=3, top_m=4, knn_k=12, tau=0.2, alpha=0.75)
     _check(got, ref)

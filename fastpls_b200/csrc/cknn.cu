@@ -496,23 +496,28 @@ knn_tile_kernel_v2(const KnnItem* __restrict__ items, KnnClassInfo ci, const int
 //           lo = bf16(x - hi), three products hi.hi + hi.lo + lo.hi
 //           (tcgen05.mma kind::f16, M128 N128 K16, FP32 accumulation in TMEM,
 //           double-buffered so the epilogue overlaps the next tile); each pair
-//           keeps the top k of its approximate values per chunk;
-//   bar     per pair, theta = the k-th largest approximate value over all its
-//           chunks.  Every approximate value is within
-//           eps = 2^-10 |x| max|y| of the exact dot (the dropped split terms
-//           are below 3 2^-18 |x||y| and the FP32 accumulation of 3 x 128
-//           products below 384 2^-23 sum|x_k y_k| <= 2^-14.4 |x||y|), so each
-//           row of the pair's exact top k has an approximate value of at least
+//           row keeps running maxima of 64 disjoint buckets of its values and
+//           writes the k largest of them per chunk;
+//   bar     per pair, theta = the k-th largest of those values over all its
+//           chunks.  They are approximate values of distinct training rows, so
+//           theta is at most the k-th largest approximate value of the class.
+//           Every approximate value is within eps = 2^-14 |x| max|y| of the
+//           exact dot: the split leaves x - hi - lo below 2^-18 |x| and drops
+//           terms below 3 2^-18 |x||y| in all (1.2e-5 |x||y|); the BF16
+//           products are exact in FP32 and the FP32 accumulation of the 3 x 128
+//           products loses at most 384 2^-23 sum|x_k y_k| <= 4.6e-5 |x||y|
+//           even with every addition truncated; 5.7e-5 < 2^-14.  So each row
+//           of the pair's exact top k has an approximate value of at least
 //           theta - 2 eps;
 //   pass 2  the same products again; every training row whose approximate
 //           value reaches that bar is scored exactly (FP64 dot of the two score
 //           rows) and folded into the pair's top-k list, which is what the
 //           FP64 tiles write and knn_merge_kernel reads.
-// Score rows up to 128 wide, neighbour lists up to 16 long.  Warp 0 loads
-// (TMA, SWIZZLE_128B boxes of 64 x 128 BF16: the A tile once, the B tiles
-// through two stages), warp 1 issues the MMAs, warps 2..5 are the epilogue
-// (one pair row per thread).  Every mbarrier wait is bounded; no cluster
-// multicast.
+// Score rows up to 128 wide, neighbour lists up to 16 long, up to 2^24
+// training rows.  Warp 0 loads (TMA, SWIZZLE_128B boxes of 64 x 128 BF16: the
+// A tile once, the B tiles through two stages), warp 1 issues the MMAs,
+// warps 2..9 are the epilogue (two per TMEM lane quarter).  Every mbarrier
+// wait is bounded; no cluster multicast.
 constexpr int kFT = 128;                  // pairs per tile = training rows per tile
 constexpr int kFK = 128;                  // contraction width (rows zero padded)
 constexpr int kFBox = 64 * kFT * 2;       // one 64-wide box of 128 BF16 rows: 16 KB
@@ -520,9 +525,12 @@ constexpr int kFOperand = 4 * kFBox;      // two planes x two boxes: 64 KB
 constexpr int kFEpiWarps = 8;             // two per TMEM lane quarter, half the columns each
 constexpr int kFThreads = 64 + 32 * kFEpiWarps;
 constexpr int kFBarOff = 3 * kFOperand;   // A, then two B stages
-constexpr int kFList = 16;                // list length the filter keeps (use_k <= 16)
-constexpr int kFCandOff = kFBarOff + 256;  // pass 2: 16 candidate rows per epilogue thread
-constexpr int kFSmem = kFCandOff + 16 * 32 * kFEpiWarps * 4 + 1024;
+constexpr int kFList = 16;                // exact list length of pass 2 (use_k <= 16)
+constexpr int kFBuckets = 32;             // pass 1: running maxima per thread
+constexpr int kFQueueOff = kFBarOff + 256;                    // pass 2: per-warp candidate queues
+constexpr int kFQueue = 32 * 16;                               // one group of 16 values per lane
+constexpr int kFRowOff = kFQueueOff + kFQueue * kFEpiWarps * 4;  // pass 2: test row of every lane
+constexpr int kFSmem = kFRowOff + 32 * kFEpiWarps * 4 + 1024;
 constexpr uint32_t kFIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kFT >> 3) << 17) |
                              (uint32_t(kFT >> 4) << 24);
 static_assert(kFSmem <= 227 * 1024, "filter tiles exceed shared memory");
@@ -645,26 +653,32 @@ knn_filter_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant
     // ---------------------------------------------------------- epilogue
     // Two warps per TMEM lane quarter, each with half of the tile's columns:
     // thread (row r, half h) loads its 64 values in one round and releases
-    // the accumulator before scoring them.  Pass 1 keeps the top kFList
-    // approximate values of its half row in registers (a branch-free max/min
-    // insertion network); pass 2 notes the training rows that reach the bar
-    // and the warp scores them exactly, 32 lanes splitting each dot, into a
-    // register list of exact values.  The two half-row lists are merged at
-    // the end.
+    // the accumulator before using them.
+    //   pass 1: 32 running maxima of disjoint buckets of the half row's
+    //           values (one max per value).  They are values of distinct
+    //           training rows, so the k-th largest of them is at most the
+    //           k-th largest approximate value, which is all the bar needs;
+    //   pass 2: the rows whose value reaches the bar go to the warp's queue,
+    //           and the warp scores them four at a time, its 32 lanes
+    //           splitting each exact FP64 dot; the lane of the pair row keeps
+    //           the row's top kFList exact values in registers (a
+    //           branch-free max/min insertion network).
+    // The two half-row lists of a pair row are merged at the end.
     const int q = warp & 3;
     const int h = (warp - 2) / 4;
     const int r = q * 32 + lane;          // pair row of the tile (TMEM lane)
     const bool row_ok = r < np;
     const int tr = row_ok ? pairs[p0 + r] % ntest : 0;
-    const int et = (warp - 2) * 32 + lane;   // epilogue thread
-    float L[kFList];
+    float M[kFBuckets];
     double D[kFList];
 #pragma unroll
-    for (int e = 0; e < kFList; ++e) {
-      L[e] = -INFINITY;
-      D[e] = -INFINITY;
-    }
-    int* cand = reinterpret_cast<int*>(smem + kFCandOff);   // [slot * (32 kFEpiWarps) + et]
+    for (int e = 0; e < kFBuckets; ++e) M[e] = -INFINITY;
+#pragma unroll
+    for (int e = 0; e < kFList; ++e) D[e] = -INFINITY;
+    int* wq = reinterpret_cast<int*>(smem + kFQueueOff) + (warp - 2) * kFQueue;
+    int* wrow = reinterpret_cast<int*>(smem + kFRowOff) + (warp - 2) * 32;
+    if (PASS == 2) wrow[lane] = tr;
+    __syncwarp();
     const float thr = (PASS == 2 && row_ok) ? bar[p0 + r] : INFINITY;
     for (int t = 0; t < ntiles; ++t) {
       const int b = t & 1;
@@ -690,48 +704,66 @@ knn_filter_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant
           const bool in = ok && row_ok && h * 64 + g * 16 + i < ncol;
           f[i] = in ? __uint_as_float(v[g][i]) : -INFINITY;
         }
-        float gm = f[0];
-#pragma unroll
-        for (int i = 1; i < 16; ++i) gm = fmaxf(gm, f[i]);
         if (PASS == 1) {
-          if (gm > L[kFList - 1]) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const float x = f[i];
-#pragma unroll
-              for (int e = kFList - 1; e > 0; --e) L[e] = fmaxf(L[e], fminf(x, L[e - 1]));
-              L[0] = fmaxf(L[0], x);
-            }
-          }
+          for (int i = 0; i < 16; ++i) M[(g * 16 + i) % kFBuckets] = fmaxf(M[(g * 16 + i) % kFBuckets], f[i]);
         } else {
-          int nc = 0;
-          if (gm >= thr) {
+          unsigned m16 = 0;
 #pragma unroll
-            for (int i = 0; i < 16; ++i)
-              if (f[i] >= thr) cand[(nc++) * (32 * kFEpiWarps) + et] = n0 + h * 64 + g * 16 + i;
+          for (int i = 0; i < 16; ++i)
+            if (f[i] >= thr) m16 |= 1u << i;
+          const int nc = __popc(m16);
+          int incl = nc;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int x = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += x;
           }
-          // exact scores of the noted rows, one warp-wide dot each
-          unsigned pend = __ballot_sync(0xffffffffu, nc > 0);
-          while (pend) {
-            const int src = __ffs(pend) - 1;
-            pend &= pend - 1;
-            const int ns = __shfl_sync(0xffffffffu, nc, src);
-            const int tsrc = __shfl_sync(0xffffffffu, tr, src);
-            const double* xr = Tq + (size_t)tsrc * K;
-            for (int u = 0; u < ns; ++u) {
-              const int gr = cand[u * (32 * kFEpiWarps) + (warp - 2) * 32 + src];
-              const double* yr = Ts + (size_t)gr * K;
-              double d = 0.0;
-              for (int k = lane; k < K; k += 32) d = fma(xr[k], yr[k], d);
+          const int total = __shfl_sync(0xffffffffu, incl, 31);
+          if (total == 0) continue;
+          int pos = incl - nc;
+          while (m16) {
+            const int i = __ffs(m16) - 1;
+            m16 &= m16 - 1;
+            wq[pos++] = (lane << 24) | (n0 + h * 64 + g * 16 + i);
+          }
+          __syncwarp();
+          // four queued rows at a time, the warp's lanes splitting each dot
+          // (every load of the four dots in flight together)
+          for (int q0 = 0; q0 < total; q0 += 4) {
+            double acc[4];
+            int own[4];
 #pragma unroll
-              for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-              if (lane == src && d > D[kFList - 1]) {
+            for (int c = 0; c < 4; ++c) {
+              acc[c] = 0.0;
+              own[c] = -1;
+              if (q0 + c < total) {
+                const int en = wq[q0 + c];
+                own[c] = en >> 24;
+                const double* xr = Tq + (size_t)wrow[own[c]] * K;
+                const double* yr = Ts + (size_t)(en & 0xFFFFFF) * K;
 #pragma unroll
-                for (int e = kFList - 1; e > 0; --e) D[e] = fmax(D[e], fmin(d, D[e - 1]));
-                D[0] = fmax(D[0], d);
+                for (int m = 0; m < kFK / 32; ++m) {
+                  const int k = lane + 32 * m;
+                  if (k < K) acc[c] = fma(xr[k], yr[k], acc[c]);
+                }
+              }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+              for (int c = 0; c < 4; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              const double dj = acc[c];
+              if (lane == own[c] && dj > D[kFList - 1]) {
+#pragma unroll
+                for (int e = kFList - 1; e > 0; --e) D[e] = fmax(D[e], fmin(dj, D[e - 1]));
+                D[0] = fmax(D[0], dj);
               }
             }
           }
+          __syncwarp();
         }
       }
       if (!ok) break;
@@ -741,7 +773,7 @@ knn_filter_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant
     if (PASS == 1) {
       float* ls = reinterpret_cast<float*>(smem);
 #pragma unroll
-      for (int e = 0; e < kFList; ++e) ls[(h * kFList + e) * kFT + r] = L[e];
+      for (int e = 0; e < kFBuckets; ++e) ls[(h * kFBuckets + e) * kFT + r] = M[e];
     } else {
       double* ls = reinterpret_cast<double*>(smem);
 #pragma unroll
@@ -749,21 +781,28 @@ knn_filter_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant
     }
   }
   // every MMA has completed (the issuer waited for them) and every epilogue
-  // thread has stored its list: merge the two halves of each pair row
+  // thread has stored its values: one thread per pair row writes its lists
   __syncthreads();
   if (warp >= 2 && warp < 6) {
     const int r = (warp & 3) * 32 + lane;
     if (r < np) {
       const int qi = p0 + r - ci.pair_offs[c];
       const long long o = ci.part_base[c] + ((long long)qi * ci.nchunks[c] + it.chunk) * use_k;
-      int ia = 0, ib = 0;
       if (PASS == 1) {
-        const float* ls = reinterpret_cast<const float*>(smem);
+        // the use_k largest of the row's 64 bucket maxima, in descending order
+        float* ls = reinterpret_cast<float*>(smem);
         for (int e = 0; e < use_k; ++e) {
-          const float va = ls[ia * kFT + r], vb = ls[(kFList + ib) * kFT + r];
-          if (!(vb > va)) { apart[o + e] = va; ++ia; } else { apart[o + e] = vb; ++ib; }
+          int best = 0;
+          float bv = ls[r];
+          for (int x = 1; x < 2 * kFBuckets; ++x) {
+            const float vx = ls[x * kFT + r];
+            if (vx > bv) { bv = vx; best = x; }
+          }
+          apart[o + e] = bv;
+          ls[best * kFT + r] = -INFINITY;
         }
       } else {
+        int ia = 0, ib = 0;
         const double* ls = reinterpret_cast<const double*>(smem);
         for (int e = 0; e < use_k; ++e) {
           const double va = ls[ia * kFT + r], vb = ls[(kFList + ib) * kFT + r];
@@ -846,7 +885,7 @@ __global__ void knn_filter_bar_kernel(const float* __restrict__ apart, KnnClassI
   const double* x = Tq + (size_t)(pairs[P] % ntest) * K;
   double s2 = 0.0;
   for (int k = 0; k < K; ++k) s2 = fma(x[k], x[k], s2);
-  const double eps = ldexp(sqrt(s2) * static_cast<double>(__uint_as_float(*ymax_bits)), -10);
+  const double eps = ldexp(sqrt(s2) * static_cast<double>(__uint_as_float(*ymax_bits)), -14);
   bar[P] = __double2float_rd(static_cast<double>(theta) - 2.0 * eps);
 }
 
@@ -1044,7 +1083,7 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
   // training-row buffers.
   const char* tv = std::getenv("FASTPLS_CKNN_TILES");
   const char sel = (tv && tv[0]) ? tv[0] : '4';
-  const bool use_filter = sel == '4' && kdim <= kFK && use_k <= kFList;
+  const bool use_filter = sel == '4' && kdim <= kFK && use_k <= kFList && ntrain < (1 << 24);
   const int tile_m = use_filter ? kFT : kTileM;   // pairs per item
   const int gran = use_filter ? kFT : kTileN;     // chunk rows are a multiple of this
   std::vector<int> poffs(C + 1, 0), chunk_rows(C, 0), nchunks(C, 0);

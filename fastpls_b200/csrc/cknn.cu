@@ -525,12 +525,10 @@ constexpr int kFOperand = 4 * kFBox;      // two planes x two boxes: 64 KB
 constexpr int kFEpiWarps = 8;             // two per TMEM lane quarter, half the columns each
 constexpr int kFThreads = 64 + 32 * kFEpiWarps;
 constexpr int kFBarOff = 3 * kFOperand;   // A, then two B stages
-constexpr int kFList = 16;                // exact list length of pass 2 (use_k <= 16)
+constexpr int kFList = 16;                // longest neighbour list of the filter
 constexpr int kFBuckets = 32;             // pass 1: running maxima per thread
-constexpr int kFQueueOff = kFBarOff + 256;                    // pass 2: per-warp candidate queues
-constexpr int kFQueue = 32 * 16;                               // one group of 16 values per lane
-constexpr int kFRowOff = kFQueueOff + kFQueue * kFEpiWarps * 4;  // pass 2: test row of every lane
-constexpr int kFSmem = kFRowOff + 32 * kFEpiWarps * 4 + 1024;
+constexpr int kFCap = 128;                // pass 2: candidate rows kept per pair
+constexpr int kFSmem = kFBarOff + 256 + 1024;
 constexpr uint32_t kFIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kFT >> 3) << 17) |
                              (uint32_t(kFT >> 4) << 24);
 static_assert(kFSmem <= 227 * 1024, "filter tiles exceed shared memory");
@@ -549,8 +547,8 @@ knn_filter_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant
                   const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                   const KnnItem* __restrict__ items, KnnClassInfo ci, const int* __restrict__ pairs, int ntest,
                   const double* __restrict__ Tq, const double* __restrict__ Ts, int K, int use_k,
-                  float* __restrict__ apart, const float* __restrict__ bar, double* __restrict__ part,
-                  int* err) {
+                  float* __restrict__ apart, const float* __restrict__ bar, int* __restrict__ ccount,
+                  int* __restrict__ crow, int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~static_cast<uintptr_t>(1023));
@@ -658,27 +656,18 @@ knn_filter_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant
     //           values (one max per value).  They are values of distinct
     //           training rows, so the k-th largest of them is at most the
     //           k-th largest approximate value, which is all the bar needs;
-    //   pass 2: the rows whose value reaches the bar go to the warp's queue,
-    //           and the warp scores them four at a time, its 32 lanes
-    //           splitting each exact FP64 dot; the lane of the pair row keeps
-    //           the row's top kFList exact values in registers (a
-    //           branch-free max/min insertion network).
-    // The two half-row lists of a pair row are merged at the end.
+    //   pass 2: the rows whose value reaches the bar are noted in the pair's
+    //           candidate slots (scored exactly by knn_exact_kernel, outside
+    //           this pipeline).
+    // The two halves of a pair row's bucket maxima are merged at the end.
     const int q = warp & 3;
     const int h = (warp - 2) / 4;
     const int r = q * 32 + lane;          // pair row of the tile (TMEM lane)
     const bool row_ok = r < np;
     const int tr = row_ok ? pairs[p0 + r] % ntest : 0;
     float M[kFBuckets];
-    double D[kFList];
 #pragma unroll
     for (int e = 0; e < kFBuckets; ++e) M[e] = -INFINITY;
-#pragma unroll
-    for (int e = 0; e < kFList; ++e) D[e] = -INFINITY;
-    int* wq = reinterpret_cast<int*>(smem + kFQueueOff) + (warp - 2) * kFQueue;
-    int* wrow = reinterpret_cast<int*>(smem + kFRowOff) + (warp - 2) * 32;
-    if (PASS == 2) wrow[lane] = tr;
-    __syncwarp();
     const float thr = (PASS == 2 && row_ok) ? bar[p0 + r] : INFINITY;
     for (int t = 0; t < ntiles; ++t) {
       const int b = t & 1;
@@ -708,106 +697,43 @@ knn_filter_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant
 #pragma unroll
           for (int i = 0; i < 16; ++i) M[(g * 16 + i) % kFBuckets] = fmaxf(M[(g * 16 + i) % kFBuckets], f[i]);
         } else {
-          unsigned m16 = 0;
 #pragma unroll
           for (int i = 0; i < 16; ++i)
-            if (f[i] >= thr) m16 |= 1u << i;
-          const int nc = __popc(m16);
-          int incl = nc;
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const int x = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += x;
-          }
-          const int total = __shfl_sync(0xffffffffu, incl, 31);
-          if (total == 0) continue;
-          int pos = incl - nc;
-          while (m16) {
-            const int i = __ffs(m16) - 1;
-            m16 &= m16 - 1;
-            wq[pos++] = (lane << 24) | (n0 + h * 64 + g * 16 + i);
-          }
-          __syncwarp();
-          // four queued rows at a time, the warp's lanes splitting each dot
-          // (every load of the four dots in flight together)
-          for (int q0 = 0; q0 < total; q0 += 4) {
-            double acc[4];
-            int own[4];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              acc[c] = 0.0;
-              own[c] = -1;
-              if (q0 + c < total) {
-                const int en = wq[q0 + c];
-                own[c] = en >> 24;
-                const double* xr = Tq + (size_t)wrow[own[c]] * K;
-                const double* yr = Ts + (size_t)(en & 0xFFFFFF) * K;
-#pragma unroll
-                for (int m = 0; m < kFK / 32; ++m) {
-                  const int k = lane + 32 * m;
-                  if (k < K) acc[c] = fma(xr[k], yr[k], acc[c]);
-                }
-              }
+            if (f[i] >= thr) {
+              const int slot = atomicAdd(ccount + p0 + r, 1);
+              if (slot < kFCap) crow[(size_t)(p0 + r) * kFCap + slot] = n0 + h * 64 + g * 16 + i;
             }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-              for (int c = 0; c < 4; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              const double dj = acc[c];
-              if (lane == own[c] && dj > D[kFList - 1]) {
-#pragma unroll
-                for (int e = kFList - 1; e > 0; --e) D[e] = fmax(D[e], fmin(dj, D[e - 1]));
-                D[0] = fmax(D[0], dj);
-              }
-            }
-          }
-          __syncwarp();
         }
       }
       if (!ok) break;
     }
-    // the half-row lists meet in the (now idle) A-tile buffer after the
-    // closing barrier below
+    // the two halves meet in the (now idle) A-tile buffer after the closing
+    // barrier below
     if (PASS == 1) {
       float* ls = reinterpret_cast<float*>(smem);
 #pragma unroll
       for (int e = 0; e < kFBuckets; ++e) ls[(h * kFBuckets + e) * kFT + r] = M[e];
-    } else {
-      double* ls = reinterpret_cast<double*>(smem);
-#pragma unroll
-      for (int e = 0; e < kFList; ++e) ls[(h * kFList + e) * kFT + r] = D[e];
     }
   }
   // every MMA has completed (the issuer waited for them) and every epilogue
-  // thread has stored its values: one thread per pair row writes its lists
+  // thread has stored its values: one thread per pair row writes its list
   __syncthreads();
-  if (warp >= 2 && warp < 6) {
+  if (PASS == 1 && warp >= 2 && warp < 6) {
     const int r = (warp & 3) * 32 + lane;
     if (r < np) {
       const int qi = p0 + r - ci.pair_offs[c];
       const long long o = ci.part_base[c] + ((long long)qi * ci.nchunks[c] + it.chunk) * use_k;
-      if (PASS == 1) {
-        // the use_k largest of the row's 64 bucket maxima, in descending order
-        float* ls = reinterpret_cast<float*>(smem);
-        for (int e = 0; e < use_k; ++e) {
-          int best = 0;
-          float bv = ls[r];
-          for (int x = 1; x < 2 * kFBuckets; ++x) {
-            const float vx = ls[x * kFT + r];
-            if (vx > bv) { bv = vx; best = x; }
-          }
-          apart[o + e] = bv;
-          ls[best * kFT + r] = -INFINITY;
+      // the use_k largest of the row's 64 bucket maxima, in descending order
+      float* ls = reinterpret_cast<float*>(smem);
+      for (int e = 0; e < use_k; ++e) {
+        int best = 0;
+        float bv = ls[r];
+        for (int x = 1; x < 2 * kFBuckets; ++x) {
+          const float vx = ls[x * kFT + r];
+          if (vx > bv) { bv = vx; best = x; }
         }
-      } else {
-        int ia = 0, ib = 0;
-        const double* ls = reinterpret_cast<const double*>(smem);
-        for (int e = 0; e < use_k; ++e) {
-          const double va = ls[ia * kFT + r], vb = ls[(kFList + ib) * kFT + r];
-          if (!(vb > va)) { part[o + e] = va; ++ia; } else { part[o + e] = vb; ++ib; }
-        }
+        apart[o + e] = bv;
+        ls[best * kFT + r] = -INFINITY;
       }
     }
   }
@@ -887,6 +813,59 @@ __global__ void knn_filter_bar_kernel(const float* __restrict__ apart, KnnClassI
   for (int k = 0; k < K; ++k) s2 = fma(x[k], x[k], s2);
   const double eps = ldexp(sqrt(s2) * static_cast<double>(__uint_as_float(*ymax_bits)), -14);
   bar[P] = __double2float_rd(static_cast<double>(theta) - 2.0 * eps);
+}
+
+// Exact scores of the candidates of every pair (one warp per class-sorted
+// pair): each lane takes candidates lane, lane + 32, ... and forms their FP64
+// dots (k in order); the use_k largest go to plist[P * use_k ..] in
+// descending order (-inf when there are fewer).  A pair with more than kFCap
+// candidates raises *overflow (its list would be incomplete).
+__global__ void knn_exact_kernel(const int* __restrict__ ccount, const int* __restrict__ crow,
+                                 const int* __restrict__ pairs, long long total_pairs, int ntest,
+                                 const double* __restrict__ Tq, const double* __restrict__ Ts, int K, int use_k,
+                                 double* __restrict__ plist, int* overflow) {
+  const long long P = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (P >= total_pairs) return;   // whole warps
+  int cnt = ccount[P];
+  if (cnt > kFCap) {
+    if (lane == 0) atomicExch(overflow, 1);
+    cnt = kFCap;
+  }
+  const double* xr = Tq + (size_t)(pairs[P] % ntest) * K;
+  double v[kFCap / 32];
+#pragma unroll
+  for (int u = 0; u < kFCap / 32; ++u) {
+    v[u] = -INFINITY;
+    const int idx = lane + 32 * u;
+    if (idx < cnt) {
+      const double* yr = Ts + (size_t)crow[(size_t)P * kFCap + idx] * K;
+      double d = 0.0;
+#pragma unroll 4
+      for (int k = 0; k < K; ++k) d = fma(xr[k], yr[k], d);
+      v[u] = d;
+    }
+  }
+  for (int e = 0; e < use_k; ++e) {
+    // the warp's largest remaining value; the lowest lane holding it gives it up
+    double m = v[0];
+#pragma unroll
+    for (int u = 1; u < kFCap / 32; ++u) m = fmax(m, v[u]);
+    double wm = m;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wm = fmax(wm, __shfl_xor_sync(0xffffffffu, wm, o));
+    const unsigned holders = __ballot_sync(0xffffffffu, m == wm && wm > -INFINITY);
+    if (holders && lane == __ffs(holders) - 1) {
+      bool done = false;
+#pragma unroll
+      for (int u = 0; u < kFCap / 32; ++u)
+        if (!done && v[u] == wm) {
+          v[u] = -INFINITY;
+          done = true;
+        }
+    }
+    if (lane == 0) plist[P * use_k + e] = holders ? wm : -INFINITY;
+  }
 }
 
 CUtensorMap make_bf16_rows_map(const __nv_bfloat16* p, int rows_pad) {
@@ -1032,7 +1011,8 @@ void candidate_centroids_device(const double* dTn, int n, int k, const int* dy, 
 
 void candidate_knn_predict_device(const double* dTt, int ntest, const double* dTr, int ntrain, int kdim,
                                   const int* dy, const double* dC, int C, const double* dbias, int top_k,
-                                  int top_m, int knn_k, double tau, double alpha, int* d_ti, double* d_ts) {
+                                  int top_m, int knn_k, double tau, double alpha, int* d_ti, double* d_ts,
+                                  bool allow_filter) {
   Context& ctx = Context::get();
   const int tk = std::max(1, std::min(top_k, C));
   const int tm = std::max(tk, std::min(std::max(1, top_m), C));
@@ -1083,7 +1063,7 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
   // training-row buffers.
   const char* tv = std::getenv("FASTPLS_CKNN_TILES");
   const char sel = (tv && tv[0]) ? tv[0] : '4';
-  const bool use_filter = sel == '4' && kdim <= kFK && use_k <= kFList && ntrain < (1 << 24);
+  const bool use_filter = allow_filter && sel == '4' && kdim <= kFK && use_k <= kFList;
   const int tile_m = use_filter ? kFT : kTileM;   // pairs per item
   const int gran = use_filter ? kFT : kTileN;     // chunk rows are a multiple of this
   std::vector<int> poffs(C + 1, 0), chunk_rows(C, 0), nchunks(C, 0);
@@ -1131,6 +1111,10 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
   double* part = ctx.arena.alloc_n<double>((size_t)std::max<long long>(part_total, 1));
   double* cscore = ctx.arena.alloc_n<double>((size_t)npairs);
   pt.mark("class rows + pair lists");
+  // the lists the merge reads: (pair, chunk) lists of the FP64 tiles, or one
+  // exact list per pair from the filter
+  KnnClassInfo ci_merge = ci;
+  const double* merge_part = part;
   if (!items.empty() && use_filter) {
     const KnnItem* ditems = upload(items.data(), items.size());
     FPLS_REQUIRE(items.size() < (1u << 31), "candidate-kNN: too many work items");
@@ -1162,6 +1146,9 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
     float* barv = ctx.arena.alloc_n<float>((size_t)std::max<long long>(total_pairs, 1));
     int* ferr = ctx.d_status + 24;
     dzero(ferr, sizeof(int));
+    int* ccount = ctx.arena.alloc_n<int>((size_t)std::max<long long>(total_pairs, 1));
+    int* crow = ctx.arena.alloc_n<int>((size_t)std::max<long long>(total_pairs, 1) * kFCap);
+    dzero(ccount, (size_t)std::max<long long>(total_pairs, 1) * sizeof(int));
     static bool fattr = false;
     if (!fattr) {
       FPLS_CUDA(cudaFuncSetAttribute(knn_filter_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
@@ -1170,7 +1157,8 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
     }
     const unsigned ng = (unsigned)items.size();
     knn_filter_kernel<1><<<ng, kFThreads, kFSmem, ctx.stream>>>(mAh, mAl, mBh, mBl, ditems, ci, pairs, ntest, Tq,
-                                                               cr.Ts, kdim, use_k, apart, nullptr, nullptr, ferr);
+                                                               cr.Ts, kdim, use_k, apart, nullptr, nullptr, nullptr,
+                                                               ferr);
     ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     pt.mark("filter pass 1");
@@ -1180,10 +1168,26 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
     FPLS_CHECK_LAUNCH();
     pt.mark("filter bar");
     knn_filter_kernel<2><<<ng, kFThreads, kFSmem, ctx.stream>>>(mAh, mAl, mBh, mBl, ditems, ci, pairs, ntest, Tq,
-                                                               cr.Ts, kdim, use_k, nullptr, barv, part, ferr);
+                                                               cr.Ts, kdim, use_k, nullptr, barv, ccount, crow,
+                                                               ferr);
     ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     pt.mark("filter pass 2");
+    // exact scores of the candidates, one list per pair
+    double* plist = ctx.arena.alloc_n<double>((size_t)std::max<long long>(total_pairs, 1) * use_k);
+    int* fover = ctx.d_status + 25;
+    dzero(fover, sizeof(int));
+    knn_exact_kernel<<<(unsigned)ceil_div(total_pairs * 32, 256), 256, 0, ctx.stream>>>(
+        ccount, crow, pairs, total_pairs, ntest, Tq, cr.Ts, kdim, use_k, plist, fover);
+    ::fpls::note_launch();
+    FPLS_CHECK_LAUNCH();
+    pt.mark("filter exact scores");
+    std::vector<int> ones(C, 1);
+    std::vector<long long> pbase(C);
+    for (int c = 0; c < C; ++c) pbase[c] = (long long)poffs[c] * use_k;
+    ci_merge.nchunks = upload(ones.data(), C);
+    ci_merge.part_base = upload(pbase.data(), C);
+    merge_part = plist;
     if (slot >= 0) {
       // algorithmic work: the three BF16 products of both passes over every
       // (candidate pair, class row); bytes: the score planes of every class's
@@ -1196,10 +1200,17 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
       }
       ctx.prof_end(slot, ctx.stream, bytes, 2.0 * 3.0 * 2.0 * work * kdim);
     }
-    int ferr_h = 0;
-    d2h(&ferr_h, ferr, sizeof(int));
+    int flags[2] = {0, 0};
+    d2h(flags, ferr, 2 * sizeof(int));
     ctx.sync();
-    if (ferr_h) throw Error(kErrCuda, "candidate-kNN: a filter tile's pipeline wait timed out");
+    if (flags[0]) throw Error(kErrCuda, "candidate-kNN: a filter tile's pipeline wait timed out");
+    if (flags[1]) {
+      // a pair had more rows within the error bar than its candidate slots
+      // hold: the call runs again on the FP64 tiles
+      candidate_knn_predict_device(dTt, ntest, dTr, ntrain, kdim, dy, dC, C, dbias, top_k, top_m, knn_k, tau,
+                                   alpha, d_ti, d_ts, false);
+      return;
+    }
   } else if (!items.empty()) {
     const KnnItem* ditems = upload(items.data(), items.size());
     FPLS_REQUIRE(items.size() < (1u << 31), "candidate-kNN: too many work items");
@@ -1268,7 +1279,8 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
   fill(cscore, (size_t)npairs, -INFINITY);
   if (total_pairs > 0) {
     knn_merge_kernel<<<ceil_div(total_pairs, 128), 128, 0, ctx.stream>>>(
-        pairs, total_pairs, cand, cbase, ci, part, use_k, tau_e, alpha_e, dbias, cscore); ::fpls::note_launch();
+        pairs, total_pairs, cand, cbase, ci_merge, merge_part, use_k, tau_e, alpha_e, dbias, cscore);
+    ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
   }
   knn_rerank_kernel<<<ceil_div(ntest, 128), 128, 0, ctx.stream>>>(cand, cscore, ntest, C, tm, tk, d_ti, d_ts); ::fpls::note_launch();

@@ -101,15 +101,18 @@ def test_candidate_knn_staged_tiles_match_oracle(lib, monkeypatch, kdim, buffers
     _check(got, ref)
 
 
-def test_candidate_knn_filter_near_ties(lib, monkeypatch):
+@pytest.mark.parametrize("copies", [8, 40])
+def test_candidate_knn_filter_near_ties(lib, monkeypatch, copies):
     # training rows that are copies of one another up to 1e-7: many
     # approximate similarities fall inside the filter's error bar around a
-    # pair's k-th neighbour, so the exact rescoring decides the list
+    # pair's k-th neighbour, so the exact rescoring decides the list (8
+    # copies); with 40 copies a pair has more such rows than its candidate
+    # slots and the call falls back to the FP64 tiles
     monkeypatch.setenv("FASTPLS_CKNN_TILES", "4")
     rng = np.random.default_rng(21)
     base, y, Tt = _zipf_case(22, 400, 90, 6, 32)
-    Tr = ok.row_l2(np.repeat(base, 8, axis=0) + 1e-7 * rng.standard_normal((3200, 32)))
-    y = np.repeat(y, 8).astype(np.int32)
+    Tr = ok.row_l2(np.repeat(base, copies, axis=0) + 1e-7 * rng.standard_normal((400 * copies, 32)))
+    y = np.repeat(y, copies).astype(np.int32)
     cents = ok.centroids(Tr, y, 6)
     got = lib.candidate_knn_predict(Tt, Tr, y, cents, top_k=3, top_m=4, knn_k=12, tau=0.2, alpha=0.75)
     ref = ok.candidate_knn_predict(Tt, Tr, y, cents, top_k=3, top_m=4, knn_k=12, tau=0.2, alpha=0.75)

@@ -167,8 +167,8 @@ KERNEL_CLASSES = {
     "gram_bf16x3": ("bf16", "split_gemm_kernel<2, 128> (tcgen05 BF16x3 row Gram, upper tiles)",
                     "gram_bf16x3_c4_traffic.json"),
     "gram_bf16x6": ("bf16", "split_gemm_kernel<3, 64> (tcgen05 BF16x6 row Gram, upper tiles)", None),
-    "split_gemm_bf16x3": ("bf16", "split_gemm_kernel<2, 64> (tcgen05 BF16x3 split GEMM)", "split_gemm_c4_traffic.json"),
-    "split_gemm_bf16x6": ("bf16", "split_gemm_kernel<3, 64> (tcgen05 BF16x6 split GEMM)", None),
+    "split_gemm_bf16x3": ("bf16", "split_gemm_kernel<2, 64 | 128> (tcgen05 BF16x3 split GEMM)", "split_gemm_c4_traffic.json"),
+    "split_gemm_bf16x6": ("bf16", "split_gemm_kernel<3, 64 | 128> (tcgen05 BF16x6 split GEMM)", None),
     "gemm_f64_dmma": ("fp64", "gemm_f64_dmma (FP64 DMMA m8n8k4 tiles)", None),
     "gemv_f64": (None, "gemv_n / gemv_t (FP64 matrix-vector passes over X)", None),
     "cknn_tiles": ("fp64", "knn_tile_kernel_v2<1> (class-grouped 64x64 FP64 DMMA similarity tiles, contraction "

@@ -450,7 +450,12 @@ __global__ void mirror_upper_f64_kernel(double* K, int n, int ldk) {
   }
 }
 
-void gram_f64(const double* X, int n, int p, int ldx, double* K, int ldk) {
+namespace {
+// Upper tiles of op(X) op(X)^T (n x n) with n = rows of op(X) and p its
+// columns, split-K partials summed in range order, then the lower triangle
+// mirrored.  TX: X is stored p x n (op(X) = X^T).
+template <bool TX>
+void gram_tiles_f64(const double* X, int n, int p, int ldx, double* K, int ldk) {
   if (n <= 0) return;
   Context& ctx = Context::get();
   cudaStream_t st = ctx.stream;
@@ -474,8 +479,11 @@ void gram_f64(const double* X, int n, int p, int ldx, double* K, int ldk) {
       dst = ctx.splitk_workspace(st, (size_t)splits * n * n);
       ldd = n;
     }
-    gemm_f64_dmma<false, true><<<dim3(g, g, splits), GEMM_THREADS, 0, st>>>(n, n, p, 1.0, X, ldx, X, ldx, 0.0, dst,
-                                                                         ldd, kps, stride, 1); ::fpls::note_launch();
+    const int slot = ctx.prof_begin("gemm_f64_dmma", st);
+    gemm_f64_dmma<TX, !TX><<<dim3(g, g, splits), GEMM_THREADS, 0, st>>>(n, n, p, 1.0, X, ldx, X, ldx, 0.0, dst,
+                                                                       ldd, kps, stride, 1); ::fpls::note_launch();
+    // algorithmic work: the upper tiles' share of 2 n^2 p flops
+    ctx.prof_end(slot, st, 8.0 * ((double)n * p + (double)n * n), (double)n * (n + BM) * p);
     FPLS_CHECK_LAUNCH();
     if (splits > 1) {
       splitk_reduce_kernel<<<grid_for((size_t)n * n, 256), 256, 0, st>>>(dst, splits, stride, n, n, ldd, 0.0, K,
@@ -486,6 +494,15 @@ void gram_f64(const double* X, int n, int p, int ldx, double* K, int ldk) {
   }
   mirror_upper_f64_kernel<<<grid_for((size_t)n * n, 256), 256, 0, st>>>(K, n, ldk); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+}
+}  // namespace
+
+void gram_f64(const double* X, int n, int p, int ldx, double* K, int ldk) {
+  gram_tiles_f64<false>(X, n, p, ldx, K, ldk);
+}
+
+void gram_t_f64(const double* S, int p, int q, int lds, double* G, int ldg) {
+  gram_tiles_f64<true>(S, q, p, lds, G, ldg);
 }
 
 void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda, const double* x,

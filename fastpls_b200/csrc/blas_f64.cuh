@@ -18,6 +18,9 @@ void gemm(bool transA, bool transB, int M, int N, int K, double alpha,
 // MMA, the lower triangle mirrored (K exactly symmetric).
 void gram_f64(const double* X, int n, int p, int ldx, double* K, int ldk);
 
+// G (q x q) = S^T S for S p x q (lds): the same upper-tile product, mirrored.
+void gram_t_f64(const double* S, int p, int q, int lds, double* G, int ldg);
+
 // y = alpha * op(A) * x + beta * y.  A is rows x cols (lda).
 void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda,
           const double* x, double beta, double* y);

@@ -101,8 +101,9 @@ void leading_left_vector(const double* S, int p, int q, double* u, unsigned int 
     return;
   }
   double* G = ctx.arena.alloc_n<double>((size_t)m * m);
-  if (right) gemm(true, false, q, q, p, 1.0, S, p, S, p, 0.0, G, q);
-  else gemm(false, true, p, p, q, 1.0, S, p, S, p, 0.0, G, p);
+  // the Gram matrix by its upper tiles only (half the multiply-adds), mirrored
+  if (right) gram_t_f64(S, p, q, p, G, q);
+  else gram_f64(S, p, q, p, G, p);
   const int l = std::min(m, 8);
   double* Y = ctx.arena.alloc_n<double>((size_t)m * l);
   double* Q = ctx.arena.alloc_n<double>((size_t)m * l);

@@ -78,6 +78,7 @@ template <int NP, int TN> struct Planes {
 };
 static_assert(Planes<3, 64>::SMEM_BYTES <= 227 * 1024, "three-plane stages exceed shared memory");
 static_assert(Planes<2, 128>::SMEM_BYTES <= 227 * 1024, "wide-tile stages exceed shared memory");
+static_assert(Planes<3, 128>::SMEM_BYTES <= 227 * 1024, "three-plane wide-tile stages exceed shared memory");
 constexpr int NUM_THREADS = 192;
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -626,7 +627,7 @@ void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K,
                     double beta, double* C, int ldc, const GemmPlan& g, const GemmScratch& s,
                     int* err, cudaStream_t st, Context* prof) {
   FPLS_REQUIRE(A.np == B.np && (A.np == 2 || A.np == 3), "split GEMM: operands with different plane counts");
-  FPLS_REQUIRE(g.bn == BN || (g.bn == BN_SYM && A.np == 2), "split GEMM: unsupported tile width");
+  FPLS_REQUIRE(g.bn == BN || g.bn == BN_SYM, "split GEMM: unsupported tile width");
   const CUtensorMap maps[6] = {make_map(A.hi, M, K, A.ld, BM),
                                make_map(A.np == 3 ? A.mid : A.lo, M, K, A.ld, BM),
                                make_map(A.lo, M, K, A.ld, BM),
@@ -639,9 +640,14 @@ void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K,
                                                       : (A.np == 3 ? "split_gemm_bf16x6" : "split_gemm_bf16x3"),
                                            st)
                         : -1;
-  if (A.np == 3) launch_split_kernel<3, BN>(maps, g, s, err, st);
-  else if (g.bn == BN_SYM) launch_split_kernel<2, BN_SYM>(maps, g, s, err, st);
-  else launch_split_kernel<2, BN>(maps, g, s, err, st);
+  if (A.np == 3) {
+    if (g.bn == BN_SYM) launch_split_kernel<3, BN_SYM>(maps, g, s, err, st);
+    else launch_split_kernel<3, BN>(maps, g, s, err, st);
+  } else if (g.bn == BN_SYM) {
+    launch_split_kernel<2, BN_SYM>(maps, g, s, err, st);
+  } else {
+    launch_split_kernel<2, BN>(maps, g, s, err, st);
+  }
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   if (prof) {
@@ -691,6 +697,19 @@ const CachedPlan& cached_plan(int M, int N, int K, int sm_count, cudaStream_t st
   return cache.emplace(key, std::move(c)).first->second;
 }
 
+// General products with at least this many rows and columns run on 128 x 128
+// tiles (FASTPLS_WIDE_TILES=0: 128 x 64): twice the multiply-adds per operand
+// byte of the 128 x 64 tiles, which the fat predictor-by-response products
+// (X^T Y of the OPLS filter: 20000 x 5000 over 50000 rows) are bound by.
+constexpr int kWideMinM = 2048, kWideMinN = 512;
+bool general_wide_tiles(int M, int N) {
+  static const int v = [] {
+    const char* e = std::getenv("FASTPLS_WIDE_TILES");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return v && M >= kWideMinM && N >= kWideMinN;
+}
+
 bool sym_wide_tiles() {
   if (const char* e = std::getenv("FASTPLS_GRAM_TILE")) return std::string(e) != "64";
   return active_tune().gram_tile != 64;
@@ -702,7 +721,7 @@ void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, dou
   // Symmetric two-plane products (the row Gram) on 128 x 128 tiles: half the
   // B re-reads of the 128 x 64 tiles and twice the MACs per operand byte read
   // by the tensor core.
-  const int bn = (upper && A.np == 2 && sym_wide_tiles()) ? BN_SYM : BN;
+  const int bn = ((upper && A.np == 2 && sym_wide_tiles()) || (!upper && general_wide_tiles(M, N))) ? BN_SYM : BN;
   const CachedPlan& c = cached_plan(M, N, K, ctx.sm_count, ctx.stream, upper, A.np == 3, bn);
   split_gemm_run(A, B, M, N, K, alpha, beta, C, ldc, c.g, c.s, ctx.d_status + 16, ctx.stream,
                  ctx.profile ? &ctx : nullptr);

@@ -34,6 +34,17 @@ def test_bf16x3_gemm_exact_inputs(lib):
     assert np.array_equal(C, A @ B)
 
 
+def test_bf16x3_gemm_wide_tiles_exact(lib):
+    # a product with at least 2048 rows and 512 columns runs on 128 x 128
+    # tiles: exact inputs must give the exact product there too, at the N edge
+    # (700 columns: a partial last tile) included
+    rng = np.random.default_rng(4)
+    A = rng.integers(-8, 9, size=(2300, 320)).astype(np.float64) / 8.0
+    B = rng.integers(-8, 9, size=(320, 700)).astype(np.float64) / 4.0
+    C = lib.bf16x3_gemm(A, B)
+    assert np.array_equal(C, A @ B)
+
+
 @pytest.fixture(scope="module")
 def c4_small():
     d = synthetic.c4_omics(seed=2, n=360, p=600, n_informative=20)

@@ -112,3 +112,13 @@ def test_plssvd_two_plane_mode(lib, both, c2_mid):
 
     p64, pbf = both(fit, "bf16x3")
     assert rel_err(pbf, p64) < 2e-4
+
+
+def test_opls_filter_mixed_wide_tiles(lib, both):
+    # X^T Y of the filter (2100 x 600) takes the 128 x 128 three-plane tiles
+    d = synthetic.c5_lowrank(seed=11, n=2500, p=2100, q=600, rank=10, n_test=10)
+    X = d["Xtrain"].astype(np.float64)
+    Y = d["Ytrain"].astype(np.float64)
+    ref, got = both(lambda: lib.opls_filter(X, Y, 2))
+    assert got["north"] == ref["north"] == 2
+    assert rel_err(got["X"], ref["X"]) < MIXED_TOL

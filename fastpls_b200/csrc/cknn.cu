@@ -686,12 +686,13 @@ knn_filter_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant
 #pragma unroll
       for (int g = 0; g < 4; ++g) {
         // values past the class's last training row (or of an absent pair
-        // row) cannot enter a list
+        // row) are NaN: they fail every comparison, so they neither raise a
+        // bucket maximum nor become candidates (not even for a bar of -inf)
         float f[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const bool in = ok && row_ok && h * 64 + g * 16 + i < ncol;
-          f[i] = in ? __uint_as_float(v[g][i]) : -INFINITY;
+          f[i] = in ? __uint_as_float(v[g][i]) : __int_as_float(0x7fc00000);
         }
         if (PASS == 1) {
 #pragma unroll
@@ -816,9 +817,10 @@ __global__ void knn_filter_bar_kernel(const float* __restrict__ apart, KnnClassI
 }
 
 // Exact scores of the candidates of every pair (one warp per class-sorted
-// pair): each lane takes candidates lane, lane + 32, ... and forms their FP64
-// dots (k in order); the use_k largest go to plist[P * use_k ..] in
-// descending order (-inf when there are fewer).  A pair with more than kFCap
+// pair): up to 32 candidates, the lanes split each FP64 dot; more, each lane
+// takes candidates lane, lane + 32, ... and forms their dots (k in order).  The
+// use_k largest go to plist[P * use_k ..] in descending order (-inf when there
+// are fewer).  A pair with more than kFCap
 // candidates raises *overflow (its list would be incomplete).
 __global__ void knn_exact_kernel(const int* __restrict__ ccount, const int* __restrict__ crow,
                                  const int* __restrict__ pairs, long long total_pairs, int ntest,
@@ -833,6 +835,41 @@ __global__ void knn_exact_kernel(const int* __restrict__ ccount, const int* __re
     cnt = kFCap;
   }
   const double* xr = Tq + (size_t)(pairs[P] % ntest) * K;
+  if (cnt <= 32) {
+    // The common case: the warp's lanes split every dot (four candidates at a
+    // time, the test row loaded once), lane c keeps candidate c's value, and
+    // each value goes to its rank in the descending list (ties by lane).
+    double xv[kFK / 32];
+#pragma unroll
+    for (int m = 0; m < kFK / 32; ++m) xv[m] = (lane + 32 * m < K) ? xr[lane + 32 * m] : 0.0;
+    double mine = -INFINITY;
+    for (int c0 = 0; c0 < cnt; c0 += 4) {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (c0 + c < cnt) {
+          const double* yr = Ts + (size_t)crow[(size_t)P * kFCap + c0 + c] * K;
+#pragma unroll
+          for (int m = 0; m < kFK / 32; ++m)
+            if (lane + 32 * m < K) acc[c] = fma(xv[m], yr[lane + 32 * m], acc[c]);
+        }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (lane == c0 + c && c0 + c < cnt) mine = acc[c];
+    }
+    if (!(mine == mine)) mine = -INFINITY;   // a NaN never enters a list
+    int rank = 0;
+    for (int j = 0; j < 32; ++j) {
+      const double vj = __shfl_sync(0xffffffffu, mine, j);
+      rank += (vj > mine || (vj == mine && j < lane)) ? 1 : 0;
+    }
+    if (rank < use_k) plist[P * use_k + rank] = mine;
+    return;
+  }
   double v[kFCap / 32];
 #pragma unroll
   for (int u = 0; u < kFCap / 32; ++u) {
@@ -1192,6 +1229,7 @@ void candidate_knn_predict_device(const double* dTt, int ntest, const double* dT
       // algorithmic work: the three BF16 products of both passes over every
       // (candidate pair, class row); bytes: the score planes of every class's
       // training rows once per 128-pair tile and pass, the pair planes once
+      // (the class's time includes the planes, the bar and the exact scores)
       double work = 0.0, bytes = 2.0 * 4.0 * kFK * (double)total_pairs;
       for (int c = 0; c < C; ++c) {
         const double rows = cr.offs[c + 1] - cr.offs[c];

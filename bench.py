@@ -438,16 +438,16 @@ def config_c2(lib, args, peaks, local):
     d = synthetic.c2_plsda(seed=1)
     X, Xt = d["Xtrain"], d["Xtest"]          # FP32, column-major
     y, C, K = d["ytrain"], d["n_classes"], 50
-    Y = opls.transformy(y)
+    Y = np.asfortranarray(opls.transformy(y), dtype=np.float64)
     n, p = X.shape
     nt = Xt.shape[0]
-    Xd, Xtd = _dev(torch, X), _dev(torch, Xt)
+    Xd, Xtd, Yd = _dev(torch, X), _dev(torch, Xt), _dev(torch, Y)
     torch.cuda.synchronize()
     kw = dict(method=1, oversample=10, power_iters=2, seed=1, store_B=False)
 
-    def step(Xa, Xta):
+    def step(Xa, Xta, Ya):
         def fn():
-            r = lib.pls_lda(Xa, Y, y, Xta, [K], C, **kw)
+            r = lib.pls_lda(Xa, Ya, y, Xta, [K], C, **kw)
             return r, lib.last_call_ms()
         return fn
 
@@ -456,15 +456,17 @@ def config_c2(lib, args, peaks, local):
     for prec in ("fp64", "bf16x3"):
         lib.set_precision(prec)
         try:
-            r_d, ms_d, _ = _timed_calls(lib, step(Xd, Xtd), steps, max(args.warmup, 2))
+            r_d, ms_d, _ = _timed_calls(lib, step(Xd, Xtd, Yd), steps, max(args.warmup, 2))
             lib.host_register(X)
             lib.host_register(Xt)
+            lib.host_register(Y)
             try:
-                r_h, ms_h, wall_h = _timed_calls(lib, step(X, Xt), steps, 1)
+                r_h, ms_h, wall_h = _timed_calls(lib, step(X, Xt, Y), steps, 1)
             finally:
                 lib.host_unregister(X)
                 lib.host_unregister(Xt)
-            kr = _profile_step(lib, step(Xd, Xtd), peaks)
+                lib.host_unregister(Y)
+            kr = _profile_step(lib, step(Xd, Xtd, Yd), peaks)
         finally:
             lib.set_precision("fp64")
         res[prec] = (r_d, ms_d, ms_h, wall_h, kr)

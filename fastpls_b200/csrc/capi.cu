@@ -933,11 +933,13 @@ int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const doubl
     const bool f32 = x_is_float32 != 0;
     Context& ctx = Context::get();
     ctx.begin_call();
+    PhaseTimer pt("PLS + LDA call");
     std::vector<int> nc(ncomp, ncomp + L);
     for (int& c : nc) c = std::max(1, c);
     // one upload of each matrix for the whole pipeline
     double* dX = upload_widened(Xtrain, f32, (size_t)n * p);
     double* dY = upload(Ytrain, (size_t)n * m);
+    pt.mark("X, Y to FP64");
     int K0 = 0;
     double* dR = nullptr;
     double* dT = nullptr;   // training scores (X - mX) / vX R, n x K0
@@ -950,6 +952,7 @@ int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const doubl
       double* dvX = ctx.arena.alloc_n<double>(p);
       double* dmY = ctx.arena.alloc_n<double>(m);
       center_scale_xy(dX, n, p, dY, m, scaling, dmX, dvX, dmY);
+      pt.mark("centre / scale");
       FitOptions opt;
       opt.scaling = scaling;
       opt.fit = fit != 0;
@@ -971,6 +974,7 @@ int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const doubl
       std::vector<double> r2(L, 0.0);
       o.R2Y = r2.data();
       plssvd_fit_centered(dX, n, p, dY, m, nc.data(), L, K0, opt, dmY, o);
+      pt.mark("PLSSVD fit");
       download(Q, o.Q, (size_t)m * K0);
       download(mY, dmY, m);
       if (B) download(B, o.B, (size_t)p * m * L);
@@ -980,6 +984,7 @@ int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const doubl
       download(hmX.data(), dmX, p);
       download(hvX.data(), dvX, p);
       ctx.sync();
+      pt.mark("fit outputs to host");
       if (R2Y) std::copy(r2.begin(), r2.end(), R2Y);
     } else {
       K0 = max_of(nc.data(), L);
@@ -1026,8 +1031,11 @@ int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const doubl
     d.priors = ctx.arena.alloc_n<double>(n_classes);
     std::vector<double> lam(U);
     d.lambda = lam.data();
+    pt.mark("prediction weights (host)");
     lda_train_prefix(dT, n, K0, y, n_classes, uq.data(), U, lda_ridge, d);
+    pt.mark("LDA train");
     lda_outputs_to_host(d, n_classes, K0, U, lda_means, lda_linear, lda_constants, lda_priors);
+    pt.mark("LDA outputs to host");
     if (ntest > 0) {
       const double* dXt = upload_widened(Xtest, f32, (size_t)ntest * p);
       const double* dRp = upload(hRp.data(), (size_t)p * K0);
@@ -1041,8 +1049,10 @@ int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const doubl
                                   n_classes, dc, n_classes, dpred + (size_t)i * ntest, nullptr);
       }
       download(pred_codes, dpred, (size_t)ntest * L);
+      pt.mark("test prediction");
     }
     ctx.sync();
+    pt.report();
     if (lda_lambda) std::copy(lam.begin(), lam.end(), lda_lambda);
     if (n_unique) *n_unique = U;
     if (unique_ncomp) std::copy(uq.begin(), uq.end(), unique_ncomp);

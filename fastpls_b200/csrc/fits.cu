@@ -195,6 +195,7 @@ void center_scale_xy(double* X, int n, int p, double* Y, int m, int scaling, dou
 int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, const int* ncomp,
                         int L, int K0, const FitOptions& opt, const double* mY, PlssvdOut out) {
   Context& ctx = Context::get();
+  PhaseTimer pt("PLSSVD fit");
   const int max_rank = static_cast<int>(std::min<long long>(shard_rows(n), std::min(p, m)));
   double* S = nullptr;
   if (!opt.xprod) {
@@ -202,6 +203,7 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
     xgemm(true, p, m, n, X, n, Y, n, S, p);
     shard_sum(S, (size_t)p * m);
   }
+  pt.mark("S = X^T Y");
   int thr = 32;
   if (const char* e = std::getenv("FASTPLS_PLSSVD_SMALL_EXACT_MAX_RANK")) {
     char* endp = nullptr;
@@ -218,6 +220,7 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
                      : truncated_svd_device(S, p, m, p, K0, opt.svd_method, opt.oversample,
                                             opt.power_iters, opt.seed, false, small_exact, out.R, p,
                                             out.s, out.Q, m);
+  pt.mark("SVD of S");
   int keff = std::min(K0, sr.rank);
   FPLS_REQUIRE(keff >= 1, "plssvd effective rank is < 1 after SVD");
   dzero(out.T, (size_t)n * K0 * sizeof(double));
@@ -225,6 +228,7 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
   double* G = ctx.arena.alloc_n<double>((size_t)keff * keff);
   gemm(true, false, keff, keff, n, 1.0, out.T, n, out.T, n, 0.0, G, keff);
   shard_sum(G, (size_t)keff * keff);
+  pt.mark("T = X R, G");
   dzero(out.C_latent, (size_t)K0 * K0 * L * sizeof(double));
   dzero(out.W_latent, (size_t)K0 * m * L * sizeof(double));
   double* D = ctx.arena.alloc_n<double>((size_t)keff * keff);
@@ -263,6 +267,8 @@ int plssvd_fit_centered(const double* X, int n, int p, const double* Y, int m, c
   int st = 0;
   d2h(&st, ctx.d_status + 2, sizeof(int));
   ctx.sync();
+  pt.mark("latent solves");
+  pt.report();
   if (st) throw Error(kErrNumerical, "plssvd latent solve failed");
   return keff;
 }

@@ -185,8 +185,11 @@ __device__ void round_robin_next(int* arr, int n) {
   arr[1] = last;
 }
 
+// With in_smem the working matrices W and V live in shared memory (after the
+// rotation tables): W is copied in first, and every rotation round touches
+// shared memory only.
 __global__ void jacobi_eig_kernel(int l, double* W, double* V, double* evals_out,
-                                  double* V_out, int ldv, const int max_sweeps) {
+                                  double* V_out, int ldv, const int max_sweeps, int in_smem) {
   extern __shared__ double sm[];
   const int npair = (l + 1) / 2;
   const int le = 2 * npair;
@@ -197,8 +200,14 @@ __global__ void jacobi_eig_kernel(int l, double* W, double* V, double* evals_out
   int* qq = pp + npair;         // [npair]
   __shared__ double scratch[32];
   __shared__ int sweep_done;
+  if (in_smem) {
+    double* Ws = reinterpret_cast<double*>(reinterpret_cast<char*>(sm) + 32 * npair);
+    for (int t = threadIdx.x; t < l * l; t += blockDim.x) Ws[t] = W[t];
+    W = Ws;
+    V = Ws + (size_t)l * l;
+  }
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) V[t] = (t % l == t / l) ? 1.0 : 0.0;
-  if (threadIdx.x == 0) for (int i = 0; i < le; ++i) arr[i] = i;
+  __shared__ int rotated;
   __syncthreads();
   // Frobenius norm for the convergence test.
   double fro = 0.0;
@@ -212,12 +221,19 @@ __global__ void jacobi_eig_kernel(int l, double* W, double* V, double* evals_out
       if (i != j) off += W[t] * W[t];
     }
     off = block_sum(off, scratch);
-    if (threadIdx.x == 0) sweep_done = (off <= thresh) ? 1 : 0;
+    if (threadIdx.x == 0) {
+      sweep_done = (off <= thresh) ? 1 : 0;
+      rotated = 0;
+    }
     __syncthreads();
     if (sweep_done) break;
     for (int r = 0; r < le - 1; ++r) {
+      // round-robin pairing of round r: position 0 stays, positions 1..le-1
+      // have turned r places (position i holds 1 + (i - 1 - r) mod (le - 1))
       for (int k = threadIdx.x; k < npair; k += blockDim.x) {
-        int p = arr[k], q = arr[le - 1 - k];
+        const int ik = le - 1 - k;
+        int p = k == 0 ? 0 : 1 + ((k - 1 - r) % (le - 1) + (le - 1)) % (le - 1);
+        int q = 1 + ((ik - 1 - r) % (le - 1) + (le - 1)) % (le - 1);
         if (p > q) { const int t = p; p = q; q = t; }
         pp[k] = p; qq[k] = q;
         double c = 1.0, s = 0.0;
@@ -225,11 +241,13 @@ __global__ void jacobi_eig_kernel(int l, double* W, double* V, double* evals_out
           const double apq = W[p + (size_t)q * l];
           const double app = W[p + (size_t)p * l];
           const double aqq = W[q + (size_t)q * l];
-          if (apq != 0.0 && fabs(apq) > 1e-300) {
+          // a rotation is skipped once the pair is decoupled to rounding
+          if (apq != 0.0 && fabs(apq) > 1e-300 && fabs(apq) > kEps * sqrt(fabs(app * aqq))) {
             const double tau = (aqq - app) / (2.0 * apq);
             const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
             c = 1.0 / sqrt(1.0 + t * t);
             s = t * c;
+            rotated = 1;
           }
         }
         cs[k] = c; sn[k] = s;
@@ -260,9 +278,8 @@ __global__ void jacobi_eig_kernel(int l, double* W, double* V, double* evals_out
         V[i + (size_t)q * l] = s * vp + c * vq;
       }
       __syncthreads();
-      if (threadIdx.x == 0) round_robin_next(arr, le);
-      __syncthreads();
     }
+    if (!rotated) break;   // a whole sweep without a rotation: converged
   }
   // Sort eigenvalues descending (selection order kept in arr).
   if (threadIdx.x == 0) {
@@ -478,8 +495,18 @@ void eig_sym_desc(int l, const double* G, int ldg, double* evals, double* V, int
   double* Vw = ctx.arena.alloc_n<double>((size_t)l * l);
   copy_matrix(W, l, G, ldg, l, l);
   const int npair = (l + 1) / 2;
-  const size_t smem = (size_t)npair * 2 * sizeof(double) + (size_t)(2 * npair + 2 * npair) * sizeof(int) + 64;
-  jacobi_eig_kernel<<<1, 1024, smem, ctx.stream>>>(l, W, Vw, evals, V, ldv, 60); ::fpls::note_launch();
+  const size_t tables = (size_t)npair * 2 * sizeof(double) + (size_t)(2 * npair + 2 * npair) * sizeof(int);
+  const size_t with_mats = tables + 2 * (size_t)l * l * sizeof(double) + 64;
+  constexpr size_t kEigSmemMax = 200 * 1024;
+  const bool in_smem = with_mats <= kEigSmemMax;
+  static bool attr_set = false;
+  if (!attr_set) {
+    FPLS_CUDA(cudaFuncSetAttribute(jacobi_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEigSmemMax));
+    attr_set = true;
+  }
+  const size_t smem = in_smem ? with_mats : tables + 64;
+  jacobi_eig_kernel<<<1, 1024, smem, ctx.stream>>>(l, W, Vw, evals, V, ldv, 60, in_smem ? 1 : 0);
+  ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 

@@ -69,8 +69,10 @@ SvdResult truncated_svd_device(const double* A, int rows, int cols, int lda, int
   if (l >= max_rank) return exact_svd(A, rows, cols, lda, target, left_only, U, ldu, s, V, ldv);
 
   Context& ctx = Context::get();
+  PhaseTimer pt("randomized SVD");
   double* Omega = ctx.arena.alloc_n<double>((size_t)cols * l);
   device_gaussian(Omega, (long long)cols * l, seed);
+  pt.mark("sketch");
   double* Y = ctx.arena.alloc_n<double>((size_t)rows * l);
   double* Z = ctx.arena.alloc_n<double>((size_t)cols * l);
   double* Qz = ctx.arena.alloc_n<double>((size_t)cols * l);
@@ -86,9 +88,11 @@ SvdResult truncated_svd_device(const double* A, int rows, int cols, int lda, int
       gemm(false, false, rows, l, cols, 1.0, A, lda, Qz, cols, 0.0, Y, rows);
     }
   }
+  pt.mark("power iterations");
   // finalize_rsvd_from_sample (src/svd_cpu_rsvd.cpp:26-93)
   double* Q = ctx.arena.alloc_n<double>((size_t)rows * l);
   qr_orthonormalize(rows, l, Y, rows, Q, rows);
+  pt.mark("QR of the sample");
   double* B = ctx.arena.alloc_n<double>((size_t)l * cols);
   gemm(true, false, l, cols, rows, 1.0, Q, rows, A, lda, 0.0, B, l);
   const int rank = std::min(max_rank, std::max(k, 1));
@@ -102,6 +106,7 @@ SvdResult truncated_svd_device(const double* A, int rows, int cols, int lda, int
     std::vector<double> evh(l);
     d2h(evh.data(), ev, l * sizeof(double));
     ctx.sync();
+    pt.mark("eig of B B^T");
     const double eps = std::numeric_limits<double>::epsilon();
     const double tol = eps * static_cast<double>(std::max(l, cols)) * std::max(evh[0], 1.0);
     int usable = 0;
@@ -117,6 +122,8 @@ SvdResult truncated_svd_device(const double* A, int rows, int cols, int lda, int
         FPLS_CHECK_LAUNCH();
       }
       res.rank = usable;
+      pt.mark("U, V");
+      pt.report();
       return res;
     }
   }

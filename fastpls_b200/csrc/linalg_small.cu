@@ -253,9 +253,36 @@ __global__ void jacobi_eig_kernel(int l, double* W, double* V, double* evals_out
         cs[k] = c; sn[k] = s;
       }
       __syncthreads();
+      if (npair <= 32) {
+        // lane = pair, warps stride over the rows / columns (no index division)
+        const int k = threadIdx.x & 31, w0 = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        const bool act = k < npair && qq[k] < l && sn[k] != 0.0;
+        const int p = act ? pp[k] : 0, q = act ? qq[k] : 0;
+        const double c = act ? cs[k] : 1.0, sv = act ? sn[k] : 0.0;
+        // rows: W <- J^T W
+        if (act)
+          for (int j = w0; j < l; j += nw) {
+            const double wp = W[p + j * l], wq = W[q + j * l];
+            W[p + j * l] = c * wp - sv * wq;
+            W[q + j * l] = sv * wp + c * wq;
+          }
+        __syncthreads();
+        // columns: W <- W J, V <- V J
+        if (act)
+          for (int i = w0; i < l; i += nw) {
+            const double wp = W[i + p * l], wq = W[i + q * l];
+            W[i + p * l] = c * wp - sv * wq;
+            W[i + q * l] = sv * wp + c * wq;
+            const double vp = V[i + p * l], vq = V[i + q * l];
+            V[i + p * l] = c * vp - sv * vq;
+            V[i + q * l] = sv * vp + c * vq;
+          }
+        __syncthreads();
+        continue;
+      }
       // rows: W <- J^T W
-      for (long long t = threadIdx.x; t < (long long)npair * l; t += blockDim.x) {
-        const int k = static_cast<int>(t % npair), j = static_cast<int>(t / npair);
+      for (int t = threadIdx.x; t < npair * l; t += blockDim.x) {
+        const int k = t % npair, j = t / npair;
         const int p = pp[k], q = qq[k];
         if (q >= l || sn[k] == 0.0) continue;
         const double c = cs[k], s = sn[k];
@@ -265,8 +292,8 @@ __global__ void jacobi_eig_kernel(int l, double* W, double* V, double* evals_out
       }
       __syncthreads();
       // columns: W <- W J, V <- V J
-      for (long long t = threadIdx.x; t < (long long)npair * l; t += blockDim.x) {
-        const int k = static_cast<int>(t % npair), i = static_cast<int>(t / npair);
+      for (int t = threadIdx.x; t < npair * l; t += blockDim.x) {
+        const int k = t % npair, i = t / npair;
         const int p = pp[k], q = qq[k];
         if (q >= l || sn[k] == 0.0) continue;
         const double c = cs[k], s = sn[k];

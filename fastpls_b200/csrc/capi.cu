@@ -175,6 +175,7 @@ int fpls_reset_workspace(char* err, size_t errlen) {
     Context::get().sync();
     split_gemm_release_cache();
     dual_release_graph();
+    simpls_release_graph();
     ozaki_release_cache();
     Context::get().release();
   });

@@ -3,10 +3,13 @@
 #include "simpls_engine.cuh"
 
 #include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
+#include <set>
 #include <string>
+#include <typeinfo>
 #include <vector>
 
 namespace fpls {
@@ -525,6 +528,79 @@ void simpls_batch_crosscov(const SimplsBatch& b, const double* /*Xc*/, const int
   FPLS_CHECK_LAUNCH();
 }
 
+namespace {
+
+// FASTPLS_LOOP_GRAPH=0 enqueues the component loop launch by launch.
+bool simpls_graph_enabled() {
+  static const int v = [] {
+    const char* e = std::getenv("FASTPLS_LOOP_GRAPH");
+    return e ? (e[0] != '0' ? 1 : 0) : 1;
+  }();
+  return v != 0;
+}
+
+// Shapes whose component loop has run once launch by launch: its GEMM plans,
+// split-K workspace and arena blocks exist, so a later call of the shape enqueues
+// launches only and can be captured.
+std::set<std::array<long long, 9>>& simpls_seen() {
+  static std::set<std::array<long long, 9>> seen;
+  return seen;
+}
+
+// The executable graph of the last captured component loop; each call captures
+// its loop and updates it in place when the topology matches, else
+// instantiates a new one (launches already in flight are not affected).
+cudaGraphExec_t g_simpls_exec = nullptr;
+
+// Returns false, with nothing enqueued, when the loop could not be captured
+// (a host step of the loop that a capture does not allow, such as the first
+// allocation of a GEMM plan); the caller then runs the loop launch by launch.
+template <typename Loop>
+bool simpls_launch_as_graph(cudaStream_t st, Loop&& loop) {
+  FPLS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaGraph_t graph = nullptr;
+  try {
+    loop();
+  } catch (...) {
+    cudaStreamEndCapture(st, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return false;
+  }
+  if (cudaStreamEndCapture(st, &graph) != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return false;
+  }
+  bool updated = false;
+  if (g_simpls_exec) {
+    cudaGraphExecUpdateResultInfo info;
+    updated = cudaGraphExecUpdate(g_simpls_exec, graph, &info) == cudaSuccess;
+    if (!updated) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(g_simpls_exec);
+      g_simpls_exec = nullptr;
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if (!updated) e = cudaGraphInstantiate(&g_simpls_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    g_simpls_exec = nullptr;
+    FPLS_CUDA(e);
+  }
+  FPLS_CUDA(cudaGraphLaunch(g_simpls_exec, st));
+  return true;
+}
+
+}  // namespace
+
+void simpls_release_graph() {
+  if (g_simpls_exec) cudaGraphExecDestroy(g_simpls_exec);
+  g_simpls_exec = nullptr;
+  simpls_seen().clear();
+}
+
 void simpls_batch_run(const SimplsBatch& b) {
   Context& ctx = Context::get();
   Eng e = make_eng(b);
@@ -576,6 +652,14 @@ void simpls_batch_run(const SimplsBatch& b) {
     marks.emplace_back(name, ev);
   };
   mark("start");
+  // The component loop as one CUDA graph once its shape has run (not while a
+  // trace or the kernel-class profiler records events, nor for row-sharded
+  // fits, whose all-reduce callback is the caller's).
+  const std::array<long long, 9> key{b.F, b.n, b.p, b.m, b.K, e.iters, b.labels ? 1 : 0, ctx.precision,
+                                     static_cast<long long>(typeid(*b.X).hash_code())};
+  const bool eligible = simpls_graph_enabled() && !trace && !ctx.profile && !shard_red;
+  const bool graph = eligible && simpls_seen().count(key) > 0;
+  auto loop = [&]() {
   k_refresh_start<<<gp, kThreads, 0, st>>>(e); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   for (int a = 0; a < b.K; ++a) {
@@ -614,6 +698,11 @@ void simpls_batch_run(const SimplsBatch& b) {
     k_deflate<<<gp, kThreads, sm_m, st>>>(e, a, a + 1 < b.K ? 1 : 0); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
     mark("deflate");
+  }
+  };
+  if (!(graph && simpls_launch_as_graph(st, loop))) {
+    loop();
+    if (eligible) simpls_seen().insert(key);
   }
   if (trace) {
     FPLS_CUDA(cudaStreamSynchronize(st));

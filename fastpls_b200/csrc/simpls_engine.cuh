@@ -71,6 +71,9 @@ struct SimplsBatch {
 // Runs K components for all fits.  Device pointers throughout; launches only.
 void simpls_batch_run(const SimplsBatch& b);
 
+// Frees the executable graph of the component loop (fpls_reset_workspace).
+void simpls_release_graph();
+
 // S_f = diag(colscale_f) [ Xc^T D_f Y - colsum_f off_f^T ] for all fits (the
 // masked cross-covariances with the fold-centred response, off_f the fold's
 // response means), via one GEMM Xc^T [D_1 Y ... D_F Y].

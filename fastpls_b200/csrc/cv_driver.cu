@@ -280,10 +280,10 @@ void fill_special_predictions(const CvFitSet& fs, const int* y, const std::vecto
 constexpr int kUploadChunkCols = 4096;
 constexpr int kUploadTailCols = 1024;
 
-std::vector<int> upload_chunks(int p) {
+std::vector<int> upload_chunks(int p, int align) {
   std::vector<int> b{0};
   while (p - b.back() > kUploadChunkCols + kUploadTailCols) b.push_back(b.back() + kUploadChunkCols);
-  const int tail0 = (p - kUploadTailCols) / 64 * 64;
+  const int tail0 = (p - kUploadTailCols) / align * align;
   if (tail0 - b.back() >= kUploadTailCols / 2) b.push_back(tail0);
   b.push_back(p);
   return b;
@@ -312,9 +312,9 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
   const bool int8_gram = opt.precision == 3 && dual;
   const bool planes_only = (opt.precision == 1 || opt.precision == 2) && dual;
   const int planes = opt.precision == 2 ? 3 : 2;  // BF16x6: hi, mid, lo planes
-  // A host X goes up in overlapped column chunks on the mixed row-space path,
-  // else in one copy first.
-  if (x_host && !planes_only) {
+  // A host X goes up in overlapped column chunks on the mixed and INT8
+  // row-space paths, else in one copy first.
+  if (x_host && !planes_only && !int8_gram) {
     if (x64) h2d(const_cast<double*>(x64), x_host, (size_t)n * p * sizeof(double));
     else h2d(const_cast<float*>(x32), x_host, (size_t)n * p * sizeof(float));
     x_host = nullptr;
@@ -328,15 +328,17 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
 
   if (x_host) {
     // X arrives in column chunks on the copy stream; each chunk's column means,
-    // BF16 planes and row-Gram contribution run as soon as it has landed, while
-    // the next chunk is in flight (copies and compute are enqueued in turn, so
-    // a pageable host buffer overlaps too).
+    // BF16 planes (or INT8 digit planes with the chunk's own row scales) and
+    // row-Gram contribution run as soon as it has landed, while the next chunk
+    // is in flight (copies and compute are enqueued in turn, so a pageable
+    // host buffer overlaps too).
     const size_t esz = x64 ? sizeof(double) : sizeof(float);
     char* dst = x64 ? reinterpret_cast<char*>(const_cast<double*>(x64)) : reinterpret_cast<char*>(const_cast<float*>(x32));
     const char* src = static_cast<const char*>(x_host);
-    const std::vector<int> bounds = upload_chunks(p);
+    const std::vector<int> bounds = upload_chunks(p, int8_gram ? 128 : 64);
     const int nch = static_cast<int>(bounds.size()) - 1;
-    xop = make_split_operator_chunked(n, p, planes);
+    xop = int8_gram ? make_ozaki_rows_chunked(n, p, int8_gram_slices(), bounds)
+                    : make_split_operator_chunked(n, p, planes);
     x0 = ar.alloc_n<double>(n);
     // the copies follow this call's earlier work on the main stream (an event
     // of their own: side_done marks the sketches, awaited later)
@@ -351,10 +353,12 @@ std::unique_ptr<CvPreparedX> cv_prepare_x(const double* x64, const float* x32, i
         if (c64) col_mean(c64, n, j1 - j0, n, mall + j0);
         else col_mean(c32, n, j1 - j0, n, mall + j0);
       }
-      split_operator_fill_columns(*xop, c64, c32, center ? mall + j0 : nullptr, j0, j1);
+      if (int8_gram) ozaki_rows_fill_chunk(*xop, c64, c32, center ? mall + j0 : nullptr, c);
+      else split_operator_fill_columns(*xop, c64, c32, center ? mall + j0 : nullptr, j0, j1);
       if (c == 0) load_centered(x64, x32, n, 1, mall, x0);
       if (c == nch - 1) FPLS_CUDA(cudaEventRecord(ctx.planes_ready, ctx.stream));
-      split_operator_gram_columns(*xop, Kg, j0, j1, c > 0);
+      if (int8_gram) ozaki_rows_gram_chunk(*xop, Kg, c, c > 0);
+      else split_operator_gram_columns(*xop, Kg, j0, j1, c > 0);
     };
     for (int c = 0; c < nch; ++c) {
       const int j0 = bounds[c], j1 = bounds[c + 1];

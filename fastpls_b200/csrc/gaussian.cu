@@ -29,6 +29,8 @@ constexpr int kN = 624;
 constexpr int kM = 397;
 constexpr int kAttempts = kN / 4;  // 156
 constexpr int kThreads = 256;
+constexpr int kScanWarps = (kAttempts + 31) / 32;  // 5
+static_assert(kScanWarps * 32 <= kThreads, "the flag scan needs whole warps");
 
 __device__ __forceinline__ uint32_t twist_word(uint32_t cur, uint32_t next, uint32_t far) {
   const uint32_t y = (cur & 0x80000000u) | (next & 0x7fffffffu);
@@ -57,6 +59,7 @@ __global__ void __launch_bounds__(kThreads) mt_gaussian_kernel(double* __restric
   __shared__ int flag[kAttempts];
   __shared__ double vx[kAttempts], vy[kAttempts];
   __shared__ int scan[kAttempts];
+  __shared__ int wsum[kScanWarps];
   double* dst = out + (long long)blockIdx.x * ld;
   if (threadIdx.x == 0) {
     uint32_t x = seeds[blockIdx.x];
@@ -110,12 +113,21 @@ __global__ void __launch_bounds__(kThreads) mt_gaussian_kernel(double* __restric
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      int s = 0;
-      for (int j = 0; j < kAttempts; ++j) {
-        scan[j] = s;
-        s += flag[j];
-      }
+    // exclusive scan of the accept flags: a ballot per warp over the first
+    // kScanWarps warps (lanes past the last attempt vote 0), then the warp
+    // totals added in warp order
+    if (threadIdx.x < kScanWarps * 32) {
+      const int j = threadIdx.x, lane = j & 31, w = j >> 5;
+      const unsigned b = __ballot_sync(0xffffffffu, j < kAttempts && flag[j]);
+      if (lane == 0) wsum[w] = __popc(b);
+      __syncwarp();
+      if (j < kAttempts) scan[j] = __popc(b & ((1u << lane) - 1u));
+    }
+    __syncthreads();
+    if (threadIdx.x < kAttempts) {
+      int off = 0;
+      for (int w = 0; w < (threadIdx.x >> 5); ++w) off += wsum[w];
+      scan[threadIdx.x] += off;
     }
     __syncthreads();
     if (threadIdx.x < kAttempts && flag[threadIdx.x]) {

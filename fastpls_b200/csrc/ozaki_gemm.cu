@@ -124,7 +124,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
                   const double* __restrict__ sB, const int4* __restrict__ segs,
                   const int* __restrict__ cta_seg_begin, const int* __restrict__ tile_seg, int n_tiles_n,
                   double* __restrict__ part, double* __restrict__ C, int ldc, int M, int N, int* err,
-                  int a_static) {
+                  int a_static, int c_accum) {
   __shared__ int epi_fail;   // raised by any epilogue warp whose wait gave up
   using L = OzLayout<S>;
   extern __shared__ uint8_t smem_raw[];
@@ -335,7 +335,10 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
 #pragma unroll
             for (int x = 0; x < 16; ++x) {
               const int col = nt * OBN + c * 16 + x;
-              if (col < N) C[row + static_cast<size_t>(col) * ldc] = acc[x] * rs * cs[c * 16 + x];
+              if (col < N) {
+                double* o = C + row + static_cast<size_t>(col) * ldc;
+                *o = (c_accum ? *o : 0.0) + acc[x] * rs * cs[c * 16 + x];
+              }
             }
           }
         } else {
@@ -356,15 +359,15 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant_
   }
 }
 
-// C[m + n*ldc] = sum of the tile's partials in segment order; tiles with one
-// segment were written by the product kernel.
+// C[m + n*ldc] = sum of the tile's partials in segment order (added to C when
+// c_accum is set); tiles with one segment were written by the product kernel.
 constexpr int kReducePieces = 8;
 
 // tile_segs (when not null) lists each tile's segment ids in contraction
 // order (plans whose segments of one tile are not consecutive).
 __global__ void ozaki_reduce_kernel(const double* __restrict__ part, const int* __restrict__ tile_seg,
                                     const int* __restrict__ tile_segs, int n_tiles_n, int M, int N,
-                                    double* __restrict__ C, int ldc) {
+                                    double* __restrict__ C, int ldc, int c_accum = 0) {
   const int tile = blockIdx.x / kReducePieces;
   const int piece = blockIdx.x % kReducePieces;
   const int s0 = tile_seg[tile], s1 = tile_seg[tile + 1];
@@ -380,7 +383,8 @@ __global__ void ozaki_reduce_kernel(const double* __restrict__ part, const int* 
       const int s = tile_segs ? tile_segs[j] : j;
       acc += part[(static_cast<size_t>(s) * OBN + nn) * OBM + mm];
     }
-    C[m + static_cast<size_t>(n) * ldc] = acc;
+    double* o = C + m + static_cast<size_t>(n) * ldc;
+    *o = (c_accum ? *o : 0.0) + acc;
   }
 }
 
@@ -443,24 +447,40 @@ __global__ void ozaki_split_kernel(const double* __restrict__ X, int klen, int c
 // Row exponents of a column-major matrix with the column means subtracted:
 // thread (row i, column range of the block) takes the largest |x_ij - mean_j|
 // and folds its binary exponent into rexp[i] by atomicMax (order-free);
-// a non-finite entry raises bad[i].
+// a non-finite entry raises bad[i].  Eight columns are loaded before any is
+// used (eight independent loads in flight per thread), kept in four running
+// maxima.
 template <typename T>
-__global__ void ozaki_row_exp_kernel(const T* __restrict__ X, int n, int p, int ld, const double* __restrict__ mean,
-                                     int cols_per_block, int* __restrict__ rexp, int* __restrict__ bad) {
+__global__ void __launch_bounds__(256) ozaki_row_exp_kernel(const T* __restrict__ X, int n, int p, int ld,
+                                                            const double* __restrict__ mean, int cols_per_block,
+                                                            int* __restrict__ rexp, int* __restrict__ bad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int j0 = blockIdx.y * cols_per_block, j1 = min(p, j0 + cols_per_block);
-  double m = 0.0;
+  double m[4] = {0.0, 0.0, 0.0, 0.0};
   bool b = false;
-  for (int j = j0; j < j1; ++j) {
+  int j = j0;
+  for (; j + 8 <= j1; j += 8) {
+    T x[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) x[u] = X[i + static_cast<size_t>(j + u) * ld];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const double v = static_cast<double>(x[u]) - (mean ? mean[j + u] : 0.0);
+      if (!isfinite(v)) b = true;
+      else m[u & 3] = fmax(m[u & 3], fabs(v));
+    }
+  }
+  for (; j < j1; ++j) {
     const double v = static_cast<double>(X[i + static_cast<size_t>(j) * ld]) - (mean ? mean[j] : 0.0);
     if (!isfinite(v)) b = true;
-    else m = fmax(m, fabs(v));
+    else m[0] = fmax(m[0], fabs(v));
   }
+  const double mx = fmax(fmax(m[0], m[1]), fmax(m[2], m[3]));
   if (b) bad[i] = 1;
-  if (m > 0.0) {
+  if (mx > 0.0) {
     int e = 0;
-    frexp(m, &e);
+    frexp(mx, &e);
     atomicMax(rexp + i, e);
   }
 }
@@ -476,47 +496,99 @@ __global__ void ozaki_row_scale_kernel(const int* __restrict__ rexp, const int* 
 
 // Digits of the rows of X - mean (n x p column-major) into the planes (row i of
 // plane s at P + s * plane_stride + i * ldk, zero padded to rows_pad x ldk):
-// tiles of 32 rows x 128 columns, read column by column (coalesced) into shared
-// memory, then each row's 128 columns cut into S signed 7-bit digits (exact
-// FP64 steps) and written as 16-byte runs.
+// tiles of R rows x 128 columns (R = 64 for FP32 input, 32 for FP64, 33 KB of
+// shared memory either way).  Each warp loads 16 columns of the tile's rows
+// (16 R / 32 independent coalesced loads per lane) into shared memory; then
+// thread (row r, column group g) turns its row's 128 R / 256 consecutive
+// entries of the group into digits and writes each plane's 16-byte runs.  The
+// S signed 7-bit digits of a = (x - mean) / 2^e (|a| < 1, the scale a power of
+// two, so every step is exact) are the base-128 digits of q = trunc(a *
+// 2^(7S)), most significant first, carrying the sign of a: one FP64 -> int64
+// truncation per entry, the same digits as S rounds of "times 128, take the
+// integer part".
+constexpr int kSplitCols = 128;
 template <typename T>
+constexpr int split_rows_per_tile() { return sizeof(T) == 4 ? 64 : 32; }
+
+template <typename T, int S>
 __global__ void __launch_bounds__(256) ozaki_split_rows_kernel(const T* __restrict__ X, int n, int p, int ld,
                                                                const double* __restrict__ mean,
                                                                const double* __restrict__ scale,
-                                                               int8_t* __restrict__ P, int ldk, size_t plane_stride,
-                                                               int S) {
-  __shared__ double tile[128][33];
-  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 128;
+                                                               int8_t* __restrict__ P, int ldk, size_t plane_stride) {
+  constexpr int R = split_rows_per_tile<T>();
+  constexpr int H = R / 32;              // 32-row halves loaded per column
+  constexpr int G = 256 / R;             // column groups
+  constexpr int RUNS = kSplitCols / G / 16;
+  __shared__ T tile[kSplitCols][R + 1];
+  __shared__ double mj[kSplitCols];
+  const int i0 = blockIdx.y * R, j0 = blockIdx.x * kSplitCols;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int c = warp; c < 128; c += 8) {
-    const int j = j0 + c, i = i0 + lane;
-    double v = 0.0;
-    if (j < p && i < n) v = static_cast<double>(X[i + static_cast<size_t>(j) * ld]) - (mean ? mean[j] : 0.0);
-    tile[c][lane] = v;
+  if (threadIdx.x < kSplitCols) {
+    const int j = j0 + threadIdx.x;
+    mj[threadIdx.x] = (mean && j < p) ? mean[j] : 0.0;
+  }
+  {
+    T v[16][H];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int j = j0 + warp * 16 + u;
+#pragma unroll
+      for (int h = 0; h < H; ++h) {
+        const int i = i0 + h * 32 + lane;
+        v[u][h] = (j < p && i < n) ? X[i + static_cast<size_t>(j) * ld] : T(0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u)
+#pragma unroll
+      for (int h = 0; h < H; ++h) tile[warp * 16 + u][h * 32 + lane] = v[u][h];
   }
   __syncthreads();
-  const int r = threadIdx.x >> 3, c0 = (threadIdx.x & 7) * 16;
+  const int r = threadIdx.x % R, g = threadIdx.x / R;
   const int i = i0 + r;
   const double sc = scale[i];
   const double inv = (isfinite(sc) && sc > 0.0) ? 1.0 / sc : 0.0;   // a power of two: exact
-  int8_t dg[kOzakiMaxSlices][16];
+  const double lift = static_cast<double>(1ll << (7 * S));
 #pragma unroll
-  for (int x = 0; x < 16; ++x) {
-    double a = tile[c0 + x][r] * inv;
-    if (!isfinite(a)) a = 0.0;
+  for (int h = 0; h < RUNS; ++h) {
+    uint32_t w[S][4];
 #pragma unroll
-    for (int s = 0; s < kOzakiMaxSlices; ++s) {
-      if (s >= S) break;
-      a *= 128.0;
-      const double d = trunc(a);
-      a -= d;
-      dg[s][x] = static_cast<int8_t>(static_cast<int>(d));
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w[s][q] = 0u;
+    const int cb = g * (kSplitCols / G) + h * 16;
+#pragma unroll
+    for (int x = 0; x < 16; ++x) {
+      const int c = cb + x;
+      const int j = j0 + c;
+      double a = (j < p && i < n) ? (static_cast<double>(tile[c][r]) - mj[c]) * inv : 0.0;
+      if (!isfinite(a)) a = 0.0;
+      const long long qv = __double2ll_rz(a * lift);
+      const unsigned long long mag = static_cast<unsigned long long>(qv < 0 ? -qv : qv);
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        int d = static_cast<int>((mag >> (7 * (S - 1 - s))) & 127ull);
+        if (qv < 0) d = -d;
+        w[s][x >> 2] |= (static_cast<uint32_t>(d) & 0xffu) << (8 * (x & 3));
+      }
     }
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+      *reinterpret_cast<int4*>(P + static_cast<size_t>(s) * plane_stride + static_cast<size_t>(i) * ldk + j0 + cb) =
+          make_int4(static_cast<int>(w[s][0]), static_cast<int>(w[s][1]), static_cast<int>(w[s][2]),
+                    static_cast<int>(w[s][3]));
   }
-  for (int s = 0; s < S; ++s) {
-    int4 w;
-    memcpy(&w, dg[s], 16);
-    *reinterpret_cast<int4*>(P + static_cast<size_t>(s) * plane_stride + static_cast<size_t>(i) * ldk + j0 + c0) = w;
+}
+
+template <typename T>
+void launch_split_rows(const T* X, int n, int p, int ld, const double* mean, const double* scale, int8_t* P,
+                       int ldk, int cols_pad, int rows_pad, size_t plane_stride, int S, cudaStream_t st) {
+  const dim3 g(cols_pad / kSplitCols, rows_pad / split_rows_per_tile<T>());
+  switch (S) {
+    case 4: ozaki_split_rows_kernel<T, 4><<<g, 256, 0, st>>>(X, n, p, ld, mean, scale, P, ldk, plane_stride); break;
+    case 5: ozaki_split_rows_kernel<T, 5><<<g, 256, 0, st>>>(X, n, p, ld, mean, scale, P, ldk, plane_stride); break;
+    case 6: ozaki_split_rows_kernel<T, 6><<<g, 256, 0, st>>>(X, n, p, ld, mean, scale, P, ldk, plane_stride); break;
+    default: ozaki_split_rows_kernel<T, 7><<<g, 256, 0, st>>>(X, n, p, ld, mean, scale, P, ldk, plane_stride); break;
   }
 }
 
@@ -670,11 +742,12 @@ const OzCached& oz_plan(int M, int N, int K, int sm_count, cudaStream_t st, bool
   return cache.emplace(key, std::move(c)).first->second;
 }
 
-// 2-D int8 tensor map over all planes stacked (rows_pad * slices rows of ldk bytes).
+// 2-D int8 tensor map over all planes stacked (rows_pad * slices rows of ldk
+// bytes, row_stride() bytes apart).
 CUtensorMap make_plane_map(const OzakiPlanes& p, int box_rows) {
   CUtensorMap m;
   cuuint64_t dims[2] = {static_cast<cuuint64_t>(p.ldk), static_cast<cuuint64_t>(p.rows_pad) * p.slices};
-  cuuint64_t strides[1] = {static_cast<cuuint64_t>(p.ldk)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(p.row_stride())};
   cuuint32_t box[2] = {static_cast<cuuint32_t>(OBK), static_cast<cuuint32_t>(box_rows)};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = tc::encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, p.data, dims, strides, box, estr,
@@ -705,7 +778,8 @@ void ensure_ozaki_attr_for(int slices) {
 
 template <int S>
 void launch_ozaki(const CUtensorMap& mA, const CUtensorMap& mB, const OzakiPlanes& A, const OzakiPlanes& B,
-                  const OzCached& c, double* C, int ldc, int* err, cudaStream_t st, bool a_static) {
+                  const OzCached& c, double* C, int ldc, int* err, cudaStream_t st, bool a_static,
+                  bool c_accum) {
   ensure_ozaki_attr<S>();
   cudaLaunchConfig_t lc = {};
   lc.gridDim = dim3(c.g.ctas);
@@ -722,7 +796,7 @@ void launch_ozaki(const CUtensorMap& mA, const CUtensorMap& mB, const OzakiPlane
                                static_cast<const double*>(A.scale), static_cast<const double*>(B.scale),
                                static_cast<const int4*>(c.segs), static_cast<const int*>(c.cta_begin),
                                static_cast<const int*>(c.tile_begin), ntn, c.part, C, ldc, m_rows, n_rows, err,
-                               a_static ? 1 : 0));
+                               a_static ? 1 : 0, c_accum ? 1 : 0));
 }
 
 struct XOperatorOzakiSym : public XOperator {
@@ -770,33 +844,143 @@ struct XOperatorOzakiRows : public XOperator {
 
 }  // namespace
 
-OzakiPlanes ozaki_split_rows(const double* x64, const float* x32, int n, int p, const double* mean, int slices) {
+namespace {
+
+// Runs the product kernel (defined below).
+const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc, bool a_static,
+                          bool sym = false, bool c_accum = false);
+
+// Row scales of the n x p column-major matrix X - mean (x64 or x32, ld n) into
+// scale (rows_pad entries: 2^e above each row's largest magnitude, 1 on the
+// padding rows, NaN for a row with a non-finite entry), then its digits into
+// the planes at P (rows ld_planes bytes apart, planes plane_stride apart),
+// columns [0, cols_pad) with zeros past p.
+void split_rows_range(const double* x64, const float* x32, int n, int p, const double* mean, int slices,
+                      int rows_pad, double* scale, int8_t* P, int ld_planes, int cols_pad, size_t plane_stride) {
   Context& ctx = Context::get();
-  OzakiPlanes pl = ozaki_alloc(n, p, slices);
   int* rexp = ctx.arena.alloc_n<int>(n);
   int* bad = ctx.arena.alloc_n<int>(n);
   FPLS_CUDA(cudaMemsetAsync(rexp, 0x80, n * sizeof(int), ctx.stream));   // a very negative sentinel
   dzero(bad, n * sizeof(int));
-  constexpr int kCols = 64;
+  constexpr int kCols = 160;
   const dim3 g1(ceil_div(n, 256), ceil_div(p, kCols));
   if (x64) ozaki_row_exp_kernel<double><<<g1, 256, 0, ctx.stream>>>(x64, n, p, n, mean, kCols, rexp, bad);
   else ozaki_row_exp_kernel<float><<<g1, 256, 0, ctx.stream>>>(x32, n, p, n, mean, kCols, rexp, bad);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
-  ozaki_row_scale_kernel<<<ceil_div(pl.rows_pad, 256), 256, 0, ctx.stream>>>(rexp, bad, n, pl.rows_pad, pl.scale);
+  ozaki_row_scale_kernel<<<ceil_div(rows_pad, 256), 256, 0, ctx.stream>>>(rexp, bad, n, rows_pad, scale);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
-  const dim3 g2(pl.ldk / 128, pl.rows_pad / 32);
-  const size_t stride = static_cast<size_t>(pl.rows_pad) * pl.ldk;
-  if (x64)
-    ozaki_split_rows_kernel<double><<<g2, 256, 0, ctx.stream>>>(x64, n, p, n, mean, pl.scale, pl.data, pl.ldk, stride,
-                                                                slices);
-  else
-    ozaki_split_rows_kernel<float><<<g2, 256, 0, ctx.stream>>>(x32, n, p, n, mean, pl.scale, pl.data, pl.ldk, stride,
-                                                               slices);
+  static_assert(OBM % 64 == 0 && OBK % kSplitCols == 0, "split tiles must divide the plane padding");
+  if (x64) launch_split_rows<double>(x64, n, p, n, mean, scale, P, ld_planes, cols_pad, rows_pad, plane_stride,
+                                     slices, ctx.stream);
+  else launch_split_rows<float>(x32, n, p, n, mean, scale, P, ld_planes, cols_pad, rows_pad, plane_stride, slices,
+                                ctx.stream);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
+}
+
+// The upper tiles of C = A A^T (set, or increased when accumulate is set); the
+// lower triangle is left to the caller.
+void ozaki_gram_upper(const OzakiPlanes& A, double* C, int ldc, bool accumulate) {
+  FPLS_REQUIRE(ldc == A.rows, "INT8 Gram: the output must be n x n with ld n");
+  Context& ctx = Context::get();
+  const int slot = ctx.prof_begin("gram_int8", ctx.stream);
+  const OzCached& c = run_ozaki(A, A, C, ldc, false, true, accumulate);
+  // the upper tiles' partials summed in contraction order (tiles with a single
+  // segment were written by the product kernel)
+  ozaki_reduce_kernel<<<c.g.tiles * kReducePieces, 256, 0, ctx.stream>>>(c.part, c.tile_begin, c.tile_segs, c.g.ntn,
+                                                                         A.rows, A.rows, C, ldc, accumulate ? 1 : 0);
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  if (slot >= 0) {
+    // algorithmic work: the S (S + 1) / 2 digit-plane pairs over the planned
+    // (upper) tiles; bytes: every plane of A once and C once
+    const double S = A.slices, n = A.rows, K = A.k;
+    int planned = 0;
+    for (int t = 0; t < c.g.tiles; ++t) planned += c.g.tile_begin[t + 1] > c.g.tile_begin[t];
+    const double frac = static_cast<double>(planned) / c.g.tiles;
+    ctx.prof_end(slot, ctx.stream, S * n * K + 8.0 * n * n * frac, 0.5 * S * (S + 1.0) * 2.0 * n * n * K * frac);
+  }
+}
+
+// X as column chunks of digit planes, each chunk with its own row scales.
+struct XOperatorOzakiRowsChunked : public XOperator {
+  OzakiPlanes xp;                  // all columns; xp.scale unused
+  std::vector<int> bounds;
+  std::vector<double*> scales;     // per chunk, rows_pad entries
+  XOperatorOzakiRowsChunked(int n_, int p_, int slices, const std::vector<int>& b) : bounds(b) {
+    n = n_;
+    p = p_;
+    FPLS_REQUIRE(bounds.size() >= 2 && bounds.front() == 0 && bounds.back() == p_,
+                 "INT8 chunks: bounds must run from 0 to p");
+    for (size_t c = 1; c + 1 < bounds.size(); ++c)
+      FPLS_REQUIRE(bounds[c] % OBK == 0 && bounds[c] > bounds[c - 1], "INT8 chunks: inner bounds must be multiples of 128");
+    xp = ozaki_alloc(n_, p_, slices);
+    for (size_t c = 0; c + 1 < bounds.size(); ++c) scales.push_back(Context::get().arena.alloc_n<double>(xp.rows_pad));
+  }
+  int chunks() const { return static_cast<int>(bounds.size()) - 1; }
+  // columns [bounds[c], bounds[c+1]) of `full` as planes of their own
+  OzakiPlanes view(const OzakiPlanes& full, int c, double* scale) const {
+    OzakiPlanes v = full;
+    v.data = full.data + bounds[c];
+    v.k = bounds[c + 1] - bounds[c];
+    v.ldk = round_up(v.k, OBK);
+    v.ld = full.row_stride();
+    v.scale = scale;
+    return v;
+  }
+  void times(const double* M, int F, double* U) override {
+    OzakiPlanes b = ozaki_alloc(F, p, xp.slices);
+    ozaki_split(M, p, b);
+    Context& ctx = Context::get();
+    for (int c = 0; c < chunks(); ++c) {
+      const OzakiPlanes a = view(xp, c, scales[c]);
+      const OzakiPlanes bc = view(b, c, b.scale);
+      const OzCached& cc = run_ozaki(a, bc, U, n, false, false, c > 0);
+      ozaki_reduce_kernel<<<cc.g.tiles * kReducePieces, 256, 0, ctx.stream>>>(cc.part, cc.tile_begin, nullptr,
+                                                                              cc.g.ntn, n, F, U, n, c > 0 ? 1 : 0);
+      ::fpls::note_launch();
+      FPLS_CHECK_LAUNCH();
+    }
+  }
+  void t_times(const double*, int, double*) override {
+    throw Error(kErrArgument, "the INT8 row operator has no transposed product");
+  }
+  void gram(double*) override { throw Error(kErrArgument, "the chunked INT8 row operator forms its Gram by chunks"); }
+};
+
+XOperatorOzakiRowsChunked& as_chunked(XOperator& op) {
+  auto* o = dynamic_cast<XOperatorOzakiRowsChunked*>(&op);
+  FPLS_REQUIRE(o != nullptr, "INT8 chunks: not a chunked INT8 row operator");
+  return *o;
+}
+
+}  // namespace
+
+OzakiPlanes ozaki_split_rows(const double* x64, const float* x32, int n, int p, const double* mean, int slices) {
+  OzakiPlanes pl = ozaki_alloc(n, p, slices);
+  split_rows_range(x64, x32, n, p, mean, slices, pl.rows_pad, pl.scale, pl.data, pl.ldk, pl.ldk,
+                   static_cast<size_t>(pl.rows_pad) * pl.ldk);
   return pl;
+}
+
+std::unique_ptr<XOperator> make_ozaki_rows_chunked(int n, int p, int slices, const std::vector<int>& bounds) {
+  return std::unique_ptr<XOperator>(new XOperatorOzakiRowsChunked(n, p, slices, bounds));
+}
+
+void ozaki_rows_fill_chunk(XOperator& op, const double* c64, const float* c32, const double* mean, int c) {
+  XOperatorOzakiRowsChunked& o = as_chunked(op);
+  FPLS_REQUIRE(c >= 0 && c < o.chunks(), "INT8 chunks: chunk index out of range");
+  const int j0 = o.bounds[c], w = o.bounds[c + 1] - j0;
+  split_rows_range(c64, c32, o.n, w, mean, o.xp.slices, o.xp.rows_pad, o.scales[c], o.xp.data + j0, o.xp.ldk,
+                   round_up(w, OBK), static_cast<size_t>(o.xp.rows_pad) * o.xp.ldk);
+}
+
+void ozaki_rows_gram_chunk(XOperator& op, double* K, int c, bool accumulate) {
+  XOperatorOzakiRowsChunked& o = as_chunked(op);
+  FPLS_REQUIRE(c >= 0 && c < o.chunks(), "INT8 chunks: chunk index out of range");
+  ozaki_gram_upper(o.view(o.xp, c, o.scales[c]), K, o.n, accumulate);
 }
 
 std::unique_ptr<XOperator> make_ozaki_rows_operator(const double* x64, const float* x32, const double* mean, int n,
@@ -833,7 +1017,7 @@ namespace {
 // Runs the product kernel: whole tiles straight to C (when C is given), the
 // others as partials in the cached plan.
 const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc, bool a_static,
-                          bool sym = false) {
+                          bool sym, bool c_accum) {
   FPLS_REQUIRE(A.slices == B.slices && A.k == B.k && A.ldk == B.ldk, "INT8 products: operands do not match");
   Context& ctx = Context::get();
   cudaStream_t st = ctx.stream;
@@ -842,10 +1026,10 @@ const OzCached& run_ozaki(const OzakiPlanes& A, const OzakiPlanes& B, double* C,
   const CUtensorMap mB = make_plane_map(B, OBN);
   int* err = ctx.d_status + 16;
   switch (A.slices) {
-    case 4: launch_ozaki<4>(mA, mB, A, B, c, C, ldc, err, st, a_static); break;
-    case 5: launch_ozaki<5>(mA, mB, A, B, c, C, ldc, err, st, a_static); break;
-    case 6: launch_ozaki<6>(mA, mB, A, B, c, C, ldc, err, st, a_static); break;
-    default: launch_ozaki<7>(mA, mB, A, B, c, C, ldc, err, st, a_static); break;
+    case 4: launch_ozaki<4>(mA, mB, A, B, c, C, ldc, err, st, a_static, c_accum); break;
+    case 5: launch_ozaki<5>(mA, mB, A, B, c, C, ldc, err, st, a_static, c_accum); break;
+    case 6: launch_ozaki<6>(mA, mB, A, B, c, C, ldc, err, st, a_static, c_accum); break;
+    default: launch_ozaki<7>(mA, mB, A, B, c, C, ldc, err, st, a_static, c_accum); break;
   }
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
@@ -863,25 +1047,7 @@ void ozaki_gemm(const OzakiPlanes& A, const OzakiPlanes& B, double* C, int ldc, 
 }
 
 void ozaki_gram(const OzakiPlanes& A, double* C, int ldc) {
-  FPLS_REQUIRE(ldc == A.rows, "INT8 Gram: the output must be n x n with ld n");
-  Context& ctx = Context::get();
-  const int slot = ctx.prof_begin("gram_int8", ctx.stream);
-  const OzCached& c = run_ozaki(A, A, C, ldc, false, true);
-  // the upper tiles' partials summed in contraction order (tiles with a single
-  // segment were written by the product kernel), then the lower triangle
-  ozaki_reduce_kernel<<<c.g.tiles * kReducePieces, 256, 0, ctx.stream>>>(c.part, c.tile_begin, c.tile_segs, c.g.ntn,
-                                                                         A.rows, A.rows, C, ldc);
-  ::fpls::note_launch();
-  FPLS_CHECK_LAUNCH();
-  if (slot >= 0) {
-    // algorithmic work: the S (S + 1) / 2 digit-plane pairs over the planned
-    // (upper) tiles; bytes: every plane of A once and C once
-    const double S = A.slices, n = A.rows, K = A.k;
-    int planned = 0;
-    for (int t = 0; t < c.g.tiles; ++t) planned += c.g.tile_begin[t + 1] > c.g.tile_begin[t];
-    const double frac = static_cast<double>(planned) / c.g.tiles;
-    ctx.prof_end(slot, ctx.stream, S * n * K + 8.0 * n * n * frac, 0.5 * S * (S + 1.0) * 2.0 * n * n * K * frac);
-  }
+  ozaki_gram_upper(A, C, ldc, false);
   mirror_upper_triangle(C, A.rows);
 }
 

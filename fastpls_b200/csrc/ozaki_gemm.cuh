@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <vector>
 
 #include "simpls_engine.cuh"
 
@@ -19,6 +20,11 @@ struct OzakiPlanes {
   int8_t* data = nullptr;
   double* scale = nullptr;
   int rows = 0, rows_pad = 0, k = 0, ldk = 0, slices = 0;
+  // Row stride in bytes when these planes are a column range of wider planes
+  // (a view: data points at the range's first column, ldk is the range's
+  // padded width); 0 when the rows are ldk apart.
+  int ld = 0;
+  int row_stride() const { return ld ? ld : ldk; }
 };
 
 // Slices per operand accepted by the kernel.
@@ -69,6 +75,21 @@ void ozaki_gram(const OzakiPlanes& A, double* C, int ldc);
 // the INT8 tensor cores; no transposed product.
 std::unique_ptr<XOperator> make_ozaki_rows_operator(const double* x64, const float* x32, const double* mean, int n,
                                                     int p, int slices);
+
+// X (n x p) arriving in column chunks (bounds[c] .. bounds[c+1], every inner
+// bound a multiple of 128): each chunk keeps its own power-of-two row scales
+// (the largest |x - mean| of the row within the chunk), so its digits are
+// made, and its share of X X^T taken, as soon as it has landed.
+//   ozaki_rows_fill_chunk   digit planes of chunk c of X - mean (c64 / c32:
+//                           the chunk's first column, ld n; mean: the chunk's
+//                           column means, or null);
+//   ozaki_rows_gram_chunk   the upper tiles of K (n x n, ld n) set (accumulate
+//                           false) or increased by chunk c's A_c A_c^T.
+// times() of the operator is X M summed over the chunks; gram() is not
+// provided (the chunks' Gram calls make it).
+std::unique_ptr<XOperator> make_ozaki_rows_chunked(int n, int p, int slices, const std::vector<int>& bounds);
+void ozaki_rows_fill_chunk(XOperator& op, const double* c64, const float* c32, const double* mean, int c);
+void ozaki_rows_gram_chunk(XOperator& op, double* K, int c, bool accumulate);
 
 // Releases the cached stream-K plans (fpls_reset_workspace).
 void ozaki_release_cache();

@@ -54,3 +54,30 @@ def test_int8_double_cv_close_to_fp64(lib):
     assert np.array_equal(a["pred"], b["pred"])
     assert slice_score_rel_err(b["inner_score"], a["inner_score"]) < 1e-5
     assert cv_labels_match(b["inner_pred"], a["inner_pred"], np.transpose(a["inner_score"], (2, 1, 0, 3)), 1e-5)[0]
+
+
+def test_int8_double_cv_host_chunks(lib):
+    """A host X wider than one upload chunk (bounds 0, 4096, 7936, 9000): each
+    chunk's digit planes carry their own row scales and its share of the row
+    Gram and of the sketch product is added as it lands.  The grid stays within
+    1e-5 of the FP64 grid's class scores and agrees with the INT8 grid on the
+    resident matrix (one set of row scales over all columns)."""
+    d = synthetic.c4_omics(seed=11, n=300, p=9000, n_informative=20)
+    outer, inner = double_cv_folds(d["y"], d["groups"], 3, 3, seed=5)
+    nc = np.arange(1, 9)
+    kw = dict(seed=1, return_scores=True)
+    a = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], precision="fp64", **kw)
+    b = lib.double_cv(d["X"], d["y"], outer, inner, nc, d["n_classes"], precision="int8", **kw)
+    assert np.array_equal(a["best_comp"], b["best_comp"])
+    assert np.array_equal(a["pred"], b["pred"])
+    assert slice_score_rel_err(b["inner_score"], a["inner_score"]) < 1e-5
+    assert cv_labels_match(b["inner_pred"], a["inner_pred"], np.transpose(a["inner_score"], (2, 1, 0, 3)), 1e-5)[0]
+    h = lib.x_upload(d["X"])
+    try:
+        r = lib.double_cv_resident(h, d["X"].shape[0], d["y"], outer, inner, nc, d["n_classes"], seed=1,
+                                   precision="int8")
+    finally:
+        lib.x_free(h)
+    assert np.array_equal(r["best_comp"], b["best_comp"])
+    assert np.array_equal(r["pred"], b["pred"])
+    assert np.max(np.abs(r["inner_accuracy"] - b["inner_accuracy"])) <= 2.0 / d["X"].shape[0]

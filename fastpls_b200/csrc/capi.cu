@@ -897,11 +897,9 @@ __global__ void widen_f32_kernel(const float* __restrict__ src, size_t total, do
     dst[t] = static_cast<double>(src[t]);
 }
 
-// A caller's matrix (FP64, or FP32 widened exactly) as a fresh FP64 device copy.
-double* upload_widened(const void* X, bool f32, size_t count) {
+// An FP32 device matrix widened exactly into a fresh FP64 copy.
+double* widen_on_device(const float* d32, size_t count) {
   Context& ctx = Context::get();
-  if (!f32) return upload(static_cast<const double*>(X), count);
-  const float* d32 = upload(static_cast<const float*>(X), count);
   double* d = ctx.arena.alloc_n<double>(count ? count : 1);
   if (count) {
     widen_f32_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(d32, count, d);
@@ -910,6 +908,41 @@ double* upload_widened(const void* X, bool f32, size_t count) {
   }
   return d;
 }
+
+// A caller's matrix (FP64, or FP32 widened exactly) as a fresh FP64 device copy.
+double* upload_widened(const void* X, bool f32, size_t count) {
+  if (!f32) return upload(static_cast<const double*>(X), count);
+  return widen_on_device(upload(static_cast<const float*>(X), count), count);
+}
+
+// A copy of a caller's matrix on the copy stream, queued behind the work the
+// main stream has enqueued so far (so that an earlier upload keeps the whole
+// link), for a later step of the same call; wait() makes the main stream wait
+// for it.  A call that leaves early (an error) waits for the copy on the host,
+// so that no copy still writes into arena memory the next call reuses.
+struct SideUpload {
+  void* dst = nullptr;
+  bool pending = false;
+  SideUpload(const void* src, size_t bytes) {
+    if (!bytes) return;
+    Context& ctx = Context::get();
+    dst = ctx.arena.alloc_n<char>(bytes);
+    FPLS_CUDA(cudaEventRecord(ctx.copy_event(0), ctx.stream));
+    FPLS_CUDA(cudaStreamWaitEvent(ctx.copy, ctx.copy_event(0), 0));
+    FPLS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx.copy));
+    FPLS_CUDA(cudaEventRecord(ctx.copy_event(1), ctx.copy));
+    pending = true;
+  }
+  void wait() {
+    if (!pending) return;
+    Context& ctx = Context::get();
+    FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.copy_event(1), 0));
+    pending = false;
+  }
+  ~SideUpload() {
+    if (pending) cudaEventSynchronize(Context::get().copy_event(1));
+  }
+};
 
 }  // namespace
 
@@ -940,6 +973,8 @@ int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const doubl
     // one upload of each matrix for the whole pipeline
     double* dX = upload_widened(Xtrain, f32, (size_t)n * p);
     double* dY = upload(Ytrain, (size_t)n * m);
+    // the test rows cross the link while the fit runs
+    SideUpload xt_up(Xtest, ntest > 0 ? (size_t)ntest * p * (f32 ? sizeof(float) : sizeof(double)) : 0);
     pt.mark("X, Y to FP64");
     int K0 = 0;
     double* dR = nullptr;
@@ -1038,7 +1073,9 @@ int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const doubl
     lda_outputs_to_host(d, n_classes, K0, U, lda_means, lda_linear, lda_constants, lda_priors);
     pt.mark("LDA outputs to host");
     if (ntest > 0) {
-      const double* dXt = upload_widened(Xtest, f32, (size_t)ntest * p);
+      xt_up.wait();
+      const double* dXt = f32 ? widen_on_device(static_cast<const float*>(xt_up.dst), (size_t)ntest * p)
+                              : static_cast<const double*>(xt_up.dst);
       const double* dRp = upload(hRp.data(), (size_t)p * K0);
       const double* doff = upload(hoff.data(), K0);
       int* dpred = ctx.arena.alloc_n<int>((size_t)ntest * L);

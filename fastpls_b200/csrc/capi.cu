@@ -915,34 +915,6 @@ double* upload_widened(const void* X, bool f32, size_t count) {
   return widen_on_device(upload(static_cast<const float*>(X), count), count);
 }
 
-// A copy of a caller's matrix on the copy stream, queued behind the work the
-// main stream has enqueued so far (so that an earlier upload keeps the whole
-// link), for a later step of the same call; wait() makes the main stream wait
-// for it.  A call that leaves early (an error) waits for the copy on the host,
-// so that no copy still writes into arena memory the next call reuses.
-struct SideUpload {
-  void* dst = nullptr;
-  bool pending = false;
-  SideUpload(const void* src, size_t bytes) {
-    if (!bytes) return;
-    Context& ctx = Context::get();
-    dst = ctx.arena.alloc_n<char>(bytes);
-    FPLS_CUDA(cudaEventRecord(ctx.copy_event(0), ctx.stream));
-    FPLS_CUDA(cudaStreamWaitEvent(ctx.copy, ctx.copy_event(0), 0));
-    FPLS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx.copy));
-    FPLS_CUDA(cudaEventRecord(ctx.copy_event(1), ctx.copy));
-    pending = true;
-  }
-  void wait() {
-    if (!pending) return;
-    Context& ctx = Context::get();
-    FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.copy_event(1), 0));
-    pending = false;
-  }
-  ~SideUpload() {
-    if (pending) cudaEventSynchronize(Context::get().copy_event(1));
-  }
-};
 
 }  // namespace
 
@@ -974,7 +946,7 @@ int fpls_pls_lda(const void* Xtrain, int x_is_float32, int n, int p, const doubl
     double* dX = upload_widened(Xtrain, f32, (size_t)n * p);
     double* dY = upload(Ytrain, (size_t)n * m);
     // the test rows cross the link while the fit runs
-    SideUpload xt_up(Xtest, ntest > 0 ? (size_t)ntest * p * (f32 ? sizeof(float) : sizeof(double)) : 0);
+    capi::SideUpload xt_up(Xtest, ntest > 0 ? (size_t)ntest * p * (f32 ? sizeof(float) : sizeof(double)) : 0);
     pt.mark("X, Y to FP64");
     int K0 = 0;
     double* dR = nullptr;

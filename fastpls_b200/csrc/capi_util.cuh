@@ -49,5 +49,37 @@ void download(T* host, const T* dev, size_t n) {
   if (host && n) d2h(host, dev, n * sizeof(T));
 }
 
+// A copy of a caller's matrix (host or device) on the copy stream, queued
+// behind the work the main stream has enqueued so far (so that an earlier
+// upload keeps the whole link), for a later step of the same call; wait()
+// makes the main stream wait for it.  A call that leaves early (an error)
+// waits for the copy on the host, so that no copy still writes into arena
+// memory the next call reuses.  Uses copy events 0 and 1 of the context.
+struct SideUpload {
+  void* dst = nullptr;
+  bool pending = false;
+  SideUpload(const void* src, size_t bytes) {
+    if (!bytes) return;
+    Context& ctx = Context::get();
+    dst = ctx.arena.alloc_n<char>(bytes);
+    FPLS_CUDA(cudaEventRecord(ctx.copy_event(0), ctx.stream));
+    FPLS_CUDA(cudaStreamWaitEvent(ctx.copy, ctx.copy_event(0), 0));
+    FPLS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx.copy));
+    FPLS_CUDA(cudaEventRecord(ctx.copy_event(1), ctx.copy));
+    pending = true;
+  }
+  SideUpload(const SideUpload&) = delete;
+  SideUpload& operator=(const SideUpload&) = delete;
+  void wait() {
+    if (!pending) return;
+    Context& ctx = Context::get();
+    FPLS_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.copy_event(1), 0));
+    pending = false;
+  }
+  ~SideUpload() {
+    if (pending) cudaEventSynchronize(Context::get().copy_event(1));
+  }
+};
+
 }  // namespace capi
 }  // namespace fpls

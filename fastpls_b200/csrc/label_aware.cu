@@ -325,7 +325,8 @@ LabelAwareFit label_aware_fit(const void* dX, bool f32, int n, int p, const int*
 void label_aware_cknn_device(const void* dX, const void* dXtest, bool f32, int n, int ntest, int p,
                              const int* dy, const int* y_host, int m, int ncomp, int scaling, int svd_method,
                              int oversample, int power_iters, unsigned int seed, int knn_k, double tau,
-                             double alpha, int top_m, int top_k, int* d_ti, double* d_ts) {
+                             double alpha, int top_m, int top_k, int* d_ti, double* d_ts,
+                             capi::SideUpload* xtest_copy) {
   Context& ctx = Context::get();
   const std::vector<int> nc = cap_plssvd_ncomp(&ncomp, 1, n, p, m, nullptr);
   LabelAwareFit f = label_aware_fit(dX, f32, n, p, dy, y_host, m, nc, scaling, svd_method, oversample,
@@ -338,6 +339,7 @@ void label_aware_cknn_device(const void* dX, const void* dXtest, bool f32, int n
   candidate_centroids_device(Tn, n, K, dy, m, cent);
   pt.mark("train scores + centroids");
   double* Xc = ctx.arena.alloc_n<double>((size_t)ntest * p);
+  if (xtest_copy) xtest_copy->wait();
   const int g = std::max(1, std::min(ceil_div((long long)ntest * p, 256), 8 * ctx.sm_count));
   if (f32)
     center_to_f64_kernel<float><<<g, 256, 0, ctx.stream>>>(static_cast<const float*>(dXtest), ntest, p, f.mX,
@@ -426,16 +428,16 @@ int fpls_label_aware_cknn(const void* Xtrain, int x_is_float32, int n, int p, co
     ctx.begin_call();
     const size_t es = x_is_float32 ? sizeof(float) : sizeof(double);
     void* dX = ctx.arena.alloc_n<char>((size_t)n * p * es);
-    void* dXt = ctx.arena.alloc_n<char>((size_t)ntest * p * es);
     h2d(dX, Xtrain, (size_t)n * p * es);
-    h2d(dXt, Xtest, (size_t)ntest * p * es);
     const int* dy = upload(y_codes, n);
+    // the test rows cross the link while the fit runs
+    capi::SideUpload xt(Xtest, (size_t)ntest * p * es);
     const int tk = std::max(1, std::min(top_k, m));
     int* d_ti = ctx.arena.alloc_n<int>((size_t)ntest * tk);
     double* d_ts = ctx.arena.alloc_n<double>((size_t)ntest * tk);
-    label_aware_cknn_device(dX, dXt, x_is_float32 != 0, n, ntest, p, dy, y_codes, m, ncomp, scaling,
+    label_aware_cknn_device(dX, xt.dst, x_is_float32 != 0, n, ntest, p, dy, y_codes, m, ncomp, scaling,
                             svd_method, oversample, power_iters, static_cast<unsigned int>(seed), knn_k,
-                            tau, alpha, top_m, top_k, d_ti, d_ts);
+                            tau, alpha, top_m, top_k, d_ti, d_ts, &xt);
     d2h(top_index, d_ti, (size_t)ntest * tk * sizeof(int));
     d2h(top_score, d_ts, (size_t)ntest * tk * sizeof(double));
     ctx.sync();
@@ -472,7 +474,7 @@ int fpls_label_aware_cknn_resident(int xtrain_handle, const int* y_codes, int m,
     double* d_ts = ctx.arena.alloc_n<double>((size_t)te.n * tk);
     label_aware_cknn_device(tr.ptr, te.ptr, tr.f32, tr.n, te.n, tr.p, dy, y_codes, m, ncomp, scaling,
                             svd_method, oversample, power_iters, static_cast<unsigned int>(seed), knn_k,
-                            tau, alpha, top_m, top_k, d_ti, d_ts);
+                            tau, alpha, top_m, top_k, d_ti, d_ts, nullptr);
     d2h(top_index, d_ti, (size_t)te.n * tk * sizeof(int));
     d2h(top_score, d_ts, (size_t)te.n * tk * sizeof(double));
     ctx.sync();

@@ -395,10 +395,15 @@ __device__ __forceinline__ double warp_max(double v) {
 }
 
 // One block per plane row j: the scale exponent from the largest |X[:, j]|,
-// then the S digits of every entry (zeros in the padding).
-__global__ void ozaki_split_kernel(const double* __restrict__ X, int klen, int cols, int ldx,
-                                   int8_t* __restrict__ P, int ldk, size_t plane_stride, int S,
-                                   double* __restrict__ scale) {
+// then the S digits of every entry (zeros in the padding).  Each thread takes
+// four consecutive entries per pass and writes one 32-bit word per plane; the
+// digits of a = x 2^-e (|a| < 1) are the 7-bit fields of trunc(a 2^(7S)), most
+// significant first, with the sign of a (the same digits as S rounds of
+// "times 128, take the integer part").
+template <int S>
+__global__ void __launch_bounds__(256) ozaki_split_kernel(const double* __restrict__ X, int klen, int cols,
+                                                          int ldx, int8_t* __restrict__ P, int ldk,
+                                                          size_t plane_stride, double* __restrict__ scale) {
   __shared__ double red[32];
   __shared__ int bad_any;
   const int j = blockIdx.x;
@@ -431,16 +436,29 @@ __global__ void ozaki_split_kernel(const double* __restrict__ X, int klen, int c
   e = max(-1000, min(1000, e));
   const double inv = pow2i(-e);
   if (threadIdx.x == 0) scale[j] = bad_any ? __longlong_as_double(0x7ff8000000000000ll) : pow2i(e);
+  const double lift = static_cast<double>(1ll << (7 * S));
   int8_t* row = P + static_cast<size_t>(j) * ldk;
-  for (int i = threadIdx.x; i < ldk; i += blockDim.x) {
-    double a = (j < cols && i < klen) ? x[i] * inv : 0.0;
-    if (!isfinite(a)) a = 0.0;
-    for (int s = 0; s < S; ++s) {
-      a *= 128.0;
-      const double d = trunc(a);
-      a -= d;
-      row[static_cast<size_t>(s) * plane_stride + i] = static_cast<int8_t>(static_cast<int>(d));
+  for (int i0 = 4 * threadIdx.x; i0 < ldk; i0 += 4 * blockDim.x) {
+    uint32_t wd[S];
+#pragma unroll
+    for (int s2 = 0; s2 < S; ++s2) wd[s2] = 0u;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u;
+      double a = (j < cols && i < klen) ? x[i] * inv : 0.0;
+      if (!isfinite(a)) a = 0.0;
+      const long long q = __double2ll_rz(a * lift);
+      const unsigned long long mag = static_cast<unsigned long long>(q < 0 ? -q : q);
+#pragma unroll
+      for (int s2 = 0; s2 < S; ++s2) {
+        int d = static_cast<int>((mag >> (7 * (S - 1 - s2))) & 127ull);
+        if (q < 0) d = -d;
+        wd[s2] |= (static_cast<uint32_t>(d) & 0xffu) << (8 * u);
+      }
     }
+#pragma unroll
+    for (int s2 = 0; s2 < S; ++s2)
+      *reinterpret_cast<uint32_t*>(row + static_cast<size_t>(s2) * plane_stride + i0) = wd[s2];
   }
 }
 
@@ -1005,9 +1023,17 @@ OzakiPlanes ozaki_alloc(int rows, int k, int slices) {
 
 void ozaki_split(const double* X, int ldx, const OzakiPlanes& out) {
   Context& ctx = Context::get();
-  ozaki_split_kernel<<<out.rows_pad, 256, 0, ctx.stream>>>(X, out.k, out.rows, ldx, out.data, out.ldk,
-                                                           static_cast<size_t>(out.rows_pad) * out.ldk,
-                                                           out.slices, out.scale);
+  const size_t stride = static_cast<size_t>(out.rows_pad) * out.ldk;
+  switch (out.slices) {
+    case 4: ozaki_split_kernel<4><<<out.rows_pad, 256, 0, ctx.stream>>>(X, out.k, out.rows, ldx, out.data, out.ldk,
+                                                                        stride, out.scale); break;
+    case 5: ozaki_split_kernel<5><<<out.rows_pad, 256, 0, ctx.stream>>>(X, out.k, out.rows, ldx, out.data, out.ldk,
+                                                                        stride, out.scale); break;
+    case 6: ozaki_split_kernel<6><<<out.rows_pad, 256, 0, ctx.stream>>>(X, out.k, out.rows, ldx, out.data, out.ldk,
+                                                                        stride, out.scale); break;
+    default: ozaki_split_kernel<7><<<out.rows_pad, 256, 0, ctx.stream>>>(X, out.k, out.rows, ldx, out.data, out.ldk,
+                                                                         stride, out.scale); break;
+  }
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }

@@ -246,16 +246,20 @@ constexpr int kReduceSplit = 8;
 
 // tile_segs (when not null) lists each tile's segment ids in contraction
 // order; otherwise a tile's segments are the consecutive ids s0 .. s1 - 1.
+// skip_empty (upper-triangle plans, whose lower tiles are mirrored afterwards):
+// tiles without segments are left as they are.
 template <int TN>
 __global__ void split_reduce_kernel(const float* __restrict__ part, const int* __restrict__ tile_seg,
                                     const int* __restrict__ tile_segs, int n_tiles_n, int M, int N,
-                                    double alpha, double beta, double* __restrict__ C, int ldc) {
+                                    double alpha, double beta, double* __restrict__ C, int ldc,
+                                    int skip_empty) {
   constexpr int BN = TN;
   // kReduceSplit blocks per tile, each covering BN / kReduceSplit columns.
   const int tile = blockIdx.x / kReduceSplit;
   const int part_idx = blockIdx.x % kReduceSplit;
   const int mt = tile / n_tiles_n, nt = tile % n_tiles_n;
   const int s0 = tile_seg[tile], s1 = tile_seg[tile + 1];
+  if (skip_empty && s0 == s1) return;
   const int e0 = part_idx * (BM * BN / kReduceSplit), e1 = e0 + BM * BN / kReduceSplit;
   for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
     const int mm = e % BM, nn = e / BM;
@@ -662,10 +666,10 @@ void split_gemm_run(const SplitPair& A, const SplitPair& B, int M, int N, int K,
   }
   if (g.bn == BN_SYM)
     split_reduce_kernel<BN_SYM><<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, s.tile_segs, g.ntn, M, N,
-                                                                         alpha, beta, C, ldc);
+                                                                         alpha, beta, C, ldc, upper_plan ? 1 : 0);
   else
     split_reduce_kernel<BN><<<g.tiles * kReduceSplit, 256, 0, st>>>(s.part, s.tile_begin, s.tile_segs, g.ntn, M, N,
-                                                                     alpha, beta, C, ldc);
+                                                                     alpha, beta, C, ldc, upper_plan ? 1 : 0);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
@@ -727,18 +731,31 @@ void split_gemm(const SplitPair& A, const SplitPair& B, int M, int N, int K, dou
                  ctx.profile ? &ctx : nullptr);
 }
 
-__global__ void mirror_upper_kernel(double* K, int n) {
-  const size_t total = (size_t)n * n;
-  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-    const int i = static_cast<int>(t % n), j = static_cast<int>(t / n);
-    if (i > j) K[t] = K[j + (size_t)i * n];
+// Block (ti, tj), ti <= tj, reads the upper 32 x 32 tile (rows ti, columns tj)
+// with column reads, and writes its transpose into the lower tile (rows tj,
+// columns ti) with column writes; a diagonal block writes only below the
+// diagonal.  Blocks below the diagonal have nothing to do.
+__global__ void __launch_bounds__(256) mirror_upper_kernel(double* K, int n) {
+  __shared__ double t[32][33];
+  const int ti = blockIdx.x, tj = blockIdx.y;
+  if (ti > tj) return;
+  const int x = threadIdx.x & 31, y0 = threadIdx.x >> 5;
+  for (int y = y0; y < 32; y += 8) {
+    const int r = ti * 32 + x, c = tj * 32 + y;
+    if (r < n && c < n) t[y][x] = K[r + static_cast<size_t>(c) * n];
+  }
+  __syncthreads();
+  for (int y = y0; y < 32; y += 8) {
+    const int r = tj * 32 + x, c = ti * 32 + y;   // lower entry (r, c) = upper entry (c, r)
+    if (r < n && c < n && r > c) K[r + static_cast<size_t>(c) * n] = t[x][y];
   }
 }
 
 // K[i, j] = K[j, i] for i > j (n x n).
 void mirror_upper(double* K, int n) {
   Context& ctx = Context::get();
-  mirror_upper_kernel<<<4 * ctx.sm_count, 256, 0, ctx.stream>>>(K, n); ::fpls::note_launch();
+  const int nt = (n + 31) / 32;
+  mirror_upper_kernel<<<dim3(nt, nt), 256, 0, ctx.stream>>>(K, n); ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
 }
 

@@ -260,18 +260,29 @@ __global__ void split_reduce_kernel(const float* __restrict__ part, const int* _
   const int mt = tile / n_tiles_n, nt = tile % n_tiles_n;
   const int s0 = tile_seg[tile], s1 = tile_seg[tile + 1];
   if (skip_empty && s0 == s1) return;
+  // four consecutive rows of one column per thread (16-byte partial loads),
+  // the segments summed in contraction order
   const int e0 = part_idx * (BM * BN / kReduceSplit), e1 = e0 + BM * BN / kReduceSplit;
-  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+  for (int e = e0 + 4 * threadIdx.x; e < e1; e += 4 * blockDim.x) {
     const int mm = e % BM, nn = e / BM;
     const int m = mt * BM + mm, n = nt * BN + nn;
     if (m >= M || n >= N) continue;
-    double acc = 0.0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const float* pc = part + static_cast<size_t>(nn) * BM + mm;
     for (int j = s0; j < s1; ++j) {
       const int s = tile_segs ? tile_segs[j] : j;
-      acc += static_cast<double>(part[(static_cast<size_t>(s) * BN + nn) * BM + mm]);
+      const float4 v = *reinterpret_cast<const float4*>(pc + static_cast<size_t>(s) * BN * BM);
+      acc[0] += static_cast<double>(v.x);
+      acc[1] += static_cast<double>(v.y);
+      acc[2] += static_cast<double>(v.z);
+      acc[3] += static_cast<double>(v.w);
     }
-    double* cp = C + m + static_cast<size_t>(n) * ldc;
-    *cp = (beta == 0.0) ? alpha * acc : alpha * acc + beta * *cp;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (m + u >= M) break;
+      double* cp = C + m + u + static_cast<size_t>(n) * ldc;
+      *cp = (beta == 0.0) ? alpha * acc[u] : alpha * acc[u] + beta * *cp;
+    }
   }
 }
 

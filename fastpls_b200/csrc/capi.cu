@@ -1417,13 +1417,16 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
                                                                   d_best, d_bcomp);
     ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
-    std::vector<double> acc_all((size_t)Ko * L);
-    std::vector<int> bcomp_all(Ko);
-    download(acc_all.data(), d_acc, (size_t)Ko * L);
-    download(bcomp_all.data(), d_bcomp, Ko);
     int* d_out = ctx.arena.alloc_n<int>(n);
     gather_outer_pred_kernel<<<ceil_div(n, 256), 256, 0, ctx.stream>>>(res.d_pred, d_slot, d_best, d_fb, S, L, n, d_out); ::fpls::note_launch();
     FPLS_CHECK_LAUNCH();
+    // the accuracies, chosen ncomp and outer predictions through page-locked
+    // staging: asynchronous copies, one synchronisation below
+    const size_t b_acc = (size_t)Ko * L * sizeof(double), b_bc = (size_t)Ko * sizeof(int), b_out = (size_t)n * sizeof(int);
+    char* stg = ctx.host_staging(b_acc + b_bc + b_out);
+    d2h(stg, d_acc, b_acc);
+    d2h(stg + b_acc, d_bcomp, b_bc);
+    d2h(stg + b_acc + b_bc, d_out, b_out);
     double* d_oscore = nullptr;
     if (outer_score) {
       d_oscore = ctx.arena.alloc_n<double>((size_t)n * m);
@@ -1444,17 +1447,24 @@ static void double_cv_impl(const void* X, int x_is_float32, bool x_on_device, in
         download(inner_score + (size_t)ids[s] * L * n * m, res.d_score + (size_t)s * L * n * m, (size_t)L * n * m);
     std::vector<int> pred_all;
     if (outer_ids) {
-      pred_all.resize(n);
-      download(pred_all.data(), d_out, n);
       if (inner_pred)
         for (int s = 0; s < S; ++s)
           download(inner_pred + (size_t)ids[s] * L * n, res.d_pred + (size_t)s * L * n, (size_t)L * n);
     } else {
-      download(outer_pred, d_out, n);
       if (inner_pred) download(inner_pred, res.d_pred, (size_t)Ko * L * n);
     }
     pt.mark("ncomp + outer");
     ctx.sync();
+    std::vector<double> acc_all((size_t)Ko * L);
+    std::vector<int> bcomp_all(Ko);
+    std::memcpy(acc_all.data(), stg, b_acc);
+    std::memcpy(bcomp_all.data(), stg + b_acc, b_bc);
+    if (outer_ids) {
+      pred_all.resize(n);
+      std::memcpy(pred_all.data(), stg + b_acc + b_bc, b_out);
+    } else if (outer_pred) {
+      std::memcpy(outer_pred, stg + b_acc + b_bc, b_out);
+    }
     for (int s = 0; s < S; ++s) {
       const int o = ids[s];
       if (best_comp) best_comp[o] = bcomp_all[o];

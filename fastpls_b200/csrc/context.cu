@@ -142,6 +142,20 @@ void Context::release() {
   arena.release();
   for (auto& b : splitk) cudaFree(b.ptr);
   splitk.clear();
+  if (staging) cudaFreeHost(staging);
+  staging = nullptr;
+  staging_cap = 0;
+}
+
+char* Context::host_staging(size_t bytes) {
+  if (bytes <= staging_cap) return staging;
+  // grow: earlier copies into the old buffer must have landed
+  FPLS_CUDA(cudaStreamSynchronize(stream));
+  if (staging) FPLS_CUDA(cudaFreeHost(staging));
+  staging = nullptr;
+  staging_cap = std::max(bytes, std::max<size_t>(2 * staging_cap, 1 << 16));
+  FPLS_CUDA(cudaMallocHost(&staging, staging_cap));
+  return staging;
 }
 
 double* Context::splitk_workspace(cudaStream_t st, size_t elems) {

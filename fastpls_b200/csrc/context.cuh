@@ -74,6 +74,12 @@ struct Context {
   struct StreamBuffer { cudaStream_t stream; double* ptr; size_t cap; };
   std::vector<StreamBuffer> splitk;
   double* splitk_workspace(cudaStream_t st, size_t elems);
+  // Page-locked host staging for the small results of a call (grown on
+  // demand, kept across calls): copies into it stay asynchronous, so a call
+  // gathers its results with one synchronisation instead of one per copy.
+  char* staging = nullptr;
+  size_t staging_cap = 0;
+  char* host_staging(size_t bytes);
 
   // Row-sharded fit in progress (null otherwise): the caller's all-reduce
   // and the row count over all ranks.

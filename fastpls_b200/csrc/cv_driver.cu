@@ -161,16 +161,20 @@ __global__ void pred_counts_kernel(const int* __restrict__ pred, int L, int n, c
 // Class predictions of the test rows of every fit for every ncomp slice from the
 // kept scores: y_a = sum_{b<=a} (t_b[i] / ||t_b||) q_b + mY_f, label = first argmax.
 // MB bounds the class count so that the running scores stay in registers.
+// Thread k of fit f takes the fit's k-th test row (tidx[f * tstride + k], k <
+// tcnt[f]), so no warp runs for training rows.
 template <int MB>
 __global__ void cv_predict_kernel(int F, int n, int m, int K, int L, const int* __restrict__ ncomp,
-                                  const int* __restrict__ order, const uint8_t* __restrict__ test,
+                                  const int* __restrict__ order, const int* __restrict__ tidx,
+                                  const int* __restrict__ tcnt, int tstride,
                                   const int* __restrict__ group, const double* __restrict__ Tkeep,
                                   const double* __restrict__ tnorm, const double* __restrict__ Q,
                                   const int* __restrict__ ncomp_done, const double* __restrict__ mYf,
                                   int* __restrict__ pred, double* __restrict__ score) {
   const int f = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !test[(size_t)f * n + i]) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= tcnt[f]) return;
+  const int i = tidx[(size_t)f * tstride + k];
   const int done = ncomp_done[f];
   const int g = group[f];
   double y[MB];
@@ -441,7 +445,7 @@ void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, cons
   double* x0 = px.x0;
   std::unique_ptr<XOperator>& xop = px.xop;
   std::vector<uint8_t> tr((size_t)Fa * n), te((size_t)Fa * n);
-  std::vector<int> grp(Fa), ntrain(Fa);
+  std::vector<int> grp(Fa), ntrain(Fa), tcnt(Fa, 0);
   std::vector<double> inv_nf(Fa), mYf((size_t)Fa * m), mYall(m, 0.0), dY((size_t)Fa * m);
   for (int i = 0; i < n; ++i) mYall[y[i] - 1] += 1.0 / n;
   for (int a = 0; a < Fa; ++a) {
@@ -449,6 +453,7 @@ void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, cons
     std::copy(fs.train.begin() + (size_t)f * n, fs.train.begin() + (size_t)(f + 1) * n, tr.begin() + (size_t)a * n);
     std::copy(fs.test.begin() + (size_t)f * n, fs.test.begin() + (size_t)(f + 1) * n, te.begin() + (size_t)a * n);
     grp[a] = fs.group[f];
+    for (int i = 0; i < n; ++i) tcnt[a] += te[(size_t)a * n + i] != 0;
     int nt = 0;
     if (!fs.n_train.empty()) {
       nt = fs.n_train[f];
@@ -464,7 +469,6 @@ void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, cons
     }
   }
   uint8_t* d_tr = ar.alloc_n<uint8_t>(tr.size());
-  uint8_t* d_te = ar.alloc_n<uint8_t>(te.size());
   int* d_grp = ar.alloc_n<int>(Fa);
   int* d_nt = ar.alloc_n<int>(Fa);
   double* d_inv = ar.alloc_n<double>(Fa);
@@ -476,7 +480,6 @@ void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, cons
   std::vector<int> lab0(n);
   for (int i = 0; i < n; ++i) lab0[i] = y[i] - 1;
   h2d(d_tr, tr.data(), tr.size());
-  h2d(d_te, te.data(), te.size());
   h2d(d_grp, grp.data(), Fa * sizeof(int));
   h2d(d_nt, ntrain.data(), Fa * sizeof(int));
   h2d(d_inv, inv_nf.data(), Fa * sizeof(double));
@@ -576,16 +579,29 @@ void run_batched(const CvFitSet& fs, const int* y, const int* ncomp, int L, cons
     pt.mark("simpls");
   }
   int* d_pred = res.d_pred;
-  const dim3 pgrid(ceil_div(n, 128), Fa);
+  // every fit's test rows as a compact list (the prediction threads)
+  const int tstride = std::max(1, *std::max_element(tcnt.begin(), tcnt.end()));
+  std::vector<int> tidx((size_t)Fa * tstride, 0);
+  for (int a = 0; a < Fa; ++a) {
+    int k = 0;
+    for (int i = 0; i < n; ++i)
+      if (te[(size_t)a * n + i]) tidx[(size_t)a * tstride + k++] = i;
+  }
+  int* d_tidx = ar.alloc_n<int>(tidx.size());
+  int* d_tcnt = ar.alloc_n<int>(Fa);
+  h2d(d_tidx, tidx.data(), tidx.size() * sizeof(int));
+  h2d(d_tcnt, tcnt.data(), Fa * sizeof(int));
+  const dim3 pgrid(ceil_div(tstride, 128), Fa);
   if (m <= 8)
-    cv_predict_kernel<8><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_te, d_grp, Tko, tno, Qo, ncd,
-                                                        d_mYf, d_pred, res.d_score);
+    cv_predict_kernel<8><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_tidx, d_tcnt, tstride, d_grp,
+                                                        Tko, tno, Qo, ncd, d_mYf, d_pred, res.d_score);
   else if (m <= 32)
-    cv_predict_kernel<32><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_te, d_grp, Tko, tno, Qo, ncd,
-                                                         d_mYf, d_pred, res.d_score);
+    cv_predict_kernel<32><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_tidx, d_tcnt, tstride, d_grp,
+                                                         Tko, tno, Qo, ncd, d_mYf, d_pred, res.d_score);
   else
-    cv_predict_kernel<kMaxClassesCv><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_te, d_grp, Tko,
-                                                                    tno, Qo, ncd, d_mYf, d_pred, res.d_score);
+    cv_predict_kernel<kMaxClassesCv><<<pgrid, 128, 0, ctx.stream>>>(Fa, n, m, K, L, d_nc, d_order, d_tidx, d_tcnt,
+                                                                    tstride, d_grp, Tko, tno, Qo, ncd, d_mYf, d_pred,
+                                                                    res.d_score);
   ::fpls::note_launch();
   FPLS_CHECK_LAUNCH();
   pt.mark("predict");

@@ -42,3 +42,22 @@ def test_level_sums_fit_int32():
     # 64 * 128 terms of 127^2 each
     for s in range(4, 8):
         assert s * 64 * 128 * 127 ** 2 < 2 ** 31
+
+
+@pytest.mark.parametrize("slices", [4, 5, 6, 7])
+def test_digit_fields_equal_iterated_digits(slices):
+    """The split kernels take each entry's digits as the 7-bit fields of one
+    truncation q = trunc(a 2^(7S)) (a = x 2^-e, |a| < 1), most significant
+    first, with the sign of a.  They equal the S rounds of "times 128, take
+    the integer part" of the model, entry for entry."""
+    rng = np.random.default_rng(slices)
+    rows = rng.standard_normal((40, 300)) * np.exp(rng.normal(0.0, 4.0, size=(40, 1)))
+    rows[3, :7] = [0.0, -0.0, 1e-300, -1e-300, 2.0 ** -60, -(1.0 - 2.0 ** -53), 5e-324]
+    rows[4] = np.nextafter(1.0, 0.0) * np.sign(rng.standard_normal(300))
+    planes, scale = im.split_digits(rows, slices)
+    a = rows / scale[:, None]
+    q = np.trunc(a * 2.0 ** (7 * slices)).astype(np.int64)
+    mag, sign = np.abs(q), np.where(q < 0, -1, 1)
+    for s in range(slices):
+        field = sign * ((mag >> (7 * (slices - 1 - s))) & 127)
+        assert np.array_equal(field, planes[s]), f"plane {s}"

@@ -501,8 +501,41 @@ void gram_f64(const double* X, int n, int p, int ldx, double* K, int ldk) {
   gram_tiles_f64<false>(X, n, p, ldx, K, ldk);
 }
 
+namespace {
+// B (cols x rows, ld ldb) = A^T for A (rows x cols, ld lda), column-major both,
+// through 32 x 32 shared-memory tiles (column reads and column writes).
+__global__ void __launch_bounds__(256) transpose_f64_kernel(const double* __restrict__ A, int rows, int cols,
+                                                            int lda, double* __restrict__ B, int ldb) {
+  __shared__ double t[32][33];
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int x = threadIdx.x & 31, y0 = threadIdx.x >> 5;
+  for (int y = y0; y < 32; y += 8) {
+    const int r = r0 + x, c = c0 + y;
+    if (r < rows && c < cols) t[y][x] = A[r + static_cast<size_t>(c) * lda];
+  }
+  __syncthreads();
+  for (int y = y0; y < 32; y += 8) {
+    const int c = c0 + x, r = r0 + y;   // B(c, r) = A(r, c)
+    if (r < rows && c < cols) B[c + static_cast<size_t>(r) * ldb] = t[x][y];
+  }
+}
+}  // namespace
+
+// G = S^T S through a transposed copy of S (q x p), so that the Gram's DMMA
+// tiles read both operands in the layout of the row Gram X X^T (A along M,
+// B along N) instead of reading S^T in place, for one extra pass over S.
 void gram_t_f64(const double* S, int p, int q, int lds, double* G, int ldg) {
-  gram_tiles_f64<true>(S, q, p, lds, G, ldg);
+  if (q <= 0) return;
+  if (p <= 0) {
+    gram_tiles_f64<true>(S, q, p, lds, G, ldg);
+    return;
+  }
+  Context& ctx = Context::get();
+  double* St = ctx.arena.alloc_n<double>(static_cast<size_t>(q) * p);
+  transpose_f64_kernel<<<dim3(ceil_div(p, 32), ceil_div(q, 32)), 256, 0, ctx.stream>>>(S, p, q, lds, St, q);
+  ::fpls::note_launch();
+  FPLS_CHECK_LAUNCH();
+  gram_tiles_f64<false>(St, q, p, q, G, ldg);
 }
 
 void gemv(bool trans, int rows, int cols, double alpha, const double* A, int lda, const double* x,
